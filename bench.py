@@ -1,0 +1,347 @@
+"""Benchmark of the GPU hot path: the statics of the 580 x 580 shell plate (2,021,880 equations), factorisation of K
+in the reference's symbolic order plus the solve of a 64-column load block, to a relative residual of 1e-10 per column,
+on one B200 (replicas on N GPUs: every rank factorises and solves its own copy; no data-path collective).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gpu|reference] [--workload plate580|plate100]
+
+Prints one JSON line (rank 0). `value` is the device time of one step with its inputs resident in HBM (factorise +
+solve + refinement), seconds; `e2e` the same step through the C ABI with host buffers (pinned), the copies included;
+`roofline` the dominant kernel of a profiled factorisation against the measured peak; `cpu_baseline` the reference's
+own factorisation and solve (oracle/_ref, built from its sources) on the host cores, on the same matrix.
+`--impl reference` times that CPU path alone on the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(ROOT, "tests", "golden", "orderings")
+
+WORKLOADS = {
+    # name: (plate size, right-hand sides)
+    "plate580": (580, 64),
+    "plate100": (100, 1),
+    "plate200": (200, 64),
+}
+
+
+def parse():
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=["gpu", "reference"], default="gpu")
+    parser.add_argument("--workload", choices=sorted(WORKLOADS), default="plate580")
+    parser.add_argument("--tolerance", type=float, default=1.0e-10)
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-e2e", action="store_true")
+    return parser.parse_args()
+
+
+def load_workload(name):
+    """The plate model, the reference's node order and supernode partition (tests/golden/orderings, made by the
+    reference), the stiffness in that order and the load block."""
+    from o_o_solver_b200 import workloads
+
+    size, columns = WORKLOADS[name]
+    fixture = np.load(os.path.join(GOLDEN, f"plate{size}.npz"))
+    model = workloads.Model(workloads.PlateSpec(size, size))
+    order = fixture["node_order"]
+    csc = model.csc(order)
+    loads = model.loads(order, columns)
+    return model, fixture, csc, loads
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._thread = None
+
+    def __enter__(self):
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([v.strip() for v in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        sm_max = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 5 + k and "Active" in s[5 + k]
+                          and "Not" not in s[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(sm_max) if sm_max else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def fp64_gemm_peak(torch, device):
+    """The FP64 denominator: cuBLAS DGEMM (torch.matmul float64, 8192^3) throughput on this GPU, best of 5."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 0.0
+    for _ in range(5):
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record()
+        torch.matmul(a, b)
+        stop.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (start.elapsed_time(stop) / 1e3))
+    del a, b
+    torch.cuda.empty_cache()
+    return best / 1e12
+
+
+def cpu_baseline(fixture, csc, loads, threads, tolerance):
+    """The reference's factorisation + solve (oracle/_ref/liboos_ref.so) of the same matrix on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from o_o_solver_b200 import workloads
+
+    model_graph = fixture["_graph"]
+    sym = oracle.analyse(*model_graph, given_order=fixture["node_order"], threads=threads)
+    start = time.perf_counter()
+    factor = oracle.factorise(sym, csc.offsets, csc.rows, csc.values, threads=threads)
+    x = factor.solve(loads, threads=threads)
+    seconds = time.perf_counter() - start
+    r = loads - workloads.lower_csc_multiply(csc, x)
+    resid = float((np.linalg.norm(r, axis=0) / np.linalg.norm(loads, axis=0)).max())
+    return {"seconds": seconds, "factor_seconds": factor.seconds, "residual": resid,
+            "kernel": ["reference", "avx2", "avx512"][factor.kernel] if factor.kernel < 3 else str(factor.kernel)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    model, fixture, csc, loads = load_workload(args.workload)
+    fixture = dict(fixture)
+    fixture["_graph"] = (model.offsets, model.neighbours, model.weights)
+    threads = os.cpu_count() or 1
+    times = []
+    result = None
+    for step in range(args.warmup + args.steps):
+        result = cpu_baseline(fixture, csc, loads, threads, args.tolerance)
+        if step >= args.warmup:
+            times.append(result["seconds"])
+    value = statistics.median(times)
+    line = {
+        "metric": "plate statics factor+solve time (2M-dof, 64 RHS)" if args.workload == "plate580" else
+        f"{args.workload} statics factor+solve time",
+        "value": value, "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded loads on a generated shell plate)",
+        "config": {"workload": args.workload, "equations": int(csc.dimension), "rhs": int(loads.shape[1])},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "reference",
+                         "sample": f"full {args.workload} factor + {loads.shape[1]}-column solve, kernel family "
+                                   f"{result['kernel']}, residual {result['residual']:.2e}"},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+
+    from o_o_solver_b200 import FactorSolve, SupernodalFactor, SymbolicFactor, SymmetricCsc, linalg, workloads
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local_rank))
+
+    model, fixture, csc, loads = load_workload(args.workload)
+    n = csc.dimension
+    columns = loads.shape[1]
+    symbolic = SymbolicFactor.from_partition(model.offsets, model.neighbours, model.weights, fixture["node_order"],
+                                             fixture["first_position"], fixture["parent"])
+    factor = SupernodalFactor(symbolic, device=local_rank)
+    stream = torch.cuda.ExternalStream(factor.stream)
+    dev = torch.device("cuda", local_rank)
+    d_csc = SymmetricCsc(torch.from_numpy(csc.offsets).to(dev), torch.from_numpy(csc.rows).to(dev),
+                         torch.from_numpy(csc.values).to(dev))
+    d_loads = torch.from_numpy(np.ascontiguousarray(loads.T)).to(dev)  # (columns, n): columns contiguous
+    d_x = torch.empty_like(d_loads)
+    torch.cuda.synchronize()
+    solver = FactorSolve(factor)
+
+    def step():
+        factor.refactorise(d_csc)
+        with torch.cuda.stream(stream):
+            d_x.copy_(d_loads)
+        solver.solve(d_x.t())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        stop.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    seconds = start.elapsed_time(stop) / 1e3 / args.steps
+    if dist:
+        t = torch.tensor([seconds], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        seconds = float(t.item())
+
+    # Residual of the last step's solutions (host check).
+    x = d_x.t().cpu().numpy()
+    resid = float((np.linalg.norm(loads - workloads.lower_csc_multiply(csc, x), axis=0)
+                   / np.linalg.norm(loads, axis=0)).max())
+    factor_launches, solve_launches = factor.launch_counts(columns)
+    launches = args.steps * (factor_launches + solve_launches)
+
+    # End to end through the C ABI with host (pinned) buffers.
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+        h_offsets, h_rows, h_values = pin(csc.offsets), pin(csc.rows), pin(csc.values)
+        h_csc = SymmetricCsc(h_offsets, h_rows, h_values)
+        h_b = np.asfortranarray(loads)
+        h_x = torch.empty((columns, n), dtype=torch.float64).pin_memory().numpy().T
+        e2e_times = []
+        for k in range(max(1, min(3, args.steps)) + 1):
+            h_x[...] = h_b
+            t0 = time.perf_counter()
+            factor.refactorise(h_csc)
+            solver.solve(h_x)
+            if k > 0:
+                e2e_times.append(time.perf_counter() - t0)
+        h2d = csc.offsets.nbytes + csc.rows.nbytes + csc.values.nbytes + loads.nbytes
+        e2e = {"value": statistics.median(e2e_times), "unit": "s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(loads.nbytes)}
+
+    # Roofline of the dominant kernel: one profiled factorisation.
+    factor.profile(True)
+    factor.refactorise(d_csc)
+    stats = factor.kernel_stats()
+    factor.profile(False)
+    dominant = max(stats, key=lambda k: stats[k]["seconds"])
+    d = stats[dominant]
+    peaks, peak_source = measured_peaks()
+    compute_bound = dominant in ("panel_update", "update_matrix", "panel_rows", "diagonal_blocks")
+    if compute_bound:
+        fp64 = fp64_gemm_peak(torch, dev)
+        achieved = d["flops"] / d["seconds"] / 1e12
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64,
+                    "traffic": None, "kernel": dominant, "launches": d["launches"],
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor)",
+                    "share": d["seconds"] / sum(v["seconds"] for v in stats.values())}
+    else:
+        achieved = d["bytes"] / d["seconds"] / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": dominant,
+                    "launches": d["launches"], "peak_source": f"hbm_gbs ({peak_source})",
+                    "share": d["seconds"] / sum(v["seconds"] for v in stats.values())}
+    kernel_table = {k: {"ms": round(v["seconds"] * 1e3, 3), "launches": v["launches"],
+                        "tflops": round(v["flops"] / v["seconds"] / 1e12, 3) if v["seconds"] > 0 else None,
+                        "gbs": round(v["bytes"] / v["seconds"] / 1e9, 1) if v["seconds"] > 0 else None}
+                    for k, v in stats.items()}
+
+    baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            fixture = dict(fixture)
+            fixture["_graph"] = (model.offsets, model.neighbours, model.weights)
+            threads = os.cpu_count() or 1
+            cb = cpu_baseline(fixture, csc, loads, threads, args.tolerance)
+            baseline = {"value": cb["seconds"], "unit": "s", "cores": threads, "kind": "reference",
+                        "sample": f"one full {args.workload} factor + {columns}-column solve "
+                                  f"({cb['kernel']} kernels, factor {cb['factor_seconds']:.3f} s, "
+                                  f"residual {cb['residual']:.2e})"}
+        except Exception as error:  # the reference library is test infrastructure: absent, no baseline
+            baseline = {"value": None, "unit": "s", "cores": 0, "kind": "reference", "sample": f"unavailable: {error}"}
+
+    if rank == 0:
+        line = {
+            "metric": "plate statics factor+solve time (2M-dof, 64 RHS)" if args.workload == "plate580" else
+            f"{args.workload} statics factor+solve time",
+            "value": seconds / world, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": seconds * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded loads on a generated shell plate)",
+            "config": {"workload": args.workload, "equations": n, "rhs": columns, "form": "plain FP64",
+                       "flops_per_factor": symbolic.flop_count, "l2": "inputs larger than L2 (panels 6 GB)",
+                       "parallelism": f"replicas x{world}"},
+            "residual": resid, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
+            "kernels": kernel_table, "clocks": clocks.summary(), "cpu_baseline": baseline,
+            "factor_tflops": symbolic.flop_count / seconds / 1e12,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_gpu(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

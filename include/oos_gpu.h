@@ -1,0 +1,167 @@
+/* oos_gpu.h: the C ABI of the B200 implementation of O_o_Solver's numeric hot path, the supernodal multifrontal
+ * LDL^T factorisation and its solves (plain FP64 form).
+ *
+ * The entry points replace, one for one, the reference's C++ boundary of that path (paths within jcdulas/O_o_Solver):
+ *
+ *   oosgpu_symbolic_create        the SymbolicFactor a factorisation is given
+ *                                 (include/oos/linalg/symbolic/SymbolicFactor.hpp:37-126: firstColumn, columnCount,
+ *                                 rows, supernodes().parent)
+ *   oosgpu_symbolic_from_partition the row-structure step of SymbolicFactor::analyse
+ *                                 (src/linalg/symbolic/SymbolicFactor.cpp:227-290)
+ *   oosgpu_factorise              SupernodalFactor::factorise, positive definite mode
+ *                                 (include/oos/linalg/supernodal/SupernodalFactor.hpp:181-183)
+ *   oosgpu_factor_panel           SupernodalFactor::panel (SupernodalFactor.hpp:203)
+ *   oosgpu_solve                  FactorSolve::solve (include/oos/linalg/supernodal/FactorSolve.hpp:81)
+ *
+ * Conventions: plain pointers and sizes; `_device` variants take device pointers (the caller's stream order is the
+ * handle's stream, oosgpu_factor_stream), the others host pointers (copies included). Every call returns a status
+ * (OOSGPU_OK or an error code mapping one of the reference's exceptions) and leaves a message for
+ * oosgpu_last_error() on failure. The library owns its device memory; the caller owns every buffer it passes. One
+ * handle is used by one thread at a time (no internal locking), as the reference's factor is built by one thread.
+ */
+#ifndef OOS_GPU_H
+#define OOS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: each maps an exception of the reference's boundary. */
+enum
+{
+    OOSGPU_OK = 0,
+    OOSGPU_INVALID_ARGUMENT = 1, /* std::invalid_argument */
+    OOSGPU_MEMORY_BUDGET = 2,    /* base::MemoryBudgetError (device memory) */
+    OOSGPU_SINGULAR = 3,         /* base::SingularityError (zero pivot; ratio test with bail-out >= 0) */
+    OOSGPU_CANCELLED = 4,        /* base::OperationCancelledError */
+    OOSGPU_CUDA_ERROR = 5,       /* a CUDA runtime error (no counterpart: the reference runs on the CPU) */
+    OOSGPU_INTERNAL = 6,         /* base::InternalError */
+    OOSGPU_NOT_FACTORISED = 7,   /* std::logic_error: solve before factorise */
+    OOSGPU_SOLVER = 8            /* base::SolverError */
+};
+
+/* The message of the last failed call on this thread. */
+const char* oosgpu_last_error(void);
+/* 1 when a CUDA device is usable, 0 otherwise (the library never falls back to the CPU). */
+int oosgpu_device_count(void);
+
+/* ---- symbolic structure ---------------------------------------------------------------------------------------- */
+typedef struct oosgpu_symbolic oosgpu_symbolic;
+
+/* From the arrays of a reference SymbolicFactor: supernode s owns columns [first_column[s], first_column[s + 1]),
+ * its rows below them are rows[row_start[s] .. row_start[s + 1]) ascending, parent[s] = -1 for a root; children
+ * before parents. Checked (OOSGPU_INVALID_ARGUMENT). */
+int oosgpu_symbolic_create(int32_t dof_count, int32_t supernode_count, const int32_t* first_column,
+                           const int32_t* parent, const int64_t* row_start, const int32_t* rows,
+                           oosgpu_symbolic** out);
+/* From a node graph (sorted symmetric adjacency), node weights (DOFs per node), the final node order and a supernode
+ * partition of the positions (first_position: count + 1, parent: count): the row structures R(s) computed as
+ * SymbolicFactor::analyse does. */
+int oosgpu_symbolic_from_partition(int32_t node_count, const int64_t* offsets, const int32_t* neighbours,
+                                   const int32_t* weights, const int32_t* node_at_position, int32_t supernode_count,
+                                   const int32_t* first_position, const int32_t* parent, oosgpu_symbolic** out);
+/* sizes[0..7]: dofs, supernodes, row entries, panel values, factor entries, levels, update values, 0;
+ * flops: SymbolicFactor::flopCount. */
+int oosgpu_symbolic_sizes(const oosgpu_symbolic* symbolic, int64_t sizes[8], double* flops);
+int oosgpu_symbolic_rows(const oosgpu_symbolic* symbolic, int64_t* row_start, int32_t* rows);
+void oosgpu_symbolic_destroy(oosgpu_symbolic* symbolic);
+
+/* ---- factorisation --------------------------------------------------------------------------------------------- */
+typedef struct oosgpu_factor oosgpu_factor;
+
+/* FactorOptions (SupernodalFactor.hpp:63-97), positive definite mode. */
+typedef struct
+{
+    double max_ratio;                /* PivotPolicy::maxRatio (PARAM MaxDiagonalRatio), default 1e7 */
+    int32_t bailout;                 /* PivotPolicy::bailout (SingularityBailOut): < 0 continues past flagged pivots */
+    const double* reference_diagonal; /* FactorOptions::referenceDiagonal (host, dimension values) or NULL */
+} oosgpu_factor_options;
+
+/* What a factorisation found (SupernodalFactor accessors and PivotDiagnostics). */
+typedef struct
+{
+    int64_t positive;
+    int64_t negative;
+    int64_t zero;
+    int64_t delayed;
+    int64_t two_by_two;
+    int64_t issue_count;            /* pivots flagged by the ratio test */
+    int32_t equation_of_largest;    /* PivotDiagnostics::equationOfLargestRatio */
+    int32_t zero_pivot_count;       /* supernodes stopped by a zero pivot (SingularityError) */
+    double largest_ratio;
+    int32_t issues[16];             /* the first flagged equations, increasing */
+    int32_t zero_pivots[16];        /* the first zero-pivot equations, increasing */
+    double device_seconds;          /* the factorisation's device time (CUDA events) */
+} oosgpu_factor_info;
+
+/* A factor of `symbolic` on CUDA device `device` (the symbolic structure is copied: it may be destroyed after). */
+int oosgpu_factor_create(const oosgpu_symbolic* symbolic, int device, oosgpu_factor** out);
+void oosgpu_factor_destroy(oosgpu_factor* factor);
+/* The CUDA stream (cudaStream_t) the handle runs on. */
+void* oosgpu_factor_stream(oosgpu_factor* factor);
+
+/* Factorises the lower-triangle CSC (col_offsets: dimension + 1, rows ascending from the diagonal, values) given in
+ * the symbolic factor's equation order. Host arrays. OOSGPU_SINGULAR: a zero pivot, or the ratio test flagged pivots
+ * with bailout >= 0 (the info is filled either way). */
+int oosgpu_factorise(oosgpu_factor* factor, int32_t dimension, const int64_t* col_offsets, const int32_t* rows,
+                     const double* values, const oosgpu_factor_options* options, oosgpu_factor_info* info);
+/* The same on device arrays (stream-ordered on the handle's stream). */
+int oosgpu_factorise_device(oosgpu_factor* factor, int32_t dimension, int64_t terms, const int64_t* col_offsets,
+                            const int32_t* rows, const double* values, const oosgpu_factor_options* options,
+                            oosgpu_factor_info* info);
+
+/* The panel of supernode s (host copies): eliminated columns, rows; values (rows x eliminated, column-major),
+ * row equations and the 2x2 subdiagonal (zeros in positive definite mode) when the pointers are not NULL. */
+int oosgpu_factor_panel(oosgpu_factor* factor, int32_t s, int64_t* eliminated, int64_t* row_count, double* values,
+                        int32_t* rows, double* subdiagonal);
+
+/* B <- A^-1 B, B column-major dimension x columns (leading dimension ld), host memory. */
+int oosgpu_solve(oosgpu_factor* factor, double* b, int64_t ld, int64_t columns);
+/* The same on device memory (stream-ordered on the handle's stream). */
+int oosgpu_solve_device(oosgpu_factor* factor, double* b, int64_t ld, int64_t columns);
+/* The device time of the last solve (CUDA events), seconds. */
+double oosgpu_last_solve_seconds(oosgpu_factor* factor);
+
+/* ---- measurement (no counterpart in the reference: its RunReport carries stage times only,
+ *      include/oos/api/Analyses.hpp:182-199) ---------------------------------------------------------------------- */
+/* Brackets every launch of the following factorisations with CUDA events (enable != 0). */
+int oosgpu_factor_profile(oosgpu_factor* factor, int32_t enable);
+/* After a profiled factorisation, per launch kind k < kinds (0 small fronts, 1 assembly, 2 diagonal blocks, 3 panel
+ * rows, 4 panel update, 5 update-matrix Schur product): device seconds, launches, algorithmic flops and bytes. */
+int oosgpu_factor_kernel_stats(oosgpu_factor* factor, int32_t kinds, double* seconds, int64_t* launches,
+                               double* flops, double* bytes);
+/* counts[0]: kernels one factorisation launches; counts[1]: kernels one solve of `columns` right-hand sides
+ * launches. */
+int oosgpu_factor_launch_counts(oosgpu_factor* factor, int64_t columns, int64_t counts[2]);
+
+/* ---- model-side helpers (no counterpart in the reference's linalg: they stand in for its assembly and DOF
+ *      selection, src/assembly and SymmetricCsc::fromBlocks, src/linalg/sparse/SymmetricCsc.cpp:41) ---------------- */
+typedef struct oosgpu_model oosgpu_model;
+
+/* A plate of nx x ny flat-shell quadrilaterals on lx x ly, thickness t, clamped along x = 0, 6 DOFs per node. */
+int oosgpu_model_plate(int32_t nx, int32_t ny, double lx, double ly, double thickness, double young, double poisson,
+                       double pressure, oosgpu_model** out);
+/* A cube of n^3 trilinear hexahedra, clamped on z = 0, lumped mass, 3 DOFs per node. */
+int oosgpu_model_hex(int32_t n, double edge, double young, double poisson, double density, oosgpu_model** out);
+void oosgpu_model_destroy(oosgpu_model* model);
+/* sizes[0..3]: free nodes, DOFs per node, adjacency entries, 0 */
+int oosgpu_model_sizes(const oosgpu_model* model, int64_t sizes[4]);
+/* The node graph (offsets: nodes + 1, neighbours) and coordinates (3 per node); NULL pointers are skipped. */
+int oosgpu_model_graph(const oosgpu_model* model, int64_t* offsets, int32_t* neighbours, double* coordinates);
+int oosgpu_model_csc_terms(const oosgpu_model* model, const int32_t* node_at_position, int64_t* terms);
+/* which: 0 stiffness, 1 lumped mass on the stiffness pattern. */
+int oosgpu_model_csc(const oosgpu_model* model, const int32_t* node_at_position, int32_t which, int64_t* col_offsets,
+                     int32_t* rows, double* values);
+/* Column 0 the pressure load; columns j >= 1: `points` seeded nodes (splitmix64, seed_base + j) with N(0, sigma)
+ * forces on their out-of-plane translation. rhs column-major, leading dimension ld. */
+int oosgpu_model_loads(const oosgpu_model* model, const int32_t* node_at_position, int64_t columns,
+                       uint64_t seed_base, int32_t points, double sigma, double* rhs, int64_t ld);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,16 @@
+"""B200 implementation of O_o_Solver's numeric hot path: the supernodal multifrontal LDL^T factorisation and its
+solves on the GPU, behind the reference's factorisation interface (SymbolicFactor, SupernodalFactor.factorise,
+FactorSolve.solve) and a C ABI (include/oos_gpu.h)."""
+
+from .linalg import (  # noqa: F401
+    FactorOptions,
+    FactorSolve,
+    Inertia,
+    MemoryBudgetError,
+    PivotPolicy,
+    SingularityError,
+    SupernodalFactor,
+    SymbolicFactor,
+    SymmetricCsc,
+    device_count,
+)

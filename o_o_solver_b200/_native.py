@@ -1,0 +1,120 @@
+"""ctypes bindings of the library's C ABI (include/oos_gpu.h). The library is the only implementation: when it is
+missing, loading fails with an error naming the build command (there is no CPU fallback)."""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+from . import build as _build
+
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+
+class FactorOptions(ctypes.Structure):
+    _fields_ = [("max_ratio", ctypes.c_double), ("bailout", ctypes.c_int32), ("reference_diagonal", _f64p)]
+
+
+class FactorInfo(ctypes.Structure):
+    _fields_ = [
+        ("positive", ctypes.c_int64),
+        ("negative", ctypes.c_int64),
+        ("zero", ctypes.c_int64),
+        ("delayed", ctypes.c_int64),
+        ("two_by_two", ctypes.c_int64),
+        ("issue_count", ctypes.c_int64),
+        ("equation_of_largest", ctypes.c_int32),
+        ("zero_pivot_count", ctypes.c_int32),
+        ("largest_ratio", ctypes.c_double),
+        ("issues", ctypes.c_int32 * 16),
+        ("zero_pivots", ctypes.c_int32 * 16),
+        ("device_seconds", ctypes.c_double),
+    ]
+
+
+# The exported symbols and their signatures: (name, restype, argtypes).
+SIGNATURES = [
+    ("oosgpu_last_error", ctypes.c_char_p, []),
+    ("oosgpu_device_count", ctypes.c_int, []),
+    ("oosgpu_symbolic_create", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _i32p, _i32p, _i64p, _i32p,
+                                              ctypes.POINTER(_vp)]),
+    ("oosgpu_symbolic_from_partition", ctypes.c_int, [ctypes.c_int32, _i64p, _i32p, _i32p, _i32p, ctypes.c_int32,
+                                                      _i32p, _i32p, ctypes.POINTER(_vp)]),
+    ("oosgpu_symbolic_sizes", ctypes.c_int, [_vp, _i64p, _f64p]),
+    ("oosgpu_symbolic_rows", ctypes.c_int, [_vp, _i64p, _i32p]),
+    ("oosgpu_symbolic_destroy", None, [_vp]),
+    ("oosgpu_factor_create", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("oosgpu_factor_destroy", None, [_vp]),
+    ("oosgpu_factor_stream", _vp, [_vp]),
+    ("oosgpu_factorise", ctypes.c_int, [_vp, ctypes.c_int32, _i64p, _i32p, _f64p, ctypes.POINTER(FactorOptions),
+                                        ctypes.POINTER(FactorInfo)]),
+    ("oosgpu_factorise_device", ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int64, _vp, _vp, _vp,
+                                               ctypes.POINTER(FactorOptions), ctypes.POINTER(FactorInfo)]),
+    ("oosgpu_factor_panel", ctypes.c_int, [_vp, ctypes.c_int32, _i64p, _i64p, _f64p, _i32p, _f64p]),
+    ("oosgpu_solve", ctypes.c_int, [_vp, _f64p, ctypes.c_int64, ctypes.c_int64]),
+    ("oosgpu_solve_device", ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int64]),
+    ("oosgpu_last_solve_seconds", ctypes.c_double, [_vp]),
+    ("oosgpu_factor_profile", ctypes.c_int, [_vp, ctypes.c_int32]),
+    ("oosgpu_factor_kernel_stats", ctypes.c_int, [_vp, ctypes.c_int32, _f64p, _i64p, _f64p, _f64p]),
+    ("oosgpu_factor_launch_counts", ctypes.c_int, [_vp, ctypes.c_int64, _i64p]),
+    ("oosgpu_model_plate", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                          ctypes.POINTER(_vp)]),
+    ("oosgpu_model_hex", ctypes.c_int, [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, ctypes.POINTER(_vp)]),
+    ("oosgpu_model_destroy", None, [_vp]),
+    ("oosgpu_model_sizes", ctypes.c_int, [_vp, _i64p]),
+    ("oosgpu_model_graph", ctypes.c_int, [_vp, _i64p, _i32p, _f64p]),
+    ("oosgpu_model_csc_terms", ctypes.c_int, [_vp, _i32p, _i64p]),
+    ("oosgpu_model_csc", ctypes.c_int, [_vp, _i32p, ctypes.c_int32, _i64p, _i32p, _f64p]),
+    ("oosgpu_model_loads", ctypes.c_int, [_vp, _i32p, ctypes.c_int64, ctypes.c_uint64, ctypes.c_int32,
+                                          ctypes.c_double, _f64p, ctypes.c_int64]),
+]
+
+_lib = None
+
+
+def library_path() -> str:
+    return _build.LIBRARY
+
+
+def load(build_if_missing: bool = False):
+    """The loaded library. build_if_missing compiles it first (nvcc); otherwise a missing library is an error."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIBRARY
+    if build_if_missing:
+        _build.build()
+    if not os.path.exists(path):
+        raise RuntimeError(f"the CUDA library is not built: {path} (python -m o_o_solver_b200.build)")
+    lib = ctypes.CDLL(path)
+    for name, restype, argtypes in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+    _lib = lib
+    return lib
+
+
+class NativeError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+def check(status: int):
+    if status != 0:
+        raise NativeError(status, load().oosgpu_last_error().decode())
+
+
+def ptr(array, kind):
+    if array is None:
+        return None
+    return array.ctypes.data_as(kind)
+
+
+i32p, i64p, f64p, vp = _i32p, _i64p, _f64p, _vp

@@ -1,0 +1,327 @@
+// The kernels of the solves with a positive definite supernodal factor: X = L^-T D^-1 L^-1 B, forward over the
+// supernodes children first, then the diagonal, then backward (FactorSolve.cpp:31-158).
+//
+// The right-hand sides are held by rows on the device (the values of an equation for the tile's columns contiguous,
+// as the reference's row-stored blocks, FactorSolve.hpp): X[eq * width + col]. The forward sweep is multifrontal: a
+// supernode receives its children's update rows (in increasing child order, each row's sum fixed), eliminates its own
+// rows and leaves the update rows of R(s) for its parent, so no two supernodes write one value and the sums do not
+// depend on the scheduling. The backward sweep gathers the solved rows R(s) and substitutes back.
+//
+// Small supernodes (c <= 64) run one block each; larger ones run as 64-column steps of a diagonal block solve and tile
+// products on the FP64 tensor cores (tileProduct).
+
+#include "kernels.cuh"
+
+#include <cstdint>
+
+namespace oosgpu::device
+{
+
+
+constexpr int SOLVE_BLOCK = 64;
+constexpr int SOLVE_THREADS = 256;
+
+// Adds the children's update rows into the supernode's rows of X (positions < c) and into its own update rows
+// (zeroed first), children in increasing order.
+__device__ void gatherChildren(const SolveArgs& a, const FrontDesc& f, double* xF, int ldxF)
+{
+    const int w = a.width;
+    double* own = a.updates + f.rowStart * w;
+    for (int e = threadIdx.x; e < f.r * w; e += blockDim.x)
+        own[e] = 0.0;
+    __syncthreads();
+    for (int q = 0; q < f.childCount; ++q)
+    {
+        const FrontDesc ch = a.fronts[a.children[f.childStart + q]];
+        const std::int32_t* map = a.relpos + ch.rowStart;
+        const double* source = a.updates + ch.rowStart * w;
+        for (int e = threadIdx.x; e < ch.r * w; e += blockDim.x)
+        {
+            const int i = e / w;
+            const int col = e - i * w;
+            const int position = map[i];
+            if (position < f.c)
+                xF[position * ldxF + col] += source[e];
+            else
+                own[(position - f.c) * w + col] += source[e];
+        }
+        __syncthreads();
+    }
+}
+
+// Forward sweep of a small supernode (c <= SOLVE_BLOCK): x_F <- L11^-1 (b_F + children), u_s <- children - L21 x_F.
+__global__ void __launch_bounds__(SOLVE_THREADS) forwardSmall(SolveArgs a, const std::int32_t* list)
+{
+    extern __shared__ double xF[]; // c x width
+    const FrontDesc f = a.fronts[list[blockIdx.x]];
+    const int w = a.width;
+    const int n = f.c + f.r;
+    double* xRows = a.x + static_cast<std::int64_t>(f.first) * w;
+    for (int e = threadIdx.x; e < f.c * w; e += blockDim.x)
+        xF[e] = xRows[e];
+    __syncthreads();
+    gatherChildren(a, f, xF, w);
+    const double* panel = a.panels + f.panel;
+    for (int q = 0; q < f.c; ++q)
+    {
+        for (int e = threadIdx.x; e < (f.c - q - 1) * w; e += blockDim.x)
+        {
+            const int i = q + 1 + e / w;
+            const int col = e % w;
+            xF[i * w + col] -= panel[i + static_cast<std::int64_t>(q) * n] * xF[q * w + col];
+        }
+        __syncthreads();
+    }
+    double* own = a.updates + f.rowStart * w;
+    for (int e = threadIdx.x; e < f.r * w; e += blockDim.x)
+    {
+        const int i = e / w;
+        const int col = e - i * w;
+        double sum = own[e];
+        for (int q = 0; q < f.c; ++q)
+            sum -= panel[f.c + i + static_cast<std::int64_t>(q) * n] * xF[q * w + col];
+        own[e] = sum;
+    }
+    for (int e = threadIdx.x; e < f.c * w; e += blockDim.x)
+        xRows[e] = xF[e];
+}
+
+// The children's update rows of a large supernode, into X's rows of its columns (in place) and its update rows.
+__global__ void __launch_bounds__(SOLVE_THREADS) forwardGather(SolveArgs a, const std::int32_t* list)
+{
+    const FrontDesc f = a.fronts[list[blockIdx.x]];
+    gatherChildren(a, f, a.x + static_cast<std::int64_t>(f.first) * a.width, a.width);
+}
+
+// The unit lower triangle of step t of a large supernode: rows [k0, k0 + kb) of x_F, in shared memory.
+__global__ void __launch_bounds__(SOLVE_THREADS) forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
+{
+    __shared__ double xb[SOLVE_BLOCK * SOLVE_BLOCK];
+    const FrontDesc f = a.fronts[list[blockIdx.x]];
+    const int w = a.width;
+    const std::int64_t n = f.c + f.r;
+    const int kb = min(SOLVE_BLOCK, f.c - k0);
+    double* xRows = a.x + static_cast<std::int64_t>(f.first + k0) * w;
+    const double* l = a.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
+    for (int e = threadIdx.x; e < kb * w; e += blockDim.x)
+        xb[e] = xRows[e];
+    __syncthreads();
+    for (int q = 0; q < kb; ++q)
+    {
+        for (int e = threadIdx.x; e < (kb - q - 1) * w; e += blockDim.x)
+        {
+            const int i = q + 1 + e / w;
+            const int col = e % w;
+            xb[i * w + col] -= l[i + q * n] * xb[q * w + col];
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < kb * w; e += blockDim.x)
+        xRows[e] = xb[e];
+}
+
+// Step t's block applied to the rows below it: a tile of 64 rows either in x_F (i0 < c, task.k0 = 0) or in the update
+// rows (i0 >= c, task.k0 = 1); C -= L(i, k0:k0+kb) x_block.
+__global__ void __launch_bounds__(TILE_THREADS) forwardUpdate(SolveArgs a, const TileTask* tasks, int k0)
+{
+    __shared__ double smemA[TILE_K * (TILE + TILE_PAD)];
+    __shared__ double smemB[TILE_K * (TILE + TILE_PAD)];
+    const TileTask task = tasks[blockIdx.x];
+    const FrontDesc f = a.fronts[task.front];
+    const std::int64_t n = f.c + f.r;
+    const int w = a.width;
+    const double* panel = a.panels + f.panel;
+    TileOperands op;
+    op.a = panel + task.i0 + static_cast<std::int64_t>(k0) * n;
+    op.aRowStride = 1;
+    op.aColStride = n;
+    op.b = a.x + static_cast<std::int64_t>(f.first + k0) * w;
+    op.bRowStride = 1;
+    op.bColStride = w;
+    op.bIndex = nullptr;
+    op.d = nullptr;
+    op.dStride = 0;
+    if (task.i0 < f.c)
+    {
+        op.c = a.x + static_cast<std::int64_t>(f.first + task.i0) * w;
+        op.m = min(TILE, f.c - task.i0);
+    }
+    else
+    {
+        op.c = a.updates + (f.rowStart + (task.i0 - f.c)) * w;
+        op.m = static_cast<int>(n - task.i0 < TILE ? n - task.i0 : TILE);
+    }
+    op.cRowStride = w;
+    op.cColStride = 1;
+    op.n = w;
+    op.k = min(SOLVE_BLOCK, f.c - k0);
+    op.lower = false;
+    op.lowerOffset = 0;
+    tileProduct(op, smemA, smemB);
+}
+
+// The diagonal sweep: X[eq] /= d_eq.
+__global__ void diagonalSweep(SolveArgs a, const std::int32_t* supernodeOfColumn, int dimension)
+{
+    const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int w = a.width;
+    if (e >= static_cast<std::int64_t>(dimension) * w)
+        return;
+    const int eq = static_cast<int>(e / w);
+    const FrontDesc f = a.fronts[supernodeOfColumn[eq]];
+    const int k = eq - f.first;
+    const std::int64_t n = f.c + f.r;
+    a.x[e] = a.x[e] / a.panels[f.panel + k + k * n];
+}
+
+// Backward sweep of a small supernode: x_F <- L11^-T (x_F - L21^T X[R(s)]).
+__global__ void __launch_bounds__(SOLVE_THREADS) backwardSmall(SolveArgs a, const std::int32_t* list)
+{
+    extern __shared__ double xF[];
+    const FrontDesc f = a.fronts[list[blockIdx.x]];
+    const int w = a.width;
+    const std::int64_t n = f.c + f.r;
+    const double* panel = a.panels + f.panel;
+    const std::int32_t* rows = a.rows + f.rowStart;
+    double* xRows = a.x + static_cast<std::int64_t>(f.first) * w;
+    for (int e = threadIdx.x; e < f.c * w; e += blockDim.x)
+    {
+        const int q = e / w;
+        const int col = e - q * w;
+        double sum = xRows[e];
+        const double* l = panel + f.c + static_cast<std::int64_t>(q) * n;
+        for (int i = 0; i < f.r; ++i)
+            sum -= l[i] * a.x[static_cast<std::int64_t>(rows[i]) * w + col];
+        xF[e] = sum;
+    }
+    __syncthreads();
+    for (int i = f.c - 1; i > 0; --i)
+    {
+        for (int e = threadIdx.x; e < i * w; e += blockDim.x)
+        {
+            const int q = e / w;
+            const int col = e - q * w;
+            xF[q * w + col] -= panel[i + static_cast<std::int64_t>(q) * n] * xF[i * w + col];
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < f.c * w; e += blockDim.x)
+        xRows[e] = xF[e];
+}
+
+// x_F -= L21^T X[R(s)] for a large supernode, by tiles of 64 of its columns (A = L21^T read along its rows).
+__global__ void __launch_bounds__(TILE_THREADS) backwardRows(SolveArgs a, const TileTask* tasks)
+{
+    __shared__ double smemA[TILE_K * (TILE + TILE_PAD)];
+    __shared__ double smemB[TILE_K * (TILE + TILE_PAD)];
+    const TileTask task = tasks[blockIdx.x];
+    const FrontDesc f = a.fronts[task.front];
+    const std::int64_t n = f.c + f.r;
+    const int w = a.width;
+    TileOperands op;
+    op.a = a.panels + f.panel + f.c + static_cast<std::int64_t>(task.i0) * n;
+    op.aRowStride = n;
+    op.aColStride = 1;
+    op.b = a.x;
+    op.bRowStride = 1;
+    op.bColStride = w;
+    op.bIndex = a.rows + f.rowStart;
+    op.d = nullptr;
+    op.dStride = 0;
+    op.c = a.x + static_cast<std::int64_t>(f.first + task.i0) * w;
+    op.cRowStride = w;
+    op.cColStride = 1;
+    op.m = min(TILE, f.c - task.i0);
+    op.n = w;
+    op.k = f.r;
+    op.lower = false;
+    op.lowerOffset = 0;
+    tileProduct<true>(op, smemA, smemB);
+}
+
+// The unit upper triangle L11^T of step t (rows [k0, k0 + kb) of x_F), in shared memory.
+__global__ void __launch_bounds__(SOLVE_THREADS) backwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
+{
+    __shared__ double xb[SOLVE_BLOCK * SOLVE_BLOCK];
+    const FrontDesc f = a.fronts[list[blockIdx.x]];
+    const int w = a.width;
+    const std::int64_t n = f.c + f.r;
+    const int kb = min(SOLVE_BLOCK, f.c - k0);
+    double* xRows = a.x + static_cast<std::int64_t>(f.first + k0) * w;
+    const double* l = a.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
+    for (int e = threadIdx.x; e < kb * w; e += blockDim.x)
+        xb[e] = xRows[e];
+    __syncthreads();
+    for (int i = kb - 1; i > 0; --i)
+    {
+        for (int e = threadIdx.x; e < i * w; e += blockDim.x)
+        {
+            const int q = e / w;
+            const int col = e - q * w;
+            xb[q * w + col] -= l[i + q * n] * xb[i * w + col];
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < kb * w; e += blockDim.x)
+        xRows[e] = xb[e];
+}
+
+// After step t's block is solved, its terms leave the rows above it: x_F[q] -= sum_{i in block} L(i, q) x_F[i] for
+// q in a tile of [0, k0).
+__global__ void __launch_bounds__(TILE_THREADS) backwardUpdate(SolveArgs a, const TileTask* tasks, int k0)
+{
+    __shared__ double smemA[TILE_K * (TILE + TILE_PAD)];
+    __shared__ double smemB[TILE_K * (TILE + TILE_PAD)];
+    const TileTask task = tasks[blockIdx.x];
+    const FrontDesc f = a.fronts[task.front];
+    const std::int64_t n = f.c + f.r;
+    const int w = a.width;
+    TileOperands op;
+    // A(ii, p) = L(k0 + p, i0 + ii) = panel[k0 + p + (i0 + ii) n]
+    op.a = a.panels + f.panel + k0 + static_cast<std::int64_t>(task.i0) * n;
+    op.aRowStride = n;
+    op.aColStride = 1;
+    op.b = a.x + static_cast<std::int64_t>(f.first + k0) * w;
+    op.bRowStride = 1;
+    op.bColStride = w;
+    op.bIndex = nullptr;
+    op.d = nullptr;
+    op.dStride = 0;
+    op.c = a.x + static_cast<std::int64_t>(f.first + task.i0) * w;
+    op.cRowStride = w;
+    op.cColStride = 1;
+    op.m = min(TILE, k0 - task.i0);
+    op.n = w;
+    op.k = min(SOLVE_BLOCK, f.c - k0);
+    op.lower = false;
+    op.lowerOffset = 0;
+    tileProduct<true>(op, smemA, smemB);
+}
+
+// Column-major B (ld) <-> rows of X (width columns from column c0).
+__global__ void toRows(const double* b, std::int64_t ld, int c0, int width, int dimension, double* x,
+                       const double* scale)
+{
+    const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= static_cast<std::int64_t>(dimension) * width)
+        return;
+    const int col = static_cast<int>(e / dimension);
+    const int i = static_cast<int>(e - static_cast<std::int64_t>(col) * dimension);
+    const double s = scale != nullptr ? scale[i] : 1.0;
+    x[static_cast<std::int64_t>(i) * width + col] = b[static_cast<std::int64_t>(c0 + col) * ld + i] * s;
+}
+
+__global__ void fromRows(const double* x, int c0, int width, int dimension, double* b, std::int64_t ld,
+                         const double* scale)
+{
+    const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= static_cast<std::int64_t>(dimension) * width)
+        return;
+    const int col = static_cast<int>(e / dimension);
+    const int i = static_cast<int>(e - static_cast<std::int64_t>(col) * dimension);
+    const double s = scale != nullptr ? scale[i] : 1.0;
+    // x + 0.0: a solved value is never -0 (the reference writes x + 0 back, SolveSweeps.cpp:448-457).
+    b[static_cast<std::int64_t>(c0 + col) * ld + i] = x[static_cast<std::int64_t>(i) * width + col] * s + 0.0;
+}
+
+} // namespace oosgpu::device

@@ -1,0 +1,971 @@
+// The factor object on the GPU and the C ABI of include/oos_gpu.h.
+//
+// A factor owns, on its device: the plan's arrays (descriptors, children, rows, positions, task lists), the panels
+// (the reference's layout: supernode s at the sum of c(c + r) before it, column-major, leading dimension c + r), the
+// update matrices of every supernode (each r x r), a copy of the matrix, and the solve's work rows. It runs every
+// launch of a factorisation or a solve on its own stream; a factorisation reads back only its pivot summary.
+
+#include "../device/kernels.cuh"
+#include "host_api.hpp"
+#include "plan.hpp"
+
+#include "oos_gpu.h"
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace oosgpu
+{
+
+namespace
+{
+
+thread_local std::string g_lastError;
+
+void check(cudaError_t status, const char* what)
+{
+    if (status != cudaSuccess)
+        throw Error(status == cudaErrorMemoryAllocation ? STATUS_MEMORY_BUDGET : STATUS_CUDA,
+                    std::string(what) + ": " + cudaGetErrorString(status));
+}
+
+constexpr int NO_PIVOT = 0x7f7f7f7f; // the byte pattern 0x7f: "no zero pivot"
+constexpr int ISSUE_CAPACITY = 1 << 16;
+constexpr int SOLVE_WIDTH = 64;
+constexpr int SMALL_THREADS = 256;
+
+// A device allocation owned by the factor.
+template <typename T> class DeviceArray
+{
+public:
+    DeviceArray() = default;
+    DeviceArray(const DeviceArray&) = delete;
+    DeviceArray& operator=(const DeviceArray&) = delete;
+    ~DeviceArray() { release(); }
+    void allocate(std::size_t count, const char* what)
+    {
+        if (count <= m_count && m_data != nullptr)
+            return;
+        release();
+        void* p = nullptr;
+        check(cudaMalloc(&p, std::max<std::size_t>(count, 1) * sizeof(T)), what);
+        m_data = static_cast<T*>(p);
+        m_count = count;
+    }
+    void upload(const std::vector<T>& host, cudaStream_t stream, const char* what)
+    {
+        allocate(host.size(), what);
+        if (!host.empty())
+            check(cudaMemcpyAsync(m_data, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, stream), what);
+    }
+    void release()
+    {
+        if (m_data != nullptr)
+            cudaFree(m_data);
+        m_data = nullptr;
+        m_count = 0;
+    }
+    [[nodiscard]] T* get() const noexcept { return m_data; }
+    [[nodiscard]] std::size_t size() const noexcept { return m_count; }
+
+private:
+    T* m_data = nullptr;
+    std::size_t m_count = 0;
+};
+
+unsigned blocksFor(std::int64_t items, int threads)
+{
+    return static_cast<unsigned>((items + threads - 1) / threads);
+}
+
+} // namespace
+
+class GpuFactor
+{
+public:
+    GpuFactor(const Symbolic& symbolic, int device) : m_symbolic(symbolic), m_device(device)
+    {
+        check(cudaSetDevice(device), "cudaSetDevice");
+        m_plan = buildPlan(symbolic);
+        check(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaEventCreate(&m_start), "cudaEventCreate");
+        check(cudaEventCreate(&m_stop), "cudaEventCreate");
+        m_fronts.upload(m_plan.fronts, m_stream, "plan: fronts");
+        m_children.upload(m_plan.children, m_stream, "plan: children");
+        m_rows.upload(m_plan.rows, m_stream, "plan: rows");
+        m_relpos.upload(m_plan.relpos, m_stream, "plan: positions");
+        m_supernodeOfColumn.upload(m_plan.supernodeOfColumn, m_stream, "plan: columns");
+        m_lists.upload(m_plan.lists, m_stream, "plan: lists");
+        m_tiles.upload(m_plan.tiles, m_stream, "plan: tiles");
+        m_pieces.upload(m_plan.pieces, m_stream, "plan: pieces");
+        m_zeroPivot.allocate(static_cast<std::size_t>(m_plan.supernodeCount), "factor: zero pivots");
+        m_counters.allocate(8, "factor: counters");
+        m_issues.allocate(ISSUE_CAPACITY, "factor: issues");
+        const std::size_t summaryBlocks = blocksFor(std::max(m_plan.dimension, 1), 256);
+        m_blockRatio.allocate(summaryBlocks, "factor: ratios");
+        m_blockEquation.allocate(summaryBlocks, "factor: ratio equations");
+        m_structureError.allocate(1, "factor: structure check");
+        // Shared memory of the small-front kernel: the largest small front, square.
+        const int order = m_plan.largestSmallOrder;
+        m_smallSmem = static_cast<std::size_t>(order) * (order + 1) * sizeof(double);
+        if (m_smallSmem > 48 * 1024)
+            check(cudaFuncSetAttribute(device::smallFronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(m_smallSmem)),
+                  "smallFronts shared memory");
+        check(cudaStreamSynchronize(m_stream), "plan upload");
+    }
+
+    ~GpuFactor()
+    {
+        cudaSetDevice(m_device);
+        if (m_stream != nullptr)
+            cudaStreamSynchronize(m_stream);
+        cudaEventDestroy(m_start);
+        cudaEventDestroy(m_stop);
+        for (cudaEvent_t e : m_profileEvents)
+            cudaEventDestroy(e);
+        if (m_stream != nullptr)
+            cudaStreamDestroy(m_stream);
+    }
+
+    [[nodiscard]] cudaStream_t stream() const noexcept { return m_stream; }
+    [[nodiscard]] const Plan& plan() const noexcept { return m_plan; }
+
+    void factorise(std::int32_t dimension, std::int64_t terms, const std::int64_t* offsets, const std::int32_t* rows,
+                   const double* values, bool onDevice, const oosgpu_factor_options* options, oosgpu_factor_info* info)
+    {
+        check(cudaSetDevice(m_device), "cudaSetDevice");
+        if (dimension != m_plan.dimension)
+            throw Error(STATUS_INVALID_ARGUMENT,
+                        "supernodal factorisation: the matrix has " + std::to_string(dimension) +
+                            " equations and the symbolic factor " + std::to_string(m_plan.dimension) +
+                            "; factorise the matrix assembled on the graph and in the order of its symbolic analysis");
+        const double maxRatio = options != nullptr ? options->max_ratio : 1.0e7;
+        const int bailout = options != nullptr ? options->bailout : 0;
+        m_panels.allocate(static_cast<std::size_t>(m_plan.panelValues), "factor: panels");
+        m_updates.allocate(static_cast<std::size_t>(m_plan.updateValues), "factor: update matrices");
+        const std::int64_t* dOffsets = offsets;
+        const std::int32_t* dRows = rows;
+        const double* dValues = values;
+        if (!onDevice)
+        {
+            if (offsets[dimension] != terms && terms >= 0)
+                throw Error(STATUS_INVALID_ARGUMENT, "supernodal factorisation: the offsets do not end at the terms");
+            terms = offsets[dimension];
+            m_cscOffsets.allocate(static_cast<std::size_t>(dimension) + 1, "factor: matrix offsets");
+            m_cscRows.allocate(static_cast<std::size_t>(terms), "factor: matrix rows");
+            m_cscValues.allocate(static_cast<std::size_t>(terms), "factor: matrix values");
+            check(cudaMemcpyAsync(m_cscOffsets.get(), offsets, (static_cast<std::size_t>(dimension) + 1) * sizeof(std::int64_t),
+                                  cudaMemcpyHostToDevice, m_stream),
+                  "upload offsets");
+            check(cudaMemcpyAsync(m_cscRows.get(), rows, static_cast<std::size_t>(terms) * sizeof(std::int32_t),
+                                  cudaMemcpyHostToDevice, m_stream),
+                  "upload rows");
+            check(cudaMemcpyAsync(m_cscValues.get(), values, static_cast<std::size_t>(terms) * sizeof(double),
+                                  cudaMemcpyHostToDevice, m_stream),
+                  "upload values");
+            dOffsets = m_cscOffsets.get();
+            dRows = m_cscRows.get();
+            dValues = m_cscValues.get();
+        }
+        if (!m_annotated)
+        {
+            // The matrix terms of each supernode's columns, for the launches' algorithmic bytes.
+            std::vector<std::int64_t> hostOffsets(static_cast<std::size_t>(dimension) + 1);
+            if (onDevice)
+                check(cudaMemcpy(hostOffsets.data(), offsets, hostOffsets.size() * sizeof(std::int64_t),
+                                 cudaMemcpyDeviceToHost),
+                      "download offsets");
+            else
+                std::copy_n(offsets, hostOffsets.size(), hostOffsets.begin());
+            std::vector<std::int64_t> termsOfFront(static_cast<std::size_t>(m_plan.supernodeCount));
+            for (std::int32_t s = 0; s < m_plan.supernodeCount; ++s)
+            {
+                const device::FrontDesc& f = m_plan.fronts[static_cast<std::size_t>(s)];
+                termsOfFront[static_cast<std::size_t>(s)] =
+                    hostOffsets[static_cast<std::size_t>(f.first + f.c)] - hostOffsets[static_cast<std::size_t>(f.first)];
+            }
+            annotate(m_plan, termsOfFront);
+            m_annotated = true;
+        }
+        const double* referenceDiagonal = nullptr;
+        if (options != nullptr && options->reference_diagonal != nullptr)
+        {
+            m_referenceDiagonal.allocate(static_cast<std::size_t>(dimension), "factor: reference diagonal");
+            check(cudaMemcpyAsync(m_referenceDiagonal.get(), options->reference_diagonal,
+                                  static_cast<std::size_t>(dimension) * sizeof(double), cudaMemcpyHostToDevice, m_stream),
+                  "upload reference diagonal");
+            referenceDiagonal = m_referenceDiagonal.get();
+        }
+
+        device::FactorArgs args{m_fronts.get(),   m_children.get(), m_rows.get(),  m_relpos.get(),
+                                dOffsets,         dRows,            dValues,       m_panels.get(),
+                                m_updates.get(),  m_zeroPivot.get()};
+        check(cudaEventRecord(m_start, m_stream), "event");
+        check(cudaMemsetAsync(m_zeroPivot.get(), 0x7f, static_cast<std::size_t>(m_plan.supernodeCount) * sizeof(std::int32_t),
+                              m_stream),
+              "memset");
+        check(cudaMemsetAsync(m_structureError.get(), 0x7f, sizeof(std::int32_t), m_stream), "memset");
+        check(cudaMemsetAsync(m_counters.get(), 0, 8 * sizeof(unsigned long long), m_stream), "memset");
+        runFactorLaunches(args);
+        const unsigned summaryBlocks = blocksFor(std::max(dimension, 1), 256);
+        device::pivotSummary<<<summaryBlocks, 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), dimension,
+                                                                   referenceDiagonal, maxRatio, m_counters.get(),
+                                                                   m_issues.get(), ISSUE_CAPACITY, m_blockRatio.get(),
+                                                                   m_blockEquation.get());
+        check(cudaGetLastError(), "pivot summary launch");
+        check(cudaEventRecord(m_stop, m_stream), "event");
+
+        // The summary back on the host.
+        std::vector<unsigned long long> counters(8);
+        std::vector<std::int32_t> zeroPivot(static_cast<std::size_t>(m_plan.supernodeCount));
+        std::vector<double> blockRatio(summaryBlocks);
+        std::vector<std::int32_t> blockEquation(summaryBlocks);
+        std::int32_t structureError = 0;
+        check(cudaMemcpyAsync(counters.data(), m_counters.get(), 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                              m_stream),
+              "download counters");
+        check(cudaMemcpyAsync(zeroPivot.data(), m_zeroPivot.get(), zeroPivot.size() * sizeof(std::int32_t),
+                              cudaMemcpyDeviceToHost, m_stream),
+              "download zero pivots");
+        check(cudaMemcpyAsync(blockRatio.data(), m_blockRatio.get(), summaryBlocks * sizeof(double),
+                              cudaMemcpyDeviceToHost, m_stream),
+              "download ratios");
+        check(cudaMemcpyAsync(blockEquation.data(), m_blockEquation.get(), summaryBlocks * sizeof(std::int32_t),
+                              cudaMemcpyDeviceToHost, m_stream),
+              "download ratio equations");
+        check(cudaMemcpyAsync(&structureError, m_structureError.get(), sizeof(std::int32_t), cudaMemcpyDeviceToHost,
+                              m_stream),
+              "download structure check");
+        check(cudaStreamSynchronize(m_stream), "factorisation");
+        m_profileValid = m_profile;
+        float milliseconds = 0.0f;
+        check(cudaEventElapsedTime(&milliseconds, m_start, m_stop), "event time");
+        m_factorised = false;
+        if (structureError != NO_PIVOT)
+            throw Error(STATUS_INVALID_ARGUMENT,
+                        "supernodal factorisation: column " + std::to_string(structureError) +
+                            " of the matrix has an entry outside the structure of the symbolic factor; build the CSC in "
+                            "the order of the symbolic factor, on the graph it was analysed on");
+
+        oosgpu_factor_info result{};
+        result.positive = static_cast<std::int64_t>(counters[0]);
+        result.negative = static_cast<std::int64_t>(counters[1]);
+        result.zero = static_cast<std::int64_t>(counters[2]);
+        result.issue_count = static_cast<std::int64_t>(counters[3]);
+        result.device_seconds = milliseconds / 1000.0;
+        result.largest_ratio = 0.0;
+        result.equation_of_largest = -1;
+        for (unsigned b = 0; b < summaryBlocks; ++b)
+            if (blockEquation[b] != INT_MAX &&
+                (result.equation_of_largest < 0 || blockRatio[b] > result.largest_ratio))
+            {
+                result.largest_ratio = blockRatio[b];
+                result.equation_of_largest = blockEquation[b];
+            }
+        // Issues in elimination order (equation order in positive definite mode).
+        const auto issueCount = static_cast<std::size_t>(std::min<std::int64_t>(result.issue_count, ISSUE_CAPACITY));
+        if (issueCount > 0)
+        {
+            std::vector<std::int32_t> issues(issueCount);
+            check(cudaMemcpy(issues.data(), m_issues.get(), issueCount * sizeof(std::int32_t), cudaMemcpyDeviceToHost),
+                  "download issues");
+            std::sort(issues.begin(), issues.end());
+            for (std::size_t k = 0; k < std::min<std::size_t>(16, issues.size()); ++k)
+                result.issues[k] = issues[k];
+        }
+        // Zero pivots: a supernode with a failed descendant is not counted (the reference skips it).
+        std::vector<char> failedBelow(static_cast<std::size_t>(m_plan.supernodeCount), 0);
+        std::vector<std::int32_t> zeroEquations;
+        for (std::int32_t s = 0; s < m_plan.supernodeCount; ++s)
+        {
+            const auto at = static_cast<std::size_t>(s);
+            const bool failed = zeroPivot[at] != NO_PIVOT;
+            if (failed && failedBelow[at] == 0)
+                zeroEquations.push_back(m_plan.fronts[at].first + zeroPivot[at]);
+            const std::int32_t p = m_plan.fronts[at].parent;
+            if (p >= 0 && (failed || failedBelow[at] != 0))
+                failedBelow[static_cast<std::size_t>(p)] = 1;
+        }
+        result.zero_pivot_count = static_cast<std::int32_t>(zeroEquations.size());
+        for (std::size_t k = 0; k < std::min<std::size_t>(16, zeroEquations.size()); ++k)
+            result.zero_pivots[k] = zeroEquations[k];
+        if (info != nullptr)
+            *info = result;
+        if (!zeroEquations.empty())
+        {
+            std::string names;
+            for (std::size_t k = 0; k < std::min<std::size_t>(10, zeroEquations.size()); ++k)
+                names += "  equation " + std::to_string(zeroEquations[k]) + "\n";
+            throw Error(STATUS_SINGULAR, "the stiffness matrix is singular: " + std::to_string(zeroEquations.size()) +
+                                             " zero (or not finite) pivots met in the factorisation, a mechanism or an "
+                                             "unconstrained DOF at:\n" +
+                                             names);
+        }
+        if (result.issue_count > 0 && bailout >= 0)
+            throw Error(STATUS_SINGULAR, "the ratio test flagged " + std::to_string(result.issue_count) +
+                                             " pivots (MaxDiagonalRatio " + std::to_string(maxRatio) +
+                                             "; the first at equation " + std::to_string(result.issues[0]) + ")");
+        m_factorised = true;
+    }
+
+    void solve(double* b, std::int64_t ld, std::int64_t columns, bool onDevice)
+    {
+        check(cudaSetDevice(m_device), "cudaSetDevice");
+        if (!m_factorised)
+            throw Error(STATUS_NOT_FACTORISED, "FactorSolve: no factor (factorise first, or the last one failed)");
+        const std::int32_t n = m_plan.dimension;
+        if (ld < n || columns < 0)
+            throw Error(STATUS_INVALID_ARGUMENT, "FactorSolve::solve: expected " + std::to_string(n) +
+                                                     " rows (leading dimension >= rows), found leading dimension " +
+                                                     std::to_string(ld));
+        if (columns == 0 || n == 0)
+            return;
+        m_work.allocate(static_cast<std::size_t>(n) * SOLVE_WIDTH, "solve: rows");
+        m_updateRows.allocate(static_cast<std::size_t>(std::max<std::int64_t>(m_plan.rowEntries, 1)) * SOLVE_WIDTH,
+                              "solve: update rows");
+        double* deviceB = b;
+        if (!onDevice)
+        {
+            m_hostB.allocate(static_cast<std::size_t>(n) * static_cast<std::size_t>(columns), "solve: right-hand sides");
+            deviceB = m_hostB.get();
+            check(cudaMemcpy2DAsync(deviceB, static_cast<std::size_t>(n) * sizeof(double), b,
+                                    static_cast<std::size_t>(ld) * sizeof(double), static_cast<std::size_t>(n) * sizeof(double),
+                                    static_cast<std::size_t>(columns), cudaMemcpyHostToDevice, m_stream),
+                  "upload right-hand sides");
+        }
+        const std::int64_t deviceLd = onDevice ? ld : n;
+        check(cudaEventRecord(m_start, m_stream), "event");
+        for (std::int64_t c0 = 0; c0 < columns; c0 += SOLVE_WIDTH)
+        {
+            const int width = static_cast<int>(std::min<std::int64_t>(SOLVE_WIDTH, columns - c0));
+            const std::int64_t items = static_cast<std::int64_t>(n) * width;
+            device::toRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(deviceB, deviceLd, static_cast<int>(c0), width,
+                                                                        n, m_work.get(), nullptr);
+            device::SolveArgs args{m_fronts.get(), m_children.get(), m_rows.get(), m_relpos.get(),
+                                   m_panels.get(), m_work.get(),     m_updateRows.get(), width};
+            runSweep(args, m_plan.forwardLaunches);
+            device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), n);
+            runSweep(args, m_plan.backwardLaunches);
+            device::fromRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(m_work.get(), static_cast<int>(c0), width, n,
+                                                                          deviceB, deviceLd, nullptr);
+            check(cudaGetLastError(), "solve launch");
+        }
+        check(cudaEventRecord(m_stop, m_stream), "event");
+        if (!onDevice)
+            check(cudaMemcpy2DAsync(b, static_cast<std::size_t>(ld) * sizeof(double), deviceB,
+                                    static_cast<std::size_t>(n) * sizeof(double), static_cast<std::size_t>(n) * sizeof(double),
+                                    static_cast<std::size_t>(columns), cudaMemcpyDeviceToHost, m_stream),
+                  "download solutions");
+        check(cudaStreamSynchronize(m_stream), "solve");
+        float milliseconds = 0.0f;
+        check(cudaEventElapsedTime(&milliseconds, m_start, m_stop), "event time");
+        m_lastSolveSeconds = milliseconds / 1000.0;
+    }
+
+    void panel(std::int32_t s, std::int64_t* eliminated, std::int64_t* rowCount, double* values, std::int32_t* rows,
+               double* subdiagonal)
+    {
+        check(cudaSetDevice(m_device), "cudaSetDevice");
+        if (s < 0 || s >= m_plan.supernodeCount)
+            throw Error(STATUS_INVALID_ARGUMENT, "panel: supernode out of range");
+        if (!m_factorised)
+            throw Error(STATUS_NOT_FACTORISED, "panel: no factor");
+        const device::FrontDesc& f = m_plan.fronts[static_cast<std::size_t>(s)];
+        const std::int64_t n = f.c + f.r;
+        *eliminated = f.c;
+        *rowCount = n;
+        if (values != nullptr)
+            check(cudaMemcpy(values, m_panels.get() + f.panel, static_cast<std::size_t>(n * f.c) * sizeof(double),
+                             cudaMemcpyDeviceToHost),
+                  "download panel");
+        if (rows != nullptr)
+        {
+            for (std::int32_t k = 0; k < f.c; ++k)
+                rows[k] = f.first + k;
+            std::copy_n(m_plan.rows.data() + f.rowStart, f.r, rows + f.c);
+        }
+        if (subdiagonal != nullptr)
+            std::fill_n(subdiagonal, f.c, 0.0);
+    }
+
+    [[nodiscard]] double lastSolveSeconds() const noexcept { return m_lastSolveSeconds; }
+
+    // Profiling: each factorisation launch bracketed by events; after a factorisation, the device time, launches,
+    // algorithmic flops and bytes of each launch kind of it.
+    void setProfile(bool enable) { m_profile = enable; }
+    void kernelStats(int kinds, double* seconds, std::int64_t* launches, double* flops, double* bytes)
+    {
+        check(cudaSetDevice(m_device), "cudaSetDevice");
+        for (int k = 0; k < kinds; ++k)
+        {
+            seconds[k] = 0.0;
+            launches[k] = 0;
+            flops[k] = 0.0;
+            bytes[k] = 0.0;
+        }
+        if (!m_profileValid)
+            throw Error(STATUS_NOT_FACTORISED, "kernel statistics: no profiled factorisation");
+        for (std::size_t index = 0; index < m_plan.factorLaunches.size(); ++index)
+        {
+            const Launch& launch = m_plan.factorLaunches[index];
+            const int kind = static_cast<int>(launch.kind);
+            if (kind >= kinds)
+                continue;
+            float ms = 0.0f;
+            check(cudaEventElapsedTime(&ms, m_profileEvents[2 * index], m_profileEvents[2 * index + 1]), "profile time");
+            seconds[kind] += ms / 1000.0;
+            launches[kind] += 1;
+            flops[kind] += launch.flops;
+            bytes[kind] += launch.bytes;
+        }
+    }
+    [[nodiscard]] std::int64_t factorLaunchCount() const noexcept
+    {
+        return static_cast<std::int64_t>(m_plan.factorLaunches.size()) + 1;
+    }
+    [[nodiscard]] std::int64_t solveLaunchCount(std::int64_t columns) const noexcept
+    {
+        const std::int64_t tiles = (columns + SOLVE_WIDTH - 1) / SOLVE_WIDTH;
+        return tiles * (static_cast<std::int64_t>(m_plan.forwardLaunches.size() + m_plan.backwardLaunches.size()) + 3);
+    }
+
+private:
+    void runFactorLaunches(const device::FactorArgs& args)
+    {
+        std::size_t index = 0;
+        for (const Launch& launch : m_plan.factorLaunches)
+        {
+            if (m_profile)
+                check(cudaEventRecord(profileEvent(2 * index), m_stream), "profile event");
+            launchFactor(launch, args);
+            if (m_profile)
+                check(cudaEventRecord(profileEvent(2 * index + 1), m_stream), "profile event");
+            ++index;
+        }
+        check(cudaGetLastError(), "factorisation launch");
+    }
+
+    cudaEvent_t profileEvent(std::size_t k)
+    {
+        while (m_profileEvents.size() <= k)
+        {
+            cudaEvent_t e = nullptr;
+            check(cudaEventCreate(&e), "cudaEventCreate");
+            m_profileEvents.push_back(e);
+        }
+        return m_profileEvents[k];
+    }
+
+    void launchFactor(const Launch& launch, const device::FactorArgs& args)
+    {
+        {
+            switch (launch.kind)
+            {
+            case LaunchKind::SmallFronts:
+            {
+                const std::size_t smem = static_cast<std::size_t>(launch.smemOrder) * (launch.smemOrder + 1) * sizeof(double);
+                device::smallFronts<<<launch.count, SMALL_THREADS, smem, m_stream>>>(
+                    args, m_lists.get() + launch.offset, m_structureError.get());
+                break;
+            }
+            case LaunchKind::AssembleFronts:
+                device::assembleFronts<<<launch.count, 256, 0, m_stream>>>(args, m_pieces.get() + launch.offset,
+                                                                           m_structureError.get());
+                break;
+            case LaunchKind::DiagonalBlocks:
+                device::diagonalBlocks<<<launch.count, 256, 0, m_stream>>>(args, m_lists.get() + launch.offset,
+                                                                           launch.k0);
+                break;
+            case LaunchKind::PanelRows:
+                device::panelRows<<<launch.count, 128, 0, m_stream>>>(args, m_tiles.get() + launch.offset, launch.k0);
+                break;
+            case LaunchKind::PanelUpdate:
+                device::panelUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(
+                    args, m_tiles.get() + launch.offset, launch.k0);
+                break;
+            case LaunchKind::UpdateMatrix:
+                device::updateMatrix<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(
+                    args, m_tiles.get() + launch.offset);
+                break;
+            default:
+                throw Error(STATUS_INTERNAL, "factorisation plan: a solve launch in the factor sequence");
+            }
+        }
+    }
+
+    void runSweep(const device::SolveArgs& args, const std::vector<Launch>& launches)
+    {
+        for (const Launch& launch : launches)
+        {
+            const std::int32_t* list = m_lists.get() + launch.offset;
+            const device::TileTask* tiles = m_tiles.get() + launch.offset;
+            const std::size_t smallSmem = static_cast<std::size_t>(std::max(launch.smemOrder, 1)) * args.width * sizeof(double);
+            switch (launch.kind)
+            {
+            case LaunchKind::ForwardSmall:
+                device::forwardSmall<<<launch.count, 256, smallSmem, m_stream>>>(args, list);
+                break;
+            case LaunchKind::ForwardGather:
+                device::forwardGather<<<launch.count, 256, 0, m_stream>>>(args, list);
+                break;
+            case LaunchKind::ForwardDiagonal:
+                device::forwardDiagonal<<<launch.count, 256, 0, m_stream>>>(args, list, launch.k0);
+                break;
+            case LaunchKind::ForwardUpdate:
+                device::forwardUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles, launch.k0);
+                break;
+            case LaunchKind::BackwardSmall:
+                device::backwardSmall<<<launch.count, 256, smallSmem, m_stream>>>(args, list);
+                break;
+            case LaunchKind::BackwardRows:
+                device::backwardRows<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles);
+                break;
+            case LaunchKind::BackwardDiagonal:
+                device::backwardDiagonal<<<launch.count, 256, 0, m_stream>>>(args, list, launch.k0);
+                break;
+            case LaunchKind::BackwardUpdate:
+                device::backwardUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles, launch.k0);
+                break;
+            default:
+                throw Error(STATUS_INTERNAL, "solve plan: a factorisation launch in a sweep");
+            }
+        }
+    }
+
+    Symbolic m_symbolic;
+    int m_device = 0;
+    Plan m_plan;
+    cudaStream_t m_stream = nullptr;
+    cudaEvent_t m_start = nullptr;
+    cudaEvent_t m_stop = nullptr;
+    DeviceArray<device::FrontDesc> m_fronts;
+    DeviceArray<std::int32_t> m_children;
+    DeviceArray<std::int32_t> m_rows;
+    DeviceArray<std::int32_t> m_relpos;
+    DeviceArray<std::int32_t> m_supernodeOfColumn;
+    DeviceArray<std::int32_t> m_lists;
+    DeviceArray<device::TileTask> m_tiles;
+    DeviceArray<device::AssemblyTask> m_pieces;
+    DeviceArray<std::int32_t> m_zeroPivot;
+    DeviceArray<unsigned long long> m_counters;
+    DeviceArray<std::int32_t> m_issues;
+    DeviceArray<double> m_blockRatio;
+    DeviceArray<std::int32_t> m_blockEquation;
+    DeviceArray<std::int32_t> m_structureError;
+    DeviceArray<double> m_panels;
+    DeviceArray<double> m_updates;
+    DeviceArray<std::int64_t> m_cscOffsets;
+    DeviceArray<std::int32_t> m_cscRows;
+    DeviceArray<double> m_cscValues;
+    DeviceArray<double> m_referenceDiagonal;
+    DeviceArray<double> m_work;
+    DeviceArray<double> m_updateRows;
+    DeviceArray<double> m_hostB;
+    std::size_t m_smallSmem = 0;
+    bool m_factorised = false;
+    bool m_profile = false;
+    bool m_profileValid = false;
+    bool m_annotated = false;
+    std::vector<cudaEvent_t> m_profileEvents;
+    double m_lastSolveSeconds = 0.0;
+};
+
+namespace
+{
+
+template <typename F> int guarded(F&& body)
+{
+    try
+    {
+        body();
+        return STATUS_OK;
+    }
+    catch (const Error& error)
+    {
+        g_lastError = error.what();
+        return error.status();
+    }
+    catch (const std::bad_alloc&)
+    {
+        g_lastError = "host memory exhausted";
+        return STATUS_MEMORY_BUDGET;
+    }
+    catch (const std::exception& error)
+    {
+        g_lastError = error.what();
+        return STATUS_INTERNAL;
+    }
+}
+
+} // namespace
+} // namespace oosgpu
+
+struct oosgpu_symbolic
+{
+    oosgpu::Symbolic symbolic;
+    std::int32_t levels = 0;
+    std::int64_t updateValues = 0;
+};
+
+struct oosgpu_factor
+{
+    std::unique_ptr<oosgpu::GpuFactor> factor;
+};
+
+struct oosgpu_model
+{
+    oosgpu::Model model;
+};
+
+using oosgpu::guarded;
+
+namespace
+{
+
+void summarise(oosgpu_symbolic& handle)
+{
+    handle.symbolic.validate();
+    std::vector<std::int32_t> level(static_cast<std::size_t>(handle.symbolic.supernodeCount), 0);
+    std::int32_t top = 0;
+    std::int64_t update = 0;
+    for (std::int32_t s = 0; s < handle.symbolic.supernodeCount; ++s)
+    {
+        const std::int32_t p = handle.symbolic.parent[static_cast<std::size_t>(s)];
+        if (p >= 0)
+            level[static_cast<std::size_t>(p)] = std::max(level[static_cast<std::size_t>(p)], level[static_cast<std::size_t>(s)] + 1);
+        top = std::max(top, level[static_cast<std::size_t>(s)]);
+        const std::int64_t r = handle.symbolic.rowCount(s);
+        update += r * r;
+    }
+    handle.levels = handle.symbolic.supernodeCount == 0 ? 0 : top + 1;
+    handle.updateValues = update;
+}
+
+void requirePointer(const void* p, const char* what)
+{
+    if (p == nullptr)
+        throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT, std::string(what) + " is null");
+}
+
+} // namespace
+
+extern "C" const char* oosgpu_last_error(void)
+{
+    return oosgpu::g_lastError.c_str();
+}
+
+extern "C" int oosgpu_device_count(void)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return 0;
+    }
+    return count;
+}
+
+extern "C" int oosgpu_symbolic_create(int32_t dof_count, int32_t supernode_count, const int32_t* first_column,
+                                      const int32_t* parent, const int64_t* row_start, const int32_t* rows,
+                                      oosgpu_symbolic** out)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(out, "out");
+            requirePointer(first_column, "first_column");
+            requirePointer(parent, "parent");
+            requirePointer(row_start, "row_start");
+            if (supernode_count < 0)
+                throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT, "negative supernode count");
+            auto handle = std::make_unique<oosgpu_symbolic>();
+            oosgpu::Symbolic& s = handle->symbolic;
+            s.dofCount = dof_count;
+            s.supernodeCount = supernode_count;
+            s.firstColumn.assign(first_column, first_column + supernode_count + 1);
+            s.parent.assign(parent, parent + supernode_count);
+            s.rowStart.assign(row_start, row_start + supernode_count + 1);
+            if (row_start[supernode_count] > 0)
+                requirePointer(rows, "rows");
+            s.rows.assign(rows, rows + row_start[supernode_count]);
+            summarise(*handle);
+            *out = handle.release();
+        });
+}
+
+extern "C" int oosgpu_symbolic_from_partition(int32_t node_count, const int64_t* offsets, const int32_t* neighbours,
+                                              const int32_t* weights, const int32_t* node_at_position,
+                                              int32_t supernode_count, const int32_t* first_position,
+                                              const int32_t* parent, oosgpu_symbolic** out)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(out, "out");
+            requirePointer(offsets, "offsets");
+            requirePointer(weights, "weights");
+            requirePointer(node_at_position, "node_at_position");
+            requirePointer(first_position, "first_position");
+            requirePointer(parent, "parent");
+            auto handle = std::make_unique<oosgpu_symbolic>();
+            handle->symbolic = oosgpu::rowStructures(node_count, offsets, neighbours, weights, node_at_position,
+                                                     supernode_count, first_position, parent);
+            summarise(*handle);
+            *out = handle.release();
+        });
+}
+
+extern "C" int oosgpu_symbolic_sizes(const oosgpu_symbolic* symbolic, int64_t sizes[8], double* flops)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(symbolic, "symbolic");
+            const oosgpu::Symbolic& s = symbolic->symbolic;
+            sizes[0] = s.dofCount;
+            sizes[1] = s.supernodeCount;
+            sizes[2] = static_cast<int64_t>(s.rows.size());
+            sizes[3] = s.panelValueCount();
+            sizes[4] = s.factorEntryCount();
+            sizes[5] = symbolic->levels;
+            sizes[6] = symbolic->updateValues;
+            sizes[7] = 0;
+            if (flops != nullptr)
+                *flops = s.flopCount();
+        });
+}
+
+extern "C" int oosgpu_symbolic_rows(const oosgpu_symbolic* symbolic, int64_t* row_start, int32_t* rows)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(symbolic, "symbolic");
+            const oosgpu::Symbolic& s = symbolic->symbolic;
+            std::copy(s.rowStart.begin(), s.rowStart.end(), row_start);
+            std::copy(s.rows.begin(), s.rows.end(), rows);
+        });
+}
+
+extern "C" void oosgpu_symbolic_destroy(oosgpu_symbolic* symbolic)
+{
+    delete symbolic;
+}
+
+extern "C" int oosgpu_factor_create(const oosgpu_symbolic* symbolic, int device, oosgpu_factor** out)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(symbolic, "symbolic");
+            requirePointer(out, "out");
+            auto handle = std::make_unique<oosgpu_factor>();
+            handle->factor = std::make_unique<oosgpu::GpuFactor>(symbolic->symbolic, device);
+            *out = handle.release();
+        });
+}
+
+extern "C" void oosgpu_factor_destroy(oosgpu_factor* factor)
+{
+    delete factor;
+}
+
+extern "C" void* oosgpu_factor_stream(oosgpu_factor* factor)
+{
+    return factor == nullptr ? nullptr : static_cast<void*>(factor->factor->stream());
+}
+
+extern "C" int oosgpu_factorise(oosgpu_factor* factor, int32_t dimension, const int64_t* col_offsets,
+                                const int32_t* rows, const double* values, const oosgpu_factor_options* options,
+                                oosgpu_factor_info* info)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            requirePointer(col_offsets, "col_offsets");
+            factor->factor->factorise(dimension, -1, col_offsets, rows, values, false, options, info);
+        });
+}
+
+extern "C" int oosgpu_factorise_device(oosgpu_factor* factor, int32_t dimension, int64_t terms,
+                                       const int64_t* col_offsets, const int32_t* rows, const double* values,
+                                       const oosgpu_factor_options* options, oosgpu_factor_info* info)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            requirePointer(col_offsets, "col_offsets");
+            factor->factor->factorise(dimension, terms, col_offsets, rows, values, true, options, info);
+        });
+}
+
+extern "C" int oosgpu_factor_panel(oosgpu_factor* factor, int32_t s, int64_t* eliminated, int64_t* row_count,
+                                   double* values, int32_t* rows, double* subdiagonal)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            factor->factor->panel(s, eliminated, row_count, values, rows, subdiagonal);
+        });
+}
+
+extern "C" int oosgpu_solve(oosgpu_factor* factor, double* b, int64_t ld, int64_t columns)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            factor->factor->solve(b, ld, columns, false);
+        });
+}
+
+extern "C" int oosgpu_solve_device(oosgpu_factor* factor, double* b, int64_t ld, int64_t columns)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            factor->factor->solve(b, ld, columns, true);
+        });
+}
+
+extern "C" double oosgpu_last_solve_seconds(oosgpu_factor* factor)
+{
+    return factor == nullptr ? 0.0 : factor->factor->lastSolveSeconds();
+}
+
+extern "C" int oosgpu_model_plate(int32_t nx, int32_t ny, double lx, double ly, double thickness, double young,
+                                  double poisson, double pressure, oosgpu_model** out)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(out, "out");
+            auto handle = std::make_unique<oosgpu_model>();
+            handle->model = oosgpu::Model::plate(nx, ny, lx, ly, thickness, young, poisson, pressure);
+            *out = handle.release();
+        });
+}
+
+extern "C" int oosgpu_model_hex(int32_t n, double edge, double young, double poisson, double density,
+                                oosgpu_model** out)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(out, "out");
+            auto handle = std::make_unique<oosgpu_model>();
+            handle->model = oosgpu::Model::hexBlock(n, edge, young, poisson, density);
+            *out = handle.release();
+        });
+}
+
+extern "C" void oosgpu_model_destroy(oosgpu_model* model)
+{
+    delete model;
+}
+
+extern "C" int oosgpu_model_sizes(const oosgpu_model* model, int64_t sizes[4])
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(model, "model");
+            sizes[0] = model->model.nodeCount();
+            sizes[1] = model->model.nodeDofs();
+            sizes[2] = static_cast<int64_t>(model->model.neighbours().size());
+            sizes[3] = 0;
+        });
+}
+
+extern "C" int oosgpu_model_graph(const oosgpu_model* model, int64_t* offsets, int32_t* neighbours,
+                                  double* coordinates)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(model, "model");
+            const oosgpu::Model& m = model->model;
+            if (offsets != nullptr)
+                std::copy(m.offsets().begin(), m.offsets().end(), offsets);
+            if (neighbours != nullptr)
+                std::copy(m.neighbours().begin(), m.neighbours().end(), neighbours);
+            if (coordinates != nullptr)
+                std::copy(m.coordinates().begin(), m.coordinates().end(), coordinates);
+        });
+}
+
+extern "C" int oosgpu_model_csc_terms(const oosgpu_model* model, const int32_t* node_at_position, int64_t* terms)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(model, "model");
+            requirePointer(node_at_position, "node_at_position");
+            *terms = model->model.cscTermCount(node_at_position);
+        });
+}
+
+extern "C" int oosgpu_model_csc(const oosgpu_model* model, const int32_t* node_at_position, int32_t which,
+                                int64_t* col_offsets, int32_t* rows, double* values)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(model, "model");
+            requirePointer(node_at_position, "node_at_position");
+            model->model.toCsc(node_at_position, which, col_offsets, rows, values);
+        });
+}
+
+extern "C" int oosgpu_model_loads(const oosgpu_model* model, const int32_t* node_at_position, int64_t columns,
+                                  uint64_t seed_base, int32_t points, double sigma, double* rhs, int64_t ld)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(model, "model");
+            requirePointer(node_at_position, "node_at_position");
+            model->model.loads(node_at_position, columns, seed_base, points, sigma, rhs, ld);
+        });
+}
+
+extern "C" int oosgpu_factor_profile(oosgpu_factor* factor, int32_t enable)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            factor->factor->setProfile(enable != 0);
+        });
+}
+
+extern "C" int oosgpu_factor_kernel_stats(oosgpu_factor* factor, int32_t kinds, double* seconds, int64_t* launches,
+                                          double* flops, double* bytes)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            factor->factor->kernelStats(kinds, seconds, launches, flops, bytes);
+        });
+}
+
+extern "C" int oosgpu_factor_launch_counts(oosgpu_factor* factor, int64_t columns, int64_t counts[2])
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            counts[0] = factor->factor->factorLaunchCount();
+            counts[1] = factor->factor->solveLaunchCount(columns);
+        });
+}

@@ -1,0 +1,120 @@
+// Host-side C++ types of the library: the workload models, the symbolic structure the factorisation runs on and
+// the errors that the C ABI turns into status codes.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace oosgpu
+{
+
+// Status codes of the C ABI (include/oos_gpu.h), one per exception class of the reference's boundary.
+enum Status : int
+{
+    STATUS_OK = 0,
+    STATUS_INVALID_ARGUMENT = 1, // std::invalid_argument
+    STATUS_MEMORY_BUDGET = 2,    // base::MemoryBudgetError
+    STATUS_SINGULAR = 3,         // base::SingularityError
+    STATUS_CANCELLED = 4,        // base::OperationCancelledError
+    STATUS_CUDA = 5,             // a CUDA runtime error
+    STATUS_INTERNAL = 6,         // base::InternalError
+    STATUS_NOT_FACTORISED = 7,   // std::logic_error: a solve before a factorisation
+    STATUS_SOLVER = 8            // base::SolverError (Lanczos: contradicting Sturm counts, no usable shift)
+};
+
+// An error carrying its C-ABI status.
+class Error : public std::runtime_error
+{
+public:
+    Error(Status status, const std::string& message) : std::runtime_error(message), m_status(status) {}
+    [[nodiscard]] Status status() const noexcept { return m_status; }
+
+private:
+    Status m_status;
+};
+
+// A structured finite-element model: free nodes, their graph, node-block stiffness, lumped mass and loads.
+class Model
+{
+public:
+    Model();
+
+    // A flat plate nx by ny rectangular shells of lx by ly, clamped along x = 0.
+    [[nodiscard]] static Model plate(std::int32_t nx, std::int32_t ny, double lx, double ly, double thickness,
+                                     double young, double poisson, double pressure);
+    // A cube of n^3 trilinear hexahedra of edge `edge`, clamped on its base z = 0, lumped mass.
+    [[nodiscard]] static Model hexBlock(std::int32_t n, double edge, double young, double poisson, double density);
+
+    [[nodiscard]] std::int32_t nodeCount() const noexcept { return m_nodeCount; }
+    [[nodiscard]] int nodeDofs() const noexcept { return m_nodeDofs; }
+    [[nodiscard]] const std::vector<std::int64_t>& offsets() const noexcept { return m_offsets; }
+    [[nodiscard]] const std::vector<std::int32_t>& neighbours() const noexcept { return m_neighbours; }
+    [[nodiscard]] const std::vector<double>& coordinates() const noexcept { return m_coordinates; }
+    [[nodiscard]] const std::vector<std::int32_t>& gridIndex() const noexcept { return m_gridIndex; }
+
+    void firstColumns(const std::int32_t* nodeAtPosition, std::int32_t* firstColumnOfPosition) const;
+    [[nodiscard]] std::int64_t cscTermCount(const std::int32_t* nodeAtPosition) const;
+    void toCsc(const std::int32_t* nodeAtPosition, int which, std::int64_t* offsets, std::int32_t* rows,
+               double* values) const;
+    void loads(const std::int32_t* nodeAtPosition, std::int64_t columns, std::uint64_t seedBase,
+               std::int32_t pointsPerPattern, double sigma, double* rhs, std::int64_t ld) const;
+
+private:
+    void buildGraph(const std::vector<std::vector<std::int32_t>>& elements);
+    void assemble(const std::vector<std::vector<std::int32_t>>& elements, const double* elementMatrix, int nodeDofs);
+    [[nodiscard]] std::int64_t slot(std::int32_t node, std::int32_t neighbour) const;
+
+    std::int32_t m_nodeCount = 0;
+    int m_nodeDofs = 0;
+    std::vector<std::int64_t> m_offsets;
+    std::vector<std::int32_t> m_neighbours;
+    std::vector<double> m_coordinates;
+    std::vector<std::int32_t> m_gridIndex;
+    std::vector<std::vector<std::int32_t>> m_elementsOfNode;
+    std::vector<double> m_diagonalBlocks;
+    std::vector<double> m_offBlocks;
+    std::vector<double> m_lumpedMass;
+    std::vector<double> m_pressureLoad;
+};
+
+// The symbolic structure of a factorisation as the reference's SymbolicFactor exposes it
+// (include/oos/linalg/symbolic/SymbolicFactor.hpp:37-126): supernode s owns the DOF columns
+// [firstColumn[s], firstColumn[s + 1]), its rows below them are rows[rowStart[s] .. rowStart[s + 1]) ascending, and
+// parent[s] is -1 for a root. Children come before their parents.
+struct Symbolic
+{
+    std::int32_t dofCount = 0;
+    std::int32_t supernodeCount = 0;
+    std::vector<std::int32_t> firstColumn; // supernodeCount + 1
+    std::vector<std::int32_t> parent;      // supernodeCount
+    std::vector<std::int64_t> rowStart;    // supernodeCount + 1
+    std::vector<std::int32_t> rows;
+
+    [[nodiscard]] std::int32_t columnCount(std::int32_t s) const noexcept
+    {
+        return firstColumn[static_cast<std::size_t>(s) + 1] - firstColumn[static_cast<std::size_t>(s)];
+    }
+    [[nodiscard]] std::int32_t rowCount(std::int32_t s) const noexcept
+    {
+        return static_cast<std::int32_t>(rowStart[static_cast<std::size_t>(s) + 1] - rowStart[static_cast<std::size_t>(s)]);
+    }
+
+    // Checks the invariants the factorisation relies on; throws Error(STATUS_INVALID_ARGUMENT).
+    void validate() const;
+    // SymbolicFactor::flopCount (SymbolicFactor.hpp:97-99): per column with m entries below the diagonal,
+    // m(m + 1) + 2m.
+    [[nodiscard]] double flopCount() const;
+    [[nodiscard]] std::int64_t panelValueCount() const;
+    [[nodiscard]] std::int64_t factorEntryCount() const;
+};
+
+// The row structures of a supernode partition (SymbolicFactor.cpp:227-290): R(s) = (adjacency of the nodes of s
+// union R(children)) beyond the last position of s, expanded to DOF rows. nodeAtPosition: the final node order;
+// firstPosition: supernodeCount + 1 node positions; parent: per supernode.
+Symbolic rowStructures(std::int32_t nodeCount, const std::int64_t* offsets, const std::int32_t* neighbours,
+                       const std::int32_t* weights, const std::int32_t* nodeAtPosition, std::int32_t supernodeCount,
+                       const std::int32_t* firstPosition, const std::int32_t* parent);
+
+} // namespace oosgpu

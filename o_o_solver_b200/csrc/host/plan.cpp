@@ -1,0 +1,447 @@
+// Builds the GPU plan of a symbolic structure (plan.hpp).
+
+#include "plan.hpp"
+
+#include <algorithm>
+#include <string>
+
+namespace oosgpu
+{
+namespace
+{
+
+using device::AssemblyTask;
+using device::FrontDesc;
+using device::TileTask;
+
+constexpr int BLOCK = 64;
+constexpr int PANEL_ROWS = 128;
+
+void addList(Plan& plan, std::vector<Launch>& launches, LaunchKind kind, const std::vector<std::int32_t>& list,
+             std::int32_t k0 = 0, std::int32_t smemOrder = 0)
+{
+    if (list.empty())
+        return;
+    launches.push_back({kind, static_cast<std::int64_t>(plan.lists.size()), static_cast<std::int32_t>(list.size()), k0,
+                        smemOrder});
+    plan.lists.insert(plan.lists.end(), list.begin(), list.end());
+}
+
+void addTiles(Plan& plan, std::vector<Launch>& launches, LaunchKind kind, const std::vector<TileTask>& tiles,
+              std::int32_t k0 = 0)
+{
+    if (tiles.empty())
+        return;
+    launches.push_back({kind, static_cast<std::int64_t>(plan.tiles.size()), static_cast<std::int32_t>(tiles.size()), k0, 0});
+    plan.tiles.insert(plan.tiles.end(), tiles.begin(), tiles.end());
+}
+
+// Elements (i, j), i >= j, of a tile of m rows from i0 and n columns from j0 (lower part only when lower).
+double lowerElements(std::int64_t i0, std::int64_t j0, std::int64_t m, std::int64_t n, bool lower)
+{
+    if (!lower)
+        return static_cast<double>(m * n);
+    double count = 0.0;
+    for (std::int64_t jj = 0; jj < n; ++jj)
+    {
+        const std::int64_t firstRow = std::max<std::int64_t>(0, j0 + jj - i0);
+        if (firstRow < m)
+            count += static_cast<double>(m - firstRow);
+    }
+    return count;
+}
+
+// The factorisation flops of columns [k0, k1) of a front of order n: per column k, m = n - k - 1 below the diagonal,
+// m(m + 1) + 2m (SymbolicFactor::flopCount's count).
+double columnFlops(std::int64_t n, std::int64_t k0, std::int64_t k1)
+{
+    double flops = 0.0;
+    for (std::int64_t k = k0; k < k1; ++k)
+    {
+        const double m = static_cast<double>(n - k - 1);
+        flops += m * (m + 1.0) + 2.0 * m;
+    }
+    return flops;
+}
+
+} // namespace
+
+// The algorithmic flops and bytes of every launch of the factorisation (Launch::flops, Launch::bytes).
+void annotate(Plan& plan, const std::vector<std::int64_t>& cscTermsOfFront)
+{
+    constexpr double V = sizeof(double);
+    for (Launch& launch : plan.factorLaunches)
+    {
+        double flops = 0.0;
+        double bytes = 0.0;
+        const auto front = [&](std::int32_t s) -> const FrontDesc& { return plan.fronts[static_cast<std::size_t>(s)]; };
+        const auto childBytes = [&](const FrontDesc& f)
+        {
+            double b = 0.0;
+            for (std::int32_t q = 0; q < f.childCount; ++q)
+            {
+                const FrontDesc& ch = front(plan.children[static_cast<std::size_t>(f.childStart + q)]);
+                b += 3.0 * V * static_cast<double>(ch.r) * (ch.r + 1) / 2.0;
+            }
+            return b;
+        };
+        for (std::int32_t k = 0; k < launch.count; ++k)
+        {
+            const std::size_t at = static_cast<std::size_t>(launch.offset + k);
+            switch (launch.kind)
+            {
+            case LaunchKind::SmallFronts:
+            {
+                const std::int32_t s = plan.lists[at];
+                const FrontDesc& f = front(s);
+                const std::int64_t n = f.c + f.r;
+                flops += columnFlops(n, 0, f.c);
+                // The front's children read, its CSC terms read, its panel and update matrix written.
+                bytes += childBytes(f) / 3.0 + 12.0 * static_cast<double>(cscTermsOfFront[static_cast<std::size_t>(s)]) +
+                         V * static_cast<double>(n * f.c) + V * static_cast<double>(f.r) * (f.r + 1) / 2.0;
+                break;
+            }
+            case LaunchKind::AssembleFronts:
+            {
+                const AssemblyTask& piece = plan.pieces[at];
+                const FrontDesc& f = front(piece.front);
+                const std::int64_t n = f.c + f.r;
+                for (std::int64_t j = piece.j0; j < piece.j1; ++j)
+                    bytes += V * static_cast<double>(j < f.c ? n : n - j);
+                if (piece.j0 == 0)
+                    bytes += childBytes(f) + 12.0 * static_cast<double>(cscTermsOfFront[static_cast<std::size_t>(piece.front)]);
+                break;
+            }
+            case LaunchKind::DiagonalBlocks:
+            {
+                const FrontDesc& f = front(plan.lists[at]);
+                const std::int64_t kb = std::min<std::int64_t>(BLOCK, f.c - launch.k0);
+                flops += columnFlops(kb, 0, kb);
+                bytes += 2.0 * V * static_cast<double>(kb * (kb + 1) / 2);
+                break;
+            }
+            case LaunchKind::PanelRows:
+            {
+                const TileTask& t = plan.tiles[at];
+                const FrontDesc& f = front(t.front);
+                const std::int64_t n = f.c + f.r;
+                const std::int64_t kb = std::min<std::int64_t>(BLOCK, f.c - launch.k0);
+                const std::int64_t rows = std::min<std::int64_t>(PANEL_ROWS, n - t.i0);
+                flops += static_cast<double>(rows) * static_cast<double>(kb * (kb - 1) + kb);
+                bytes += 2.0 * V * static_cast<double>(rows * kb);
+                break;
+            }
+            case LaunchKind::PanelUpdate:
+            {
+                const TileTask& t = plan.tiles[at];
+                const FrontDesc& f = front(t.front);
+                const std::int64_t n = f.c + f.r;
+                const std::int64_t m = std::min<std::int64_t>(device::TILE, n - t.i0);
+                const std::int64_t w = std::min<std::int64_t>(device::TILE, f.c - t.j0);
+                const double elements = lowerElements(t.i0, t.j0, m, w, t.i0 == t.j0);
+                flops += 2.0 * BLOCK * elements;
+                bytes += 2.0 * V * elements;
+                break;
+            }
+            case LaunchKind::UpdateMatrix:
+            {
+                const TileTask& t = plan.tiles[at];
+                const FrontDesc& f = front(t.front);
+                const std::int64_t m = std::min<std::int64_t>(device::TILE, f.r - t.i0);
+                const std::int64_t w = std::min<std::int64_t>(device::TILE, f.r - t.j0);
+                const double elements = lowerElements(t.i0, t.j0, m, w, t.i0 == t.j0);
+                flops += 2.0 * static_cast<double>(f.c) * elements;
+                bytes += 2.0 * V * elements;
+                break;
+            }
+            default:
+                break;
+            }
+        }
+        launch.flops = flops;
+        launch.bytes = bytes;
+    }
+}
+
+Plan buildPlan(const Symbolic& symbolic)
+{
+    Plan plan;
+    const std::int32_t count = symbolic.supernodeCount;
+    const auto total = static_cast<std::size_t>(count);
+    plan.dimension = symbolic.dofCount;
+    plan.supernodeCount = count;
+    plan.fronts.resize(total);
+    plan.rows = symbolic.rows;
+    plan.rowEntries = static_cast<std::int64_t>(symbolic.rows.size());
+    plan.flops = symbolic.flopCount();
+    plan.factorEntries = symbolic.factorEntryCount();
+
+    // Children, in increasing order.
+    std::vector<std::int32_t> childCount(total, 0);
+    for (std::int32_t s = 0; s < count; ++s)
+        if (symbolic.parent[static_cast<std::size_t>(s)] >= 0)
+            ++childCount[static_cast<std::size_t>(symbolic.parent[static_cast<std::size_t>(s)])];
+    std::vector<std::int32_t> childStart(total + 1, 0);
+    for (std::size_t s = 0; s < total; ++s)
+        childStart[s + 1] = childStart[s] + childCount[s];
+    plan.children.assign(static_cast<std::size_t>(childStart[total]), 0);
+    {
+        std::vector<std::int32_t> next(childStart.begin(), childStart.end() - 1);
+        for (std::int32_t s = 0; s < count; ++s)
+        {
+            const std::int32_t p = symbolic.parent[static_cast<std::size_t>(s)];
+            if (p >= 0)
+                plan.children[static_cast<std::size_t>(next[static_cast<std::size_t>(p)]++)] = s;
+        }
+    }
+
+    // Descriptors: the panels in the reference's layout (supernode s at the sum of c(c + r) before it), the update
+    // matrices each its own r x r block.
+    std::int64_t panel = 0;
+    std::int64_t update = 0;
+    for (std::int32_t s = 0; s < count; ++s)
+    {
+        const auto at = static_cast<std::size_t>(s);
+        FrontDesc& f = plan.fronts[at];
+        const std::int64_t c = symbolic.columnCount(s);
+        const std::int64_t r = symbolic.rowCount(s);
+        f.panel = panel;
+        f.update = update;
+        f.rowStart = symbolic.rowStart[at];
+        f.first = symbolic.firstColumn[at];
+        f.c = static_cast<std::int32_t>(c);
+        f.r = static_cast<std::int32_t>(r);
+        f.childStart = childStart[at];
+        f.childCount = childCount[at];
+        f.parent = symbolic.parent[at];
+        panel += c * (c + r);
+        update += r * r;
+    }
+    plan.panelValues = panel;
+    plan.updateValues = update;
+
+    // Positions of each supernode's rows in its parent's front (both ascending: a merge).
+    plan.relpos.assign(symbolic.rows.size(), 0);
+    for (std::int32_t s = 0; s < count; ++s)
+    {
+        const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+        if (f.parent < 0)
+            continue;
+        const FrontDesc& p = plan.fronts[static_cast<std::size_t>(f.parent)];
+        std::int64_t cursor = p.rowStart;
+        const std::int64_t end = p.rowStart + p.r;
+        for (std::int64_t k = f.rowStart; k < f.rowStart + f.r; ++k)
+        {
+            const std::int32_t row = symbolic.rows[static_cast<std::size_t>(k)];
+            if (row >= p.first && row < p.first + p.c)
+            {
+                plan.relpos[static_cast<std::size_t>(k)] = row - p.first;
+                continue;
+            }
+            while (cursor < end && symbolic.rows[static_cast<std::size_t>(cursor)] < row)
+                ++cursor;
+            if (cursor == end || symbolic.rows[static_cast<std::size_t>(cursor)] != row)
+                throw Error(STATUS_INVALID_ARGUMENT, "plan: row " + std::to_string(row) + " of supernode " +
+                                                         std::to_string(s) + " is not in its parent's front");
+            plan.relpos[static_cast<std::size_t>(k)] = p.c + static_cast<std::int32_t>(cursor - p.rowStart);
+        }
+    }
+
+    plan.supernodeOfColumn.assign(static_cast<std::size_t>(plan.dimension), 0);
+    for (std::int32_t s = 0; s < count; ++s)
+        for (std::int32_t j = symbolic.firstColumn[static_cast<std::size_t>(s)];
+             j < symbolic.firstColumn[static_cast<std::size_t>(s) + 1]; ++j)
+            plan.supernodeOfColumn[static_cast<std::size_t>(j)] = s;
+
+    // Levels.
+    plan.level.assign(total, 0);
+    std::int32_t maxLevel = 0;
+    for (std::int32_t s = 0; s < count; ++s)
+    {
+        const std::int32_t p = symbolic.parent[static_cast<std::size_t>(s)];
+        if (p >= 0)
+            plan.level[static_cast<std::size_t>(p)] =
+                std::max(plan.level[static_cast<std::size_t>(p)], plan.level[static_cast<std::size_t>(s)] + 1);
+        maxLevel = std::max(maxLevel, plan.level[static_cast<std::size_t>(s)]);
+    }
+    plan.levelCount = count == 0 ? 0 : maxLevel + 1;
+    std::vector<std::vector<std::int32_t>> byLevel(static_cast<std::size_t>(plan.levelCount));
+    for (std::int32_t s = 0; s < count; ++s)
+        byLevel[static_cast<std::size_t>(plan.level[static_cast<std::size_t>(s)])].push_back(s);
+
+    std::vector<std::vector<Launch>> backwardByLevel(static_cast<std::size_t>(plan.levelCount));
+    for (std::int32_t level = 0; level < plan.levelCount; ++level)
+    {
+        const auto& members = byLevel[static_cast<std::size_t>(level)];
+        // ---- factorisation ----
+        std::vector<std::int32_t> small64;
+        std::vector<std::int32_t> small128;
+        std::vector<std::int32_t> large;
+        std::int32_t order64 = 0;
+        std::int32_t order128 = 0;
+        for (const std::int32_t s : members)
+        {
+            const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+            const std::int32_t n = f.c + f.r;
+            if (n <= SMALL_ORDER_LOW)
+            {
+                small64.push_back(s);
+                order64 = std::max(order64, n);
+            }
+            else if (n <= SMALL_ORDER)
+            {
+                small128.push_back(s);
+                order128 = std::max(order128, n);
+            }
+            else
+                large.push_back(s);
+        }
+        plan.largestSmallOrder = std::max({plan.largestSmallOrder, order64, order128});
+        addList(plan, plan.factorLaunches, LaunchKind::SmallFronts, small64, 0, order64);
+        addList(plan, plan.factorLaunches, LaunchKind::SmallFronts, small128, 0, order128);
+        if (!large.empty())
+        {
+            std::vector<AssemblyTask> pieces;
+            std::int32_t maxColumns = 0;
+            for (const std::int32_t s : large)
+            {
+                const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+                const std::int32_t n = f.c + f.r;
+                maxColumns = std::max(maxColumns, f.c);
+                std::int64_t values = 0;
+                std::int32_t start = 0;
+                for (std::int32_t p = 0; p < n; ++p)
+                {
+                    values += n - p;
+                    if (values >= ASSEMBLY_PIECE_VALUES || p + 1 == n)
+                    {
+                        pieces.push_back({s, start, p + 1, 0});
+                        start = p + 1;
+                        values = 0;
+                    }
+                }
+            }
+            plan.factorLaunches.push_back({LaunchKind::AssembleFronts, static_cast<std::int64_t>(plan.pieces.size()),
+                                           static_cast<std::int32_t>(pieces.size()), 0, 0});
+            plan.pieces.insert(plan.pieces.end(), pieces.begin(), pieces.end());
+            for (std::int32_t k0 = 0; k0 < maxColumns; k0 += BLOCK)
+            {
+                std::vector<std::int32_t> diagonal;
+                std::vector<TileTask> rowTasks;
+                std::vector<TileTask> updateTiles;
+                for (const std::int32_t s : large)
+                {
+                    const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+                    if (f.c <= k0)
+                        continue;
+                    const std::int32_t n = f.c + f.r;
+                    const std::int32_t kb = std::min(BLOCK, f.c - k0);
+                    diagonal.push_back(s);
+                    for (std::int32_t i0 = k0 + kb; i0 < n; i0 += PANEL_ROWS)
+                        rowTasks.push_back({s, i0, 0, 0});
+                    const std::int32_t origin = k0 + BLOCK;
+                    for (std::int32_t j0 = origin; j0 < f.c; j0 += device::TILE)
+                        for (std::int32_t i0 = j0; i0 < n; i0 += device::TILE)
+                            updateTiles.push_back({s, i0, j0, 0});
+                }
+                addList(plan, plan.factorLaunches, LaunchKind::DiagonalBlocks, diagonal, k0);
+                addTiles(plan, plan.factorLaunches, LaunchKind::PanelRows, rowTasks, k0);
+                addTiles(plan, plan.factorLaunches, LaunchKind::PanelUpdate, updateTiles, k0);
+            }
+            std::vector<TileTask> schur;
+            for (const std::int32_t s : large)
+            {
+                const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+                for (std::int32_t j0 = 0; j0 < f.r; j0 += device::TILE)
+                    for (std::int32_t i0 = j0; i0 < f.r; i0 += device::TILE)
+                        schur.push_back({s, i0, j0, 0});
+            }
+            // The longest products first (a tile's work grows with the front's columns).
+            std::stable_sort(schur.begin(), schur.end(), [&](const TileTask& x, const TileTask& y)
+                             { return plan.fronts[static_cast<std::size_t>(x.front)].c >
+                                      plan.fronts[static_cast<std::size_t>(y.front)].c; });
+            addTiles(plan, plan.factorLaunches, LaunchKind::UpdateMatrix, schur);
+        }
+
+        // ---- forward sweep ----
+        std::vector<std::int32_t> solveSmall;
+        std::vector<std::int32_t> solveLarge;
+        std::int32_t maxSmallColumns = 0;
+        std::int32_t maxColumns = 0;
+        for (const std::int32_t s : members)
+        {
+            const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+            if (f.c <= SOLVE_SMALL_COLUMNS)
+            {
+                solveSmall.push_back(s);
+                maxSmallColumns = std::max(maxSmallColumns, f.c);
+            }
+            else
+            {
+                solveLarge.push_back(s);
+                maxColumns = std::max(maxColumns, f.c);
+            }
+        }
+        addList(plan, plan.forwardLaunches, LaunchKind::ForwardSmall, solveSmall, 0, maxSmallColumns);
+        addList(plan, plan.forwardLaunches, LaunchKind::ForwardGather, solveLarge);
+        for (std::int32_t k0 = 0; k0 < maxColumns; k0 += BLOCK)
+        {
+            std::vector<std::int32_t> diagonal;
+            std::vector<TileTask> below;
+            for (const std::int32_t s : solveLarge)
+            {
+                const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+                if (f.c <= k0)
+                    continue;
+                diagonal.push_back(s);
+                const std::int32_t kb = std::min(BLOCK, f.c - k0);
+                for (std::int32_t i0 = k0 + kb; i0 < f.c; i0 += device::TILE)
+                    below.push_back({s, i0, 0, 0});
+                for (std::int32_t i0 = f.c; i0 < f.c + f.r; i0 += device::TILE)
+                    below.push_back({s, i0, 0, 1});
+            }
+            addList(plan, plan.forwardLaunches, LaunchKind::ForwardDiagonal, diagonal, k0);
+            addTiles(plan, plan.forwardLaunches, LaunchKind::ForwardUpdate, below, k0);
+        }
+
+        // ---- backward sweep (collected per level, emitted top level first) ----
+        std::vector<Launch>& backward = backwardByLevel[static_cast<std::size_t>(level)];
+        addList(plan, backward, LaunchKind::BackwardSmall, solveSmall, 0, maxSmallColumns);
+        std::vector<TileTask> rowTiles;
+        for (const std::int32_t s : solveLarge)
+        {
+            const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+            if (f.r == 0)
+                continue;
+            for (std::int32_t i0 = 0; i0 < f.c; i0 += device::TILE)
+                rowTiles.push_back({s, i0, 0, 0});
+        }
+        addTiles(plan, backward, LaunchKind::BackwardRows, rowTiles);
+        const std::int32_t steps = (maxColumns + BLOCK - 1) / BLOCK;
+        for (std::int32_t t = steps - 1; t >= 0; --t)
+        {
+            const std::int32_t k0 = t * BLOCK;
+            std::vector<std::int32_t> diagonal;
+            std::vector<TileTask> above;
+            for (const std::int32_t s : solveLarge)
+            {
+                const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+                if (f.c <= k0)
+                    continue;
+                diagonal.push_back(s);
+                for (std::int32_t i0 = 0; i0 < k0; i0 += device::TILE)
+                    above.push_back({s, i0, 0, 0});
+            }
+            addList(plan, backward, LaunchKind::BackwardDiagonal, diagonal, k0);
+            addTiles(plan, backward, LaunchKind::BackwardUpdate, above, k0);
+        }
+    }
+    for (std::int32_t level = plan.levelCount; level-- > 0;)
+    {
+        const auto& launches = backwardByLevel[static_cast<std::size_t>(level)];
+        plan.backwardLaunches.insert(plan.backwardLaunches.end(), launches.begin(), launches.end());
+    }
+    return plan;
+}
+
+} // namespace oosgpu

@@ -1,0 +1,94 @@
+// The plan of a factorisation on the GPU, built once per symbolic structure on the host (the counterpart of the
+// reference's FactorSchedule and SolvePlan, src/linalg/supernodal/FactorSchedule.cpp:24-120, SolvePlan.cpp:59): the
+// front descriptors, the positions of every child's rows in its parent's front, the levels of the supernode tree
+// (a supernode's level is one more than its highest child's: the fronts of one level are independent), and for
+// each level the batched launches of the factorisation and of the sweeps.
+#pragma once
+
+#include "../device/common.cuh"
+#include "host_api.hpp"
+
+#include <cstdint>
+#include <vector>
+
+namespace oosgpu
+{
+
+// Fronts whose order is at most SMALL_ORDER are factorised whole in shared memory, one block each.
+constexpr int SMALL_ORDER_LOW = 64;
+constexpr int SMALL_ORDER = 128;
+// The columns of a large front's assembly piece: about this many elements of its lower triangle.
+constexpr std::int64_t ASSEMBLY_PIECE_VALUES = std::int64_t{1} << 16;
+// Supernodes with at most this many columns are swept by one block.
+constexpr int SOLVE_SMALL_COLUMNS = 64;
+
+enum class LaunchKind : int
+{
+    SmallFronts,
+    AssembleFronts,
+    DiagonalBlocks,
+    PanelRows,
+    PanelUpdate,
+    UpdateMatrix,
+    ForwardSmall,
+    ForwardGather,
+    ForwardDiagonal,
+    ForwardUpdate,
+    BackwardSmall,
+    BackwardRows,
+    BackwardDiagonal,
+    BackwardUpdate
+};
+
+// One batched launch: `count` items from `offset` in the array of its kind (front lists: int32; tiles: TileTask;
+// assembly pieces: AssemblyTask); k0 the step's first column; smemOrder the largest front order of a small batch.
+struct Launch
+{
+    LaunchKind kind;
+    std::int64_t offset;
+    std::int32_t count;
+    std::int32_t k0;
+    std::int32_t smemOrder;
+    // Algorithmic work of the launch (the roofline's numerator): useful flops (the multiply-adds of the lower
+    // triangles a launch updates, twice) and the bytes it must move at least.
+    double flops = 0.0;
+    double bytes = 0.0;
+};
+
+constexpr int LAUNCH_KIND_COUNT = 14;
+
+struct Plan
+{
+    std::int32_t dimension = 0;
+    std::int32_t supernodeCount = 0;
+    std::int32_t levelCount = 0;
+    std::vector<device::FrontDesc> fronts;
+    std::vector<std::int32_t> children;
+    std::vector<std::int32_t> rows;
+    std::vector<std::int32_t> relpos;
+    std::vector<std::int32_t> supernodeOfColumn;
+    std::vector<std::int32_t> level;
+    std::int64_t panelValues = 0;
+    std::int64_t updateValues = 0;
+    std::int64_t rowEntries = 0;
+    std::int32_t largestSmallOrder = 0;
+    double flops = 0.0;
+    std::int64_t factorEntries = 0;
+
+    // Task arrays (uploaded once) and the launch sequences that index them.
+    std::vector<std::int32_t> lists;
+    std::vector<device::TileTask> tiles;
+    std::vector<device::AssemblyTask> pieces;
+    std::vector<Launch> factorLaunches;
+    std::vector<Launch> forwardLaunches;
+    std::vector<Launch> backwardLaunches;
+};
+
+// Builds the plan of a validated symbolic structure.
+Plan buildPlan(const Symbolic& symbolic);
+
+// Sets the algorithmic flops and bytes of every factorisation launch; cscTermsOfFront: the matrix terms in each
+// supernode's columns.
+void annotate(Plan& plan, const std::vector<std::int64_t>& cscTermsOfFront);
+
+} // namespace oosgpu

@@ -1,0 +1,330 @@
+"""The reference's factorisation interface over the GPU library, with the same names, argument meanings and errors
+(jcdulas/O_o_Solver, include/oos/linalg): SymbolicFactor (the structure a factorisation is given), SupernodalFactor
+.factorise, FactorSolve.solve, the FactorOptions / PivotPolicy fields, and the exceptions the C ABI's status codes map
+(SingularityError, MemoryBudgetError, ...).
+
+Every call runs the CUDA library (include/oos_gpu.h); nothing here computes on the CPU.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as nat
+
+# ---- errors: one per status code (include/oos_gpu.h), named after the reference's exceptions ----------------------
+
+
+class SolverError(RuntimeError):
+    """base::SolverError."""
+
+
+class SingularityError(SolverError):
+    """base::SingularityError: a zero pivot, or pivots flagged by the ratio test with SingularityBailOut >= 0."""
+
+
+class MemoryBudgetError(MemoryError):
+    """base::MemoryBudgetError (device memory)."""
+
+
+class OperationCancelledError(RuntimeError):
+    """base::OperationCancelledError."""
+
+
+class CudaError(RuntimeError):
+    """A CUDA runtime error (no counterpart in the CPU reference)."""
+
+
+class InternalError(RuntimeError):
+    """base::InternalError."""
+
+
+_ERRORS = {
+    1: ValueError,  # std::invalid_argument
+    2: MemoryBudgetError,
+    3: SingularityError,
+    4: OperationCancelledError,
+    5: CudaError,
+    6: InternalError,
+    7: RuntimeError,  # std::logic_error: solve before factorise
+    8: SolverError,
+}
+
+
+def _check(status: int):
+    if status != 0:
+        raise _ERRORS.get(status, RuntimeError)(nat.load().oosgpu_last_error().decode())
+
+
+def device_count() -> int:
+    return int(nat.load().oosgpu_device_count())
+
+
+# ---- symbolic structure ----------------------------------------------------------------------------------------------
+
+
+class SymbolicFactor:
+    """The symbolic structure of a factorisation (include/oos/linalg/symbolic/SymbolicFactor.hpp:37-126): supernode s
+    owns the DOF columns [first_column[s], first_column[s + 1]), its rows below them are rows(s), ascending, and
+    parent[s] is -1 for a root."""
+
+    def __init__(self, handle):
+        self._handle = handle
+        sizes = np.zeros(8, dtype=np.int64)
+        flops = ctypes.c_double()
+        _check(nat.load().oosgpu_symbolic_sizes(handle, nat.ptr(sizes, nat.i64p), ctypes.byref(flops)))
+        (self.dof_count, self.supernode_count, self.row_entry_count, self.panel_value_count,
+         self.factor_entry_count, self.level_count, self.update_value_count) = (int(v) for v in sizes[:7])
+        self.flop_count = float(flops.value)
+
+    @classmethod
+    def from_arrays(cls, dof_count, first_column, parent, row_start, rows):
+        first_column = np.ascontiguousarray(first_column, dtype=np.int32)
+        parent = np.ascontiguousarray(parent, dtype=np.int32)
+        row_start = np.ascontiguousarray(row_start, dtype=np.int64)
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+        handle = nat.vp()
+        _check(nat.load().oosgpu_symbolic_create(int(dof_count), len(parent), nat.ptr(first_column, nat.i32p),
+                                                 nat.ptr(parent, nat.i32p), nat.ptr(row_start, nat.i64p),
+                                                 nat.ptr(rows, nat.i32p), ctypes.byref(handle)))
+        return cls(handle)
+
+    @classmethod
+    def from_partition(cls, offsets, neighbours, weights, node_at_position, first_position, parent):
+        """The row structures of a supernode partition of the final node order (SymbolicFactor::analyse's last
+        step)."""
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        neighbours = np.ascontiguousarray(neighbours, dtype=np.int32)
+        weights = np.ascontiguousarray(weights, dtype=np.int32)
+        order = np.ascontiguousarray(node_at_position, dtype=np.int32)
+        first_position = np.ascontiguousarray(first_position, dtype=np.int32)
+        parent = np.ascontiguousarray(parent, dtype=np.int32)
+        handle = nat.vp()
+        _check(nat.load().oosgpu_symbolic_from_partition(len(weights), nat.ptr(offsets, nat.i64p),
+                                                         nat.ptr(neighbours, nat.i32p), nat.ptr(weights, nat.i32p),
+                                                         nat.ptr(order, nat.i32p), len(parent),
+                                                         nat.ptr(first_position, nat.i32p), nat.ptr(parent, nat.i32p),
+                                                         ctypes.byref(handle)))
+        return cls(handle)
+
+    def row_structure(self):
+        row_start = np.zeros(self.supernode_count + 1, dtype=np.int64)
+        rows = np.zeros(max(self.row_entry_count, 1), dtype=np.int32)
+        _check(nat.load().oosgpu_symbolic_rows(self._handle, nat.ptr(row_start, nat.i64p), nat.ptr(rows, nat.i32p)))
+        return row_start, rows[: self.row_entry_count]
+
+    def close(self):
+        if self._handle:
+            nat.load().oosgpu_symbolic_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- factorisation ---------------------------------------------------------------------------------------------------
+
+
+@dataclass
+class PivotPolicy:
+    """PivotPolicy (include/oos/linalg/supernodal/PivotDiagnostics.hpp:34-44)."""
+
+    max_ratio: float = 1.0e7
+    bailout: int = 0
+
+
+@dataclass
+class FactorOptions:
+    """FactorOptions (SupernodalFactor.hpp:63-97) of the positive definite mode."""
+
+    pivot_policy: PivotPolicy = field(default_factory=PivotPolicy)
+    reference_diagonal: np.ndarray | None = None
+
+
+@dataclass
+class Inertia:
+    positive: int = 0
+    negative: int = 0
+    zero: int = 0
+
+
+@dataclass
+class PivotDiagnostics:
+    issue_count: int = 0
+    largest_ratio: float = 0.0
+    equation_of_largest_ratio: int = -1
+    issues: list = field(default_factory=list)
+
+
+class SymmetricCsc:
+    """A lower-triangle CSC in the factor's equation order (SymmetricCsc.hpp:40-103): int64 column offsets, int32 rows
+    ascending from the diagonal, float64 values. Host arrays, or device tensors (torch) for the device entry points."""
+
+    def __init__(self, offsets, rows, values):
+        self.offsets = offsets
+        self.rows = rows
+        self.values = values
+
+    @property
+    def dimension(self) -> int:
+        return len(self.offsets) - 1
+
+
+class SupernodalFactor:
+    """The numeric LDL^T of a sparse symmetric matrix on the GPU (SupernodalFactor.hpp:171-292), positive definite
+    mode. factorise() allocates the panels and update matrices on the device on its first call; later calls on the same
+    structure reuse them (the reference's FactorOptions::storage)."""
+
+    def __init__(self, symbolic: SymbolicFactor, device: int = 0):
+        self.symbolic = symbolic
+        self._handle = nat.vp()
+        _check(nat.load().oosgpu_factor_create(symbolic._handle, device, ctypes.byref(self._handle)))
+        self.inertia = Inertia()
+        self.pivot_diagnostics = PivotDiagnostics()
+        self.device_seconds = 0.0
+        self.zero_pivots = []
+
+    @classmethod
+    def factorise(cls, symbolic: SymbolicFactor, matrix: SymmetricCsc, options: FactorOptions | None = None,
+                  device: int = 0) -> "SupernodalFactor":
+        factor = cls(symbolic, device)
+        factor.refactorise(matrix, options)
+        return factor
+
+    def _options(self, options):
+        options = options or FactorOptions()
+        native = nat.FactorOptions()
+        native.max_ratio = options.pivot_policy.max_ratio
+        native.bailout = options.pivot_policy.bailout
+        self._reference = None
+        if options.reference_diagonal is not None:
+            self._reference = np.ascontiguousarray(options.reference_diagonal, dtype=np.float64)
+            native.reference_diagonal = nat.ptr(self._reference, nat.f64p)
+        return native
+
+    def refactorise(self, matrix: SymmetricCsc, options: FactorOptions | None = None):
+        """A new factorisation of a matrix of the same structure (host or device arrays)."""
+        native = self._options(options)
+        info = nat.FactorInfo()
+        lib = nat.load()
+        if isinstance(matrix.offsets, np.ndarray):
+            offsets = np.ascontiguousarray(matrix.offsets, dtype=np.int64)
+            rows = np.ascontiguousarray(matrix.rows, dtype=np.int32)
+            values = np.ascontiguousarray(matrix.values, dtype=np.float64)
+            status = lib.oosgpu_factorise(self._handle, len(offsets) - 1, nat.ptr(offsets, nat.i64p),
+                                          nat.ptr(rows, nat.i32p), nat.ptr(values, nat.f64p), ctypes.byref(native),
+                                          ctypes.byref(info))
+        else:
+            status = lib.oosgpu_factorise_device(self._handle, matrix.offsets.numel() - 1, matrix.rows.numel(),
+                                                 matrix.offsets.data_ptr(), matrix.rows.data_ptr(),
+                                                 matrix.values.data_ptr(), ctypes.byref(native), ctypes.byref(info))
+        self._record(info)
+        _check(status)
+        return self
+
+    def _record(self, info):
+        self.inertia = Inertia(int(info.positive), int(info.negative), int(info.zero))
+        self.pivot_diagnostics = PivotDiagnostics(int(info.issue_count), float(info.largest_ratio),
+                                                  int(info.equation_of_largest),
+                                                  list(info.issues[: min(16, int(info.issue_count))]))
+        self.zero_pivots = list(info.zero_pivots[: min(16, int(info.zero_pivot_count))])
+        self.delayed_pivot_count = int(info.delayed)
+        self.two_by_two_pivot_count = int(info.two_by_two)
+        self.device_seconds = float(info.device_seconds)
+
+    @property
+    def stream(self) -> int:
+        return int(nat.load().oosgpu_factor_stream(self._handle) or 0)
+
+    KERNEL_KINDS = ["small_fronts", "assemble_fronts", "diagonal_blocks", "panel_rows", "panel_update",
+                    "update_matrix"]
+
+    def profile(self, enable: bool = True):
+        """Brackets every launch of the following factorisations with CUDA events (kernel_stats())."""
+        _check(nat.load().oosgpu_factor_profile(self._handle, 1 if enable else 0))
+
+    def kernel_stats(self) -> dict:
+        """Per kernel kind of the last profiled factorisation: device seconds, launches, algorithmic flops, bytes."""
+        kinds = len(self.KERNEL_KINDS)
+        seconds = np.zeros(kinds)
+        launches = np.zeros(kinds, dtype=np.int64)
+        flops = np.zeros(kinds)
+        bytes_ = np.zeros(kinds)
+        _check(nat.load().oosgpu_factor_kernel_stats(self._handle, kinds, nat.ptr(seconds, nat.f64p),
+                                                     nat.ptr(launches, nat.i64p), nat.ptr(flops, nat.f64p),
+                                                     nat.ptr(bytes_, nat.f64p)))
+        return {name: {"seconds": float(seconds[k]), "launches": int(launches[k]), "flops": float(flops[k]),
+                       "bytes": float(bytes_[k])} for k, name in enumerate(self.KERNEL_KINDS)}
+
+    def launch_counts(self, columns: int):
+        """(kernels of one factorisation, kernels of one solve of `columns` right-hand sides)."""
+        counts = np.zeros(2, dtype=np.int64)
+        _check(nat.load().oosgpu_factor_launch_counts(self._handle, columns, nat.ptr(counts, nat.i64p)))
+        return int(counts[0]), int(counts[1])
+
+    def panel(self, s: int):
+        """(values rows x eliminated, row equations, subdiagonal) of supernode s (SupernodalFactor::panel)."""
+        lib = nat.load()
+        e = ctypes.c_int64()
+        r = ctypes.c_int64()
+        _check(lib.oosgpu_factor_panel(self._handle, s, ctypes.byref(e), ctypes.byref(r), None, None, None))
+        values = np.zeros((e.value, r.value))
+        rows = np.zeros(r.value, dtype=np.int32)
+        sub = np.zeros(max(e.value, 1))
+        _check(lib.oosgpu_factor_panel(self._handle, s, ctypes.byref(e), ctypes.byref(r), nat.ptr(values, nat.f64p),
+                                       nat.ptr(rows, nat.i32p), nat.ptr(sub, nat.f64p)))
+        return values.T.copy(), rows, sub[: e.value]
+
+    def close(self):
+        if self._handle:
+            nat.load().oosgpu_factor_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FactorSolve:
+    """Solves with a supernodal factor (FactorSolve.hpp:59-100): B <- A^-1 B for many right-hand sides."""
+
+    def __init__(self, factor: SupernodalFactor):
+        self.factor = factor
+        self.device_seconds = 0.0
+
+    def solve(self, b):
+        """In place on a float64 array (n,) or (n, k) (host: Fortran order or a column; device: a torch tensor whose
+        columns are contiguous, i.e. the transpose of a contiguous (k, n) tensor, or a 1-D tensor)."""
+        lib = nat.load()
+        if isinstance(b, np.ndarray):
+            if b.dtype != np.float64:
+                raise ValueError("FactorSolve.solve: expected float64 right-hand sides")
+            if b.ndim == 1:
+                if not b.flags.c_contiguous:
+                    raise ValueError("FactorSolve.solve: expected a contiguous vector")
+                n, k, ld = b.shape[0], 1, b.shape[0]
+            else:
+                if not b.flags.f_contiguous:
+                    raise ValueError("FactorSolve.solve: expected a column-major (Fortran-order) block")
+                n, k = b.shape
+                ld = n
+            _check(lib.oosgpu_solve(self.factor._handle, nat.ptr(b, nat.f64p), ld, k))
+        else:
+            if b.dim() == 1:
+                n, k, ld = b.shape[0], 1, b.shape[0]
+            else:
+                n, k = b.shape
+                if b.stride(0) != 1:
+                    raise ValueError("FactorSolve.solve: expected a device block with contiguous columns")
+                ld = b.stride(1) if k > 1 else n
+            _check(lib.oosgpu_solve_device(self.factor._handle, b.data_ptr(), ld, k))
+        self.device_seconds = float(lib.oosgpu_last_solve_seconds(self.factor._handle))
+        return b

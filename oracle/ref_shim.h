@@ -1,0 +1,80 @@
+/* C entry points over the reference's own linear algebra (jcdulas/O_o_Solver, modules base + linalg), built from its
+ * sources by oracle/Makefile into oracle/_ref/liboos_ref.so.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is the checker of the GPU path (tests, smoke, the CPU-baseline leg of the
+ * benchmark); the product never links or calls it.
+ *
+ * Every function returns 0 on success, or -1 with a message in the shim's last-error buffer (ref_last_error) when
+ * the reference threw. Arrays are caller-owned. */
+#ifndef OOS_REF_SHIM_H
+#define OOS_REF_SHIM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ref_symbolic ref_symbolic;
+typedef struct ref_factor ref_factor;
+
+const char* ref_last_error(void);
+
+/* ConstrainedOrdering::order (src/linalg/ordering/ConstrainedOrdering.cpp:28-66) then SymbolicFactor::analyse
+ * (src/linalg/symbolic/SymbolicFactor.cpp:167) on a node graph. method: 0 automatic, 1 minimum degree,
+ * 2 nested dissection, 3 natural; 4 = the order given in `given_order` (node at each position). amalgamate: 1 the
+ * default AmalgamationThresholds, 0 none (fundamental supernodes). coords: 3 doubles per node, or NULL. */
+ref_symbolic* ref_analyse(int32_t node_count, const int64_t* offsets, const int32_t* neighbours,
+                          const int32_t* weights, const double* coords, int method, const int32_t* given_order,
+                          int amalgamate, int threads);
+void ref_symbolic_free(ref_symbolic* s);
+
+/* sizes[0..9]: nodes, dofs, supernodes, row entries, panel values, factor entries, largest front values,
+ * update-stack peak values, trailing dofs, 0 */
+void ref_sym_sizes(const ref_symbolic* s, int64_t sizes[10]);
+double ref_sym_flops(const ref_symbolic* s);
+/* seconds spent in ordering and in analyse */
+void ref_sym_times(const ref_symbolic* s, double times[2]);
+void ref_sym_node_order(const ref_symbolic* s, int32_t* node_at_position);
+void ref_sym_first_columns(const ref_symbolic* s, int32_t* first_column_of_position /* nodes + 1 */);
+void ref_sym_supernodes(const ref_symbolic* s, int32_t* first_position /* count + 1 */, int32_t* parent);
+void ref_sym_rows(const ref_symbolic* s, int64_t* row_start /* count + 1 */, int32_t* rows);
+
+/* SupernodalFactor::factorise (src/linalg/supernodal/SupernodalFactor.cpp:12-28) on a lower-triangle CSC in the
+ * symbolic factor's order. pivoting: 0 positive definite, 1 indefinite. family: -1 automatic (KernelSelection),
+ * 0 reference, 1 avx2, 2 avx512. max_ratio/bailout: PivotPolicy (bailout < 0 continues past flagged pivots).
+ * seconds[0] = wall time of factorise. */
+ref_factor* ref_factorise(const ref_symbolic* s, int32_t dimension, const int64_t* col_offsets, const int32_t* rows,
+                          const double* values, int pivoting, int family, int threads, double max_ratio, int bailout,
+                          double* seconds);
+void ref_factor_free(ref_factor* f);
+/* info[0..7]: positive, negative, zero, delayed pivots, 2x2 pivots, pivot issue count, equation of largest ratio,
+ * kernel kind */
+void ref_factor_info(const ref_factor* f, int64_t info[8], double* largest_ratio);
+/* The panel of supernode s: eliminated columns, rows; values column-major (rows x eliminated, leading dimension
+ * rows) copied into `values` when not NULL, the row equations into `rows`, the 2x2 subdiagonal into `subdiagonal`
+ * (eliminated values; zeros in positive definite mode). */
+int ref_factor_panel(const ref_factor* f, int32_t s, int64_t* eliminated, int64_t* row_count, double* values,
+                     int32_t* rows, double* subdiagonal);
+/* FactorSolve::solve (src/linalg/supernodal/FactorSolve.cpp:176-190): B <- A^-1 B in place, B column-major. */
+int ref_solve(const ref_factor* f, double* b, int64_t ld, int64_t columns, int threads, double* seconds);
+
+/* SparsePencil + BlockLanczos::solve (src/linalg/eigen/SparsePencil.cpp, BlockLanczos.cpp:87-244): the lowest
+ * mode_count eigenpairs of K x = lambda M x. eigenvalues: mode_count; eigenvectors: dimension x mode_count (may be
+ * NULL). shifts: up to max_shifts records of (shift, sturm count, block steps, restarts, converged, has run);
+ * counts[0..3]: modes found, factorisations, shift records, verified count. seconds[0]: wall time of solve. */
+int ref_modes(const ref_symbolic* s, int32_t dimension, const int64_t* col_offsets, const int32_t* rows,
+              const double* stiffness, const double* mass, int64_t mode_count, int64_t block_size, int family,
+              int threads, double* eigenvalues, double* eigenvectors, double* shifts, int64_t max_shifts,
+              int64_t counts[4], double* seconds);
+
+/* pencilScaleOf (src/linalg/eigen/PencilScaling.cpp:64-80): the power-of-two scales of a stiffness CSC. */
+int ref_pencil_scale(int32_t dimension, const int64_t* col_offsets, const int32_t* rows, const double* values,
+                     double* scale);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,78 @@
+"""Generates the golden fixtures of the tests and the benchmark from the reference itself (oracle/_ref/liboos_ref.so,
+built from the reference's sources by oracle/Makefile). Run in a container that has the reference:
+
+    make -C oracle REF=/path/to/O_o_Solver && python tests/golden/make_golden.py
+
+Writes, for each workload of the benchmark and the tests:
+  orderings/<name>.npz   the reference's final node order (ConstrainedOrdering, then SymbolicFactor::analyse's
+                         postorder) and its supernode partition (first positions, parents): the symbolic stage the
+                         reference computes, reused as it is by the GPU path (the row structures follow from them);
+  solutions/<name>.npz   for small cases: the reference's inertia, pivot diagnostics and solutions of seeded
+                         right-hand sides (the known answers the GPU path is checked against on the GPU box, where the
+                         reference is not built).
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+ORDERINGS = {
+    # name: (kind, size)
+    "plate6": ("plate", 6),
+    "plate20": ("plate", 20),
+    "plate100": ("plate", 100),
+    "plate580": ("plate", 580),
+    "hex4": ("hex", 4),
+    "hex8": ("hex", 8),
+    "hex14": ("hex", 14),
+    "hex30": ("hex", 30),
+    "hex60": ("hex", 60),
+}
+SOLUTIONS = ["plate6", "plate20", "hex4", "hex8"]
+
+
+def model_of(kind, size):
+    from o_o_solver_b200 import workloads
+
+    return workloads.Model(workloads.PlateSpec(size, size) if kind == "plate" else workloads.HexSpec(size))
+
+
+def main():
+    import oracle
+
+    os.makedirs(os.path.join(HERE, "orderings"), exist_ok=True)
+    os.makedirs(os.path.join(HERE, "solutions"), exist_ok=True)
+    threads = os.cpu_count() or 1
+    for name, (kind, size) in ORDERINGS.items():
+        model = model_of(kind, size)
+        sym = oracle.analyse(model.offsets, model.neighbours, model.weights, model.coordinates, threads=threads)
+        np.savez_compressed(os.path.join(HERE, "orderings", name + ".npz"), node_order=sym.node_order,
+                            first_position=sym.first_position, parent=sym.parent, flops=np.array(sym.flops),
+                            dof_count=np.array(sym.dof_count), supernode_count=np.array(sym.supernode_count))
+        print(f"{name}: {sym.dof_count} DOFs, {sym.supernode_count} supernodes, {sym.flops:.3e} flops")
+        if name not in SOLUTIONS:
+            continue
+        csc = model.csc(sym.node_order)
+        factor = oracle.factorise(sym, csc.offsets, csc.rows, csc.values, family=0)
+        rng = np.random.default_rng(20261203)
+        b = np.asfortranarray(rng.standard_normal((sym.dof_count, 3)))
+        x = factor.solve(b)
+        np.savez_compressed(os.path.join(HERE, "solutions", name + ".npz"), b=b, x=x,
+                            inertia=np.array([factor.positive, factor.negative, factor.zero]),
+                            issue_count=np.array(factor.issue_count),
+                            equation_of_largest=np.array(factor.equation_of_largest),
+                            largest_ratio=np.array(factor.largest_ratio),
+                            diagonal=np.array([factor.panel(s)[0].diagonal() for s in range(sym.supernode_count)],
+                                              dtype=object) if False else np.zeros(0))
+
+
+if __name__ == "__main__":
+    main()
