@@ -35,6 +35,14 @@ class FactorInfo(ctypes.Structure):
     ]
 
 
+class RefineOptions(ctypes.Structure):
+    _fields_ = [("tolerance", ctypes.c_double), ("max_steps", ctypes.c_int32)]
+
+
+class RefineInfo(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int32), ("residual", ctypes.c_double), ("device_seconds", ctypes.c_double)]
+
+
 # The exported symbols and their signatures: (name, restype, argtypes).
 SIGNATURES = [
     ("oosgpu_last_error", ctypes.c_char_p, []),
@@ -57,6 +65,10 @@ SIGNATURES = [
     ("oosgpu_solve", ctypes.c_int, [_vp, _f64p, ctypes.c_int64, ctypes.c_int64]),
     ("oosgpu_solve_device", ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int64]),
     ("oosgpu_last_solve_seconds", ctypes.c_double, [_vp]),
+    ("oosgpu_solve_refined", ctypes.c_int, [_vp, _f64p, ctypes.c_int64, _f64p, ctypes.c_int64, ctypes.c_int64,
+                                            ctypes.POINTER(RefineOptions), ctypes.POINTER(RefineInfo)]),
+    ("oosgpu_solve_refined_device", ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.c_int64,
+                                                   ctypes.POINTER(RefineOptions), ctypes.POINTER(RefineInfo)]),
     ("oosgpu_factor_profile", ctypes.c_int, [_vp, ctypes.c_int32]),
     ("oosgpu_factor_kernel_stats", ctypes.c_int, [_vp, ctypes.c_int32, _f64p, _i64p, _f64p, _f64p]),
     ("oosgpu_factor_launch_counts", ctypes.c_int, [_vp, ctypes.c_int64, _i64p]),

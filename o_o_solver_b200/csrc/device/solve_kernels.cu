@@ -325,3 +325,48 @@ __global__ void fromRows(const double* x, int c0, int width, int dimension, doub
 }
 
 } // namespace oosgpu::device
+
+namespace oosgpu::device
+{
+
+// ------------------------------------------------------------------------------------------------------------------
+// Iterative refinement in FP64 (the fixed-precision refinement of LAPACK xPORFS, which the reference applies to free
+// bodies, include/oos/linalg/dense/IterativeRefinement.hpp:39-64): R = B - A X on the rows of a tile, with A given by
+// the full symmetric pattern of its lower CSC (both triangles, each row's columns ascending, `source` the index of
+// each term in the CSC's values), one warp per row, each lane its columns; the squared column norms of R and of B are
+// accumulated for the convergence test.
+// ------------------------------------------------------------------------------------------------------------------
+__global__ void residualRows(const std::int64_t* rowStart, const std::int32_t* columns, const std::int32_t* source,
+                             const double* values, const double* b, const double* x, double* r, int width,
+                             int dimension, double* norms)
+{
+    const int warpsPerBlock = blockDim.x >> 5;
+    const int row = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= dimension)
+        return;
+    const std::int64_t begin = rowStart[row];
+    const std::int64_t end = rowStart[row + 1];
+    for (int c = lane; c < width; c += 32)
+    {
+        double sum = 0.0;
+        for (std::int64_t k = begin; k < end; ++k)
+            sum += values[source[k]] * x[static_cast<std::int64_t>(columns[k]) * width + c];
+        const std::int64_t at = static_cast<std::int64_t>(row) * width + c;
+        const double bc = b[at];
+        const double rc = bc - sum;
+        r[at] = rc;
+        atomicAdd(norms + c, rc * rc);
+        atomicAdd(norms + 64 + c, bc * bc);
+    }
+}
+
+// X += R on a tile's rows.
+__global__ void addRows(double* x, const double* r, std::int64_t count)
+{
+    const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e < count)
+        x[e] += r[e];
+}
+
+} // namespace oosgpu::device

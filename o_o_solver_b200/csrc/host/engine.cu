@@ -13,6 +13,8 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -202,6 +204,10 @@ public:
             referenceDiagonal = m_referenceDiagonal.get();
         }
 
+        m_matrixOffsets = dOffsets;
+        m_matrixRows = dRows;
+        m_matrixValues = dValues;
+        m_matrixTerms = onDevice ? terms : offsets[dimension];
         device::FactorArgs args{m_fronts.get(),   m_children.get(), m_rows.get(),  m_relpos.get(),
                                 dOffsets,         dRows,            dValues,       m_panels.get(),
                                 m_updates.get(),  m_zeroPivot.get()};
@@ -346,11 +352,7 @@ public:
             const std::int64_t items = static_cast<std::int64_t>(n) * width;
             device::toRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(deviceB, deviceLd, static_cast<int>(c0), width,
                                                                         n, m_work.get(), nullptr);
-            device::SolveArgs args{m_fronts.get(), m_children.get(), m_rows.get(), m_relpos.get(),
-                                   m_panels.get(), m_work.get(),     m_updateRows.get(), width};
-            runSweep(args, m_plan.forwardLaunches);
-            device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), n);
-            runSweep(args, m_plan.backwardLaunches);
+            sweeps(m_work.get(), width);
             device::fromRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(m_work.get(), static_cast<int>(c0), width, n,
                                                                           deviceB, deviceLd, nullptr);
             check(cudaGetLastError(), "solve launch");
@@ -365,6 +367,172 @@ public:
         float milliseconds = 0.0f;
         check(cudaEventElapsedTime(&milliseconds, m_start, m_stop), "event time");
         m_lastSolveSeconds = milliseconds / 1000.0;
+    }
+
+    // The three sweeps on a tile of `width` columns stored by rows (n x width) in x.
+    void sweeps(double* x, int width)
+    {
+        const std::int32_t n = m_plan.dimension;
+        const std::int64_t items = static_cast<std::int64_t>(n) * width;
+        device::SolveArgs args{m_fronts.get(), m_children.get(), m_rows.get(), m_relpos.get(),
+                               m_panels.get(), x,                m_updateRows.get(), width};
+        runSweep(args, m_plan.forwardLaunches);
+        device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), n);
+        runSweep(args, m_plan.backwardLaunches);
+    }
+
+    // The full symmetric pattern of the factorised matrix (both triangles, rows ascending), for the residuals: built
+    // once on the host from the matrix's structure, each term pointing at its value in the lower CSC.
+    void ensureFullPattern()
+    {
+        if (m_fullTerms == m_matrixTerms && m_fullStart.get() != nullptr)
+            return;
+        const std::int32_t n = m_plan.dimension;
+        std::vector<std::int64_t> offsets(static_cast<std::size_t>(n) + 1);
+        std::vector<std::int32_t> rows(static_cast<std::size_t>(m_matrixTerms));
+        check(cudaMemcpy(offsets.data(), m_matrixOffsets, offsets.size() * sizeof(std::int64_t), cudaMemcpyDeviceToHost),
+              "download offsets");
+        check(cudaMemcpy(rows.data(), m_matrixRows, rows.size() * sizeof(std::int32_t), cudaMemcpyDeviceToHost),
+              "download rows");
+        if (m_matrixTerms > INT32_MAX)
+            throw Error(STATUS_INVALID_ARGUMENT, "refinement: more than 2^31 matrix terms");
+        std::vector<std::int64_t> start(static_cast<std::size_t>(n) + 1, 0);
+        for (std::int32_t j = 0; j < n; ++j)
+            for (std::int64_t k = offsets[static_cast<std::size_t>(j)]; k < offsets[static_cast<std::size_t>(j) + 1]; ++k)
+            {
+                const std::int32_t i = rows[static_cast<std::size_t>(k)];
+                ++start[static_cast<std::size_t>(i) + 1]; // (i, j) in row i
+                if (i != j)
+                    ++start[static_cast<std::size_t>(j) + 1]; // (j, i) in row j
+            }
+        for (std::int32_t i = 0; i < n; ++i)
+            start[static_cast<std::size_t>(i) + 1] += start[static_cast<std::size_t>(i)];
+        std::vector<std::int32_t> columns(static_cast<std::size_t>(start[static_cast<std::size_t>(n)]));
+        std::vector<std::int32_t> source(columns.size());
+        std::vector<std::int64_t> next(start.begin(), start.end() - 1);
+        // Row i: the terms (i, j), j < i, from the columns j < i in increasing j, then column i's own terms.
+        for (std::int32_t j = 0; j < n; ++j)
+        {
+            for (std::int64_t k = offsets[static_cast<std::size_t>(j)]; k < offsets[static_cast<std::size_t>(j) + 1]; ++k)
+            {
+                const std::int32_t i = rows[static_cast<std::size_t>(k)];
+                if (i == j)
+                    continue;
+                const auto at = static_cast<std::size_t>(next[static_cast<std::size_t>(i)]++);
+                columns[at] = j;
+                source[at] = static_cast<std::int32_t>(k);
+            }
+            for (std::int64_t k = offsets[static_cast<std::size_t>(j)]; k < offsets[static_cast<std::size_t>(j) + 1]; ++k)
+            {
+                const auto at = static_cast<std::size_t>(next[static_cast<std::size_t>(j)]++);
+                columns[at] = rows[static_cast<std::size_t>(k)];
+                source[at] = static_cast<std::int32_t>(k);
+            }
+        }
+        m_fullStart.upload(start, m_stream, "refinement: pattern");
+        m_fullColumns.upload(columns, m_stream, "refinement: pattern");
+        m_fullSource.upload(source, m_stream, "refinement: pattern");
+        check(cudaStreamSynchronize(m_stream), "refinement pattern");
+        m_fullTerms = m_matrixTerms;
+    }
+
+    // X = A^-1 B refined in FP64 until every column's relative residual ||b - A x|| / ||b|| is at most `tolerance`
+    // or maxSteps corrections were made; B and X column-major (host or device).
+    void solveRefined(const double* b, std::int64_t ldb, double* x, std::int64_t ldx, std::int64_t columns,
+                      bool onDevice, double tolerance, int maxSteps, oosgpu_refine_info* info)
+    {
+        check(cudaSetDevice(m_device), "cudaSetDevice");
+        if (!m_factorised)
+            throw Error(STATUS_NOT_FACTORISED, "refinement: no factor (factorise first, or the last one failed)");
+        const std::int32_t n = m_plan.dimension;
+        if (ldb < n || ldx < n || columns < 0 || maxSteps < 0)
+            throw Error(STATUS_INVALID_ARGUMENT, "refinement: leading dimensions below the rows, or negative counts");
+        oosgpu_refine_info result{};
+        if (columns == 0 || n == 0)
+        {
+            if (info != nullptr)
+                *info = result;
+            return;
+        }
+        ensureFullPattern();
+        const std::size_t tile = static_cast<std::size_t>(n) * SOLVE_WIDTH;
+        m_work.allocate(tile, "solve: rows");
+        m_bRows.allocate(tile, "refinement: right-hand side rows");
+        m_rRows.allocate(tile, "refinement: residual rows");
+        m_norms.allocate(128, "refinement: norms");
+        m_updateRows.allocate(static_cast<std::size_t>(std::max<std::int64_t>(m_plan.rowEntries, 1)) * SOLVE_WIDTH,
+                              "solve: update rows");
+        const double* deviceB = b;
+        double* deviceX = x;
+        std::int64_t dLdb = ldb;
+        std::int64_t dLdx = ldx;
+        if (!onDevice)
+        {
+            m_hostB.allocate(static_cast<std::size_t>(n) * static_cast<std::size_t>(columns), "refinement: B");
+            m_hostX.allocate(static_cast<std::size_t>(n) * static_cast<std::size_t>(columns), "refinement: X");
+            check(cudaMemcpy2DAsync(m_hostB.get(), static_cast<std::size_t>(n) * sizeof(double), b,
+                                    static_cast<std::size_t>(ldb) * sizeof(double), static_cast<std::size_t>(n) * sizeof(double),
+                                    static_cast<std::size_t>(columns), cudaMemcpyHostToDevice, m_stream),
+                  "upload right-hand sides");
+            deviceB = m_hostB.get();
+            deviceX = m_hostX.get();
+            dLdb = n;
+            dLdx = n;
+        }
+        check(cudaEventRecord(m_start, m_stream), "event");
+        std::vector<double> norms(128);
+        for (std::int64_t c0 = 0; c0 < columns; c0 += SOLVE_WIDTH)
+        {
+            const int width = static_cast<int>(std::min<std::int64_t>(SOLVE_WIDTH, columns - c0));
+            const std::int64_t items = static_cast<std::int64_t>(n) * width;
+            device::toRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(deviceB, dLdb, static_cast<int>(c0), width, n,
+                                                                        m_bRows.get(), nullptr);
+            check(cudaMemcpyAsync(m_work.get(), m_bRows.get(), static_cast<std::size_t>(items) * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, m_stream),
+                  "copy right-hand sides");
+            sweeps(m_work.get(), width);
+            for (int step = 0;; ++step)
+            {
+                check(cudaMemsetAsync(m_norms.get(), 0, 128 * sizeof(double), m_stream), "memset");
+                constexpr int WARPS = 8;
+                device::residualRows<<<blocksFor(n, WARPS), 32 * WARPS, 0, m_stream>>>(
+                    m_fullStart.get(), m_fullColumns.get(), m_fullSource.get(), m_matrixValues, m_bRows.get(),
+                    m_work.get(), m_rRows.get(), width, n, m_norms.get());
+                check(cudaMemcpyAsync(norms.data(), m_norms.get(), 128 * sizeof(double), cudaMemcpyDeviceToHost,
+                                      m_stream),
+                      "download norms");
+                check(cudaStreamSynchronize(m_stream), "refinement residual");
+                double worst = 0.0;
+                for (int c = 0; c < width; ++c)
+                    worst = std::max(worst, norms[static_cast<std::size_t>(64 + c)] > 0.0
+                                                ? std::sqrt(norms[static_cast<std::size_t>(c)] / norms[static_cast<std::size_t>(64 + c)])
+                                                : std::sqrt(norms[static_cast<std::size_t>(c)]));
+                if (worst <= tolerance || step >= maxSteps)
+                {
+                    result.steps = std::max(result.steps, step);
+                    result.residual = std::max(result.residual, worst);
+                    break;
+                }
+                sweeps(m_rRows.get(), width);
+                device::addRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(m_work.get(), m_rRows.get(), items);
+            }
+            device::fromRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(m_work.get(), static_cast<int>(c0), width, n,
+                                                                          deviceX, dLdx, nullptr);
+            check(cudaGetLastError(), "refinement launch");
+        }
+        check(cudaEventRecord(m_stop, m_stream), "event");
+        if (!onDevice)
+            check(cudaMemcpy2DAsync(x, static_cast<std::size_t>(ldx) * sizeof(double), deviceX,
+                                    static_cast<std::size_t>(n) * sizeof(double), static_cast<std::size_t>(n) * sizeof(double),
+                                    static_cast<std::size_t>(columns), cudaMemcpyDeviceToHost, m_stream),
+                  "download solutions");
+        check(cudaStreamSynchronize(m_stream), "refinement");
+        float milliseconds = 0.0f;
+        check(cudaEventElapsedTime(&milliseconds, m_start, m_stop), "event time");
+        result.device_seconds = milliseconds / 1000.0;
+        m_lastSolveSeconds = result.device_seconds;
+        if (info != nullptr)
+            *info = result;
     }
 
     void panel(std::int32_t s, std::int64_t* eliminated, std::int64_t* rowCount, double* values, std::int32_t* rows,
@@ -566,6 +734,18 @@ private:
     DeviceArray<double> m_work;
     DeviceArray<double> m_updateRows;
     DeviceArray<double> m_hostB;
+    DeviceArray<double> m_hostX;
+    DeviceArray<double> m_bRows;
+    DeviceArray<double> m_rRows;
+    DeviceArray<double> m_norms;
+    DeviceArray<std::int64_t> m_fullStart;
+    DeviceArray<std::int32_t> m_fullColumns;
+    DeviceArray<std::int32_t> m_fullSource;
+    std::int64_t m_fullTerms = -1;
+    const std::int64_t* m_matrixOffsets = nullptr;
+    const std::int32_t* m_matrixRows = nullptr;
+    const double* m_matrixValues = nullptr;
+    std::int64_t m_matrixTerms = 0;
     std::size_t m_smallSmem = 0;
     bool m_factorised = false;
     bool m_profile = false;
@@ -967,5 +1147,32 @@ extern "C" int oosgpu_factor_launch_counts(oosgpu_factor* factor, int64_t column
             requirePointer(factor, "factor");
             counts[0] = factor->factor->factorLaunchCount();
             counts[1] = factor->factor->solveLaunchCount(columns);
+        });
+}
+
+extern "C" int oosgpu_solve_refined(oosgpu_factor* factor, const double* b, int64_t ldb, double* x, int64_t ldx,
+                                    int64_t columns, const oosgpu_refine_options* options, oosgpu_refine_info* info)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            const double tolerance = options != nullptr ? options->tolerance : 1.0e-10;
+            const int steps = options != nullptr ? options->max_steps : 10;
+            factor->factor->solveRefined(b, ldb, x, ldx, columns, false, tolerance, steps, info);
+        });
+}
+
+extern "C" int oosgpu_solve_refined_device(oosgpu_factor* factor, const double* b, int64_t ldb, double* x, int64_t ldx,
+                                           int64_t columns, const oosgpu_refine_options* options,
+                                           oosgpu_refine_info* info)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            const double tolerance = options != nullptr ? options->tolerance : 1.0e-10;
+            const int steps = options != nullptr ? options->max_steps : 10;
+            factor->factor->solveRefined(b, ldb, x, ldx, columns, true, tolerance, steps, info);
         });
 }

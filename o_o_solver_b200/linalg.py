@@ -328,3 +328,46 @@ class FactorSolve:
             _check(lib.oosgpu_solve_device(self.factor._handle, b.data_ptr(), ld, k))
         self.device_seconds = float(lib.oosgpu_last_solve_seconds(self.factor._handle))
         return b
+
+
+def _block_layout(a):
+    """(rows, columns, leading dimension) of a column-major host array or a device tensor with contiguous columns."""
+    if isinstance(a, np.ndarray):
+        if a.ndim == 1:
+            return a.shape[0], 1, a.shape[0]
+        if not a.flags.f_contiguous:
+            raise ValueError("expected a column-major (Fortran-order) block")
+        return a.shape[0], a.shape[1], a.shape[0]
+    if a.dim() == 1:
+        return a.shape[0], 1, a.shape[0]
+    if a.stride(0) != 1:
+        raise ValueError("expected a device block with contiguous columns")
+    return a.shape[0], a.shape[1], (a.stride(1) if a.shape[1] > 1 else a.shape[0])
+
+
+@dataclass
+class RefinementInfo:
+    steps: int
+    residual: float
+    device_seconds: float
+
+
+def solve_refined(factor: SupernodalFactor, b, x, tolerance: float = 1.0e-10, max_steps: int = 10) -> RefinementInfo:
+    """X = A^-1 B refined in FP64 on the device until every column's relative residual is at most `tolerance`
+    (oosgpu_solve_refined): B and X float64, both host (column-major) or both device tensors."""
+    lib = nat.load()
+    n, k, ldb = _block_layout(b)
+    nx, kx, ldx = _block_layout(x)
+    if (n, k) != (nx, kx):
+        raise ValueError("solve_refined: B and X differ in shape")
+    options = nat.RefineOptions(tolerance, max_steps)
+    info = nat.RefineInfo()
+    if isinstance(b, np.ndarray):
+        if b.dtype != np.float64 or x.dtype != np.float64:
+            raise ValueError("solve_refined: expected float64 blocks")
+        _check(lib.oosgpu_solve_refined(factor._handle, nat.ptr(b, nat.f64p), ldb, nat.ptr(x, nat.f64p), ldx, k,
+                                        ctypes.byref(options), ctypes.byref(info)))
+    else:
+        _check(lib.oosgpu_solve_refined_device(factor._handle, b.data_ptr(), ldb, x.data_ptr(), ldx, k,
+                                               ctypes.byref(options), ctypes.byref(info)))
+    return RefinementInfo(int(info.steps), float(info.residual), float(info.device_seconds))
