@@ -124,22 +124,24 @@ int oosgpu_solve(oosgpu_factor* factor, double* b, int64_t ld, int64_t columns);
 int oosgpu_solve_device(oosgpu_factor* factor, double* b, int64_t ld, int64_t columns);
 /* The device time of the last solve (CUDA events), seconds. */
 double oosgpu_last_solve_seconds(oosgpu_factor* factor);
-
 /* FP64 iterative refinement around the solve (the fixed-precision refinement of LAPACK xPORFS that the reference
  * applies to free bodies, include/oos/linalg/dense/IterativeRefinement.hpp:39-64): X = A^-1 B, then while a column's
- * relative residual ||b - A x||_2 / ||b||_2 exceeds `tolerance`, x += A^-1 (b - A x), at most max_steps times. The
- * residuals use the last factorised matrix (a host matrix's device copy, or the caller's device arrays, which must
- * then outlive the factorisation's use). */
+ * normwise backward error ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) exceeds `tolerance`,
+ * x += A^-1 (b - A x), at most max_steps times. (The relative residual ||b - A x||_2 / ||b||_2 is reported, not
+ * tested: on an ill-conditioned stiffness its FP64 floor, about eps ||A|| ||x|| / ||b||, can lie above any useful
+ * tolerance whatever the solve.) The residuals use the last factorised matrix (a host matrix's device copy, or the
+ * caller's device arrays, which must then outlive the factorisation's use). */
 typedef struct
 {
-    double tolerance;  /* default 1e-10 */
+    double tolerance;  /* on the normwise backward error; default 1e-10 */
     int32_t max_steps; /* default 10 */
 } oosgpu_refine_options;
 typedef struct
 {
     int32_t steps;         /* corrections made (the most over the column tiles) */
-    double residual;       /* the largest final relative residual over the columns */
+    double residual;       /* the largest final relative residual ||b - A x||_2 / ||b||_2 over the columns */
     double device_seconds; /* device time of the solve and its refinement */
+    double backward_error; /* the largest final normwise backward error over the columns */
 } oosgpu_refine_info;
 /* B (ldb) and X (ldx) column-major, host memory; B is not modified. */
 int oosgpu_solve_refined(oosgpu_factor* factor, const double* b, int64_t ldb, double* x, int64_t ldx, int64_t columns,

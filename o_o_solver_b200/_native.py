@@ -40,7 +40,8 @@ class RefineOptions(ctypes.Structure):
 
 
 class RefineInfo(ctypes.Structure):
-    _fields_ = [("steps", ctypes.c_int32), ("residual", ctypes.c_double), ("device_seconds", ctypes.c_double)]
+    _fields_ = [("steps", ctypes.c_int32), ("residual", ctypes.c_double), ("device_seconds", ctypes.c_double),
+                ("backward_error", ctypes.c_double)]
 
 
 # The exported symbols and their signatures: (name, restype, argtypes).

@@ -333,9 +333,18 @@ namespace oosgpu::device
 // Iterative refinement in FP64 (the fixed-precision refinement of LAPACK xPORFS, which the reference applies to free
 // bodies, include/oos/linalg/dense/IterativeRefinement.hpp:39-64): R = B - A X on the rows of a tile, with A given by
 // the full symmetric pattern of its lower CSC (both triangles, each row's columns ascending, `source` the index of
-// each term in the CSC's values), one warp per row, each lane its columns; the squared column norms of R and of B are
-// accumulated for the convergence test.
+// each term in the CSC's values), one warp per row, each lane its columns. For the convergence test it accumulates,
+// per column, the squared 2-norms of R and B and the infinity norms of R, B and X, and the infinity norm of A (the
+// largest row sum of |a_ij|): the normwise backward error ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf) (Rigal and
+// Gaches) and the relative residual ||r||_2 / ||b||_2 follow. norms: [0, 64) sum r^2, [64, 128) sum b^2,
+// [128, 192) max |r|, [192, 256) max |b|, [256, 320) max |x|, [320] ||A||_inf.
 // ------------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void atomicMaxNonNegative(double* target, double value)
+{
+    // For non-negative doubles the order of their bit patterns as integers is their order.
+    atomicMax(reinterpret_cast<unsigned long long*>(target), static_cast<unsigned long long>(__double_as_longlong(value)));
+}
+
 __global__ void residualRows(const std::int64_t* rowStart, const std::int32_t* columns, const std::int32_t* source,
                              const double* values, const double* b, const double* x, double* r, int width,
                              int dimension, double* norms)
@@ -347,6 +356,13 @@ __global__ void residualRows(const std::int64_t* rowStart, const std::int32_t* c
         return;
     const std::int64_t begin = rowStart[row];
     const std::int64_t end = rowStart[row + 1];
+    if (lane == 0)
+    {
+        double rowSum = 0.0;
+        for (std::int64_t k = begin; k < end; ++k)
+            rowSum += fabs(values[source[k]]);
+        atomicMaxNonNegative(norms + 320, rowSum);
+    }
     for (int c = lane; c < width; c += 32)
     {
         double sum = 0.0;
@@ -358,6 +374,9 @@ __global__ void residualRows(const std::int64_t* rowStart, const std::int32_t* c
         r[at] = rc;
         atomicAdd(norms + c, rc * rc);
         atomicAdd(norms + 64 + c, bc * bc);
+        atomicMaxNonNegative(norms + 128 + c, fabs(rc));
+        atomicMaxNonNegative(norms + 192 + c, fabs(bc));
+        atomicMaxNonNegative(norms + 256 + c, fabs(x[at]));
     }
 }
 

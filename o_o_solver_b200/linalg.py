@@ -350,10 +350,11 @@ class RefinementInfo:
     steps: int
     residual: float
     device_seconds: float
+    backward_error: float
 
 
 def solve_refined(factor: SupernodalFactor, b, x, tolerance: float = 1.0e-10, max_steps: int = 10) -> RefinementInfo:
-    """X = A^-1 B refined in FP64 on the device until every column's relative residual is at most `tolerance`
+    """X = A^-1 B refined in FP64 on the device until every column's normwise backward error is at most `tolerance`
     (oosgpu_solve_refined): B and X float64, both host (column-major) or both device tensors."""
     lib = nat.load()
     n, k, ldb = _block_layout(b)
@@ -370,4 +371,5 @@ def solve_refined(factor: SupernodalFactor, b, x, tolerance: float = 1.0e-10, ma
     else:
         _check(lib.oosgpu_solve_refined_device(factor._handle, b.data_ptr(), ldb, x.data_ptr(), ldx, k,
                                                ctypes.byref(options), ctypes.byref(info)))
-    return RefinementInfo(int(info.steps), float(info.residual), float(info.device_seconds))
+    return RefinementInfo(int(info.steps), float(info.residual), float(info.device_seconds),
+                          float(info.backward_error))

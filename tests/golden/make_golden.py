@@ -29,6 +29,7 @@ ORDERINGS = {
     "plate6": ("plate", 6),
     "plate20": ("plate", 20),
     "plate100": ("plate", 100),
+    "plate200": ("plate", 200),
     "plate580": ("plate", 580),
     "hex4": ("hex", 4),
     "hex8": ("hex", 8),
@@ -69,9 +70,7 @@ def main():
                             inertia=np.array([factor.positive, factor.negative, factor.zero]),
                             issue_count=np.array(factor.issue_count),
                             equation_of_largest=np.array(factor.equation_of_largest),
-                            largest_ratio=np.array(factor.largest_ratio),
-                            diagonal=np.array([factor.panel(s)[0].diagonal() for s in range(sym.supernode_count)],
-                                              dtype=object) if False else np.zeros(0))
+                            largest_ratio=np.array(factor.largest_ratio))
 
 
 if __name__ == "__main__":

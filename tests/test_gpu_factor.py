@@ -54,9 +54,22 @@ def gpu_symbolic(sym):
 
 
 def residual(csc, x, b):
+    """||b - A x|| / ||b|| per column."""
     from o_o_solver_b200 import workloads
 
-    return relative_columns(b - workloads.lower_csc_multiply(csc, x), b)
+    return relative_columns(workloads.lower_csc_multiply(csc, x), b)
+
+
+def backward_error(csc, x, b):
+    """The normwise backward error ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) per column (Rigal-Gaches)."""
+    from o_o_solver_b200 import workloads
+
+    r = b - workloads.lower_csc_multiply(csc, x)
+    absolute = workloads.SymmetricCsc(csc.offsets, csc.rows, np.abs(csc.values))
+    norm_a = workloads.lower_csc_multiply(absolute, np.ones((csc.dimension, 1)))[:, 0].max()
+    if r.ndim == 1:
+        r, x, b = r[:, None], x[:, None], b[:, None]
+    return np.abs(r).max(axis=0) / (norm_a * np.abs(x).max(axis=0) + np.abs(b).max(axis=0))
 
 
 @pytest.mark.parametrize("name", list(CASES))
@@ -100,6 +113,7 @@ def test_solve_matches_reference(name, columns, lib, oracle_mod, gpu):
     FactorSolve(factor).solve(x)
     assert np.all(np.isfinite(x))
     assert residual(csc, x, b).max() <= 10.0 * residual(csc, x_ref, b).max() + 1e-13
+    assert backward_error(csc, x, b).max() <= 1e-15
     assert relative_columns(x, x_ref).max() <= 100.0 * spread + 1e-12
 
 
@@ -218,3 +232,49 @@ def test_solve_before_factorise_is_refused(lib, oracle_mod, gpu):
     factor = SupernodalFactor(gpu_symbolic(sym))
     with pytest.raises(RuntimeError):
         FactorSolve(factor).solve(np.zeros((sym.dof_count, 1), order="F"))
+
+
+@pytest.mark.parametrize("name", ["plate100", "hex14"])
+def test_refinement_reaches_tolerance(name, lib, oracle_mod, gpu):
+    """FP64 refinement on the device stops on the normwise backward error: the device's own measure agrees with the
+    host's, the refined solution's backward error is at the level of FP64 rounding, and its relative residual is no
+    worse than the reference's solve's (the thin plate's floor is the cancellation in b - A x)."""
+    from o_o_solver_b200 import SupernodalFactor, linalg
+
+    model, sym, csc = build_case(name, oracle_mod)
+    b = np.asfortranarray(np.random.default_rng(5).standard_normal((sym.dof_count, 9)))
+    if model.node_dofs == 6:
+        b[:, :4] = model.loads(sym.node_order, 4)
+    factor = SupernodalFactor.factorise(gpu_symbolic(sym), csc)
+    x = np.zeros_like(b, order="F")
+    # A tolerance below what one solve reaches: the corrections run (at most 3).
+    info = linalg.solve_refined(factor, b, x, tolerance=1.0e-18, max_steps=3)
+    assert info.steps == 3
+    host = backward_error(csc, x, b).max()
+    assert host <= 1.0e-15, (host, info)
+    assert info.backward_error == pytest.approx(host, rel=0.5)
+    ref = oracle_mod.factorise(sym, csc.offsets, csc.rows, csc.values, family=0)
+    assert residual(csc, x, b).max() <= 2.0 * residual(csc, ref.solve(b), b).max() + 1e-14
+    # The usual tolerance is met by the solve alone (no correction).
+    info = linalg.solve_refined(factor, b, x, tolerance=1.0e-12)
+    assert info.steps == 0 and info.backward_error <= 1.0e-12
+    x_ref = ref.solve(b)
+    # The refined solution is at least as close to the reference's as the reference's two kernel families are.
+    spread = relative_columns(oracle_mod.factorise(sym, csc.offsets, csc.rows, csc.values, family=1).solve(b),
+                              x_ref).max()
+    assert relative_columns(x, x_ref).max() <= 100.0 * spread + 1e-12
+
+
+def test_refinement_on_device_arrays(lib, oracle_mod, gpu):
+    torch = gpu
+    from o_o_solver_b200 import SupernodalFactor, linalg
+
+    model, sym, csc = build_case("plate20", oracle_mod)
+    factor = SupernodalFactor.factorise(gpu_symbolic(sym), csc)
+    b = model.loads(sym.node_order, 3)
+    d_b = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    d_x = torch.zeros_like(d_b)
+    info = linalg.solve_refined(factor, d_b.t(), d_x.t(), tolerance=1.0e-12)
+    torch.cuda.synchronize()
+    assert backward_error(csc, d_x.cpu().numpy().T, b).max() <= 1.0e-15, info
+    assert np.array_equal(d_b.cpu().numpy().T, b)  # B untouched
