@@ -124,6 +124,15 @@ int oosgpu_solve(oosgpu_factor* factor, double* b, int64_t ld, int64_t columns);
 int oosgpu_solve_device(oosgpu_factor* factor, double* b, int64_t ld, int64_t columns);
 /* The device time of the last solve (CUDA events), seconds. */
 double oosgpu_last_solve_seconds(oosgpu_factor* factor);
+
+/* oosgpu_solve_device without allocating: no counterpart in the reference (its solves run in host memory). For
+ * callers that cannot call cudaMalloc once running (a fixed device-memory budget handed over at set-up, allocations
+ * forbidden afterwards). Its scratch is a fixed 16 MiB device array in the library (2^21 doubles, held on every GPU
+ * that loads the library until exit); a factor needing more than that for one right-hand side (equations plus update
+ * rows) is refused with OOSGPU_INVALID_ARGUMENT. The first call on a device looks the array's address up (make it
+ * before any stream capture). All calls share the array: calls that overlap on the GPU race. */
+int oosgpu_solve_device_noalloc(oosgpu_factor* factor, double* b, int64_t ld, int64_t columns);
+
 /* FP64 iterative refinement around the solve (the fixed-precision refinement of LAPACK xPORFS that the reference
  * applies to free bodies, include/oos/linalg/dense/IterativeRefinement.hpp:39-64): X = A^-1 B, then while a column's
  * normwise backward error ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) exceeds `tolerance`,

@@ -66,6 +66,7 @@ SIGNATURES = [
     ("oosgpu_solve", ctypes.c_int, [_vp, _f64p, ctypes.c_int64, ctypes.c_int64]),
     ("oosgpu_solve_device", ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int64]),
     ("oosgpu_last_solve_seconds", ctypes.c_double, [_vp]),
+    ("oosgpu_solve_device_noalloc", ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int64]),
     ("oosgpu_solve_refined", ctypes.c_int, [_vp, _f64p, ctypes.c_int64, _f64p, ctypes.c_int64, ctypes.c_int64,
                                             ctypes.POINTER(RefineOptions), ctypes.POINTER(RefineInfo)]),
     ("oosgpu_solve_refined_device", ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.c_int64,

@@ -6,6 +6,7 @@
 // launch of a factorisation or a solve on its own stream; a factorisation reads back only its pivot summary.
 
 #include "../device/kernels.cuh"
+#include "factor_internal.hpp"
 #include "host_api.hpp"
 #include "plan.hpp"
 
@@ -16,6 +17,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -379,6 +381,56 @@ public:
         runSweep(args, m_plan.forwardLaunches);
         device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), n);
         runSweep(args, m_plan.backwardLaunches);
+    }
+
+    // The device this factor lives on.
+    [[nodiscard]] int deviceOrdinal() const noexcept { return m_device; }
+
+    // The solve of solve(b, ld, columns, true) with its scratch (the rows of a column tile and the update rows of the
+    // forward sweep) in the caller's device memory `scratch` of `capacity` values instead of the factor's own
+    // buffers: nothing is allocated. The tile is narrowed to what the scratch holds.
+    void solveInScratch(double* b, std::int64_t ld, std::int64_t columns, double* scratch, std::size_t capacity)
+    {
+        check(cudaSetDevice(m_device), "cudaSetDevice");
+        const std::int32_t n = m_plan.dimension;
+        const std::size_t perColumn = static_cast<std::size_t>(n) + static_cast<std::size_t>(std::max<std::int64_t>(m_plan.rowEntries, 1));
+        if (perColumn > capacity)
+            throw Error(STATUS_INVALID_ARGUMENT,
+                        "solve without allocation: this factor needs " + std::to_string(perColumn) +
+                            " scratch values per right-hand side (equations plus update rows), more than the " +
+                            std::to_string(capacity) + " of the fixed scratch; use oosgpu_solve_device");
+        if (!m_factorised)
+            throw Error(STATUS_NOT_FACTORISED, "FactorSolve: no factor (factorise first, or the last one failed)");
+        if (ld < n || columns < 0)
+            throw Error(STATUS_INVALID_ARGUMENT, "FactorSolve::solve: expected " + std::to_string(n) +
+                                                     " rows (leading dimension >= rows), found leading dimension " +
+                                                     std::to_string(ld));
+        if (columns == 0 || n == 0)
+            return;
+        const int width = static_cast<int>(std::min<std::size_t>(SOLVE_WIDTH, capacity / perColumn));
+        double* work = scratch;
+        double* updateRows = scratch + static_cast<std::size_t>(n) * static_cast<std::size_t>(width);
+        check(cudaEventRecord(m_start, m_stream), "event");
+        for (std::int64_t c0 = 0; c0 < columns; c0 += width)
+        {
+            const int tileWidth = static_cast<int>(std::min<std::int64_t>(width, columns - c0));
+            const std::int64_t items = static_cast<std::int64_t>(n) * tileWidth;
+            device::toRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(b, ld, static_cast<int>(c0), tileWidth, n, work,
+                                                                        nullptr);
+            device::SolveArgs args{m_fronts.get(), m_children.get(), m_rows.get(), m_relpos.get(),
+                                   m_panels.get(), work,             updateRows,   tileWidth};
+            runSweep(args, m_plan.forwardLaunches);
+            device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), n);
+            runSweep(args, m_plan.backwardLaunches);
+            device::fromRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(work, static_cast<int>(c0), tileWidth, n, b, ld,
+                                                                          nullptr);
+            check(cudaGetLastError(), "solve launch");
+        }
+        check(cudaEventRecord(m_stop, m_stream), "event");
+        check(cudaStreamSynchronize(m_stream), "solve");
+        float milliseconds = 0.0f;
+        check(cudaEventElapsedTime(&milliseconds, m_start, m_stop), "event time");
+        m_lastSolveSeconds = milliseconds / 1000.0;
     }
 
     // The full symmetric pattern of the factorised matrix (both triangles, rows ascending), for the residuals: built
@@ -812,6 +864,30 @@ struct oosgpu_model
 
 using oosgpu::guarded;
 
+namespace oosgpu
+{
+
+int runGuarded(const std::function<void()>& body)
+{
+    return guarded(body);
+}
+
+int factorDevice(const oosgpu_factor* factor)
+{
+    if (factor == nullptr)
+        throw Error(STATUS_INVALID_ARGUMENT, "factor is null");
+    return factor->factor->deviceOrdinal();
+}
+
+void solveFactorInScratch(oosgpu_factor* factor, double* b, std::int64_t ld, std::int64_t columns, double* scratch,
+                          std::size_t capacity)
+{
+    if (factor == nullptr)
+        throw Error(STATUS_INVALID_ARGUMENT, "factor is null");
+    factor->factor->solveInScratch(b, ld, columns, scratch, capacity);
+}
+
+} // namespace oosgpu
 
 namespace
 {
