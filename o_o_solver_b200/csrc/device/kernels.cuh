@@ -45,7 +45,7 @@ __global__ void pivotSummary(FactorArgs args, const std::int32_t* supernodeOfCol
                              const double* referenceDiagonal, double maxRatio, unsigned long long* counters,
                              std::int32_t* issues, int issueCapacity, double* blockRatio, std::int32_t* blockEquation);
 __global__ void forwardSmall(SolveArgs a, const std::int32_t* list);
-__global__ void forwardGather(SolveArgs a, const std::int32_t* list);
+__global__ void forwardGather(SolveArgs a, const TileTask* tasks);
 __global__ void forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0);
 __global__ void forwardUpdate(SolveArgs a, const TileTask* tasks, int k0);
 __global__ void diagonalSweep(SolveArgs a, const std::int32_t* supernodeOfColumn, int dimension);

@@ -86,38 +86,114 @@ __global__ void __launch_bounds__(SOLVE_THREADS) forwardSmall(SolveArgs a, const
         xRows[e] = xF[e];
 }
 
-// The children's update rows of a large supernode, into X's rows of its columns (in place) and its update rows.
-__global__ void __launch_bounds__(SOLVE_THREADS) forwardGather(SolveArgs a, const std::int32_t* list)
+// The children's update rows of a large supernode, for the front positions [i0, j0) of a task: into X's rows of its
+// columns (in place) and its own update rows (zeroed first). Each block owns its positions and adds the children in
+// increasing order, so every row's sum is the same whatever the split; a child's rows landing in the range are
+// consecutive (positions increase with the rows), found by bisection.
+__global__ void __launch_bounds__(SOLVE_THREADS) forwardGather(SolveArgs a, const TileTask* tasks)
 {
-    const FrontDesc f = a.fronts[list[blockIdx.x]];
-    gatherChildren(a, f, a.x + static_cast<std::int64_t>(f.first) * a.width, a.width);
-}
-
-// The unit lower triangle of step t of a large supernode: rows [k0, k0 + kb) of x_F, in shared memory.
-__global__ void __launch_bounds__(SOLVE_THREADS) forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
-{
-    __shared__ double xb[SOLVE_BLOCK * SOLVE_BLOCK];
-    const FrontDesc f = a.fronts[list[blockIdx.x]];
+    __shared__ int range[2];
+    const TileTask task = tasks[blockIdx.x];
+    const FrontDesc f = a.fronts[task.front];
     const int w = a.width;
-    const std::int64_t n = f.c + f.r;
-    const int kb = min(SOLVE_BLOCK, f.c - k0);
-    double* xRows = a.x + static_cast<std::int64_t>(f.first + k0) * w;
-    const double* l = a.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
-    for (int e = threadIdx.x; e < kb * w; e += blockDim.x)
-        xb[e] = xRows[e];
+    const int p0 = task.i0;
+    const int p1 = task.j0;
+    double* xF = a.x + static_cast<std::int64_t>(f.first) * w;
+    double* own = a.updates + f.rowStart * w;
+    const int firstOwn = max(p0, f.c);
+    for (int e = threadIdx.x; e < (p1 - firstOwn) * w; e += blockDim.x)
+        own[static_cast<std::int64_t>(firstOwn - f.c) * w + e] = 0.0;
     __syncthreads();
-    for (int q = 0; q < kb; ++q)
+    for (int q = 0; q < f.childCount; ++q)
     {
-        for (int e = threadIdx.x; e < (kb - q - 1) * w; e += blockDim.x)
+        const FrontDesc ch = a.fronts[a.children[f.childStart + q]];
+        const std::int32_t* map = a.relpos + ch.rowStart;
+        if (threadIdx.x == 0)
         {
-            const int i = q + 1 + e / w;
-            const int col = e % w;
-            xb[i * w + col] -= l[i + q * n] * xb[q * w + col];
+            int lo = 0;
+            int hi = ch.r;
+            while (lo < hi)
+            {
+                const int mid = (lo + hi) >> 1;
+                if (map[mid] < p0)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            int end = lo;
+            hi = ch.r;
+            while (end < hi)
+            {
+                const int mid = (end + hi) >> 1;
+                if (map[mid] < p1)
+                    end = mid + 1;
+                else
+                    hi = mid;
+            }
+            range[0] = lo;
+            range[1] = end;
+        }
+        __syncthreads();
+        const int lo = range[0];
+        const double* source = a.updates + ch.rowStart * w;
+        for (int e = threadIdx.x; e < (range[1] - lo) * w; e += blockDim.x)
+        {
+            const int i = lo + e / w;
+            const int col = e - (e / w) * w;
+            const int position = map[i];
+            const double value = source[static_cast<std::int64_t>(i) * w + col];
+            if (position < f.c)
+                xF[static_cast<std::int64_t>(position) * w + col] += value;
+            else
+                own[static_cast<std::int64_t>(position - f.c) * w + col] += value;
         }
         __syncthreads();
     }
-    for (int e = threadIdx.x; e < kb * w; e += blockDim.x)
-        xRows[e] = xb[e];
+}
+
+// The 64 x 64 diagonal block of L at step k0 of a large supernode, staged in shared memory (zero outside the block):
+// l[q * SOLVE_BLOCK + i] = L(k0 + i, k0 + q).
+__device__ __forceinline__ int stageDiagonalBlock(const SolveArgs& a, const FrontDesc& f, int k0, double* l)
+{
+    const std::int64_t n = f.c + f.r;
+    const int kb = min(SOLVE_BLOCK, f.c - k0);
+    const double* panel = a.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
+    for (int e = threadIdx.x; e < SOLVE_BLOCK * SOLVE_BLOCK; e += blockDim.x)
+    {
+        const int q = e / SOLVE_BLOCK;
+        const int i = e - q * SOLVE_BLOCK;
+        l[e] = q < kb && i < kb ? panel[i + static_cast<std::int64_t>(q) * n] : 0.0;
+    }
+    __syncthreads();
+    return kb;
+}
+
+// The unit lower triangle of step t of a large supernode: rows [k0, k0 + kb) of x_F. One thread per right-hand-side
+// column carries its column through the whole triangle in registers (no barrier inside the triangle), reading the
+// block of L from shared memory by broadcast; each value receives its terms in increasing q.
+__global__ void __launch_bounds__(SOLVE_BLOCK) forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
+{
+    __shared__ double l[SOLVE_BLOCK * SOLVE_BLOCK];
+    const FrontDesc f = a.fronts[list[blockIdx.x]];
+    const int w = a.width;
+    const int kb = stageDiagonalBlock(a, f, k0, l);
+    const int col = threadIdx.x;
+    if (col >= w)
+        return;
+    double* xRows = a.x + static_cast<std::int64_t>(f.first + k0) * w + col;
+    double x[SOLVE_BLOCK];
+#pragma unroll
+    for (int i = 0; i < SOLVE_BLOCK; ++i)
+        x[i] = i < kb ? xRows[static_cast<std::int64_t>(i) * w] : 0.0;
+#pragma unroll
+    for (int i = 1; i < SOLVE_BLOCK; ++i)
+#pragma unroll
+        for (int q = 0; q < i; ++q)
+            x[i] -= l[q * SOLVE_BLOCK + i] * x[q];
+#pragma unroll
+    for (int i = 0; i < SOLVE_BLOCK; ++i)
+        if (i < kb)
+            xRows[static_cast<std::int64_t>(i) * w] = x[i];
 }
 
 // Step t's block applied to the rows below it: a tile of 64 rows either in x_F (i0 < c, task.k0 = 0) or in the update
@@ -239,31 +315,30 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardRows(SolveArgs a, const 
     tileProduct<true>(op, smemA, smemB);
 }
 
-// The unit upper triangle L11^T of step t (rows [k0, k0 + kb) of x_F), in shared memory.
-__global__ void __launch_bounds__(SOLVE_THREADS) backwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
+// The unit upper triangle L11^T of step t (rows [k0, k0 + kb) of x_F): as forwardDiagonal, from the last row up.
+__global__ void __launch_bounds__(SOLVE_BLOCK) backwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
 {
-    __shared__ double xb[SOLVE_BLOCK * SOLVE_BLOCK];
+    __shared__ double l[SOLVE_BLOCK * SOLVE_BLOCK];
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
-    const std::int64_t n = f.c + f.r;
-    const int kb = min(SOLVE_BLOCK, f.c - k0);
-    double* xRows = a.x + static_cast<std::int64_t>(f.first + k0) * w;
-    const double* l = a.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
-    for (int e = threadIdx.x; e < kb * w; e += blockDim.x)
-        xb[e] = xRows[e];
-    __syncthreads();
-    for (int i = kb - 1; i > 0; --i)
-    {
-        for (int e = threadIdx.x; e < i * w; e += blockDim.x)
-        {
-            const int q = e / w;
-            const int col = e - q * w;
-            xb[q * w + col] -= l[i + q * n] * xb[i * w + col];
-        }
-        __syncthreads();
-    }
-    for (int e = threadIdx.x; e < kb * w; e += blockDim.x)
-        xRows[e] = xb[e];
+    const int kb = stageDiagonalBlock(a, f, k0, l);
+    const int col = threadIdx.x;
+    if (col >= w)
+        return;
+    double* xRows = a.x + static_cast<std::int64_t>(f.first + k0) * w + col;
+    double x[SOLVE_BLOCK];
+#pragma unroll
+    for (int i = 0; i < SOLVE_BLOCK; ++i)
+        x[i] = i < kb ? xRows[static_cast<std::int64_t>(i) * w] : 0.0;
+#pragma unroll
+    for (int i = SOLVE_BLOCK - 1; i > 0; --i)
+#pragma unroll
+        for (int q = 0; q < i; ++q)
+            x[q] -= l[q * SOLVE_BLOCK + i] * x[i];
+#pragma unroll
+    for (int i = 0; i < SOLVE_BLOCK; ++i)
+        if (i < kb)
+            xRows[static_cast<std::int64_t>(i) * w] = x[i];
 }
 
 // After step t's block is solved, its terms leave the rows above it: x_F[q] -= sum_{i in block} L(i, q) x_F[i] for
@@ -345,39 +420,65 @@ __device__ __forceinline__ void atomicMaxNonNegative(double* target, double valu
     atomicMax(reinterpret_cast<unsigned long long*>(target), static_cast<unsigned long long>(__double_as_longlong(value)));
 }
 
+// Each warp takes rows row0, row0 + (all warps), ...; each lane keeps its columns' norms (at most two columns, width
+// <= 64) in registers and adds them to the accumulators once at the end.
 __global__ void residualRows(const std::int64_t* rowStart, const std::int32_t* columns, const std::int32_t* source,
                              const double* values, const double* b, const double* x, double* r, int width,
                              int dimension, double* norms)
 {
     const int warpsPerBlock = blockDim.x >> 5;
-    const int row = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
-    if (row >= dimension)
-        return;
-    const std::int64_t begin = rowStart[row];
-    const std::int64_t end = rowStart[row + 1];
-    if (lane == 0)
+    const int totalWarps = gridDim.x * warpsPerBlock;
+    double sumR[2] = {0.0, 0.0};
+    double sumB[2] = {0.0, 0.0};
+    double maxR[2] = {0.0, 0.0};
+    double maxB[2] = {0.0, 0.0};
+    double maxX[2] = {0.0, 0.0};
+    double maxRowSum = 0.0;
+    for (int row = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5); row < dimension; row += totalWarps)
     {
+        const std::int64_t begin = rowStart[row];
+        const std::int64_t end = rowStart[row + 1];
         double rowSum = 0.0;
-        for (std::int64_t k = begin; k < end; ++k)
+        for (std::int64_t k = begin + lane; k < end; k += 32)
             rowSum += fabs(values[source[k]]);
-        atomicMaxNonNegative(norms + 320, rowSum);
+        for (int offset = 16; offset > 0; offset >>= 1)
+            rowSum += __shfl_xor_sync(0xffffffffu, rowSum, offset);
+        maxRowSum = fmax(maxRowSum, rowSum);
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+        {
+            const int c = lane + 32 * h;
+            if (c >= width)
+                continue;
+            double sum = 0.0;
+            for (std::int64_t k = begin; k < end; ++k)
+                sum += values[source[k]] * x[static_cast<std::int64_t>(columns[k]) * width + c];
+            const std::int64_t at = static_cast<std::int64_t>(row) * width + c;
+            const double bc = b[at];
+            const double rc = bc - sum;
+            r[at] = rc;
+            sumR[h] += rc * rc;
+            sumB[h] += bc * bc;
+            maxR[h] = fmax(maxR[h], fabs(rc));
+            maxB[h] = fmax(maxB[h], fabs(bc));
+            maxX[h] = fmax(maxX[h], fabs(x[at]));
+        }
     }
-    for (int c = lane; c < width; c += 32)
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
     {
-        double sum = 0.0;
-        for (std::int64_t k = begin; k < end; ++k)
-            sum += values[source[k]] * x[static_cast<std::int64_t>(columns[k]) * width + c];
-        const std::int64_t at = static_cast<std::int64_t>(row) * width + c;
-        const double bc = b[at];
-        const double rc = bc - sum;
-        r[at] = rc;
-        atomicAdd(norms + c, rc * rc);
-        atomicAdd(norms + 64 + c, bc * bc);
-        atomicMaxNonNegative(norms + 128 + c, fabs(rc));
-        atomicMaxNonNegative(norms + 192 + c, fabs(bc));
-        atomicMaxNonNegative(norms + 256 + c, fabs(x[at]));
+        const int c = lane + 32 * h;
+        if (c >= width)
+            continue;
+        atomicAdd(norms + c, sumR[h]);
+        atomicAdd(norms + 64 + c, sumB[h]);
+        atomicMaxNonNegative(norms + 128 + c, maxR[h]);
+        atomicMaxNonNegative(norms + 192 + c, maxB[h]);
+        atomicMaxNonNegative(norms + 256 + c, maxX[h]);
     }
+    if (lane == 0)
+        atomicMaxNonNegative(norms + 320, maxRowSum);
 }
 
 // X += R on a tile's rows.

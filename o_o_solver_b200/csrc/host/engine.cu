@@ -547,7 +547,9 @@ public:
             {
                 check(cudaMemsetAsync(m_norms.get(), 0, 384 * sizeof(double), m_stream), "memset");
                 constexpr int WARPS = 8;
-                device::residualRows<<<blocksFor(n, WARPS), 32 * WARPS, 0, m_stream>>>(
+                // A grid of a few blocks per SM: each warp strides over the rows, its norms flushed once.
+                const unsigned residualBlocks = std::min<unsigned>(blocksFor(n, WARPS), 148u * 8u);
+                device::residualRows<<<residualBlocks, 32 * WARPS, 0, m_stream>>>(
                     m_fullStart.get(), m_fullColumns.get(), m_fullSource.get(), m_matrixValues, m_bRows.get(),
                     m_work.get(), m_rRows.get(), width, n, m_norms.get());
                 check(cudaMemcpyAsync(norms.data(), m_norms.get(), 384 * sizeof(double), cudaMemcpyDeviceToHost,
@@ -739,10 +741,10 @@ private:
                 device::forwardSmall<<<launch.count, 256, smallSmem, m_stream>>>(args, list);
                 break;
             case LaunchKind::ForwardGather:
-                device::forwardGather<<<launch.count, 256, 0, m_stream>>>(args, list);
+                device::forwardGather<<<launch.count, 256, 0, m_stream>>>(args, tiles);
                 break;
             case LaunchKind::ForwardDiagonal:
-                device::forwardDiagonal<<<launch.count, 256, 0, m_stream>>>(args, list, launch.k0);
+                device::forwardDiagonal<<<launch.count, 64, 0, m_stream>>>(args, list, launch.k0);
                 break;
             case LaunchKind::ForwardUpdate:
                 device::forwardUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles, launch.k0);
@@ -754,7 +756,7 @@ private:
                 device::backwardRows<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles);
                 break;
             case LaunchKind::BackwardDiagonal:
-                device::backwardDiagonal<<<launch.count, 256, 0, m_stream>>>(args, list, launch.k0);
+                device::backwardDiagonal<<<launch.count, 64, 0, m_stream>>>(args, list, launch.k0);
                 break;
             case LaunchKind::BackwardUpdate:
                 device::backwardUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles, launch.k0);

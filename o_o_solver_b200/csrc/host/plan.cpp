@@ -383,7 +383,19 @@ Plan buildPlan(const Symbolic& symbolic)
             }
         }
         addList(plan, plan.forwardLaunches, LaunchKind::ForwardSmall, solveSmall, 0, maxSmallColumns);
-        addList(plan, plan.forwardLaunches, LaunchKind::ForwardGather, solveLarge);
+        {
+            // The children's update rows of the large supernodes, by ranges of GATHER_POSITIONS front positions.
+            constexpr std::int32_t GATHER_POSITIONS = 256;
+            std::vector<TileTask> ranges;
+            for (const std::int32_t s : solveLarge)
+            {
+                const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+                const std::int32_t n = f.c + f.r;
+                for (std::int32_t p0 = 0; p0 < n; p0 += GATHER_POSITIONS)
+                    ranges.push_back({s, p0, std::min(n, p0 + GATHER_POSITIONS), 0});
+            }
+            addTiles(plan, plan.forwardLaunches, LaunchKind::ForwardGather, ranges);
+        }
         for (std::int32_t k0 = 0; k0 < maxColumns; k0 += BLOCK)
         {
             std::vector<std::int32_t> diagonal;
