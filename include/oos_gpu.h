@@ -72,12 +72,16 @@ void oosgpu_symbolic_destroy(oosgpu_symbolic* symbolic);
 /* ---- factorisation --------------------------------------------------------------------------------------------- */
 typedef struct oosgpu_factor oosgpu_factor;
 
-/* FactorOptions (SupernodalFactor.hpp:63-97), positive definite mode. */
+/* FactorOptions (SupernodalFactor.hpp:63-97). */
 typedef struct
 {
     double max_ratio;                /* PivotPolicy::maxRatio (PARAM MaxDiagonalRatio), default 1e7 */
     int32_t bailout;                 /* PivotPolicy::bailout (SingularityBailOut): < 0 continues past flagged pivots */
     const double* reference_diagonal; /* FactorOptions::referenceDiagonal (host, dimension values) or NULL */
+    /* FactorOptions::pivoting: 0 PivotingMode::PositiveDefinite, 1 PivotingMode::Indefinite (Bunch-Kaufman 1x1/2x2
+     * pivots within each front; zero pivots counted in the inertia, not refused; the ratio test is not applied; a
+     * pivot that would be delayed to a parent front is refused with OOSGPU_SOLVER) */
+    int32_t pivoting;
 } oosgpu_factor_options;
 
 /* What a factorisation found (SupernodalFactor accessors and PivotDiagnostics). */
@@ -170,6 +174,78 @@ int oosgpu_factor_kernel_stats(oosgpu_factor* factor, int32_t kinds, double* sec
 /* counts[0]: kernels one factorisation launches; counts[1]: kernels one solve of `columns` right-hand sides
  * launches. */
 int oosgpu_factor_launch_counts(oosgpu_factor* factor, int64_t columns, int64_t counts[2]);
+
+/* ---- shifted pencil: the ShiftedPencil plug-in (include/oos/linalg/eigen/ShiftedPencil.hpp:55-88) as SparsePencil
+ *      implements it (include/oos/linalg/eigen/SparsePencil.hpp:29-85) -------------------------------------------- */
+typedef struct oosgpu_pencil oosgpu_pencil;
+
+/* K and M: lower CSC of one structure (the symbolic factor's equation order), host arrays, copied. Refused: another
+ * dimension (OOSGPU_INVALID_ARGUMENT), a negative or infinite mass diagonal term (OOSGPU_SOLVER). */
+int oosgpu_pencil_create(const oosgpu_symbolic* symbolic, int device, int32_t dimension, const int64_t* col_offsets,
+                         const int32_t* rows, const double* stiffness, const double* mass, oosgpu_pencil** out);
+void oosgpu_pencil_destroy(oosgpu_pencil* pencil);
+void* oosgpu_pencil_stream(oosgpu_pencil* pencil);
+/* ShiftedPencil::factorise: S (K - shift M) S factorised in indefinite mode; info->negative is the Sturm count of the
+ * shift, info->zero > 0 a singular shift (returned, not refused). */
+int oosgpu_pencil_factorise(oosgpu_pencil* pencil, double shift, oosgpu_factor_info* info);
+/* ShiftedPencil::solve: X <- (K - shift M)^-1 X with the last factor, X column-major on the device. */
+int oosgpu_pencil_solve_device(oosgpu_pencil* pencil, double* x, int64_t ld, int64_t columns);
+/* ShiftedPencil::multiplyMass: Y <- M X, device blocks (a lumped mass by its diagonal). */
+int oosgpu_pencil_multiply_mass_device(oosgpu_pencil* pencil, const double* x, int64_t ldx, double* y, int64_t ldy,
+                                       int64_t columns);
+/* ShiftedPencil::diagonalRayleighBound (min K_ii / M_ii over K_ii, M_ii > 0), SparsePencil::hasDiagonalMass and
+ * factorisationCount. */
+int oosgpu_pencil_properties(const oosgpu_pencil* pencil, double* rayleigh_bound, int32_t* lumped,
+                             int64_t* factorisations);
+
+/* ---- eigenvalue analysis: BlockLanczos::solve (include/oos/linalg/eigen/BlockLanczos.hpp:102-161,
+ *      src/linalg/eigen/BlockLanczos.cpp:84-246) over the GPU pencil ------------------------------------------------ */
+
+/* EigenRequest (include/oos/linalg/eigen/EigenRequest.hpp:21-35): every root of [lower, upper] (mode_count 0), or the
+ * lowest mode_count roots above lower_bound (and below upper_bound when finite); lower_bound <= 0: from the lowest
+ * root. Infinite bounds are +-INFINITY. */
+typedef struct oosgpu_eigen_request
+{
+    double lower_bound;
+    double upper_bound;
+    int64_t mode_count;
+} oosgpu_eigen_request;
+
+/* LanczosOptions (BlockLanczos.hpp:21-64): the block size, the modes one shift converges, the tolerance of
+ * ||Op y - theta y||_M <= tol |theta|, the shifts and the thick restarts allowed, the seed of the random starts. */
+typedef struct oosgpu_lanczos_options
+{
+    int64_t block_size;
+    int64_t modes_per_shift;
+    double convergence_tolerance;
+    int64_t maximum_shifts;
+    int64_t maximum_restarts;
+    uint64_t seed;
+} oosgpu_lanczos_options;
+
+/* The reference's defaults (block 7, 40 modes per shift, 1e-10, 40 shifts, 20 restarts, its seed). */
+void oosgpu_lanczos_defaults(oosgpu_lanczos_options* options);
+
+typedef struct oosgpu_modes oosgpu_modes;
+
+/* The eigenpairs of `request` (options null: the defaults). Errors as the reference's: OOSGPU_INVALID_ARGUMENT for a
+ * request or settings out of range, OOSGPU_SOLVER for a pencil singular at every shift tried, contradicting Sturm
+ * counts or unbounded negative roots, OOSGPU_MEMORY_BUDGET when the basis does not fit in device memory. */
+int oosgpu_modes_solve(oosgpu_pencil* pencil, const oosgpu_eigen_request* request,
+                       const oosgpu_lanczos_options* options, oosgpu_modes** out);
+/* counts: [0] eigenpairs, [1] factorisations, [2] shifts, [3] verified by the Sturm counts, [4] complete (0/1),
+ * [5] Lanczos block steps; seconds: [0] wall seconds of the solve, [1] device seconds of its factorisations. */
+int oosgpu_modes_summary(const oosgpu_modes* modes, int64_t counts[6], double seconds[2]);
+/* The eigenvalues (increasing) and their residual bounds ||Op y - theta y||_M / |theta|. */
+int oosgpu_modes_values(const oosgpu_modes* modes, double* eigenvalues, double* residual_bounds);
+/* The M-orthonormal eigenvectors, dimension x count, into host memory of leading dimension ld. */
+int oosgpu_modes_vectors(const oosgpu_modes* modes, double* vectors, int64_t ld);
+/* The eigenvectors in device memory (dimension x count, leading dimension dimension), owned by `modes`. */
+const double* oosgpu_modes_vectors_device(const oosgpu_modes* modes);
+/* 7 values per shift (ShiftRecord, BlockLanczos.hpp:68-78): shift, purpose (0 lowest bound, 1 lower bound, 2 upper
+ * bound, 3 advance, 4 fill gap), Sturm count, Lanczos run (0/1), block steps, restarts, converged pairs. */
+int oosgpu_modes_shifts(const oosgpu_modes* modes, double* records);
+void oosgpu_modes_destroy(oosgpu_modes* modes);
 
 /* ---- model-side helpers (no counterpart in the reference's linalg: they stand in for its assembly and DOF
  *      selection, src/assembly and SymmetricCsc::fromBlocks, src/linalg/sparse/SymmetricCsc.cpp:41) ---------------- */

@@ -1,6 +1,6 @@
 """B200 implementation of O_o_Solver's numeric hot path: the supernodal multifrontal LDL^T factorisation and its
 solves on the GPU, behind the reference's factorisation interface (SymbolicFactor, SupernodalFactor.factorise,
-FactorSolve.solve) and a C ABI (include/oos_gpu.h)."""
+FactorSolve.solve), the shifted pencil of its eigenvalue analysis (SparsePencil) and a C ABI (include/oos_gpu.h)."""
 
 from .linalg import (  # noqa: F401
     FactorOptions,
@@ -8,7 +8,10 @@ from .linalg import (  # noqa: F401
     Inertia,
     MemoryBudgetError,
     PivotPolicy,
+    ShiftFactorisation,
     SingularityError,
+    SolverError,
+    SparsePencil,
     SupernodalFactor,
     SymbolicFactor,
     SymmetricCsc,

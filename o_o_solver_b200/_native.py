@@ -15,7 +15,8 @@ _vp = ctypes.c_void_p
 
 
 class FactorOptions(ctypes.Structure):
-    _fields_ = [("max_ratio", ctypes.c_double), ("bailout", ctypes.c_int32), ("reference_diagonal", _f64p)]
+    _fields_ = [("max_ratio", ctypes.c_double), ("bailout", ctypes.c_int32), ("reference_diagonal", _f64p),
+                ("pivoting", ctypes.c_int32)]
 
 
 class FactorInfo(ctypes.Structure):
@@ -42,6 +43,16 @@ class RefineOptions(ctypes.Structure):
 class RefineInfo(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_int32), ("residual", ctypes.c_double), ("device_seconds", ctypes.c_double),
                 ("backward_error", ctypes.c_double)]
+
+
+class EigenRequest(ctypes.Structure):
+    _fields_ = [("lower_bound", ctypes.c_double), ("upper_bound", ctypes.c_double), ("mode_count", ctypes.c_int64)]
+
+
+class LanczosOptions(ctypes.Structure):
+    _fields_ = [("block_size", ctypes.c_int64), ("modes_per_shift", ctypes.c_int64),
+                ("convergence_tolerance", ctypes.c_double), ("maximum_shifts", ctypes.c_int64),
+                ("maximum_restarts", ctypes.c_int64), ("seed", ctypes.c_uint64)]
 
 
 # The exported symbols and their signatures: (name, restype, argtypes).
@@ -74,6 +85,24 @@ SIGNATURES = [
     ("oosgpu_factor_profile", ctypes.c_int, [_vp, ctypes.c_int32]),
     ("oosgpu_factor_kernel_stats", ctypes.c_int, [_vp, ctypes.c_int32, _f64p, _i64p, _f64p, _f64p]),
     ("oosgpu_factor_launch_counts", ctypes.c_int, [_vp, ctypes.c_int64, _i64p]),
+    ("oosgpu_pencil_create", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int32, _i64p, _i32p, _f64p, _f64p,
+                                            ctypes.POINTER(_vp)]),
+    ("oosgpu_pencil_destroy", None, [_vp]),
+    ("oosgpu_pencil_stream", _vp, [_vp]),
+    ("oosgpu_pencil_factorise", ctypes.c_int, [_vp, ctypes.c_double, ctypes.POINTER(FactorInfo)]),
+    ("oosgpu_pencil_solve_device", ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int64]),
+    ("oosgpu_pencil_multiply_mass_device", ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_int64,
+                                                          ctypes.c_int64]),
+    ("oosgpu_pencil_properties", ctypes.c_int, [_vp, _f64p, _i32p, _i64p]),
+    ("oosgpu_lanczos_defaults", None, [ctypes.POINTER(LanczosOptions)]),
+    ("oosgpu_modes_solve", ctypes.c_int, [_vp, ctypes.POINTER(EigenRequest), ctypes.POINTER(LanczosOptions),
+                                          ctypes.POINTER(_vp)]),
+    ("oosgpu_modes_summary", ctypes.c_int, [_vp, _i64p, _f64p]),
+    ("oosgpu_modes_values", ctypes.c_int, [_vp, _f64p, _f64p]),
+    ("oosgpu_modes_vectors", ctypes.c_int, [_vp, _f64p, ctypes.c_int64]),
+    ("oosgpu_modes_vectors_device", _vp, [_vp]),
+    ("oosgpu_modes_shifts", ctypes.c_int, [_vp, _f64p]),
+    ("oosgpu_modes_destroy", None, [_vp]),
     ("oosgpu_model_plate", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                           ctypes.POINTER(_vp)]),

@@ -23,6 +23,20 @@ struct FactorArgs
     std::int32_t* zeroPivot; // per supernode: the first zero (or non-finite) pivot's column in it
 };
 
+// The state of an indefinite factorisation beside its panels.
+struct PivotArgs
+{
+    std::int32_t* perm;        // per pivot position: its natural equation (a permutation within each supernode)
+    double* subdiagonal;       // per pivot position: e_k of a 2x2 block at its first column, 0 elsewhere
+    std::int32_t* status;      // per supernode: bit 1 the block path's threshold test failed, bit 2 a pivot delayed
+    std::int32_t* stepPerm;    // per supernode, 64 values: the interchanges of the current step's diagonal block
+    std::int32_t* stepSwapped; // per supernode: the current step's diagonal block interchanged columns
+    double* w;                 // W = L D of the current step's rows, n x 64 per large front at wOffset
+    const std::int64_t* wOffset;
+    std::int32_t* frontPerm;   // scratch of the exact path (one front at a time)
+    double* frontSub;
+};
+
 struct SolveArgs
 {
     const FrontDesc* fronts;
@@ -61,5 +75,54 @@ __global__ void residualRows(const std::int64_t* rowStart, const std::int32_t* c
                              const double* values, const double* b, const double* x, double* r, int width,
                              int dimension, double* norms);
 __global__ void addRows(double* x, const double* r, std::int64_t count);
+
+__global__ void smallFrontsPivoted(FactorArgs args, PivotArgs pivots, const std::int32_t* list,
+                                   std::int32_t* structureError);
+__global__ void pivotedDiagonal(FactorArgs args, PivotArgs pivots, const std::int32_t* list, int k0);
+__global__ void permuteEarlierRows(FactorArgs args, PivotArgs pivots, const TileTask* tasks, int k0);
+__global__ void panelRowsPivoted(FactorArgs args, PivotArgs pivots, const TileTask* tasks, int k0);
+__global__ void updatePivoted(FactorArgs args, PivotArgs pivots, const TileTask* tasks, int k0);
+__global__ void pivotedFront(FactorArgs args, PivotArgs pivots, std::int32_t s, double* work,
+                             std::int32_t* structureError);
+__global__ void inertiaPivoted(FactorArgs args, PivotArgs pivots, const std::int32_t* supernodeOfColumn, int dimension,
+                               unsigned long long* counters);
+__global__ void identityPermutation(std::int32_t* perm, int dimension);
+__global__ void invertPermutation(const std::int32_t* perm, std::int32_t* inverse, int dimension);
+__global__ void remapPivotOrder(const FrontDesc* fronts, const std::int32_t* rows, const std::int32_t* relpos,
+                                const std::int32_t* inverse, std::int32_t* rowsPivot, std::int32_t* relposPivot,
+                                int supernodes);
+__global__ void toRowsPivoted(const double* b, std::int64_t ld, int c0, int width, int dimension, double* x,
+                              const std::int32_t* perm, const double* scale);
+__global__ void fromRowsPivoted(const double* x, int c0, int width, int dimension, double* b, std::int64_t ld,
+                                const std::int32_t* perm, const double* scale);
+__global__ void diagonalSweepPivoted(SolveArgs a, const std::int32_t* supernodeOfColumn, const double* subdiagonal,
+                                     int dimension);
+
+// The block kernels of the Lanczos run (block_kernels.cu).
+constexpr int GRAM_THREADS = 256;
+constexpr int GRAM_BLOCKS_MAX = 296; // 2 per SM
+constexpr int COMBINE_ROWS = 32;
+constexpr int COMBINE_THREADS = 256;
+
+__global__ void randomBlock(double* x, std::int64_t ld, int rows, int columns, std::uint64_t state);
+__global__ void gramPartials(const double* a, std::int64_t lda, int m, const double* y, std::int64_t ldy, int w,
+                             int rows, int rowsPerBlock, double* partials);
+__global__ void reducePartials(const double* partials, int blocks, int count, double* out);
+__global__ void subtractProduct(double* w, std::int64_t ldw, int width, const double* a, std::int64_t lda, int m,
+                                const double* c, std::int64_t ldc, int rows);
+__global__ void combineRows(const double* a, std::int64_t lda, int m, const double* s, std::int64_t lds, int k,
+                            double* out, std::int64_t ldo, int rows, const double* next, std::int64_t ldn, int b,
+                            const double* correction);
+__global__ void scaleColumn(double* x, double* y, double s, int rows);
+__global__ void scaleColumns(double* x, std::int64_t ldx, double* y, std::int64_t ldy, const double* s, int rows,
+                             int columns);
+
+__global__ void shiftedMatrix(const std::int64_t* offsets, const std::int32_t* rows, const double* stiffness,
+                              const double* mass, double sigma, const double* scale, double* values, int dimension);
+__global__ void diagonalProduct(const double* m, const double* x, std::int64_t ldx, double* y, std::int64_t ldy,
+                                int dimension, int columns);
+__global__ void symmetricProduct(const std::int64_t* rowStart, const std::int32_t* columns, const std::int32_t* source,
+                                 const double* values, const double* x, std::int64_t ldx, double* y, std::int64_t ldy,
+                                 int dimension, int width);
 
 } // namespace oosgpu::device

@@ -1,0 +1,751 @@
+// The indefinite multifrontal LDL^T on the GPU (the reference's PivotingMode::Indefinite: the shifted matrices of the
+// eigenvalue solver), and the pieces of the solves that follow its pivots.
+//
+// - bunchKaufman: the reference's Bunch-Kaufman pivoting restricted to a front's candidate columns
+//   (src/linalg/kernels/reference/DenseBlockKernels.cpp:448-580, LAPACK dsytf2, lower): 1x1 and 2x2 pivots with
+//   alpha = (1 + sqrt 17) / 8, a candidate whose column maximum lies outside the candidates taken as a 1x1 pivot when
+//   |a_kk| >= 0.01 colmax and delayed otherwise, ties of the maxima to the first index. It runs on a whole small front
+//   in shared memory (smallFrontsPivoted), on a large front's diagonal block (pivotedDiagonal), and on a whole front
+//   in global memory (pivotedFront, the exact path of a front the block path refuses).
+// - large fronts, per 64-column block: Bunch-Kaufman inside the diagonal block (its columns are all candidates and its
+//   rows the only ones searched), then the rows below solved against it (L = A L11^-T D^-1, 2x2 blocks by the dsytf2
+//   formula) with an a-posteriori threshold test |l_ij| <= 1/u, u = 0.01 (the reference's delay threshold), and the
+//   trailing front updated by tile products C -= L W^T with W = L D. A front whose test fails is refactorised by the
+//   exact path. The pivots may differ from the reference's, the inertia may not (Sylvester's law): every Sturm count
+//   is the reference's.
+// - the pivot order: every supernode permutes only its own columns (no delayed pivot crosses a front), so the factor
+//   is P A P^T = L D L^T with P a permutation within each supernode's columns; the solves run in pivot order on the
+//   same kernels, with the maps of rows remapped (remapPivotOrder) and 2x2 blocks in the diagonal sweep.
+
+#include "assembly.cuh"
+#include "kernels.cuh"
+
+#include <cstdint>
+
+namespace oosgpu::device
+{
+
+namespace
+{
+
+constexpr double BK_ALPHA = 0.6403882032022076;  // (1 + sqrt(17)) / 8
+constexpr double DELAY_THRESHOLD = 0.01;          // the reference's DELAYED_PIVOT_THRESHOLD
+constexpr double GROWTH_LIMIT = 1.0 / DELAY_THRESHOLD;
+
+// The column maximum |a(i, k)| over i in (k, n) and its first row, on the whole block (ties to the first index).
+// scratchValue / scratchIndex: one slot per warp.
+template <typename At>
+__device__ void columnMax(At at, int k, int n, double* scratchValue, int* scratchIndex, double& best, int& where)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+    double value = 0.0;
+    int index = k;
+    for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x)
+    {
+        const double v = fabs(at(i, k));
+        if (v > value)
+        {
+            value = v;
+            index = i;
+        }
+    }
+    for (int offset = 16; offset > 0; offset >>= 1)
+    {
+        const double v = __shfl_xor_sync(0xffffffffu, value, offset);
+        const int idx = __shfl_xor_sync(0xffffffffu, index, offset);
+        if (v > value || (v == value && idx < index))
+        {
+            value = v;
+            index = idx;
+        }
+    }
+    if (lane == 0)
+    {
+        scratchValue[warp] = value;
+        scratchIndex[warp] = index;
+    }
+    __syncthreads();
+    best = 0.0;
+    where = k;
+    for (int w = 0; w < warps; ++w)
+        if (scratchValue[w] > best || (scratchValue[w] == best && scratchIndex[w] < where && scratchValue[w] > 0.0))
+        {
+            best = scratchValue[w];
+            where = scratchIndex[w];
+        }
+    __syncthreads();
+}
+
+// max |a(imax, j)| over j in [k, imax) and |a(i, imax)| over i in (imax, n).
+template <typename At>
+__device__ double rowMax(At at, int k, int imax, int n, double* scratchValue)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+    double value = 0.0;
+    for (int j = k + threadIdx.x; j < imax; j += blockDim.x)
+        value = fmax(value, fabs(at(imax, j)));
+    for (int i = imax + 1 + threadIdx.x; i < n; i += blockDim.x)
+        value = fmax(value, fabs(at(i, imax)));
+    for (int offset = 16; offset > 0; offset >>= 1)
+        value = fmax(value, __shfl_xor_sync(0xffffffffu, value, offset));
+    if (lane == 0)
+        scratchValue[warp] = value;
+    __syncthreads();
+    double best = 0.0;
+    for (int w = 0; w < warps; ++w)
+        best = fmax(best, scratchValue[w]);
+    __syncthreads();
+    return best;
+}
+
+// The symmetric interchange of rows and columns s < t of the lower-stored block: the rows s and t of the columns
+// before s, the two diagonal terms, the column s and the row t between them, the columns s and t below t.
+template <typename At> __device__ void swapSymmetric(At at, int n, int s, int t)
+{
+    for (int e = threadIdx.x; e < n; e += blockDim.x)
+    {
+        if (e < s)
+        {
+            const double x = at(s, e);
+            at(s, e) = at(t, e);
+            at(t, e) = x;
+        }
+        else if (e == s)
+        {
+            const double x = at(s, s);
+            at(s, s) = at(t, t);
+            at(t, t) = x;
+        }
+        else if (e < t)
+        {
+            const double x = at(e, s);
+            at(e, s) = at(t, e);
+            at(t, e) = x;
+        }
+        else if (e > t)
+        {
+            const double x = at(e, s);
+            at(e, s) = at(e, t);
+            at(e, t) = x;
+        }
+    }
+    __syncthreads();
+}
+
+struct TwoByTwoInverse
+{
+    double d11;
+    double d22;
+    double s;
+};
+
+// The coefficients of the inverse of a 2 x 2 pivot [[a, b], [b, c]] in LAPACK dsytf2's form (no determinant formed):
+// x0 = s (d11 r0 - r1), x1 = s (d22 r1 - r0).
+__device__ __forceinline__ TwoByTwoInverse invertTwoByTwo(double a, double b, double c)
+{
+    const double d11 = c / b;
+    const double d22 = a / b;
+    const double t = 1.0 / (d11 * d22 - 1.0);
+    return {d11, d22, t / b};
+}
+
+// Bunch-Kaufman on the block `at` (n x n lower, the first `candidates` columns the candidates) by the whole thread
+// block. perm: the block positions' origins (permuted with the interchanges); subdiagonal: e_k of each 2x2 pivot at its
+// first column, 0 elsewhere. Returns the columns eliminated (< candidates when some were delayed).
+template <typename At>
+__device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* subdiagonal, double* scratchValue,
+                            int* scratchIndex)
+{
+    for (int i = threadIdx.x; i < candidates; i += blockDim.x)
+    {
+        perm[i] = i;
+        subdiagonal[i] = 0.0;
+    }
+    __syncthreads();
+    int k = 0;
+    int end = candidates;
+    int passStart = 0;
+    while (true)
+    {
+        while (k < end)
+        {
+            const double absakk = fabs(at(k, k));
+            double colmax;
+            int imax;
+            columnMax(at, k, n, scratchValue, scratchIndex, colmax, imax);
+            if (absakk == 0.0 && colmax == 0.0)
+            {
+                k += 1; // a zero column: a zero pivot, L(:, k) = 0
+                continue;
+            }
+            int blockSize = 1;
+            int swapWith = k;
+            if (absakk < BK_ALPHA * colmax && imax >= end)
+            {
+                if (absakk < DELAY_THRESHOLD * colmax)
+                {
+                    --end;
+                    if (k != end)
+                    {
+                        swapSymmetric(at, n, k, end);
+                        if (threadIdx.x == 0)
+                        {
+                            const int x = perm[k];
+                            perm[k] = perm[end];
+                            perm[end] = x;
+                        }
+                        __syncthreads();
+                    }
+                    continue;
+                }
+            }
+            else if (absakk < BK_ALPHA * colmax)
+            {
+                const double rowmax = rowMax(at, k, imax, n, scratchValue);
+                if (absakk >= BK_ALPHA * colmax * (colmax / rowmax))
+                    swapWith = k;
+                else if (fabs(at(imax, imax)) >= BK_ALPHA * rowmax)
+                    swapWith = imax;
+                else
+                {
+                    swapWith = imax;
+                    blockSize = 2;
+                }
+            }
+            const int moved = k + blockSize - 1;
+            if (swapWith != moved)
+            {
+                swapSymmetric(at, n, moved, swapWith);
+                if (threadIdx.x == 0)
+                {
+                    const int x = perm[moved];
+                    perm[moved] = perm[swapWith];
+                    perm[swapWith] = x;
+                }
+                __syncthreads();
+            }
+            if (blockSize == 1)
+            {
+                const double pivot = at(k, k);
+                for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x)
+                    at(i, k) = at(i, k) / pivot;
+                __syncthreads();
+                const int warp = threadIdx.x >> 5;
+                const int warps = blockDim.x >> 5;
+                const int lane = threadIdx.x & 31;
+                for (int j = k + 1 + warp; j < n; j += warps)
+                {
+                    const double w = at(j, k) * pivot;
+                    for (int i = j + lane; i < n; i += 32)
+                        at(i, j) -= at(i, k) * w;
+                }
+                __syncthreads();
+            }
+            else
+            {
+                const double d0 = at(k, k);
+                const double e = at(k + 1, k);
+                const double d1 = at(k + 1, k + 1);
+                const TwoByTwoInverse inverse = invertTwoByTwo(d0, e, d1);
+                __syncthreads();
+                for (int i = k + 2 + threadIdx.x; i < n; i += blockDim.x)
+                {
+                    const double r0 = at(i, k);
+                    const double r1 = at(i, k + 1);
+                    at(i, k) = inverse.s * (inverse.d11 * r0 - r1);
+                    at(i, k + 1) = inverse.s * (inverse.d22 * r1 - r0);
+                }
+                if (threadIdx.x == 0)
+                {
+                    subdiagonal[k] = e;
+                    at(k + 1, k) = 0.0;
+                }
+                __syncthreads();
+                const int warp = threadIdx.x >> 5;
+                const int warps = blockDim.x >> 5;
+                const int lane = threadIdx.x & 31;
+                for (int j = k + 2 + warp; j < n; j += warps)
+                {
+                    const double w0 = at(j, k) * d0 + at(j, k + 1) * e;
+                    const double w1 = at(j, k) * e + at(j, k + 1) * d1;
+                    for (int i = j + lane; i < n; i += 32)
+                    {
+                        double v = at(i, j);
+                        v -= at(i, k) * w0;
+                        v -= at(i, k + 1) * w1;
+                        at(i, j) = v;
+                    }
+                }
+                __syncthreads();
+            }
+            k += blockSize;
+        }
+        if (end == candidates || k == passStart)
+            break;
+        passStart = k;
+        end = candidates;
+    }
+    return k;
+}
+
+struct SharedAt
+{
+    double* a;
+    int ld;
+    __device__ double& operator()(int i, int j) const { return a[i + j * ld]; }
+};
+
+struct GlobalAt
+{
+    double* a;
+    std::int64_t ld;
+    __device__ double& operator()(int i, int j) const { return a[i + static_cast<std::int64_t>(j) * ld]; }
+};
+
+} // namespace
+
+// ------------------------------------------------------------------------------------------------------------------
+// Small fronts, indefinite: assembled in shared memory as smallFronts does, then Bunch-Kaufman on the c candidates;
+// the panel (pivot order), the 2x2 subdiagonals, the permutation of the supernode's columns and the update matrix
+// written out. A front that delays a pivot is flagged (status bit 2).
+// ------------------------------------------------------------------------------------------------------------------
+__global__ void smallFrontsPivoted(FactorArgs args, PivotArgs pivots, const std::int32_t* list,
+                                   std::int32_t* structureError)
+{
+    extern __shared__ double front[];
+    __shared__ double scratchValue[32];
+    __shared__ int scratchIndex[32];
+    __shared__ int perm[128];
+    __shared__ double sub[128];
+    const std::int32_t s = list[blockIdx.x];
+    const FrontDesc f = args.fronts[s];
+    const int n = f.c + f.r;
+    const int ld = n + 1;
+    assembleFrontBy(
+        args, f, [&](int i, int j) -> double& { return front[i + j * ld]; }, structureError);
+    const int eliminated = bunchKaufman(SharedAt{front, ld}, n, f.c, perm, sub, scratchValue, scratchIndex);
+    if (eliminated < f.c && threadIdx.x == 0)
+        atomicOr(pivots.status + s, 2 | (min(eliminated, 0xfffff) << 8));
+    double* panel = args.panels + f.panel;
+    for (int e = threadIdx.x; e < n * f.c; e += blockDim.x)
+    {
+        const int j = e / n;
+        const int i = e - j * n;
+        panel[e] = i >= j ? front[i + j * ld] : 0.0;
+    }
+    for (int j = threadIdx.x; j < f.c; j += blockDim.x)
+    {
+        pivots.perm[f.first + j] = f.first + perm[j];
+        pivots.subdiagonal[f.first + j] = sub[j];
+    }
+    if (f.r > 0)
+    {
+        double* update = args.updates + f.update;
+        for (int e = threadIdx.x; e < f.r * f.r; e += blockDim.x)
+        {
+            const int j = e / f.r;
+            const int i = e - j * f.r;
+            if (i >= j)
+                update[e] = front[(f.c + i) + (f.c + j) * ld];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Large fronts, indefinite, step k0: Bunch-Kaufman inside the kb x kb diagonal block. The block's interchanges are
+// carried to the supernode's permutation and to the rows of L already computed (columns before k0); the rows below
+// the block take them when panelRowsPivoted reads them (pivots.stepPerm).
+// ------------------------------------------------------------------------------------------------------------------
+__global__ void pivotedDiagonal(FactorArgs args, PivotArgs pivots, const std::int32_t* list, int k0)
+{
+    constexpr int B = 64;
+    constexpr int LD = B + 1;
+    __shared__ double a[B * LD];
+    __shared__ double scratchValue[32];
+    __shared__ int scratchIndex[32];
+    __shared__ int perm[B];
+    __shared__ double sub[B];
+    __shared__ std::int32_t oldOrigin[B];
+    const std::int32_t s = list[blockIdx.x];
+    const FrontDesc f = args.fronts[s];
+    const std::int64_t n = f.c + f.r;
+    const int kb = min(B, f.c - k0);
+    double* block = args.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
+    for (int e = threadIdx.x; e < kb * kb; e += blockDim.x)
+    {
+        const int j = e / kb;
+        const int i = e - j * kb;
+        a[i + j * LD] = block[i + static_cast<std::int64_t>(j) * n];
+    }
+    __syncthreads();
+    const int eliminated = bunchKaufman(SharedAt{a, LD}, kb, kb, perm, sub, scratchValue, scratchIndex);
+    if (eliminated < kb && threadIdx.x == 0)
+        atomicOr(pivots.status + s, 2);
+    for (int e = threadIdx.x; e < kb * kb; e += blockDim.x)
+    {
+        const int j = e / kb;
+        const int i = e - j * kb;
+        if (i >= j)
+            block[i + static_cast<std::int64_t>(j) * n] = a[i + j * LD];
+    }
+    for (int j = threadIdx.x; j < kb; j += blockDim.x)
+    {
+        pivots.stepPerm[static_cast<std::int64_t>(s) * B + j] = perm[j];
+        pivots.subdiagonal[f.first + k0 + j] = sub[j];
+        oldOrigin[j] = pivots.perm[f.first + k0 + j];
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < kb; j += blockDim.x)
+        pivots.perm[f.first + k0 + j] = oldOrigin[perm[j]];
+    if (threadIdx.x == 0)
+    {
+        int swapped = 0;
+        for (int j = 0; j < kb; ++j)
+            swapped |= perm[j] != j;
+        pivots.stepSwapped[s] = swapped;
+    }
+}
+
+// The rows of L already computed (columns before k0) follow the diagonal block's interchanges of step k0: a task
+// (front, i0) takes the columns [i0, i0 + 64) of it, a warp per column; nothing to do when the block kept its order.
+__global__ void permuteEarlierRows(FactorArgs args, PivotArgs pivots, const TileTask* tasks, int k0)
+{
+    constexpr int B = 64;
+    __shared__ double staged[8][B];
+    const TileTask task = tasks[blockIdx.x];
+    const std::int32_t s = task.front;
+    if (pivots.stepSwapped[s] == 0)
+        return;
+    const FrontDesc f = args.fronts[s];
+    const std::int64_t n = f.c + f.r;
+    const int kb = min(B, f.c - k0);
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const std::int32_t* perm = pivots.stepPerm + static_cast<std::int64_t>(s) * B;
+    for (int q = task.i0 + warp; q < min(task.i0 + B, k0); q += blockDim.x >> 5)
+    {
+        double* column = args.panels + f.panel + k0 + static_cast<std::int64_t>(q) * n;
+        for (int j = lane; j < kb; j += 32)
+            staged[warp][j] = column[j];
+        __syncwarp();
+        for (int j = lane; j < kb; j += 32)
+            column[j] = staged[warp][perm[j]];
+        __syncwarp();
+    }
+}
+
+__global__ void identityPermutation(std::int32_t* perm, int dimension)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < dimension)
+        perm[j] = j;
+}
+
+// The rows below the diagonal block of step k0, one thread each: the row's entries in the block's columns read in
+// pivot order, Y = A L11^-T (the unit lower block from pivotedDiagonal), L = Y D^-1 (2x2 blocks by the dsytf2 formula),
+// L written to the panel and W = L D = Y to the front's W buffer; a coefficient above 1/u (or not finite) flags the
+// front (status bit 1).
+__global__ void __launch_bounds__(128) panelRowsPivoted(FactorArgs args, PivotArgs pivots, const TileTask* tasks,
+                                                        int k0)
+{
+    constexpr int B = 64;
+    __shared__ double l11[B * B]; // l11[j * B + q] = L(k0 + j, k0 + q), q < j
+    __shared__ double d[B];
+    __shared__ double e[B];
+    __shared__ int perm[B];
+    const TileTask task = tasks[blockIdx.x];
+    const std::int32_t s = task.front;
+    const FrontDesc f = args.fronts[s];
+    const std::int64_t n = f.c + f.r;
+    const int kb = min(B, f.c - k0);
+    const double* block = args.panels + f.panel + k0 + k0 * n;
+    for (int x = threadIdx.x; x < B * B; x += blockDim.x)
+    {
+        const int j = x / B;
+        const int q = x - j * B;
+        l11[x] = j < kb && q < j ? block[j + static_cast<std::int64_t>(q) * n] : 0.0;
+    }
+    for (int j = threadIdx.x; j < B; j += blockDim.x)
+    {
+        d[j] = j < kb ? block[j + static_cast<std::int64_t>(j) * n] : 1.0;
+        e[j] = j < kb ? pivots.subdiagonal[f.first + k0 + j] : 0.0;
+        perm[j] = j < kb ? pivots.stepPerm[static_cast<std::int64_t>(s) * B + j] : j;
+    }
+    __syncthreads();
+    const std::int64_t row = task.i0 + threadIdx.x;
+    if (row >= n)
+        return;
+    double* base = args.panels + f.panel + k0 * n + row;
+    double y[B];
+#pragma unroll
+    for (int j = 0; j < B; ++j)
+        y[j] = j < kb ? base[static_cast<std::int64_t>(perm[j]) * n] : 0.0;
+#pragma unroll
+    for (int j = 1; j < B; ++j)
+    {
+        double v = y[j];
+#pragma unroll
+        for (int q = 0; q < j; ++q)
+            v -= y[q] * l11[j * B + q];
+        y[j] = v;
+    }
+    double* w = pivots.w + pivots.wOffset[s] + row;
+    bool bad = false;
+    int j = 0;
+    while (j < kb)
+    {
+        if (j + 1 < kb && e[j] != 0.0)
+        {
+            const TwoByTwoInverse inverse = invertTwoByTwo(d[j], e[j], d[j + 1]);
+            const double r0 = y[j];
+            const double r1 = y[j + 1];
+            const double l0 = inverse.s * (inverse.d11 * r0 - r1);
+            const double l1 = inverse.s * (inverse.d22 * r1 - r0);
+            base[static_cast<std::int64_t>(j) * n] = l0;
+            base[static_cast<std::int64_t>(j + 1) * n] = l1;
+            w[static_cast<std::int64_t>(j) * n] = r0;
+            w[static_cast<std::int64_t>(j + 1) * n] = r1;
+            bad = bad || !(fabs(l0) <= GROWTH_LIMIT) || !(fabs(l1) <= GROWTH_LIMIT);
+            j += 2;
+        }
+        else
+        {
+            const double l = y[j] / d[j];
+            base[static_cast<std::int64_t>(j) * n] = l;
+            w[static_cast<std::int64_t>(j) * n] = y[j];
+            bad = bad || !(fabs(l) <= GROWTH_LIMIT);
+            j += 1;
+        }
+    }
+    if (bad)
+        atomicOr(pivots.status + s, 1);
+}
+
+// The trailing front of step k0 (columns [k0 + 64, n), the panel's and the update matrix's) minus L W^T over the
+// block's columns: task (front, i0, j0) a 64 x 64 tile of the front, j0 < c in the panel, j0 >= c in the update
+// matrix (tiles never straddle c).
+__global__ void __launch_bounds__(TILE_THREADS) updatePivoted(FactorArgs args, PivotArgs pivots, const TileTask* tasks,
+                                                              int k0)
+{
+    __shared__ double smemA[TILE_K * (TILE + TILE_PAD)];
+    __shared__ double smemB[TILE_K * (TILE + TILE_PAD)];
+    const TileTask task = tasks[blockIdx.x];
+    const FrontDesc f = args.fronts[task.front];
+    const std::int64_t n = f.c + f.r;
+    double* panel = args.panels + f.panel;
+    TileOperands op;
+    op.a = panel + task.i0 + static_cast<std::int64_t>(k0) * n;
+    op.aRowStride = 1;
+    op.aColStride = n;
+    op.b = pivots.w + pivots.wOffset[task.front] + task.j0;
+    op.bRowStride = 1;
+    op.bColStride = n;
+    op.bIndex = nullptr;
+    op.d = nullptr;
+    op.dStride = 0;
+    if (task.j0 < f.c)
+    {
+        op.c = panel + task.i0 + static_cast<std::int64_t>(task.j0) * n;
+        op.cColStride = n;
+        op.n = min(TILE, f.c - task.j0);
+    }
+    else
+    {
+        op.c = args.updates + f.update + (task.i0 - f.c) + static_cast<std::int64_t>(task.j0 - f.c) * f.r;
+        op.cColStride = f.r;
+        op.n = min(TILE, static_cast<int>(n) - task.j0);
+    }
+    op.cRowStride = 1;
+    op.m = static_cast<int>(n - task.i0 < TILE ? n - task.i0 : TILE);
+    op.k = min(64, f.c - k0);
+    op.lower = task.i0 == task.j0;
+    op.lowerOffset = 0;
+    tileProduct(op, smemA, smemB);
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// The exact path of one front (a front the block path refused): assembled whole in `work` (n x n, global memory),
+// Bunch-Kaufman on its candidates by one block, then the panel, the permutation, the subdiagonals and the update
+// matrix written out as smallFrontsPivoted writes them.
+// ------------------------------------------------------------------------------------------------------------------
+__global__ void pivotedFront(FactorArgs args, PivotArgs pivots, std::int32_t s, double* work,
+                             std::int32_t* structureError)
+{
+    __shared__ double scratchValue[32];
+    __shared__ int scratchIndex[32];
+    const FrontDesc f = args.fronts[s];
+    const int n = f.c + f.r;
+    const std::int64_t ld = n;
+    assembleFrontBy(
+        args, f, [&](int i, int j) -> double& { return work[i + static_cast<std::int64_t>(j) * ld]; },
+        structureError);
+    int* perm = pivots.frontPerm;
+    double* sub = pivots.frontSub;
+    const int eliminated = bunchKaufman(GlobalAt{work, ld}, n, f.c, perm, sub, scratchValue, scratchIndex);
+    if (threadIdx.x == 0)
+        pivots.status[s] = eliminated < f.c ? 2 | (min(eliminated, 0xfffff) << 8) : 0;
+    double* panel = args.panels + f.panel;
+    for (std::int64_t x = threadIdx.x; x < static_cast<std::int64_t>(n) * f.c; x += blockDim.x)
+    {
+        const std::int64_t j = x / n;
+        const std::int64_t i = x - j * n;
+        panel[x] = i >= j ? work[i + j * ld] : 0.0;
+    }
+    for (int j = threadIdx.x; j < f.c; j += blockDim.x)
+    {
+        pivots.perm[f.first + j] = f.first + perm[j];
+        pivots.subdiagonal[f.first + j] = sub[j];
+    }
+    if (f.r > 0)
+    {
+        double* update = args.updates + f.update;
+        for (std::int64_t x = threadIdx.x; x < static_cast<std::int64_t>(f.r) * f.r; x += blockDim.x)
+        {
+            const std::int64_t j = x / f.r;
+            const std::int64_t i = x - j * f.r;
+            if (i >= j)
+                update[x] = work[(f.c + i) + (f.c + j) * ld];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Inertia of D with 2x2 blocks (MultifrontalDriver.cpp:763-790): a 2x2 block by the sign of its determinant (negative:
+// one of each; positive: two of the sign of its first term; zero: one zero and one of the sign of its trace), a 1x1
+// pivot by its sign. counters: [positive, negative, zero, 2x2 blocks].
+// ------------------------------------------------------------------------------------------------------------------
+__global__ void inertiaPivoted(FactorArgs args, PivotArgs pivots, const std::int32_t* supernodeOfColumn, int dimension,
+                               unsigned long long* counters)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= dimension)
+        return;
+    const FrontDesc f = args.fronts[supernodeOfColumn[j]];
+    const int k = j - f.first;
+    const std::int64_t n = f.c + f.r;
+    const double* panel = args.panels + f.panel;
+    if (k > 0 && pivots.subdiagonal[j - 1] != 0.0)
+        return; // the second column of a 2x2 block
+    const double pivot = panel[k + k * n];
+    if (k + 1 < f.c && pivots.subdiagonal[j] != 0.0)
+    {
+        const double second = panel[(k + 1) + (k + 1) * n];
+        const double e = pivots.subdiagonal[j];
+        const double determinant = pivot * second - e * e;
+        if (determinant < 0.0)
+        {
+            atomicAdd(counters + 0, 1ull);
+            atomicAdd(counters + 1, 1ull);
+        }
+        else if (determinant > 0.0)
+            atomicAdd(counters + (pivot > 0.0 ? 0 : 1), 2ull);
+        else
+        {
+            atomicAdd(counters + 2, 1ull);
+            const double trace = pivot + second;
+            atomicAdd(counters + (trace > 0.0 ? 0 : trace < 0.0 ? 1 : 2), 1ull);
+        }
+        atomicAdd(counters + 3, 1ull);
+        return;
+    }
+    atomicAdd(counters + (pivot > 0.0 ? 0 : pivot < 0.0 ? 1 : 2), 1ull);
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// The solves in pivot order.
+// ------------------------------------------------------------------------------------------------------------------
+// inverse[perm[j]] = j.
+__global__ void invertPermutation(const std::int32_t* perm, std::int32_t* inverse, int dimension)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < dimension)
+        inverse[perm[j]] = j;
+}
+
+// The maps of rows in pivot order: each row of R(s) as its pivot position, each row's position in the parent's front
+// with the parent's columns in their pivot order. One block per supernode.
+__global__ void remapPivotOrder(const FrontDesc* fronts, const std::int32_t* rows, const std::int32_t* relpos,
+                                const std::int32_t* inverse, std::int32_t* rowsPivot, std::int32_t* relposPivot,
+                                int supernodes)
+{
+    const int s = blockIdx.x;
+    if (s >= supernodes)
+        return;
+    const FrontDesc f = fronts[s];
+    const FrontDesc* parent = f.parent >= 0 ? fronts + f.parent : nullptr;
+    for (int k = threadIdx.x; k < f.r; k += blockDim.x)
+    {
+        const std::int64_t at = f.rowStart + k;
+        rowsPivot[at] = inverse[rows[at]];
+        if (parent != nullptr)
+        {
+            const int position = relpos[at];
+            relposPivot[at] = position < parent->c ? inverse[parent->first + position] - parent->first : position;
+        }
+    }
+}
+
+// Column-major B (ld) -> rows of X in pivot order: X[j] = scale[q] B[q], q = perm[j].
+__global__ void toRowsPivoted(const double* b, std::int64_t ld, int c0, int width, int dimension, double* x,
+                              const std::int32_t* perm, const double* scale)
+{
+    const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= static_cast<std::int64_t>(dimension) * width)
+        return;
+    const int col = static_cast<int>(e / dimension);
+    const int j = static_cast<int>(e - static_cast<std::int64_t>(col) * dimension);
+    const int q = perm[j];
+    const double s = scale != nullptr ? scale[q] : 1.0;
+    x[static_cast<std::int64_t>(j) * width + col] = b[static_cast<std::int64_t>(c0 + col) * ld + q] * s;
+}
+
+// Rows of X in pivot order -> column-major B: B[q] = scale[q] X[j] + 0, q = perm[j].
+__global__ void fromRowsPivoted(const double* x, int c0, int width, int dimension, double* b, std::int64_t ld,
+                                const std::int32_t* perm, const double* scale)
+{
+    const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= static_cast<std::int64_t>(dimension) * width)
+        return;
+    const int col = static_cast<int>(e / dimension);
+    const int j = static_cast<int>(e - static_cast<std::int64_t>(col) * dimension);
+    const int q = perm[j];
+    const double s = scale != nullptr ? scale[q] : 1.0;
+    b[static_cast<std::int64_t>(c0 + col) * ld + q] = x[static_cast<std::int64_t>(j) * width + col] * s + 0.0;
+}
+
+// The diagonal sweep with 1x1 and 2x2 pivots: x <- D^-1 x (a 2x2 block by the dsytf2 formula, as the reference's
+// block-diagonal solve).
+__global__ void diagonalSweepPivoted(SolveArgs a, const std::int32_t* supernodeOfColumn, const double* subdiagonal,
+                                     int dimension)
+{
+    const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int w = a.width;
+    if (e >= static_cast<std::int64_t>(dimension) * w)
+        return;
+    const int j = static_cast<int>(e / w);
+    const int col = static_cast<int>(e - static_cast<std::int64_t>(j) * w);
+    const FrontDesc f = a.fronts[supernodeOfColumn[j]];
+    const int k = j - f.first;
+    const std::int64_t n = f.c + f.r;
+    const double* panel = a.panels + f.panel;
+    if (k > 0 && subdiagonal[j - 1] != 0.0)
+        return; // solved with its block's first column
+    double* x = a.x + static_cast<std::int64_t>(j) * w + col;
+    if (k + 1 < f.c && subdiagonal[j] != 0.0)
+    {
+        const TwoByTwoInverse inverse =
+            invertTwoByTwo(panel[k + k * n], subdiagonal[j], panel[(k + 1) + (k + 1) * n]);
+        const double r0 = x[0];
+        const double r1 = x[w];
+        x[0] = inverse.s * (inverse.d11 * r0 - r1);
+        x[w] = inverse.s * (inverse.d22 * r1 - r0);
+        return;
+    }
+    x[0] = x[0] / panel[k + k * n];
+}
+
+} // namespace oosgpu::device

@@ -8,6 +8,7 @@
 #include "../device/kernels.cuh"
 #include "factor_internal.hpp"
 #include "host_api.hpp"
+#include "lanczos.hpp"
 #include "plan.hpp"
 
 #include "oos_gpu.h"
@@ -219,6 +220,13 @@ public:
               "memset");
         check(cudaMemsetAsync(m_structureError.get(), 0x7f, sizeof(std::int32_t), m_stream), "memset");
         check(cudaMemsetAsync(m_counters.get(), 0, 8 * sizeof(unsigned long long), m_stream), "memset");
+        if (options != nullptr && options->pivoting != 0)
+        {
+            factoriseIndefinite(args, dimension, info);
+            return;
+        }
+        m_pivoted = false;
+        m_singular = false;
         runFactorLaunches(args);
         const unsigned summaryBlocks = blocksFor(std::max(dimension, 1), 256);
         device::pivotSummary<<<summaryBlocks, 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), dimension,
@@ -321,11 +329,179 @@ public:
         m_factorised = true;
     }
 
+    // The indefinite factorisation (the reference's PivotingMode::Indefinite), after the common set-up of factorise():
+    // the pivoted launches level by level; at the end of each level the host reads the fronts' status, refactorises by
+    // the exact path every large front whose threshold test failed, and refuses a pivot delayed to a parent (the GPU
+    // path keeps each front's pivots inside it). Then the inertia with 2x2 blocks and the maps of the pivot order.
+    void factoriseIndefinite(const device::FactorArgs& args, std::int32_t dimension, oosgpu_factor_info* info)
+    {
+        const auto count = static_cast<std::size_t>(m_plan.supernodeCount);
+        const auto n = static_cast<std::size_t>(dimension);
+        m_pivoted = false;
+        m_singular = false;
+        m_factorised = false;
+        m_perm.allocate(n, "indefinite: permutation");
+        m_inversePerm.allocate(n, "indefinite: inverse permutation");
+        m_subdiagonal.allocate(n, "indefinite: 2x2 subdiagonal");
+        m_status.allocate(count, "indefinite: status");
+        m_stepPerm.allocate(count * 64, "indefinite: block interchanges");
+        m_stepSwapped.allocate(count, "indefinite: block interchanged");
+        m_w.allocate(static_cast<std::size_t>(std::max<std::int64_t>(m_plan.wValues, 1)), "indefinite: W");
+        if (m_wOffset.get() == nullptr)
+            m_wOffset.upload(m_plan.wOffset, m_stream, "indefinite: W offsets");
+        m_frontPerm.allocate(static_cast<std::size_t>(std::max(m_plan.largestColumns, 1)), "indefinite: front scratch");
+        m_frontSub.allocate(static_cast<std::size_t>(std::max(m_plan.largestColumns, 1)), "indefinite: front scratch");
+        m_rowsPivot.allocate(static_cast<std::size_t>(std::max<std::int64_t>(m_plan.rowEntries, 1)), "indefinite: rows");
+        m_relposPivot.allocate(static_cast<std::size_t>(std::max<std::int64_t>(m_plan.rowEntries, 1)),
+                               "indefinite: positions");
+        if (!m_pivotedSmemSet && m_smallSmem > 48 * 1024)
+        {
+            check(cudaFuncSetAttribute(device::smallFrontsPivoted, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(m_smallSmem)),
+                  "smallFrontsPivoted shared memory");
+            m_pivotedSmemSet = true;
+        }
+        device::PivotArgs pivots{m_perm.get(),  m_subdiagonal.get(), m_status.get(),    m_stepPerm.get(),
+                                 m_stepSwapped.get(), m_w.get(),    m_wOffset.get(),   m_frontPerm.get(),
+                                 m_frontSub.get()};
+        device::identityPermutation<<<blocksFor(dimension, 256), 256, 0, m_stream>>>(m_perm.get(), dimension);
+        check(cudaMemsetAsync(m_subdiagonal.get(), 0, n * sizeof(double), m_stream), "memset");
+        check(cudaMemsetAsync(m_status.get(), 0, count * sizeof(std::int32_t), m_stream), "memset");
+        check(cudaMemsetAsync(m_stepSwapped.get(), 0, count * sizeof(std::int32_t), m_stream), "memset");
+        std::vector<std::int32_t> status(count);
+        for (const Launch& launch : m_plan.pivotedLaunches)
+        {
+            const std::int32_t* list = m_lists.get() + launch.offset;
+            const device::TileTask* tiles = m_tiles.get() + launch.offset;
+            switch (launch.kind)
+            {
+            case LaunchKind::SmallFrontsPivoted:
+            {
+                const std::size_t smem = static_cast<std::size_t>(launch.smemOrder) * (launch.smemOrder + 1) * sizeof(double);
+                device::smallFrontsPivoted<<<launch.count, SMALL_THREADS, smem, m_stream>>>(args, pivots, list,
+                                                                                            m_structureError.get());
+                break;
+            }
+            case LaunchKind::AssembleFronts:
+                device::assembleFronts<<<launch.count, 256, 0, m_stream>>>(args, m_pieces.get() + launch.offset,
+                                                                           m_structureError.get());
+                break;
+            case LaunchKind::PivotedDiagonal:
+                device::pivotedDiagonal<<<launch.count, 256, 0, m_stream>>>(args, pivots, list, launch.k0);
+                break;
+            case LaunchKind::PermuteEarlierRows:
+                device::permuteEarlierRows<<<launch.count, 256, 0, m_stream>>>(args, pivots, tiles, launch.k0);
+                break;
+            case LaunchKind::PanelRowsPivoted:
+                device::panelRowsPivoted<<<launch.count, 128, 0, m_stream>>>(args, pivots, tiles, launch.k0);
+                break;
+            case LaunchKind::UpdatePivoted:
+                device::updatePivoted<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, pivots, tiles,
+                                                                                          launch.k0);
+                break;
+            case LaunchKind::LevelEnd:
+            {
+                check(cudaGetLastError(), "indefinite factorisation launch");
+                check(cudaMemcpyAsync(status.data(), m_status.get(), count * sizeof(std::int32_t),
+                                      cudaMemcpyDeviceToHost, m_stream),
+                      "download status");
+                check(cudaStreamSynchronize(m_stream), "indefinite factorisation level");
+                for (const std::int32_t s : m_plan.frontsOfLevel[static_cast<std::size_t>(launch.k0)])
+                {
+                    const std::int32_t flags = status[static_cast<std::size_t>(s)];
+                    if ((flags & 2) != 0)
+                        throw delayedPivot(s, flags);
+                    if ((flags & 1) != 0)
+                        exactFront(args, pivots, s);
+                }
+                break;
+            }
+            default:
+                throw Error(STATUS_INTERNAL, "indefinite plan: an unexpected launch");
+            }
+        }
+        check(cudaGetLastError(), "indefinite factorisation launch");
+        device::inertiaPivoted<<<blocksFor(std::max(dimension, 1), 256), 256, 0, m_stream>>>(
+            args, pivots, m_supernodeOfColumn.get(), dimension, m_counters.get());
+        device::invertPermutation<<<blocksFor(std::max(dimension, 1), 256), 256, 0, m_stream>>>(
+            m_perm.get(), m_inversePerm.get(), dimension);
+        device::remapPivotOrder<<<std::max(m_plan.supernodeCount, 1), 128, 0, m_stream>>>(
+            m_fronts.get(), m_rows.get(), m_relpos.get(), m_inversePerm.get(), m_rowsPivot.get(), m_relposPivot.get(),
+            m_plan.supernodeCount);
+        check(cudaGetLastError(), "indefinite summary launch");
+        check(cudaEventRecord(m_stop, m_stream), "event");
+        std::vector<unsigned long long> counters(8);
+        std::int32_t structureError = 0;
+        check(cudaMemcpyAsync(counters.data(), m_counters.get(), 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                              m_stream),
+              "download counters");
+        check(cudaMemcpyAsync(&structureError, m_structureError.get(), sizeof(std::int32_t), cudaMemcpyDeviceToHost,
+                              m_stream),
+              "download structure check");
+        check(cudaStreamSynchronize(m_stream), "indefinite factorisation");
+        float milliseconds = 0.0f;
+        check(cudaEventElapsedTime(&milliseconds, m_start, m_stop), "event time");
+        if (structureError != NO_PIVOT)
+            throw Error(STATUS_INVALID_ARGUMENT,
+                        "supernodal factorisation: column " + std::to_string(structureError) +
+                            " of the matrix has an entry outside the structure of the symbolic factor; build the CSC in "
+                            "the order of the symbolic factor, on the graph it was analysed on");
+        oosgpu_factor_info result{};
+        result.positive = static_cast<std::int64_t>(counters[0]);
+        result.negative = static_cast<std::int64_t>(counters[1]);
+        result.zero = static_cast<std::int64_t>(counters[2]);
+        result.two_by_two = static_cast<std::int64_t>(counters[3]);
+        result.equation_of_largest = -1;
+        result.device_seconds = milliseconds / 1000.0;
+        if (info != nullptr)
+            *info = result;
+        m_pivoted = true;
+        m_singular = result.zero > 0;
+        m_factorised = true;
+    }
+
+    [[nodiscard]] Error delayedPivot(std::int32_t s, std::int32_t flags) const
+    {
+        const device::FrontDesc& f = m_plan.fronts[static_cast<std::size_t>(s)];
+        return Error(STATUS_SOLVER,
+                     "indefinite factorisation: a pivot of supernode " + std::to_string(s) + " (level " +
+                         std::to_string(m_plan.level[static_cast<std::size_t>(s)]) + ", " + std::to_string(f.c) +
+                         " columns, " + std::to_string(f.r) + " rows below, " + std::to_string(f.childCount) +
+                         " children) would be delayed to its parent front after " + std::to_string(flags >> 8) +
+                         " pivots (its column maximum lies outside its candidates and its diagonal is below 0.01 of "
+                         "it); the GPU path keeps every pivot in its own front");
+    }
+
+    // The exact path of front s: assembled whole, Bunch-Kaufman on its candidates by one block.
+    void exactFront(const device::FactorArgs& args, const device::PivotArgs& pivots, std::int32_t s)
+    {
+        const device::FrontDesc& f = m_plan.fronts[static_cast<std::size_t>(s)];
+        const std::size_t order = static_cast<std::size_t>(f.c) + static_cast<std::size_t>(f.r);
+        m_frontWork.allocate(order * order, "indefinite: exact front");
+        device::pivotedFront<<<1, 1024, 0, m_stream>>>(args, pivots, s, m_frontWork.get(), m_structureError.get());
+        check(cudaGetLastError(), "exact front launch");
+        std::int32_t flags = 0;
+        check(cudaMemcpyAsync(&flags, m_status.get() + s, sizeof(std::int32_t), cudaMemcpyDeviceToHost, m_stream),
+              "download status");
+        check(cudaStreamSynchronize(m_stream), "exact front");
+        ++m_exactFronts;
+        if ((flags & 2) != 0)
+            throw delayedPivot(s, flags);
+    }
+
+    void requireSolvable() const
+    {
+        if (!m_factorised)
+            throw Error(STATUS_NOT_FACTORISED, "FactorSolve: no factor (factorise first, or the last one failed)");
+        if (m_singular)
+            throw Error(STATUS_SINGULAR, "FactorSolve: the factor has a zero pivot (the shifted matrix is singular); "
+                                         "move the shift");
+    }
+
     void solve(double* b, std::int64_t ld, std::int64_t columns, bool onDevice)
     {
         check(cudaSetDevice(m_device), "cudaSetDevice");
-        if (!m_factorised)
-            throw Error(STATUS_NOT_FACTORISED, "FactorSolve: no factor (factorise first, or the last one failed)");
+        requireSolvable();
         const std::int32_t n = m_plan.dimension;
         if (ld < n || columns < 0)
             throw Error(STATUS_INVALID_ARGUMENT, "FactorSolve::solve: expected " + std::to_string(n) +
@@ -352,11 +528,10 @@ public:
         {
             const int width = static_cast<int>(std::min<std::int64_t>(SOLVE_WIDTH, columns - c0));
             const std::int64_t items = static_cast<std::int64_t>(n) * width;
-            device::toRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(deviceB, deviceLd, static_cast<int>(c0), width,
-                                                                        n, m_work.get(), nullptr);
+            (void)items;
+            rowsIn(deviceB, deviceLd, static_cast<int>(c0), width, m_work.get());
             sweeps(m_work.get(), width);
-            device::fromRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(m_work.get(), static_cast<int>(c0), width, n,
-                                                                          deviceB, deviceLd, nullptr);
+            rowsOut(m_work.get(), static_cast<int>(c0), width, deviceB, deviceLd);
             check(cudaGetLastError(), "solve launch");
         }
         check(cudaEventRecord(m_stop, m_stream), "event");
@@ -371,15 +546,52 @@ public:
         m_lastSolveSeconds = milliseconds / 1000.0;
     }
 
-    // The three sweeps on a tile of `width` columns stored by rows (n x width) in x.
-    void sweeps(double* x, int width)
+    // A column tile of B (columns [c0, c0 + width), leading dimension ld) into rows of x, in pivot order after an
+    // indefinite factorisation, scaled by the solve's scale when one is set (a pencil's S).
+    void rowsIn(const double* b, std::int64_t ld, int c0, int width, double* x)
     {
         const std::int32_t n = m_plan.dimension;
         const std::int64_t items = static_cast<std::int64_t>(n) * width;
-        device::SolveArgs args{m_fronts.get(), m_children.get(), m_rows.get(), m_relpos.get(),
-                               m_panels.get(), x,                m_updateRows.get(), width};
+        if (m_pivoted)
+            device::toRowsPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(b, ld, c0, width, n, x, m_perm.get(),
+                                                                               m_solveScale);
+        else
+            device::toRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(b, ld, c0, width, n, x, m_solveScale);
+    }
+
+    // The rows of x back into the column tile of B.
+    void rowsOut(const double* x, int c0, int width, double* b, std::int64_t ld)
+    {
+        const std::int32_t n = m_plan.dimension;
+        const std::int64_t items = static_cast<std::int64_t>(n) * width;
+        if (m_pivoted)
+            device::fromRowsPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(x, c0, width, n, b, ld, m_perm.get(),
+                                                                                 m_solveScale);
+        else
+            device::fromRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(x, c0, width, n, b, ld, m_solveScale);
+    }
+
+    // The three sweeps on a tile of `width` columns stored by rows (n x width) in x (in pivot order after an indefinite
+    // factorisation: the maps of rows in pivot order, 2x2 blocks in the diagonal sweep); the update rows of the forward
+    // sweep in `updateRows` (the factor's own when null).
+    void sweeps(double* x, int width, double* updateRows = nullptr)
+    {
+        const std::int32_t n = m_plan.dimension;
+        const std::int64_t items = static_cast<std::int64_t>(n) * width;
+        device::SolveArgs args{m_fronts.get(),
+                               m_children.get(),
+                               m_pivoted ? m_rowsPivot.get() : m_rows.get(),
+                               m_pivoted ? m_relposPivot.get() : m_relpos.get(),
+                               m_panels.get(),
+                               x,
+                               updateRows != nullptr ? updateRows : m_updateRows.get(),
+                               width};
         runSweep(args, m_plan.forwardLaunches);
-        device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), n);
+        if (m_pivoted)
+            device::diagonalSweepPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(),
+                                                                                      m_subdiagonal.get(), n);
+        else
+            device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), n);
         runSweep(args, m_plan.backwardLaunches);
     }
 
@@ -399,8 +611,7 @@ public:
                         "solve without allocation: this factor needs " + std::to_string(perColumn) +
                             " scratch values per right-hand side (equations plus update rows), more than the " +
                             std::to_string(capacity) + " of the fixed scratch; use oosgpu_solve_device");
-        if (!m_factorised)
-            throw Error(STATUS_NOT_FACTORISED, "FactorSolve: no factor (factorise first, or the last one failed)");
+        requireSolvable();
         if (ld < n || columns < 0)
             throw Error(STATUS_INVALID_ARGUMENT, "FactorSolve::solve: expected " + std::to_string(n) +
                                                      " rows (leading dimension >= rows), found leading dimension " +
@@ -415,15 +626,10 @@ public:
         {
             const int tileWidth = static_cast<int>(std::min<std::int64_t>(width, columns - c0));
             const std::int64_t items = static_cast<std::int64_t>(n) * tileWidth;
-            device::toRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(b, ld, static_cast<int>(c0), tileWidth, n, work,
-                                                                        nullptr);
-            device::SolveArgs args{m_fronts.get(), m_children.get(), m_rows.get(), m_relpos.get(),
-                                   m_panels.get(), work,             updateRows,   tileWidth};
-            runSweep(args, m_plan.forwardLaunches);
-            device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), n);
-            runSweep(args, m_plan.backwardLaunches);
-            device::fromRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(work, static_cast<int>(c0), tileWidth, n, b, ld,
-                                                                          nullptr);
+            (void)items;
+            rowsIn(b, ld, static_cast<int>(c0), tileWidth, work);
+            sweeps(work, tileWidth, updateRows);
+            rowsOut(work, static_cast<int>(c0), tileWidth, b, ld);
             check(cudaGetLastError(), "solve launch");
         }
         check(cudaEventRecord(m_stop, m_stream), "event");
@@ -494,8 +700,7 @@ public:
                       bool onDevice, double tolerance, int maxSteps, oosgpu_refine_info* info)
     {
         check(cudaSetDevice(m_device), "cudaSetDevice");
-        if (!m_factorised)
-            throw Error(STATUS_NOT_FACTORISED, "refinement: no factor (factorise first, or the last one failed)");
+        requireSolvable();
         const std::int32_t n = m_plan.dimension;
         if (ldb < n || ldx < n || columns < 0 || maxSteps < 0)
             throw Error(STATUS_INVALID_ARGUMENT, "refinement: leading dimensions below the rows, or negative counts");
@@ -537,8 +742,7 @@ public:
         {
             const int width = static_cast<int>(std::min<std::int64_t>(SOLVE_WIDTH, columns - c0));
             const std::int64_t items = static_cast<std::int64_t>(n) * width;
-            device::toRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(deviceB, dLdb, static_cast<int>(c0), width, n,
-                                                                        m_bRows.get(), nullptr);
+            rowsIn(deviceB, dLdb, static_cast<int>(c0), width, m_bRows.get());
             check(cudaMemcpyAsync(m_work.get(), m_bRows.get(), static_cast<std::size_t>(items) * sizeof(double),
                                   cudaMemcpyDeviceToDevice, m_stream),
                   "copy right-hand sides");
@@ -578,8 +782,7 @@ public:
                 sweeps(m_rRows.get(), width);
                 device::addRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(m_work.get(), m_rRows.get(), items);
             }
-            device::fromRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(m_work.get(), static_cast<int>(c0), width, n,
-                                                                          deviceX, dLdx, nullptr);
+            rowsOut(m_work.get(), static_cast<int>(c0), width, deviceX, dLdx);
             check(cudaGetLastError(), "refinement launch");
         }
         check(cudaEventRecord(m_stop, m_stream), "event");
@@ -628,6 +831,37 @@ public:
     // Profiling: each factorisation launch bracketed by events; after a factorisation, the device time, launches,
     // algorithmic flops and bytes of each launch kind of it.
     void setProfile(bool enable) { m_profile = enable; }
+
+    // The scale every solve applies to its right-hand sides and its solutions (a pencil's S: X <- S A^-1 S B); null
+    // for none. Device memory, dimension values, owned by the caller.
+    void setSolveScale(const double* scale) { m_solveScale = scale; }
+
+    // Y = A X with A of the last factorisation's structure and the given values (its lower CSC's terms), X and Y
+    // column-major device blocks of `width` columns.
+    // The device structure (lower CSC offsets and rows) of the matrices later factorisations and symmetric products
+    // use, before any factorisation (the pencil's products with a coupled mass).
+    void useStructure(const std::int64_t* offsets, const std::int32_t* rows, std::int64_t terms)
+    {
+        m_matrixOffsets = offsets;
+        m_matrixRows = rows;
+        m_matrixTerms = terms;
+    }
+
+    void multiplySymmetric(const double* values, const double* x, std::int64_t ldx, double* y, std::int64_t ldy,
+                           int width)
+    {
+        check(cudaSetDevice(m_device), "cudaSetDevice");
+        if (m_matrixOffsets == nullptr)
+            throw Error(STATUS_NOT_FACTORISED, "symmetric product: no matrix structure yet (factorise first)");
+        ensureFullPattern();
+        const std::int32_t n = m_plan.dimension;
+        constexpr int WARPS = 8;
+        device::symmetricProduct<<<blocksFor(n, WARPS), 32 * WARPS, 0, m_stream>>>(
+            m_fullStart.get(), m_fullColumns.get(), m_fullSource.get(), values, x, ldx, y, ldy, n, width);
+        check(cudaGetLastError(), "symmetric product launch");
+    }
+
+    [[nodiscard]] std::int64_t exactFronts() const noexcept { return m_exactFronts; }
     void kernelStats(int kinds, double* seconds, std::int64_t* launches, double* flops, double* bytes)
     {
         check(cudaSetDevice(m_device), "cudaSetDevice");
@@ -796,6 +1030,25 @@ private:
     DeviceArray<double> m_work;
     DeviceArray<double> m_updateRows;
     DeviceArray<double> m_hostB;
+    // indefinite mode
+    DeviceArray<std::int32_t> m_perm;
+    DeviceArray<std::int32_t> m_inversePerm;
+    DeviceArray<double> m_subdiagonal;
+    DeviceArray<std::int32_t> m_status;
+    DeviceArray<std::int32_t> m_stepPerm;
+    DeviceArray<std::int32_t> m_stepSwapped;
+    DeviceArray<double> m_w;
+    DeviceArray<std::int64_t> m_wOffset;
+    DeviceArray<std::int32_t> m_frontPerm;
+    DeviceArray<double> m_frontSub;
+    DeviceArray<double> m_frontWork;
+    DeviceArray<std::int32_t> m_rowsPivot;
+    DeviceArray<std::int32_t> m_relposPivot;
+    bool m_pivoted = false;
+    bool m_singular = false;
+    bool m_pivotedSmemSet = false;
+    std::int64_t m_exactFronts = 0;
+    const double* m_solveScale = nullptr;
     DeviceArray<double> m_hostX;
     DeviceArray<double> m_bRows;
     DeviceArray<double> m_rRows;
@@ -857,6 +1110,177 @@ struct oosgpu_symbolic
 struct oosgpu_factor
 {
     std::unique_ptr<oosgpu::GpuFactor> factor;
+};
+
+namespace oosgpu
+{
+
+// The shifted pencil (K, M) on the GPU: the reference's SparsePencil (include/oos/linalg/eigen/SparsePencil.hpp:29-85,
+// src/linalg/eigen/SparsePencil.cpp:55-157) behind its ShiftedPencil interface. K and M share one structure (the
+// lower CSC of the symbolic factor's order); factorise(sigma) forms S (K - sigma M) S on the device with the scales of
+// pencilScaleOf (powers of two near 1/sqrt(K_ii), src/linalg/eigen/PencilScaling.cpp:12-31) and factorises it in
+// indefinite mode; solve() gives (K - sigma M)^-1 X = S (S (K - sigma M) S)^-1 S X; multiplyMass() uses the diagonal of
+// a lumped mass (every off-diagonal term zero), the full pattern otherwise.
+class GpuPencil
+{
+public:
+    GpuPencil(const Symbolic& symbolic, int device, std::int32_t dimension, const std::int64_t* offsets,
+              const std::int32_t* rows, const double* stiffness, const double* mass)
+        : m_factor(symbolic, device), m_device(device), m_dimension(dimension)
+    {
+        if (dimension != symbolic.dofCount)
+            throw Error(STATUS_INVALID_ARGUMENT, "SparsePencil: the matrices have " + std::to_string(dimension) +
+                                                     " equations, the symbolic factor " +
+                                                     std::to_string(symbolic.dofCount) +
+                                                     "; analyse the pattern the matrices were converted on");
+        const auto n = static_cast<std::size_t>(dimension);
+        m_terms = offsets[dimension];
+        std::vector<double> scale(n, 1.0);
+        std::vector<double> massDiagonal(n, 0.0);
+        m_rayleighBound = INFINITY;
+        m_lumped = true;
+        for (std::size_t j = 0; j < n; ++j)
+        {
+            const std::int64_t first = offsets[j];
+            const bool hasDiagonal = first < offsets[j + 1] && static_cast<std::size_t>(rows[first]) == j;
+            const double k = hasDiagonal ? stiffness[first] : 0.0;
+            const double m = hasDiagonal ? mass[first] : 0.0;
+            if (!std::isfinite(m) || m < 0.0)
+                throw Error(STATUS_SOLVER, "eigenvalue analysis: the mass matrix has the diagonal term " +
+                                               std::to_string(m) + " at equation " + std::to_string(j) +
+                                               "; the Lanczos method needs a positive semi-definite mass matrix");
+            if (m > 0.0 && k > 0.0)
+                m_rayleighBound = std::min(m_rayleighBound, k / m);
+            massDiagonal[j] = m;
+            // pencilScaleOf: K_ii = f 2^e with f in [0.5, 1): the scale 2^(-(e/2)) leaves a scaled diagonal in [1/4, 2).
+            if (k > 0.0 && std::isfinite(k))
+            {
+                int exponent = 0;
+                std::frexp(k, &exponent);
+                scale[j] = std::ldexp(1.0, -(exponent / 2));
+            }
+            for (std::int64_t t = first; t < offsets[j + 1]; ++t)
+                if (static_cast<std::size_t>(rows[t]) != j && mass[t] != 0.0)
+                    m_lumped = false;
+        }
+        const cudaStream_t stream = m_factor.stream();
+        const auto upload = [&](auto& array, const auto* host, std::size_t count, const char* what)
+        {
+            array.allocate(count, what);
+            check(cudaMemcpyAsync(array.get(), host, count * sizeof(*host), cudaMemcpyHostToDevice, stream), what);
+        };
+        upload(m_offsets, offsets, n + 1, "pencil: offsets");
+        upload(m_rows, rows, static_cast<std::size_t>(m_terms), "pencil: rows");
+        upload(m_stiffness, stiffness, static_cast<std::size_t>(m_terms), "pencil: stiffness");
+        upload(m_mass, mass, static_cast<std::size_t>(m_terms), "pencil: mass");
+        upload(m_massDiagonal, massDiagonal.data(), n, "pencil: mass diagonal");
+        upload(m_scale, scale.data(), n, "pencil: scales");
+        m_shifted.allocate(static_cast<std::size_t>(m_terms), "pencil: shifted matrix");
+        check(cudaStreamSynchronize(stream), "pencil upload");
+        m_factor.setSolveScale(m_scale.get());
+        m_factor.useStructure(m_offsets.get(), m_rows.get(), m_terms);
+    }
+
+    // ShiftedPencil::factorise: the inertia of K - sigma M (a singular factor returned, not refused).
+    oosgpu_factor_info factorise(double shift)
+    {
+        check(cudaSetDevice(m_device), "cudaSetDevice");
+        constexpr int WARPS = 8;
+        device::shiftedMatrix<<<blocksFor(m_dimension, WARPS), 32 * WARPS, 0, m_factor.stream()>>>(
+            m_offsets.get(), m_rows.get(), m_stiffness.get(), m_mass.get(), shift, m_scale.get(), m_shifted.get(),
+            m_dimension);
+        check(cudaGetLastError(), "shifted matrix launch");
+        oosgpu_factor_options options{1.0e7, -1, nullptr, 1};
+        oosgpu_factor_info info{};
+        m_factor.factorise(m_dimension, m_terms, m_offsets.get(), m_rows.get(), m_shifted.get(), true, &options, &info);
+        ++m_factorisations;
+        m_shift = shift;
+        return info;
+    }
+
+    void solve(double* x, std::int64_t ld, std::int64_t columns) { m_factor.solve(x, ld, columns, true); }
+
+    void multiplyMass(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, std::int64_t columns)
+    {
+        check(cudaSetDevice(m_device), "cudaSetDevice");
+        if (ldx < m_dimension || ldy < m_dimension || columns < 0)
+            throw Error(STATUS_INVALID_ARGUMENT, "SparsePencil::multiplyMass: leading dimensions below the rows");
+        if (m_lumped)
+        {
+            const std::int64_t items = static_cast<std::int64_t>(m_dimension) * columns;
+            device::diagonalProduct<<<blocksFor(std::max<std::int64_t>(items, 1), 256), 256, 0, m_factor.stream()>>>(
+                m_massDiagonal.get(), x, ldx, y, ldy, m_dimension, static_cast<int>(columns));
+            check(cudaGetLastError(), "mass product launch");
+            return;
+        }
+        for (std::int64_t c0 = 0; c0 < columns; c0 += 32)
+            m_factor.multiplySymmetric(m_mass.get(), x + c0 * ldx, ldx, y + c0 * ldy, ldy,
+                                       static_cast<int>(std::min<std::int64_t>(32, columns - c0)));
+    }
+
+    [[nodiscard]] cudaStream_t stream() const noexcept { return m_factor.stream(); }
+    [[nodiscard]] double rayleighBound() const noexcept { return m_rayleighBound; }
+    [[nodiscard]] bool lumped() const noexcept { return m_lumped; }
+    [[nodiscard]] std::int64_t factorisations() const noexcept { return m_factorisations; }
+    [[nodiscard]] std::int32_t dimension() const noexcept { return m_dimension; }
+    [[nodiscard]] GpuFactor& factor() noexcept { return m_factor; }
+    [[nodiscard]] const double* massDiagonal() const noexcept { return m_massDiagonal.get(); }
+
+private:
+    GpuFactor m_factor;
+    int m_device = 0;
+    std::int32_t m_dimension = 0;
+    std::int64_t m_terms = 0;
+    double m_rayleighBound = 0.0;
+    bool m_lumped = true;
+    std::int64_t m_factorisations = 0;
+    double m_shift = 0.0;
+    DeviceArray<std::int64_t> m_offsets;
+    DeviceArray<std::int32_t> m_rows;
+    DeviceArray<double> m_stiffness;
+    DeviceArray<double> m_mass;
+    DeviceArray<double> m_massDiagonal;
+    DeviceArray<double> m_scale;
+    DeviceArray<double> m_shifted;
+};
+
+// The GPU pencil behind the Lanczos driver's ShiftedPencil interface.
+class PencilOperations final : public eigen::ShiftedPencil
+{
+public:
+    explicit PencilOperations(GpuPencil& pencil) : m_pencil(pencil) {}
+
+    [[nodiscard]] std::int32_t dimension() const override { return m_pencil.dimension(); }
+    eigen::Inertia factorise(double shift) override
+    {
+        const oosgpu_factor_info info = m_pencil.factorise(shift);
+        m_seconds = info.device_seconds;
+        return {info.positive, info.negative, info.zero};
+    }
+    void solve(double* x, std::int64_t ld, std::int64_t columns) override { m_pencil.solve(x, ld, columns); }
+    void multiplyMass(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, std::int64_t columns) override
+    {
+        m_pencil.multiplyMass(x, ldx, y, ldy, columns);
+    }
+    [[nodiscard]] double diagonalRayleighBound() const override { return m_pencil.rayleighBound(); }
+    [[nodiscard]] cudaStream_t stream() const override { return m_pencil.stream(); }
+    [[nodiscard]] double lastFactorSeconds() const override { return m_seconds; }
+
+private:
+    GpuPencil& m_pencil;
+    double m_seconds = 0.0;
+};
+
+} // namespace oosgpu
+
+struct oosgpu_pencil
+{
+    std::unique_ptr<oosgpu::GpuPencil> pencil;
+};
+
+struct oosgpu_modes
+{
+    oosgpu::eigen::EigenSolution solution;
 };
 
 struct oosgpu_model
@@ -1262,4 +1686,228 @@ extern "C" int oosgpu_solve_refined_device(oosgpu_factor* factor, const double* 
             const int steps = options != nullptr ? options->max_steps : 10;
             factor->factor->solveRefined(b, ldb, x, ldx, columns, true, tolerance, steps, info);
         });
+}
+
+extern "C" int oosgpu_pencil_create(const oosgpu_symbolic* symbolic, int device, int32_t dimension,
+                                    const int64_t* col_offsets, const int32_t* rows, const double* stiffness,
+                                    const double* mass, oosgpu_pencil** out)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(symbolic, "symbolic");
+            requirePointer(col_offsets, "col_offsets");
+            requirePointer(rows, "rows");
+            requirePointer(stiffness, "stiffness");
+            requirePointer(mass, "mass");
+            requirePointer(out, "out");
+            auto handle = std::make_unique<oosgpu_pencil>();
+            handle->pencil = std::make_unique<oosgpu::GpuPencil>(symbolic->symbolic, device, dimension, col_offsets,
+                                                                 rows, stiffness, mass);
+            *out = handle.release();
+        });
+}
+
+extern "C" void oosgpu_pencil_destroy(oosgpu_pencil* pencil)
+{
+    delete pencil;
+}
+
+extern "C" void* oosgpu_pencil_stream(oosgpu_pencil* pencil)
+{
+    return pencil == nullptr ? nullptr : static_cast<void*>(pencil->pencil->stream());
+}
+
+extern "C" int oosgpu_pencil_factorise(oosgpu_pencil* pencil, double shift, oosgpu_factor_info* info)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(pencil, "pencil");
+            const oosgpu_factor_info result = pencil->pencil->factorise(shift);
+            if (info != nullptr)
+                *info = result;
+        });
+}
+
+extern "C" int oosgpu_pencil_solve_device(oosgpu_pencil* pencil, double* x, int64_t ld, int64_t columns)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(pencil, "pencil");
+            pencil->pencil->solve(x, ld, columns);
+        });
+}
+
+extern "C" int oosgpu_pencil_multiply_mass_device(oosgpu_pencil* pencil, const double* x, int64_t ldx, double* y,
+                                                  int64_t ldy, int64_t columns)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(pencil, "pencil");
+            pencil->pencil->multiplyMass(x, ldx, y, ldy, columns);
+            oosgpu::check(cudaStreamSynchronize(pencil->pencil->stream()), "mass product");
+        });
+}
+
+extern "C" int oosgpu_pencil_properties(const oosgpu_pencil* pencil, double* rayleigh_bound, int32_t* lumped,
+                                        int64_t* factorisations)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(pencil, "pencil");
+            if (rayleigh_bound != nullptr)
+                *rayleigh_bound = pencil->pencil->rayleighBound();
+            if (lumped != nullptr)
+                *lumped = pencil->pencil->lumped() ? 1 : 0;
+            if (factorisations != nullptr)
+                *factorisations = pencil->pencil->factorisations();
+        });
+}
+
+extern "C" void oosgpu_lanczos_defaults(oosgpu_lanczos_options* options)
+{
+    if (options == nullptr)
+        return;
+    const oosgpu::eigen::LanczosOptions defaults;
+    options->block_size = static_cast<int64_t>(defaults.blockSize);
+    options->modes_per_shift = static_cast<int64_t>(defaults.modesPerShift);
+    options->convergence_tolerance = defaults.convergenceTolerance;
+    options->maximum_shifts = static_cast<int64_t>(defaults.maximumShifts);
+    options->maximum_restarts = static_cast<int64_t>(defaults.maximumRestarts);
+    options->seed = defaults.seed;
+}
+
+extern "C" int oosgpu_modes_solve(oosgpu_pencil* pencil, const oosgpu_eigen_request* request,
+                                  const oosgpu_lanczos_options* options, oosgpu_modes** out)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(pencil, "pencil");
+            requirePointer(request, "request");
+            requirePointer(out, "out");
+            *out = nullptr;
+            if (request->mode_count < 0)
+                throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT, "eigenvalue request: a negative mode count");
+            oosgpu::eigen::EigenRequest eigenRequest;
+            eigenRequest.lowerBound = request->lower_bound;
+            eigenRequest.upperBound = request->upper_bound;
+            eigenRequest.modeCount = static_cast<std::size_t>(request->mode_count);
+            oosgpu::eigen::LanczosOptions lanczos;
+            if (options != nullptr)
+            {
+                const auto count = [](int64_t value, const char* what)
+                {
+                    if (value < 0)
+                        throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT,
+                                            std::string("BlockLanczos: a negative ") + what);
+                    return static_cast<std::size_t>(value);
+                };
+                lanczos.blockSize = count(options->block_size, "block size");
+                lanczos.modesPerShift = count(options->modes_per_shift, "count of modes per shift");
+                lanczos.convergenceTolerance = options->convergence_tolerance;
+                lanczos.maximumShifts = count(options->maximum_shifts, "shift limit");
+                lanczos.maximumRestarts = count(options->maximum_restarts, "restart limit");
+                lanczos.seed = options->seed;
+            }
+            oosgpu::check(cudaSetDevice(pencil->pencil->factor().deviceOrdinal()), "cudaSetDevice");
+            oosgpu::PencilOperations operations(*pencil->pencil);
+            auto handle = std::make_unique<oosgpu_modes>();
+            handle->solution = oosgpu::eigen::solveModes(operations, eigenRequest, lanczos);
+            *out = handle.release();
+        });
+}
+
+extern "C" int oosgpu_modes_summary(const oosgpu_modes* modes, int64_t counts[6], double seconds[2])
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(modes, "modes");
+            const auto& s = modes->solution;
+            if (counts != nullptr)
+            {
+                counts[0] = static_cast<int64_t>(s.eigenvalues.size());
+                counts[1] = static_cast<int64_t>(s.factorisationCount);
+                counts[2] = static_cast<int64_t>(s.shifts.size());
+                counts[3] = static_cast<int64_t>(s.verifiedCount);
+                counts[4] = s.isComplete ? 1 : 0;
+                counts[5] = static_cast<int64_t>(s.blockSteps);
+            }
+            if (seconds != nullptr)
+            {
+                seconds[0] = s.seconds;
+                seconds[1] = s.factorSeconds;
+            }
+        });
+}
+
+extern "C" int oosgpu_modes_values(const oosgpu_modes* modes, double* eigenvalues, double* residual_bounds)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(modes, "modes");
+            const auto& s = modes->solution;
+            if (eigenvalues != nullptr)
+                std::copy(s.eigenvalues.begin(), s.eigenvalues.end(), eigenvalues);
+            if (residual_bounds != nullptr)
+                std::copy(s.residualBounds.begin(), s.residualBounds.end(), residual_bounds);
+        });
+}
+
+extern "C" int oosgpu_modes_vectors(const oosgpu_modes* modes, double* vectors, int64_t ld)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(modes, "modes");
+            requirePointer(vectors, "vectors");
+            const auto& s = modes->solution;
+            if (ld < s.dimension)
+                throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT, "modes: the leading dimension is below the rows");
+            if (s.eigenvalues.empty() || s.dimension == 0)
+                return;
+            oosgpu::check(cudaMemcpy2D(vectors, static_cast<std::size_t>(ld) * sizeof(double), s.eigenvectors.get(),
+                                       static_cast<std::size_t>(s.dimension) * sizeof(double),
+                                       static_cast<std::size_t>(s.dimension) * sizeof(double), s.eigenvalues.size(),
+                                       cudaMemcpyDeviceToHost),
+                          "download eigenvectors");
+        });
+}
+
+extern "C" const double* oosgpu_modes_vectors_device(const oosgpu_modes* modes)
+{
+    return modes == nullptr ? nullptr : modes->solution.eigenvectors.get();
+}
+
+extern "C" int oosgpu_modes_shifts(const oosgpu_modes* modes, double* records)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(modes, "modes");
+            requirePointer(records, "records");
+            std::size_t k = 0;
+            for (const auto& record : modes->solution.shifts)
+            {
+                double* out = records + 7 * k++;
+                out[0] = record.shift;
+                out[1] = static_cast<double>(static_cast<int>(record.purpose));
+                out[2] = static_cast<double>(record.sturmCount);
+                out[3] = record.hasLanczosRun ? 1.0 : 0.0;
+                out[4] = static_cast<double>(record.blockSteps);
+                out[5] = static_cast<double>(record.restarts);
+                out[6] = static_cast<double>(record.convergedCount);
+            }
+        });
+}
+
+extern "C" void oosgpu_modes_destroy(oosgpu_modes* modes)
+{
+    delete modes;
 }

@@ -247,6 +247,12 @@ Plan buildPlan(const Symbolic& symbolic)
         }
     }
 
+    plan.wOffset.assign(total, 0);
+    for (const FrontDesc& f : plan.fronts)
+    {
+        plan.largestFrontOrder = std::max(plan.largestFrontOrder, f.c + f.r);
+        plan.largestColumns = std::max(plan.largestColumns, f.c);
+    }
     plan.supernodeOfColumn.assign(static_cast<std::size_t>(plan.dimension), 0);
     for (std::int32_t s = 0; s < count; ++s)
         for (std::int32_t j = symbolic.firstColumn[static_cast<std::size_t>(s)];
@@ -362,6 +368,65 @@ Plan buildPlan(const Symbolic& symbolic)
                                       plan.fronts[static_cast<std::size_t>(y.front)].c; });
             addTiles(plan, plan.factorLaunches, LaunchKind::UpdateMatrix, schur);
         }
+
+        // ---- factorisation, indefinite mode ----
+        plan.frontsOfLevel.push_back(members);
+        plan.largeFrontsOfLevel.push_back(large);
+        addList(plan, plan.pivotedLaunches, LaunchKind::SmallFrontsPivoted, small64, 0, order64);
+        addList(plan, plan.pivotedLaunches, LaunchKind::SmallFrontsPivoted, small128, 0, order128);
+        if (!large.empty())
+        {
+            for (auto it = plan.factorLaunches.rbegin(); it != plan.factorLaunches.rend(); ++it)
+                if (it->kind == LaunchKind::AssembleFronts)
+                {
+                    plan.pivotedLaunches.push_back(*it);
+                    break;
+                }
+            std::int64_t w = 0;
+            std::int32_t maxColumns = 0;
+            for (const std::int32_t s : large)
+            {
+                const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+                plan.wOffset[static_cast<std::size_t>(s)] = w;
+                w += static_cast<std::int64_t>(f.c + f.r) * BLOCK;
+                maxColumns = std::max(maxColumns, f.c);
+            }
+            plan.wValues = std::max(plan.wValues, w);
+            for (std::int32_t k0 = 0; k0 < maxColumns; k0 += BLOCK)
+            {
+                std::vector<std::int32_t> diagonal;
+                std::vector<TileTask> earlier;
+                std::vector<TileTask> rowTasks;
+                std::vector<TileTask> trailing;
+                for (const std::int32_t s : large)
+                {
+                    const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+                    if (f.c <= k0)
+                        continue;
+                    const std::int32_t n = f.c + f.r;
+                    const std::int32_t kb = std::min(BLOCK, f.c - k0);
+                    diagonal.push_back(s);
+                    for (std::int32_t q = 0; q < k0; q += BLOCK)
+                        earlier.push_back({s, q, 0, 0});
+                    for (std::int32_t i0 = k0 + kb; i0 < n; i0 += PANEL_ROWS)
+                        rowTasks.push_back({s, i0, 0, 0});
+                    // The trailing front: the panel's columns after the block, then the update matrix's, in tiles of
+                    // 64 that never straddle column c.
+                    for (std::int32_t j0 = k0 + kb; j0 < n;)
+                    {
+                        const std::int32_t width = j0 < f.c ? std::min(device::TILE, f.c - j0) : device::TILE;
+                        for (std::int32_t i0 = j0; i0 < n; i0 += device::TILE)
+                            trailing.push_back({s, i0, j0, 0});
+                        j0 += width;
+                    }
+                }
+                addList(plan, plan.pivotedLaunches, LaunchKind::PivotedDiagonal, diagonal, k0);
+                addTiles(plan, plan.pivotedLaunches, LaunchKind::PermuteEarlierRows, earlier, k0);
+                addTiles(plan, plan.pivotedLaunches, LaunchKind::PanelRowsPivoted, rowTasks, k0);
+                addTiles(plan, plan.pivotedLaunches, LaunchKind::UpdatePivoted, trailing, k0);
+            }
+        }
+        plan.pivotedLaunches.push_back({LaunchKind::LevelEnd, 0, 0, level, 0});
 
         // ---- forward sweep ----
         std::vector<std::int32_t> solveSmall;

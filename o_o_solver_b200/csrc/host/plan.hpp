@@ -37,7 +37,14 @@ enum class LaunchKind : int
     BackwardSmall,
     BackwardRows,
     BackwardDiagonal,
-    BackwardUpdate
+    BackwardUpdate,
+    // indefinite mode
+    SmallFrontsPivoted,
+    PivotedDiagonal,
+    PermuteEarlierRows,
+    PanelRowsPivoted,
+    UpdatePivoted,
+    LevelEnd // the host checks the level's fronts (k0: the level) and runs the exact path where needed
 };
 
 // One batched launch: `count` items from `offset` in the array of its kind (front lists: int32; tiles: TileTask;
@@ -82,6 +89,17 @@ struct Plan
     std::vector<Launch> factorLaunches;
     std::vector<Launch> forwardLaunches;
     std::vector<Launch> backwardLaunches;
+
+    // Indefinite mode: the launches (assembly shared with the positive definite sequence), the large fronts of each
+    // level, and each large front's W buffer (n x 64 values at wOffset; the fronts of one level apart, the levels
+    // sharing the buffer).
+    std::vector<Launch> pivotedLaunches;
+    std::vector<std::vector<std::int32_t>> largeFrontsOfLevel;
+    std::vector<std::vector<std::int32_t>> frontsOfLevel;
+    std::vector<std::int64_t> wOffset;
+    std::int64_t wValues = 0;
+    std::int32_t largestFrontOrder = 0;
+    std::int32_t largestColumns = 0;
 };
 
 // Builds the plan of a validated symbolic structure.

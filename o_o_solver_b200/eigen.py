@@ -1,0 +1,124 @@
+"""The reference's eigenvalue interface over the GPU library (jcdulas/O_o_Solver, include/oos/linalg/eigen): an
+EigenRequest, the LanczosOptions, and BlockLanczos(options).solve(pencil, request) -> EigenSolution, with a
+SparsePencil (o_o_solver_b200.linalg) as the pencil. The Lanczos basis, the blocks and the eigenvectors stay in
+device memory; the projected problem and the Sturm walk are host logic of the library (C++).
+
+Every call runs the CUDA library (include/oos_gpu.h); nothing here computes on the CPU.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as nat
+from .linalg import SparsePencil, _check
+
+PURPOSES = ["lowest_bound", "lower_bound", "upper_bound", "advance", "fill_gap"]
+
+
+@dataclass
+class EigenRequest:
+    """EigenRequest (EigenRequest.hpp:21-35): every root of [lower_bound, upper_bound] (mode_count 0), or the lowest
+    mode_count roots above lower_bound (below upper_bound when finite). lower_bound <= 0 starts from the lowest root."""
+
+    lower_bound: float = -math.inf
+    upper_bound: float = math.inf
+    mode_count: int = 0
+
+
+def _defaults():
+    options = nat.LanczosOptions()
+    nat.load().oosgpu_lanczos_defaults(ctypes.byref(options))
+    return options
+
+
+@dataclass
+class LanczosOptions:
+    """LanczosOptions (BlockLanczos.hpp:21-64); None takes the reference's default."""
+
+    block_size: int | None = None
+    modes_per_shift: int | None = None
+    convergence_tolerance: float | None = None
+    maximum_shifts: int | None = None
+    maximum_restarts: int | None = None
+    seed: int | None = None
+
+    def native(self):
+        options = _defaults()
+        for name in ("block_size", "modes_per_shift", "convergence_tolerance", "maximum_shifts", "maximum_restarts",
+                     "seed"):
+            value = getattr(self, name)
+            if value is not None:
+                setattr(options, name, value)
+        return options
+
+
+@dataclass
+class ShiftRecord:
+    """ShiftRecord (BlockLanczos.hpp:68-78)."""
+
+    shift: float
+    purpose: str
+    sturm_count: int
+    has_lanczos_run: bool
+    block_steps: int
+    restarts: int
+    converged_count: int
+
+
+@dataclass
+class EigenSolution:
+    """EigenSolution (BlockLanczos.hpp:81-100): eigenvalues increasing, M-orthonormal eigenvectors (host copy, n x k),
+    the residual bounds, the shifts, and the solve's wall seconds and its factorisations' device seconds."""
+
+    eigenvalues: np.ndarray
+    eigenvectors: np.ndarray | None
+    residual_bounds: np.ndarray
+    shifts: list = field(default_factory=list)
+    factorisation_count: int = 0
+    verified_count: int = 0
+    is_complete: bool = False
+    block_steps: int = 0
+    seconds: float = 0.0
+    factor_seconds: float = 0.0
+
+
+class BlockLanczos:
+    """BlockLanczos (BlockLanczos.hpp:102-161) on the GPU."""
+
+    def __init__(self, options: LanczosOptions | None = None):
+        self.options = options or LanczosOptions()
+
+    def solve(self, pencil: SparsePencil, request: EigenRequest, vectors: bool = True) -> EigenSolution:
+        lib = nat.load()
+        native_request = nat.EigenRequest(float(request.lower_bound), float(request.upper_bound),
+                                          int(request.mode_count))
+        options = self.options.native()
+        handle = nat.vp()
+        _check(lib.oosgpu_modes_solve(pencil._handle, ctypes.byref(native_request), ctypes.byref(options),
+                                      ctypes.byref(handle)))
+        try:
+            counts = np.zeros(6, dtype=np.int64)
+            seconds = np.zeros(2)
+            _check(lib.oosgpu_modes_summary(handle, nat.ptr(counts, nat.i64p), nat.ptr(seconds, nat.f64p)))
+            k = int(counts[0])
+            values = np.zeros(max(k, 1))
+            bounds = np.zeros(max(k, 1))
+            _check(lib.oosgpu_modes_values(handle, nat.ptr(values, nat.f64p), nat.ptr(bounds, nat.f64p)))
+            phi = None
+            if vectors:
+                phi = np.zeros((pencil.dimension, k), order="F")
+                if k > 0:
+                    _check(lib.oosgpu_modes_vectors(handle, nat.ptr(phi, nat.f64p), pencil.dimension))
+            records = np.zeros((max(int(counts[2]), 1), 7))
+            _check(lib.oosgpu_modes_shifts(handle, nat.ptr(records, nat.f64p)))
+            shifts = [ShiftRecord(float(r[0]), PURPOSES[int(r[1])], int(r[2]), bool(r[3]), int(r[4]), int(r[5]),
+                                  int(r[6])) for r in records[: int(counts[2])]]
+            return EigenSolution(values[:k], phi, bounds[:k], shifts, int(counts[1]), int(counts[3]),
+                                 bool(counts[4]), int(counts[5]), float(seconds[0]), float(seconds[1]))
+        finally:
+            lib.oosgpu_modes_destroy(handle)

@@ -141,10 +141,13 @@ class PivotPolicy:
 
 @dataclass
 class FactorOptions:
-    """FactorOptions (SupernodalFactor.hpp:63-97) of the positive definite mode."""
+    """FactorOptions (SupernodalFactor.hpp:63-97). pivoting: "positive_definite" (PivotingMode::PositiveDefinite:
+    no pivoting, the ratio test, a zero pivot refused) or "indefinite" (PivotingMode::Indefinite: Bunch-Kaufman 1x1 /
+    2x2 pivots within each front, zero pivots counted in the inertia)."""
 
     pivot_policy: PivotPolicy = field(default_factory=PivotPolicy)
     reference_diagonal: np.ndarray | None = None
+    pivoting: str = "positive_definite"
 
 
 @dataclass
@@ -202,6 +205,9 @@ class SupernodalFactor:
         native = nat.FactorOptions()
         native.max_ratio = options.pivot_policy.max_ratio
         native.bailout = options.pivot_policy.bailout
+        if options.pivoting not in ("positive_definite", "indefinite"):
+            raise ValueError(f"FactorOptions.pivoting: expected positive_definite or indefinite, found {options.pivoting}")
+        native.pivoting = 1 if options.pivoting == "indefinite" else 0
         self._reference = None
         if options.reference_diagonal is not None:
             self._reference = np.ascontiguousarray(options.reference_diagonal, dtype=np.float64)
@@ -236,6 +242,7 @@ class SupernodalFactor:
         self.zero_pivots = list(info.zero_pivots[: min(16, int(info.zero_pivot_count))])
         self.delayed_pivot_count = int(info.delayed)
         self.two_by_two_pivot_count = int(info.two_by_two)
+        self.is_singular = self.inertia.zero > 0
         self.device_seconds = float(info.device_seconds)
 
     @property
@@ -373,3 +380,125 @@ def solve_refined(factor: SupernodalFactor, b, x, tolerance: float = 1.0e-10, ma
                                                ctypes.byref(options), ctypes.byref(info)))
     return RefinementInfo(int(info.steps), float(info.residual), float(info.device_seconds),
                           float(info.backward_error))
+
+
+# ---- the shifted pencil of an eigenvalue analysis --------------------------------------------------------------------
+
+
+@dataclass
+class ShiftFactorisation:
+    """ShiftFactorisation (include/oos/linalg/eigen/ShiftedPencil.hpp:34-42): the inertia of K - shift M, whose
+    negative count is the Sturm count of the shift."""
+
+    shift: float
+    inertia: Inertia
+    two_by_two: int = 0
+
+    @property
+    def sturm_count(self) -> int:
+        return self.inertia.negative
+
+    @property
+    def is_singular(self) -> bool:
+        return self.inertia.zero > 0
+
+
+class SparsePencil:
+    """SparsePencil (include/oos/linalg/eigen/SparsePencil.hpp:29-85) on the GPU: the pencil (K, M) of two lower CSC
+    matrices of one structure. factorise(shift) factorises S (K - shift M) S in indefinite mode (S the powers of two of
+    PencilScaling); solve() applies (K - shift M)^-1 and multiply_mass() M to device blocks with contiguous columns
+    (torch tensors) or to column-major host arrays (copied through the device)."""
+
+    def __init__(self, symbolic: SymbolicFactor, stiffness: SymmetricCsc, mass: SymmetricCsc, device: int = 0):
+        offsets = np.ascontiguousarray(stiffness.offsets, dtype=np.int64)
+        rows = np.ascontiguousarray(stiffness.rows, dtype=np.int32)
+        if not (np.array_equal(offsets, np.asarray(mass.offsets)) and np.array_equal(rows, np.asarray(mass.rows))):
+            raise ValueError("SparsePencil: the stiffness and the mass differ in structure")
+        k = np.ascontiguousarray(stiffness.values, dtype=np.float64)
+        m = np.ascontiguousarray(mass.values, dtype=np.float64)
+        self.symbolic = symbolic
+        self.device = device
+        self._handle = nat.vp()
+        _check(nat.load().oosgpu_pencil_create(symbolic._handle, device, len(offsets) - 1, nat.ptr(offsets, nat.i64p),
+                                               nat.ptr(rows, nat.i32p), nat.ptr(k, nat.f64p), nat.ptr(m, nat.f64p),
+                                               ctypes.byref(self._handle)))
+        self._dimension = len(offsets) - 1
+
+    @property
+    def dimension(self) -> int:
+        return self._dimension
+
+    @property
+    def stream(self) -> int:
+        return int(nat.load().oosgpu_pencil_stream(self._handle) or 0)
+
+    def _properties(self):
+        bound = ctypes.c_double()
+        lumped = ctypes.c_int32()
+        count = ctypes.c_int64()
+        _check(nat.load().oosgpu_pencil_properties(self._handle, ctypes.byref(bound), ctypes.byref(lumped),
+                                                   ctypes.byref(count)))
+        return bound.value, bool(lumped.value), int(count.value)
+
+    @property
+    def diagonal_rayleigh_bound(self) -> float:
+        return self._properties()[0]
+
+    @property
+    def has_diagonal_mass(self) -> bool:
+        return self._properties()[1]
+
+    @property
+    def factorisation_count(self) -> int:
+        return self._properties()[2]
+
+    def factorise(self, shift: float) -> ShiftFactorisation:
+        info = nat.FactorInfo()
+        _check(nat.load().oosgpu_pencil_factorise(self._handle, float(shift), ctypes.byref(info)))
+        return ShiftFactorisation(float(shift), Inertia(int(info.positive), int(info.negative), int(info.zero)),
+                                  int(info.two_by_two))
+
+    def _device_call(self, fn, *blocks):
+        """Runs fn on device blocks; host blocks are copied to the device and the last one back."""
+        if all(not isinstance(b, np.ndarray) for b in blocks):
+            fn(*blocks)
+            return blocks[-1]
+        import torch
+
+        staged = []
+        for b in blocks:
+            n, k, _ = _block_layout(b)
+            t = torch.empty((k, n), dtype=torch.float64, device=f"cuda:{self.device}").t()
+            t.copy_(torch.from_numpy(np.asarray(b).reshape(n, k, order="F")))
+            staged.append(t)
+        fn(*staged)
+        torch.cuda.synchronize(self.device)
+        out = blocks[-1]
+        out.reshape(out.shape[0], -1, order="F")[...] = staged[-1].cpu().numpy()
+        return out
+
+    def solve(self, block):
+        """X <- (K - shift M)^-1 X with the last factor, in place."""
+        def run(x):
+            n, k, ld = _block_layout(x)
+            _check(nat.load().oosgpu_pencil_solve_device(self._handle, x.data_ptr(), ld, k))
+        return self._device_call(run, block)
+
+    def multiply_mass(self, x, y):
+        """Y <- M X (distinct storage)."""
+        def run(a, b):
+            n, k, ldx = _block_layout(a)
+            _, _, ldy = _block_layout(b)
+            _check(nat.load().oosgpu_pencil_multiply_mass_device(self._handle, a.data_ptr(), ldx, b.data_ptr(), ldy, k))
+        return self._device_call(run, x, y)
+
+    def close(self):
+        if self._handle:
+            nat.load().oosgpu_pencil_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

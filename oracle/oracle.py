@@ -65,8 +65,9 @@ def ref_lib():
     lib.ref_factor_info.argtypes = [_vp, _i64p, _f64p]
     lib.ref_factor_panel.argtypes = [_vp, ctypes.c_int32, _i64p, _i64p, _f64p, _i32p, _f64p]
     lib.ref_solve.argtypes = [_vp, _f64p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, _f64p]
-    lib.ref_modes.argtypes = [_vp, ctypes.c_int32, _i64p, _i32p, _f64p, _f64p, ctypes.c_int64, ctypes.c_int64,
-                              ctypes.c_int, ctypes.c_int, _f64p, _f64p, _f64p, ctypes.c_int64, _i64p, _f64p]
+    lib.ref_modes.argtypes = [_vp, ctypes.c_int32, _i64p, _i32p, _f64p, _f64p, ctypes.c_double, ctypes.c_double,
+                              ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int, _f64p,
+                              ctypes.c_int64, _f64p, _f64p, ctypes.c_int64, _i64p, _f64p]
     lib.ref_pencil_scale.argtypes = [ctypes.c_int32, _i64p, _i32p, _f64p, _f64p]
     _ref = lib
     return lib
@@ -216,21 +217,25 @@ def factorise(symbolic: RefSymbolic, offsets, rows, values, indefinite=False, fa
 
 
 def modes(symbolic: RefSymbolic, offsets, rows, stiffness, mass, mode_count, block_size=8, family=-1, threads=1,
-          vectors=True):
+          vectors=True, lower=-np.inf, upper=np.inf, modes_per_shift=0, capacity=None):
+    """SparsePencil + BlockLanczos::solve of the request (lower, upper, mode_count). shifts: one row per shift of
+    (shift, purpose, sturm count, has run, block steps, restarts, converged)."""
     lib = ref_lib()
     n = symbolic.dof_count
     offsets = np.ascontiguousarray(offsets, dtype=np.int64)
     rows = np.ascontiguousarray(rows, dtype=np.int32)
     stiffness = np.ascontiguousarray(stiffness, dtype=np.float64)
     mass = np.ascontiguousarray(mass, dtype=np.float64)
-    values = np.zeros(mode_count)
-    vecs = np.zeros((mode_count, n)) if vectors else None
-    shifts = np.zeros((64, 6))
-    counts = np.zeros(4, dtype=np.int64)
+    capacity = capacity if capacity is not None else max(mode_count, 1)
+    values = np.zeros(capacity)
+    vecs = np.zeros((capacity, n)) if vectors else None
+    shifts = np.zeros((64, 7))
+    counts = np.zeros(5, dtype=np.int64)
     seconds = np.zeros(1)
     _check(lib.ref_modes(symbolic.handle, n, _ptr(offsets, _i64p), _ptr(rows, _i32p), _ptr(stiffness, _f64p),
-                         _ptr(mass, _f64p), mode_count, block_size, family, threads, _ptr(values, _f64p),
-                         _ptr(vecs, _f64p), _ptr(shifts, _f64p), 64, _ptr(counts, _i64p), _ptr(seconds, _f64p)))
+                         _ptr(mass, _f64p), lower, upper, mode_count, block_size, modes_per_shift, family, threads,
+                         _ptr(values, _f64p), capacity, _ptr(vecs, _f64p), _ptr(shifts, _f64p), 64,
+                         _ptr(counts, _i64p), _ptr(seconds, _f64p)))
     found = int(counts[0])
     return {
         "eigenvalues": values[:found],
@@ -238,6 +243,7 @@ def modes(symbolic: RefSymbolic, offsets, rows, stiffness, mass, mode_count, blo
         "shifts": shifts[: int(min(counts[2], 64))],
         "factorisations": int(counts[1]),
         "verified": int(counts[3]),
+        "complete": bool(counts[4]),
         "seconds": float(seconds[0]),
     }
 

@@ -304,9 +304,10 @@ extern "C" int ref_solve(const ref_factor* f, double* b, int64_t ld, int64_t col
 }
 
 extern "C" int ref_modes(const ref_symbolic* s, int32_t dimension, const int64_t* col_offsets, const int32_t* rows,
-                         const double* stiffness, const double* mass, int64_t mode_count, int64_t block_size,
-                         int family, int threads, double* eigenvalues, double* eigenvectors, double* shifts,
-                         int64_t max_shifts, int64_t counts[4], double* seconds)
+                         const double* stiffness, const double* mass, double lower, double upper, int64_t mode_count,
+                         int64_t block_size, int64_t modes_per_shift, int family, int threads, double* eigenvalues,
+                         int64_t capacity, double* eigenvectors, double* shifts, int64_t max_shifts,
+                         int64_t counts[5], double* seconds)
 {
     return guarded(
         [&]
@@ -333,13 +334,17 @@ extern "C" int ref_modes(const ref_symbolic* s, int32_t dimension, const int64_t
             LanczosOptions lanczos;
             if (block_size > 0)
                 lanczos.blockSize = static_cast<std::size_t>(block_size);
+            if (modes_per_shift > 0)
+                lanczos.modesPerShift = static_cast<std::size_t>(modes_per_shift);
             EigenRequest request;
+            request.lowerBound = lower;
+            request.upperBound = upper;
             request.modeCount = static_cast<std::size_t>(mode_count);
             const EigenSolution solution = BlockLanczos(lanczos).solve(pencil, request, kernels, budget);
             if (seconds != nullptr)
                 seconds[0] = secondsSince(start);
             const std::size_t found = std::min<std::size_t>(solution.eigenvalues.size(),
-                                                            static_cast<std::size_t>(mode_count));
+                                                            static_cast<std::size_t>(capacity));
             for (std::size_t j = 0; j < found; ++j)
             {
                 eigenvalues[j] = solution.eigenvalues[j];
@@ -352,18 +357,20 @@ extern "C" int ref_modes(const ref_symbolic* s, int32_t dimension, const int64_t
             for (std::size_t r = 0; r < records && shifts != nullptr; ++r)
             {
                 const ShiftRecord& record = solution.shifts[r];
-                double* out = shifts + 6 * r;
+                double* out = shifts + 7 * r;
                 out[0] = record.shift;
-                out[1] = static_cast<double>(record.sturmCount);
-                out[2] = static_cast<double>(record.blockSteps);
-                out[3] = static_cast<double>(record.restarts);
-                out[4] = static_cast<double>(record.convergedCount);
-                out[5] = record.hasLanczosRun ? 1.0 : 0.0;
+                out[1] = static_cast<double>(static_cast<int>(record.purpose));
+                out[2] = static_cast<double>(record.sturmCount);
+                out[3] = record.hasLanczosRun ? 1.0 : 0.0;
+                out[4] = static_cast<double>(record.blockSteps);
+                out[5] = static_cast<double>(record.restarts);
+                out[6] = static_cast<double>(record.convergedCount);
             }
             counts[0] = static_cast<int64_t>(found);
             counts[1] = static_cast<int64_t>(solution.factorisationCount);
             counts[2] = static_cast<int64_t>(solution.shifts.size());
             counts[3] = static_cast<int64_t>(solution.verifiedCount);
+            counts[4] = solution.isComplete ? 1 : 0;
         });
 }
 

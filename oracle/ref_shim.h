@@ -60,14 +60,17 @@ int ref_factor_panel(const ref_factor* f, int32_t s, int64_t* eliminated, int64_
 /* FactorSolve::solve (src/linalg/supernodal/FactorSolve.cpp:176-190): B <- A^-1 B in place, B column-major. */
 int ref_solve(const ref_factor* f, double* b, int64_t ld, int64_t columns, int threads, double* seconds);
 
-/* SparsePencil + BlockLanczos::solve (src/linalg/eigen/SparsePencil.cpp, BlockLanczos.cpp:87-244): the lowest
- * mode_count eigenpairs of K x = lambda M x. eigenvalues: mode_count; eigenvectors: dimension x mode_count (may be
- * NULL). shifts: up to max_shifts records of (shift, sturm count, block steps, restarts, converged, has run);
- * counts[0..3]: modes found, factorisations, shift records, verified count. seconds[0]: wall time of solve. */
+/* SparsePencil + BlockLanczos::solve (src/linalg/eigen/SparsePencil.cpp, BlockLanczos.cpp:87-244): the eigenpairs of
+ * K x = lambda M x that the request (lower, upper, mode_count: EigenRequest) asks for. block_size and
+ * modes_per_shift: LanczosOptions (0: the default). eigenvalues: up to `capacity`; eigenvectors: dimension x capacity
+ * (may be NULL). shifts: up to max_shifts records of (shift, purpose, sturm count, has run, block steps, restarts,
+ * converged); counts[0..4]: modes found, factorisations, shift records, verified count, complete. seconds[0]: wall
+ * time of the solve. */
 int ref_modes(const ref_symbolic* s, int32_t dimension, const int64_t* col_offsets, const int32_t* rows,
-              const double* stiffness, const double* mass, int64_t mode_count, int64_t block_size, int family,
-              int threads, double* eigenvalues, double* eigenvectors, double* shifts, int64_t max_shifts,
-              int64_t counts[4], double* seconds);
+              const double* stiffness, const double* mass, double lower, double upper, int64_t mode_count,
+              int64_t block_size, int64_t modes_per_shift, int family, int threads, double* eigenvalues,
+              int64_t capacity, double* eigenvectors, double* shifts, int64_t max_shifts, int64_t counts[5],
+              double* seconds);
 
 /* pencilScaleOf (src/linalg/eigen/PencilScaling.cpp:64-80): the power-of-two scales of a stiffness CSC. */
 int ref_pencil_scale(int32_t dimension, const int64_t* col_offsets, const int32_t* rows, const double* values,

@@ -1,0 +1,174 @@
+"""The block shift-invert Lanczos solver on the GPU (BlockLanczos::solve over a SparsePencil) against the reference's
+own solve of the same pencil: the eigenvalues within 1e-9 relative, every Sturm count of the GPU's shifts the
+reference's inertia of that shift, the request verified and complete, the eigenvectors M-orthonormal with small
+residuals, and the refusals of the reference for requests and settings out of range."""
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import has_gpu
+
+pytestmark = pytest.mark.gpu
+
+EIGENVALUE_TOLERANCE = 1e-9
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    if not has_gpu():
+        pytest.skip("no CUDA device")
+    import torch
+
+    torch.cuda.init()
+    return torch
+
+
+def problem(kind, size, oracle):
+    from o_o_solver_b200 import SymbolicFactor, SymmetricCsc, workloads
+
+    model = workloads.Model(workloads.PlateSpec(size, size) if kind == "plate" else workloads.HexSpec(size))
+    sym = oracle.analyse(model.offsets, model.neighbours, model.weights, model.coordinates)
+    k = model.csc(sym.node_order, 0)
+    if kind == "hex":
+        m = model.csc(sym.node_order, 1)
+    else:  # the translations of a 2 mm aluminium sheet; no rotary inertia (a mass with a null space)
+        values = np.zeros_like(k.values)
+        mass = np.zeros(sym.dof_count)
+        mass[np.arange(sym.dof_count) % 6 < 3] = 2700.0 * 0.002 / (size * size)
+        values[k.offsets[:-1]] = mass
+        m = SymmetricCsc(k.offsets, k.rows, values)
+    symbolic = SymbolicFactor.from_arrays(sym.dof_count, sym.first_column, sym.parent, sym.row_start, sym.rows)
+    return sym, symbolic, k, m
+
+
+def sturm_count(oracle, sym, k, m, sigma):
+    scale = oracle.pencil_scale(k.offsets, k.rows, k.values)
+    cols = np.repeat(np.arange(k.dimension), np.diff(k.offsets))
+    values = (k.values - sigma * m.values) * scale[k.rows] * scale[cols]
+    ref = oracle.factorise(sym, k.offsets, k.rows, values, indefinite=True, family=0)
+    return ref.negative
+
+
+def pair_residuals(k, m, values, vectors):
+    """||K phi - lambda M phi|| / ||K phi|| per pair, and phi^T M phi."""
+    from o_o_solver_b200 import workloads
+
+    kphi = workloads.lower_csc_multiply(k, vectors)
+    mphi = workloads.lower_csc_multiply(m, vectors)
+    return np.linalg.norm(kphi - mphi * values, axis=0) / np.linalg.norm(kphi, axis=0), vectors.T @ mphi
+
+
+def check_pairs(k, m, values, vectors, reference=None):
+    """M-orthonormal eigenvectors whose residuals are at most 1e-8, or ten times the reference's own residuals of
+    the same pairs (a stiff pencil amplifies the vectors' rounding in ||K phi - lambda M phi||)."""
+    residual, gram = pair_residuals(k, m, values, vectors)
+    bound = np.full_like(residual, 1e-8)
+    if reference is not None:
+        bound = np.maximum(bound, 10.0 * pair_residuals(k, m, *reference)[0])
+    assert np.all(residual <= bound), (residual, bound)
+    assert np.abs(gram - np.eye(len(values))).max() <= 1e-10
+
+
+@pytest.mark.parametrize("kind,size,modes,block", [("hex", 8, 20, 8), ("plate", 24, 12, 7), ("hex", 12, 30, 8)])
+def test_lowest_modes_match_reference(kind, size, modes, block, lib, oracle_mod, gpu):
+    from o_o_solver_b200 import SparsePencil
+    from o_o_solver_b200.eigen import BlockLanczos, EigenRequest, LanczosOptions
+
+    sym, symbolic, k, m = problem(kind, size, oracle_mod)
+    ref = oracle_mod.modes(sym, k.offsets, k.rows, k.values, m.values, modes, block_size=block)
+    pencil = SparsePencil(symbolic, k, m)
+    solution = BlockLanczos(LanczosOptions(block_size=block)).solve(pencil, EigenRequest(mode_count=modes))
+    assert solution.is_complete and solution.verified_count == modes
+    assert len(solution.eigenvalues) == modes
+    assert np.all(np.diff(solution.eigenvalues) >= 0)
+    relative = np.abs(solution.eigenvalues - ref["eigenvalues"]) / np.abs(ref["eigenvalues"])
+    assert relative.max() <= EIGENVALUE_TOLERANCE, relative
+    assert np.all(solution.residual_bounds <= 1e-10)
+    check_pairs(k, m, solution.eigenvalues, solution.eigenvectors, (ref["eigenvalues"], ref["eigenvectors"]))
+    # Every Sturm point of the GPU's walk is the reference's inertia at that shift.
+    for record in solution.shifts:
+        assert record.sturm_count == sturm_count(oracle_mod, sym, k, m, record.shift), record
+    assert solution.factorisation_count == pencil.factorisation_count
+
+
+def test_range_request(lib, oracle_mod, gpu):
+    """Every root of [lower, upper] (bounds between roots, a repeated root inside): the reference's roots of the same
+    request, the Sturm points at both bounds first."""
+    from o_o_solver_b200 import SparsePencil
+    from o_o_solver_b200.eigen import BlockLanczos, EigenRequest, LanczosOptions
+
+    sym, symbolic, k, m = problem("hex", 8, oracle_mod)
+    lowest = oracle_mod.modes(sym, k.offsets, k.rows, k.values, m.values, 24, block_size=8, vectors=False)
+    ref = lowest["eigenvalues"]
+    lower = 0.5 * (ref[3] + ref[4])
+    upper = 0.5 * (ref[18] + ref[19])
+    expected = oracle_mod.modes(sym, k.offsets, k.rows, k.values, m.values, 0, block_size=8, lower=lower,
+                                upper=upper, capacity=64)
+    assert expected["complete"]
+    pencil = SparsePencil(symbolic, k, m)
+    solution = BlockLanczos(LanczosOptions(block_size=8)).solve(pencil, EigenRequest(lower, upper, 0))
+    assert solution.is_complete
+    assert len(solution.eigenvalues) == len(expected["eigenvalues"]) == 15
+    values = expected["eigenvalues"]
+    assert np.abs(solution.eigenvalues - values).max() <= EIGENVALUE_TOLERANCE * np.abs(values).max()
+    purposes = [r.purpose for r in solution.shifts]
+    assert purposes[0] == "upper_bound" and purposes[1] == "lower_bound"
+    for record in solution.shifts:
+        assert record.sturm_count == sturm_count(oracle_mod, sym, k, m, record.shift), record
+    check_pairs(k, m, solution.eigenvalues, solution.eigenvectors, (values, expected["eigenvectors"]))
+
+
+def test_thick_restarts(lib, oracle_mod, gpu):
+    """A basis of a few blocks (4 modes per shift) for 16 modes: many restarts and shifts, the reference's roots."""
+    from o_o_solver_b200 import SparsePencil
+    from o_o_solver_b200.eigen import BlockLanczos, EigenRequest, LanczosOptions
+
+    sym, symbolic, k, m = problem("hex", 8, oracle_mod)
+    ref = oracle_mod.modes(sym, k.offsets, k.rows, k.values, m.values, 16, block_size=4, modes_per_shift=4)
+    assert ref["complete"] and any(row[5] > 0 for row in ref["shifts"])
+    pencil = SparsePencil(symbolic, k, m)
+    solution = BlockLanczos(LanczosOptions(block_size=4, modes_per_shift=4)).solve(pencil,
+                                                                                   EigenRequest(mode_count=16))
+    assert solution.is_complete and len(solution.eigenvalues) == 16
+    assert any(r.restarts > 0 for r in solution.shifts)
+    relative = np.abs(solution.eigenvalues - ref["eigenvalues"]) / ref["eigenvalues"]
+    assert relative.max() <= EIGENVALUE_TOLERANCE, relative
+    for record in solution.shifts:
+        assert record.sturm_count == sturm_count(oracle_mod, sym, k, m, record.shift), record
+    check_pairs(k, m, solution.eigenvalues, solution.eigenvectors, (ref["eigenvalues"], ref["eigenvectors"]))
+
+
+def test_same_bits_twice(lib, oracle_mod, gpu):
+    """The seeded starts and the fixed orders of every sum: two solves give the same bits."""
+    from o_o_solver_b200 import SparsePencil
+    from o_o_solver_b200.eigen import BlockLanczos, EigenRequest, LanczosOptions
+
+    sym, symbolic, k, m = problem("hex", 6, oracle_mod)
+    pencil = SparsePencil(symbolic, k, m)
+    first = BlockLanczos(LanczosOptions(block_size=4)).solve(pencil, EigenRequest(mode_count=10))
+    second = BlockLanczos(LanczosOptions(block_size=4)).solve(pencil, EigenRequest(mode_count=10))
+    assert np.array_equal(first.eigenvalues, second.eigenvalues)
+    assert np.array_equal(first.eigenvectors, second.eigenvectors)
+
+
+def test_refusals(lib, oracle_mod, gpu):
+    from o_o_solver_b200 import SparsePencil
+    from o_o_solver_b200.eigen import BlockLanczos, EigenRequest, LanczosOptions
+
+    sym, symbolic, k, m = problem("hex", 4, oracle_mod)
+    pencil = SparsePencil(symbolic, k, m)
+    with pytest.raises(ValueError, match="neither a mode count nor an upper bound"):
+        BlockLanczos().solve(pencil, EigenRequest())
+    with pytest.raises(ValueError, match="must be above the lower bound"):
+        BlockLanczos().solve(pencil, EigenRequest(10.0, 5.0, 0))
+    with pytest.raises(ValueError, match="convergence tolerance"):
+        BlockLanczos(LanczosOptions(convergence_tolerance=0.5)).solve(pencil, EigenRequest(mode_count=3))
+    with pytest.raises(ValueError, match="block size"):
+        BlockLanczos(LanczosOptions(block_size=0)).solve(pencil, EigenRequest(mode_count=3))
+    assert pencil.factorisation_count == 0
+    # Still usable after the refusals.
+    solution = BlockLanczos(LanczosOptions(block_size=4)).solve(pencil, EigenRequest(mode_count=3))
+    assert solution.is_complete and len(solution.eigenvalues) == 3
+    assert math.isfinite(solution.eigenvalues[0])
