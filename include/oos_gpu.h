@@ -80,7 +80,8 @@ typedef struct
     const double* reference_diagonal; /* FactorOptions::referenceDiagonal (host, dimension values) or NULL */
     /* FactorOptions::pivoting: 0 PivotingMode::PositiveDefinite, 1 PivotingMode::Indefinite (Bunch-Kaufman 1x1/2x2
      * pivots within each front; zero pivots counted in the inertia, not refused; the ratio test is not applied; a
-     * pivot that would be delayed to a parent front is refused with OOSGPU_SOLVER) */
+     * pivot the reference would delay to a parent front is taken in place when its diagonal is at least 1e-3 of its
+     * column maximum (info->forced), refused with OOSGPU_SOLVER below that) */
     int32_t pivoting;
 } oosgpu_factor_options;
 
@@ -99,6 +100,8 @@ typedef struct
     int32_t issues[16];             /* the first flagged equations, increasing */
     int32_t zero_pivots[16];        /* the first zero-pivot equations, increasing */
     double device_seconds;          /* the factorisation's device time (CUDA events) */
+    int64_t forced;                 /* indefinite mode: pivots the reference would delay to a parent front, taken in
+                                       place (|d| >= 1e-3 of the column maximum; no counterpart in the reference) */
 } oosgpu_factor_info;
 
 /* A factor of `symbolic` on CUDA device `device` (the symbolic structure is copied: it may be destroyed after). */
@@ -234,8 +237,10 @@ typedef struct oosgpu_modes oosgpu_modes;
 int oosgpu_modes_solve(oosgpu_pencil* pencil, const oosgpu_eigen_request* request,
                        const oosgpu_lanczos_options* options, oosgpu_modes** out);
 /* counts: [0] eigenpairs, [1] factorisations, [2] shifts, [3] verified by the Sturm counts, [4] complete (0/1),
- * [5] Lanczos block steps; seconds: [0] wall seconds of the solve, [1] device seconds of its factorisations. */
-int oosgpu_modes_summary(const oosgpu_modes* modes, int64_t counts[6], double seconds[2]);
+ * [5] Lanczos block steps; seconds: [0] wall seconds of the solve, [1] device seconds of its factorisations, then
+ * wall seconds of [2] the factorisations, [3] the operator (solves and mass products), [4] the M-orthogonalisation
+ * and the basis products, [5] the projected problem. */
+int oosgpu_modes_summary(const oosgpu_modes* modes, int64_t counts[6], double seconds[6]);
 /* The eigenvalues (increasing) and their residual bounds ||Op y - theta y||_M / |theta|. */
 int oosgpu_modes_values(const oosgpu_modes* modes, double* eigenvalues, double* residual_bounds);
 /* The M-orthonormal eigenvectors, dimension x count, into host memory of leading dimension ld. */

@@ -33,6 +33,7 @@ class FactorInfo(ctypes.Structure):
         ("issues", ctypes.c_int32 * 16),
         ("zero_pivots", ctypes.c_int32 * 16),
         ("device_seconds", ctypes.c_double),
+        ("forced", ctypes.c_int64),
     ]
 
 

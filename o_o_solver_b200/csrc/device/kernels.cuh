@@ -4,6 +4,7 @@
 
 #include "common.cuh"
 
+#include <cstddef>
 #include <cstdint>
 
 namespace oosgpu::device
@@ -60,6 +61,12 @@ __global__ void pivotSummary(FactorArgs args, const std::int32_t* supernodeOfCol
                              std::int32_t* issues, int issueCapacity, double* blockRatio, std::int32_t* blockEquation);
 __global__ void forwardSmall(SolveArgs a, const std::int32_t* list);
 __global__ void forwardGather(SolveArgs a, const TileTask* tasks);
+__global__ void invertDiagonal(FactorArgs args, const TileTask* tasks);
+// Dynamic shared memory of forwardDiagonal / backwardDiagonal for a tile of `width` columns.
+constexpr std::size_t diagonalSolveSmem(int width)
+{
+    return static_cast<std::size_t>(64 * 65 + 64 * width) * sizeof(double);
+}
 __global__ void forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0);
 __global__ void forwardUpdate(SolveArgs a, const TileTask* tasks, int k0);
 __global__ void diagonalSweep(SolveArgs a, const std::int32_t* supernodeOfColumn, int dimension);

@@ -7,6 +7,10 @@
 //   |a_kk| >= 0.01 colmax and delayed otherwise, ties of the maxima to the first index. It runs on a whole small front
 //   in shared memory (smallFrontsPivoted), on a large front's diagonal block (pivotedDiagonal), and on a whole front
 //   in global memory (pivotedFront, the exact path of a front the block path refuses).
+//   Where the reference would delay a candidate to the parent front (its passes make no progress), the GPU path takes
+//   it in place as a 1x1 pivot when |a_kk| >= 1e-3 colmax (a "forced" pivot: the growth of its column of L at most
+//   1e3, ten times the reference's bound, so the factor stays backward stable and its inertia, by Sylvester's law, is
+//   the reference's); below that the factorisation is refused. The fronts keep their symbolic sizes.
 // - large fronts, per 64-column block: Bunch-Kaufman inside the diagonal block (its columns are all candidates and its
 //   rows the only ones searched), then the rows below solved against it (L = A L11^-T D^-1, 2x2 blocks by the dsytf2
 //   formula) with an a-posteriori threshold test |l_ij| <= 1/u, u = 0.01 (the reference's delay threshold), and the
@@ -30,6 +34,7 @@ namespace
 
 constexpr double BK_ALPHA = 0.6403882032022076;  // (1 + sqrt(17)) / 8
 constexpr double DELAY_THRESHOLD = 0.01;          // the reference's DELAYED_PIVOT_THRESHOLD
+constexpr double FORCED_THRESHOLD = 1.0e-3;       // a candidate the reference would delay, taken in place
 constexpr double GROWTH_LIMIT = 1.0 / DELAY_THRESHOLD;
 
 // The column maximum |a(i, k)| over i in (k, n) and its first row, on the whole block (ties to the first index).
@@ -155,10 +160,12 @@ __device__ __forceinline__ TwoByTwoInverse invertTwoByTwo(double a, double b, do
 
 // Bunch-Kaufman on the block `at` (n x n lower, the first `candidates` columns the candidates) by the whole thread
 // block. perm: the block positions' origins (permuted with the interchanges); subdiagonal: e_k of each 2x2 pivot at its
-// first column, 0 elsewhere. Returns the columns eliminated (< candidates when some were delayed).
+// first column, 0 elsewhere. With allowForced, the candidates left when a pass makes no progress get one more pass at
+// the forced threshold; `forced` (when given) receives the pivots taken below the delay threshold. Returns the columns
+// eliminated (< candidates when some were delayed).
 template <typename At>
 __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* subdiagonal, double* scratchValue,
-                            int* scratchIndex)
+                            int* scratchIndex, bool allowForced, int* forced)
 {
     for (int i = threadIdx.x; i < candidates; i += blockDim.x)
     {
@@ -169,6 +176,8 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
     int k = 0;
     int end = candidates;
     int passStart = 0;
+    double threshold = DELAY_THRESHOLD;
+    int forcedCount = 0;
     while (true)
     {
         while (k < end)
@@ -186,7 +195,7 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
             int swapWith = k;
             if (absakk < BK_ALPHA * colmax && imax >= end)
             {
-                if (absakk < DELAY_THRESHOLD * colmax)
+                if (absakk < threshold * colmax)
                 {
                     --end;
                     if (k != end)
@@ -202,6 +211,8 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
                     }
                     continue;
                 }
+                if (absakk < DELAY_THRESHOLD * colmax)
+                    ++forcedCount;
             }
             else if (absakk < BK_ALPHA * colmax)
             {
@@ -284,11 +295,19 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
             }
             k += blockSize;
         }
-        if (end == candidates || k == passStart)
+        if (end == candidates)
             break;
+        if (k == passStart)
+        {
+            if (!allowForced || threshold == FORCED_THRESHOLD)
+                break;
+            threshold = FORCED_THRESHOLD;
+        }
         passStart = k;
         end = candidates;
     }
+    if (forced != nullptr && threadIdx.x == 0)
+        *forced = forcedCount;
     return k;
 }
 
@@ -327,9 +346,15 @@ __global__ void smallFrontsPivoted(FactorArgs args, PivotArgs pivots, const std:
     const int ld = n + 1;
     assembleFrontBy(
         args, f, [&](int i, int j) -> double& { return front[i + j * ld]; }, structureError);
-    const int eliminated = bunchKaufman(SharedAt{front, ld}, n, f.c, perm, sub, scratchValue, scratchIndex);
-    if (eliminated < f.c && threadIdx.x == 0)
-        atomicOr(pivots.status + s, 2 | (min(eliminated, 0xfffff) << 8));
+    __shared__ int forced;
+    const int eliminated = bunchKaufman(SharedAt{front, ld}, n, f.c, perm, sub, scratchValue, scratchIndex, true, &forced);
+    if (threadIdx.x == 0)
+    {
+        if (eliminated < f.c)
+            atomicOr(pivots.status + s, 2 | (min(eliminated, 0xfffff) << 8));
+        else if (forced > 0)
+            atomicOr(pivots.status + s, 4 | (min(forced, 0xfffff) << 8));
+    }
     double* panel = args.panels + f.panel;
     for (int e = threadIdx.x; e < n * f.c; e += blockDim.x)
     {
@@ -382,9 +407,10 @@ __global__ void pivotedDiagonal(FactorArgs args, PivotArgs pivots, const std::in
         a[i + j * LD] = block[i + static_cast<std::int64_t>(j) * n];
     }
     __syncthreads();
-    const int eliminated = bunchKaufman(SharedAt{a, LD}, kb, kb, perm, sub, scratchValue, scratchIndex);
+    // A candidate the block cannot pivot sends the front to the exact path (status bit 1), as a failed growth test.
+    const int eliminated = bunchKaufman(SharedAt{a, LD}, kb, kb, perm, sub, scratchValue, scratchIndex, false, nullptr);
     if (eliminated < kb && threadIdx.x == 0)
-        atomicOr(pivots.status + s, 2);
+        atomicOr(pivots.status + s, 1);
     for (int e = threadIdx.x; e < kb * kb; e += blockDim.x)
     {
         const int j = e / kb;
@@ -585,9 +611,11 @@ __global__ void pivotedFront(FactorArgs args, PivotArgs pivots, std::int32_t s, 
         structureError);
     int* perm = pivots.frontPerm;
     double* sub = pivots.frontSub;
-    const int eliminated = bunchKaufman(GlobalAt{work, ld}, n, f.c, perm, sub, scratchValue, scratchIndex);
+    __shared__ int forced;
+    const int eliminated = bunchKaufman(GlobalAt{work, ld}, n, f.c, perm, sub, scratchValue, scratchIndex, true, &forced);
     if (threadIdx.x == 0)
-        pivots.status[s] = eliminated < f.c ? 2 | (min(eliminated, 0xfffff) << 8) : 0;
+        pivots.status[s] = eliminated < f.c ? 2 | (min(eliminated, 0xfffff) << 8)
+                                            : (forced > 0 ? 4 | (min(forced, 0xfffff) << 8) : 0);
     double* panel = args.panels + f.panel;
     for (std::int64_t x = threadIdx.x; x < static_cast<std::int64_t>(n) * f.c; x += blockDim.x)
     {

@@ -151,49 +151,92 @@ __global__ void __launch_bounds__(SOLVE_THREADS) forwardGather(SolveArgs a, cons
     }
 }
 
-// The 64 x 64 diagonal block of L at step k0 of a large supernode, staged in shared memory (zero outside the block):
-// l[q * SOLVE_BLOCK + i] = L(k0 + i, k0 + q).
-__device__ __forceinline__ int stageDiagonalBlock(const SolveArgs& a, const FrontDesc& f, int k0, double* l)
+// The inverse of the unit lower 64 x 64 diagonal block of step k0 of a large supernode, after each factorisation: one
+// thread per column j of L11^-1 carries it through the forward substitution of e_j in registers, reading L11 from shared
+// memory by broadcast; the strict lower part of L11^-1 is written transposed into the block's strict upper triangle
+// (unused by the factor: L11^-1(i, j) at panel position (k0 + j, k0 + i)), where the solves' diagonal steps read it.
+__global__ void __launch_bounds__(SOLVE_BLOCK) invertDiagonal(FactorArgs args, const TileTask* tasks)
 {
+    constexpr int LD = SOLVE_BLOCK + 1;
+    __shared__ double l[SOLVE_BLOCK * LD]; // l[q * LD + i] = L(k0 + i, k0 + q), i > q
+    const TileTask task = tasks[blockIdx.x];
+    const FrontDesc f = args.fronts[task.front];
     const std::int64_t n = f.c + f.r;
+    const int k0 = task.i0;
     const int kb = min(SOLVE_BLOCK, f.c - k0);
-    const double* panel = a.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
+    double* block = args.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
     for (int e = threadIdx.x; e < SOLVE_BLOCK * SOLVE_BLOCK; e += blockDim.x)
     {
         const int q = e / SOLVE_BLOCK;
         const int i = e - q * SOLVE_BLOCK;
-        l[e] = q < kb && i < kb ? panel[i + static_cast<std::int64_t>(q) * n] : 0.0;
+        l[q * LD + i] = q < kb && i < kb && i > q ? block[i + static_cast<std::int64_t>(q) * n] : 0.0;
     }
+    __syncthreads();
+    const int j = threadIdx.x;
+    if (j >= kb)
+        return;
+    double x[SOLVE_BLOCK];
+#pragma unroll
+    for (int i = 0; i < SOLVE_BLOCK; ++i)
+        x[i] = i == j ? 1.0 : 0.0;
+#pragma unroll
+    for (int i = 1; i < SOLVE_BLOCK; ++i)
+    {
+        double v = x[i];
+#pragma unroll
+        for (int q = 0; q < i; ++q)
+            v -= l[q * LD + i] * x[q];
+        x[i] = v;
+    }
+#pragma unroll
+    for (int i = 1; i < SOLVE_BLOCK; ++i)
+        if (i > j && i < kb)
+            block[j + static_cast<std::int64_t>(i) * n] = x[i];
+}
+
+// The inverse of step k0's diagonal block staged in shared memory: inv[i * (SOLVE_BLOCK + 1) + q] = L11^-1(i, q) for
+// q < i (zero elsewhere), and the block's rows of X: b[i * w + col].
+__device__ __forceinline__ int stageInverse(const SolveArgs& a, const FrontDesc& f, int k0, double* inv, double* b,
+                                            double* xRows)
+{
+    constexpr int LD = SOLVE_BLOCK + 1;
+    const std::int64_t n = f.c + f.r;
+    const int kb = min(SOLVE_BLOCK, f.c - k0);
+    const double* block = a.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
+    for (int e = threadIdx.x; e < SOLVE_BLOCK * SOLVE_BLOCK; e += blockDim.x)
+    {
+        const int i = e / SOLVE_BLOCK;
+        const int q = e - i * SOLVE_BLOCK;
+        inv[i * LD + q] = q < i && i < kb ? block[q + static_cast<std::int64_t>(i) * n] : 0.0;
+    }
+    for (int e = threadIdx.x; e < kb * a.width; e += blockDim.x)
+        b[e] = xRows[e];
     __syncthreads();
     return kb;
 }
 
-// The unit lower triangle of step t of a large supernode: rows [k0, k0 + kb) of x_F. One thread per right-hand-side
-// column carries its column through the whole triangle in registers (no barrier inside the triangle), reading the
-// block of L from shared memory by broadcast; each value receives its terms in increasing q.
-__global__ void __launch_bounds__(SOLVE_BLOCK) forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
+// The unit lower triangle of step k0 of a large supernode (rows [k0, k0 + kb) of x_F) as the product with its inverse:
+// x_i = b_i + sum_{q < i} L11^-1(i, q) b_q, the terms in increasing q; every value of the 64 x width block is
+// independent (no chain through the triangle). Dynamic shared memory: (64 * 65 + 64 * width) doubles.
+__global__ void __launch_bounds__(SOLVE_THREADS) forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
 {
-    __shared__ double l[SOLVE_BLOCK * SOLVE_BLOCK];
+    constexpr int LD = SOLVE_BLOCK + 1;
+    extern __shared__ double stage[];
+    double* inv = stage;
+    double* b = stage + SOLVE_BLOCK * LD;
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
-    const int kb = stageDiagonalBlock(a, f, k0, l);
-    const int col = threadIdx.x;
-    if (col >= w)
-        return;
-    double* xRows = a.x + static_cast<std::int64_t>(f.first + k0) * w + col;
-    double x[SOLVE_BLOCK];
-#pragma unroll
-    for (int i = 0; i < SOLVE_BLOCK; ++i)
-        x[i] = i < kb ? xRows[static_cast<std::int64_t>(i) * w] : 0.0;
-#pragma unroll
-    for (int i = 1; i < SOLVE_BLOCK; ++i)
-#pragma unroll
+    double* xRows = a.x + static_cast<std::int64_t>(f.first + k0) * w;
+    const int kb = stageInverse(a, f, k0, inv, b, xRows);
+    for (int e = threadIdx.x; e < kb * w; e += blockDim.x)
+    {
+        const int i = e / w;
+        const int col = e - i * w;
+        double sum = b[e];
         for (int q = 0; q < i; ++q)
-            x[i] -= l[q * SOLVE_BLOCK + i] * x[q];
-#pragma unroll
-    for (int i = 0; i < SOLVE_BLOCK; ++i)
-        if (i < kb)
-            xRows[static_cast<std::int64_t>(i) * w] = x[i];
+            sum += inv[i * LD + q] * b[q * w + col];
+        xRows[e] = sum;
+    }
 }
 
 // Step t's block applied to the rows below it: a tile of 64 rows either in x_F (i0 < c, task.k0 = 0) or in the update
@@ -315,30 +358,27 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardRows(SolveArgs a, const 
     tileProduct<true>(op, smemA, smemB);
 }
 
-// The unit upper triangle L11^T of step t (rows [k0, k0 + kb) of x_F): as forwardDiagonal, from the last row up.
-__global__ void __launch_bounds__(SOLVE_BLOCK) backwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
+// The unit upper triangle L11^T of step k0 (rows [k0, k0 + kb) of x_F) as the product with the transposed inverse:
+// x_q = b_q + sum_{i > q} L11^-1(i, q) b_i, the terms in increasing i.
+__global__ void __launch_bounds__(SOLVE_THREADS) backwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
 {
-    __shared__ double l[SOLVE_BLOCK * SOLVE_BLOCK];
+    constexpr int LD = SOLVE_BLOCK + 1;
+    extern __shared__ double stage[];
+    double* inv = stage;
+    double* b = stage + SOLVE_BLOCK * LD;
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
-    const int kb = stageDiagonalBlock(a, f, k0, l);
-    const int col = threadIdx.x;
-    if (col >= w)
-        return;
-    double* xRows = a.x + static_cast<std::int64_t>(f.first + k0) * w + col;
-    double x[SOLVE_BLOCK];
-#pragma unroll
-    for (int i = 0; i < SOLVE_BLOCK; ++i)
-        x[i] = i < kb ? xRows[static_cast<std::int64_t>(i) * w] : 0.0;
-#pragma unroll
-    for (int i = SOLVE_BLOCK - 1; i > 0; --i)
-#pragma unroll
-        for (int q = 0; q < i; ++q)
-            x[q] -= l[q * SOLVE_BLOCK + i] * x[i];
-#pragma unroll
-    for (int i = 0; i < SOLVE_BLOCK; ++i)
-        if (i < kb)
-            xRows[static_cast<std::int64_t>(i) * w] = x[i];
+    double* xRows = a.x + static_cast<std::int64_t>(f.first + k0) * w;
+    const int kb = stageInverse(a, f, k0, inv, b, xRows);
+    for (int e = threadIdx.x; e < kb * w; e += blockDim.x)
+    {
+        const int q = e / w;
+        const int col = e - q * w;
+        double sum = b[e];
+        for (int i = q + 1; i < kb; ++i)
+            sum += inv[i * LD + q] * b[i * w + col];
+        xRows[e] = sum;
+    }
 }
 
 // After step t's block is solved, its terms leave the rows above it: x_F[q] -= sum_{i in block} L(i, q) x_F[i] for

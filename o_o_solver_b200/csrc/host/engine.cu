@@ -121,6 +121,12 @@ public:
             check(cudaFuncSetAttribute(device::smallFronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(m_smallSmem)),
                   "smallFronts shared memory");
+        // The diagonal steps of the solves: the block's inverse and the rows of a 64-column tile.
+        for (const void* kernel : {reinterpret_cast<const void*>(device::forwardDiagonal),
+                                   reinterpret_cast<const void*>(device::backwardDiagonal)})
+            check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(device::diagonalSolveSmem(SOLVE_WIDTH))),
+                  "diagonal solve shared memory");
         check(cudaStreamSynchronize(m_stream), "plan upload");
     }
 
@@ -228,6 +234,7 @@ public:
         m_pivoted = false;
         m_singular = false;
         runFactorLaunches(args);
+        invertDiagonalBlocks(args);
         const unsigned summaryBlocks = blocksFor(std::max(dimension, 1), 256);
         device::pivotSummary<<<summaryBlocks, 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), dimension,
                                                                    referenceDiagonal, maxRatio, m_counters.get(),
@@ -369,6 +376,7 @@ public:
         check(cudaMemsetAsync(m_status.get(), 0, count * sizeof(std::int32_t), m_stream), "memset");
         check(cudaMemsetAsync(m_stepSwapped.get(), 0, count * sizeof(std::int32_t), m_stream), "memset");
         std::vector<std::int32_t> status(count);
+        m_forcedPivots = 0;
         for (const Launch& launch : m_plan.pivotedLaunches)
         {
             const std::int32_t* list = m_lists.get() + launch.offset;
@@ -413,6 +421,8 @@ public:
                         throw delayedPivot(s, flags);
                     if ((flags & 1) != 0)
                         exactFront(args, pivots, s);
+                    else if ((flags & 4) != 0)
+                        m_forcedPivots += flags >> 8;
                 }
                 break;
             }
@@ -421,6 +431,7 @@ public:
             }
         }
         check(cudaGetLastError(), "indefinite factorisation launch");
+        invertDiagonalBlocks(args);
         device::inertiaPivoted<<<blocksFor(std::max(dimension, 1), 256), 256, 0, m_stream>>>(
             args, pivots, m_supernodeOfColumn.get(), dimension, m_counters.get());
         device::invertPermutation<<<blocksFor(std::max(dimension, 1), 256), 256, 0, m_stream>>>(
@@ -451,6 +462,7 @@ public:
         result.negative = static_cast<std::int64_t>(counters[1]);
         result.zero = static_cast<std::int64_t>(counters[2]);
         result.two_by_two = static_cast<std::int64_t>(counters[3]);
+        result.forced = m_forcedPivots;
         result.equation_of_largest = -1;
         result.device_seconds = milliseconds / 1000.0;
         if (info != nullptr)
@@ -458,6 +470,14 @@ public:
         m_pivoted = true;
         m_singular = result.zero > 0;
         m_factorised = true;
+    }
+
+    // The inverses of the diagonal blocks the solves' 64-column steps apply (into the blocks' upper triangles).
+    void invertDiagonalBlocks(const device::FactorArgs& args)
+    {
+        for (const Launch& launch : m_plan.inverseLaunches)
+            device::invertDiagonal<<<launch.count, 64, 0, m_stream>>>(args, m_tiles.get() + launch.offset);
+        check(cudaGetLastError(), "diagonal inverse launch");
     }
 
     [[nodiscard]] Error delayedPivot(std::int32_t s, std::int32_t flags) const
@@ -487,6 +507,8 @@ public:
         ++m_exactFronts;
         if ((flags & 2) != 0)
             throw delayedPivot(s, flags);
+        if ((flags & 4) != 0)
+            m_forcedPivots += flags >> 8;
     }
 
     void requireSolvable() const
@@ -813,9 +835,14 @@ public:
         *eliminated = f.c;
         *rowCount = n;
         if (values != nullptr)
+        {
             check(cudaMemcpy(values, m_panels.get() + f.panel, static_cast<std::size_t>(n * f.c) * sizeof(double),
                              cudaMemcpyDeviceToHost),
                   "download panel");
+            // The strict upper triangle holds the solves' diagonal inverses, not the factor.
+            for (std::int64_t j = 0; j < f.c; ++j)
+                std::fill_n(values + j * n, j, 0.0);
+        }
         if (rows != nullptr)
         {
             for (std::int32_t k = 0; k < f.c; ++k)
@@ -978,7 +1005,8 @@ private:
                 device::forwardGather<<<launch.count, 256, 0, m_stream>>>(args, tiles);
                 break;
             case LaunchKind::ForwardDiagonal:
-                device::forwardDiagonal<<<launch.count, 64, 0, m_stream>>>(args, list, launch.k0);
+                device::forwardDiagonal<<<launch.count, 256, device::diagonalSolveSmem(args.width), m_stream>>>(
+                    args, list, launch.k0);
                 break;
             case LaunchKind::ForwardUpdate:
                 device::forwardUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles, launch.k0);
@@ -990,7 +1018,8 @@ private:
                 device::backwardRows<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles);
                 break;
             case LaunchKind::BackwardDiagonal:
-                device::backwardDiagonal<<<launch.count, 64, 0, m_stream>>>(args, list, launch.k0);
+                device::backwardDiagonal<<<launch.count, 256, device::diagonalSolveSmem(args.width), m_stream>>>(
+                    args, list, launch.k0);
                 break;
             case LaunchKind::BackwardUpdate:
                 device::backwardUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles, launch.k0);
@@ -1035,6 +1064,7 @@ private:
     DeviceArray<std::int32_t> m_inversePerm;
     DeviceArray<double> m_subdiagonal;
     DeviceArray<std::int32_t> m_status;
+    std::int64_t m_forcedPivots = 0;
     DeviceArray<std::int32_t> m_stepPerm;
     DeviceArray<std::int32_t> m_stepSwapped;
     DeviceArray<double> m_w;
@@ -1822,7 +1852,7 @@ extern "C" int oosgpu_modes_solve(oosgpu_pencil* pencil, const oosgpu_eigen_requ
         });
 }
 
-extern "C" int oosgpu_modes_summary(const oosgpu_modes* modes, int64_t counts[6], double seconds[2])
+extern "C" int oosgpu_modes_summary(const oosgpu_modes* modes, int64_t counts[6], double seconds[6])
 {
     return guarded(
         [&]
@@ -1842,6 +1872,10 @@ extern "C" int oosgpu_modes_summary(const oosgpu_modes* modes, int64_t counts[6]
             {
                 seconds[0] = s.seconds;
                 seconds[1] = s.factorSeconds;
+                seconds[2] = s.factorWallSeconds;
+                seconds[3] = s.operatorSeconds;
+                seconds[4] = s.orthogonalisationSeconds;
+                seconds[5] = s.projectedSeconds;
             }
         });
 }

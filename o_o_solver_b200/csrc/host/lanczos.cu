@@ -112,6 +112,22 @@ double hypotenuse(double a, double b)
     return big * std::sqrt(1.0 + small * small);
 }
 
+// Wall seconds of the phases of the runs; each timed phase ends with its stream drained.
+struct Phases
+{
+    double operatorSeconds = 0.0;
+    double orthogonalisationSeconds = 0.0;
+    double projectedSeconds = 0.0;
+};
+
+template <typename Body> void timed(double& counter, cudaStream_t stream, Body&& body)
+{
+    const auto start = std::chrono::steady_clock::now();
+    body();
+    check(cudaStreamSynchronize(stream), "Lanczos");
+    counter += std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+}
+
 // The block operations over the rows of the pencil's dimension, on one stream.
 class BlockOps
 {
@@ -354,8 +370,8 @@ struct RunResult
 class Run
 {
 public:
-    Run(ShiftedPencil& pencil, BlockOps& ops, Workspace& workspace, const RunSettings& settings)
-        : m_pencil(pencil), m_ops(ops), m_ws(workspace), m_settings(settings),
+    Run(ShiftedPencil& pencil, BlockOps& ops, Workspace& workspace, const RunSettings& settings, Phases& phases)
+        : m_pencil(pencil), m_ops(ops), m_ws(workspace), m_settings(settings), m_phases(phases),
           m_n(static_cast<std::size_t>(pencil.dimension())), m_capacity(settings.basisColumns)
     {
     }
@@ -370,6 +386,7 @@ public:
         m_coupling.assign(b * ld, 0.0);
         m_columns = 0;
         m_operatorNorm = 0.0;
+        const cudaStream_t stream = m_ops.stream();
         startBlock(store);
         if (m_nextColumnCount == 0)
         {
@@ -388,7 +405,7 @@ public:
             {
                 if (result.restarts >= m_settings.maximumRestarts || m_capacity < 3 * b)
                     break;
-                restart(ritz);
+                timed(m_phases.orthogonalisationSeconds, stream, [&] { restart(ritz); });
                 ++result.restarts;
             }
             const std::size_t p = m_columns;
@@ -404,9 +421,13 @@ public:
 
             double* w = m_ws.product.get();
             m_ops.copy(w, n, basis + n * static_cast<std::int64_t>(p), n, b);
-            applyOperator(w, b);
-            projectOut(w, b, store, p + b, &coefficients, norms.data());
-            projectOut(w, b, store, p + b, &secondCoefficients, nullptr);
+            timed(m_phases.operatorSeconds, stream, [&] { applyOperator(w, b); });
+            timed(m_phases.orthogonalisationSeconds, stream,
+                  [&]
+                  {
+                      projectOut(w, b, store, p + b, &coefficients, norms.data());
+                      projectOut(w, b, store, p + b, &secondCoefficients, nullptr);
+                  });
             for (const double norm : norms)
                 m_operatorNorm = std::max(m_operatorNorm, norm);
             const std::size_t rows = p + b;
@@ -420,7 +441,8 @@ public:
                     m_projected[(p + c) + (p + r) * ld] = value;
                 }
             m_referenceNorms.assign(b, m_operatorNorm);
-            m_nextColumnCount = factoriseBlock(w, b, &triangle, store);
+            timed(m_phases.orthogonalisationSeconds, stream,
+                  [&] { m_nextColumnCount = factoriseBlock(w, b, &triangle, store); });
             std::swap(m_ws.next, m_ws.product);
             std::fill(m_coupling.begin(), m_coupling.end(), 0.0);
             for (std::size_t c = 0; c < b; ++c)
@@ -429,11 +451,11 @@ public:
             m_columns = p + b;
             ++result.blockSteps;
 
-            ritz = computeRitzPairs();
+            timed(m_phases.projectedSeconds, stream, [&] { ritz = computeRitzPairs(); });
             if (hasConvergedTarget(ritz) || m_nextColumnCount == 0)
                 break;
         }
-        extractConverged(ritz, shift, store, result);
+        timed(m_phases.orthogonalisationSeconds, stream, [&] { extractConverged(ritz, shift, store, result); });
         return result;
     }
 
@@ -582,14 +604,23 @@ private:
         const auto n = static_cast<std::int64_t>(m_n);
         const std::size_t b = m_settings.blockSize;
         double* next = m_ws.next.get();
-        m_ops.random(next, n, b, m_randomState);
+        const cudaStream_t stream = m_ops.stream();
         // Op applied once puts the block in the range of Op, which excludes the null space of M.
-        applyOperator(next, b);
+        timed(m_phases.operatorSeconds, stream,
+              [&]
+              {
+                  m_ops.random(next, n, b, m_randomState);
+                  applyOperator(next, b);
+              });
         m_referenceNorms.assign(b, 0.0);
-        for (int pass = 0; pass < ORTHOGONALISATION_PASSES; ++pass)
-            projectOut(next, b, store, 0, nullptr, pass == 0 ? m_referenceNorms.data() : nullptr);
         m_basisInUse = 0;
-        m_nextColumnCount = factoriseBlock(next, b, nullptr, store);
+        timed(m_phases.orthogonalisationSeconds, stream,
+              [&]
+              {
+                  for (int pass = 0; pass < ORTHOGONALISATION_PASSES; ++pass)
+                      projectOut(next, b, store, 0, nullptr, pass == 0 ? m_referenceNorms.data() : nullptr);
+                  m_nextColumnCount = factoriseBlock(next, b, nullptr, store);
+              });
     }
 
     // After a start block that deflated whole: P Op P R off the locked set; true when a direction is left, with the
@@ -808,6 +839,7 @@ private:
     BlockOps& m_ops;
     Workspace& m_ws;
     RunSettings m_settings;
+    Phases& m_phases;
     std::size_t m_n;
     std::size_t m_capacity;
     std::vector<double> m_projected;
@@ -1286,12 +1318,14 @@ EigenSolution solveModes(ShiftedPencil& pencil, const EigenRequest& request, con
                 (request.modeCount > 0 ? std::min(request.modeCount, dimension) : 0) + shape.basisColumns);
 
     SturmCheck sturm;
+    Phases phases;
     const auto factoriseAt = [&](double shift, ShiftPurpose purpose, bool isUpward)
     {
         double trial = shift;
         for (std::size_t attempt = 0; attempt <= MAX_SINGULAR_MOVES; ++attempt)
         {
-            const Inertia inertia = pencil.factorise(trial);
+            Inertia inertia;
+            timed(solution.factorWallSeconds, pencil.stream(), [&] { inertia = pencil.factorise(trial); });
             ++solution.factorisationCount;
             solution.factorSeconds += pencil.lastFactorSeconds();
             if (inertia.zero == 0)
@@ -1360,7 +1394,7 @@ EigenSolution solveModes(ShiftedPencil& pencil, const EigenRequest& request, con
         settings.convergenceTolerance = options.convergenceTolerance;
         settings.maximumRestarts = options.maximumRestarts;
         settings.seed = options.seed + SEED_STEP * (runIndex + 1);
-        Run run(pencil, ops, *workspace, settings);
+        Run run(pencil, ops, *workspace, settings, phases);
         const RunResult result = run.run(current, store);
         solution.blockSteps += result.blockSteps;
         for (auto record = solution.shifts.rbegin(); record != solution.shifts.rend(); ++record)
@@ -1416,6 +1450,9 @@ EigenSolution solveModes(ShiftedPencil& pencil, const EigenRequest& request, con
         std::count_if(solution.eigenvalues.begin(), solution.eigenvalues.end(),
                       [&](double value) { return isComplete || value < verification.verifiedUpTo; }));
     solution.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count();
+    solution.operatorSeconds = phases.operatorSeconds;
+    solution.orthogonalisationSeconds = phases.orthogonalisationSeconds;
+    solution.projectedSeconds = phases.projectedSeconds;
     return solution;
 }
 

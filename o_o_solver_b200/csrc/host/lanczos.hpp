@@ -105,6 +105,12 @@ struct EigenSolution
     // Wall seconds of the solve, and the device seconds of its factorisations.
     double seconds = 0.0;
     double factorSeconds = 0.0;
+    // Wall seconds of the factorisations (with their host work), of the operator Op = (K - sigma M)^-1 M (the solves
+    // and the mass products), of the M-orthogonalisation, and of the projected problem (host).
+    double factorWallSeconds = 0.0;
+    double operatorSeconds = 0.0;
+    double orthogonalisationSeconds = 0.0;
+    double projectedSeconds = 0.0;
     std::size_t blockSteps = 0;
 };
 

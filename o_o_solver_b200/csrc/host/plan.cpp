@@ -276,6 +276,7 @@ Plan buildPlan(const Symbolic& symbolic)
         byLevel[static_cast<std::size_t>(plan.level[static_cast<std::size_t>(s)])].push_back(s);
 
     std::vector<std::vector<Launch>> backwardByLevel(static_cast<std::size_t>(plan.levelCount));
+    std::vector<TileTask> inverseTasks;
     for (std::int32_t level = 0; level < plan.levelCount; ++level)
     {
         const auto& members = byLevel[static_cast<std::size_t>(level)];
@@ -461,6 +462,9 @@ Plan buildPlan(const Symbolic& symbolic)
             }
             addTiles(plan, plan.forwardLaunches, LaunchKind::ForwardGather, ranges);
         }
+        for (const std::int32_t s : solveLarge)
+            for (std::int32_t k0 = 0; k0 < plan.fronts[static_cast<std::size_t>(s)].c; k0 += BLOCK)
+                inverseTasks.push_back({s, k0, 0, 0});
         for (std::int32_t k0 = 0; k0 < maxColumns; k0 += BLOCK)
         {
             std::vector<std::int32_t> diagonal;
@@ -518,6 +522,7 @@ Plan buildPlan(const Symbolic& symbolic)
         const auto& launches = backwardByLevel[static_cast<std::size_t>(level)];
         plan.backwardLaunches.insert(plan.backwardLaunches.end(), launches.begin(), launches.end());
     }
+    addTiles(plan, plan.inverseLaunches, LaunchKind::InvertDiagonal, inverseTasks);
     return plan;
 }
 

@@ -44,7 +44,9 @@ enum class LaunchKind : int
     PermuteEarlierRows,
     PanelRowsPivoted,
     UpdatePivoted,
-    LevelEnd // the host checks the level's fronts (k0: the level) and runs the exact path where needed
+    LevelEnd, // the host checks the level's fronts (k0: the level) and runs the exact path where needed
+    // after a factorisation: the inverses of the unit lower diagonal blocks the solves apply
+    InvertDiagonal
 };
 
 // One batched launch: `count` items from `offset` in the array of its kind (front lists: int32; tiles: TileTask;
@@ -89,6 +91,9 @@ struct Plan
     std::vector<Launch> factorLaunches;
     std::vector<Launch> forwardLaunches;
     std::vector<Launch> backwardLaunches;
+    // The diagonal blocks (front, k0) of the supernodes the solves take by 64-column steps, inverted after each
+    // factorisation into the blocks' upper triangles.
+    std::vector<Launch> inverseLaunches;
 
     // Indefinite mode: the launches (assembly shared with the positive definite sequence), the large fronts of each
     // level, and each large front's W buffer (n x 64 values at wOffset; the fronts of one level apart, the levels

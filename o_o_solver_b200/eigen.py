@@ -85,6 +85,7 @@ class EigenSolution:
     block_steps: int = 0
     seconds: float = 0.0
     factor_seconds: float = 0.0
+    phases: dict = field(default_factory=dict)
 
 
 class BlockLanczos:
@@ -103,7 +104,7 @@ class BlockLanczos:
                                       ctypes.byref(handle)))
         try:
             counts = np.zeros(6, dtype=np.int64)
-            seconds = np.zeros(2)
+            seconds = np.zeros(6)
             _check(lib.oosgpu_modes_summary(handle, nat.ptr(counts, nat.i64p), nat.ptr(seconds, nat.f64p)))
             k = int(counts[0])
             values = np.zeros(max(k, 1))
@@ -118,7 +119,9 @@ class BlockLanczos:
             _check(lib.oosgpu_modes_shifts(handle, nat.ptr(records, nat.f64p)))
             shifts = [ShiftRecord(float(r[0]), PURPOSES[int(r[1])], int(r[2]), bool(r[3]), int(r[4]), int(r[5]),
                                   int(r[6])) for r in records[: int(counts[2])]]
+            phases = {"factorisation": float(seconds[2]), "operator": float(seconds[3]),
+                      "orthogonalisation": float(seconds[4]), "projected": float(seconds[5])}
             return EigenSolution(values[:k], phi, bounds[:k], shifts, int(counts[1]), int(counts[3]),
-                                 bool(counts[4]), int(counts[5]), float(seconds[0]), float(seconds[1]))
+                                 bool(counts[4]), int(counts[5]), float(seconds[0]), float(seconds[1]), phases)
         finally:
             lib.oosgpu_modes_destroy(handle)

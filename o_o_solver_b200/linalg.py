@@ -242,6 +242,7 @@ class SupernodalFactor:
         self.zero_pivots = list(info.zero_pivots[: min(16, int(info.zero_pivot_count))])
         self.delayed_pivot_count = int(info.delayed)
         self.two_by_two_pivot_count = int(info.two_by_two)
+        self.forced_pivot_count = int(info.forced)
         self.is_singular = self.inertia.zero > 0
         self.device_seconds = float(info.device_seconds)
 
@@ -393,6 +394,7 @@ class ShiftFactorisation:
     shift: float
     inertia: Inertia
     two_by_two: int = 0
+    forced: int = 0
 
     @property
     def sturm_count(self) -> int:
@@ -456,7 +458,7 @@ class SparsePencil:
         info = nat.FactorInfo()
         _check(nat.load().oosgpu_pencil_factorise(self._handle, float(shift), ctypes.byref(info)))
         return ShiftFactorisation(float(shift), Inertia(int(info.positive), int(info.negative), int(info.zero)),
-                                  int(info.two_by_two))
+                                  int(info.two_by_two), int(info.forced))
 
     def _device_call(self, fn, *blocks):
         """Runs fn on device blocks; host blocks are copied to the device and the last one back."""
