@@ -12,6 +12,11 @@ solve + refinement), seconds; `e2e` the same step through the C ABI with host bu
 `roofline` the dominant kernel of a profiled factorisation against the measured peak; `cpu_baseline` the reference's
 own factorisation and solve (oracle/_ref, built from its sources) on the host cores, on the same matrix.
 `--impl reference` times that CPU path alone on the same workload.
+
+The line's `modes` object is the other half of the metric: the lowest 20 modes of the 60^3 hexahedral block
+(669,780 equations) by the GPU block shift-invert Lanczos (block 8), wall seconds of the whole solve (factorisations,
+Lanczos runs, Sturm checks), its eigenvalues against the reference's recorded ones (tests/golden/modes), its e2e
+through the public API from host arrays, and the reference beside it on the 30^3 block (a bounded CPU sample).
 """
 
 from __future__ import annotations
@@ -48,6 +53,9 @@ def parse():
     parser.add_argument("--tolerance", type=float, default=1.0e-10)
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-e2e", action="store_true")
+    parser.add_argument("--modes-workload", choices=["hex60", "hex30", "hex14", "none"], default="hex60",
+                        help="the modes leg: the lowest 20 modes of the n^3 hexahedral block, block size 8")
+    parser.add_argument("--modes-steps", type=int, default=2)
     return parser.parse_args()
 
 
@@ -169,6 +177,113 @@ def cpu_baseline(fixture, csc, loads, threads, tolerance):
     resid, backward = accuracy(csc, x, loads)
     return {"seconds": seconds, "factor_seconds": factor.seconds, "residual": resid, "backward_error": backward,
             "kernel": ["reference", "avx2", "avx512"][factor.kernel] if factor.kernel < 3 else str(factor.kernel)}
+
+
+def load_modes_workload(name):
+    """The hexahedral block, the reference's ordering and partition (tests/golden/orderings), K and the lumped M."""
+    from o_o_solver_b200 import workloads
+
+    size = int(name[3:])
+    fixture = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    model = workloads.Model(workloads.HexSpec(size))
+    order = fixture["node_order"]
+    return model, fixture, model.csc(order, 0), model.csc(order, 1)
+
+
+def reference_modes(name, threads):
+    """The reference's SparsePencil + BlockLanczos::solve (oracle/_ref) of the same pencil: (seconds, eigenvalues)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    model, fixture, k, m = load_modes_workload(name)
+    sym = oracle.analyse(model.offsets, model.neighbours, model.weights, given_order=fixture["node_order"],
+                         threads=threads)
+    result = oracle.modes(sym, k.offsets, k.rows, k.values, m.values, MODES, block_size=MODES_BLOCK, threads=threads,
+                          vectors=False)
+    return result["seconds"], result["eigenvalues"], result["factorisations"]
+
+
+MODES = 20
+MODES_BLOCK = 8
+
+
+def gpu_modes(name, device, steps, warmup=1, e2e=False):
+    """The lowest 20 modes on the GPU (SparsePencil + BlockLanczos, block 8): the median wall seconds of `steps`
+    solves after `warmup`, the last solution, and with e2e the wall seconds of the public API from host arrays
+    (the pencil built from the host CSC, the eigenvectors copied back)."""
+    from o_o_solver_b200 import SparsePencil, SymbolicFactor
+    from o_o_solver_b200.eigen import BlockLanczos, EigenRequest, LanczosOptions
+
+    model, fixture, k, m = load_modes_workload(name)
+    symbolic = SymbolicFactor.from_partition(model.offsets, model.neighbours, model.weights, fixture["node_order"],
+                                             fixture["first_position"], fixture["parent"])
+    pencil = SparsePencil(symbolic, k, m, device=device)
+    solver = BlockLanczos(LanczosOptions(block_size=MODES_BLOCK))
+    request = EigenRequest(mode_count=MODES)
+    times = []
+    solution = None
+    for step in range(warmup + steps):
+        solution = solver.solve(pencil, request, vectors=False)
+        if step >= warmup:
+            times.append(solution.seconds)
+    result = {"seconds": statistics.median(times), "solution": solution, "symbolic": symbolic, "dimension": k.dimension}
+    if e2e:
+        pencil.close()
+        t0 = time.perf_counter()
+        fresh = SparsePencil(symbolic, k, m, device=device)
+        full = solver.solve(fresh, request, vectors=True)
+        result["e2e"] = time.perf_counter() - t0
+        result["h2d"] = int(k.offsets.nbytes + k.rows.nbytes + k.values.nbytes + m.values.nbytes)
+        result["d2h"] = int(full.eigenvectors.nbytes + full.eigenvalues.nbytes)
+        fresh.close()
+    return result
+
+
+def modes_leg(args, device, rank, world):
+    """The modes half of the metric: GPU time of the lowest 20 modes of the workload, its accuracy against the
+    reference's recorded eigenvalues (tests/golden/modes), the phases of the solve, and on one GPU the reference
+    beside it on a bounded sample (the 30^3 block, seconds on the host cores)."""
+    name = args.modes_workload
+    run = gpu_modes(name, device, args.modes_steps, e2e=not args.no_e2e)
+    solution = run["solution"]
+    out = {"workload": f"{name}: {name[3:]}^3 trilinear hexahedra, base clamped, steel, lumped mass, "
+                       f"{run['dimension']} equations; lowest {MODES} modes, block {MODES_BLOCK}",
+           "value": run["seconds"], "unit": "s", "factorisations": solution.factorisation_count,
+           "block_steps": solution.block_steps, "complete": solution.is_complete,
+           "verified": solution.verified_count, "phases_s": {k: round(v, 4) for k, v in solution.phases.items()},
+           "factor_device_s": round(solution.factor_seconds, 4)}
+    golden = os.path.join(ROOT, "tests", "golden", "modes", f"{name}.npz")
+    if os.path.exists(golden):
+        expected = np.load(golden)["eigenvalues"]
+        out["eigenvalue_max_rel_error_vs_reference"] = float(
+            np.max(np.abs(solution.eigenvalues - expected) / np.abs(expected)))
+        out["reference_recorded_s"] = float(np.load(golden)["seconds"])
+        out["reference_recorded_threads"] = int(np.load(golden)["threads"])
+    # Operator roofline: the solves read the factor twice (forward, backward) per block step.
+    entries = run["symbolic"].factor_entry_count
+    solves = solution.block_steps + sum(1 for r in solution.shifts if r.has_lanczos_run)
+    if solution.phases.get("operator", 0.0) > 0.0 and solves > 0:
+        bytes_per_solve = 2.0 * 8.0 * entries + 3.0 * 8.0 * run["dimension"] * MODES_BLOCK * 2
+        out["operator_gbs"] = round(bytes_per_solve * solves / solution.phases["operator"] / 1e9, 1)
+    if "e2e" in run:
+        out["e2e"] = {"value": run["e2e"], "unit": "s", "h2d_bytes_per_step": run["h2d"],
+                      "d2h_bytes_per_step": run["d2h"]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample = "hex30"
+        try:
+            threads = os.cpu_count() or 1
+            ref_seconds, ref_values, ref_factorisations = reference_modes(sample, threads)
+            gpu_sample = gpu_modes(sample, device, 1)
+            out["cpu_baseline"] = {
+                "value": ref_seconds, "unit": "s", "cores": threads, "kind": "reference",
+                "sample": f"the same request on the 30^3 block (86,490 equations): reference "
+                          f"{ref_seconds:.2f} s ({ref_factorisations} factorisations), GPU {gpu_sample['seconds']:.3f} s "
+                          f"on that sample, eigenvalues agree to "
+                          f"{float(np.max(np.abs(gpu_sample['solution'].eigenvalues - ref_values) / ref_values)):.1e}"}
+        except Exception as error:  # the reference library is test infrastructure: absent, no baseline
+            out["cpu_baseline"] = {"value": None, "unit": "s", "cores": 0, "kind": "reference",
+                                   "sample": f"unavailable: {error}"}
+    return out
 
 
 def run_reference(args, rank, world):
@@ -330,6 +445,8 @@ def run_gpu(args, rank, world, local_rank):
         except Exception as error:  # the reference library is test infrastructure: absent, no baseline
             baseline = {"value": None, "unit": "s", "cores": 0, "kind": "reference", "sample": f"unavailable: {error}"}
 
+    modes = modes_leg(args, local_rank, rank, world) if args.modes_workload != "none" else None
+
     if rank == 0:
         line = {
             "metric": "plate statics factor+solve time (2M-dof, 64 RHS)" if args.workload == "plate580" else
@@ -342,7 +459,7 @@ def run_gpu(args, rank, world, local_rank):
                        "parallelism": f"replicas x{world}"},
             "residual": resid, "backward_error": backward, "refinement": refinement, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "kernels": kernel_table, "clocks": clocks.summary(), "cpu_baseline": baseline,
-            "factor_tflops": symbolic.flop_count / seconds / 1e12,
+            "factor_tflops": symbolic.flop_count / seconds / 1e12, "modes": modes,
         }
         print(json.dumps(line), flush=True)
     if dist:

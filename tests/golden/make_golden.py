@@ -9,7 +9,11 @@ Writes, for each workload of the benchmark and the tests:
                          reference computes, reused as it is by the GPU path (the row structures follow from them);
   solutions/<name>.npz   for small cases: the reference's inertia, pivot diagnostics and solutions of seeded
                          right-hand sides (the known answers the GPU path is checked against on the GPU box, where the
-                         reference is not built).
+                         reference is not built);
+  modes/<name>.npz       the reference's lowest modes of a pencil (SparsePencil + BlockLanczos::solve, block 8): the
+                         eigenvalues, the shifts with their Sturm counts, the factorisations.
+
+    python tests/golden/make_golden.py [--modes-only] [--with-large-modes]
 """
 
 from __future__ import annotations
@@ -38,6 +42,44 @@ ORDERINGS = {
     "hex60": ("hex", 60),
 }
 SOLUTIONS = ["plate6", "plate20", "hex4", "hex8"]
+# name: (modes, block size); the large ones (minutes on a few cores) only with --with-large-modes.
+MODES = {"hex8": (20, 8), "hex14": (20, 8), "plate20": (12, 7), "hex30": (20, 8)}
+LARGE_MODES = {"hex60": (20, 8)}
+
+
+def pencil_of(kind, model, sym):
+    """K and M in the reference's order: the hex's lumped mass, or for a plate the translations of a 2 mm aluminium
+    sheet without rotary inertia (a mass with a null space)."""
+    from o_o_solver_b200 import SymmetricCsc
+
+    k = model.csc(sym.node_order, 0)
+    if kind == "hex":
+        return k, model.csc(sym.node_order, 1)
+    size = model.spec.nx
+    values = np.zeros_like(k.values)
+    mass = np.zeros(sym.dof_count)
+    mass[np.arange(sym.dof_count) % 6 < 3] = 2700.0 * 0.002 / (size * size)
+    values[k.offsets[:-1]] = mass
+    return k, SymmetricCsc(k.offsets, k.rows, values)
+
+
+def make_modes(names, threads):
+    import oracle
+
+    os.makedirs(os.path.join(HERE, "modes"), exist_ok=True)
+    for name, (count, block) in names.items():
+        kind, size = ORDERINGS[name]
+        model = model_of(kind, size)
+        sym = oracle.analyse(model.offsets, model.neighbours, model.weights, model.coordinates, threads=threads)
+        k, m = pencil_of(kind, model, sym)
+        result = oracle.modes(sym, k.offsets, k.rows, k.values, m.values, count, block_size=block, threads=threads,
+                              vectors=False)
+        np.savez_compressed(os.path.join(HERE, "modes", name + ".npz"), eigenvalues=result["eigenvalues"],
+                            shifts=result["shifts"], factorisations=np.array(result["factorisations"]),
+                            verified=np.array(result["verified"]), block_size=np.array(block),
+                            seconds=np.array(result["seconds"]), threads=np.array(threads))
+        print(f"{name}: {count} modes in {result['seconds']:.1f} s on {threads} threads, "
+              f"{result['factorisations']} factorisations, lowest {result['eigenvalues'][0]:.6e}")
 
 
 def model_of(kind, size):
@@ -49,9 +91,19 @@ def model_of(kind, size):
 def main():
     import oracle
 
+    threads = os.cpu_count() or 1
+    if "--modes-only" not in sys.argv:
+        make_orderings(threads)
+    make_modes(MODES, threads)
+    if "--with-large-modes" in sys.argv:
+        make_modes(LARGE_MODES, threads)
+
+
+def make_orderings(threads):
+    import oracle
+
     os.makedirs(os.path.join(HERE, "orderings"), exist_ok=True)
     os.makedirs(os.path.join(HERE, "solutions"), exist_ok=True)
-    threads = os.cpu_count() or 1
     for name, (kind, size) in ORDERINGS.items():
         model = model_of(kind, size)
         sym = oracle.analyse(model.offsets, model.neighbours, model.weights, model.coordinates, threads=threads)

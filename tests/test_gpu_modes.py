@@ -4,6 +4,7 @@ reference's inertia of that shift, the request verified and complete, the eigenv
 residuals, and the refusals of the reference for requests and settings out of range."""
 
 import math
+import os
 
 import numpy as np
 import pytest
@@ -172,3 +173,45 @@ def test_refusals(lib, oracle_mod, gpu):
     solution = BlockLanczos(LanczosOptions(block_size=4)).solve(pencil, EigenRequest(mode_count=3))
     assert solution.is_complete and len(solution.eigenvalues) == 3
     assert math.isfinite(solution.eigenvalues[0])
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.mark.parametrize("name", ["hex8", "hex14", "plate20", "hex30"])
+def test_modes_match_golden(name, lib, gpu):
+    """Against the reference's own solve recorded in tests/golden/modes (no reference library needed): the symbolic
+    structure from the reference's ordering, the eigenvalues within 1e-9, the same Sturm count at every shift the
+    reference made, the same factorisations."""
+    from o_o_solver_b200 import SparsePencil, SymbolicFactor, SymmetricCsc, workloads
+    from o_o_solver_b200.eigen import BlockLanczos, EigenRequest, LanczosOptions
+
+    golden = np.load(os.path.join(GOLDEN, "modes", name + ".npz"))
+    order = np.load(os.path.join(GOLDEN, "orderings", name + ".npz"))
+    kind, size = ("plate", int(name[5:])) if name.startswith("plate") else ("hex", int(name[3:]))
+    model = workloads.Model(workloads.PlateSpec(size, size) if kind == "plate" else workloads.HexSpec(size))
+    symbolic = SymbolicFactor.from_partition(model.offsets, model.neighbours, model.weights, order["node_order"],
+                                             order["first_position"], order["parent"])
+    k = model.csc(order["node_order"], 0)
+    if kind == "hex":
+        m = model.csc(order["node_order"], 1)
+    else:
+        values = np.zeros_like(k.values)
+        mass = np.zeros(k.dimension)
+        mass[np.arange(k.dimension) % 6 < 3] = 2700.0 * 0.002 / (size * size)
+        values[k.offsets[:-1]] = mass
+        m = SymmetricCsc(k.offsets, k.rows, values)
+    pencil = SparsePencil(symbolic, k, m)
+    expected = golden["eigenvalues"]
+    solution = BlockLanczos(LanczosOptions(block_size=int(golden["block_size"]))).solve(
+        pencil, EigenRequest(mode_count=len(expected)))
+    assert solution.is_complete and solution.verified_count == len(expected)
+    relative = np.abs(solution.eigenvalues - expected) / np.abs(expected)
+    assert relative.max() <= EIGENVALUE_TOLERANCE, relative
+    reference_counts = {float(row[0]): int(row[2]) for row in golden["shifts"]}
+    for record in solution.shifts:
+        if record.shift in reference_counts:
+            assert record.sturm_count == reference_counts[record.shift], record
+    assert solution.factorisation_count == int(golden["factorisations"])
+    residual, gram = pair_residuals(k, m, solution.eigenvalues, solution.eigenvectors)
+    assert np.abs(gram - np.eye(len(expected))).max() <= 1e-10
