@@ -44,7 +44,6 @@ struct AssemblyTask
 };
 
 constexpr int TILE = 64;
-constexpr int TILE_K = 16;
 constexpr int TILE_PAD = 8; // smem row stride 72 doubles: the m8n8k4 fragment loads take 2 wavefronts (no conflict)
 constexpr int TILE_THREADS = 128;
 
@@ -88,21 +87,47 @@ struct TileOperands
     int lowerOffset;
 };
 
-// One 64 x 64 tile on a block of TILE_THREADS threads (4 warps of 32 x 32). The K loop stages TILE_K-deep slices of A
-// and of W = B * D in shared memory (register double buffering: the next slice is loaded while the current one is
-// multiplied), the products run on the FP64 tensor cores (DMMA m8n8k4), and C is read, reduced and written once.
-// smemA/smemB: TILE_K * (TILE + TILE_PAD) doubles each. A_BY_ROWS: A's rows are contiguous in memory (aColStride 1),
-// so the loads of A run along p (16 consecutive doubles per row) instead of along the rows.
+// The K pipeline of tileProduct: TILE_STAGES slices of TILE_SLICE columns of K in flight, each slice holding A and B
+// (TILE_SLICE rows of TILE + TILE_PAD doubles) and the slice's d values.
+constexpr int TILE_SLICE = 8;
+constexpr int TILE_STAGES = 4;
+constexpr int TILE_STAGE_DOUBLES = 2 * TILE_SLICE * (TILE + TILE_PAD) + TILE_SLICE;
+constexpr int TILE_SMEM_DOUBLES = TILE_STAGES * TILE_STAGE_DOUBLES; // 37,120 bytes
+
+// An 8-byte asynchronous copy global -> shared; zero-filled (nothing read) when `valid` is false.
+__device__ __forceinline__ void copyAsync8(double* sharedDst, const double* globalSrc, bool valid)
+{
+    const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(sharedDst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(globalSrc), "r"(valid ? 8 : 0)
+                 : "memory");
+}
+
+__device__ __forceinline__ void commitAsyncCopies()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+template <int PENDING> __device__ __forceinline__ void waitAsyncCopies()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
+}
+
+// One 64 x 64 tile on a block of TILE_THREADS threads (4 warps of 32 x 32). The K loop streams slices of A and B
+// (TILE_SLICE deep) and of d into shared memory by asynchronous copies, TILE_STAGES slices in flight, so the loads of
+// later slices overlap the products of the current one; the products run on the FP64 tensor cores (DMMA m8n8k4), each
+// fragment of B multiplied by its d_p as it is read (W = B D, rounded once as before), and C is read, reduced and
+// written once. smem: TILE_SMEM_DOUBLES doubles. B's rows are contiguous in memory (bRowStride 1 in every caller);
+// A_BY_ROWS: A's rows are contiguous along p (aColStride 1), else along the rows (aRowStride 1).
 template <bool A_BY_ROWS = false>
-__device__ __forceinline__ void tileProduct(const TileOperands& op, double* smemA, double* smemB)
+__device__ __forceinline__ void tileProduct(const TileOperands& op, double* smem)
 {
     constexpr int LD = TILE + TILE_PAD;
-    constexpr int PER_THREAD = TILE * TILE_K / TILE_THREADS; // 8
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
     const int wm = (warp >> 1) * 32;
     const int wn = (warp & 1) * 32;
+    const bool scaled = op.d != nullptr;
 
     double acc[4][4][2];
 #pragma unroll
@@ -114,87 +139,83 @@ __device__ __forceinline__ void tileProduct(const TileOperands& op, double* smem
             acc[mi][ni][1] = 0.0;
         }
 
-    double ra[PER_THREAD];
-    double rb[PER_THREAD];
-    const auto load = [&](int kbase)
+    const int slices = (op.k + TILE_SLICE - 1) / TILE_SLICE;
+    const auto issue = [&](int slice)
     {
+        double* sA = smem + (slice % TILE_STAGES) * TILE_STAGE_DOUBLES;
+        double* sB = sA + TILE_SLICE * LD;
+        double* sD = sB + TILE_SLICE * LD;
+        const int kbase = slice * TILE_SLICE;
 #pragma unroll
-        for (int q = 0; q < PER_THREAD; ++q)
+        for (int q = 0; q < TILE * TILE_SLICE / TILE_THREADS; ++q)
         {
             const int e = tid + q * TILE_THREADS;
-            const int ii = e & (TILE - 1);
-            const int p = e >> 6;
-            const int kp = kbase + p;
-            const int iiA = A_BY_ROWS ? (e >> 4) : ii;
-            const int pA = A_BY_ROWS ? (e & (TILE_K - 1)) : p;
-            const int kpA = kbase + pA;
-            double va = 0.0;
-            double vb = 0.0;
-            if (kpA < op.k && iiA < op.m)
-                va = op.a[iiA * op.aRowStride + static_cast<std::int64_t>(kpA) * op.aColStride];
-            if (kp < op.k)
+            const int ii = A_BY_ROWS ? (e / TILE_SLICE) : (e & (TILE - 1));
+            const int pa = A_BY_ROWS ? (e & (TILE_SLICE - 1)) : (e / TILE);
+            const int kpa = kbase + pa;
+            const bool okA = kpa < op.k && ii < op.m;
+            copyAsync8(sA + pa * LD + ii,
+                       okA ? op.a + ii * op.aRowStride + static_cast<std::int64_t>(kpa) * op.aColStride : op.a, okA);
+            const int jj = e & (TILE - 1);
+            const int pb = e / TILE;
+            const int kpb = kbase + pb;
+            const bool okB = kpb < op.k && jj < op.n;
+            const double* srcB = op.b;
+            if (okB)
             {
-                if (ii < op.n)
-                {
-                    const std::int64_t row = op.bIndex != nullptr ? op.bIndex[kp] : kp;
-                    vb = op.b[ii * op.bRowStride + row * op.bColStride];
-                    if (op.d != nullptr)
-                        vb *= op.d[static_cast<std::int64_t>(kp) * op.dStride];
-                }
+                const std::int64_t row = op.bIndex != nullptr ? op.bIndex[kpb] : kpb;
+                srcB = op.b + jj * op.bRowStride + row * op.bColStride;
             }
-            ra[q] = va;
-            rb[q] = vb;
+            copyAsync8(sB + pb * LD + jj, srcB, okB);
         }
-    };
-    const auto store = [&]()
-    {
-#pragma unroll
-        for (int q = 0; q < PER_THREAD; ++q)
+        if (tid < TILE_SLICE)
         {
-            const int e = tid + q * TILE_THREADS;
-            const int ii = e & (TILE - 1);
-            const int p = e >> 6;
-            if (A_BY_ROWS)
-                smemA[(e & (TILE_K - 1)) * LD + (e >> 4)] = ra[q];
-            else
-                smemA[p * LD + ii] = ra[q];
-            smemB[p * LD + ii] = rb[q];
+            const bool okD = scaled && kbase + tid < op.k;
+            copyAsync8(sD + tid, okD ? op.d + static_cast<std::int64_t>(kbase + tid) * op.dStride : op.b, okD);
         }
+        commitAsyncCopies();
     };
 
-    load(0);
-    store();
-    __syncthreads();
-    for (int kbase = 0; kbase < op.k; kbase += TILE_K)
-    {
-        const bool more = kbase + TILE_K < op.k;
-        if (more)
-            load(kbase + TILE_K);
 #pragma unroll
-        for (int kk = 0; kk < TILE_K; kk += 4)
+    for (int s = 0; s < TILE_STAGES - 1; ++s)
+    {
+        if (s < slices)
+            issue(s);
+        else
+            commitAsyncCopies();
+    }
+    for (int t = 0; t < slices; ++t)
+    {
+        waitAsyncCopies<TILE_STAGES - 2>();
+        __syncthreads();
+        if (t + TILE_STAGES - 1 < slices)
+            issue(t + TILE_STAGES - 1);
+        else
+            commitAsyncCopies();
+        const double* sA = smem + (t % TILE_STAGES) * TILE_STAGE_DOUBLES;
+        const double* sB = sA + TILE_SLICE * LD;
+        const double* sD = sB + TILE_SLICE * LD;
+#pragma unroll
+        for (int kk = 0; kk < TILE_SLICE; kk += 4)
         {
             const int pr = kk + (lane & 3);
+            const double dp = scaled ? sD[pr] : 1.0;
             double fa[4];
             double fb[4];
 #pragma unroll
             for (int mi = 0; mi < 4; ++mi)
-                fa[mi] = smemA[pr * LD + wm + mi * 8 + (lane >> 2)];
+                fa[mi] = sA[pr * LD + wm + mi * 8 + (lane >> 2)];
 #pragma unroll
             for (int ni = 0; ni < 4; ++ni)
-                fb[ni] = smemB[pr * LD + wn + ni * 8 + (lane >> 2)];
+                fb[ni] = scaled ? sB[pr * LD + wn + ni * 8 + (lane >> 2)] * dp : sB[pr * LD + wn + ni * 8 + (lane >> 2)];
 #pragma unroll
             for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
                 for (int ni = 0; ni < 4; ++ni)
                     dmma8x8x4(acc[mi][ni], fa[mi], fb[ni]);
         }
-        __syncthreads();
-        if (more)
-        {
-            store();
-            __syncthreads();
-        }
     }
+    waitAsyncCopies<0>();
 
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)

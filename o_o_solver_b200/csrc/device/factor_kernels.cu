@@ -253,109 +253,205 @@ __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int3
 // ------------------------------------------------------------------------------------------------------------------
 // Blocked elimination of a large front's panel, step t (columns [k0, k0 + kb), k0 = 64 t):
 //   diagonalBlocks: the kb x kb diagonal block eliminated in shared memory by one block per front;
-//   panelRows: the rows below it, L(i, :) = A(i, :) L11^-T D^-1, one block per front and 128 rows, each thread a row
-//              (the chain of the right-looking algorithm: a_ij - sum_k l_ik w_jk, then / d_j);
+//   panelRowsInverse: the rows below it, L(i, :) = A(i, :) L11^-T D^-1, as a product with the block's inverse on the
+//              FP64 tensor cores, one block per front and 128 rows;
 //   trailing panel update and final update-matrix SYRK: tile products (tileProduct).
 // ------------------------------------------------------------------------------------------------------------------
 constexpr int BLOCK = 64;
 
-__global__ void diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0)
+__global__ void __launch_bounds__(BLOCK) diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0)
 {
     __shared__ double a[BLOCK * (BLOCK + 1)];
+    __shared__ double column[BLOCK]; // column k of the step, before scaling
+    __shared__ double scaled[BLOCK]; // w_i = l_ik d_k of the step
     const std::int32_t s = list[blockIdx.x];
     const FrontDesc f = args.fronts[s];
     const int n = f.c + f.r;
     const int kb = min(BLOCK, f.c - k0);
     constexpr int LD = BLOCK + 1;
     double* panel = args.panels + f.panel + static_cast<std::int64_t>(k0) * n + k0;
-    const int tid = threadIdx.x;
-    const int threads = blockDim.x;
-    const int warp = tid >> 5;
-    const int lane = tid & 31;
-    const int warps = threads >> 5;
-    for (int e = tid; e < kb * kb; e += threads)
-    {
-        const int j = e / kb;
-        const int i = e - j * kb;
-        a[i + j * LD] = panel[i + static_cast<std::int64_t>(j) * n];
-    }
-    __syncthreads();
-    for (int k = 0; k < kb; ++k)
-    {
-        const double pivot = a[k + k * LD];
-        if (isBadPivot(pivot) && tid == 0)
-            atomicMin(args.zeroPivot + s, k0 + k);
-        for (int i = k + 1 + tid; i < kb; i += threads)
-            a[i + k * LD] = a[i + k * LD] / pivot;
-        __syncthreads();
-        for (int j = k + 1 + warp; j < kb; j += warps)
-        {
-            const double w = a[j + k * LD] * pivot;
-            for (int i = j + lane; i < kb; i += 32)
-                a[i + j * LD] -= a[i + k * LD] * w;
-        }
-        __syncthreads();
-    }
-    for (int e = tid; e < kb * kb; e += threads)
-    {
-        const int j = e / kb;
-        const int i = e - j * kb;
-        if (i >= j)
-            panel[i + static_cast<std::int64_t>(j) * n] = a[i + j * LD];
-    }
-}
-
-constexpr int ROWS_PER_BLOCK = 128;
-
-__global__ void __launch_bounds__(ROWS_PER_BLOCK) panelRows(FactorArgs args, const TileTask* tasks, int k0)
-{
-    __shared__ double w[BLOCK * BLOCK]; // w[j * BLOCK + k] = L11(j, k) * d_k
-    __shared__ double dinv[BLOCK];
-    const TileTask task = tasks[blockIdx.x];
-    const FrontDesc f = args.fronts[task.front];
-    const int n = f.c + f.r;
-    const int kb = min(BLOCK, f.c - k0);
-    const double* diag = args.panels + f.panel + static_cast<std::int64_t>(k0) * n + k0;
-    for (int e = threadIdx.x; e < BLOCK * BLOCK; e += blockDim.x)
+    const int t = threadIdx.x; // this thread's row of the block
+    // Staged by asynchronous copies (all of a thread's loads in flight at once), zeros outside the block.
+    for (int e = t; e < BLOCK * BLOCK; e += BLOCK)
     {
         const int j = e / BLOCK;
-        const int k = e - j * BLOCK;
-        double value = 0.0;
-        if (j < kb && k < j)
-            value = diag[j + static_cast<std::int64_t>(k) * n] * diag[k + static_cast<std::int64_t>(k) * n];
-        w[e] = value;
+        const int i = e - j * BLOCK;
+        const bool inside = i < kb && j < kb;
+        copyAsync8(a + i + j * LD, inside ? panel + i + static_cast<std::int64_t>(j) * n : panel, inside);
     }
-    for (int k = threadIdx.x; k < BLOCK; k += blockDim.x)
-        dinv[k] = k < kb ? diag[k + static_cast<std::int64_t>(k) * n] : 1.0;
+    commitAsyncCopies();
+    waitAsyncCopies<0>();
     __syncthreads();
-    const int row = task.i0 + threadIdx.x;
-    if (row >= n)
+    // Row t in registers; the right-looking chain of the reference per element (l_ik = a_ik / d_k, then
+    // a_ij -= l_ik (l_jk d_k) for k increasing), two barriers of two warps per column.
+    double r[BLOCK];
+#pragma unroll
+    for (int j = 0; j < BLOCK; ++j)
+        r[j] = a[t + j * LD];
+#pragma unroll
+    for (int k = 0; k < BLOCK; ++k)
+    {
+        if (k < kb)
+        {
+            if (t >= k)
+                column[t] = r[k];
+            __syncthreads();
+            const double pivot = column[k];
+            if (t == k && isBadPivot(pivot))
+                atomicMin(args.zeroPivot + s, k0 + k);
+            double l = 0.0;
+            if (t > k)
+            {
+                l = column[t] / pivot;
+                r[k] = l;
+                scaled[t] = l * pivot;
+            }
+            __syncthreads();
+            if (t > k)
+            {
+#pragma unroll
+                for (int j = k + 1; j < BLOCK; ++j)
+                    if (j <= t)
+                        r[j] -= l * scaled[j];
+            }
+        }
+    }
+    // The factor back (lower triangle and D) and into shared memory for the inverse.
+#pragma unroll
+    for (int j = 0; j < BLOCK; ++j)
+        if (j <= t && t < kb)
+        {
+            panel[t + static_cast<std::int64_t>(j) * n] = r[j];
+            a[t + j * LD] = r[j];
+        }
+    __syncthreads();
+    // L11^-1 into the block's strict upper triangle (L11^-1(i, j) at (j, i)): thread j carries column j of the inverse
+    // through the forward substitution of e_j in registers. panelRowsInverse reads it for the rows below; the solves'
+    // diagonal steps read it too.
+    const int j = t;
+    if (j >= kb)
         return;
-    double* base = args.panels + f.panel + static_cast<std::int64_t>(k0) * n + row;
     double x[BLOCK];
 #pragma unroll
-    for (int j = 0; j < BLOCK; ++j)
-        x[j] = j < kb ? base[static_cast<std::int64_t>(j) * n] : 0.0;
+    for (int i = 0; i < BLOCK; ++i)
+        x[i] = i == j ? 1.0 : 0.0;
 #pragma unroll
-    for (int j = 0; j < BLOCK; ++j)
+    for (int i = 1; i < BLOCK; ++i)
     {
-        double v = x[j];
+        double v = x[i];
 #pragma unroll
-        for (int k = 0; k < j; ++k)
-            v -= x[k] * w[j * BLOCK + k];
-        x[j] = v / dinv[j];
+        for (int q = 0; q < i; ++q)
+            v -= a[i + q * LD] * x[q];
+        x[i] = v;
     }
 #pragma unroll
-    for (int j = 0; j < BLOCK; ++j)
-        if (j < kb)
-            base[static_cast<std::int64_t>(j) * n] = x[j];
+    for (int i = 1; i < BLOCK; ++i)
+        if (i > j && i < kb)
+            panel[j + static_cast<std::int64_t>(i) * n] = x[i];
+}
+
+// The rows below step k0's diagonal block, L21 = A21 L11^-T D^-1, as products on the FP64 tensor cores: for each
+// 64-row half of a 128-row task, Y = A21 (L11^-1)^T with L11^-1 from the block's strict upper triangle (unit diagonal),
+// then l_ij = y_ij / d_j, written in place (a block stages its rows before it writes them). Dynamic shared memory:
+// PANEL_ROWS_INVERSE_SMEM bytes.
+__global__ void __launch_bounds__(TILE_THREADS) panelRowsInverse(FactorArgs args, const TileTask* tasks, int k0)
+{
+    constexpr int LD = TILE + TILE_PAD;
+    extern __shared__ double stage[];
+    double* sA = stage;           // sA[p * LD + ii] = A21(ii, p)
+    double* sB = sA + BLOCK * LD; // sB[p * LD + jj] = L11^-1(jj, p) for p < jj, 1 for p == jj, 0 above
+    double* sd = sB + BLOCK * LD; // d_j
+    const TileTask task = tasks[blockIdx.x];
+    const FrontDesc f = args.fronts[task.front];
+    const std::int64_t n = f.c + f.r;
+    const int kb = min(BLOCK, f.c - k0);
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int wm = (warp >> 1) * 32;
+    const int wn = (warp & 1) * 32;
+    const double* block = args.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
+    // The block's strict upper triangle (L11^-1 transposed) and its diagonal, by asynchronous copies; the diagonal
+    // slots then become the unit diagonal of L11^-1 and everything below it zero.
+    for (int e = tid; e < BLOCK * BLOCK; e += blockDim.x)
+    {
+        const int jj = e / BLOCK;
+        const int p = e - jj * BLOCK;
+        const bool inside = p <= jj && jj < kb;
+        copyAsync8(sB + p * LD + jj, inside ? block + p + static_cast<std::int64_t>(jj) * n : block, inside);
+    }
+    commitAsyncCopies();
+    waitAsyncCopies<0>();
+    __syncthreads();
+    for (int j = tid; j < BLOCK; j += blockDim.x)
+    {
+        sd[j] = j < kb ? sB[j * LD + j] : 1.0;
+        sB[j * LD + j] = j < kb ? 1.0 : 0.0;
+    }
+    for (int half = 0; half < 2; ++half)
+    {
+        const std::int64_t i0 = task.i0 + half * TILE;
+        if (i0 >= n)
+            break;
+        const int m = static_cast<int>(n - i0 < TILE ? n - i0 : TILE);
+        double* rows = args.panels + f.panel + i0 + static_cast<std::int64_t>(k0) * n;
+        for (int e = tid; e < BLOCK * TILE; e += blockDim.x)
+        {
+            const int p = e / TILE;
+            const int ii = e - p * TILE;
+            const bool inside = p < kb && ii < m;
+            copyAsync8(sA + p * LD + ii, inside ? rows + ii + static_cast<std::int64_t>(p) * n : rows, inside);
+        }
+        commitAsyncCopies();
+        waitAsyncCopies<0>();
+        __syncthreads();
+        double acc[4][4][2];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+            {
+                acc[mi][ni][0] = 0.0;
+                acc[mi][ni][1] = 0.0;
+            }
+#pragma unroll 4
+        for (int kk = 0; kk < BLOCK; kk += 4)
+        {
+            const int pr = kk + (lane & 3);
+            double fa[4];
+            double fb[4];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+                fa[mi] = sA[pr * LD + wm + mi * 8 + (lane >> 2)];
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+                fb[ni] = sB[pr * LD + wn + ni * 8 + (lane >> 2)];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+                    dmma8x8x4(acc[mi][ni], fa[mi], fb[ni]);
+        }
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                {
+                    const int ii = wm + mi * 8 + (lane >> 2);
+                    const int jj = wn + ni * 8 + (lane & 3) * 2 + h;
+                    if (ii < m && jj < kb)
+                        rows[ii + static_cast<std::int64_t>(jj) * n] = acc[mi][ni][h] / sd[jj];
+                }
+        __syncthreads();
+    }
 }
 
 // Trailing panel update of step t: columns [o, c), rows [o, n), o = k0 + 64, K = the step's 64 columns.
 __global__ void __launch_bounds__(TILE_THREADS) panelUpdate(FactorArgs args, const TileTask* tasks, int k0)
 {
-    __shared__ double smemA[TILE_K * (TILE + TILE_PAD)];
-    __shared__ double smemB[TILE_K * (TILE + TILE_PAD)];
+    __shared__ double smem[TILE_SMEM_DOUBLES];
     const TileTask task = tasks[blockIdx.x];
     const FrontDesc f = args.fronts[task.front];
     const std::int64_t n = f.c + f.r;
@@ -378,14 +474,13 @@ __global__ void __launch_bounds__(TILE_THREADS) panelUpdate(FactorArgs args, con
     op.k = BLOCK;
     op.lower = task.i0 == task.j0;
     op.lowerOffset = 0;
-    tileProduct(op, smemA, smemB);
+    tileProduct(op, smem);
 }
 
 // The Schur update of the update matrix: U(i, j) -= sum_{k < c} L(c + i, k) d_k L(c + j, k), lower tiles.
 __global__ void __launch_bounds__(TILE_THREADS) updateMatrix(FactorArgs args, const TileTask* tasks)
 {
-    __shared__ double smemA[TILE_K * (TILE + TILE_PAD)];
-    __shared__ double smemB[TILE_K * (TILE + TILE_PAD)];
+    __shared__ double smem[TILE_SMEM_DOUBLES];
     const TileTask task = tasks[blockIdx.x];
     const FrontDesc f = args.fronts[task.front];
     const std::int64_t n = f.c + f.r;
@@ -408,7 +503,7 @@ __global__ void __launch_bounds__(TILE_THREADS) updateMatrix(FactorArgs args, co
     op.k = f.c;
     op.lower = task.i0 == task.j0;
     op.lowerOffset = 0;
-    tileProduct(op, smemA, smemB);
+    tileProduct(op, smem);
 }
 
 // ------------------------------------------------------------------------------------------------------------------

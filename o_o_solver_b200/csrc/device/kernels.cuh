@@ -53,7 +53,8 @@ struct SolveArgs
 __global__ void assembleFronts(FactorArgs args, const AssemblyTask* tasks, std::int32_t* structureError);
 __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int32_t* structureError);
 __global__ void diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0);
-__global__ void panelRows(FactorArgs args, const TileTask* tasks, int k0);
+__global__ void panelRowsInverse(FactorArgs args, const TileTask* tasks, int k0);
+constexpr std::size_t PANEL_ROWS_INVERSE_SMEM = (2 * 64 * (TILE + TILE_PAD) + 64) * sizeof(double);
 __global__ void panelUpdate(FactorArgs args, const TileTask* tasks, int k0);
 __global__ void updateMatrix(FactorArgs args, const TileTask* tasks);
 __global__ void pivotSummary(FactorArgs args, const std::int32_t* supernodeOfColumn, int dimension,

@@ -404,8 +404,10 @@ __global__ void pivotedDiagonal(FactorArgs args, PivotArgs pivots, const std::in
     {
         const int j = e / kb;
         const int i = e - j * kb;
-        a[i + j * LD] = block[i + static_cast<std::int64_t>(j) * n];
+        copyAsync8(a + i + j * LD, block + i + static_cast<std::int64_t>(j) * n, true);
     }
+    commitAsyncCopies();
+    waitAsyncCopies<0>();
     __syncthreads();
     // A candidate the block cannot pivot sends the front to the exact path (status bit 1), as a failed growth test.
     const int eliminated = bunchKaufman(SharedAt{a, LD}, kb, kb, perm, sub, scratchValue, scratchIndex, false, nullptr);
@@ -557,8 +559,7 @@ __global__ void __launch_bounds__(128) panelRowsPivoted(FactorArgs args, PivotAr
 __global__ void __launch_bounds__(TILE_THREADS) updatePivoted(FactorArgs args, PivotArgs pivots, const TileTask* tasks,
                                                               int k0)
 {
-    __shared__ double smemA[TILE_K * (TILE + TILE_PAD)];
-    __shared__ double smemB[TILE_K * (TILE + TILE_PAD)];
+    __shared__ double smem[TILE_SMEM_DOUBLES];
     const TileTask task = tasks[blockIdx.x];
     const FrontDesc f = args.fronts[task.front];
     const std::int64_t n = f.c + f.r;
@@ -590,7 +591,7 @@ __global__ void __launch_bounds__(TILE_THREADS) updatePivoted(FactorArgs args, P
     op.k = min(64, f.c - k0);
     op.lower = task.i0 == task.j0;
     op.lowerOffset = 0;
-    tileProduct(op, smemA, smemB);
+    tileProduct(op, smem);
 }
 
 // ------------------------------------------------------------------------------------------------------------------

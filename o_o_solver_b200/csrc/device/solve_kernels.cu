@@ -169,8 +169,11 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) invertDiagonal(FactorArgs args, c
     {
         const int q = e / SOLVE_BLOCK;
         const int i = e - q * SOLVE_BLOCK;
-        l[q * LD + i] = q < kb && i < kb && i > q ? block[i + static_cast<std::int64_t>(q) * n] : 0.0;
+        const bool inside = q < kb && i < kb && i > q;
+        copyAsync8(l + q * LD + i, inside ? block + i + static_cast<std::int64_t>(q) * n : block, inside);
     }
+    commitAsyncCopies();
+    waitAsyncCopies<0>();
     __syncthreads();
     const int j = threadIdx.x;
     if (j >= kb)
@@ -207,10 +210,13 @@ __device__ __forceinline__ int stageInverse(const SolveArgs& a, const FrontDesc&
     {
         const int i = e / SOLVE_BLOCK;
         const int q = e - i * SOLVE_BLOCK;
-        inv[i * LD + q] = q < i && i < kb ? block[q + static_cast<std::int64_t>(i) * n] : 0.0;
+        const bool inside = q < i && i < kb;
+        copyAsync8(inv + i * LD + q, inside ? block + q + static_cast<std::int64_t>(i) * n : block, inside);
     }
     for (int e = threadIdx.x; e < kb * a.width; e += blockDim.x)
-        b[e] = xRows[e];
+        copyAsync8(b + e, xRows + e, true);
+    commitAsyncCopies();
+    waitAsyncCopies<0>();
     __syncthreads();
     return kb;
 }
@@ -243,8 +249,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) forwardDiagonal(SolveArgs a, co
 // rows (i0 >= c, task.k0 = 1); C -= L(i, k0:k0+kb) x_block.
 __global__ void __launch_bounds__(TILE_THREADS) forwardUpdate(SolveArgs a, const TileTask* tasks, int k0)
 {
-    __shared__ double smemA[TILE_K * (TILE + TILE_PAD)];
-    __shared__ double smemB[TILE_K * (TILE + TILE_PAD)];
+    __shared__ double smem[TILE_SMEM_DOUBLES];
     const TileTask task = tasks[blockIdx.x];
     const FrontDesc f = a.fronts[task.front];
     const std::int64_t n = f.c + f.r;
@@ -276,7 +281,7 @@ __global__ void __launch_bounds__(TILE_THREADS) forwardUpdate(SolveArgs a, const
     op.k = min(SOLVE_BLOCK, f.c - k0);
     op.lower = false;
     op.lowerOffset = 0;
-    tileProduct(op, smemA, smemB);
+    tileProduct(op, smem);
 }
 
 // The diagonal sweep: X[eq] /= d_eq.
@@ -331,8 +336,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) backwardSmall(SolveArgs a, cons
 // x_F -= L21^T X[R(s)] for a large supernode, by tiles of 64 of its columns (A = L21^T read along its rows).
 __global__ void __launch_bounds__(TILE_THREADS) backwardRows(SolveArgs a, const TileTask* tasks)
 {
-    __shared__ double smemA[TILE_K * (TILE + TILE_PAD)];
-    __shared__ double smemB[TILE_K * (TILE + TILE_PAD)];
+    __shared__ double smem[TILE_SMEM_DOUBLES];
     const TileTask task = tasks[blockIdx.x];
     const FrontDesc f = a.fronts[task.front];
     const std::int64_t n = f.c + f.r;
@@ -355,7 +359,7 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardRows(SolveArgs a, const 
     op.k = f.r;
     op.lower = false;
     op.lowerOffset = 0;
-    tileProduct<true>(op, smemA, smemB);
+    tileProduct<true>(op, smem);
 }
 
 // The unit upper triangle L11^T of step k0 (rows [k0, k0 + kb) of x_F) as the product with the transposed inverse:
@@ -385,8 +389,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) backwardDiagonal(SolveArgs a, c
 // q in a tile of [0, k0).
 __global__ void __launch_bounds__(TILE_THREADS) backwardUpdate(SolveArgs a, const TileTask* tasks, int k0)
 {
-    __shared__ double smemA[TILE_K * (TILE + TILE_PAD)];
-    __shared__ double smemB[TILE_K * (TILE + TILE_PAD)];
+    __shared__ double smem[TILE_SMEM_DOUBLES];
     const TileTask task = tasks[blockIdx.x];
     const FrontDesc f = a.fronts[task.front];
     const std::int64_t n = f.c + f.r;
@@ -410,7 +413,7 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardUpdate(SolveArgs a, cons
     op.k = min(SOLVE_BLOCK, f.c - k0);
     op.lower = false;
     op.lowerOffset = 0;
-    tileProduct<true>(op, smemA, smemB);
+    tileProduct<true>(op, smem);
 }
 
 // Column-major B (ld) <-> rows of X (width columns from column c0).

@@ -121,6 +121,9 @@ public:
             check(cudaFuncSetAttribute(device::smallFronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(m_smallSmem)),
                   "smallFronts shared memory");
+        check(cudaFuncSetAttribute(device::panelRowsInverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(device::PANEL_ROWS_INVERSE_SMEM)),
+              "panel rows shared memory");
         // The diagonal steps of the solves: the block's inverse and the rows of a 64-column tile.
         for (const void* kernel : {reinterpret_cast<const void*>(device::forwardDiagonal),
                                    reinterpret_cast<const void*>(device::backwardDiagonal)})
@@ -969,11 +972,12 @@ private:
                                                                            m_structureError.get());
                 break;
             case LaunchKind::DiagonalBlocks:
-                device::diagonalBlocks<<<launch.count, 256, 0, m_stream>>>(args, m_lists.get() + launch.offset,
-                                                                           launch.k0);
+                device::diagonalBlocks<<<launch.count, 64, 0, m_stream>>>(args, m_lists.get() + launch.offset,
+                                                                          launch.k0);
                 break;
             case LaunchKind::PanelRows:
-                device::panelRows<<<launch.count, 128, 0, m_stream>>>(args, m_tiles.get() + launch.offset, launch.k0);
+                device::panelRowsInverse<<<launch.count, device::TILE_THREADS, device::PANEL_ROWS_INVERSE_SMEM,
+                                           m_stream>>>(args, m_tiles.get() + launch.offset, launch.k0);
                 break;
             case LaunchKind::PanelUpdate:
                 device::panelUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(
