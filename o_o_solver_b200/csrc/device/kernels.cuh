@@ -68,6 +68,11 @@ constexpr std::size_t diagonalSolveSmem(int width)
 {
     return static_cast<std::size_t>(64 * 65 + 64 * width) * sizeof(double);
 }
+// Dynamic shared memory of forwardSmall / backwardSmall: the inverse and a c x width block.
+constexpr std::size_t smallSolveSmem(int columns, int width)
+{
+    return static_cast<std::size_t>(64 * 65 + columns * width) * sizeof(double);
+}
 __global__ void forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0);
 __global__ void forwardUpdate(SolveArgs a, const TileTask* tasks, int k0);
 __global__ void diagonalSweep(SolveArgs a, const std::int32_t* supernodeOfColumn, int dimension);

@@ -20,6 +20,7 @@ namespace oosgpu::device
 
 constexpr int SOLVE_BLOCK = 64;
 constexpr int SOLVE_THREADS = 256;
+constexpr int SOLVE_WIDTH_MAX = 64; // the widest tile of right-hand sides
 
 // Adds the children's update rows into the supernode's rows of X (positions < c) and into its own update rows
 // (zeroed first), children in increasing order.
@@ -35,6 +36,7 @@ __device__ void gatherChildren(const SolveArgs& a, const FrontDesc& f, double* x
         const FrontDesc ch = a.fronts[a.children[f.childStart + q]];
         const std::int32_t* map = a.relpos + ch.rowStart;
         const double* source = a.updates + ch.rowStart * w;
+#pragma unroll 4
         for (int e = threadIdx.x; e < ch.r * w; e += blockDim.x)
         {
             const int i = e / w;
@@ -49,35 +51,77 @@ __device__ void gatherChildren(const SolveArgs& a, const FrontDesc& f, double* x
     }
 }
 
-// Forward sweep of a small supernode (c <= SOLVE_BLOCK): x_F <- L11^-1 (b_F + children), u_s <- children - L21 x_F.
+// The inverse of a small supernode's unit lower triangle L11 (c <= 64), from its strict upper triangle:
+// inv[i * (SOLVE_BLOCK + 1) + q] = L11^-1(i, q) for q < i < c, zero elsewhere (asynchronous copies, not waited for).
+__device__ __forceinline__ void stageSmallInverse(const SolveArgs& a, const FrontDesc& f, double* inv)
+{
+    constexpr int LD = SOLVE_BLOCK + 1;
+    const std::int64_t n = f.c + f.r;
+    const double* panel = a.panels + f.panel;
+    for (int e = threadIdx.x; e < SOLVE_BLOCK * SOLVE_BLOCK; e += blockDim.x)
+    {
+        const int i = e / SOLVE_BLOCK;
+        const int q = e - i * SOLVE_BLOCK;
+        const bool inside = q < i && i < f.c;
+        copyAsync8(inv + i * LD + q, inside ? panel + q + static_cast<std::int64_t>(i) * n : panel, inside);
+    }
+}
+
+// Forward sweep of a small supernode (c <= SOLVE_BLOCK): x_F <- L11^-1 (b_F + children), a product with the inverse
+// of L11 (every value independent), then u_s <- children - L21 x_F. Dynamic shared memory: c * width + 64 * 65
+// doubles.
 __global__ void __launch_bounds__(SOLVE_THREADS) forwardSmall(SolveArgs a, const std::int32_t* list)
 {
-    extern __shared__ double xF[]; // c x width
+    constexpr int LD = SOLVE_BLOCK + 1;
+    extern __shared__ double stage[];
+    double* inv = stage;                      // 64 x 65
+    double* xF = stage + SOLVE_BLOCK * LD;    // c x width
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
-    const int n = f.c + f.r;
     double* xRows = a.x + static_cast<std::int64_t>(f.first) * w;
+    stageSmallInverse(a, f, inv);
     for (int e = threadIdx.x; e < f.c * w; e += blockDim.x)
-        xF[e] = xRows[e];
+        copyAsync8(xF + e, xRows + e, true);
+    commitAsyncCopies();
+    waitAsyncCopies<0>();
     __syncthreads();
     gatherChildren(a, f, xF, w);
-    const double* panel = a.panels + f.panel;
-    for (int q = 0; q < f.c; ++q)
+    // x = L11^-1 b: each thread its values of the block, into registers, then back after a barrier.
+    constexpr int PER_THREAD = SOLVE_BLOCK * SOLVE_WIDTH_MAX / SOLVE_THREADS;
+    double y[PER_THREAD];
+#pragma unroll
+    for (int u = 0; u < PER_THREAD; ++u)
     {
-        for (int e = threadIdx.x; e < (f.c - q - 1) * w; e += blockDim.x)
+        const int e = threadIdx.x + u * SOLVE_THREADS;
+        y[u] = 0.0;
+        if (e < f.c * w)
         {
-            const int i = q + 1 + e / w;
-            const int col = e % w;
-            xF[i * w + col] -= panel[i + static_cast<std::int64_t>(q) * n] * xF[q * w + col];
+            const int i = e / w;
+            const int col = e - i * w;
+            double sum = xF[e];
+            for (int q = 0; q < i; ++q)
+                sum += inv[i * LD + q] * xF[q * w + col];
+            y[u] = sum;
         }
-        __syncthreads();
     }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < PER_THREAD; ++u)
+    {
+        const int e = threadIdx.x + u * SOLVE_THREADS;
+        if (e < f.c * w)
+            xF[e] = y[u];
+    }
+    __syncthreads();
+    const std::int64_t n = f.c + f.r;
+    const double* panel = a.panels + f.panel;
     double* own = a.updates + f.rowStart * w;
     for (int e = threadIdx.x; e < f.r * w; e += blockDim.x)
     {
         const int i = e / w;
         const int col = e - i * w;
         double sum = own[e];
+#pragma unroll 8
         for (int q = 0; q < f.c; ++q)
             sum -= panel[f.c + i + static_cast<std::int64_t>(q) * n] * xF[q * w + col];
         own[e] = sum;
@@ -298,39 +342,44 @@ __global__ void diagonalSweep(SolveArgs a, const std::int32_t* supernodeOfColumn
     a.x[e] = a.x[e] / a.panels[f.panel + k + k * n];
 }
 
-// Backward sweep of a small supernode: x_F <- L11^-T (x_F - L21^T X[R(s)]).
+// Backward sweep of a small supernode: x_F <- L11^-T (x_F - L21^T X[R(s)]), the triangle as a product with the
+// transposed inverse. Dynamic shared memory as forwardSmall.
 __global__ void __launch_bounds__(SOLVE_THREADS) backwardSmall(SolveArgs a, const std::int32_t* list)
 {
-    extern __shared__ double xF[];
+    constexpr int LD = SOLVE_BLOCK + 1;
+    extern __shared__ double stage[];
+    double* inv = stage;
+    double* xF = stage + SOLVE_BLOCK * LD;
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
     const std::int64_t n = f.c + f.r;
     const double* panel = a.panels + f.panel;
     const std::int32_t* rows = a.rows + f.rowStart;
     double* xRows = a.x + static_cast<std::int64_t>(f.first) * w;
+    stageSmallInverse(a, f, inv);
+    commitAsyncCopies();
     for (int e = threadIdx.x; e < f.c * w; e += blockDim.x)
     {
         const int q = e / w;
         const int col = e - q * w;
         double sum = xRows[e];
         const double* l = panel + f.c + static_cast<std::int64_t>(q) * n;
+#pragma unroll 8
         for (int i = 0; i < f.r; ++i)
             sum -= l[i] * a.x[static_cast<std::int64_t>(rows[i]) * w + col];
         xF[e] = sum;
     }
+    waitAsyncCopies<0>();
     __syncthreads();
-    for (int i = f.c - 1; i > 0; --i)
-    {
-        for (int e = threadIdx.x; e < i * w; e += blockDim.x)
-        {
-            const int q = e / w;
-            const int col = e - q * w;
-            xF[q * w + col] -= panel[i + static_cast<std::int64_t>(q) * n] * xF[i * w + col];
-        }
-        __syncthreads();
-    }
     for (int e = threadIdx.x; e < f.c * w; e += blockDim.x)
-        xRows[e] = xF[e];
+    {
+        const int q = e / w;
+        const int col = e - q * w;
+        double sum = xF[e];
+        for (int i = q + 1; i < f.c; ++i)
+            sum += inv[i * LD + q] * xF[i * w + col];
+        xRows[e] = sum;
+    }
 }
 
 // x_F -= L21^T X[R(s)] for a large supernode, by tiles of 64 of its columns (A = L21^T read along its rows).
@@ -416,30 +465,55 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardUpdate(SolveArgs a, cons
     tileProduct<true>(op, smem);
 }
 
-// Column-major B (ld) <-> rows of X (width columns from column c0).
+// Column-major B (ld) <-> rows of X (width columns from column c0), by 32 x 32 tiles transposed in shared memory so
+// that both the column reads and the row writes are coalesced. Block (32, 8); grid (rows / 32, width / 32).
 __global__ void toRows(const double* b, std::int64_t ld, int c0, int width, int dimension, double* x,
                        const double* scale)
 {
-    const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (e >= static_cast<std::int64_t>(dimension) * width)
-        return;
-    const int col = static_cast<int>(e / dimension);
-    const int i = static_cast<int>(e - static_cast<std::int64_t>(col) * dimension);
-    const double s = scale != nullptr ? scale[i] : 1.0;
-    x[static_cast<std::int64_t>(i) * width + col] = b[static_cast<std::int64_t>(c0 + col) * ld + i] * s;
+    __shared__ double tile[32][33];
+    const int i0 = blockIdx.x * 32;
+    const int col0 = blockIdx.y * 32;
+    const int tx = threadIdx.x;
+    for (int c = threadIdx.y; c < 32; c += blockDim.y)
+    {
+        const int col = col0 + c;
+        const int i = i0 + tx;
+        if (col < width && i < dimension)
+            tile[c][tx] = b[static_cast<std::int64_t>(c0 + col) * ld + i] * (scale != nullptr ? scale[i] : 1.0);
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y)
+    {
+        const int i = i0 + r;
+        const int col = col0 + tx;
+        if (col < width && i < dimension)
+            x[static_cast<std::int64_t>(i) * width + col] = tile[tx][r];
+    }
 }
 
 __global__ void fromRows(const double* x, int c0, int width, int dimension, double* b, std::int64_t ld,
                          const double* scale)
 {
-    const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (e >= static_cast<std::int64_t>(dimension) * width)
-        return;
-    const int col = static_cast<int>(e / dimension);
-    const int i = static_cast<int>(e - static_cast<std::int64_t>(col) * dimension);
-    const double s = scale != nullptr ? scale[i] : 1.0;
-    // x + 0.0: a solved value is never -0 (the reference writes x + 0 back, SolveSweeps.cpp:448-457).
-    b[static_cast<std::int64_t>(c0 + col) * ld + i] = x[static_cast<std::int64_t>(i) * width + col] * s + 0.0;
+    __shared__ double tile[32][33];
+    const int i0 = blockIdx.x * 32;
+    const int col0 = blockIdx.y * 32;
+    const int tx = threadIdx.x;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y)
+    {
+        const int i = i0 + r;
+        const int col = col0 + tx;
+        if (col < width && i < dimension)
+            tile[tx][r] = x[static_cast<std::int64_t>(i) * width + col];
+    }
+    __syncthreads();
+    for (int c = threadIdx.y; c < 32; c += blockDim.y)
+    {
+        const int col = col0 + c;
+        const int i = i0 + tx;
+        // x + 0.0: a solved value is never -0 (the reference writes x + 0 back, SolveSweeps.cpp:448-457).
+        if (col < width && i < dimension)
+            b[static_cast<std::int64_t>(c0 + col) * ld + i] = tile[c][tx] * (scale != nullptr ? scale[i] : 1.0) + 0.0;
+    }
 }
 
 } // namespace oosgpu::device

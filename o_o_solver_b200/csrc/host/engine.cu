@@ -130,6 +130,11 @@ public:
             check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(device::diagonalSolveSmem(SOLVE_WIDTH))),
                   "diagonal solve shared memory");
+        for (const void* kernel : {reinterpret_cast<const void*>(device::forwardSmall),
+                                   reinterpret_cast<const void*>(device::backwardSmall)})
+            check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(device::smallSolveSmem(SOLVE_SMALL_COLUMNS, SOLVE_WIDTH))),
+                  "small solve shared memory");
         check(cudaStreamSynchronize(m_stream), "plan upload");
     }
 
@@ -581,7 +586,8 @@ public:
             device::toRowsPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(b, ld, c0, width, n, x, m_perm.get(),
                                                                                m_solveScale);
         else
-            device::toRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(b, ld, c0, width, n, x, m_solveScale);
+            device::toRows<<<dim3(blocksFor(n, 32), blocksFor(width, 32)), dim3(32, 8), 0, m_stream>>>(
+                b, ld, c0, width, n, x, m_solveScale);
     }
 
     // The rows of x back into the column tile of B.
@@ -593,7 +599,8 @@ public:
             device::fromRowsPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(x, c0, width, n, b, ld, m_perm.get(),
                                                                                  m_solveScale);
         else
-            device::fromRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(x, c0, width, n, b, ld, m_solveScale);
+            device::fromRows<<<dim3(blocksFor(n, 32), blocksFor(width, 32)), dim3(32, 8), 0, m_stream>>>(
+                x, c0, width, n, b, ld, m_solveScale);
     }
 
     // The three sweeps on a tile of `width` columns stored by rows (n x width) in x (in pivot order after an indefinite
@@ -999,7 +1006,7 @@ private:
         {
             const std::int32_t* list = m_lists.get() + launch.offset;
             const device::TileTask* tiles = m_tiles.get() + launch.offset;
-            const std::size_t smallSmem = static_cast<std::size_t>(std::max(launch.smemOrder, 1)) * args.width * sizeof(double);
+            const std::size_t smallSmem = device::smallSolveSmem(std::max(launch.smemOrder, 1), args.width);
             switch (launch.kind)
             {
             case LaunchKind::ForwardSmall:

@@ -462,7 +462,7 @@ Plan buildPlan(const Symbolic& symbolic)
             }
             addTiles(plan, plan.forwardLaunches, LaunchKind::ForwardGather, ranges);
         }
-        for (const std::int32_t s : solveLarge)
+        for (const std::int32_t s : members)
             for (std::int32_t k0 = 0; k0 < plan.fronts[static_cast<std::size_t>(s)].c; k0 += BLOCK)
                 inverseTasks.push_back({s, k0, 0, 0});
         for (std::int32_t k0 = 0; k0 < maxColumns; k0 += BLOCK)

@@ -91,8 +91,8 @@ struct Plan
     std::vector<Launch> factorLaunches;
     std::vector<Launch> forwardLaunches;
     std::vector<Launch> backwardLaunches;
-    // The diagonal blocks (front, k0) of the supernodes the solves take by 64-column steps, inverted after each
-    // factorisation into the blocks' upper triangles.
+    // The 64-column diagonal blocks (front, k0) of every supernode, inverted after each factorisation into the blocks'
+    // upper triangles (the solves apply the inverses).
     std::vector<Launch> inverseLaunches;
 
     // Indefinite mode: the launches (assembly shared with the positive definite sequence), the large fronts of each
