@@ -94,6 +94,8 @@ __global__ void smallFrontsPivoted(FactorArgs args, PivotArgs pivots, const std:
 __global__ void pivotedDiagonal(FactorArgs args, PivotArgs pivots, const std::int32_t* list, int k0);
 __global__ void permuteEarlierRows(FactorArgs args, PivotArgs pivots, const TileTask* tasks, int k0);
 __global__ void panelRowsPivoted(FactorArgs args, PivotArgs pivots, const TileTask* tasks, int k0);
+__global__ void panelRowsPivotedInverse(FactorArgs args, PivotArgs pivots, const TileTask* tasks, int k0);
+constexpr std::size_t PANEL_ROWS_PIVOTED_SMEM = PANEL_ROWS_INVERSE_SMEM + 64 * (sizeof(double) + sizeof(int));
 __global__ void updatePivoted(FactorArgs args, PivotArgs pivots, const TileTask* tasks, int k0);
 __global__ void pivotedFront(FactorArgs args, PivotArgs pivots, std::int32_t s, double* work,
                              std::int32_t* structureError);

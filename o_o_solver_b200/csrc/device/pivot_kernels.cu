@@ -311,6 +311,32 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
     return k;
 }
 
+// Column j of the inverse of the unit lower 64 x 64 block `a` (column-major, leading dimension 65, zero outside its
+// kb x kb corner) by forward substitution of e_j in registers, written into block's strict upper triangle
+// (L^-1(i, j) at (j, i)). Not inlined: its registers are its own, not added to the Bunch-Kaufman kernel's.
+__device__ __noinline__ void invertColumn(const double* a, int j, int kb, double* block, std::int64_t n)
+{
+    constexpr int B = 64;
+    constexpr int LD = B + 1;
+    double x[B];
+#pragma unroll
+    for (int i = 0; i < B; ++i)
+        x[i] = i == j ? 1.0 : 0.0;
+#pragma unroll
+    for (int i = 1; i < B; ++i)
+    {
+        double v = x[i];
+#pragma unroll
+        for (int q = 0; q < i; ++q)
+            v -= a[i + q * LD] * x[q];
+        x[i] = v;
+    }
+#pragma unroll
+    for (int i = 1; i < B; ++i)
+        if (i > j && i < kb)
+            block[j + static_cast<std::int64_t>(i) * n] = x[i];
+}
+
 struct SharedAt
 {
     double* a;
@@ -436,6 +462,163 @@ __global__ void pivotedDiagonal(FactorArgs args, PivotArgs pivots, const std::in
             swapped |= perm[j] != j;
         pivots.stepSwapped[s] = swapped;
     }
+    // L11^-1 (unit lower, zero below each 2x2 pivot) into the block's strict upper triangle, as diagonalBlocks does:
+    // the columns of the inverse by forward substitution of e_j, a column per thread at a time.
+    for (int e = threadIdx.x; e < B * B; e += blockDim.x)
+    {
+        const int q = e / B;
+        const int i = e - q * B;
+        if (i >= kb || q >= kb)
+            a[i + q * LD] = 0.0;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < kb; j += blockDim.x)
+        invertColumn(a, j, kb, block, n);
+}
+
+// The rows below step k0's diagonal block of an indefinite front, as products with the block's inverse: the row's
+// entries in the block's columns read in pivot order, Y = A (L11^-1)^T on the FP64 tensor cores (L11^-1 from the
+// block's strict upper triangle), then L = Y D^-1 (2x2 blocks by the dsytf2 formula) written to the panel, W = L D = Y
+// to the front's W buffer, and a coefficient above 1/u (or not finite) flags the front (status bit 1). 64-row halves
+// of a 128-row task; dynamic shared memory PANEL_ROWS_INVERSE_SMEM bytes plus 64 doubles and 64 ints.
+__global__ void __launch_bounds__(TILE_THREADS) panelRowsPivotedInverse(FactorArgs args, PivotArgs pivots,
+                                                                        const TileTask* tasks, int k0)
+{
+    constexpr int B = 64;
+    constexpr int LD = TILE + TILE_PAD;
+    extern __shared__ double stage[];
+    double* sA = stage;       // sA[p * LD + ii] = A(ii, perm p); then Y(ii, jj) at sA[jj * LD + ii]
+    double* sB = sA + B * LD; // L11^-1(jj, p) at sB[p * LD + jj], unit diagonal, zero above
+    double* sd = sB + B * LD; // d_j
+    double* se = sd + B;      // e_j of a 2x2 pivot at its first column
+    int* sperm = reinterpret_cast<int*>(se + B);
+    const TileTask task = tasks[blockIdx.x];
+    const std::int32_t s = task.front;
+    const FrontDesc f = args.fronts[s];
+    const std::int64_t n = f.c + f.r;
+    const int kb = min(B, f.c - k0);
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int wm = (warp >> 1) * 32;
+    const int wn = (warp & 1) * 32;
+    const double* block = args.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
+    for (int e = tid; e < B * B; e += blockDim.x)
+    {
+        const int jj = e / B;
+        const int p = e - jj * B;
+        const bool inside = p <= jj && jj < kb;
+        copyAsync8(sB + p * LD + jj, inside ? block + p + static_cast<std::int64_t>(jj) * n : block, inside);
+    }
+    for (int j = tid; j < B; j += blockDim.x)
+    {
+        se[j] = j < kb ? pivots.subdiagonal[f.first + k0 + j] : 0.0;
+        sperm[j] = j < kb ? pivots.stepPerm[static_cast<std::int64_t>(s) * B + j] : j;
+    }
+    commitAsyncCopies();
+    waitAsyncCopies<0>();
+    __syncthreads();
+    for (int j = tid; j < B; j += blockDim.x)
+    {
+        sd[j] = j < kb ? sB[j * LD + j] : 1.0;
+        sB[j * LD + j] = j < kb ? 1.0 : 0.0;
+    }
+    bool bad = false;
+    for (int half = 0; half < 2; ++half)
+    {
+        const std::int64_t i0 = task.i0 + half * TILE;
+        if (i0 >= n)
+            break;
+        const int m = static_cast<int>(n - i0 < TILE ? n - i0 : TILE);
+        double* rows = args.panels + f.panel + i0 + static_cast<std::int64_t>(k0) * n;
+        double* w = pivots.w + pivots.wOffset[s] + i0;
+        for (int e = tid; e < B * TILE; e += blockDim.x)
+        {
+            const int p = e / TILE;
+            const int ii = e - p * TILE;
+            const bool inside = p < kb && ii < m;
+            copyAsync8(sA + p * LD + ii, inside ? rows + ii + static_cast<std::int64_t>(sperm[p]) * n : rows, inside);
+        }
+        commitAsyncCopies();
+        waitAsyncCopies<0>();
+        __syncthreads();
+        double acc[4][4][2];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+            {
+                acc[mi][ni][0] = 0.0;
+                acc[mi][ni][1] = 0.0;
+            }
+#pragma unroll 4
+        for (int kk = 0; kk < B; kk += 4)
+        {
+            const int pr = kk + (lane & 3);
+            double fa[4];
+            double fb[4];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+                fa[mi] = sA[pr * LD + wm + mi * 8 + (lane >> 2)];
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+                fb[ni] = sB[pr * LD + wn + ni * 8 + (lane >> 2)];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+                    dmma8x8x4(acc[mi][ni], fa[mi], fb[ni]);
+        }
+        __syncthreads();
+        // Y into shared memory (over A: every product has read it), column jj at sA[jj * LD].
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                {
+                    const int ii = wm + mi * 8 + (lane >> 2);
+                    const int jj = wn + ni * 8 + (lane & 3) * 2 + h;
+                    sA[jj * LD + ii] = acc[mi][ni][h];
+                }
+        __syncthreads();
+        // L = Y D^-1 by rows, 1x1 and 2x2 pivots.
+        if (tid < m)
+        {
+            const int ii = tid;
+            int j = 0;
+            while (j < kb)
+            {
+                if (j + 1 < kb && se[j] != 0.0)
+                {
+                    const TwoByTwoInverse inverse = invertTwoByTwo(sd[j], se[j], sd[j + 1]);
+                    const double r0 = sA[j * LD + ii];
+                    const double r1 = sA[(j + 1) * LD + ii];
+                    const double l0 = inverse.s * (inverse.d11 * r0 - r1);
+                    const double l1 = inverse.s * (inverse.d22 * r1 - r0);
+                    rows[ii + static_cast<std::int64_t>(j) * n] = l0;
+                    rows[ii + static_cast<std::int64_t>(j + 1) * n] = l1;
+                    w[ii + static_cast<std::int64_t>(j) * n] = r0;
+                    w[ii + static_cast<std::int64_t>(j + 1) * n] = r1;
+                    bad = bad || !(fabs(l0) <= GROWTH_LIMIT) || !(fabs(l1) <= GROWTH_LIMIT);
+                    j += 2;
+                }
+                else
+                {
+                    const double r0 = sA[j * LD + ii];
+                    const double l = r0 / sd[j];
+                    rows[ii + static_cast<std::int64_t>(j) * n] = l;
+                    w[ii + static_cast<std::int64_t>(j) * n] = r0;
+                    bad = bad || !(fabs(l) <= GROWTH_LIMIT);
+                    j += 1;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (bad)
+        atomicOr(pivots.status + s, 1);
 }
 
 // The rows of L already computed (columns before k0) follow the diagonal block's interchanges of step k0: a task

@@ -124,6 +124,9 @@ public:
         check(cudaFuncSetAttribute(device::panelRowsInverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(device::PANEL_ROWS_INVERSE_SMEM)),
               "panel rows shared memory");
+        check(cudaFuncSetAttribute(device::panelRowsPivotedInverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(device::PANEL_ROWS_PIVOTED_SMEM)),
+              "pivoted panel rows shared memory");
         // The diagonal steps of the solves: the block's inverse and the rows of a 64-column tile.
         for (const void* kernel : {reinterpret_cast<const void*>(device::forwardDiagonal),
                                    reinterpret_cast<const void*>(device::backwardDiagonal)})
@@ -409,7 +412,8 @@ public:
                 device::permuteEarlierRows<<<launch.count, 256, 0, m_stream>>>(args, pivots, tiles, launch.k0);
                 break;
             case LaunchKind::PanelRowsPivoted:
-                device::panelRowsPivoted<<<launch.count, 128, 0, m_stream>>>(args, pivots, tiles, launch.k0);
+                device::panelRowsPivotedInverse<<<launch.count, device::TILE_THREADS, device::PANEL_ROWS_PIVOTED_SMEM,
+                                                  m_stream>>>(args, pivots, tiles, launch.k0);
                 break;
             case LaunchKind::UpdatePivoted:
                 device::updatePivoted<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, pivots, tiles,
