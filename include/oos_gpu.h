@@ -83,6 +83,10 @@ typedef struct
      * pivot the reference would delay to a parent front is taken in place when its diagonal is at least 1e-3 of its
      * column maximum (info->forced), refused with OOSGPU_SOLVER below that) */
     int32_t pivoting;
+    /* FP64 (0), or mixed (1, positive definite mode only): the update matrices of the large fronts by 3xTF32 products
+     * on the tcgen05 tensor cores with FP32 accumulation (about FP32 accuracy; refine the solves in FP64). No
+     * counterpart in the reference. */
+    int32_t precision;
 } oosgpu_factor_options;
 
 /* What a factorisation found (SupernodalFactor accessors and PivotDiagnostics). */

@@ -16,7 +16,7 @@ _vp = ctypes.c_void_p
 
 class FactorOptions(ctypes.Structure):
     _fields_ = [("max_ratio", ctypes.c_double), ("bailout", ctypes.c_int32), ("reference_diagonal", _f64p),
-                ("pivoting", ctypes.c_int32)]
+                ("pivoting", ctypes.c_int32), ("precision", ctypes.c_int32)]
 
 
 class FactorInfo(ctypes.Structure):

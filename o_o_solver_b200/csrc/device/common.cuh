@@ -44,6 +44,7 @@ struct AssemblyTask
 };
 
 constexpr int TILE = 64;
+constexpr int MIXED_TILE = 128; // the tiles of the mixed-precision (tcgen05) update matrices
 constexpr int TILE_PAD = 8; // smem row stride 72 doubles: the m8n8k4 fragment loads take 2 wavefronts (no conflict)
 constexpr int TILE_THREADS = 128;
 

@@ -57,6 +57,10 @@ __global__ void panelRowsInverse(FactorArgs args, const TileTask* tasks, int k0)
 constexpr std::size_t PANEL_ROWS_INVERSE_SMEM = (2 * 64 * (TILE + TILE_PAD) + 64) * sizeof(double);
 __global__ void panelUpdate(FactorArgs args, const TileTask* tasks, int k0);
 __global__ void updateMatrix(FactorArgs args, const TileTask* tasks);
+// The mixed-precision update matrix (3xTF32 on tcgen05, mixed_kernels.cu): 128 x 128 tiles; error set to 1 when a
+// bounded wait on the tensor cores ran out.
+__global__ void updateMatrixMixed(FactorArgs args, const TileTask* tasks, int* error);
+constexpr std::size_t MIXED_UPDATE_SMEM = 2 * 4 * 128 * 16 * 4 + 1024;
 __global__ void pivotSummary(FactorArgs args, const std::int32_t* supernodeOfColumn, int dimension,
                              const double* referenceDiagonal, double maxRatio, unsigned long long* counters,
                              std::int32_t* issues, int issueCapacity, double* blockRatio, std::int32_t* blockEquation);

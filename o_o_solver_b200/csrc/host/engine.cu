@@ -114,6 +114,7 @@ public:
         m_blockRatio.allocate(summaryBlocks, "factor: ratios");
         m_blockEquation.allocate(summaryBlocks, "factor: ratio equations");
         m_structureError.allocate(1, "factor: structure check");
+        m_mixedError.allocate(1, "factor: tensor-core status");
         // Shared memory of the small-front kernel: the largest small front, square.
         const int order = m_plan.largestSmallOrder;
         m_smallSmem = static_cast<std::size_t>(order) * (order + 1) * sizeof(double);
@@ -121,6 +122,9 @@ public:
             check(cudaFuncSetAttribute(device::smallFronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(m_smallSmem)),
                   "smallFronts shared memory");
+        check(cudaFuncSetAttribute(device::updateMatrixMixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(device::MIXED_UPDATE_SMEM)),
+              "mixed update shared memory");
         check(cudaFuncSetAttribute(device::panelRowsInverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(device::PANEL_ROWS_INVERSE_SMEM)),
               "panel rows shared memory");
@@ -244,6 +248,12 @@ public:
         }
         m_pivoted = false;
         m_singular = false;
+        m_mixed = options != nullptr && options->precision == 1;
+        if (options != nullptr && options->precision != 0 && options->precision != 1)
+            throw Error(STATUS_INVALID_ARGUMENT, "FactorOptions: precision must be 0 (FP64) or 1 (mixed), found " +
+                                                     std::to_string(options->precision));
+        if (m_mixed)
+            check(cudaMemsetAsync(m_mixedError.get(), 0, sizeof(int), m_stream), "memset");
         runFactorLaunches(args);
         invertDiagonalBlocks(args);
         const unsigned summaryBlocks = blocksFor(std::max(dimension, 1), 256);
@@ -275,8 +285,18 @@ public:
         check(cudaMemcpyAsync(&structureError, m_structureError.get(), sizeof(std::int32_t), cudaMemcpyDeviceToHost,
                               m_stream),
               "download structure check");
+        int mixedError = 0;
+        if (m_mixed)
+            check(cudaMemcpyAsync(&mixedError, m_mixedError.get(), sizeof(int), cudaMemcpyDeviceToHost, m_stream),
+                  "download tensor-core status");
         check(cudaStreamSynchronize(m_stream), "factorisation");
         m_profileValid = m_profile;
+        if (mixedError != 0)
+        {
+            m_factorised = false;
+            throw Error(STATUS_INTERNAL, "mixed-precision factorisation: a bounded wait on the tensor cores ran out "
+                                         "(the update matrices are incomplete)");
+        }
         float milliseconds = 0.0f;
         check(cudaEventElapsedTime(&milliseconds, m_start, m_stop), "event time");
         m_factorised = false;
@@ -947,7 +967,15 @@ private:
         {
             if (m_profile)
                 check(cudaEventRecord(profileEvent(2 * index), m_stream), "profile event");
-            launchFactor(launch, args);
+            const std::int32_t mixed = m_mixed ? m_plan.mixedOfFactorLaunch[index] : -1;
+            if (mixed >= 0)
+            {
+                const Launch& replacement = m_plan.mixedLaunches[static_cast<std::size_t>(mixed)];
+                device::updateMatrixMixed<<<replacement.count, 256, device::MIXED_UPDATE_SMEM, m_stream>>>(
+                    args, m_tiles.get() + replacement.offset, m_mixedError.get());
+            }
+            else
+                launchFactor(launch, args);
             if (m_profile)
                 check(cudaEventRecord(profileEvent(2 * index + 1), m_stream), "profile event");
             ++index;
@@ -1065,6 +1093,8 @@ private:
     DeviceArray<double> m_blockRatio;
     DeviceArray<std::int32_t> m_blockEquation;
     DeviceArray<std::int32_t> m_structureError;
+    DeviceArray<int> m_mixedError;
+    bool m_mixed = false;
     DeviceArray<double> m_panels;
     DeviceArray<double> m_updates;
     DeviceArray<std::int64_t> m_cscOffsets;

@@ -367,7 +367,26 @@ Plan buildPlan(const Symbolic& symbolic)
             std::stable_sort(schur.begin(), schur.end(), [&](const TileTask& x, const TileTask& y)
                              { return plan.fronts[static_cast<std::size_t>(x.front)].c >
                                       plan.fronts[static_cast<std::size_t>(y.front)].c; });
+            const std::size_t at = plan.factorLaunches.size();
             addTiles(plan, plan.factorLaunches, LaunchKind::UpdateMatrix, schur);
+            // The same update matrices by 128 x 128 tiles, for the mixed-precision form.
+            std::vector<TileTask> mixed;
+            for (const std::int32_t s : large)
+            {
+                const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+                for (std::int32_t j0 = 0; j0 < f.r; j0 += device::MIXED_TILE)
+                    for (std::int32_t i0 = j0; i0 < f.r; i0 += device::MIXED_TILE)
+                        mixed.push_back({s, i0, j0, 0});
+            }
+            std::stable_sort(mixed.begin(), mixed.end(), [&](const TileTask& x, const TileTask& y)
+                             { return plan.fronts[static_cast<std::size_t>(x.front)].c >
+                                      plan.fronts[static_cast<std::size_t>(y.front)].c; });
+            if (!schur.empty() && !mixed.empty())
+            {
+                plan.mixedOfFactorLaunch.resize(plan.factorLaunches.size(), -1);
+                plan.mixedOfFactorLaunch[at] = static_cast<std::int32_t>(plan.mixedLaunches.size());
+                addTiles(plan, plan.mixedLaunches, LaunchKind::UpdateMatrixMixed, mixed);
+            }
         }
 
         // ---- factorisation, indefinite mode ----
@@ -523,6 +542,7 @@ Plan buildPlan(const Symbolic& symbolic)
         plan.backwardLaunches.insert(plan.backwardLaunches.end(), launches.begin(), launches.end());
     }
     addTiles(plan, plan.inverseLaunches, LaunchKind::InvertDiagonal, inverseTasks);
+    plan.mixedOfFactorLaunch.resize(plan.factorLaunches.size(), -1);
     return plan;
 }
 

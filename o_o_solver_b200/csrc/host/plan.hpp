@@ -46,7 +46,9 @@ enum class LaunchKind : int
     UpdatePivoted,
     LevelEnd, // the host checks the level's fronts (k0: the level) and runs the exact path where needed
     // after a factorisation: the inverses of the unit lower diagonal blocks the solves apply
-    InvertDiagonal
+    InvertDiagonal,
+    // mixed precision: the update matrices by 128 x 128 tiles on tcgen05 (3xTF32), in place of UpdateMatrix
+    UpdateMatrixMixed
 };
 
 // One batched launch: `count` items from `offset` in the array of its kind (front lists: int32; tiles: TileTask;
@@ -94,6 +96,9 @@ struct Plan
     // The 64-column diagonal blocks (front, k0) of every supernode, inverted after each factorisation into the blocks'
     // upper triangles (the solves apply the inverses).
     std::vector<Launch> inverseLaunches;
+    // Mixed precision: for each factorisation launch, the index of the launch that replaces it (-1: none).
+    std::vector<Launch> mixedLaunches;
+    std::vector<std::int32_t> mixedOfFactorLaunch;
 
     // Indefinite mode: the launches (assembly shared with the positive definite sequence), the large fronts of each
     // level, and each large front's W buffer (n x 64 values at wOffset; the fronts of one level apart, the levels

@@ -148,6 +148,9 @@ class FactorOptions:
     pivot_policy: PivotPolicy = field(default_factory=PivotPolicy)
     reference_diagonal: np.ndarray | None = None
     pivoting: str = "positive_definite"
+    # "fp64", or "mixed": the update matrices by 3xTF32 products on the tcgen05 tensor cores (about FP32 accuracy;
+    # solve_refined recovers FP64 accuracy). Not in the reference.
+    precision: str = "fp64"
 
 
 @dataclass
@@ -208,6 +211,9 @@ class SupernodalFactor:
         if options.pivoting not in ("positive_definite", "indefinite"):
             raise ValueError(f"FactorOptions.pivoting: expected positive_definite or indefinite, found {options.pivoting}")
         native.pivoting = 1 if options.pivoting == "indefinite" else 0
+        if options.precision not in ("fp64", "mixed"):
+            raise ValueError(f"FactorOptions.precision: expected fp64 or mixed, found {options.precision}")
+        native.precision = 1 if options.precision == "mixed" else 0
         self._reference = None
         if options.reference_diagonal is not None:
             self._reference = np.ascontiguousarray(options.reference_diagonal, dtype=np.float64)
