@@ -155,6 +155,10 @@ typedef struct
 {
     double tolerance;  /* on the normwise backward error; default 1e-10 */
     int32_t max_steps; /* default 10 */
+    /* 0: each correction is one solve (classical refinement); k in [1, 12]: each correction solves
+     * A^-1-preconditioned A d = r by GMRES with at most k Krylov vectors (GMRES-IR, for a factor less accurate than
+     * the matrix's conditioning needs, e.g. the mixed-precision form). No counterpart in the reference. */
+    int32_t krylov;
 } oosgpu_refine_options;
 typedef struct
 {

@@ -38,7 +38,7 @@ class FactorInfo(ctypes.Structure):
 
 
 class RefineOptions(ctypes.Structure):
-    _fields_ = [("tolerance", ctypes.c_double), ("max_steps", ctypes.c_int32)]
+    _fields_ = [("tolerance", ctypes.c_double), ("max_steps", ctypes.c_int32), ("krylov", ctypes.c_int32)]
 
 
 class RefineInfo(ctypes.Structure):

@@ -93,6 +93,18 @@ __global__ void residualRows(const std::int64_t* rowStart, const std::int32_t* c
                              int dimension, double* norms);
 __global__ void addRows(double* x, const double* r, std::int64_t count);
 
+// The GMRES refinement (gmres_kernels.cu).
+constexpr int GMRES_MAX_VECTORS = 12; // the Krylov vectors of one correction
+__global__ void multiplyRows(const std::int64_t* rowStart, const std::int32_t* columns, const std::int32_t* source,
+                             const double* values, const double* x, double* y, int width, int dimension);
+__global__ void dotRowsPartials(const double* v, std::int64_t stride, int vectors, const double* w, int width,
+                                int dimension, int rowsPerBlock, double* partials);
+__global__ void subtractRowsCombination(double* w, const double* v, std::int64_t stride, int vectors,
+                                        const double* coef, int width, std::int64_t items);
+__global__ void addRowsCombination(double* x, const double* v, std::int64_t stride, int vectors, const double* y,
+                                   int width, std::int64_t items);
+__global__ void scaleRowsColumns(const double* in, double* out, const double* s, int width, std::int64_t items);
+
 __global__ void smallFrontsPivoted(FactorArgs args, PivotArgs pivots, const std::int32_t* list,
                                    std::int32_t* structureError);
 __global__ void pivotedDiagonal(FactorArgs args, PivotArgs pivots, const std::int32_t* list, int k0);

@@ -42,6 +42,8 @@ constexpr int NO_PIVOT = 0x7f7f7f7f; // the byte pattern 0x7f: "no zero pivot"
 constexpr int ISSUE_CAPACITY = 1 << 16;
 constexpr int SOLVE_WIDTH = 64;
 constexpr int SMALL_THREADS = 256;
+// The relative fall of each column's preconditioned residual that ends a GMRES correction.
+constexpr double GMRES_INNER_TOLERANCE = 1.0e-4;
 
 // A device allocation owned by the factor.
 template <typename T> class DeviceArray
@@ -752,14 +754,156 @@ public:
 
     // X = A^-1 B refined in FP64 until every column's normwise backward error ||b - A x||_inf / (||A||_inf ||x||_inf +
     // ||b||_inf) is at most `tolerance` or maxSteps corrections were made; B and X column-major (host or device).
+    // Per-column inner products of `vectors` row blocks v_i (stride values apart) with w: out[i * width + c].
+    void dotRows(const double* v, std::int64_t stride, int vectors, const double* w, int width, std::vector<double>& out)
+    {
+        const std::int32_t n = m_plan.dimension;
+        const int blocks = std::clamp((n + 1023) / 1024, 1, 592);
+        const int rowsPerBlock = (n + blocks - 1) / blocks;
+        const std::size_t count = static_cast<std::size_t>(vectors) * static_cast<std::size_t>(width);
+        m_gmresPartials.allocate(count * static_cast<std::size_t>(blocks), "refinement: partial sums");
+        m_gmresValues.allocate(static_cast<std::size_t>(device::GMRES_MAX_VECTORS) * 64, "refinement: coefficients");
+        device::dotRowsPartials<<<blocks, 256, 0, m_stream>>>(v, stride, vectors, w, width, n, rowsPerBlock,
+                                                               m_gmresPartials.get());
+        device::reducePartials<<<blocksFor(static_cast<std::int64_t>(count), 128), 128, 0, m_stream>>>(
+            m_gmresPartials.get(), blocks, static_cast<int>(count), m_gmresValues.get());
+        check(cudaGetLastError(), "refinement inner products");
+        out.resize(count);
+        check(cudaMemcpyAsync(out.data(), m_gmresValues.get(), count * sizeof(double), cudaMemcpyDeviceToHost, m_stream),
+              "download inner products");
+        check(cudaStreamSynchronize(m_stream), "refinement inner products");
+    }
+
+    // Uploads per-column coefficients (vectors x width) for the combination kernels.
+    const double* uploadCoefficients(const std::vector<double>& values)
+    {
+        m_gmresCoefficients.allocate(static_cast<std::size_t>(device::GMRES_MAX_VECTORS) * 64,
+                                     "refinement: coefficients");
+        check(cudaMemcpyAsync(m_gmresCoefficients.get(), values.data(), values.size() * sizeof(double),
+                              cudaMemcpyHostToDevice, m_stream),
+              "upload coefficients");
+        check(cudaStreamSynchronize(m_stream), "upload coefficients");
+        return m_gmresCoefficients.get();
+    }
+
+    // One GMRES correction of the tile in x (rows, `width` columns), the residual b - A x in m_rRows: each column's
+    // system M^-1 A d = M^-1 r (M^-1 the factor's solve) by GMRES with at most `krylov` vectors, the basis
+    // orthogonalised by classical Gram-Schmidt twice, the Hessenberg matrix reduced by Givens rotations on the host;
+    // it ends when every column's preconditioned residual has fallen by innerTolerance, then x += V y.
+    void gmresCorrection(double* x, int width, int krylov, double innerTolerance)
+    {
+        const std::int32_t n = m_plan.dimension;
+        const std::int64_t items = static_cast<std::int64_t>(n) * width;
+        const std::int64_t stride = items;
+        const auto w = static_cast<std::size_t>(width);
+        const auto m = static_cast<std::size_t>(krylov);
+        m_krylov.allocate(static_cast<std::size_t>(krylov + 1) * static_cast<std::size_t>(items), "refinement: Krylov");
+        double* basis = m_krylov.get();
+        const unsigned elementBlocks = blocksFor(items, 256);
+        check(cudaMemcpyAsync(basis, m_rRows.get(), static_cast<std::size_t>(items) * sizeof(double),
+                              cudaMemcpyDeviceToDevice, m_stream),
+              "copy residual");
+        sweeps(basis, width);
+        std::vector<double> values;
+        dotRows(basis, stride, 1, basis, width, values);
+        std::vector<double> beta(w);
+        std::vector<double> inverse(w);
+        for (std::size_t c = 0; c < w; ++c)
+        {
+            beta[c] = std::sqrt(std::max(values[c], 0.0));
+            inverse[c] = beta[c] > 0.0 ? 1.0 / beta[c] : 0.0;
+        }
+        device::scaleRowsColumns<<<elementBlocks, 256, 0, m_stream>>>(basis, basis, uploadCoefficients(inverse), width,
+                                                                       items);
+        // Per column: H (m + 1) x m by columns, the rotations, the rotated right-hand side g.
+        std::vector<double> h(w * (m + 1) * m, 0.0);
+        std::vector<double> cs(w * m, 0.0);
+        std::vector<double> sn(w * m, 0.0);
+        std::vector<double> g(w * (m + 1), 0.0);
+        const auto H = [&](std::size_t c, std::size_t i, std::size_t j) -> double& { return h[(c * m + j) * (m + 1) + i]; };
+        for (std::size_t c = 0; c < w; ++c)
+            g[c * (m + 1)] = beta[c];
+        std::size_t used = 0;
+        constexpr int WARPS = 8;
+        const unsigned rowBlocks = std::min<unsigned>(blocksFor(n, WARPS), 148u * 8u);
+        for (std::size_t j = 0; j < m; ++j)
+        {
+            double* vj = basis + static_cast<std::int64_t>(j) * stride;
+            double* next = basis + static_cast<std::int64_t>(j + 1) * stride;
+            device::multiplyRows<<<rowBlocks, 32 * WARPS, 0, m_stream>>>(m_fullStart.get(), m_fullColumns.get(),
+                                                                         m_fullSource.get(), m_matrixValues, vj, next,
+                                                                         width, n);
+            sweeps(next, width);
+            for (int pass = 0; pass < 2; ++pass)
+            {
+                dotRows(basis, stride, static_cast<int>(j + 1), next, width, values);
+                device::subtractRowsCombination<<<elementBlocks, 256, 0, m_stream>>>(
+                    next, basis, stride, static_cast<int>(j + 1), uploadCoefficients(values), width, items);
+                for (std::size_t i = 0; i <= j; ++i)
+                    for (std::size_t c = 0; c < w; ++c)
+                        H(c, i, j) += values[i * w + c];
+            }
+            dotRows(next, stride, 1, next, width, values);
+            for (std::size_t c = 0; c < w; ++c)
+            {
+                const double norm = std::sqrt(std::max(values[c], 0.0));
+                H(c, j + 1, j) = norm;
+                inverse[c] = norm > 0.0 ? 1.0 / norm : 0.0;
+            }
+            device::scaleRowsColumns<<<elementBlocks, 256, 0, m_stream>>>(next, next, uploadCoefficients(inverse),
+                                                                           width, items);
+            used = j + 1;
+            double worst = 0.0;
+            for (std::size_t c = 0; c < w; ++c)
+            {
+                for (std::size_t i = 0; i < j; ++i)
+                {
+                    const double t = cs[c * m + i] * H(c, i, j) + sn[c * m + i] * H(c, i + 1, j);
+                    H(c, i + 1, j) = -sn[c * m + i] * H(c, i, j) + cs[c * m + i] * H(c, i + 1, j);
+                    H(c, i, j) = t;
+                }
+                const double a = H(c, j, j);
+                const double b = H(c, j + 1, j);
+                const double r = std::hypot(a, b);
+                cs[c * m + j] = r > 0.0 ? a / r : 1.0;
+                sn[c * m + j] = r > 0.0 ? b / r : 0.0;
+                H(c, j, j) = r;
+                H(c, j + 1, j) = 0.0;
+                g[c * (m + 1) + j + 1] = -sn[c * m + j] * g[c * (m + 1) + j];
+                g[c * (m + 1) + j] = cs[c * m + j] * g[c * (m + 1) + j];
+                if (beta[c] > 0.0)
+                    worst = std::max(worst, std::abs(g[c * (m + 1) + j + 1]) / beta[c]);
+            }
+            if (worst <= innerTolerance)
+                break;
+        }
+        // y from the triangular H, then x += V y.
+        std::vector<double> y(used * w, 0.0);
+        for (std::size_t c = 0; c < w; ++c)
+            for (std::size_t i = used; i-- > 0;)
+            {
+                double sum = g[c * (m + 1) + i];
+                for (std::size_t q = i + 1; q < used; ++q)
+                    sum -= H(c, i, q) * y[q * w + c];
+                y[i * w + c] = H(c, i, i) != 0.0 ? sum / H(c, i, i) : 0.0;
+            }
+        device::addRowsCombination<<<elementBlocks, 256, 0, m_stream>>>(x, basis, stride, static_cast<int>(used),
+                                                                         uploadCoefficients(y), width, items);
+        check(cudaGetLastError(), "GMRES correction");
+    }
+
     void solveRefined(const double* b, std::int64_t ldb, double* x, std::int64_t ldx, std::int64_t columns,
-                      bool onDevice, double tolerance, int maxSteps, oosgpu_refine_info* info)
+                      bool onDevice, double tolerance, int maxSteps, oosgpu_refine_info* info, int krylov = 0)
     {
         check(cudaSetDevice(m_device), "cudaSetDevice");
         requireSolvable();
         const std::int32_t n = m_plan.dimension;
         if (ldb < n || ldx < n || columns < 0 || maxSteps < 0)
             throw Error(STATUS_INVALID_ARGUMENT, "refinement: leading dimensions below the rows, or negative counts");
+        if (krylov < 0 || krylov > device::GMRES_MAX_VECTORS)
+            throw Error(STATUS_INVALID_ARGUMENT, "refinement: the Krylov vectors of a GMRES correction must be in [0, " +
+                                                     std::to_string(device::GMRES_MAX_VECTORS) + "], found " +
+                                                     std::to_string(krylov));
         oosgpu_refine_info result{};
         if (columns == 0 || n == 0)
         {
@@ -834,6 +978,11 @@ public:
                     result.residual = std::max(result.residual, worstResidual);
                     result.backward_error = std::max(result.backward_error, worst);
                     break;
+                }
+                if (krylov > 0)
+                {
+                    gmresCorrection(m_work.get(), width, krylov, GMRES_INNER_TOLERANCE);
+                    continue;
                 }
                 sweeps(m_rRows.get(), width);
                 device::addRows<<<blocksFor(items, 256), 256, 0, m_stream>>>(m_work.get(), m_rRows.get(), items);
@@ -1094,6 +1243,10 @@ private:
     DeviceArray<std::int32_t> m_blockEquation;
     DeviceArray<std::int32_t> m_structureError;
     DeviceArray<int> m_mixedError;
+    DeviceArray<double> m_krylov;
+    DeviceArray<double> m_gmresPartials;
+    DeviceArray<double> m_gmresValues;
+    DeviceArray<double> m_gmresCoefficients;
     bool m_mixed = false;
     DeviceArray<double> m_panels;
     DeviceArray<double> m_updates;
@@ -1745,7 +1898,8 @@ extern "C" int oosgpu_solve_refined(oosgpu_factor* factor, const double* b, int6
             requirePointer(factor, "factor");
             const double tolerance = options != nullptr ? options->tolerance : 1.0e-10;
             const int steps = options != nullptr ? options->max_steps : 10;
-            factor->factor->solveRefined(b, ldb, x, ldx, columns, false, tolerance, steps, info);
+            const int krylov = options != nullptr ? options->krylov : 0;
+            factor->factor->solveRefined(b, ldb, x, ldx, columns, false, tolerance, steps, info, krylov);
         });
 }
 
@@ -1759,7 +1913,8 @@ extern "C" int oosgpu_solve_refined_device(oosgpu_factor* factor, const double* 
             requirePointer(factor, "factor");
             const double tolerance = options != nullptr ? options->tolerance : 1.0e-10;
             const int steps = options != nullptr ? options->max_steps : 10;
-            factor->factor->solveRefined(b, ldb, x, ldx, columns, true, tolerance, steps, info);
+            const int krylov = options != nullptr ? options->krylov : 0;
+            factor->factor->solveRefined(b, ldb, x, ldx, columns, true, tolerance, steps, info, krylov);
         });
 }
 

@@ -367,15 +367,17 @@ class RefinementInfo:
     backward_error: float
 
 
-def solve_refined(factor: SupernodalFactor, b, x, tolerance: float = 1.0e-10, max_steps: int = 10) -> RefinementInfo:
+def solve_refined(factor: SupernodalFactor, b, x, tolerance: float = 1.0e-10, max_steps: int = 10,
+                  krylov: int = 0) -> RefinementInfo:
     """X = A^-1 B refined in FP64 on the device until every column's normwise backward error is at most `tolerance`
-    (oosgpu_solve_refined): B and X float64, both host (column-major) or both device tensors."""
+    (oosgpu_solve_refined): B and X float64, both host (column-major) or both device tensors. krylov > 0: each
+    correction by GMRES with at most that many Krylov vectors, the factor's solve as preconditioner (GMRES-IR)."""
     lib = nat.load()
     n, k, ldb = _block_layout(b)
     nx, kx, ldx = _block_layout(x)
     if (n, k) != (nx, kx):
         raise ValueError("solve_refined: B and X differ in shape")
-    options = nat.RefineOptions(tolerance, max_steps)
+    options = nat.RefineOptions(tolerance, max_steps, krylov)
     info = nat.RefineInfo()
     if isinstance(b, np.ndarray):
         if b.dtype != np.float64 or x.dtype != np.float64:
