@@ -17,6 +17,10 @@ The line's `modes` object is the other half of the metric: the lowest 20 modes o
 (669,780 equations) by the GPU block shift-invert Lanczos (block 8), wall seconds of the whole solve (factorisations,
 Lanczos runs, Sturm checks), its eigenvalues against the reference's recorded ones (tests/golden/modes), its e2e
 through the public API from host arrays, and the reference beside it on the 30^3 block (a bounded CPU sample).
+
+`forms.mixed` is the mixed-precision form on the same plate: the factorisation with its update matrices by 3xTF32
+products on the tcgen05 tensor cores, the rate of that kernel beside the FP64 one, and FP64 GMRES refinement of its
+solves (8 Krylov vectors, at most 3 corrections) with the backward error it reaches.
 """
 
 from __future__ import annotations
@@ -56,6 +60,7 @@ def parse():
     parser.add_argument("--modes-workload", choices=["hex60", "hex30", "hex14", "none"], default="hex60",
                         help="the modes leg: the lowest 20 modes of the n^3 hexahedral block, block size 8")
     parser.add_argument("--modes-steps", type=int, default=2)
+    parser.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
     return parser.parse_args()
 
 
@@ -286,6 +291,43 @@ def modes_leg(args, device, rank, world):
     return out
 
 
+def mixed_leg(factor, d_csc, d_loads, d_x, fp64_stats, tolerance, dev, torch):
+    """The mixed-precision form on the same plate: the factorisation with its update matrices by 3xTF32 products on
+    tcgen05 (device seconds, that kernel's rate beside the FP64 one), then FP64 refinement by GMRES corrections (8
+    Krylov vectors, at most 3 corrections): the backward error it reaches and the time, against the FP64 solution."""
+    from o_o_solver_b200 import FactorOptions, linalg
+
+    options = FactorOptions(precision="mixed")
+    factor.profile(True)
+    factor.refactorise(d_csc, options)
+    factor.refactorise(d_csc, options)
+    stats = factor.kernel_stats()
+    factor.profile(False)
+    factor.refactorise(d_csc, options)
+    factor_seconds = factor.device_seconds
+    reference = d_x.clone()
+    x = torch.empty_like(d_x)
+    start = time.perf_counter()
+    info = linalg.solve_refined(factor, d_loads.t(), x.t(), tolerance=tolerance, max_steps=3, krylov=8)
+    torch.cuda.synchronize()
+    refine_seconds = time.perf_counter() - start
+    difference = float(((x - reference).norm(dim=1) / reference.norm(dim=1)).max())
+    um, um64 = stats["update_matrix"], fp64_stats["update_matrix"]
+    factor.refactorise(d_csc)  # the FP64 factor back
+    return {
+        "factor_device_s": factor_seconds,
+        "update_matrix": {"mixed_ms": round(um["seconds"] * 1e3, 3),
+                          "mixed_tflops": round(um["flops"] / um["seconds"] / 1e12, 2),
+                          "fp64_ms": round(um64["seconds"] * 1e3, 3),
+                          "fp64_tflops": round(um64["flops"] / um64["seconds"] / 1e12, 2),
+                          "kernel": "updateMatrixMixed: tcgen05.mma kind::tf32, 3 products, TMEM accumulator"},
+        "gmres_ir": {"krylov": 8, "corrections": info.steps, "backward_error": info.backward_error,
+                     "reaches_tolerance": bool(info.backward_error <= tolerance), "seconds": refine_seconds,
+                     "max_rel_difference_vs_fp64_solution": difference},
+        "step_s": factor_seconds + refine_seconds,
+    }
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -446,6 +488,7 @@ def run_gpu(args, rank, world, local_rank):
             baseline = {"value": None, "unit": "s", "cores": 0, "kind": "reference", "sample": f"unavailable: {error}"}
 
     modes = modes_leg(args, local_rank, rank, world) if args.modes_workload != "none" else None
+    mixed = None if args.no_mixed else mixed_leg(factor, d_csc, d_loads, d_x, stats, args.tolerance, dev, torch)
 
     if rank == 0:
         line = {
@@ -459,7 +502,7 @@ def run_gpu(args, rank, world, local_rank):
                        "parallelism": f"replicas x{world}"},
             "residual": resid, "backward_error": backward, "refinement": refinement, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "kernels": kernel_table, "clocks": clocks.summary(), "cpu_baseline": baseline,
-            "factor_tflops": symbolic.flop_count / seconds / 1e12, "modes": modes,
+            "factor_tflops": symbolic.flop_count / seconds / 1e12, "modes": modes, "forms": {"mixed": mixed},
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -120,10 +120,14 @@ public:
         // Shared memory of the small-front kernel: the largest small front, square.
         const int order = m_plan.largestSmallOrder;
         m_smallSmem = static_cast<std::size_t>(order) * (order + 1) * sizeof(double);
-        if (m_smallSmem > 48 * 1024)
-            check(cudaFuncSetAttribute(device::smallFronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(m_smallSmem)),
-                  "smallFronts shared memory");
+        // A kernel's shared-memory limit is the process's, not this factor's: every factor sets the largest any plan
+        // can need, so that no factor lowers another's.
+        const auto smallLimit = static_cast<int>(static_cast<std::size_t>(SMALL_ORDER) * (SMALL_ORDER + 1) * sizeof(double));
+        check(cudaFuncSetAttribute(device::smallFronts, cudaFuncAttributeMaxDynamicSharedMemorySize, smallLimit),
+              "smallFronts shared memory");
+        check(cudaFuncSetAttribute(device::smallFrontsPivoted, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   smallLimit),
+              "smallFrontsPivoted shared memory");
         check(cudaFuncSetAttribute(device::updateMatrixMixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(device::MIXED_UPDATE_SMEM)),
               "mixed update shared memory");
@@ -394,13 +398,6 @@ public:
         m_rowsPivot.allocate(static_cast<std::size_t>(std::max<std::int64_t>(m_plan.rowEntries, 1)), "indefinite: rows");
         m_relposPivot.allocate(static_cast<std::size_t>(std::max<std::int64_t>(m_plan.rowEntries, 1)),
                                "indefinite: positions");
-        if (!m_pivotedSmemSet && m_smallSmem > 48 * 1024)
-        {
-            check(cudaFuncSetAttribute(device::smallFrontsPivoted, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(m_smallSmem)),
-                  "smallFrontsPivoted shared memory");
-            m_pivotedSmemSet = true;
-        }
         device::PivotArgs pivots{m_perm.get(),  m_subdiagonal.get(), m_status.get(),    m_stepPerm.get(),
                                  m_stepSwapped.get(), m_w.get(),    m_wOffset.get(),   m_frontPerm.get(),
                                  m_frontSub.get()};
@@ -1119,9 +1116,11 @@ private:
             const std::int32_t mixed = m_mixed ? m_plan.mixedOfFactorLaunch[index] : -1;
             if (mixed >= 0)
             {
+                check(cudaGetLastError(), "factorisation launch before the mixed update");
                 const Launch& replacement = m_plan.mixedLaunches[static_cast<std::size_t>(mixed)];
                 device::updateMatrixMixed<<<replacement.count, 256, device::MIXED_UPDATE_SMEM, m_stream>>>(
                     args, m_tiles.get() + replacement.offset, m_mixedError.get());
+                check(cudaGetLastError(), "mixed update launch");
             }
             else
                 launchFactor(launch, args);
@@ -1274,7 +1273,6 @@ private:
     DeviceArray<std::int32_t> m_relposPivot;
     bool m_pivoted = false;
     bool m_singular = false;
-    bool m_pivotedSmemSet = false;
     std::int64_t m_exactFronts = 0;
     const double* m_solveScale = nullptr;
     DeviceArray<double> m_hostX;

@@ -189,13 +189,11 @@ public:
                                                      " columns is wider than the products by rows allow (" +
                                                      std::to_string(MAX_SHARED_BYTES / device::COMBINE_ROWS / 8) +
                                                      "); lower the modes per shift or the block size");
-        if (shared > m_combineShared)
-        {
+        if (shared > 48 * 1024)
+            // The limit is the process's: the largest, so that no solve lowers another's.
             check(cudaFuncSetAttribute(device::combineRows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(shared)),
+                                       static_cast<int>(MAX_SHARED_BYTES)),
                   "Lanczos: shared memory of the basis products");
-            m_combineShared = shared;
-        }
         device::combineRows<<<blocksFor(m_rows, device::COMBINE_ROWS), device::COMBINE_THREADS, shared, m_stream>>>(
             a, lda, static_cast<int>(m), s, lds, static_cast<int>(k), out, ldo, m_rows, next, ldn,
             static_cast<int>(b), correction);
@@ -271,7 +269,6 @@ private:
     int m_blocks = 1;
     int m_rowsPerBlock = 1;
     Scratch m_partials;
-    std::size_t m_combineShared = 48 * 1024;
     std::int64_t m_launches = 0;
 };
 
