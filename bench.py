@@ -364,13 +364,9 @@ def run_gpu(args, rank, world, local_rank):
     from o_o_solver_b200 import FactorSolve, SupernodalFactor, SymbolicFactor, SymmetricCsc, linalg, workloads
 
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-        from datetime import timedelta
+    from o_o_solver_b200.replicas import Replicas
 
-        dist = dist_mod
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local_rank))
+    replicas = Replicas("nccl", timeout_s=600.0, device=torch.device("cuda", local_rank))
 
     model, fixture, csc, loads = load_workload(args.workload)
     n = csc.dimension
@@ -401,8 +397,7 @@ def run_gpu(args, rank, world, local_rank):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
@@ -412,14 +407,9 @@ def run_gpu(args, rank, world, local_rank):
             step()
         stop.record(stream)
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
-    seconds = start.elapsed_time(stop) / 1e3 / args.steps
-    if dist:
-        t = torch.tensor([seconds], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        seconds = float(t.item())
+    seconds = replicas.slowest(start.elapsed_time(stop) / 1e3 / args.steps)
 
     # Residual of the last step's solutions (host check of the device's own test).
     x = d_x.t().cpu().numpy()
@@ -505,9 +495,7 @@ def run_gpu(args, rank, world, local_rank):
             "factor_tflops": symbolic.flop_count / seconds / 1e12, "modes": modes, "forms": {"mixed": mixed},
         }
         print(json.dumps(line), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.close()
 
 
 def main():

@@ -12,7 +12,9 @@
 #include "oos/linalg/dense/KernelSelection.hpp"
 #include "oos/linalg/eigen/BlockLanczos.hpp"
 #include "oos/linalg/eigen/PencilScaling.hpp"
+#include "oos/linalg/eigen/ShiftStrategy.hpp"
 #include "oos/linalg/eigen/SparsePencil.hpp"
+#include "oos/linalg/eigen/SturmCheck.hpp"
 #include "oos/linalg/ordering/ConstrainedOrdering.hpp"
 #include "oos/linalg/ordering/NodeGraph.hpp"
 #include "oos/linalg/ordering/NodePermutation.hpp"
@@ -387,5 +389,52 @@ extern "C" int ref_pencil_scale(int32_t dimension, const int64_t* col_offsets, c
                 std::span<const std::int32_t>(rows, terms), std::span<const double>(values, terms), budget);
             const auto scales = pencilScaleOf(k, budget);
             std::copy(scales.span().begin(), scales.span().end(), scale);
+        });
+}
+
+extern "C" int ref_sturm_verify(int64_t points, const double* shifts, const int64_t* counts, int64_t values,
+                                const double* sorted, double result[6])
+{
+    return guarded(
+        [&]
+        {
+            SturmCheck sturm;
+            for (int64_t k = 0; k < points; ++k)
+                sturm.addPoint({shifts[k], static_cast<std::size_t>(counts[k])});
+            const SturmVerification v =
+                sturm.verify(std::span<const double>(sorted, static_cast<std::size_t>(values)));
+            result[0] = v.verifiedUpTo;
+            result[1] = static_cast<double>(v.verifiedCount);
+            result[2] = v.hasMismatch ? 1.0 : 0.0;
+            result[3] = v.mismatch.lower;
+            result[4] = v.mismatch.upper;
+            result[5] = static_cast<double>(v.mismatch.expectedCount) * 1e6 + static_cast<double>(v.mismatch.foundCount);
+        });
+}
+
+extern "C" int ref_shift_next(double lower, double upper, int64_t mode_count, double scale, const double verification[6],
+                              int64_t values, const double* sorted, int64_t ritz_count, const double* ritz,
+                              int64_t shift_count, const double* lanczos_shifts, double* shift, int32_t* purpose)
+{
+    return guarded(
+        [&]
+        {
+            EigenRequest request;
+            request.lowerBound = lower;
+            request.upperBound = upper;
+            request.modeCount = static_cast<std::size_t>(mode_count);
+            const ShiftStrategy strategy(request, scale);
+            SturmVerification v;
+            v.verifiedUpTo = verification[0];
+            v.verifiedCount = static_cast<std::size_t>(verification[1]);
+            v.hasMismatch = verification[2] != 0.0;
+            v.mismatch.lower = verification[3];
+            v.mismatch.upper = verification[4];
+            const ShiftChoice choice = strategy.nextShift(
+                v, std::span<const double>(sorted, static_cast<std::size_t>(values)),
+                std::span<const double>(ritz, static_cast<std::size_t>(ritz_count)),
+                std::span<const double>(lanczos_shifts, static_cast<std::size_t>(shift_count)));
+            *shift = choice.shift;
+            *purpose = static_cast<int32_t>(choice.purpose);
         });
 }

@@ -72,6 +72,16 @@ int ref_modes(const ref_symbolic* s, int32_t dimension, const int64_t* col_offse
               int64_t capacity, double* eigenvectors, double* shifts, int64_t max_shifts, int64_t counts[5],
               double* seconds);
 
+/* SturmCheck::addPoint + verify (src/linalg/eigen/SturmCheck.cpp): result = verifiedUpTo, verifiedCount,
+ * hasMismatch, mismatch.lower, mismatch.upper, expected * 1e6 + found. */
+int ref_sturm_verify(int64_t points, const double* shifts, const int64_t* counts, int64_t values, const double* sorted,
+                     double result[6]);
+/* ShiftStrategy(request, scale).nextShift (src/linalg/eigen/ShiftStrategy.cpp:121-193); verification as
+ * ref_sturm_verify's result. */
+int ref_shift_next(double lower, double upper, int64_t mode_count, double scale, const double verification[6],
+                   int64_t values, const double* sorted, int64_t ritz_count, const double* ritz, int64_t shift_count,
+                   const double* lanczos_shifts, double* shift, int32_t* purpose);
+
 /* pencilScaleOf (src/linalg/eigen/PencilScaling.cpp:64-80): the power-of-two scales of a stiffness CSC. */
 int ref_pencil_scale(int32_t dimension, const int64_t* col_offsets, const int32_t* rows, const double* values,
                      double* scale);
