@@ -260,6 +260,23 @@ const double* oosgpu_modes_vectors_device(const oosgpu_modes* modes);
 int oosgpu_modes_shifts(const oosgpu_modes* modes, double* records);
 void oosgpu_modes_destroy(oosgpu_modes* modes);
 
+/* ---- the host logic of the shift-invert Lanczos, exposed for its callers and its tests (no device needed) ---- */
+
+/* SmallEigenSolver over a symmetric p x p matrix (src/linalg/dense/SmallEigenSolver.cpp): eigenvalues increasing,
+ * eigenvectors as columns (p x p, leading dimension p), each signed so that its first component of largest magnitude
+ * is positive. `a` is read in its lower triangle, column-major with leading dimension ld. */
+int oosgpu_symmetric_eigen(const double* a, int64_t p, int64_t ld, double* eigenvalues, double* eigenvectors);
+/* SturmCheck::addPoint for each (shift, count) then verify (src/linalg/eigen/SturmCheck.cpp) against the sorted
+ * eigenvalues found: result = verified up to, verified count, has mismatch (0/1), mismatch lower, mismatch upper,
+ * expected count * 1e6 + found count. */
+int oosgpu_sturm_verify(int64_t points, const double* shifts, const int64_t* counts, int64_t values,
+                        const double* sorted, double result[6]);
+/* ShiftStrategy(request, scale).nextShift (src/linalg/eigen/ShiftStrategy.cpp:121-193): verification in
+ * oosgpu_sturm_verify's layout; purpose as in oosgpu_modes_shifts. */
+int oosgpu_shift_next(double lower, double upper, int64_t mode_count, double scale, const double verification[6],
+                      int64_t values, const double* sorted, int64_t ritz_count, const double* ritz,
+                      int64_t shift_count, const double* lanczos_shifts, double* shift, int32_t* purpose);
+
 /* ---- model-side helpers (no counterpart in the reference's linalg: they stand in for its assembly and DOF
  *      selection, src/assembly and SymmetricCsc::fromBlocks, src/linalg/sparse/SymmetricCsc.cpp:41) ---------------- */
 typedef struct oosgpu_model oosgpu_model;

@@ -104,6 +104,11 @@ SIGNATURES = [
     ("oosgpu_modes_vectors_device", _vp, [_vp]),
     ("oosgpu_modes_shifts", ctypes.c_int, [_vp, _f64p]),
     ("oosgpu_modes_destroy", None, [_vp]),
+    ("oosgpu_symmetric_eigen", ctypes.c_int, [_f64p, ctypes.c_int64, ctypes.c_int64, _f64p, _f64p]),
+    ("oosgpu_sturm_verify", ctypes.c_int, [ctypes.c_int64, _f64p, _i64p, ctypes.c_int64, _f64p, _f64p]),
+    ("oosgpu_shift_next", ctypes.c_int, [ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_double, _f64p,
+                                         ctypes.c_int64, _f64p, ctypes.c_int64, _f64p, ctypes.c_int64, _f64p,
+                                         _f64p, _i32p]),
     ("oosgpu_model_plate", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                           ctypes.POINTER(_vp)]),

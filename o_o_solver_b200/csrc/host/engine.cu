@@ -2143,3 +2143,105 @@ extern "C" void oosgpu_modes_destroy(oosgpu_modes* modes)
 {
     delete modes;
 }
+
+namespace
+{
+
+oosgpu::eigen::SturmVerification verificationFrom(const double v[6])
+{
+    oosgpu::eigen::SturmVerification verification;
+    verification.verifiedUpTo = v[0];
+    verification.verifiedCount = static_cast<std::size_t>(v[1]);
+    verification.hasMismatch = v[2] != 0.0;
+    verification.mismatch.lower = v[3];
+    verification.mismatch.upper = v[4];
+    return verification;
+}
+
+std::span<const double> valuesOf(const double* values, int64_t count, const char* name)
+{
+    if (count < 0)
+        throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT, std::string(name) + ": a negative count");
+    if (count > 0)
+        requirePointer(values, name);
+    return {values, static_cast<std::size_t>(count)};
+}
+
+} // namespace
+
+extern "C" int oosgpu_symmetric_eigen(const double* a, int64_t p, int64_t ld, double* eigenvalues,
+                                      double* eigenvectors)
+{
+    return guarded(
+        [&]
+        {
+            if (p < 0 || ld < std::max<int64_t>(p, 1))
+                throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT,
+                                    "symmetric eigenproblem: expected an order >= 0 and a leading dimension >= it");
+            if (p == 0)
+                return;
+            requirePointer(a, "a");
+            requirePointer(eigenvalues, "eigenvalues");
+            requirePointer(eigenvectors, "eigenvectors");
+            std::vector<double> values;
+            std::vector<double> vectors;
+            oosgpu::eigen::decomposeSymmetric(a, static_cast<std::size_t>(p), static_cast<std::size_t>(ld), values,
+                                              vectors);
+            std::copy(values.begin(), values.end(), eigenvalues);
+            std::copy(vectors.begin(), vectors.end(), eigenvectors);
+        });
+}
+
+extern "C" int oosgpu_sturm_verify(int64_t points, const double* shifts, const int64_t* counts, int64_t values,
+                                   const double* sorted, double result[6])
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(result, "result");
+            const std::span<const double> shiftSpan = valuesOf(shifts, points, "shifts");
+            if (points > 0)
+                requirePointer(counts, "counts");
+            oosgpu::eigen::SturmCheck sturm;
+            for (std::size_t k = 0; k < shiftSpan.size(); ++k)
+            {
+                if (counts[k] < 0)
+                    throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT, "Sturm point: a negative count");
+                sturm.addPoint({shiftSpan[k], static_cast<std::size_t>(counts[k])});
+            }
+            const oosgpu::eigen::SturmVerification v = sturm.verify(valuesOf(sorted, values, "sorted"));
+            result[0] = v.verifiedUpTo;
+            result[1] = static_cast<double>(v.verifiedCount);
+            result[2] = v.hasMismatch ? 1.0 : 0.0;
+            result[3] = v.mismatch.lower;
+            result[4] = v.mismatch.upper;
+            result[5] = static_cast<double>(v.mismatch.expectedCount) * 1e6 +
+                        static_cast<double>(v.mismatch.foundCount);
+        });
+}
+
+extern "C" int oosgpu_shift_next(double lower, double upper, int64_t mode_count, double scale,
+                                 const double verification[6], int64_t values, const double* sorted,
+                                 int64_t ritz_count, const double* ritz, int64_t shift_count,
+                                 const double* lanczos_shifts, double* shift, int32_t* purpose)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(verification, "verification");
+            requirePointer(shift, "shift");
+            requirePointer(purpose, "purpose");
+            if (mode_count < 0)
+                throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT, "eigenvalue request: a negative mode count");
+            oosgpu::eigen::EigenRequest request;
+            request.lowerBound = lower;
+            request.upperBound = upper;
+            request.modeCount = static_cast<std::size_t>(mode_count);
+            const oosgpu::eigen::ShiftStrategy strategy(request, scale);
+            const oosgpu::eigen::ShiftChoice choice = strategy.nextShift(
+                verificationFrom(verification), valuesOf(sorted, values, "sorted"), valuesOf(ritz, ritz_count, "ritz"),
+                valuesOf(lanczos_shifts, shift_count, "lanczos shifts"));
+            *shift = choice.shift;
+            *purpose = static_cast<int32_t>(choice.purpose);
+        });
+}

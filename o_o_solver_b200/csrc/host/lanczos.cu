@@ -1108,6 +1108,9 @@ void decomposeSymmetric(const double* a, std::size_t p, std::size_t ld, std::vec
     for (std::size_t j = 0; j < p; ++j)
         for (std::size_t i = j; i < p; ++i)
         {
+            if (!std::isfinite(a[i + j * ld]))
+                throw Error(STATUS_SOLVER, "symmetric eigenproblem: the term (" + std::to_string(i) + ", " +
+                                               std::to_string(j) + ") of the matrix is not finite");
             m[i + j * p] = a[i + j * ld];
             m[j + i * p] = a[i + j * ld];
         }

@@ -125,3 +125,64 @@ class BlockLanczos:
                                  bool(counts[4]), int(counts[5]), float(seconds[0]), float(seconds[1]), phases)
         finally:
             lib.oosgpu_modes_destroy(handle)
+
+
+@dataclass
+class SturmVerification:
+    """SturmVerification (SturmCheck.hpp:14-70): the eigenvalues below `verified_up_to` that the Sturm counts confirm,
+    and the first interval whose count disagrees with the eigenvalues found (expected, found)."""
+
+    verified_up_to: float
+    verified_count: int
+    has_mismatch: bool = False
+    mismatch_lower: float = 0.0
+    mismatch_upper: float = 0.0
+    mismatch_expected: int = 0
+    mismatch_found: int = 0
+
+    def _packed(self):
+        return np.array([self.verified_up_to, self.verified_count, float(self.has_mismatch), self.mismatch_lower,
+                         self.mismatch_upper, self.mismatch_expected * 1e6 + self.mismatch_found])
+
+
+def symmetric_eigen(a):
+    """SmallEigenSolver::decompose (src/linalg/dense/SmallEigenSolver.cpp:261-297) of the lower triangle of `a`:
+    (eigenvalues increasing, eigenvectors as columns signed by their first largest component). The projected problem
+    of each Lanczos step uses this routine."""
+    a = np.asfortranarray(a, dtype=np.float64)
+    p = a.shape[0]
+    values = np.zeros(max(p, 1))
+    vectors = np.zeros((p, p), order="F")
+    _check(nat.load().oosgpu_symmetric_eigen(nat.ptr(a, nat.f64p), p, max(p, 1), nat.ptr(values, nat.f64p),
+                                             nat.ptr(vectors, nat.f64p)))
+    return values[:p], vectors
+
+
+def sturm_verify(points, sorted_values) -> SturmVerification:
+    """SturmCheck::addPoint for each (shift, count below it), then verify against the eigenvalues found
+    (src/linalg/eigen/SturmCheck.cpp)."""
+    shifts = np.array([float(s) for s, _ in points])
+    counts = np.array([int(c) for _, c in points], dtype=np.int64)
+    values = np.ascontiguousarray(sorted_values, dtype=np.float64)
+    r = np.zeros(6)
+    _check(nat.load().oosgpu_sturm_verify(len(shifts), nat.ptr(shifts, nat.f64p), nat.ptr(counts, nat.i64p),
+                                          len(values), nat.ptr(values, nat.f64p), nat.ptr(r, nat.f64p)))
+    expected, found = divmod(int(round(r[5])), 1000000)
+    return SturmVerification(float(r[0]), int(r[1]), bool(r[2]), float(r[3]), float(r[4]), expected, found)
+
+
+def next_shift(request: EigenRequest, scale: float, verification: SturmVerification, sorted_values, ritz_estimates,
+               lanczos_shifts):
+    """ShiftStrategy(request, scale).nextShift (src/linalg/eigen/ShiftStrategy.cpp:121-193): (shift, purpose)."""
+    values = np.ascontiguousarray(sorted_values, dtype=np.float64)
+    ritz = np.ascontiguousarray(ritz_estimates, dtype=np.float64)
+    shifts = np.ascontiguousarray(lanczos_shifts, dtype=np.float64)
+    packed = verification._packed()
+    shift = np.zeros(1)
+    purpose = np.zeros(1, dtype=np.int32)
+    _check(nat.load().oosgpu_shift_next(float(request.lower_bound), float(request.upper_bound),
+                                        int(request.mode_count), float(scale), nat.ptr(packed, nat.f64p),
+                                        len(values), nat.ptr(values, nat.f64p), len(ritz), nat.ptr(ritz, nat.f64p),
+                                        len(shifts), nat.ptr(shifts, nat.f64p), nat.ptr(shift, nat.f64p),
+                                        nat.ptr(purpose, nat.i32p)))
+    return float(shift[0]), PURPOSES[int(purpose[0])]

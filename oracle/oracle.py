@@ -69,6 +69,11 @@ def ref_lib():
                               ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int, _f64p,
                               ctypes.c_int64, _f64p, _f64p, ctypes.c_int64, _i64p, _f64p]
     lib.ref_pencil_scale.argtypes = [ctypes.c_int32, _i64p, _i32p, _f64p, _f64p]
+    lib.ref_symmetric_eigen.argtypes = [_f64p, ctypes.c_int64, ctypes.c_int64, _f64p, _f64p]
+    lib.ref_sturm_verify.argtypes = [ctypes.c_int64, _f64p, _i64p, ctypes.c_int64, _f64p, _f64p]
+    lib.ref_shift_next.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_double, _f64p,
+                                   ctypes.c_int64, _f64p, ctypes.c_int64, _f64p, ctypes.c_int64, _f64p, _f64p,
+                                   ctypes.POINTER(ctypes.c_int32)]
     _ref = lib
     return lib
 
@@ -257,6 +262,45 @@ def pencil_scale(offsets, rows, values):
     scale = np.zeros(n)
     _check(lib.ref_pencil_scale(n, _ptr(offsets, _i64p), _ptr(rows, _i32p), _ptr(values, _f64p), _ptr(scale, _f64p)))
     return scale
+
+
+def symmetric_eigen(a):
+    """SmallEigenSolver::decompose (src/linalg/dense/SmallEigenSolver.cpp:261-297): (eigenvalues, eigenvectors)."""
+    lib = ref_lib()
+    a = np.asfortranarray(a, dtype=np.float64)
+    p = a.shape[0]
+    values = np.zeros(p)
+    vectors = np.zeros((p, p), order="F")
+    _check(lib.ref_symmetric_eigen(_ptr(a, _f64p), p, max(p, 1), _ptr(values, _f64p), _ptr(vectors, _f64p)))
+    return values, vectors
+
+
+def sturm_verify(points, sorted_values):
+    """SturmCheck::addPoint then verify (src/linalg/eigen/SturmCheck.cpp) over (shift, count) points: the six
+    values verified up to, verified count, has mismatch, mismatch lower, mismatch upper, expected * 1e6 + found."""
+    lib = ref_lib()
+    shifts = np.array([p[0] for p in points], dtype=np.float64)
+    counts = np.array([p[1] for p in points], dtype=np.int64)
+    values = np.ascontiguousarray(sorted_values, dtype=np.float64)
+    result = np.zeros(6)
+    _check(lib.ref_sturm_verify(len(points), _ptr(shifts, _f64p), _ptr(counts, _i64p), len(values),
+                                _ptr(values, _f64p), _ptr(result, _f64p)))
+    return result
+
+
+def shift_next(lower, upper, mode_count, scale, verification, sorted_values, ritz, lanczos_shifts):
+    """ShiftStrategy(request, scale).nextShift (src/linalg/eigen/ShiftStrategy.cpp:121-193): (shift, purpose)."""
+    lib = ref_lib()
+    verification = np.ascontiguousarray(verification, dtype=np.float64)
+    values = np.ascontiguousarray(sorted_values, dtype=np.float64)
+    ritz = np.ascontiguousarray(ritz, dtype=np.float64)
+    shifts = np.ascontiguousarray(lanczos_shifts, dtype=np.float64)
+    shift = np.zeros(1)
+    purpose = ctypes.c_int32(0)
+    _check(lib.ref_shift_next(lower, upper, mode_count, scale, _ptr(verification, _f64p), len(values),
+                              _ptr(values, _f64p), len(ritz), _ptr(ritz, _f64p), len(shifts), _ptr(shifts, _f64p),
+                              _ptr(shift, _f64p), ctypes.byref(purpose)))
+    return float(shift[0]), int(purpose.value)
 
 
 def port_lib():

@@ -10,6 +10,7 @@
 #include "oos/base/threading/ThreadPool.hpp"
 #include "oos/linalg/dense/DenseKernels.hpp"
 #include "oos/linalg/dense/KernelSelection.hpp"
+#include "oos/linalg/dense/SmallEigenSolver.hpp"
 #include "oos/linalg/eigen/BlockLanczos.hpp"
 #include "oos/linalg/eigen/PencilScaling.hpp"
 #include "oos/linalg/eigen/ShiftStrategy.hpp"
@@ -436,5 +437,23 @@ extern "C" int ref_shift_next(double lower, double upper, int64_t mode_count, do
                 std::span<const double>(lanczos_shifts, static_cast<std::size_t>(shift_count)));
             *shift = choice.shift;
             *purpose = static_cast<int32_t>(choice.purpose);
+        });
+}
+
+extern "C" int ref_symmetric_eigen(const double* a, int64_t p, int64_t ld, double* eigenvalues, double* eigenvectors)
+{
+    return guarded(
+        [&]
+        {
+            base::MemoryBudget budget{UNBOUNDED};
+            const auto n = static_cast<std::size_t>(p);
+            const SymmetricEigenDecomposition d =
+                SmallEigenSolver::decompose(ConstDenseMatrixView(a, n, n, static_cast<std::size_t>(ld)), budget);
+            for (std::size_t j = 0; j < n; ++j)
+            {
+                eigenvalues[j] = d.eigenvalues[j];
+                for (std::size_t i = 0; i < n; ++i)
+                    eigenvectors[i + j * n] = d.eigenvectors(i, j);
+            }
         });
 }

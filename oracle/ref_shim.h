@@ -82,6 +82,10 @@ int ref_shift_next(double lower, double upper, int64_t mode_count, double scale,
                    int64_t values, const double* sorted, int64_t ritz_count, const double* ritz, int64_t shift_count,
                    const double* lanczos_shifts, double* shift, int32_t* purpose);
 
+/* SmallEigenSolver::decompose (src/linalg/dense/SmallEigenSolver.cpp:261-297) of the lower triangle of a, column-major
+ * leading dimension ld: eigenvalues increasing, eigenvectors p x p (leading dimension p). */
+int ref_symmetric_eigen(const double* a, int64_t p, int64_t ld, double* eigenvalues, double* eigenvectors);
+
 /* pencilScaleOf (src/linalg/eigen/PencilScaling.cpp:64-80): the power-of-two scales of a stiffness CSC. */
 int ref_pencil_scale(int32_t dimension, const int64_t* col_offsets, const int32_t* rows, const double* values,
                      double* scale);
