@@ -61,6 +61,13 @@ def parse():
                         help="the modes leg: the lowest 20 modes of the n^3 hexahedral block, block size 8")
     parser.add_argument("--modes-steps", type=int, default=2)
     parser.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
+    parser.add_argument("--factor-only", metavar="MODEL:PRECISION", default=None,
+                        help="factorise one model (plate<N> or hex<N> with an ordering under tests/golden/orderings; "
+                             "precision fp64 or mixed) --steps times and print the factor's kernel statistics: the "
+                             "small case for kernel captures")
+    parser.add_argument("--launch-profile", metavar="PATH", default=None,
+                        help="with --factor-only: also solve 64 load columns and write both launch lists (kind, "
+                             "blocks, step column, device seconds) to PATH as JSON")
     return parser.parse_args()
 
 
@@ -498,8 +505,50 @@ def run_gpu(args, rank, world, local_rank):
     replicas.close()
 
 
+def factor_only(args):
+    """Factorise one model --steps times (after --warmup untimed ones) on cuda:0 and print its kernel statistics."""
+    import torch
+
+    from o_o_solver_b200 import FactorOptions, SupernodalFactor, SymbolicFactor, workloads
+
+    name, _, precision = args.factor_only.partition(":")
+    kind = "plate" if name.startswith("plate") else "hex"
+    size = int(name[len(kind):])
+    fixture = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    model = workloads.Model(workloads.PlateSpec(size, size) if kind == "plate" else workloads.HexSpec(size))
+    order = fixture["node_order"]
+    symbolic = SymbolicFactor.from_partition(model.offsets, model.neighbours, model.weights, order,
+                                             fixture["first_position"], fixture["parent"])
+    options = FactorOptions(precision=precision or "fp64")
+    stiffness = model.csc(order, 0)
+    torch.cuda.init()
+    factor = SupernodalFactor.factorise(symbolic, stiffness, options)
+    for _ in range(max(args.warmup - 1, 0)):
+        factor.refactorise(stiffness, options)
+    factor.profile(True)
+    start = time.perf_counter()
+    for _ in range(args.steps):
+        factor.refactorise(stiffness, options)
+    seconds = (time.perf_counter() - start) / max(args.steps, 1)
+    if args.launch_profile:
+        from o_o_solver_b200 import linalg
+
+        loads = torch.from_numpy(np.ascontiguousarray(model.loads(order, 64).T)).to("cuda")
+        x = torch.empty_like(loads)
+        linalg.solve_refined(factor, loads.t(), x.t(), tolerance=1.0, max_steps=0)
+        torch.cuda.synchronize()
+        with open(args.launch_profile, "w") as out:
+            json.dump({"factor": factor.launch_profile("factor"), "solve": factor.launch_profile("solve")}, out)
+    print(json.dumps({"factor_only": name, "precision": options.precision, "equations": int(symbolic.dof_count),
+                      "wall_seconds_per_factor": seconds, "kernels": factor.kernel_stats()}), flush=True)
+    factor.close()
+
+
 def main():
     args = parse()
+    if args.factor_only:
+        factor_only(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -1,5 +1,6 @@
-/* oos_gpu.h: the C ABI of the B200 implementation of O_o_Solver's numeric hot path, the supernodal multifrontal
- * LDL^T factorisation and its solves (plain FP64 form).
+/* oos_gpu.h: the C ABI of the B200 implementation of O_o_Solver's numeric hot path: the supernodal multifrontal
+ * LDL^T factorisation (positive definite and indefinite), its solves, and the shift-invert block Lanczos built on
+ * them.
  *
  * The entry points replace, one for one, the reference's C++ boundary of that path (paths within jcdulas/O_o_Solver):
  *
@@ -8,10 +9,18 @@
  *                                 rows, supernodes().parent)
  *   oosgpu_symbolic_from_partition the row-structure step of SymbolicFactor::analyse
  *                                 (src/linalg/symbolic/SymbolicFactor.cpp:227-290)
- *   oosgpu_factorise              SupernodalFactor::factorise, positive definite mode
+ *   oosgpu_factorise              SupernodalFactor::factorise, both pivoting modes
  *                                 (include/oos/linalg/supernodal/SupernodalFactor.hpp:181-183)
  *   oosgpu_factor_panel           SupernodalFactor::panel (SupernodalFactor.hpp:203)
  *   oosgpu_solve                  FactorSolve::solve (include/oos/linalg/supernodal/FactorSolve.hpp:81)
+ *   oosgpu_solve_refined          IterativeRefinement (src/linalg/dense/IterativeRefinement.cpp) over the factor
+ *   oosgpu_pencil_*               SparsePencil (include/oos/linalg/eigen/SparsePencil.hpp): factorise at a shift
+ *                                 (Sturm count), solve, mass product
+ *   oosgpu_modes_*                BlockLanczos::solve (src/linalg/eigen/BlockLanczos.cpp:87-244) and its
+ *                                 EigenSolution
+ *   oosgpu_symmetric_eigen, oosgpu_sturm_verify, oosgpu_shift_next
+ *                                 the Lanczos host logic: SmallEigenSolver, SturmCheck, ShiftStrategy
+ *
  *
  * Conventions: plain pointers and sizes; `_device` variants take device pointers (the caller's stream order is the
  * handle's stream, oosgpu_factor_stream), the others host pointers (copies included). Every call returns a status
@@ -176,8 +185,16 @@ int oosgpu_solve_refined_device(oosgpu_factor* factor, const double* b, int64_t 
 
 /* ---- measurement (no counterpart in the reference: its RunReport carries stage times only,
  *      include/oos/api/Analyses.hpp:182-199) ---------------------------------------------------------------------- */
-/* Brackets every launch of the following factorisations with CUDA events (enable != 0). */
+/* Brackets every launch of the following factorisations and solve sweeps with CUDA events (enable != 0). */
 int oosgpu_factor_profile(oosgpu_factor* factor, int32_t enable);
+/* The launches of the last profiled factorisation (which 0) or of the sweeps of the last profiled solve's last column
+ * tile (which 1), in launch order: kind (the plan's launch kinds: 0 small fronts, 1 assembly, 2 diagonal blocks,
+ * 3 panel rows, 4 panel update, 5 update matrix, 6 forward small, 7 forward gather, 8 forward diagonal, 9 forward
+ * update, 10 backward small, 11 backward rows, 12 backward diagonal, 13 backward update, 14-19 the indefinite
+ * kinds, 20 diagonal inverses, 22 the diagonal sweep), blocks, first column of the step, device seconds. At most
+ * `capacity` are written; *total is how many there are. */
+int oosgpu_factor_launch_profile(oosgpu_factor* factor, int32_t which, int64_t capacity, int32_t* kinds,
+                                 int32_t* counts, int32_t* k0, double* seconds, int64_t* total);
 /* After a profiled factorisation, per launch kind k < kinds (0 small fronts, 1 assembly, 2 diagonal blocks, 3 panel
  * rows, 4 panel update, 5 update-matrix Schur product): device seconds, launches, algorithmic flops and bytes. */
 int oosgpu_factor_kernel_stats(oosgpu_factor* factor, int32_t kinds, double* seconds, int64_t* launches,

@@ -84,6 +84,8 @@ SIGNATURES = [
     ("oosgpu_solve_refined_device", ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.c_int64,
                                                    ctypes.POINTER(RefineOptions), ctypes.POINTER(RefineInfo)]),
     ("oosgpu_factor_profile", ctypes.c_int, [_vp, ctypes.c_int32]),
+    ("oosgpu_factor_launch_profile", ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _i32p,
+                                                    _f64p, _i64p]),
     ("oosgpu_factor_kernel_stats", ctypes.c_int, [_vp, ctypes.c_int32, _f64p, _i64p, _f64p, _f64p]),
     ("oosgpu_factor_launch_counts", ctypes.c_int, [_vp, ctypes.c_int64, _i64p]),
     ("oosgpu_pencil_create", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int32, _i64p, _i32p, _f64p, _f64p,

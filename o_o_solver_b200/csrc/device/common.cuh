@@ -113,14 +113,29 @@ template <int PENDING> __device__ __forceinline__ void waitAsyncCopies()
     asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
 }
 
-// One 64 x 64 tile on a block of TILE_THREADS threads (4 warps of 32 x 32). The K loop streams slices of A and B
-// (TILE_SLICE deep) and of d into shared memory by asynchronous copies, TILE_STAGES slices in flight, so the loads of
-// later slices overlap the products of the current one; the products run on the FP64 tensor cores (DMMA m8n8k4), each
-// fragment of B multiplied by its d_p as it is read (W = B D, rounded once as before), and C is read, reduced and
-// written once. smem: TILE_SMEM_DOUBLES doubles. B's rows are contiguous in memory (bRowStride 1 in every caller);
-// A_BY_ROWS: A's rows are contiguous along p (aColStride 1), else along the rows (aRowStride 1).
-template <bool A_BY_ROWS = false>
-__device__ __forceinline__ void tileProduct(const TileOperands& op, double* smem)
+// The accumulators of one thread: acc[mi][ni][h] is element (tileRow(mi), tileColumn(ni, h)) of the 64 x 64 tile.
+using TileAccumulators = double[4][4][2];
+
+__device__ __forceinline__ int tileRow(int mi)
+{
+    return ((threadIdx.x >> 5) >> 1) * 32 + mi * 8 + ((threadIdx.x & 31) >> 2);
+}
+
+__device__ __forceinline__ int tileColumn(int ni, int h)
+{
+    return ((threadIdx.x >> 5) & 1) * 32 + ni * 8 + (threadIdx.x & 3) * 2 + h;
+}
+
+// One 64 x 64 tile on a block of TILE_THREADS threads (4 warps of 32 x 32): acc = A B (D) over the K range of `op`
+// (op.c and op.lower unused). The K loop streams slices of A and B (TILE_SLICE deep) and of d into shared memory by
+// asynchronous copies, TILE_STAGES slices in flight, so the loads of later slices overlap the products of the current
+// one; the products run on the FP64 tensor cores (DMMA m8n8k4), each fragment of B multiplied by its d_p as it is read
+// (W = B D, rounded once); ACCUMULATE: onto the values acc holds (else from zero). smem: TILE_SMEM_DOUBLES doubles. B's rows are contiguous in memory (bRowStride 1 in every
+// caller); A_BY_ROWS: A's rows are contiguous along p (aColStride 1), else along the rows (aRowStride 1). Every
+// asynchronous copy of the block has completed on return, but other threads may still read `smem`: synchronise before
+// reusing it.
+template <bool A_BY_ROWS = false, bool ACCUMULATE = false>
+__device__ __forceinline__ void tileAccumulate(const TileOperands& op, double* smem, TileAccumulators& acc)
 {
     constexpr int LD = TILE + TILE_PAD;
     const int tid = threadIdx.x;
@@ -130,15 +145,17 @@ __device__ __forceinline__ void tileProduct(const TileOperands& op, double* smem
     const int wn = (warp & 1) * 32;
     const bool scaled = op.d != nullptr;
 
-    double acc[4][4][2];
+    if (!ACCUMULATE)
+    {
 #pragma unroll
-    for (int mi = 0; mi < 4; ++mi)
+        for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
-        {
-            acc[mi][ni][0] = 0.0;
-            acc[mi][ni][1] = 0.0;
-        }
+            for (int ni = 0; ni < 4; ++ni)
+            {
+                acc[mi][ni][0] = 0.0;
+                acc[mi][ni][1] = 0.0;
+            }
+    }
 
     const int slices = (op.k + TILE_SLICE - 1) / TILE_SLICE;
     const auto issue = [&](int slice)
@@ -217,7 +234,15 @@ __device__ __forceinline__ void tileProduct(const TileOperands& op, double* smem
         }
     }
     waitAsyncCopies<0>();
+}
 
+// C -= A B (D) on one 64 x 64 tile (tileAccumulate), C read, reduced and written once; op.lower keeps the elements
+// ii + lowerOffset >= jj only.
+template <bool A_BY_ROWS = false>
+__device__ __forceinline__ void tileProduct(const TileOperands& op, double* smem)
+{
+    TileAccumulators acc;
+    tileAccumulate<A_BY_ROWS>(op, smem, acc);
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -225,8 +250,8 @@ __device__ __forceinline__ void tileProduct(const TileOperands& op, double* smem
 #pragma unroll
             for (int h = 0; h < 2; ++h)
             {
-                const int ii = wm + mi * 8 + (lane >> 2);
-                const int jj = wn + ni * 8 + (lane & 3) * 2 + h;
+                const int ii = tileRow(mi);
+                const int jj = tileColumn(ni, h);
                 if (ii < op.m && jj < op.n && (!op.lower || ii + op.lowerOffset >= jj))
                 {
                     double* target = op.c + ii * op.cRowStride + jj * op.cColStride;

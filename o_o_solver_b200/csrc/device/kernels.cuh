@@ -48,6 +48,13 @@ struct SolveArgs
     double* x;       // n x width, by rows
     double* updates; // update rows of every supernode: rowStart[s] * width, r x width by rows
     int width;
+    // The gather lists of the forward sweep (slot first + p for a column position p < c, dimension + rowStart + k for
+    // an update row; entries: indexes of children's update rows, children in increasing order) and, after an
+    // indefinite factorisation, the pivot order (the column at pivot position j is perm[j]; null otherwise).
+    const std::int64_t* gatherStart;
+    const std::int32_t* gatherRows;
+    const std::int32_t* perm;
+    int dimension;
 };
 
 __global__ void assembleFronts(FactorArgs args, const AssemblyTask* tasks, std::int32_t* structureError);
@@ -64,7 +71,7 @@ constexpr std::size_t MIXED_UPDATE_SMEM = 2 * 4 * 128 * 16 * 4 + 1024;
 __global__ void pivotSummary(FactorArgs args, const std::int32_t* supernodeOfColumn, int dimension,
                              const double* referenceDiagonal, double maxRatio, unsigned long long* counters,
                              std::int32_t* issues, int issueCapacity, double* blockRatio, std::int32_t* blockEquation);
-__global__ void forwardSmall(SolveArgs a, const std::int32_t* list);
+__global__ void forwardSmall(SolveArgs a, const std::int32_t* list, int cmax);
 __global__ void forwardGather(SolveArgs a, const TileTask* tasks);
 __global__ void invertDiagonal(FactorArgs args, const TileTask* tasks);
 // Dynamic shared memory of forwardDiagonal / backwardDiagonal for a tile of `width` columns.
@@ -72,15 +79,16 @@ constexpr std::size_t diagonalSolveSmem(int width)
 {
     return static_cast<std::size_t>(64 * 65 + 64 * width) * sizeof(double);
 }
-// Dynamic shared memory of forwardSmall / backwardSmall: the inverse and a c x width block.
+// Dynamic shared memory of forwardSmall / backwardSmall for supernodes of at most `columns` columns: the tile
+// pipeline, the inverse (c x (c + 1)) and a c x width block.
 constexpr std::size_t smallSolveSmem(int columns, int width)
 {
-    return static_cast<std::size_t>(64 * 65 + columns * width) * sizeof(double);
+    return static_cast<std::size_t>(TILE_SMEM_DOUBLES + columns * (columns + 1) + columns * width) * sizeof(double);
 }
 __global__ void forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0);
 __global__ void forwardUpdate(SolveArgs a, const TileTask* tasks, int k0);
 __global__ void diagonalSweep(SolveArgs a, const std::int32_t* supernodeOfColumn, int dimension);
-__global__ void backwardSmall(SolveArgs a, const std::int32_t* list);
+__global__ void backwardSmall(SolveArgs a, const std::int32_t* list, int cmax);
 __global__ void backwardRows(SolveArgs a, const TileTask* tasks);
 __global__ void backwardDiagonal(SolveArgs a, const std::int32_t* list, int k0);
 __global__ void backwardUpdate(SolveArgs a, const TileTask* tasks, int k0);

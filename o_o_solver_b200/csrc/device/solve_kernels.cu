@@ -20,179 +20,249 @@ namespace oosgpu::device
 
 constexpr int SOLVE_BLOCK = 64;
 constexpr int SOLVE_THREADS = 256;
-constexpr int SOLVE_WIDTH_MAX = 64; // the widest tile of right-hand sides
 
-// Adds the children's update rows into the supernode's rows of X (positions < c) and into its own update rows
-// (zeroed first), children in increasing order.
-__device__ void gatherChildren(const SolveArgs& a, const FrontDesc& f, double* xF, int ldxF)
+// g += the children's update rows that land at the slots of a tile's rows (slotOf(ii) for the rows ii < rows, all
+// width columns), element (tileRow(mi), tileColumn(ni, h)) of the tile in g[mi][ni][h] as the tile products hold it.
+// The rows are added in rounds (the k-th entry of every row's gather list in round k), so each value takes its
+// children in increasing order and every round's loads are independent of each other.
+template <typename SlotOf>
+__device__ __forceinline__ void gatherTile(const SolveArgs& a, int rows, SlotOf slotOf, TileAccumulators& g)
 {
-    const int w = a.width;
-    double* own = a.updates + f.rowStart * w;
-    for (int e = threadIdx.x; e < f.r * w; e += blockDim.x)
-        own[e] = 0.0;
-    __syncthreads();
-    for (int q = 0; q < f.childCount; ++q)
+    std::int64_t next[4];
+    std::int64_t end[4];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
     {
-        const FrontDesc ch = a.fronts[a.children[f.childStart + q]];
-        const std::int32_t* map = a.relpos + ch.rowStart;
-        const double* source = a.updates + ch.rowStart * w;
-#pragma unroll 4
-        for (int e = threadIdx.x; e < ch.r * w; e += blockDim.x)
+        const int ii = tileRow(mi);
+        next[mi] = 0;
+        end[mi] = 0;
+        if (ii < rows)
         {
-            const int i = e / w;
-            const int col = e - i * w;
-            const int position = map[i];
-            if (position < f.c)
-                xF[position * ldxF + col] += source[e];
-            else
-                own[(position - f.c) * w + col] += source[e];
+            const std::int64_t slot = slotOf(ii);
+            next[mi] = a.gatherStart[slot];
+            end[mi] = a.gatherStart[slot + 1];
         }
-        __syncthreads();
     }
-}
-
-// The inverse of a small supernode's unit lower triangle L11 (c <= 64), from its strict upper triangle:
-// inv[i * (SOLVE_BLOCK + 1) + q] = L11^-1(i, q) for q < i < c, zero elsewhere (asynchronous copies, not waited for).
-__device__ __forceinline__ void stageSmallInverse(const SolveArgs& a, const FrontDesc& f, double* inv)
-{
-    constexpr int LD = SOLVE_BLOCK + 1;
-    const std::int64_t n = f.c + f.r;
-    const double* panel = a.panels + f.panel;
-    for (int e = threadIdx.x; e < SOLVE_BLOCK * SOLVE_BLOCK; e += blockDim.x)
+    for (;;)
     {
-        const int i = e / SOLVE_BLOCK;
-        const int q = e - i * SOLVE_BLOCK;
-        const bool inside = q < i && i < f.c;
-        copyAsync8(inv + i * LD + q, inside ? panel + q + static_cast<std::int64_t>(i) * n : panel, inside);
+        std::int64_t row[4];
+        bool any = false;
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+        {
+            row[mi] = next[mi] < end[mi] ? a.gatherRows[next[mi]] : -1;
+            any = any || row[mi] >= 0;
+            ++next[mi];
+        }
+        if (!any)
+            break;
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+        {
+            if (row[mi] < 0)
+                continue;
+            const double* source = a.updates + row[mi] * a.width;
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                {
+                    const int jj = tileColumn(ni, h);
+                    if (jj < a.width)
+                        g[mi][ni][h] += source[jj];
+                }
+        }
     }
 }
 
-// Forward sweep of a small supernode (c <= SOLVE_BLOCK): x_F <- L11^-1 (b_F + children), a product with the inverse
-// of L11 (every value independent), then u_s <- children - L21 x_F. Dynamic shared memory: c * width + 64 * 65
-// doubles.
-__global__ void __launch_bounds__(SOLVE_THREADS) forwardSmall(SolveArgs a, const std::int32_t* list)
+// The gather slot of column position p < c of a supernode (in pivot order after an indefinite factorisation), and of
+// its update row k.
+__device__ __forceinline__ std::int64_t columnSlot(const SolveArgs& a, const FrontDesc& f, int p)
 {
-    constexpr int LD = SOLVE_BLOCK + 1;
+    return a.perm != nullptr ? a.perm[f.first + p] : f.first + p;
+}
+
+__device__ __forceinline__ std::int64_t rowSlot(const SolveArgs& a, const FrontDesc& f, int k)
+{
+    return a.dimension + f.rowStart + k;
+}
+
+// The strict lower triangle of a small supernode's L11^-1 (c <= 64) from the strict upper triangle of its diagonal
+// block: inv[i * (c + 1) + q] = L11^-1(i, q) for q < i < c (asynchronous copies, committed by the caller).
+__device__ __forceinline__ void stageSmallInverse(const double* panel, std::int64_t n, int c, double* inv)
+{
+    for (int e = threadIdx.x; e < c * c; e += blockDim.x)
+    {
+        const int i = e / c;
+        const int q = e - i * c;
+        const bool inside = q < i;
+        copyAsync8(inv + i * (c + 1) + q, inside ? panel + q + static_cast<std::int64_t>(i) * n : panel, inside);
+    }
+}
+
+// Forward sweep of a small supernode (c <= 64), one block of TILE_THREADS: x_F <- L11^-1 (b_F + children's rows at
+// F), as the product with the inverse of L11 (every value independent); then the update rows by 64-row tiles,
+// u_s = (children's rows at R(s), in the children's order) - L21 x_F, the product on the FP64 tensor cores
+// (tileAccumulate) and each tile written once. The children's rows come by the gather lists: every value has one
+// owner thread, no barrier between children. Dynamic shared memory: smallSolveSmem(cmax, width) with cmax the launch's
+// largest c.
+__global__ void __launch_bounds__(TILE_THREADS) forwardSmall(SolveArgs a, const std::int32_t* list, int cmax)
+{
     extern __shared__ double stage[];
-    double* inv = stage;                      // 64 x 65
-    double* xF = stage + SOLVE_BLOCK * LD;    // c x width
+    double* pipe = stage;                    // the tile pipeline
+    double* inv = stage + TILE_SMEM_DOUBLES; // c x (c + 1)
+    double* xF = inv + cmax * (cmax + 1);    // c x width
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
-    double* xRows = a.x + static_cast<std::int64_t>(f.first) * w;
-    stageSmallInverse(a, f, inv);
-    for (int e = threadIdx.x; e < f.c * w; e += blockDim.x)
-        copyAsync8(xF + e, xRows + e, true);
-    commitAsyncCopies();
-    waitAsyncCopies<0>();
-    __syncthreads();
-    gatherChildren(a, f, xF, w);
-    // x = L11^-1 b: each thread its values of the block, into registers, then back after a barrier.
-    constexpr int PER_THREAD = SOLVE_BLOCK * SOLVE_WIDTH_MAX / SOLVE_THREADS;
-    double y[PER_THREAD];
-#pragma unroll
-    for (int u = 0; u < PER_THREAD; ++u)
-    {
-        const int e = threadIdx.x + u * SOLVE_THREADS;
-        y[u] = 0.0;
-        if (e < f.c * w)
-        {
-            const int i = e / w;
-            const int col = e - i * w;
-            double sum = xF[e];
-            for (int q = 0; q < i; ++q)
-                sum += inv[i * LD + q] * xF[q * w + col];
-            y[u] = sum;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < PER_THREAD; ++u)
-    {
-        const int e = threadIdx.x + u * SOLVE_THREADS;
-        if (e < f.c * w)
-            xF[e] = y[u];
-    }
-    __syncthreads();
+    const int c = f.c;
     const std::int64_t n = f.c + f.r;
     const double* panel = a.panels + f.panel;
-    double* own = a.updates + f.rowStart * w;
-    for (int e = threadIdx.x; e < f.r * w; e += blockDim.x)
+    double* xRows = a.x + static_cast<std::int64_t>(f.first) * w;
+    stageSmallInverse(panel, n, c, inv);
+    commitAsyncCopies();
+    {
+        TileAccumulators g;
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                {
+                    const int ii = tileRow(mi);
+                    const int jj = tileColumn(ni, h);
+                    g[mi][ni][h] = ii < c && jj < w ? xRows[ii * w + jj] : 0.0;
+                }
+        gatherTile(a, c, [&](int ii) { return columnSlot(a, f, ii); }, g);
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                {
+                    const int ii = tileRow(mi);
+                    const int jj = tileColumn(ni, h);
+                    if (ii < c && jj < w)
+                        xF[ii * w + jj] = g[mi][ni][h];
+                }
+    }
+    waitAsyncCopies<0>();
+    __syncthreads();
+    for (int e = threadIdx.x; e < c * w; e += blockDim.x)
     {
         const int i = e / w;
         const int col = e - i * w;
-        double sum = own[e];
-#pragma unroll 8
-        for (int q = 0; q < f.c; ++q)
-            sum -= panel[f.c + i + static_cast<std::int64_t>(q) * n] * xF[q * w + col];
-        own[e] = sum;
+        double sum = xF[e];
+        for (int q = 0; q < i; ++q)
+            sum += inv[i * (c + 1) + q] * xF[q * w + col];
+        xRows[e] = sum;
     }
-    for (int e = threadIdx.x; e < f.c * w; e += blockDim.x)
-        xRows[e] = xF[e];
+    __syncthreads();
+    double* own = a.updates + f.rowStart * w;
+    for (int i0 = 0; i0 < f.r; i0 += TILE)
+    {
+        TileOperands op;
+        op.a = panel + c + i0; // A(ii, p) = L(c + i0 + ii, p)
+        op.aRowStride = 1;
+        op.aColStride = n;
+        op.b = xRows;
+        op.bRowStride = 1;
+        op.bColStride = w;
+        op.bIndex = nullptr;
+        op.d = nullptr;
+        op.dStride = 0;
+        op.c = nullptr;
+        op.cRowStride = 0;
+        op.cColStride = 0;
+        op.m = min(TILE, f.r - i0);
+        op.n = w;
+        op.k = c;
+        op.lower = false;
+        op.lowerOffset = 0;
+        // acc = -(children's rows) + L21 x_F; the update rows are -acc
+        TileAccumulators acc;
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+            {
+                acc[mi][ni][0] = 0.0;
+                acc[mi][ni][1] = 0.0;
+            }
+        gatherTile(a, op.m, [&](int ii) { return rowSlot(a, f, i0 + ii); }, acc);
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+            {
+                acc[mi][ni][0] = -acc[mi][ni][0];
+                acc[mi][ni][1] = -acc[mi][ni][1];
+            }
+        tileAccumulate<false, true>(op, pipe, acc);
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                {
+                    const int ii = tileRow(mi);
+                    const int jj = tileColumn(ni, h);
+                    if (ii < op.m && jj < w)
+                        own[static_cast<std::int64_t>(i0 + ii) * w + jj] = -acc[mi][ni][h];
+                }
+        __syncthreads();
+    }
 }
 
-// The children's update rows of a large supernode, for the front positions [i0, j0) of a task: into X's rows of its
-// columns (in place) and its own update rows (zeroed first). Each block owns its positions and adds the children in
-// increasing order, so every row's sum is the same whatever the split; a child's rows landing in the range are
-// consecutive (positions increase with the rows), found by bisection.
-__global__ void __launch_bounds__(SOLVE_THREADS) forwardGather(SolveArgs a, const TileTask* tasks)
+// The children's update rows of a large supernode, for the front positions [i0, j0) of a task (at most 64): added into
+// X's rows of its columns (in place) and into its own update rows (which they set), by the gather lists (gatherTile):
+// every value one thread, the children in increasing order, so every sum is the same whatever the split. One block
+// of TILE_THREADS.
+__global__ void __launch_bounds__(TILE_THREADS) forwardGather(SolveArgs a, const TileTask* tasks)
 {
-    __shared__ int range[2];
     const TileTask task = tasks[blockIdx.x];
     const FrontDesc f = a.fronts[task.front];
     const int w = a.width;
-    const int p0 = task.i0;
-    const int p1 = task.j0;
+    const int rows = min(task.j0 - task.i0, TILE);
     double* xF = a.x + static_cast<std::int64_t>(f.first) * w;
     double* own = a.updates + f.rowStart * w;
-    const int firstOwn = max(p0, f.c);
-    for (int e = threadIdx.x; e < (p1 - firstOwn) * w; e += blockDim.x)
-        own[static_cast<std::int64_t>(firstOwn - f.c) * w + e] = 0.0;
-    __syncthreads();
-    for (int q = 0; q < f.childCount; ++q)
-    {
-        const FrontDesc ch = a.fronts[a.children[f.childStart + q]];
-        const std::int32_t* map = a.relpos + ch.rowStart;
-        if (threadIdx.x == 0)
-        {
-            int lo = 0;
-            int hi = ch.r;
-            while (lo < hi)
+    TileAccumulators g;
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
             {
-                const int mid = (lo + hi) >> 1;
-                if (map[mid] < p0)
-                    lo = mid + 1;
-                else
-                    hi = mid;
+                const int p = task.i0 + tileRow(mi);
+                const int jj = tileColumn(ni, h);
+                g[mi][ni][h] = tileRow(mi) < rows && jj < w && p < f.c ? xF[static_cast<std::int64_t>(p) * w + jj] : 0.0;
             }
-            int end = lo;
-            hi = ch.r;
-            while (end < hi)
+    gatherTile(a, rows,
+               [&](int ii)
+               {
+                   const int p = task.i0 + ii;
+                   return p < f.c ? columnSlot(a, f, p) : rowSlot(a, f, p - f.c);
+               },
+               g);
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
             {
-                const int mid = (end + hi) >> 1;
-                if (map[mid] < p1)
-                    end = mid + 1;
+                const int p = task.i0 + tileRow(mi);
+                const int jj = tileColumn(ni, h);
+                if (tileRow(mi) >= rows || jj >= w)
+                    continue;
+                if (p < f.c)
+                    xF[static_cast<std::int64_t>(p) * w + jj] = g[mi][ni][h];
                 else
-                    hi = mid;
+                    own[static_cast<std::int64_t>(p - f.c) * w + jj] = g[mi][ni][h];
             }
-            range[0] = lo;
-            range[1] = end;
-        }
-        __syncthreads();
-        const int lo = range[0];
-        const double* source = a.updates + ch.rowStart * w;
-        for (int e = threadIdx.x; e < (range[1] - lo) * w; e += blockDim.x)
-        {
-            const int i = lo + e / w;
-            const int col = e - (e / w) * w;
-            const int position = map[i];
-            const double value = source[static_cast<std::int64_t>(i) * w + col];
-            if (position < f.c)
-                xF[static_cast<std::int64_t>(position) * w + col] += value;
-            else
-                own[static_cast<std::int64_t>(position - f.c) * w + col] += value;
-        }
-        __syncthreads();
-    }
 }
 
 // The inverse of the unit lower 64 x 64 diagonal block of step k0 of a large supernode, after each factorisation: one
@@ -342,42 +412,65 @@ __global__ void diagonalSweep(SolveArgs a, const std::int32_t* supernodeOfColumn
     a.x[e] = a.x[e] / a.panels[f.panel + k + k * n];
 }
 
-// Backward sweep of a small supernode: x_F <- L11^-T (x_F - L21^T X[R(s)]), the triangle as a product with the
-// transposed inverse. Dynamic shared memory as forwardSmall.
-__global__ void __launch_bounds__(SOLVE_THREADS) backwardSmall(SolveArgs a, const std::int32_t* list)
+// Backward sweep of a small supernode (c <= 64), one block of TILE_THREADS: x_F <- L11^-T (x_F - L21^T X[R(s)]),
+// L21^T X[R(s)] as one tile product over K = r on the FP64 tensor cores (the rows of X gathered by R(s)), the
+// triangle as the product with the transposed inverse. Dynamic shared memory: smallSolveSmem(cmax, width).
+__global__ void __launch_bounds__(TILE_THREADS) backwardSmall(SolveArgs a, const std::int32_t* list, int cmax)
 {
-    constexpr int LD = SOLVE_BLOCK + 1;
     extern __shared__ double stage[];
-    double* inv = stage;
-    double* xF = stage + SOLVE_BLOCK * LD;
+    double* pipe = stage;                    // the tile pipeline, then x_F (c x width)
+    double* inv = stage + TILE_SMEM_DOUBLES; // c x (c + 1)
+    (void)cmax;
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
+    const int c = f.c;
     const std::int64_t n = f.c + f.r;
     const double* panel = a.panels + f.panel;
-    const std::int32_t* rows = a.rows + f.rowStart;
     double* xRows = a.x + static_cast<std::int64_t>(f.first) * w;
-    stageSmallInverse(a, f, inv);
+    stageSmallInverse(panel, n, c, inv);
     commitAsyncCopies();
-    for (int e = threadIdx.x; e < f.c * w; e += blockDim.x)
-    {
-        const int q = e / w;
-        const int col = e - q * w;
-        double sum = xRows[e];
-        const double* l = panel + f.c + static_cast<std::int64_t>(q) * n;
-#pragma unroll 8
-        for (int i = 0; i < f.r; ++i)
-            sum -= l[i] * a.x[static_cast<std::int64_t>(rows[i]) * w + col];
-        xF[e] = sum;
-    }
-    waitAsyncCopies<0>();
+    TileOperands op;
+    op.a = panel + c; // A(q, i) = L(c + i, q)
+    op.aRowStride = n;
+    op.aColStride = 1;
+    op.b = a.x;
+    op.bRowStride = 1;
+    op.bColStride = w;
+    op.bIndex = a.rows + f.rowStart;
+    op.d = nullptr;
+    op.dStride = 0;
+    op.c = nullptr;
+    op.cRowStride = 0;
+    op.cColStride = 0;
+    op.m = c;
+    op.n = w;
+    op.k = f.r;
+    op.lower = false;
+    op.lowerOffset = 0;
+    TileAccumulators acc;
+    tileAccumulate<true>(op, pipe, acc);
     __syncthreads();
-    for (int e = threadIdx.x; e < f.c * w; e += blockDim.x)
+    double* xF = pipe;
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+            {
+                const int ii = tileRow(mi);
+                const int jj = tileColumn(ni, h);
+                if (ii < c && jj < w)
+                    xF[ii * w + jj] = xRows[ii * w + jj] - acc[mi][ni][h];
+            }
+    __syncthreads();
+    for (int e = threadIdx.x; e < c * w; e += blockDim.x)
     {
         const int q = e / w;
         const int col = e - q * w;
         double sum = xF[e];
-        for (int i = q + 1; i < f.c; ++i)
-            sum += inv[i * LD + q] * xF[i * w + col];
+        for (int i = q + 1; i < c; ++i)
+            sum += inv[i * (c + 1) + q] * xF[i * w + col];
         xRows[e] = sum;
     }
 }

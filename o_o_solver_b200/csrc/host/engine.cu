@@ -105,6 +105,8 @@ public:
         m_children.upload(m_plan.children, m_stream, "plan: children");
         m_rows.upload(m_plan.rows, m_stream, "plan: rows");
         m_relpos.upload(m_plan.relpos, m_stream, "plan: positions");
+        m_gatherStart.upload(m_plan.gatherStart, m_stream, "plan: gather lists");
+        m_gatherRows.upload(m_plan.gatherRows, m_stream, "plan: gather lists");
         m_supernodeOfColumn.upload(m_plan.supernodeOfColumn, m_stream, "plan: columns");
         m_lists.upload(m_plan.lists, m_stream, "plan: lists");
         m_tiles.upload(m_plan.tiles, m_stream, "plan: tiles");
@@ -159,6 +161,8 @@ public:
         cudaEventDestroy(m_start);
         cudaEventDestroy(m_stop);
         for (cudaEvent_t e : m_profileEvents)
+            cudaEventDestroy(e);
+        for (cudaEvent_t e : m_solveEvents)
             cudaEventDestroy(e);
         if (m_stream != nullptr)
             cudaStreamDestroy(m_stream);
@@ -640,14 +644,22 @@ public:
                                m_panels.get(),
                                x,
                                updateRows != nullptr ? updateRows : m_updateRows.get(),
-                               width};
+                               width,
+                               m_gatherStart.get(),
+                               m_gatherRows.get(),
+                               m_pivoted ? m_perm.get() : nullptr,
+                               n};
+        m_solveRecords.clear();
         runSweep(args, m_plan.forwardLaunches);
+        const std::size_t record = beginSolveRecord(DIAGONAL_SWEEP_KIND, static_cast<std::int32_t>(blocksFor(items, 256)), 0);
         if (m_pivoted)
             device::diagonalSweepPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(),
                                                                                       m_subdiagonal.get(), n);
         else
             device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), n);
+        endSolveRecord(record);
         runSweep(args, m_plan.backwardLaunches);
+        m_solveProfileValid = m_profile;
     }
 
     // The device this factor lives on.
@@ -1095,6 +1107,42 @@ public:
             bytes[kind] += launch.bytes;
         }
     }
+    // The launches of the last profiled factorisation (which 0) or solve sweeps (which 1): kind, blocks, first
+    // column of the step and device seconds; returns how many there are (at most `capacity` written).
+    std::int64_t launchProfile(int which, std::int64_t capacity, std::int32_t* kinds, std::int32_t* counts,
+                               std::int32_t* k0, double* seconds)
+    {
+        check(cudaSetDevice(m_device), "cudaSetDevice");
+        check(cudaStreamSynchronize(m_stream), "profile");
+        const bool factor = which == 0;
+        if (factor ? !m_profileValid : !m_solveProfileValid)
+            throw Error(STATUS_NOT_FACTORISED, factor ? "launch profile: no profiled factorisation"
+                                                      : "launch profile: no profiled solve");
+        const std::size_t total = factor ? m_plan.factorLaunches.size() : m_solveRecords.size();
+        for (std::size_t index = 0; index < total && static_cast<std::int64_t>(index) < capacity; ++index)
+        {
+            float ms = 0.0f;
+            if (factor)
+            {
+                const Launch& launch = m_plan.factorLaunches[index];
+                kinds[index] = static_cast<std::int32_t>(launch.kind);
+                counts[index] = launch.count;
+                k0[index] = launch.k0;
+                check(cudaEventElapsedTime(&ms, m_profileEvents[2 * index], m_profileEvents[2 * index + 1]),
+                      "profile time");
+            }
+            else
+            {
+                kinds[index] = m_solveRecords[index].kind;
+                counts[index] = m_solveRecords[index].count;
+                k0[index] = m_solveRecords[index].k0;
+                check(cudaEventElapsedTime(&ms, m_solveEvents[2 * index], m_solveEvents[2 * index + 1]),
+                      "profile time");
+            }
+            seconds[index] = ms / 1000.0;
+        }
+        return static_cast<std::int64_t>(total);
+    }
     [[nodiscard]] std::int64_t factorLaunchCount() const noexcept
     {
         return static_cast<std::int64_t>(m_plan.factorLaunches.size()) + 1;
@@ -1187,13 +1235,15 @@ private:
             const std::int32_t* list = m_lists.get() + launch.offset;
             const device::TileTask* tiles = m_tiles.get() + launch.offset;
             const std::size_t smallSmem = device::smallSolveSmem(std::max(launch.smemOrder, 1), args.width);
+            const std::size_t record = beginSolveRecord(static_cast<std::int32_t>(launch.kind), launch.count, launch.k0);
             switch (launch.kind)
             {
             case LaunchKind::ForwardSmall:
-                device::forwardSmall<<<launch.count, 256, smallSmem, m_stream>>>(args, list);
+                device::forwardSmall<<<launch.count, device::TILE_THREADS, smallSmem, m_stream>>>(
+                    args, list, std::max(launch.smemOrder, 1));
                 break;
             case LaunchKind::ForwardGather:
-                device::forwardGather<<<launch.count, 256, 0, m_stream>>>(args, tiles);
+                device::forwardGather<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles);
                 break;
             case LaunchKind::ForwardDiagonal:
                 device::forwardDiagonal<<<launch.count, 256, device::diagonalSolveSmem(args.width), m_stream>>>(
@@ -1203,7 +1253,8 @@ private:
                 device::forwardUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles, launch.k0);
                 break;
             case LaunchKind::BackwardSmall:
-                device::backwardSmall<<<launch.count, 256, smallSmem, m_stream>>>(args, list);
+                device::backwardSmall<<<launch.count, device::TILE_THREADS, smallSmem, m_stream>>>(
+                    args, list, std::max(launch.smemOrder, 1));
                 break;
             case LaunchKind::BackwardRows:
                 device::backwardRows<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles);
@@ -1218,7 +1269,31 @@ private:
             default:
                 throw Error(STATUS_INTERNAL, "solve plan: a factorisation launch in a sweep");
             }
+            endSolveRecord(record);
         }
+    }
+
+    // Per-launch device times of the last profiled solve's sweeps (its last column tile): events around each launch
+    // when profiling is on.
+    std::size_t beginSolveRecord(std::int32_t kind, std::int32_t count, std::int32_t k0)
+    {
+        if (!m_profile)
+            return 0;
+        const std::size_t index = m_solveRecords.size();
+        m_solveRecords.push_back({kind, count, k0});
+        while (m_solveEvents.size() < 2 * (index + 1))
+        {
+            cudaEvent_t e = nullptr;
+            check(cudaEventCreate(&e), "profile event");
+            m_solveEvents.push_back(e);
+        }
+        check(cudaEventRecord(m_solveEvents[2 * index], m_stream), "profile event");
+        return index;
+    }
+    void endSolveRecord(std::size_t index)
+    {
+        if (m_profile)
+            check(cudaEventRecord(m_solveEvents[2 * index + 1], m_stream), "profile event");
     }
 
     Symbolic m_symbolic;
@@ -1231,6 +1306,8 @@ private:
     DeviceArray<std::int32_t> m_children;
     DeviceArray<std::int32_t> m_rows;
     DeviceArray<std::int32_t> m_relpos;
+    DeviceArray<std::int64_t> m_gatherStart;
+    DeviceArray<std::int32_t> m_gatherRows;
     DeviceArray<std::int32_t> m_supernodeOfColumn;
     DeviceArray<std::int32_t> m_lists;
     DeviceArray<device::TileTask> m_tiles;
@@ -1291,6 +1368,17 @@ private:
     bool m_factorised = false;
     bool m_profile = false;
     bool m_profileValid = false;
+    bool m_solveProfileValid = false;
+    struct SolveRecord
+    {
+        std::int32_t kind;
+        std::int32_t count;
+        std::int32_t k0;
+    };
+    // The kind code of the diagonal sweep in a solve's launch profile (after the plan's launch kinds).
+    static constexpr std::int32_t DIAGONAL_SWEEP_KIND = 22;
+    std::vector<SolveRecord> m_solveRecords;
+    std::vector<cudaEvent_t> m_solveEvents;
     bool m_annotated = false;
     std::vector<cudaEvent_t> m_profileEvents;
     double m_lastSolveSeconds = 0.0;
@@ -1873,6 +1961,27 @@ extern "C" int oosgpu_factor_kernel_stats(oosgpu_factor* factor, int32_t kinds, 
         {
             requirePointer(factor, "factor");
             factor->factor->kernelStats(kinds, seconds, launches, flops, bytes);
+        });
+}
+
+extern "C" int oosgpu_factor_launch_profile(oosgpu_factor* factor, int32_t which, int64_t capacity, int32_t* kinds,
+                                            int32_t* counts, int32_t* k0, double* seconds, int64_t* total)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            requirePointer(total, "total");
+            if (which != 0 && which != 1)
+                throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT, "launch profile: which is 0 or 1");
+            if (capacity > 0)
+            {
+                requirePointer(kinds, "kinds");
+                requirePointer(counts, "counts");
+                requirePointer(k0, "k0");
+                requirePointer(seconds, "seconds");
+            }
+            *total = factor->factor->launchProfile(which, capacity, kinds, counts, k0, seconds);
         });
 }
 

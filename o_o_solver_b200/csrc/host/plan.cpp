@@ -3,6 +3,7 @@
 #include "plan.hpp"
 
 #include <algorithm>
+#include <cstdint>
 #include <string>
 
 namespace oosgpu
@@ -247,6 +248,47 @@ Plan buildPlan(const Symbolic& symbolic)
         }
     }
 
+    // Gather lists (the transpose of relpos, children in increasing order within each slot).
+    if (static_cast<std::int64_t>(symbolic.rows.size()) > INT32_MAX)
+        throw Error(STATUS_INVALID_ARGUMENT, "plan: more than 2^31 row entries");
+    const std::size_t slots = static_cast<std::size_t>(plan.dimension) + symbolic.rows.size();
+    plan.gatherStart.assign(slots + 1, 0);
+    const auto slotOf = [&](const FrontDesc& p, std::int32_t position)
+    {
+        return position < p.c ? static_cast<std::size_t>(p.first + position)
+                              : static_cast<std::size_t>(plan.dimension) + static_cast<std::size_t>(p.rowStart) +
+                                    static_cast<std::size_t>(position - p.c);
+    };
+    for (std::int32_t s = 0; s < count; ++s)
+    {
+        const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+        if (f.parent < 0)
+            continue;
+        const FrontDesc& p = plan.fronts[static_cast<std::size_t>(f.parent)];
+        for (std::int64_t k = f.rowStart; k < f.rowStart + f.r; ++k)
+            ++plan.gatherStart[slotOf(p, plan.relpos[static_cast<std::size_t>(k)]) + 1];
+    }
+    for (std::size_t slot = 0; slot < slots; ++slot)
+        plan.gatherStart[slot + 1] += plan.gatherStart[slot];
+    plan.gatherRows.assign(static_cast<std::size_t>(plan.gatherStart[slots]), 0);
+    {
+        std::vector<std::int64_t> next(plan.gatherStart.begin(), plan.gatherStart.end() - 1);
+        // children of each parent in increasing order: the parent's child list is in that order
+        for (std::int32_t s = 0; s < count; ++s)
+        {
+            const FrontDesc& p = plan.fronts[static_cast<std::size_t>(s)];
+            for (std::int32_t q = 0; q < p.childCount; ++q)
+            {
+                const FrontDesc& ch = plan.fronts[static_cast<std::size_t>(plan.children[static_cast<std::size_t>(p.childStart + q)])];
+                for (std::int64_t k = ch.rowStart; k < ch.rowStart + ch.r; ++k)
+                {
+                    const std::size_t slot = slotOf(p, plan.relpos[static_cast<std::size_t>(k)]);
+                    plan.gatherRows[static_cast<std::size_t>(next[slot]++)] = static_cast<std::int32_t>(k);
+                }
+            }
+        }
+    }
+
     plan.wOffset.assign(total, 0);
     for (const FrontDesc& f : plan.fronts)
     {
@@ -470,7 +512,7 @@ Plan buildPlan(const Symbolic& symbolic)
         addList(plan, plan.forwardLaunches, LaunchKind::ForwardSmall, solveSmall, 0, maxSmallColumns);
         {
             // The children's update rows of the large supernodes, by ranges of GATHER_POSITIONS front positions.
-            constexpr std::int32_t GATHER_POSITIONS = 256;
+            constexpr std::int32_t GATHER_POSITIONS = 64;
             std::vector<TileTask> ranges;
             for (const std::int32_t s : solveLarge)
             {

@@ -77,6 +77,11 @@ struct Plan
     std::vector<std::int32_t> children;
     std::vector<std::int32_t> rows;
     std::vector<std::int32_t> relpos;
+    // The forward solve's gather lists: for each slot (a supernode's column position p < c: slot first + p; an update
+    // row k of R(s): slot dimension + rowStart + k) the update rows of the children that land there, children in
+    // increasing order: gatherRows[gatherStart[slot] .. gatherStart[slot + 1]) (indexes into the row arrays).
+    std::vector<std::int64_t> gatherStart;
+    std::vector<std::int32_t> gatherRows;
     std::vector<std::int32_t> supernodeOfColumn;
     std::vector<std::int32_t> level;
     std::int64_t panelValues = 0;

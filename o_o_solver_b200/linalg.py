@@ -260,7 +260,8 @@ class SupernodalFactor:
                     "update_matrix"]
 
     def profile(self, enable: bool = True):
-        """Brackets every launch of the following factorisations with CUDA events (kernel_stats())."""
+        """Brackets every launch of the following factorisations and solves with CUDA events (kernel_stats(),
+        launch_profile())."""
         _check(nat.load().oosgpu_factor_profile(self._handle, 1 if enable else 0))
 
     def kernel_stats(self) -> dict:
@@ -275,6 +276,29 @@ class SupernodalFactor:
                                                      nat.ptr(bytes_, nat.f64p)))
         return {name: {"seconds": float(seconds[k]), "launches": int(launches[k]), "flops": float(flops[k]),
                        "bytes": float(bytes_[k])} for k, name in enumerate(self.KERNEL_KINDS)}
+
+    LAUNCH_KINDS = ["small_fronts", "assemble_fronts", "diagonal_blocks", "panel_rows", "panel_update",
+                    "update_matrix", "forward_small", "forward_gather", "forward_diagonal", "forward_update",
+                    "backward_small", "backward_rows", "backward_diagonal", "backward_update",
+                    "small_fronts_pivoted", "pivoted_diagonal", "permute_earlier_rows", "panel_rows_pivoted",
+                    "update_pivoted", "level_end", "invert_diagonal", "update_matrix_mixed", "diagonal_sweep"]
+
+    def launch_profile(self, which: str = "factor"):
+        """The launches of the last profiled factorisation ("factor") or solve ("solve"), in order: a list of
+        (kind, blocks, first column of the step, device seconds)."""
+        code = {"factor": 0, "solve": 1}[which]
+        total = ctypes.c_int64()
+        lib = nat.load()
+        _check(lib.oosgpu_factor_launch_profile(self._handle, code, 0, None, None, None, None, ctypes.byref(total)))
+        count = int(total.value)
+        kinds = np.zeros(max(count, 1), dtype=np.int32)
+        blocks = np.zeros(max(count, 1), dtype=np.int32)
+        k0 = np.zeros(max(count, 1), dtype=np.int32)
+        seconds = np.zeros(max(count, 1))
+        _check(lib.oosgpu_factor_launch_profile(self._handle, code, count, nat.ptr(kinds, nat.i32p),
+                                                nat.ptr(blocks, nat.i32p), nat.ptr(k0, nat.i32p),
+                                                nat.ptr(seconds, nat.f64p), ctypes.byref(total)))
+        return [(self.LAUNCH_KINDS[kinds[i]], int(blocks[i]), int(k0[i]), float(seconds[i])) for i in range(count)]
 
     def launch_counts(self, columns: int):
         """(kernels of one factorisation, kernels of one solve of `columns` right-hand sides)."""
