@@ -47,6 +47,9 @@ constexpr int TILE = 64;
 constexpr int MIXED_TILE = 128; // the tiles of the mixed-precision (tcgen05) update matrices
 constexpr int TILE_PAD = 8; // smem row stride 72 doubles: the m8n8k4 fragment loads take 2 wavefronts (no conflict)
 constexpr int TILE_THREADS = 128;
+// The columns of a large supernode one diagonal step of the solves covers (four 64 x 64 diagonal blocks; the products
+// with the rows below or above then run with K = SOLVE_STEP).
+constexpr int SOLVE_STEP = 256;
 
 __device__ __forceinline__ void dmma8x8x4(double (&d)[2], double a, double b)
 {
@@ -234,6 +237,41 @@ __device__ __forceinline__ void tileAccumulate(const TileOperands& op, double* s
         }
     }
     waitAsyncCopies<0>();
+}
+
+// acc += A B on one 64 x 64 tile with both operands in shared memory (TILE_THREADS threads, the fragments of
+// tileAccumulate): A(ii, p) = a[ii * lda + p], or a[p * lda + ii] when A_TRANSPOSED; B(p, jj) = b[p * ldb + jj];
+// p < k, k a multiple of 4, and A and B hold zeros (not garbage) wherever a product term lies outside their extents.
+// ldb = TILE + TILE_PAD keeps the B fragments free of bank conflicts.
+template <bool A_TRANSPOSED>
+__device__ __forceinline__ void sharedTileProduct(const double* a, int lda, const double* b, int ldb, int k,
+                                                  TileAccumulators& acc)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int wm = (warp >> 1) * 32;
+    const int wn = (warp & 1) * 32;
+#pragma unroll 4
+    for (int kk = 0; kk < k; kk += 4)
+    {
+        const int pr = kk + (lane & 3);
+        double fa[4];
+        double fb[4];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+        {
+            const int ii = wm + mi * 8 + (lane >> 2);
+            fa[mi] = A_TRANSPOSED ? a[pr * lda + ii] : a[ii * lda + pr];
+        }
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+            fb[ni] = b[pr * ldb + wn + ni * 8 + (lane >> 2)];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+                dmma8x8x4(acc[mi][ni], fa[mi], fb[ni]);
+    }
 }
 
 // C -= A B (D) on one 64 x 64 tile (tileAccumulate), C read, reduced and written once; op.lower keeps the elements

@@ -74,16 +74,24 @@ __global__ void pivotSummary(FactorArgs args, const std::int32_t* supernodeOfCol
 __global__ void forwardSmall(SolveArgs a, const std::int32_t* list, int cmax);
 __global__ void forwardGather(SolveArgs a, const TileTask* tasks);
 __global__ void invertDiagonal(FactorArgs args, const TileTask* tasks);
-// Dynamic shared memory of forwardDiagonal / backwardDiagonal for a tile of `width` columns.
-constexpr std::size_t diagonalSolveSmem(int width)
+// Dynamic shared memory of forwardDiagonal / backwardDiagonal: the tile pipeline, one block's inverse and a 64-row block
+// of TILE + TILE_PAD (laid out for the widest tile of right-hand sides).
+constexpr std::size_t STEP_SOLVE_SMEM = static_cast<std::size_t>(TILE_SMEM_DOUBLES + 64 * 65 + 64 * (TILE + TILE_PAD)) *
+                                        sizeof(double);
+// The inverse region of forwardSmall / backwardSmall for c4 (the columns rounded up to 4): c4 x (c4 + 1) values and
+// room for the tensor-core fragment reads of rows up to 63.
+__host__ __device__ constexpr int smallInverseDoubles(int c4)
 {
-    return static_cast<std::size_t>(64 * 65 + 64 * width) * sizeof(double);
+    return 64 * (c4 + 1) + 64;
 }
 // Dynamic shared memory of forwardSmall / backwardSmall for supernodes of at most `columns` columns: the tile
-// pipeline, the inverse (c x (c + 1)) and a c x width block.
-constexpr std::size_t smallSolveSmem(int columns, int width)
+// pipeline, the inverse region and an x_F block of c4 rows by TILE + TILE_PAD (laid out for the widest tile of
+// right-hand sides).
+constexpr std::size_t smallSolveSmem(int columns)
 {
-    return static_cast<std::size_t>(TILE_SMEM_DOUBLES + columns * (columns + 1) + columns * width) * sizeof(double);
+    return static_cast<std::size_t>(TILE_SMEM_DOUBLES + smallInverseDoubles((columns + 3) & ~3) +
+                                    ((columns + 3) & ~3) * (TILE + TILE_PAD)) *
+           sizeof(double);
 }
 __global__ void forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0);
 __global__ void forwardUpdate(SolveArgs a, const TileTask* tasks, int k0);

@@ -19,7 +19,6 @@ namespace oosgpu::device
 
 
 constexpr int SOLVE_BLOCK = 64;
-constexpr int SOLVE_THREADS = 256;
 
 // g += the children's update rows that land at the slots of a tile's rows (slotOf(ii) for the rows ii < rows, all
 // width columns), element (tileRow(mi), tileColumn(ni, h)) of the tile in g[mi][ni][h] as the tile products hold it.
@@ -87,16 +86,27 @@ __device__ __forceinline__ std::int64_t rowSlot(const SolveArgs& a, const FrontD
     return a.dimension + f.rowStart + k;
 }
 
+// The columns of a small supernode rounded up to the product's K step (4), and the leading dimension of the
+// x_F block in shared memory (conflict-free B fragments).
+__device__ __forceinline__ int roundFour(int c)
+{
+    return (c + 3) & ~3;
+}
+constexpr int XF_LD = TILE + TILE_PAD;
+
 // The strict lower triangle of a small supernode's L11^-1 (c <= 64) from the strict upper triangle of its diagonal
-// block: inv[i * (c + 1) + q] = L11^-1(i, q) for q < i < c (asynchronous copies, committed by the caller).
+// block: inv[i * (c4 + 1) + q] = L11^-1(i, q) for q < i < c, zero elsewhere in the c4 x c4 square (c4 = c rounded up
+// to 4); asynchronous copies, committed by the caller. The region holds smallInverseDoubles(c4) doubles, so that the
+// product's fragment reads of rows up to 63 stay inside it.
 __device__ __forceinline__ void stageSmallInverse(const double* panel, std::int64_t n, int c, double* inv)
 {
-    for (int e = threadIdx.x; e < c * c; e += blockDim.x)
+    const int c4 = roundFour(c);
+    for (int e = threadIdx.x; e < c4 * c4; e += blockDim.x)
     {
-        const int i = e / c;
-        const int q = e - i * c;
-        const bool inside = q < i;
-        copyAsync8(inv + i * (c + 1) + q, inside ? panel + q + static_cast<std::int64_t>(i) * n : panel, inside);
+        const int i = e / c4;
+        const int q = e - i * c4;
+        const bool inside = q < i && i < c;
+        copyAsync8(inv + i * (c4 + 1) + q, inside ? panel + q + static_cast<std::int64_t>(i) * n : panel, inside);
     }
 }
 
@@ -109,9 +119,9 @@ __device__ __forceinline__ void stageSmallInverse(const double* panel, std::int6
 __global__ void __launch_bounds__(TILE_THREADS) forwardSmall(SolveArgs a, const std::int32_t* list, int cmax)
 {
     extern __shared__ double stage[];
-    double* pipe = stage;                    // the tile pipeline
-    double* inv = stage + TILE_SMEM_DOUBLES; // c x (c + 1)
-    double* xF = inv + cmax * (cmax + 1);    // c x width
+    double* pipe = stage;                                      // the tile pipeline
+    double* inv = stage + TILE_SMEM_DOUBLES;                   // L11^-1, c4 x (c4 + 1)
+    double* xF = inv + smallInverseDoubles(roundFour(cmax));   // c4 x XF_LD
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
     const int c = f.c;
@@ -143,20 +153,36 @@ __global__ void __launch_bounds__(TILE_THREADS) forwardSmall(SolveArgs a, const 
                 {
                     const int ii = tileRow(mi);
                     const int jj = tileColumn(ni, h);
-                    if (ii < c && jj < w)
-                        xF[ii * w + jj] = g[mi][ni][h];
+                    if (ii < roundFour(c))
+                        xF[ii * XF_LD + jj] = ii < c && jj < w ? g[mi][ni][h] : 0.0;
                 }
     }
     waitAsyncCopies<0>();
     __syncthreads();
-    for (int e = threadIdx.x; e < c * w; e += blockDim.x)
+    // x_F = (I + strict lower of L11^-1) b on the tensor cores
     {
-        const int i = e / w;
-        const int col = e - i * w;
-        double sum = xF[e];
-        for (int q = 0; q < i; ++q)
-            sum += inv[i * (c + 1) + q] * xF[q * w + col];
-        xRows[e] = sum;
+        TileAccumulators t;
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+            {
+                t[mi][ni][0] = 0.0;
+                t[mi][ni][1] = 0.0;
+            }
+        sharedTileProduct<false>(inv, roundFour(c) + 1, xF, XF_LD, roundFour(c), t);
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                {
+                    const int ii = tileRow(mi);
+                    const int jj = tileColumn(ni, h);
+                    if (ii < c && jj < w)
+                        xRows[ii * w + jj] = xF[ii * XF_LD + jj] + t[mi][ni][h];
+                }
     }
     __syncthreads();
     double* own = a.updates + f.rowStart * w;
@@ -311,14 +337,13 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) invertDiagonal(FactorArgs args, c
             block[j + static_cast<std::int64_t>(i) * n] = x[i];
 }
 
-// The inverse of step k0's diagonal block staged in shared memory: inv[i * (SOLVE_BLOCK + 1) + q] = L11^-1(i, q) for
-// q < i (zero elsewhere), and the block's rows of X: b[i * w + col].
-__device__ __forceinline__ int stageInverse(const SolveArgs& a, const FrontDesc& f, int k0, double* inv, double* b,
-                                            double* xRows)
+// Stages the strict lower triangle of the inverse of the unit lower 64 x 64 diagonal block at column k0 of a large
+// supernode (kept in that block's strict upper triangle): inv[i * 65 + q] = L11^-1(i, q) for q < i < kb. Asynchronous
+// copies, committed by the caller.
+__device__ __forceinline__ void stageBlockInverse(const SolveArgs& a, const FrontDesc& f, int k0, int kb, double* inv)
 {
     constexpr int LD = SOLVE_BLOCK + 1;
     const std::int64_t n = f.c + f.r;
-    const int kb = min(SOLVE_BLOCK, f.c - k0);
     const double* block = a.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
     for (int e = threadIdx.x; e < SOLVE_BLOCK * SOLVE_BLOCK; e += blockDim.x)
     {
@@ -327,35 +352,94 @@ __device__ __forceinline__ int stageInverse(const SolveArgs& a, const FrontDesc&
         const bool inside = q < i && i < kb;
         copyAsync8(inv + i * LD + q, inside ? block + q + static_cast<std::int64_t>(i) * n : block, inside);
     }
-    for (int e = threadIdx.x; e < kb * a.width; e += blockDim.x)
-        copyAsync8(b + e, xRows + e, true);
-    commitAsyncCopies();
-    waitAsyncCopies<0>();
-    __syncthreads();
-    return kb;
 }
 
-// The unit lower triangle of step k0 of a large supernode (rows [k0, k0 + kb) of x_F) as the product with its inverse:
-// x_i = b_i + sum_{q < i} L11^-1(i, q) b_q, the terms in increasing q; every value of the 64 x width block is
-// independent (no chain through the triangle). Dynamic shared memory: (64 * 65 + 64 * width) doubles.
-__global__ void __launch_bounds__(SOLVE_THREADS) forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
+// x = (I + strict lower of L_jj^-1) b (TRANSPOSED: its transpose) for a 64 x 64 diagonal block of a large
+// supernode, b in shared memory (64 x XF_LD, zero beyond its jb rows and w columns), inv as stageBlockInverse leaves
+// it; the product on the tensor cores, x written to the jb x w rows of X at xBlock. acc is scratch.
+template <bool TRANSPOSED>
+__device__ __forceinline__ void stepTriangle(const double* inv, const double* b, int jb, int w, double* xBlock,
+                                             TileAccumulators& acc)
+{
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+        {
+            acc[mi][ni][0] = 0.0;
+            acc[mi][ni][1] = 0.0;
+        }
+    sharedTileProduct<TRANSPOSED>(inv, SOLVE_BLOCK + 1, b, XF_LD, SOLVE_BLOCK, acc);
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+            {
+                const int ii = tileRow(mi);
+                const int jj = tileColumn(ni, h);
+                if (ii < jb && jj < w)
+                    xBlock[ii * w + jj] = b[ii * XF_LD + jj] + acc[mi][ni][h];
+            }
+}
+
+// The rows [k0, k0 + kb) of x_F of a large supernode, kb <= SOLVE_STEP, by 64-row blocks j: b_j = x_j - L(j, <j) x_<j
+// (the earlier blocks of the step, one tile product on the FP64 tensor cores), then x_j = L_jj^-1 b_j as the product
+// with the stored inverse (every value independent). One block of TILE_THREADS per supernode; dynamic shared memory
+// stepSolveSmem(width).
+__global__ void __launch_bounds__(TILE_THREADS) forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
 {
     constexpr int LD = SOLVE_BLOCK + 1;
     extern __shared__ double stage[];
-    double* inv = stage;
-    double* b = stage + SOLVE_BLOCK * LD;
+    double* pipe = stage;
+    double* inv = stage + TILE_SMEM_DOUBLES;  // 64 x 65
+    double* b = inv + SOLVE_BLOCK * LD;       // 64 x XF_LD
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
-    double* xRows = a.x + static_cast<std::int64_t>(f.first + k0) * w;
-    const int kb = stageInverse(a, f, k0, inv, b, xRows);
-    for (int e = threadIdx.x; e < kb * w; e += blockDim.x)
+    const std::int64_t n = f.c + f.r;
+    const int kb = min(SOLVE_STEP, f.c - k0);
+    double* xStep = a.x + static_cast<std::int64_t>(f.first + k0) * w;
+    for (int j0 = 0; j0 < kb; j0 += SOLVE_BLOCK)
     {
-        const int i = e / w;
-        const int col = e - i * w;
-        double sum = b[e];
-        for (int q = 0; q < i; ++q)
-            sum += inv[i * LD + q] * b[q * w + col];
-        xRows[e] = sum;
+        const int jb = min(SOLVE_BLOCK, kb - j0);
+        stageBlockInverse(a, f, k0 + j0, jb, inv);
+        commitAsyncCopies();
+        TileOperands op;
+        op.a = a.panels + f.panel + (k0 + j0) + static_cast<std::int64_t>(k0) * n; // A(ii, p) = L(k0 + j0 + ii, k0 + p)
+        op.aRowStride = 1;
+        op.aColStride = n;
+        op.b = xStep;
+        op.bRowStride = 1;
+        op.bColStride = w;
+        op.bIndex = nullptr;
+        op.d = nullptr;
+        op.dStride = 0;
+        op.c = nullptr;
+        op.cRowStride = 0;
+        op.cColStride = 0;
+        op.m = jb;
+        op.n = w;
+        op.k = j0;
+        op.lower = false;
+        op.lowerOffset = 0;
+        TileAccumulators acc;
+        tileAccumulate(op, pipe, acc);
+        double* xBlock = xStep + static_cast<std::int64_t>(j0) * w;
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                {
+                    const int ii = tileRow(mi);
+                    const int jj = tileColumn(ni, h);
+                    b[ii * XF_LD + jj] = ii < jb && jj < w ? xBlock[ii * w + jj] - acc[mi][ni][h] : 0.0;
+                }
+        __syncthreads();
+        stepTriangle<false>(inv, b, jb, w, xBlock, acc);
+        __syncthreads();
     }
 }
 
@@ -392,7 +476,7 @@ __global__ void __launch_bounds__(TILE_THREADS) forwardUpdate(SolveArgs a, const
     op.cRowStride = w;
     op.cColStride = 1;
     op.n = w;
-    op.k = min(SOLVE_BLOCK, f.c - k0);
+    op.k = min(SOLVE_STEP, f.c - k0);
     op.lower = false;
     op.lowerOffset = 0;
     tileProduct(op, smem);
@@ -418,8 +502,8 @@ __global__ void diagonalSweep(SolveArgs a, const std::int32_t* supernodeOfColumn
 __global__ void __launch_bounds__(TILE_THREADS) backwardSmall(SolveArgs a, const std::int32_t* list, int cmax)
 {
     extern __shared__ double stage[];
-    double* pipe = stage;                    // the tile pipeline, then x_F (c x width)
-    double* inv = stage + TILE_SMEM_DOUBLES; // c x (c + 1)
+    double* pipe = stage;                    // the tile pipeline, then x_F (c4 x XF_LD)
+    double* inv = stage + TILE_SMEM_DOUBLES; // L11^-1, c4 x (c4 + 1)
     (void)cmax;
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
@@ -460,19 +544,32 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardSmall(SolveArgs a, const
             {
                 const int ii = tileRow(mi);
                 const int jj = tileColumn(ni, h);
-                if (ii < c && jj < w)
-                    xF[ii * w + jj] = xRows[ii * w + jj] - acc[mi][ni][h];
+                if (ii < roundFour(c))
+                    xF[ii * XF_LD + jj] = ii < c && jj < w ? xRows[ii * w + jj] - acc[mi][ni][h] : 0.0;
             }
     __syncthreads();
-    for (int e = threadIdx.x; e < c * w; e += blockDim.x)
-    {
-        const int q = e / w;
-        const int col = e - q * w;
-        double sum = xF[e];
-        for (int i = q + 1; i < c; ++i)
-            sum += inv[i * (c + 1) + q] * xF[i * w + col];
-        xRows[e] = sum;
-    }
+    // x_F = (I + strict lower of L11^-1)^T b on the tensor cores
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+        {
+            acc[mi][ni][0] = 0.0;
+            acc[mi][ni][1] = 0.0;
+        }
+    sharedTileProduct<true>(inv, roundFour(c) + 1, xF, XF_LD, roundFour(c), acc);
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+            {
+                const int ii = tileRow(mi);
+                const int jj = tileColumn(ni, h);
+                if (ii < c && jj < w)
+                    xRows[ii * w + jj] = xF[ii * XF_LD + jj] + acc[mi][ni][h];
+            }
 }
 
 // x_F -= L21^T X[R(s)] for a large supernode, by tiles of 64 of its columns (A = L21^T read along its rows).
@@ -504,26 +601,63 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardRows(SolveArgs a, const 
     tileProduct<true>(op, smem);
 }
 
-// The unit upper triangle L11^T of step k0 (rows [k0, k0 + kb) of x_F) as the product with the transposed inverse:
-// x_q = b_q + sum_{i > q} L11^-1(i, q) b_i, the terms in increasing i.
-__global__ void __launch_bounds__(SOLVE_THREADS) backwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
+// The rows [k0, k0 + kb) of x_F of a large supernode in the backward sweep, by 64-row blocks j from the last:
+// b_j = x_j - L(>j, j)^T x_>j (the later blocks of the step, one tile product), then x_j = L_jj^-T b_j as the product
+// with the transposed inverse. One block of TILE_THREADS per supernode; dynamic shared memory stepSolveSmem(width).
+__global__ void __launch_bounds__(TILE_THREADS) backwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
 {
     constexpr int LD = SOLVE_BLOCK + 1;
     extern __shared__ double stage[];
-    double* inv = stage;
-    double* b = stage + SOLVE_BLOCK * LD;
+    double* pipe = stage;
+    double* inv = stage + TILE_SMEM_DOUBLES;  // 64 x 65
+    double* b = inv + SOLVE_BLOCK * LD;       // 64 x XF_LD
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
-    double* xRows = a.x + static_cast<std::int64_t>(f.first + k0) * w;
-    const int kb = stageInverse(a, f, k0, inv, b, xRows);
-    for (int e = threadIdx.x; e < kb * w; e += blockDim.x)
+    const std::int64_t n = f.c + f.r;
+    const int kb = min(SOLVE_STEP, f.c - k0);
+    double* xStep = a.x + static_cast<std::int64_t>(f.first + k0) * w;
+    for (int j0 = ((kb - 1) / SOLVE_BLOCK) * SOLVE_BLOCK; j0 >= 0; j0 -= SOLVE_BLOCK)
     {
-        const int q = e / w;
-        const int col = e - q * w;
-        double sum = b[e];
-        for (int i = q + 1; i < kb; ++i)
-            sum += inv[i * LD + q] * b[i * w + col];
-        xRows[e] = sum;
+        const int jb = min(SOLVE_BLOCK, kb - j0);
+        stageBlockInverse(a, f, k0 + j0, jb, inv);
+        commitAsyncCopies();
+        const int later = j0 + jb;
+        TileOperands op;
+        // A(ii, p) = L(k0 + later + p, k0 + j0 + ii)
+        op.a = a.panels + f.panel + (k0 + later) + static_cast<std::int64_t>(k0 + j0) * n;
+        op.aRowStride = n;
+        op.aColStride = 1;
+        op.b = xStep + static_cast<std::int64_t>(later) * w;
+        op.bRowStride = 1;
+        op.bColStride = w;
+        op.bIndex = nullptr;
+        op.d = nullptr;
+        op.dStride = 0;
+        op.c = nullptr;
+        op.cRowStride = 0;
+        op.cColStride = 0;
+        op.m = jb;
+        op.n = w;
+        op.k = kb - later;
+        op.lower = false;
+        op.lowerOffset = 0;
+        TileAccumulators acc;
+        tileAccumulate<true>(op, pipe, acc);
+        double* xBlock = xStep + static_cast<std::int64_t>(j0) * w;
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                {
+                    const int ii = tileRow(mi);
+                    const int jj = tileColumn(ni, h);
+                    b[ii * XF_LD + jj] = ii < jb && jj < w ? xBlock[ii * w + jj] - acc[mi][ni][h] : 0.0;
+                }
+        __syncthreads();
+        stepTriangle<true>(inv, b, jb, w, xBlock, acc);
+        __syncthreads();
     }
 }
 
@@ -552,7 +686,7 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardUpdate(SolveArgs a, cons
     op.cColStride = 1;
     op.m = min(TILE, k0 - task.i0);
     op.n = w;
-    op.k = min(SOLVE_BLOCK, f.c - k0);
+    op.k = min(SOLVE_STEP, f.c - k0);
     op.lower = false;
     op.lowerOffset = 0;
     tileProduct<true>(op, smem);

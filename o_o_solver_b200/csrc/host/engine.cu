@@ -139,16 +139,16 @@ public:
         check(cudaFuncSetAttribute(device::panelRowsPivotedInverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(device::PANEL_ROWS_PIVOTED_SMEM)),
               "pivoted panel rows shared memory");
-        // The diagonal steps of the solves: the block's inverse and the rows of a 64-column tile.
+        // The diagonal steps of the solves: the tile pipeline, a block's inverse and the rows of a 64-column tile.
         for (const void* kernel : {reinterpret_cast<const void*>(device::forwardDiagonal),
                                    reinterpret_cast<const void*>(device::backwardDiagonal)})
             check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(device::diagonalSolveSmem(SOLVE_WIDTH))),
+                                       static_cast<int>(device::STEP_SOLVE_SMEM)),
                   "diagonal solve shared memory");
         for (const void* kernel : {reinterpret_cast<const void*>(device::forwardSmall),
                                    reinterpret_cast<const void*>(device::backwardSmall)})
             check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(device::smallSolveSmem(SOLVE_SMALL_COLUMNS, SOLVE_WIDTH))),
+                                       static_cast<int>(device::smallSolveSmem(SOLVE_SMALL_COLUMNS))),
                   "small solve shared memory");
         check(cudaStreamSynchronize(m_stream), "plan upload");
     }
@@ -1234,7 +1234,7 @@ private:
         {
             const std::int32_t* list = m_lists.get() + launch.offset;
             const device::TileTask* tiles = m_tiles.get() + launch.offset;
-            const std::size_t smallSmem = device::smallSolveSmem(std::max(launch.smemOrder, 1), args.width);
+            const std::size_t smallSmem = device::smallSolveSmem(std::max(launch.smemOrder, 1));
             const std::size_t record = beginSolveRecord(static_cast<std::int32_t>(launch.kind), launch.count, launch.k0);
             switch (launch.kind)
             {
@@ -1246,8 +1246,8 @@ private:
                 device::forwardGather<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles);
                 break;
             case LaunchKind::ForwardDiagonal:
-                device::forwardDiagonal<<<launch.count, 256, device::diagonalSolveSmem(args.width), m_stream>>>(
-                    args, list, launch.k0);
+                device::forwardDiagonal<<<launch.count, device::TILE_THREADS, device::STEP_SOLVE_SMEM,
+                                           m_stream>>>(args, list, launch.k0);
                 break;
             case LaunchKind::ForwardUpdate:
                 device::forwardUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles, launch.k0);
@@ -1260,8 +1260,8 @@ private:
                 device::backwardRows<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles);
                 break;
             case LaunchKind::BackwardDiagonal:
-                device::backwardDiagonal<<<launch.count, 256, device::diagonalSolveSmem(args.width), m_stream>>>(
-                    args, list, launch.k0);
+                device::backwardDiagonal<<<launch.count, device::TILE_THREADS, device::STEP_SOLVE_SMEM,
+                                            m_stream>>>(args, list, launch.k0);
                 break;
             case LaunchKind::BackwardUpdate:
                 device::backwardUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles, launch.k0);

@@ -526,7 +526,9 @@ Plan buildPlan(const Symbolic& symbolic)
         for (const std::int32_t s : members)
             for (std::int32_t k0 = 0; k0 < plan.fronts[static_cast<std::size_t>(s)].c; k0 += BLOCK)
                 inverseTasks.push_back({s, k0, 0, 0});
-        for (std::int32_t k0 = 0; k0 < maxColumns; k0 += BLOCK)
+        // Steps of SOLVE_STEP columns: the step's diagonal blocks in one launch, then its products with the rows below.
+        constexpr std::int32_t STEP = device::SOLVE_STEP;
+        for (std::int32_t k0 = 0; k0 < maxColumns; k0 += STEP)
         {
             std::vector<std::int32_t> diagonal;
             std::vector<TileTask> below;
@@ -536,7 +538,7 @@ Plan buildPlan(const Symbolic& symbolic)
                 if (f.c <= k0)
                     continue;
                 diagonal.push_back(s);
-                const std::int32_t kb = std::min(BLOCK, f.c - k0);
+                const std::int32_t kb = std::min(STEP, f.c - k0);
                 for (std::int32_t i0 = k0 + kb; i0 < f.c; i0 += device::TILE)
                     below.push_back({s, i0, 0, 0});
                 for (std::int32_t i0 = f.c; i0 < f.c + f.r; i0 += device::TILE)
@@ -559,10 +561,10 @@ Plan buildPlan(const Symbolic& symbolic)
                 rowTiles.push_back({s, i0, 0, 0});
         }
         addTiles(plan, backward, LaunchKind::BackwardRows, rowTiles);
-        const std::int32_t steps = (maxColumns + BLOCK - 1) / BLOCK;
+        const std::int32_t steps = (maxColumns + STEP - 1) / STEP;
         for (std::int32_t t = steps - 1; t >= 0; --t)
         {
-            const std::int32_t k0 = t * BLOCK;
+            const std::int32_t k0 = t * STEP;
             std::vector<std::int32_t> diagonal;
             std::vector<TileTask> above;
             for (const std::int32_t s : solveLarge)
