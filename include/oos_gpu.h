@@ -191,7 +191,8 @@ int oosgpu_factor_profile(oosgpu_factor* factor, int32_t enable);
  * tile (which 1), in launch order: kind (the plan's launch kinds: 0 small fronts, 1 assembly, 2 diagonal blocks,
  * 3 panel rows, 4 panel update, 5 update matrix, 6 forward small, 7 forward gather, 8 forward diagonal, 9 forward
  * update, 10 backward small, 11 backward rows, 12 backward diagonal, 13 backward update, 14-19 the indefinite
- * kinds, 20 diagonal inverses, 22 the diagonal sweep), blocks, first column of the step, device seconds. At most
+ * kinds, 20 diagonal inverses, 21 the mixed update matrix, 22 the sums of split backward products, 23 the
+ * diagonal sweep), blocks, first column of the step, device seconds. At most
  * `capacity` are written; *total is how many there are. */
 int oosgpu_factor_launch_profile(oosgpu_factor* factor, int32_t which, int64_t capacity, int32_t* kinds,
                                  int32_t* counts, int32_t* k0, double* seconds, int64_t* total);

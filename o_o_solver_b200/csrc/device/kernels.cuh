@@ -55,6 +55,8 @@ struct SolveArgs
     const std::int32_t* gatherRows;
     const std::int32_t* perm;
     int dimension;
+    // The partial products of split backward row tiles: slot q at rowPartials + q * TILE * TILE (64 x 64 by rows).
+    double* rowPartials;
 };
 
 __global__ void assembleFronts(FactorArgs args, const AssemblyTask* tasks, std::int32_t* structureError);
@@ -98,6 +100,7 @@ __global__ void forwardUpdate(SolveArgs a, const TileTask* tasks, int k0);
 __global__ void diagonalSweep(SolveArgs a, const std::int32_t* supernodeOfColumn, int dimension);
 __global__ void backwardSmall(SolveArgs a, const std::int32_t* list, int cmax);
 __global__ void backwardRows(SolveArgs a, const TileTask* tasks);
+__global__ void backwardRowsReduce(SolveArgs a, const TileTask* tasks);
 __global__ void backwardDiagonal(SolveArgs a, const std::int32_t* list, int k0);
 __global__ void backwardUpdate(SolveArgs a, const TileTask* tasks, int k0);
 __global__ void toRows(const double* b, std::int64_t ld, int c0, int width, int dimension, double* x,

@@ -572,7 +572,9 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardSmall(SolveArgs a, const
             }
 }
 
-// x_F -= L21^T X[R(s)] for a large supernode, by tiles of 64 of its columns (A = L21^T read along its rows).
+// x_F -= L21^T X[R(s)] for a large supernode, by tiles of 64 of its columns (A = L21^T read along its rows). A task
+// covers the rows [j0, j0 + SOLVE_ROWS_CHUNK) of R(s) and writes its partial product to slot k0 when R(s) is split
+// (k0 >= 0), or all of R(s) straight into x_F (k0 = -1).
 __global__ void __launch_bounds__(TILE_THREADS) backwardRows(SolveArgs a, const TileTask* tasks)
 {
     __shared__ double smem[TILE_SMEM_DOUBLES];
@@ -581,13 +583,14 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardRows(SolveArgs a, const 
     const std::int64_t n = f.c + f.r;
     const int w = a.width;
     TileOperands op;
-    op.a = a.panels + f.panel + f.c + static_cast<std::int64_t>(task.i0) * n;
+    // A(ii, p) = L(c + j0 + p, i0 + ii)
+    op.a = a.panels + f.panel + f.c + task.j0 + static_cast<std::int64_t>(task.i0) * n;
     op.aRowStride = n;
     op.aColStride = 1;
     op.b = a.x;
     op.bRowStride = 1;
     op.bColStride = w;
-    op.bIndex = a.rows + f.rowStart;
+    op.bIndex = a.rows + f.rowStart + task.j0;
     op.d = nullptr;
     op.dStride = 0;
     op.c = a.x + static_cast<std::int64_t>(f.first + task.i0) * w;
@@ -595,10 +598,44 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardRows(SolveArgs a, const 
     op.cColStride = 1;
     op.m = min(TILE, f.c - task.i0);
     op.n = w;
-    op.k = f.r;
+    op.k = task.k0 < 0 ? f.r : min(SOLVE_ROWS_CHUNK, f.r - task.j0);
     op.lower = false;
     op.lowerOffset = 0;
-    tileProduct<true>(op, smem);
+    if (task.k0 < 0)
+    {
+        tileProduct<true>(op, smem);
+        return;
+    }
+    TileAccumulators acc;
+    tileAccumulate<true>(op, smem, acc);
+    double* partial = a.rowPartials + static_cast<std::int64_t>(task.k0) * (TILE * TILE);
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                partial[tileRow(mi) * TILE + tileColumn(ni, h)] = acc[mi][ni][h];
+}
+
+// x_F tile -= the sum of its split partial products (task: front, i0, first slot j0, chunks k0), summed in chunk order.
+__global__ void __launch_bounds__(TILE_THREADS) backwardRowsReduce(SolveArgs a, const TileTask* tasks)
+{
+    const TileTask task = tasks[blockIdx.x];
+    const FrontDesc f = a.fronts[task.front];
+    const int w = a.width;
+    const int m = min(TILE, f.c - task.i0);
+    double* xTile = a.x + static_cast<std::int64_t>(f.first + task.i0) * w;
+    const double* partials = a.rowPartials + static_cast<std::int64_t>(task.j0) * (TILE * TILE);
+    for (int e = threadIdx.x; e < m * w; e += blockDim.x)
+    {
+        const int ii = e / w;
+        const int jj = e - ii * w;
+        double sum = 0.0;
+        for (int q = 0; q < task.k0; ++q)
+            sum += partials[static_cast<std::int64_t>(q) * (TILE * TILE) + ii * TILE + jj];
+        xTile[e] -= sum;
+    }
 }
 
 // The rows [k0, k0 + kb) of x_F of a large supernode in the backward sweep, by 64-row blocks j from the last:

@@ -107,6 +107,9 @@ public:
         m_relpos.upload(m_plan.relpos, m_stream, "plan: positions");
         m_gatherStart.upload(m_plan.gatherStart, m_stream, "plan: gather lists");
         m_gatherRows.upload(m_plan.gatherRows, m_stream, "plan: gather lists");
+        if (m_plan.rowPartialSlots > 0)
+            m_rowPartials.allocate(static_cast<std::size_t>(m_plan.rowPartialSlots) * device::TILE * device::TILE,
+                                   "solve: split products");
         m_supernodeOfColumn.upload(m_plan.supernodeOfColumn, m_stream, "plan: columns");
         m_lists.upload(m_plan.lists, m_stream, "plan: lists");
         m_tiles.upload(m_plan.tiles, m_stream, "plan: tiles");
@@ -648,7 +651,8 @@ public:
                                m_gatherStart.get(),
                                m_gatherRows.get(),
                                m_pivoted ? m_perm.get() : nullptr,
-                               n};
+                               n,
+                               m_rowPartials.get()};
         m_solveRecords.clear();
         runSweep(args, m_plan.forwardLaunches);
         const std::size_t record = beginSolveRecord(DIAGONAL_SWEEP_KIND, static_cast<std::int32_t>(blocksFor(items, 256)), 0);
@@ -1259,6 +1263,9 @@ private:
             case LaunchKind::BackwardRows:
                 device::backwardRows<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles);
                 break;
+            case LaunchKind::BackwardRowsReduce:
+                device::backwardRowsReduce<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles);
+                break;
             case LaunchKind::BackwardDiagonal:
                 device::backwardDiagonal<<<launch.count, device::TILE_THREADS, device::STEP_SOLVE_SMEM,
                                             m_stream>>>(args, list, launch.k0);
@@ -1308,6 +1315,7 @@ private:
     DeviceArray<std::int32_t> m_relpos;
     DeviceArray<std::int64_t> m_gatherStart;
     DeviceArray<std::int32_t> m_gatherRows;
+    DeviceArray<double> m_rowPartials;
     DeviceArray<std::int32_t> m_supernodeOfColumn;
     DeviceArray<std::int32_t> m_lists;
     DeviceArray<device::TileTask> m_tiles;
@@ -1376,7 +1384,7 @@ private:
         std::int32_t k0;
     };
     // The kind code of the diagonal sweep in a solve's launch profile (after the plan's launch kinds).
-    static constexpr std::int32_t DIAGONAL_SWEEP_KIND = 22;
+    static constexpr std::int32_t DIAGONAL_SWEEP_KIND = 23;
     std::vector<SolveRecord> m_solveRecords;
     std::vector<cudaEvent_t> m_solveEvents;
     bool m_annotated = false;

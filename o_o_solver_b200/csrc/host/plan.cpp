@@ -551,16 +551,34 @@ Plan buildPlan(const Symbolic& symbolic)
         // ---- backward sweep (collected per level, emitted top level first) ----
         std::vector<Launch>& backward = backwardByLevel[static_cast<std::size_t>(level)];
         addList(plan, backward, LaunchKind::BackwardSmall, solveSmall, 0, maxSmallColumns);
+        // x_F -= L21^T X[R(s)] by 64-column tiles; R(s) longer than SOLVE_ROWS_CHUNK in chunks (task j0: the chunk's
+        // first row, k0: its partial's slot, -1 for an unsplit tile), then the partials summed in chunk order.
         std::vector<TileTask> rowTiles;
+        std::vector<TileTask> rowSums;
+        std::int64_t slots = 0;
         for (const std::int32_t s : solveLarge)
         {
             const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
             if (f.r == 0)
                 continue;
+            const std::int32_t chunks = (f.r + device::SOLVE_ROWS_CHUNK - 1) / device::SOLVE_ROWS_CHUNK;
             for (std::int32_t i0 = 0; i0 < f.c; i0 += device::TILE)
-                rowTiles.push_back({s, i0, 0, 0});
+            {
+                if (chunks == 1)
+                {
+                    rowTiles.push_back({s, i0, 0, -1});
+                    continue;
+                }
+                rowSums.push_back({s, i0, static_cast<std::int32_t>(slots), chunks});
+                for (std::int32_t q = 0; q < chunks; ++q)
+                    rowTiles.push_back({s, i0, q * device::SOLVE_ROWS_CHUNK, static_cast<std::int32_t>(slots++)});
+            }
         }
+        if (slots > INT32_MAX)
+            throw Error(STATUS_INVALID_ARGUMENT, "plan: too many split backward products in one level");
+        plan.rowPartialSlots = std::max(plan.rowPartialSlots, slots);
         addTiles(plan, backward, LaunchKind::BackwardRows, rowTiles);
+        addTiles(plan, backward, LaunchKind::BackwardRowsReduce, rowSums);
         const std::int32_t steps = (maxColumns + STEP - 1) / STEP;
         for (std::int32_t t = steps - 1; t >= 0; --t)
         {

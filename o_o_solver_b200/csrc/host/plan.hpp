@@ -48,7 +48,9 @@ enum class LaunchKind : int
     // after a factorisation: the inverses of the unit lower diagonal blocks the solves apply
     InvertDiagonal,
     // mixed precision: the update matrices by 128 x 128 tiles on tcgen05 (3xTF32), in place of UpdateMatrix
-    UpdateMatrixMixed
+    UpdateMatrixMixed,
+    // the sums of the split products of BackwardRows (supernodes with more than SOLVE_ROWS_CHUNK rows)
+    BackwardRowsReduce
 };
 
 // One batched launch: `count` items from `offset` in the array of its kind (front lists: int32; tiles: TileTask;
@@ -87,6 +89,8 @@ struct Plan
     std::int64_t panelValues = 0;
     std::int64_t updateValues = 0;
     std::int64_t rowEntries = 0;
+    // Partial products of the split BackwardRows tiles one level needs at most (each 64 x 64 values).
+    std::int64_t rowPartialSlots = 0;
     std::int32_t largestSmallOrder = 0;
     double flops = 0.0;
     std::int64_t factorEntries = 0;
