@@ -45,7 +45,11 @@ struct AssemblyTask
 
 constexpr int TILE = 64;
 constexpr int MIXED_TILE = 128; // the tiles of the mixed-precision (tcgen05) update matrices
-constexpr int TILE_PAD = 8; // smem row stride 72 doubles: the m8n8k4 fragment loads take 2 wavefronts (no conflict)
+// Shared-memory row strides of the tiles: 68 doubles, 4 more than a multiple of 16, so that the m8n8k4 fragment loads
+// (lanes 4 apart differ by one row) hit 16 distinct 8-byte banks in each half-warp.
+constexpr int TILE_PAD = 4;
+// The row stride of a staged 64 x 64 inverse block read as an m8n8k4 operand (either orientation): conflict-free too.
+constexpr int INVERSE_LD = TILE + TILE_PAD;
 constexpr int TILE_THREADS = 128;
 // The columns of a large supernode one diagonal step of the solves covers (four 64 x 64 diagonal blocks; the products
 // with the rows below or above then run with K = SOLVE_STEP).
@@ -56,7 +60,7 @@ constexpr int SOLVE_ROWS_CHUNK = 512;
 
 __device__ __forceinline__ void dmma8x8x4(double (&d)[2], double a, double b)
 {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                  : "+d"(d[0]), "+d"(d[1])
                  : "d"(a), "d"(b));
 }

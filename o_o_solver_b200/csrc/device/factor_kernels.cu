@@ -259,20 +259,27 @@ __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int3
 // ------------------------------------------------------------------------------------------------------------------
 constexpr int BLOCK = 64;
 
-__global__ void __launch_bounds__(BLOCK) diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0)
+// The diagonal block's LDL^T and the inverse of its unit lower factor, in shared memory by DIAGONAL_THREADS threads
+// with loops kept rolled: a single block runs at the top of the tree, where every instruction is fetched once, so the
+// code stays small enough for the instruction cache (a fully unrolled register version stalled on instruction fetch).
+//   elimination: for k = 0, 1, ...: l_ik = a_ik / d_k, then a_ij -= l_ik (l_jk d_k) for k < j <= i, each element's
+//   terms in k order as the reference's unblocked algorithm;
+//   inverse: X = L11^-1 row by row, X(i, j) = -sum_{j <= q < i} L(i, q) X(q, j) (four interleaved partial sums), kept
+//   in the strict upper triangle (X(i, j) at (j, i)), where panelRowsInverse and the solves read it.
+__global__ void __launch_bounds__(DIAGONAL_THREADS) diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0)
 {
-    __shared__ double a[BLOCK * (BLOCK + 1)];
-    __shared__ double column[BLOCK]; // column k of the step, before scaling
-    __shared__ double scaled[BLOCK]; // w_i = l_ik d_k of the step
+    constexpr int LD = BLOCK + 1;
+    constexpr int PARTS = DIAGONAL_THREADS / BLOCK;
+    __shared__ double a[BLOCK * LD];
+    __shared__ double scaled[BLOCK];         // w_j = l_jk d_k of the step
+    __shared__ double partial[PARTS * BLOCK]; // partial sums of a row of the inverse
     const std::int32_t s = list[blockIdx.x];
     const FrontDesc f = args.fronts[s];
     const int n = f.c + f.r;
     const int kb = min(BLOCK, f.c - k0);
-    constexpr int LD = BLOCK + 1;
     double* panel = args.panels + f.panel + static_cast<std::int64_t>(k0) * n + k0;
-    const int t = threadIdx.x; // this thread's row of the block
-    // Staged by asynchronous copies (all of a thread's loads in flight at once), zeros outside the block.
-    for (int e = t; e < BLOCK * BLOCK; e += BLOCK)
+    const int t = threadIdx.x;
+    for (int e = t; e < BLOCK * BLOCK; e += DIAGONAL_THREADS)
     {
         const int j = e / BLOCK;
         const int i = e - j * BLOCK;
@@ -282,72 +289,62 @@ __global__ void __launch_bounds__(BLOCK) diagonalBlocks(FactorArgs args, const s
     commitAsyncCopies();
     waitAsyncCopies<0>();
     __syncthreads();
-    // Row t in registers; the right-looking chain of the reference per element (l_ik = a_ik / d_k, then
-    // a_ij -= l_ik (l_jk d_k) for k increasing), two barriers of two warps per column.
-    double r[BLOCK];
-#pragma unroll
-    for (int j = 0; j < BLOCK; ++j)
-        r[j] = a[t + j * LD];
-#pragma unroll
-    for (int k = 0; k < BLOCK; ++k)
+    const int row = t & (BLOCK - 1);
+    const int part = t / BLOCK;
+#pragma unroll 1
+    for (int k = 0; k < kb; ++k)
     {
-        if (k < kb)
+        const double pivot = a[k + k * LD];
+        if (t == 0 && isBadPivot(pivot))
+            atomicMin(args.zeroPivot + s, k0 + k);
+        if (t > k && t < kb)
         {
-            if (t >= k)
-                column[t] = r[k];
-            __syncthreads();
-            const double pivot = column[k];
-            if (t == k && isBadPivot(pivot))
-                atomicMin(args.zeroPivot + s, k0 + k);
-            double l = 0.0;
-            if (t > k)
-            {
-                l = column[t] / pivot;
-                r[k] = l;
-                scaled[t] = l * pivot;
-            }
-            __syncthreads();
-            if (t > k)
-            {
-#pragma unroll
-                for (int j = k + 1; j < BLOCK; ++j)
-                    if (j <= t)
-                        r[j] -= l * scaled[j];
-            }
+            const double l = a[t + k * LD] / pivot;
+            a[t + k * LD] = l;
+            scaled[t] = l * pivot;
         }
+        __syncthreads();
+        if (row > k && row < kb)
+        {
+            const double l = a[row + k * LD];
+#pragma unroll 4
+            for (int j = k + 1 + part; j <= row; j += PARTS)
+                a[row + j * LD] -= l * scaled[j];
+        }
+        __syncthreads();
     }
-    // The factor back (lower triangle and D) and into shared memory for the inverse.
-#pragma unroll
-    for (int j = 0; j < BLOCK; ++j)
-        if (j <= t && t < kb)
-        {
-            panel[t + static_cast<std::int64_t>(j) * n] = r[j];
-            a[t + j * LD] = r[j];
-        }
-    __syncthreads();
-    // L11^-1 into the block's strict upper triangle (L11^-1(i, j) at (j, i)): thread j carries column j of the inverse
-    // through the forward substitution of e_j in registers. panelRowsInverse reads it for the rows below; the solves'
-    // diagonal steps read it too.
-    const int j = t;
-    if (j >= kb)
-        return;
-    double x[BLOCK];
-#pragma unroll
-    for (int i = 0; i < BLOCK; ++i)
-        x[i] = i == j ? 1.0 : 0.0;
-#pragma unroll
-    for (int i = 1; i < BLOCK; ++i)
+    // the inverse, row i from rows < i (thread (part, j): the terms q = part, part + PARTS, ... of X(i, j))
+#pragma unroll 1
+    for (int i = 1; i < kb; ++i)
     {
-        double v = x[i];
+        const int j = row;
+        double sum = 0.0;
+#pragma unroll 4
+        for (int q = part; q < i; q += PARTS)
+        {
+            const double x = q > j ? a[j + q * LD] : (q == j ? 1.0 : 0.0);
+            sum += a[i + q * LD] * x;
+        }
+        partial[part * BLOCK + j] = sum;
+        __syncthreads();
+        if (t < i)
+        {
+            double total = partial[t];
 #pragma unroll
-        for (int q = 0; q < i; ++q)
-            v -= a[i + q * LD] * x[q];
-        x[i] = v;
+            for (int p = 1; p < PARTS; ++p)
+                total += partial[p * BLOCK + t];
+            a[t + i * LD] = -total;
+        }
+        __syncthreads();
     }
-#pragma unroll
-    for (int i = 1; i < BLOCK; ++i)
-        if (i > j && i < kb)
-            panel[j + static_cast<std::int64_t>(i) * n] = x[i];
+    // L and D (lower triangle) and L11^-1 (strict upper triangle) back into the panel
+    for (int e = t; e < BLOCK * BLOCK; e += DIAGONAL_THREADS)
+    {
+        const int j = e / BLOCK;
+        const int i = e - j * BLOCK;
+        if (i < kb && j < kb)
+            panel[i + static_cast<std::int64_t>(j) * n] = a[i + j * LD];
+    }
 }
 
 // The rows below step k0's diagonal block, L21 = A21 L11^-T D^-1, as products on the FP64 tensor cores: for each

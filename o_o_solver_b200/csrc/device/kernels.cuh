@@ -61,6 +61,7 @@ struct SolveArgs
 
 __global__ void assembleFronts(FactorArgs args, const AssemblyTask* tasks, std::int32_t* structureError);
 __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int32_t* structureError);
+constexpr int DIAGONAL_THREADS = 256;
 __global__ void diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0);
 __global__ void panelRowsInverse(FactorArgs args, const TileTask* tasks, int k0);
 constexpr std::size_t PANEL_ROWS_INVERSE_SMEM = (2 * 64 * (TILE + TILE_PAD) + 64) * sizeof(double);
@@ -78,13 +79,19 @@ __global__ void forwardGather(SolveArgs a, const TileTask* tasks);
 __global__ void invertDiagonal(FactorArgs args, const TileTask* tasks);
 // Dynamic shared memory of forwardDiagonal / backwardDiagonal: the tile pipeline, one block's inverse and a 64-row block
 // of TILE + TILE_PAD (laid out for the widest tile of right-hand sides).
-constexpr std::size_t STEP_SOLVE_SMEM = static_cast<std::size_t>(TILE_SMEM_DOUBLES + 64 * 65 + 64 * (TILE + TILE_PAD)) *
+constexpr std::size_t STEP_SOLVE_SMEM = static_cast<std::size_t>(TILE_SMEM_DOUBLES + 64 * INVERSE_LD + 64 * (TILE + TILE_PAD)) *
                                         sizeof(double);
-// The inverse region of forwardSmall / backwardSmall for c4 (the columns rounded up to 4): c4 x (c4 + 1) values and
-// room for the tensor-core fragment reads of rows up to 63.
+// The row stride of a small supernode's staged inverse for c4 (its columns rounded up to 4): at least c4 and 4 more than
+// a multiple of 16 (conflict-free fragment reads).
+__host__ __device__ constexpr int smallInverseLd(int c4)
+{
+    return (c4 + 11) / 16 * 16 + 4;
+}
+// The inverse region of forwardSmall / backwardSmall for c4: c4 rows of smallInverseLd(c4) and room for the
+// tensor-core fragment reads of rows up to 63.
 __host__ __device__ constexpr int smallInverseDoubles(int c4)
 {
-    return 64 * (c4 + 1) + 64;
+    return 64 * smallInverseLd(c4) + 64;
 }
 // Dynamic shared memory of forwardSmall / backwardSmall for supernodes of at most `columns` columns: the tile
 // pipeline, the inverse region and an x_F block of c4 rows by TILE + TILE_PAD (laid out for the widest tile of

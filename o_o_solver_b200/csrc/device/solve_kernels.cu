@@ -95,8 +95,8 @@ __device__ __forceinline__ int roundFour(int c)
 constexpr int XF_LD = TILE + TILE_PAD;
 
 // The strict lower triangle of a small supernode's L11^-1 (c <= 64) from the strict upper triangle of its diagonal
-// block: inv[i * (c4 + 1) + q] = L11^-1(i, q) for q < i < c, zero elsewhere in the c4 x c4 square (c4 = c rounded up
-// to 4); asynchronous copies, committed by the caller. The region holds smallInverseDoubles(c4) doubles, so that the
+// block: inv[i * smallInverseLd(c4) + q] = L11^-1(i, q) for q < i < c, zero elsewhere in the c4 x c4 square (c4 = c
+// rounded up to 4); asynchronous copies, committed by the caller. The region holds smallInverseDoubles(c4) doubles, so that the
 // product's fragment reads of rows up to 63 stay inside it.
 __device__ __forceinline__ void stageSmallInverse(const double* panel, std::int64_t n, int c, double* inv)
 {
@@ -106,7 +106,8 @@ __device__ __forceinline__ void stageSmallInverse(const double* panel, std::int6
         const int i = e / c4;
         const int q = e - i * c4;
         const bool inside = q < i && i < c;
-        copyAsync8(inv + i * (c4 + 1) + q, inside ? panel + q + static_cast<std::int64_t>(i) * n : panel, inside);
+        copyAsync8(inv + i * smallInverseLd(c4) + q, inside ? panel + q + static_cast<std::int64_t>(i) * n : panel,
+                   inside);
     }
 }
 
@@ -120,7 +121,7 @@ __global__ void __launch_bounds__(TILE_THREADS) forwardSmall(SolveArgs a, const 
 {
     extern __shared__ double stage[];
     double* pipe = stage;                                      // the tile pipeline
-    double* inv = stage + TILE_SMEM_DOUBLES;                   // L11^-1, c4 x (c4 + 1)
+    double* inv = stage + TILE_SMEM_DOUBLES;                   // L11^-1, c4 rows of smallInverseLd(c4)
     double* xF = inv + smallInverseDoubles(roundFour(cmax));   // c4 x XF_LD
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
@@ -170,7 +171,7 @@ __global__ void __launch_bounds__(TILE_THREADS) forwardSmall(SolveArgs a, const 
                 t[mi][ni][0] = 0.0;
                 t[mi][ni][1] = 0.0;
             }
-        sharedTileProduct<false>(inv, roundFour(c) + 1, xF, XF_LD, roundFour(c), t);
+        sharedTileProduct<false>(inv, smallInverseLd(roundFour(c)), xF, XF_LD, roundFour(c), t);
 #pragma unroll
         for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -338,11 +339,11 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) invertDiagonal(FactorArgs args, c
 }
 
 // Stages the strict lower triangle of the inverse of the unit lower 64 x 64 diagonal block at column k0 of a large
-// supernode (kept in that block's strict upper triangle): inv[i * 65 + q] = L11^-1(i, q) for q < i < kb. Asynchronous
-// copies, committed by the caller.
+// supernode (kept in that block's strict upper triangle): inv[i * INVERSE_LD + q] = L11^-1(i, q) for q < i < kb.
+// Asynchronous copies, committed by the caller.
 __device__ __forceinline__ void stageBlockInverse(const SolveArgs& a, const FrontDesc& f, int k0, int kb, double* inv)
 {
-    constexpr int LD = SOLVE_BLOCK + 1;
+    constexpr int LD = INVERSE_LD;
     const std::int64_t n = f.c + f.r;
     const double* block = a.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
     for (int e = threadIdx.x; e < SOLVE_BLOCK * SOLVE_BLOCK; e += blockDim.x)
@@ -369,7 +370,7 @@ __device__ __forceinline__ void stepTriangle(const double* inv, const double* b,
             acc[mi][ni][0] = 0.0;
             acc[mi][ni][1] = 0.0;
         }
-    sharedTileProduct<TRANSPOSED>(inv, SOLVE_BLOCK + 1, b, XF_LD, SOLVE_BLOCK, acc);
+    sharedTileProduct<TRANSPOSED>(inv, INVERSE_LD, b, XF_LD, SOLVE_BLOCK, acc);
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -387,13 +388,13 @@ __device__ __forceinline__ void stepTriangle(const double* inv, const double* b,
 // The rows [k0, k0 + kb) of x_F of a large supernode, kb <= SOLVE_STEP, by 64-row blocks j: b_j = x_j - L(j, <j) x_<j
 // (the earlier blocks of the step, one tile product on the FP64 tensor cores), then x_j = L_jj^-1 b_j as the product
 // with the stored inverse (every value independent). One block of TILE_THREADS per supernode; dynamic shared memory
-// stepSolveSmem(width).
+// STEP_SOLVE_SMEM.
 __global__ void __launch_bounds__(TILE_THREADS) forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
 {
-    constexpr int LD = SOLVE_BLOCK + 1;
+    constexpr int LD = INVERSE_LD;
     extern __shared__ double stage[];
     double* pipe = stage;
-    double* inv = stage + TILE_SMEM_DOUBLES;  // 64 x 65
+    double* inv = stage + TILE_SMEM_DOUBLES;  // 64 x INVERSE_LD
     double* b = inv + SOLVE_BLOCK * LD;       // 64 x XF_LD
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
@@ -503,7 +504,7 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardSmall(SolveArgs a, const
 {
     extern __shared__ double stage[];
     double* pipe = stage;                    // the tile pipeline, then x_F (c4 x XF_LD)
-    double* inv = stage + TILE_SMEM_DOUBLES; // L11^-1, c4 x (c4 + 1)
+    double* inv = stage + TILE_SMEM_DOUBLES; // L11^-1, c4 rows of smallInverseLd(c4)
     (void)cmax;
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;
@@ -557,7 +558,7 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardSmall(SolveArgs a, const
             acc[mi][ni][0] = 0.0;
             acc[mi][ni][1] = 0.0;
         }
-    sharedTileProduct<true>(inv, roundFour(c) + 1, xF, XF_LD, roundFour(c), acc);
+    sharedTileProduct<true>(inv, smallInverseLd(roundFour(c)), xF, XF_LD, roundFour(c), acc);
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -640,13 +641,13 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardRowsReduce(SolveArgs a, 
 
 // The rows [k0, k0 + kb) of x_F of a large supernode in the backward sweep, by 64-row blocks j from the last:
 // b_j = x_j - L(>j, j)^T x_>j (the later blocks of the step, one tile product), then x_j = L_jj^-T b_j as the product
-// with the transposed inverse. One block of TILE_THREADS per supernode; dynamic shared memory stepSolveSmem(width).
+// with the transposed inverse. One block of TILE_THREADS per supernode; dynamic shared memory STEP_SOLVE_SMEM.
 __global__ void __launch_bounds__(TILE_THREADS) backwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
 {
-    constexpr int LD = SOLVE_BLOCK + 1;
+    constexpr int LD = INVERSE_LD;
     extern __shared__ double stage[];
     double* pipe = stage;
-    double* inv = stage + TILE_SMEM_DOUBLES;  // 64 x 65
+    double* inv = stage + TILE_SMEM_DOUBLES;  // 64 x INVERSE_LD
     double* b = inv + SOLVE_BLOCK * LD;       // 64 x XF_LD
     const FrontDesc f = a.fronts[list[blockIdx.x]];
     const int w = a.width;

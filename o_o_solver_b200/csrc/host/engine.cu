@@ -1211,8 +1211,8 @@ private:
                                                                            m_structureError.get());
                 break;
             case LaunchKind::DiagonalBlocks:
-                device::diagonalBlocks<<<launch.count, 64, 0, m_stream>>>(args, m_lists.get() + launch.offset,
-                                                                          launch.k0);
+                device::diagonalBlocks<<<launch.count, device::DIAGONAL_THREADS, 0, m_stream>>>(
+                    args, m_lists.get() + launch.offset, launch.k0);
                 break;
             case LaunchKind::PanelRows:
                 device::panelRowsInverse<<<launch.count, device::TILE_THREADS, device::PANEL_ROWS_INVERSE_SMEM,

@@ -54,7 +54,8 @@ def test_mixed_factor_refines_to_fp64(size, lib, gpu):
     assert refined.backward_error <= 1e-13 and 1 <= refined.steps <= 5, refined
     exact = torch.empty_like(b)
     linalg.solve_refined(fp64, b.t(), exact.t(), tolerance=1e-15, max_steps=0)
-    difference = (x - exact).norm(dim=1) / exact.norm(dim=1)
+    # the hexahedral block's first load column is zero (no pressure): its solution is zero in both forms
+    difference = (x - exact).norm(dim=1) / exact.norm(dim=1).clamp_min(1e-300)
     assert float(difference.max()) <= 1e-9
 
 
