@@ -54,6 +54,9 @@ constexpr int TILE_THREADS = 128;
 // The columns of a large supernode one diagonal step of the solves covers (four 64 x 64 diagonal blocks; the products
 // with the rows below or above then run with K = SOLVE_STEP).
 constexpr int SOLVE_STEP = 256;
+// The columns of a macro panel of the factorisation: the 64-column steps inside it update its own later columns, and
+// once it is done it updates the rest of the front's panel in one product of K = PANEL_MACRO.
+constexpr int PANEL_MACRO = 256;
 // The rows of R(s) one block of the backward product x_F -= L21^T X[R(s)] takes; longer R(s) are split into chunks
 // whose partial products are summed in chunk order.
 constexpr int SOLVE_ROWS_CHUNK = 512;

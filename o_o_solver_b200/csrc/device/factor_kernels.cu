@@ -445,7 +445,8 @@ __global__ void __launch_bounds__(TILE_THREADS) panelRowsInverse(FactorArgs args
     }
 }
 
-// Trailing panel update of step t: columns [o, c), rows [o, n), o = k0 + 64, K = the step's 64 columns.
+// Trailing panel update: the tile (i0, j0) of the panel's columns minus the products with the K = task.k0 columns from
+// k0 (a 64-column step within its macro panel, or a finished macro panel of PANEL_MACRO columns).
 __global__ void __launch_bounds__(TILE_THREADS) panelUpdate(FactorArgs args, const TileTask* tasks, int k0)
 {
     __shared__ double smem[TILE_SMEM_DOUBLES];
@@ -468,7 +469,7 @@ __global__ void __launch_bounds__(TILE_THREADS) panelUpdate(FactorArgs args, con
     op.cColStride = n;
     op.m = static_cast<int>(n - task.i0 < TILE ? n - task.i0 : TILE);
     op.n = min(TILE, f.c - task.j0);
-    op.k = BLOCK;
+    op.k = task.k0;
     op.lower = task.i0 == task.j0;
     op.lowerOffset = 0;
     tileProduct(op, smem);

@@ -140,7 +140,7 @@ void annotate(Plan& plan, const std::vector<std::int64_t>& cscTermsOfFront)
                 const std::int64_t m = std::min<std::int64_t>(device::TILE, n - t.i0);
                 const std::int64_t w = std::min<std::int64_t>(device::TILE, f.c - t.j0);
                 const double elements = lowerElements(t.i0, t.j0, m, w, t.i0 == t.j0);
-                flops += 2.0 * BLOCK * elements;
+                flops += 2.0 * static_cast<double>(t.k0) * elements;
                 bytes += 2.0 * V * elements;
                 break;
             }
@@ -373,11 +373,16 @@ Plan buildPlan(const Symbolic& symbolic)
             plan.factorLaunches.push_back({LaunchKind::AssembleFronts, static_cast<std::int64_t>(plan.pieces.size()),
                                            static_cast<std::int32_t>(pieces.size()), 0, 0});
             plan.pieces.insert(plan.pieces.end(), pieces.begin(), pieces.end());
+            // Two-level blocking: the 64-column steps update the trailing columns of their PANEL_MACRO-column macro
+            // panel only (K = 64); after a macro panel's last step, its columns update every later column of the panel
+            // at once (K = PANEL_MACRO), a quarter of the passes over the trailing panel.
             for (std::int32_t k0 = 0; k0 < maxColumns; k0 += BLOCK)
             {
                 std::vector<std::int32_t> diagonal;
                 std::vector<TileTask> rowTasks;
                 std::vector<TileTask> updateTiles;
+                std::vector<TileTask> macroTiles;
+                const std::int32_t macroStart = k0 / device::PANEL_MACRO * device::PANEL_MACRO;
                 for (const std::int32_t s : large)
                 {
                     const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
@@ -385,17 +390,23 @@ Plan buildPlan(const Symbolic& symbolic)
                         continue;
                     const std::int32_t n = f.c + f.r;
                     const std::int32_t kb = std::min(BLOCK, f.c - k0);
+                    const std::int32_t macroEnd = std::min(macroStart + device::PANEL_MACRO, f.c);
                     diagonal.push_back(s);
                     for (std::int32_t i0 = k0 + kb; i0 < n; i0 += PANEL_ROWS)
                         rowTasks.push_back({s, i0, 0, 0});
                     const std::int32_t origin = k0 + BLOCK;
-                    for (std::int32_t j0 = origin; j0 < f.c; j0 += device::TILE)
+                    for (std::int32_t j0 = origin; j0 < macroEnd; j0 += device::TILE)
                         for (std::int32_t i0 = j0; i0 < n; i0 += device::TILE)
-                            updateTiles.push_back({s, i0, j0, 0});
+                            updateTiles.push_back({s, i0, j0, BLOCK});
+                    if (origin >= macroEnd)
+                        for (std::int32_t j0 = macroEnd; j0 < f.c; j0 += device::TILE)
+                            for (std::int32_t i0 = j0; i0 < n; i0 += device::TILE)
+                                macroTiles.push_back({s, i0, j0, macroEnd - macroStart});
                 }
                 addList(plan, plan.factorLaunches, LaunchKind::DiagonalBlocks, diagonal, k0);
                 addTiles(plan, plan.factorLaunches, LaunchKind::PanelRows, rowTasks, k0);
                 addTiles(plan, plan.factorLaunches, LaunchKind::PanelUpdate, updateTiles, k0);
+                addTiles(plan, plan.factorLaunches, LaunchKind::PanelUpdate, macroTiles, macroStart);
             }
             std::vector<TileTask> schur;
             for (const std::int32_t s : large)
