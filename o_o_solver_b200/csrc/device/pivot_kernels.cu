@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(TILE_THREADS) panelRowsPivotedInverse(FactorAr
             break;
         const int m = static_cast<int>(n - i0 < TILE ? n - i0 : TILE);
         double* rows = args.panels + f.panel + i0 + static_cast<std::int64_t>(k0) * n;
-        double* w = pivots.w + pivots.wOffset[s] + i0;
+        double* w = pivots.w + pivots.wOffset[s] + i0 + static_cast<std::int64_t>(k0 % PANEL_MACRO) * n;
         for (int e = tid; e < B * TILE; e += blockDim.x)
         {
             const int p = e / TILE;
@@ -704,7 +704,7 @@ __global__ void __launch_bounds__(128) panelRowsPivoted(FactorArgs args, PivotAr
             v -= y[q] * l11[j * B + q];
         y[j] = v;
     }
-    double* w = pivots.w + pivots.wOffset[s] + row;
+    double* w = pivots.w + pivots.wOffset[s] + row + static_cast<std::int64_t>(k0 % PANEL_MACRO) * n;
     bool bad = false;
     int j = 0;
     while (j < kb)
@@ -736,9 +736,9 @@ __global__ void __launch_bounds__(128) panelRowsPivoted(FactorArgs args, PivotAr
         atomicOr(pivots.status + s, 1);
 }
 
-// The trailing front of step k0 (columns [k0 + 64, n), the panel's and the update matrix's) minus L W^T over the
-// block's columns: task (front, i0, j0) a 64 x 64 tile of the front, j0 < c in the panel, j0 >= c in the update
-// matrix (tiles never straddle c).
+// A tile of the trailing front minus L W^T over the K = task.k0 columns from k0 (a step's columns within its macro
+// panel, or a finished macro panel's): task (front, i0, j0) a 64 x 64 tile of the front, j0 < c in the panel, j0 >= c
+// in the update matrix (tiles never straddle c); W's columns for k0 at slice k0 % PANEL_MACRO of the front's buffer.
 __global__ void __launch_bounds__(TILE_THREADS) updatePivoted(FactorArgs args, PivotArgs pivots, const TileTask* tasks,
                                                               int k0)
 {
@@ -751,7 +751,7 @@ __global__ void __launch_bounds__(TILE_THREADS) updatePivoted(FactorArgs args, P
     op.a = panel + task.i0 + static_cast<std::int64_t>(k0) * n;
     op.aRowStride = 1;
     op.aColStride = n;
-    op.b = pivots.w + pivots.wOffset[task.front] + task.j0;
+    op.b = pivots.w + pivots.wOffset[task.front] + task.j0 + static_cast<std::int64_t>(k0 % PANEL_MACRO) * n;
     op.bRowStride = 1;
     op.bColStride = n;
     op.bIndex = nullptr;
@@ -771,7 +771,7 @@ __global__ void __launch_bounds__(TILE_THREADS) updatePivoted(FactorArgs args, P
     }
     op.cRowStride = 1;
     op.m = static_cast<int>(n - task.i0 < TILE ? n - task.i0 : TILE);
-    op.k = min(64, f.c - k0);
+    op.k = task.k0;
     op.lower = task.i0 == task.j0;
     op.lowerOffset = 0;
     tileProduct(op, smem);

@@ -461,16 +461,22 @@ Plan buildPlan(const Symbolic& symbolic)
             {
                 const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
                 plan.wOffset[static_cast<std::size_t>(s)] = w;
-                w += static_cast<std::int64_t>(f.c + f.r) * BLOCK;
+                w += static_cast<std::int64_t>(f.c + f.r) * std::min(f.c, device::PANEL_MACRO);
                 maxColumns = std::max(maxColumns, f.c);
             }
             plan.wValues = std::max(plan.wValues, w);
+            // Two-level blocking as in positive definite mode: a step updates the later columns of its macro panel
+            // (K = the step's columns, its slice of W); a finished macro panel updates the rest of the front, the panel's
+            // columns and the update matrix's (K = the macro panel's columns, all its W slices). The interchanges of a
+            // step stay inside its diagonal block, so they never touch the rows a finished macro panel's update reads.
             for (std::int32_t k0 = 0; k0 < maxColumns; k0 += BLOCK)
             {
                 std::vector<std::int32_t> diagonal;
                 std::vector<TileTask> earlier;
                 std::vector<TileTask> rowTasks;
                 std::vector<TileTask> trailing;
+                std::vector<TileTask> macroTrailing;
+                const std::int32_t macroStart = k0 / device::PANEL_MACRO * device::PANEL_MACRO;
                 for (const std::int32_t s : large)
                 {
                     const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
@@ -478,18 +484,24 @@ Plan buildPlan(const Symbolic& symbolic)
                         continue;
                     const std::int32_t n = f.c + f.r;
                     const std::int32_t kb = std::min(BLOCK, f.c - k0);
+                    const std::int32_t macroEnd = std::min(macroStart + device::PANEL_MACRO, f.c);
                     diagonal.push_back(s);
                     for (std::int32_t q = 0; q < k0; q += BLOCK)
                         earlier.push_back({s, q, 0, 0});
                     for (std::int32_t i0 = k0 + kb; i0 < n; i0 += PANEL_ROWS)
                         rowTasks.push_back({s, i0, 0, 0});
-                    // The trailing front: the panel's columns after the block, then the update matrix's, in tiles of
-                    // 64 that never straddle column c.
-                    for (std::int32_t j0 = k0 + kb; j0 < n;)
+                    for (std::int32_t j0 = k0 + kb; j0 < macroEnd; j0 += device::TILE)
+                        for (std::int32_t i0 = j0; i0 < n; i0 += device::TILE)
+                            trailing.push_back({s, i0, j0, kb});
+                    if (k0 + kb < macroEnd)
+                        continue;
+                    // The rest of the front after the macro panel: the panel's columns, then the update matrix's, in
+                    // tiles of 64 that never straddle column c.
+                    for (std::int32_t j0 = macroEnd; j0 < n;)
                     {
                         const std::int32_t width = j0 < f.c ? std::min(device::TILE, f.c - j0) : device::TILE;
                         for (std::int32_t i0 = j0; i0 < n; i0 += device::TILE)
-                            trailing.push_back({s, i0, j0, 0});
+                            macroTrailing.push_back({s, i0, j0, macroEnd - macroStart});
                         j0 += width;
                     }
                 }
@@ -497,6 +509,7 @@ Plan buildPlan(const Symbolic& symbolic)
                 addTiles(plan, plan.pivotedLaunches, LaunchKind::PermuteEarlierRows, earlier, k0);
                 addTiles(plan, plan.pivotedLaunches, LaunchKind::PanelRowsPivoted, rowTasks, k0);
                 addTiles(plan, plan.pivotedLaunches, LaunchKind::UpdatePivoted, trailing, k0);
+                addTiles(plan, plan.pivotedLaunches, LaunchKind::UpdatePivoted, macroTrailing, macroStart);
             }
         }
         plan.pivotedLaunches.push_back({LaunchKind::LevelEnd, 0, 0, level, 0});

@@ -110,8 +110,8 @@ struct Plan
     std::vector<std::int32_t> mixedOfFactorLaunch;
 
     // Indefinite mode: the launches (assembly shared with the positive definite sequence), the large fronts of each
-    // level, and each large front's W buffer (n x 64 values at wOffset; the fronts of one level apart, the levels
-    // sharing the buffer).
+    // level, and each large front's W buffer (n x min(c, PANEL_MACRO) values at wOffset: the W = L D columns of its
+    // current macro panel; the fronts of one level apart, the levels sharing the buffer).
     std::vector<Launch> pivotedLaunches;
     std::vector<std::vector<std::int32_t>> largeFrontsOfLevel;
     std::vector<std::vector<std::int32_t>> frontsOfLevel;
