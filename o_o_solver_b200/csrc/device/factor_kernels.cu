@@ -159,8 +159,11 @@ __global__ void assembleFronts(FactorArgs args, const AssemblyTask* tasks, std::
 
 // ------------------------------------------------------------------------------------------------------------------
 // Small fronts: one block per front of order n <= maxOrder, the whole front in shared memory (column-major,
-// leading dimension ld = n + 1): assembled, its c columns eliminated right-looking (each element receives its terms
-// k = 0, 1, ... in order, as the reference's unblocked algorithm), then the panel and the update matrix written out.
+// leading dimension ld = n + 1, then R(s) for the searches of the assembly): assembled, then
+//   - the c columns eliminated right-looking within the panel (columns < c): l_ik = a_ik / d_k, a_ij -= l_ik (l_jk d_k);
+//   - the update matrix, U_ij = a_ij - sum_k l_ik (l_jk d_k) for k = 0, 1, ..., c - 1, each element by one thread
+//     straight into global memory (no barrier between the terms).
+// Every element receives its terms in k order with the same products as the reference's unblocked algorithm.
 // ------------------------------------------------------------------------------------------------------------------
 __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int32_t* structureError)
 {
@@ -169,16 +172,20 @@ __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int3
     const FrontDesc f = args.fronts[s];
     const int n = f.c + f.r;
     const int ld = n + 1;
+    const int c = f.c;
     const int tid = threadIdx.x;
     const int threads = blockDim.x;
     const int warp = tid >> 5;
     const int lane = tid & 31;
     const int warps = threads >> 5;
+    std::int32_t* rows = reinterpret_cast<std::int32_t*>(front + n * ld);
 
     for (int e = tid; e < n * ld; e += threads)
         front[e] = 0.0;
+    for (int e = tid; e < f.r; e += threads)
+        rows[e] = args.rows[f.rowStart + e];
     __syncthreads();
-    for (int j = warp; j < f.c; j += warps)
+    for (int j = warp; j < c; j += warps)
     {
         const std::int32_t column = f.first + j;
         const std::int64_t begin = args.colOffsets[column];
@@ -186,7 +193,26 @@ __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int3
         for (std::int64_t k = begin + lane; k < end; k += 32)
         {
             const std::int32_t row = args.colRows[k];
-            const int position = row < column ? -1 : positionInFront(f, args.rows, row);
+            int position = -1;
+            if (row >= column)
+            {
+                if (row < f.first + c)
+                    position = row - f.first;
+                else
+                {
+                    int lo = 0;
+                    int hi = f.r;
+                    while (lo < hi)
+                    {
+                        const int mid = (lo + hi) >> 1;
+                        if (rows[mid] < row)
+                            lo = mid + 1;
+                        else
+                            hi = mid;
+                    }
+                    position = lo < f.r && rows[lo] == row ? c + lo : -1;
+                }
+            }
             if (position < 0)
             {
                 atomicMin(structureError, column);
@@ -210,8 +236,8 @@ __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int3
         }
         __syncthreads();
     }
-    // Elimination of the c columns.
-    for (int k = 0; k < f.c; ++k)
+    // The panel: the c columns eliminated, each step updating the later panel columns only.
+    for (int k = 0; k < c; ++k)
     {
         const double pivot = front[k + k * ld];
         if (isBadPivot(pivot))
@@ -222,7 +248,7 @@ __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int3
         for (int i = k + 1 + tid; i < n; i += threads)
             front[i + k * ld] = front[i + k * ld] / pivot;
         __syncthreads();
-        for (int j = k + 1 + warp; j < n; j += warps)
+        for (int j = k + 1 + warp; j < c; j += warps)
         {
             const double w = front[j + k * ld] * pivot;
             for (int i = j + lane; i < n; i += 32)
@@ -231,21 +257,48 @@ __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int3
         __syncthreads();
     }
     double* panel = args.panels + f.panel;
-    for (int e = tid; e < n * f.c; e += threads)
+    for (int e = tid; e < n * c; e += threads)
     {
         const int j = e / n;
         const int i = e - j * n;
         panel[e] = i >= j ? front[i + j * ld] : 0.0;
     }
+    // The update matrix: a warp per column, a lane per row (four rows in flight), the c terms of each element in order.
     if (f.r > 0)
     {
         double* update = args.updates + f.update;
-        for (int e = tid; e < f.r * f.r; e += threads)
+        const int r = f.r;
+        for (int jj = warp; jj < r; jj += warps)
         {
-            const int j = e / f.r;
-            const int i = e - j * f.r;
-            if (i >= j)
-                update[e] = front[(f.c + i) + (f.c + j) * ld];
+            const int j = c + jj;
+            for (int i0 = jj + lane; i0 < r; i0 += 128)
+            {
+                double acc[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                {
+                    const int ii = i0 + 32 * u;
+                    acc[u] = ii < r ? front[(c + ii) + j * ld] : 0.0;
+                }
+                for (int k = 0; k < c; ++k)
+                {
+                    const double w = front[j + k * ld] * front[k + k * ld];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                    {
+                        const int ii = i0 + 32 * u;
+                        if (ii < r)
+                            acc[u] -= front[(c + ii) + k * ld] * w;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                {
+                    const int ii = i0 + 32 * u;
+                    if (ii < r)
+                        update[ii + static_cast<std::int64_t>(jj) * r] = acc[u];
+                }
+            }
         }
     }
 }

@@ -128,7 +128,8 @@ public:
         // A kernel's shared-memory limit is the process's, not this factor's: every factor sets the largest any plan
         // can need, so that no factor lowers another's.
         const auto smallLimit = static_cast<int>(static_cast<std::size_t>(SMALL_ORDER) * (SMALL_ORDER + 1) * sizeof(double));
-        check(cudaFuncSetAttribute(device::smallFronts, cudaFuncAttributeMaxDynamicSharedMemorySize, smallLimit),
+        check(cudaFuncSetAttribute(device::smallFronts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(device::smallFrontSmem(SMALL_ORDER))),
               "smallFronts shared memory");
         check(cudaFuncSetAttribute(device::smallFrontsPivoted, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    smallLimit),
@@ -1201,7 +1202,7 @@ private:
             {
             case LaunchKind::SmallFronts:
             {
-                const std::size_t smem = static_cast<std::size_t>(launch.smemOrder) * (launch.smemOrder + 1) * sizeof(double);
+                const std::size_t smem = device::smallFrontSmem(launch.smemOrder);
                 device::smallFronts<<<launch.count, SMALL_THREADS, smem, m_stream>>>(
                     args, m_lists.get() + launch.offset, m_structureError.get());
                 break;
