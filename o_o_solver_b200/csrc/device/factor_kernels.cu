@@ -158,8 +158,8 @@ __global__ void assembleFronts(FactorArgs args, const AssemblyTask* tasks, std::
 }
 
 // ------------------------------------------------------------------------------------------------------------------
-// Small fronts: one block per front of order n <= maxOrder, the whole front in shared memory (column-major,
-// leading dimension ld = n + 1, then R(s) for the searches of the assembly): assembled, then
+// Small fronts: one block per front of order n <= maxOrder, the lower triangle of the front in shared memory (packed by
+// columns, then R(s) for the searches of the assembly): assembled, then
 //   - the c columns eliminated right-looking within the panel (columns < c): l_ik = a_ik / d_k, a_ij -= l_ik (l_jk d_k);
 //   - the update matrix, U_ij = a_ij - sum_k l_ik (l_jk d_k) for k = 0, 1, ..., c - 1, each element by one thread
 //     straight into global memory (no barrier between the terms).
@@ -171,16 +171,18 @@ __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int3
     const std::int32_t s = list[blockIdx.x];
     const FrontDesc f = args.fronts[s];
     const int n = f.c + f.r;
-    const int ld = n + 1;
     const int c = f.c;
+    // element (i, j), i >= j, of the packed lower triangle
+    const auto at = [n](int i, int j) { return j * n - ((j * (j - 1)) >> 1) + (i - j); };
     const int tid = threadIdx.x;
     const int threads = blockDim.x;
     const int warp = tid >> 5;
     const int lane = tid & 31;
     const int warps = threads >> 5;
-    std::int32_t* rows = reinterpret_cast<std::int32_t*>(front + n * ld);
+    const int packed = n * (n + 1) / 2;
+    std::int32_t* rows = reinterpret_cast<std::int32_t*>(front + packed);
 
-    for (int e = tid; e < n * ld; e += threads)
+    for (int e = tid; e < packed; e += threads)
         front[e] = 0.0;
     for (int e = tid; e < f.r; e += threads)
         rows[e] = args.rows[f.rowStart + e];
@@ -218,7 +220,7 @@ __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int3
                 atomicMin(structureError, column);
                 continue;
             }
-            front[position + j * ld] += args.colValues[k];
+            front[at(position, j)] += args.colValues[k];
         }
     }
     __syncthreads();
@@ -232,27 +234,27 @@ __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int3
             const int pj = map[jc];
             const double* column = source + static_cast<std::int64_t>(jc) * ch.r;
             for (int ic = jc + lane; ic < ch.r; ic += 32)
-                front[map[ic] + pj * ld] += column[ic];
+                front[at(map[ic], pj)] += column[ic];
         }
         __syncthreads();
     }
     // The panel: the c columns eliminated, each step updating the later panel columns only.
     for (int k = 0; k < c; ++k)
     {
-        const double pivot = front[k + k * ld];
+        const double pivot = front[at(k, k)];
         if (isBadPivot(pivot))
         {
             if (tid == 0)
                 atomicMin(args.zeroPivot + s, k);
         }
         for (int i = k + 1 + tid; i < n; i += threads)
-            front[i + k * ld] = front[i + k * ld] / pivot;
+            front[at(i, k)] = front[at(i, k)] / pivot;
         __syncthreads();
         for (int j = k + 1 + warp; j < c; j += warps)
         {
-            const double w = front[j + k * ld] * pivot;
+            const double w = front[at(j, k)] * pivot;
             for (int i = j + lane; i < n; i += 32)
-                front[i + j * ld] -= front[i + k * ld] * w;
+                front[at(i, j)] -= front[at(i, k)] * w;
         }
         __syncthreads();
     }
@@ -261,7 +263,7 @@ __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int3
     {
         const int j = e / n;
         const int i = e - j * n;
-        panel[e] = i >= j ? front[i + j * ld] : 0.0;
+        panel[e] = i >= j ? front[at(i, j)] : 0.0;
     }
     // The update matrix: a warp per column, a lane per row (four rows in flight), the c terms of each element in order.
     if (f.r > 0)
@@ -278,17 +280,17 @@ __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int3
                 for (int u = 0; u < 4; ++u)
                 {
                     const int ii = i0 + 32 * u;
-                    acc[u] = ii < r ? front[(c + ii) + j * ld] : 0.0;
+                    acc[u] = ii < r ? front[at(c + ii, j)] : 0.0;
                 }
                 for (int k = 0; k < c; ++k)
                 {
-                    const double w = front[j + k * ld] * front[k + k * ld];
+                    const double w = front[at(j, k)] * front[at(k, k)];
 #pragma unroll
                     for (int u = 0; u < 4; ++u)
                     {
                         const int ii = i0 + 32 * u;
                         if (ii < r)
-                            acc[u] -= front[(c + ii) + k * ld] * w;
+                            acc[u] -= front[at(c + ii, k)] * w;
                     }
                 }
 #pragma unroll

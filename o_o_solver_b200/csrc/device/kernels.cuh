@@ -61,11 +61,11 @@ struct SolveArgs
 
 __global__ void assembleFronts(FactorArgs args, const AssemblyTask* tasks, std::int32_t* structureError);
 __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int32_t* structureError);
-// Dynamic shared memory of smallFronts for fronts of order at most `order`: the front (order x (order + 1) values) and
-// its rows R(s).
+// Dynamic shared memory of smallFronts for fronts of order at most `order`: the front's packed lower triangle
+// (order (order + 1) / 2 values) and its rows R(s).
 constexpr std::size_t smallFrontSmem(int order)
 {
-    return static_cast<std::size_t>(order) * (order + 1) * sizeof(double) +
+    return static_cast<std::size_t>(order) * (order + 1) / 2 * sizeof(double) +
            static_cast<std::size_t>(order) * sizeof(std::int32_t);
 }
 constexpr int DIAGONAL_THREADS = 256;

@@ -323,10 +323,13 @@ Plan buildPlan(const Symbolic& symbolic)
     {
         const auto& members = byLevel[static_cast<std::size_t>(level)];
         // ---- factorisation ----
+        // Small fronts in three classes of order (shared memory per block follows the class's largest front).
         std::vector<std::int32_t> small64;
+        std::vector<std::int32_t> small96;
         std::vector<std::int32_t> small128;
         std::vector<std::int32_t> large;
         std::int32_t order64 = 0;
+        std::int32_t order96 = 0;
         std::int32_t order128 = 0;
         for (const std::int32_t s : members)
         {
@@ -337,6 +340,11 @@ Plan buildPlan(const Symbolic& symbolic)
                 small64.push_back(s);
                 order64 = std::max(order64, n);
             }
+            else if (n <= SMALL_ORDER_MIDDLE)
+            {
+                small96.push_back(s);
+                order96 = std::max(order96, n);
+            }
             else if (n <= SMALL_ORDER)
             {
                 small128.push_back(s);
@@ -345,8 +353,9 @@ Plan buildPlan(const Symbolic& symbolic)
             else
                 large.push_back(s);
         }
-        plan.largestSmallOrder = std::max({plan.largestSmallOrder, order64, order128});
+        plan.largestSmallOrder = std::max({plan.largestSmallOrder, order64, order96, order128});
         addList(plan, plan.factorLaunches, LaunchKind::SmallFronts, small64, 0, order64);
+        addList(plan, plan.factorLaunches, LaunchKind::SmallFronts, small96, 0, order96);
         addList(plan, plan.factorLaunches, LaunchKind::SmallFronts, small128, 0, order128);
         if (!large.empty())
         {
@@ -446,6 +455,7 @@ Plan buildPlan(const Symbolic& symbolic)
         plan.frontsOfLevel.push_back(members);
         plan.largeFrontsOfLevel.push_back(large);
         addList(plan, plan.pivotedLaunches, LaunchKind::SmallFrontsPivoted, small64, 0, order64);
+        addList(plan, plan.pivotedLaunches, LaunchKind::SmallFrontsPivoted, small96, 0, order96);
         addList(plan, plan.pivotedLaunches, LaunchKind::SmallFrontsPivoted, small128, 0, order128);
         if (!large.empty())
         {

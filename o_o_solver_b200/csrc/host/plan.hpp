@@ -16,6 +16,7 @@ namespace oosgpu
 
 // Fronts whose order is at most SMALL_ORDER are factorised whole in shared memory, one block each.
 constexpr int SMALL_ORDER_LOW = 64;
+constexpr int SMALL_ORDER_MIDDLE = 96;
 constexpr int SMALL_ORDER = 128;
 // The columns of a large front's assembly piece: about this many elements of its lower triangle.
 constexpr std::int64_t ASSEMBLY_PIECE_VALUES = std::int64_t{1} << 16;
