@@ -240,9 +240,16 @@ def gpu_modes(name, device, steps, warmup=1, e2e=False):
             times.append(solution.seconds)
     result = {"seconds": statistics.median(times), "solution": solution, "symbolic": symbolic, "dimension": k.dimension}
     if e2e:
+        import torch
+
+        from o_o_solver_b200 import SymmetricCsc
+
         pencil.close()
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+        h_k = SymmetricCsc(pin(k.offsets), pin(k.rows), pin(k.values))
+        h_m = SymmetricCsc(h_k.offsets, h_k.rows, pin(m.values))
         t0 = time.perf_counter()
-        fresh = SparsePencil(symbolic, k, m, device=device)
+        fresh = SparsePencil(symbolic, h_k, h_m, device=device)
         full = solver.solve(fresh, request, vectors=True)
         result["e2e"] = time.perf_counter() - t0
         result["h2d"] = int(k.offsets.nbytes + k.rows.nbytes + k.values.nbytes + m.values.nbytes)
@@ -430,7 +437,7 @@ def run_gpu(args, rank, world, local_rank):
         pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
         h_offsets, h_rows, h_values = pin(csc.offsets), pin(csc.rows), pin(csc.values)
         h_csc = SymmetricCsc(h_offsets, h_rows, h_values)
-        h_b = np.asfortranarray(loads)
+        h_b = torch.from_numpy(np.ascontiguousarray(loads.T)).pin_memory().numpy().T  # pinned, column-major
         h_x = torch.empty((columns, n), dtype=torch.float64).pin_memory().numpy().T
         e2e_times = []
         for k in range(max(1, min(3, args.steps)) + 1):
