@@ -61,13 +61,18 @@ def parse():
                         help="the modes leg: the lowest 20 modes of the n^3 hexahedral block, block size 8")
     parser.add_argument("--modes-steps", type=int, default=2)
     parser.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
-    parser.add_argument("--factor-only", metavar="MODEL:PRECISION", default=None,
+    parser.add_argument("--no-batched", action="store_true", help="skip the batched form")
+    parser.add_argument("--batch-models", type=int, default=BATCH_MODELS)
+    parser.add_argument("--batch-steps", type=int, default=3)
+    parser.add_argument("--batch-reference-sample", type=int, default=16)
+    parser.add_argument("--factor-only", metavar="MODEL:PRECISION[:PIVOTING]", default=None,
                         help="factorise one model (plate<N> or hex<N> with an ordering under tests/golden/orderings; "
                              "precision fp64 or mixed) --steps times and print the factor's kernel statistics: the "
                              "small case for kernel captures")
     parser.add_argument("--launch-profile", metavar="PATH", default=None,
                         help="with --factor-only: also solve 64 load columns and write both launch lists (kind, "
                              "blocks, step column, device seconds) to PATH as JSON")
+    parser.add_argument("--profile-rhs", type=int, default=64, help="with --launch-profile: the solve's columns")
     return parser.parse_args()
 
 
@@ -342,6 +347,118 @@ def mixed_leg(factor, d_csc, d_loads, d_x, fp64_stats, tolerance, dev, torch):
     }
 
 
+BATCH_MODELS = 512
+BATCH_RHS = 8
+
+
+def panel_fixture(cache={}):  # noqa: B006 (a cache of the reference's orderings by mesh size)
+    def fixture_of(n):
+        if n not in cache:
+            cache[n] = dict(np.load(os.path.join(GOLDEN, f"panel{n}.npz")))
+        return cache[n]
+
+    return fixture_of
+
+
+def batched_leg(args, dev, torch):
+    """The batched form: BATCH_MODELS seeded stiffened panels (2,052 to 39,852 equations each, 4 to 12 blades,
+    skin U[1, 4] mm), each with BATCH_RHS load cases, joined into one block-diagonal system (o_o_solver_b200.batch)
+    and factorised and solved together, each factorisation and solve a replayed CUDA graph of launches: in FP64
+    (`value`), and in the mixed form (update matrices by 3xTF32 products on tcgen05, then FP64 GMRES-IR to a backward
+    error of 1e-10). Median device-timed seconds of the step over the steps; the backward error of every column of
+    every panel checked on the host (the last form run, mixed); the reference on a sample of the panels (its time
+    scaled by their share of the flops)."""
+    from o_o_solver_b200 import FactorOptions, SupernodalFactor, SymmetricCsc, batch, linalg
+
+    t0 = time.perf_counter()
+    cases = batch.panel_cases(args.batch_models)
+    joined, rhs, parts = batch.panel_batch(cases, panel_fixture(), columns=BATCH_RHS)
+    build_seconds = time.perf_counter() - t0
+    d_csc = SymmetricCsc(torch.from_numpy(joined.matrix.offsets).to(dev), torch.from_numpy(joined.matrix.rows).to(dev),
+                         torch.from_numpy(joined.matrix.values).to(dev))
+    d_b = torch.from_numpy(np.ascontiguousarray(rhs.T)).to(dev)
+    d_x = torch.empty_like(d_b)
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+
+    def timed(options, krylov, max_steps):
+        factor = SupernodalFactor.factorise(joined.symbolic, d_csc, options)
+        info = None
+        for _ in range(max(args.warmup, 1)):  # the first runs also capture the graphs
+            factor.refactorise(d_csc, options)
+            info = linalg.solve_refined(factor, d_b.t(), d_x.t(), tolerance=1.0e-10, max_steps=max_steps,
+                                        krylov=krylov)
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(args.batch_steps):
+            start.record(torch.cuda.current_stream())
+            factor.refactorise(d_csc, options)
+            info = linalg.solve_refined(factor, d_b.t(), d_x.t(), tolerance=1.0e-10, max_steps=max_steps,
+                                        krylov=krylov)
+            stop.record(torch.cuda.current_stream())
+            torch.cuda.synchronize()
+            times.append(start.elapsed_time(stop) / 1e3)
+        result = {"s": statistics.median(times), "factor_device_s": factor.device_seconds,
+                  "refinement_steps": info.steps, "backward_error": info.backward_error,
+                  "inertia_negative": factor.inertia.negative}
+        factor.close()
+        return result
+
+    fp64 = timed(FactorOptions(), 0, 10)
+    mixed = timed(FactorOptions(precision="mixed"), 8, 3)
+    seconds = fp64["s"]
+    x = d_x.t().cpu().numpy()
+    # every panel's normwise backward error per column, on the host
+    worst = 0.0
+    for part, xi, bi in zip(parts, joined.split(x), joined.split(rhs)):
+        _, backward_error = accuracy(part.matrix, xi, bi)
+        worst = max(worst, backward_error)
+    out = {
+        "workload": f"{len(cases)} seeded stiffened panels ({min(p.dof_count for p in parts)} to "
+                    f"{max(p.dof_count for p in parts)} equations, 4-12 blades, skin U[1,4] mm), {BATCH_RHS} load "
+                    "cases each, one block-diagonal factorisation",
+        "models": len(cases), "equations": joined.dimension, "flops": joined.symbolic.flop_count,
+        "value": seconds, "unit": "s", "models_per_s": len(cases) / seconds,
+        "form": "FP64 factorisation and solve (CUDA graphs), backward error checked at 1e-10",
+        "fp64": fp64,
+        "mixed": dict(mixed, form="3xTF32 update matrices (tcgen05) + FP64 GMRES-IR (8 Krylov vectors, at most 3 "
+                                  "corrections) to backward error 1e-10"),
+        "max_backward_error_host": worst, "host_build_s": build_seconds,
+    }
+    # the reference on a sample of the panels, scaled by the flops
+    sample = list(range(0, len(cases), max(1, len(cases) // args.batch_reference_sample)))
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        from o_o_solver_b200 import workloads
+
+        threads = os.cpu_count() or 1
+        ref_seconds = 0.0
+        sample_flops = 0.0
+        fixture_of = panel_fixture()
+        for i in sample:
+            case = cases[i]
+            fixture = fixture_of(case.n)
+            model = workloads.Model(workloads.PanelSpec(n=case.n, stringers=case.stringers, thickness=case.thickness))
+            sym = oracle.analyse(model.offsets, model.neighbours, model.weights, given_order=fixture["node_order"],
+                                 threads=threads)
+            part = parts[i]
+            bi = np.asfortranarray(joined.split(rhs)[i])
+            t1 = time.perf_counter()
+            f = oracle.factorise(sym, part.matrix.offsets, part.matrix.rows, part.matrix.values, threads=threads)
+            f.solve(bi, threads=threads)
+            ref_seconds += time.perf_counter() - t1
+            sample_flops += sym.flops
+        out["cpu_baseline"] = {"value": ref_seconds * joined.symbolic.flop_count / sample_flops, "unit": "s",
+                               "cores": threads, "kind": "reference",
+                               "sample": f"{len(sample)} of the {len(cases)} panels factorised and solved one by one "
+                                         f"({ref_seconds:.2f} s), scaled by their share of the flops"}
+    except Exception as error:  # the reference library is test infrastructure: absent, no baseline
+        out["cpu_baseline"] = {"value": None, "unit": "s", "cores": 0, "kind": "reference",
+                               "sample": f"unavailable: {error}"}
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -493,6 +610,7 @@ def run_gpu(args, rank, world, local_rank):
 
     modes = modes_leg(args, local_rank, rank, world) if args.modes_workload != "none" else None
     mixed = None if args.no_mixed else mixed_leg(factor, d_csc, d_loads, d_x, stats, args.tolerance, dev, torch)
+    batched = None if args.no_batched else batched_leg(args, dev, torch)
 
     if rank == 0:
         line = {
@@ -506,7 +624,7 @@ def run_gpu(args, rank, world, local_rank):
                        "parallelism": f"replicas x{world}"},
             "residual": resid, "backward_error": backward, "refinement": refinement, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "kernels": kernel_table, "clocks": clocks.summary(), "cpu_baseline": baseline,
-            "factor_tflops": symbolic.flop_count / seconds / 1e12, "modes": modes, "forms": {"mixed": mixed},
+            "factor_tflops": symbolic.flop_count / seconds / 1e12, "modes": modes, "forms": {"mixed": mixed, "batched": batched},
         }
         print(json.dumps(line), flush=True)
     replicas.close()
@@ -518,7 +636,8 @@ def factor_only(args):
 
     from o_o_solver_b200 import FactorOptions, SupernodalFactor, SymbolicFactor, workloads
 
-    name, _, precision = args.factor_only.partition(":")
+    name, _, rest = args.factor_only.partition(":")
+    precision, _, pivoting = rest.partition(":")
     kind = "plate" if name.startswith("plate") else "hex"
     size = int(name[len(kind):])
     fixture = np.load(os.path.join(GOLDEN, f"{name}.npz"))
@@ -526,7 +645,7 @@ def factor_only(args):
     order = fixture["node_order"]
     symbolic = SymbolicFactor.from_partition(model.offsets, model.neighbours, model.weights, order,
                                              fixture["first_position"], fixture["parent"])
-    options = FactorOptions(precision=precision or "fp64")
+    options = FactorOptions(precision=precision or "fp64", pivoting=pivoting or "positive_definite")
     stiffness = model.csc(order, 0)
     torch.cuda.init()
     factor = SupernodalFactor.factorise(symbolic, stiffness, options)
@@ -540,7 +659,7 @@ def factor_only(args):
     if args.launch_profile:
         from o_o_solver_b200 import linalg
 
-        loads = torch.from_numpy(np.ascontiguousarray(model.loads(order, 64).T)).to("cuda")
+        loads = torch.from_numpy(np.ascontiguousarray(model.loads(order, args.profile_rhs).T)).to("cuda")
         x = torch.empty_like(loads)
         linalg.solve_refined(factor, loads.t(), x.t(), tolerance=1.0, max_steps=0)
         torch.cuda.synchronize()

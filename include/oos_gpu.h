@@ -304,6 +304,17 @@ int oosgpu_model_plate(int32_t nx, int32_t ny, double lx, double ly, double thic
                        double pressure, oosgpu_model** out);
 /* A cube of n^3 trilinear hexahedra, clamped on z = 0, lumped mass, 3 DOFs per node. */
 int oosgpu_model_hex(int32_t n, double edge, double young, double poisson, double density, oosgpu_model** out);
+/* A square skin of n x n flat shells on lx x ly (thickness t), clamped along x = 0, stiffened by `stringers` blades along x
+ * (height x thickness section, frame elements on the skin's grid lines y = k ly / (stringers + 1)); 6 DOFs per node. */
+int oosgpu_model_stiffened_panel(int32_t n, double lx, double ly, double thickness, double young, double poisson,
+                                 int32_t stringers, double blade_height, double blade_thickness, double pressure,
+                                 oosgpu_model** out);
+/* A rectangular wing box of flat shells of size h (span along y, chord along x, height along z, ribs every rib_pitch),
+ * clamped at the root y = 0, lumped mass; thicknesses: 24 zones (upper skin 8 spanwise, lower skin 8, front spar 4,
+ * rear spar 4); 6 DOFs per node. */
+int oosgpu_model_wing_box(double span, double chord, double height, double rib_pitch, double h,
+                          const double* thicknesses, double rib_thickness, double young, double poisson, double density,
+                          oosgpu_model** out);
 void oosgpu_model_destroy(oosgpu_model* model);
 /* sizes[0..3]: free nodes, DOFs per node, adjacency entries, 0 */
 int oosgpu_model_sizes(const oosgpu_model* model, int64_t sizes[4]);

@@ -116,6 +116,12 @@ SIGNATURES = [
                                           ctypes.POINTER(_vp)]),
     ("oosgpu_model_hex", ctypes.c_int, [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, ctypes.POINTER(_vp)]),
+    ("oosgpu_model_stiffened_panel", ctypes.c_int, [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                    ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_double,
+                                                    ctypes.c_double, ctypes.c_double, ctypes.POINTER(_vp)]),
+    ("oosgpu_model_wing_box", ctypes.c_int, [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, _f64p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, ctypes.POINTER(_vp)]),
     ("oosgpu_model_destroy", None, [_vp]),
     ("oosgpu_model_sizes", ctypes.c_int, [_vp, _i64p]),
     ("oosgpu_model_graph", ctypes.c_int, [_vp, _i64p, _i32p, _f64p]),

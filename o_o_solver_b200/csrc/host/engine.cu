@@ -89,6 +89,76 @@ unsigned blocksFor(std::int64_t items, int threads)
     return static_cast<unsigned>((items + threads - 1) / threads);
 }
 
+// A fixed sequence of launches on one stream replayed as a CUDA graph: captured the first time it runs with a given
+// key (the device buffers and settings the launches are given) and replayed whenever that key comes back; the last
+// GRAPHS keys are kept (a refinement or a GMRES correction alternates between a few buffers). The launches then reach
+// the GPU as one submission, without the host's cost and the gaps per launch.
+class LaunchGraph
+{
+public:
+    static constexpr std::size_t GRAPHS = 16;
+
+    LaunchGraph() = default;
+    LaunchGraph(const LaunchGraph&) = delete;
+    LaunchGraph& operator=(const LaunchGraph&) = delete;
+    ~LaunchGraph() { reset(); }
+
+    template <typename Launches> void run(cudaStream_t stream, const std::vector<std::uintptr_t>& key, Launches launches)
+    {
+        auto found = std::find_if(m_graphs.begin(), m_graphs.end(), [&](const Entry& e) { return e.key == key; });
+        if (found == m_graphs.end())
+        {
+            if (m_graphs.size() == GRAPHS)
+            {
+                cudaGraphExecDestroy(m_graphs.front().exec);
+                m_graphs.erase(m_graphs.begin());
+            }
+            check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+            try
+            {
+                launches();
+            }
+            catch (...)
+            {
+                cudaGraph_t discarded = nullptr;
+                cudaStreamEndCapture(stream, &discarded);
+                if (discarded != nullptr)
+                    cudaGraphDestroy(discarded);
+                throw;
+            }
+            cudaGraph_t graph = nullptr;
+            check(cudaStreamEndCapture(stream, &graph), "graph capture");
+            cudaGraphExec_t exec = nullptr;
+            const cudaError_t status = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            check(status, "graph instantiation");
+            m_graphs.push_back({key, exec});
+            found = m_graphs.end() - 1;
+        }
+        check(cudaGraphLaunch(found->exec, stream), "graph launch");
+    }
+
+    void reset()
+    {
+        for (const Entry& e : m_graphs)
+            cudaGraphExecDestroy(e.exec);
+        m_graphs.clear();
+    }
+
+private:
+    struct Entry
+    {
+        std::vector<std::uintptr_t> key;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Entry> m_graphs;
+};
+
+std::uintptr_t keyOf(const void* p)
+{
+    return reinterpret_cast<std::uintptr_t>(p);
+}
+
 } // namespace
 
 class GpuFactor
@@ -268,14 +338,30 @@ public:
                                                      std::to_string(options->precision));
         if (m_mixed)
             check(cudaMemsetAsync(m_mixedError.get(), 0, sizeof(int), m_stream), "memset");
-        runFactorLaunches(args);
-        invertDiagonalBlocks(args);
         const unsigned summaryBlocks = blocksFor(std::max(dimension, 1), 256);
-        device::pivotSummary<<<summaryBlocks, 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), dimension,
-                                                                   referenceDiagonal, maxRatio, m_counters.get(),
-                                                                   m_issues.get(), ISSUE_CAPACITY, m_blockRatio.get(),
-                                                                   m_blockEquation.get());
-        check(cudaGetLastError(), "pivot summary launch");
+        const auto launches = [&]
+        {
+            runFactorLaunches(args);
+            invertDiagonalBlocks(args);
+            device::pivotSummary<<<summaryBlocks, 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), dimension,
+                                                                       referenceDiagonal, maxRatio, m_counters.get(),
+                                                                       m_issues.get(), ISSUE_CAPACITY,
+                                                                       m_blockRatio.get(), m_blockEquation.get());
+            check(cudaGetLastError(), "pivot summary launch");
+        };
+        // Profiled factorisations launch one by one (events between the launches); the others replay a graph.
+        if (m_profile)
+            launches();
+        else
+        {
+            std::uint64_t ratioBits = 0;
+            std::memcpy(&ratioBits, &maxRatio, sizeof ratioBits);
+            m_factorGraph.run(m_stream,
+                              {keyOf(dOffsets), keyOf(dRows), keyOf(dValues), keyOf(referenceDiagonal),
+                               static_cast<std::uintptr_t>(ratioBits), static_cast<std::uintptr_t>(m_mixed),
+                               static_cast<std::uintptr_t>(dimension)},
+                              launches);
+        }
         check(cudaEventRecord(m_stop, m_stream), "event");
 
         // The summary back on the host.
@@ -305,6 +391,7 @@ public:
                   "download tensor-core status");
         check(cudaStreamSynchronize(m_stream), "factorisation");
         m_profileValid = m_profile;
+        m_profiledPivoted = false;
         if (mixedError != 0)
         {
             m_factorised = false;
@@ -415,10 +502,13 @@ public:
         check(cudaMemsetAsync(m_stepSwapped.get(), 0, count * sizeof(std::int32_t), m_stream), "memset");
         std::vector<std::int32_t> status(count);
         m_forcedPivots = 0;
+        std::size_t profiled = 0;
         for (const Launch& launch : m_plan.pivotedLaunches)
         {
             const std::int32_t* list = m_lists.get() + launch.offset;
             const device::TileTask* tiles = m_tiles.get() + launch.offset;
+            if (m_profile)
+                check(cudaEventRecord(profileEvent(2 * profiled), m_stream), "profile event");
             switch (launch.kind)
             {
             case LaunchKind::SmallFrontsPivoted:
@@ -468,6 +558,9 @@ public:
             default:
                 throw Error(STATUS_INTERNAL, "indefinite plan: an unexpected launch");
             }
+            if (m_profile)
+                check(cudaEventRecord(profileEvent(2 * profiled + 1), m_stream), "profile event");
+            ++profiled;
         }
         check(cudaGetLastError(), "indefinite factorisation launch");
         invertDiagonalBlocks(args);
@@ -489,6 +582,8 @@ public:
                               m_stream),
               "download structure check");
         check(cudaStreamSynchronize(m_stream), "indefinite factorisation");
+        m_profileValid = m_profile;
+        m_profiledPivoted = m_profile;
         float milliseconds = 0.0f;
         check(cudaEventElapsedTime(&milliseconds, m_start, m_stop), "event time");
         if (structureError != NO_PIVOT)
@@ -637,7 +732,9 @@ public:
     // The three sweeps on a tile of `width` columns stored by rows (n x width) in x (in pivot order after an indefinite
     // factorisation: the maps of rows in pivot order, 2x2 blocks in the diagonal sweep); the update rows of the forward
     // sweep in `updateRows` (the factor's own when null).
-    void sweeps(double* x, int width, double* updateRows = nullptr)
+    // replay: run the sweeps as a CUDA graph (captured once per buffers and width) unless the launches are profiled;
+    // the solve without allocation runs them one by one.
+    void sweeps(double* x, int width, double* updateRows = nullptr, bool replay = true)
     {
         const std::int32_t n = m_plan.dimension;
         const std::int64_t items = static_cast<std::int64_t>(n) * width;
@@ -654,16 +751,27 @@ public:
                                m_pivoted ? m_perm.get() : nullptr,
                                n,
                                m_rowPartials.get()};
+        const auto launches = [&]
+        {
+            runSweep(args, m_plan.forwardLaunches);
+            const std::size_t record =
+                beginSolveRecord(DIAGONAL_SWEEP_KIND, static_cast<std::int32_t>(blocksFor(items, 256)), 0);
+            if (m_pivoted)
+                device::diagonalSweepPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(
+                    args, m_supernodeOfColumn.get(), m_subdiagonal.get(), n);
+            else
+                device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), n);
+            endSolveRecord(record);
+            runSweep(args, m_plan.backwardLaunches);
+        };
         m_solveRecords.clear();
-        runSweep(args, m_plan.forwardLaunches);
-        const std::size_t record = beginSolveRecord(DIAGONAL_SWEEP_KIND, static_cast<std::int32_t>(blocksFor(items, 256)), 0);
-        if (m_pivoted)
-            device::diagonalSweepPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(),
-                                                                                      m_subdiagonal.get(), n);
+        if (m_profile || !replay)
+            launches();
         else
-            device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), n);
-        endSolveRecord(record);
-        runSweep(args, m_plan.backwardLaunches);
+            m_sweepGraph.run(m_stream,
+                             {keyOf(x), keyOf(args.updates), static_cast<std::uintptr_t>(width),
+                              static_cast<std::uintptr_t>(m_pivoted)},
+                             launches);
         m_solveProfileValid = m_profile;
     }
 
@@ -700,7 +808,7 @@ public:
             const std::int64_t items = static_cast<std::int64_t>(n) * tileWidth;
             (void)items;
             rowsIn(b, ld, static_cast<int>(c0), tileWidth, work);
-            sweeps(work, tileWidth, updateRows);
+            sweeps(work, tileWidth, updateRows, false);
             rowsOut(work, static_cast<int>(c0), tileWidth, b, ld);
             check(cudaGetLastError(), "solve launch");
         }
@@ -1098,9 +1206,10 @@ public:
         }
         if (!m_profileValid)
             throw Error(STATUS_NOT_FACTORISED, "kernel statistics: no profiled factorisation");
-        for (std::size_t index = 0; index < m_plan.factorLaunches.size(); ++index)
+        const std::vector<Launch>& profiledLaunches = m_profiledPivoted ? m_plan.pivotedLaunches : m_plan.factorLaunches;
+        for (std::size_t index = 0; index < profiledLaunches.size(); ++index)
         {
-            const Launch& launch = m_plan.factorLaunches[index];
+            const Launch& launch = profiledLaunches[index];
             const int kind = static_cast<int>(launch.kind);
             if (kind >= kinds)
                 continue;
@@ -1123,13 +1232,14 @@ public:
         if (factor ? !m_profileValid : !m_solveProfileValid)
             throw Error(STATUS_NOT_FACTORISED, factor ? "launch profile: no profiled factorisation"
                                                       : "launch profile: no profiled solve");
-        const std::size_t total = factor ? m_plan.factorLaunches.size() : m_solveRecords.size();
+        const std::vector<Launch>& profiledLaunches = m_profiledPivoted ? m_plan.pivotedLaunches : m_plan.factorLaunches;
+        const std::size_t total = factor ? profiledLaunches.size() : m_solveRecords.size();
         for (std::size_t index = 0; index < total && static_cast<std::int64_t>(index) < capacity; ++index)
         {
             float ms = 0.0f;
             if (factor)
             {
-                const Launch& launch = m_plan.factorLaunches[index];
+                const Launch& launch = profiledLaunches[index];
                 kinds[index] = static_cast<std::int32_t>(launch.kind);
                 counts[index] = launch.count;
                 k0[index] = launch.k0;
@@ -1315,6 +1425,8 @@ private:
     DeviceArray<std::int32_t> m_rows;
     DeviceArray<std::int32_t> m_relpos;
     DeviceArray<std::int64_t> m_gatherStart;
+    LaunchGraph m_factorGraph;
+    LaunchGraph m_sweepGraph;
     DeviceArray<std::int32_t> m_gatherRows;
     DeviceArray<double> m_rowPartials;
     DeviceArray<std::int32_t> m_supernodeOfColumn;
@@ -1378,6 +1490,7 @@ private:
     bool m_profile = false;
     bool m_profileValid = false;
     bool m_solveProfileValid = false;
+    bool m_profiledPivoted = false; // the last profiled factorisation ran the indefinite launches
     struct SolveRecord
     {
         std::int32_t kind;
@@ -1878,6 +1991,37 @@ extern "C" int oosgpu_model_hex(int32_t n, double edge, double young, double poi
             requirePointer(out, "out");
             auto handle = std::make_unique<oosgpu_model>();
             handle->model = oosgpu::Model::hexBlock(n, edge, young, poisson, density);
+            *out = handle.release();
+        });
+}
+
+extern "C" int oosgpu_model_stiffened_panel(int32_t n, double lx, double ly, double thickness, double young,
+                                            double poisson, int32_t stringers, double blade_height,
+                                            double blade_thickness, double pressure, oosgpu_model** out)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(out, "out");
+            auto handle = std::make_unique<oosgpu_model>();
+            handle->model = oosgpu::Model::stiffenedPanel(n, lx, ly, thickness, young, poisson, stringers, blade_height,
+                                                          blade_thickness, pressure);
+            *out = handle.release();
+        });
+}
+
+extern "C" int oosgpu_model_wing_box(double span, double chord, double height, double rib_pitch, double h,
+                                     const double* thicknesses, double rib_thickness, double young, double poisson,
+                                     double density, oosgpu_model** out)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(out, "out");
+            requirePointer(thicknesses, "thicknesses");
+            auto handle = std::make_unique<oosgpu_model>();
+            handle->model = oosgpu::Model::wingBox(span, chord, height, rib_pitch, h, thicknesses, rib_thickness, young,
+                                                   poisson, density);
             *out = handle.release();
         });
 }

@@ -46,6 +46,19 @@ public:
                                      double young, double poisson, double pressure);
     // A cube of n^3 trilinear hexahedra of edge `edge`, clamped on its base z = 0, lumped mass.
     [[nodiscard]] static Model hexBlock(std::int32_t n, double edge, double young, double poisson, double density);
+    // A square skin of n x n shells of lx by ly, clamped along x = 0, stiffened by `stringers` blades along x (on the
+    // grid lines y = k ly / (stringers + 1), rounded to the grid), each a Euler-Bernoulli frame element per skin edge
+    // on the skin's mid-plane with a blade section of the given height and thickness.
+    [[nodiscard]] static Model stiffenedPanel(std::int32_t n, double lx, double ly, double thickness, double young,
+                                              double poisson, std::int32_t stringers, double bladeHeight,
+                                              double bladeThickness, double pressure);
+    // A rectangular wing box of flat shells of size h: skins z = 0 and z = height over chord (x) by span (y), spars
+    // x = 0 and x = chord, ribs every ribPitch along the span; clamped at the root y = 0; lumped mass (translations
+    // rho t A / 4, rotations rho t^3 A / 48 per node of each element). thicknesses: 24 zone thicknesses (upper skin
+    // 8 spanwise zones, lower skin 8, front spar 4, rear spar 4); ribs ribThickness.
+    [[nodiscard]] static Model wingBox(double span, double chord, double height, double ribPitch, double h,
+                                       const double* thicknesses, double ribThickness, double young, double poisson,
+                                       double density);
 
     [[nodiscard]] std::int32_t nodeCount() const noexcept { return m_nodeCount; }
     [[nodiscard]] int nodeDofs() const noexcept { return m_nodeDofs; }
@@ -63,6 +76,9 @@ public:
 
 private:
     void buildGraph(const std::vector<std::vector<std::int32_t>>& elements);
+    // Adds an element matrix (nodes.size() x nodeDofs square, row-major) into the node blocks (after clearBlocks).
+    void clearBlocks();
+    void addElement(const std::vector<std::int32_t>& nodes, const double* elementMatrix);
     void assemble(const std::vector<std::vector<std::int32_t>>& elements, const double* elementMatrix, int nodeDofs);
     [[nodiscard]] std::int64_t slot(std::int32_t node, std::int32_t neighbour) const;
 

@@ -344,6 +344,223 @@ Model Model::plate(std::int32_t nx, std::int32_t ny, double lx, double ly, doubl
     return model;
 }
 
+void Model::clearBlocks()
+{
+    const auto w = static_cast<std::size_t>(m_nodeDofs);
+    m_diagonalBlocks.assign(static_cast<std::size_t>(m_nodeCount) * w * w, 0.0);
+    m_offBlocks.assign(m_neighbours.size() * w * w, 0.0);
+}
+
+void Model::addElement(const std::vector<std::int32_t>& nodes, const double* elementMatrix)
+{
+    const auto w = static_cast<std::size_t>(m_nodeDofs);
+    const std::size_t elementDofs = nodes.size() * w;
+    for (std::size_t i = 0; i < nodes.size(); ++i)
+    {
+        const std::int32_t a = nodes[i];
+        if (a < 0)
+            continue;
+        for (std::size_t j = 0; j < nodes.size(); ++j)
+        {
+            const std::int32_t b = nodes[j];
+            if (b < 0)
+                continue;
+            double* block = b == a ? m_diagonalBlocks.data() + static_cast<std::size_t>(a) * w * w
+                                   : m_offBlocks.data() + static_cast<std::size_t>(slot(a, b)) * w * w;
+            for (std::size_t cc = 0; cc < w; ++cc)
+                for (std::size_t rr = 0; rr < w; ++rr)
+                    block[rr + cc * w] += elementMatrix[(i * w + rr) * elementDofs + j * w + cc];
+        }
+    }
+}
+
+Model Model::stiffenedPanel(std::int32_t n, double lx, double ly, double thickness, double young, double poisson,
+                            std::int32_t stringers, double bladeHeight, double bladeThickness, double pressure)
+{
+    if (stringers < 0 || stringers >= n || !(bladeHeight > 0) || !(bladeThickness > 0))
+        throw std::invalid_argument("stiffened panel: expected 0 <= stringers < n and a positive blade section");
+    Model model = plate(n, n, lx, ly, thickness, young, poisson, pressure);
+    // The blades: frame elements between consecutive grid points of their grid line (already neighbours in the skin's
+    // graph); grid point (ix, iy) is free node iy * n + ix - 1 for ix >= 1 (plate's order), clamped for ix = 0.
+    const double a = lx / n;
+    const double area = bladeHeight * bladeThickness;
+    const double outOfPlane = bladeThickness * bladeHeight * bladeHeight * bladeHeight / 12.0; // bending in xz (w, ry)
+    const double inPlane = bladeHeight * bladeThickness * bladeThickness * bladeThickness / 12.0; // bending in xy
+    const double torsion = bladeHeight * bladeThickness * bladeThickness * bladeThickness / 3.0;
+    const double shearModulus = young / (2.0 * (1.0 + poisson));
+    double ke[12 * 12] = {};
+    const auto add = [&](int r, int c, double v) { ke[r * 12 + c] += v; };
+    const double L = a;
+    // axial (u) and torsion (rx)
+    for (const auto& [dof, k] : {std::pair<int, double>{0, young * area / L}, {3, shearModulus * torsion / L}})
+    {
+        add(dof, dof, k);
+        add(dof + 6, dof + 6, k);
+        add(dof, dof + 6, -k);
+        add(dof + 6, dof, -k);
+    }
+    // bending: (v, rz) with rz = v' and (w, ry) with ry = -w'
+    const auto bend = [&](int d, int r, double ei, double sign)
+    {
+        const double c = ei / (L * L * L);
+        const int idx[4] = {d, r, d + 6, r + 6};
+        const double m[4][4] = {{12, 6 * L * sign, -12, 6 * L * sign},
+                                {6 * L * sign, 4 * L * L, -6 * L * sign, 2 * L * L},
+                                {-12, -6 * L * sign, 12, -6 * L * sign},
+                                {6 * L * sign, 2 * L * L, -6 * L * sign, 4 * L * L}};
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j)
+                add(idx[i], idx[j], c * m[i][j]);
+    };
+    bend(1, 5, young * inPlane, 1.0);
+    bend(2, 4, young * outOfPlane, -1.0);
+    for (std::int32_t k = 0; k < stringers; ++k)
+    {
+        const auto iy = static_cast<std::int32_t>(std::lround(static_cast<double>(k + 1) * n / (stringers + 1)));
+        for (std::int32_t ix = 0; ix < n; ++ix)
+        {
+            const std::int32_t first = ix == 0 ? -1 : iy * n + ix - 1;
+            const std::int32_t second = iy * n + ix;
+            model.addElement({first, second}, ke);
+        }
+    }
+    return model;
+}
+
+Model Model::wingBox(double span, double chord, double height, double ribPitch, double h, const double* thicknesses,
+                     double ribThickness, double young, double poisson, double density)
+{
+    if (!(span > 0) || !(chord > 0) || !(height > 0) || !(ribPitch > 0) || !(h > 0) || thicknesses == nullptr)
+        throw std::invalid_argument("wing box: expected positive dimensions and 24 thicknesses");
+    const auto nx = static_cast<std::int32_t>(std::lround(chord / h));
+    const auto ny = static_cast<std::int32_t>(std::lround(span / h));
+    const auto nz = static_cast<std::int32_t>(std::lround(height / h));
+    const auto ribEvery = static_cast<std::int32_t>(std::lround(ribPitch / h));
+    if (nx < 1 || ny < 1 || nz < 1 || ribEvery < 1 || std::abs(nx * h - chord) > 1e-9 * chord ||
+        std::abs(ny * h - span) > 1e-9 * span || std::abs(nz * h - height) > 1e-9 * height)
+        throw std::invalid_argument("wing box: the dimensions must be whole multiples of the element size");
+    const double hz = height / nz;
+    Model model;
+    model.m_nodeDofs = 6;
+    const auto on = [&](std::int32_t ix, std::int32_t iy, std::int32_t iz)
+    { return iz == 0 || iz == nz || ix == 0 || ix == nx || iy % ribEvery == 0; };
+    std::vector<std::int32_t> freeOf(static_cast<std::size_t>(nx + 1) * (ny + 1) * (nz + 1), -1);
+    const auto index = [&](std::int32_t ix, std::int32_t iy, std::int32_t iz)
+    { return (static_cast<std::size_t>(iy) * (nz + 1) + iz) * (nx + 1) + ix; };
+    std::int32_t next = 0;
+    for (std::int32_t iy = 1; iy <= ny; ++iy) // y = 0 clamped
+        for (std::int32_t iz = 0; iz <= nz; ++iz)
+            for (std::int32_t ix = 0; ix <= nx; ++ix)
+                if (on(ix, iy, iz))
+                {
+                    freeOf[index(ix, iy, iz)] = next++;
+                    model.m_coordinates.push_back(h * ix);
+                    model.m_coordinates.push_back(h * iy);
+                    model.m_coordinates.push_back(hz * iz);
+                    model.m_gridIndex.push_back(static_cast<std::int32_t>(index(ix, iy, iz)));
+                }
+    model.m_nodeCount = next;
+    const auto at = [&](std::int32_t ix, std::int32_t iy, std::int32_t iz) { return freeOf[index(ix, iy, iz)]; };
+    // Elements by group: (nodes, group); each group one thickness and one orientation.
+    struct Group
+    {
+        int orientation; // 0: xy plane, 1: yz plane (spars), 2: xz plane (ribs)
+        double thickness;
+        double a;
+        double b;
+    };
+    std::vector<Group> groups;
+    std::vector<std::vector<std::int32_t>> elements;
+    std::vector<int> groupOf;
+    for (int z = 0; z < 24; ++z)
+        if (!(thicknesses[z] > 0))
+            throw std::invalid_argument("wing box: the zone thicknesses must be positive");
+    for (int z = 0; z < 8; ++z)
+        groups.push_back({0, thicknesses[z], h, h}); // upper skin zones 0..7
+    for (int z = 0; z < 8; ++z)
+        groups.push_back({0, thicknesses[8 + z], h, h}); // lower skin zones 8..15
+    for (int z = 0; z < 8; ++z)
+        groups.push_back({1, thicknesses[16 + z], h, hz}); // spars: front 16..19, rear 20..23
+    groups.push_back({2, ribThickness, h, hz}); // ribs: group 24
+    const auto spanZone = [&](std::int32_t ey, int zones) { return std::min(zones - 1, ey * zones / ny); };
+    for (std::int32_t ey = 0; ey < ny; ++ey)
+        for (std::int32_t ex = 0; ex < nx; ++ex)
+        {
+            // local x along global x, local y along global y
+            elements.push_back({at(ex, ey, nz), at(ex + 1, ey, nz), at(ex + 1, ey + 1, nz), at(ex, ey + 1, nz)});
+            groupOf.push_back(spanZone(ey, 8));
+            elements.push_back({at(ex, ey, 0), at(ex + 1, ey, 0), at(ex + 1, ey + 1, 0), at(ex, ey + 1, 0)});
+            groupOf.push_back(8 + spanZone(ey, 8));
+        }
+    for (std::int32_t ey = 0; ey < ny; ++ey)
+        for (std::int32_t ez = 0; ez < nz; ++ez)
+            for (const std::int32_t ix : {0, nx})
+            {
+                // local x along global y, local y along global z
+                elements.push_back({at(ix, ey, ez), at(ix, ey + 1, ez), at(ix, ey + 1, ez + 1), at(ix, ey, ez + 1)});
+                groupOf.push_back(16 + (ix == 0 ? 0 : 4) + spanZone(ey, 4));
+            }
+    for (std::int32_t iy = ribEvery; iy <= ny; iy += ribEvery)
+        for (std::int32_t ez = 0; ez < nz; ++ez)
+            for (std::int32_t ex = 0; ex < nx; ++ex)
+            {
+                // local x along global x, local y along global z
+                elements.push_back({at(ex, iy, ez), at(ex + 1, iy, ez), at(ex + 1, iy, ez + 1), at(ex, iy, ez + 1)});
+                groupOf.push_back(24);
+            }
+    model.buildGraph(elements);
+    model.clearBlocks();
+    // Rotation of each orientation: the columns are the local axes in global coordinates.
+    const double rotation[3][9] = {{1, 0, 0, 0, 1, 0, 0, 0, 1},   // xy: local (x, y, n) = (x, y, z)
+                                   {0, 0, 1, 1, 0, 0, 0, 1, 0},   // yz: local x = y, local y = z, n = x
+                                   {1, 0, 0, 0, 0, -1, 0, 1, 0}}; // xz: local x = x, local y = z, n = -y
+    std::vector<std::vector<double>> matrices;
+    for (const Group& g : groups)
+    {
+        std::vector<double> local(SHELL_DOFS * SHELL_DOFS);
+        shellStiffness(g.a, g.b, g.thickness, young, poisson, local.data());
+        // global = T local T^T with T = blockdiag(R) over the 8 triples of DOFs (R(i, j) = rotation[i * 3 + j])
+        const double* r = rotation[g.orientation];
+        std::vector<double> tmp(SHELL_DOFS * SHELL_DOFS, 0.0);
+        std::vector<double> global(SHELL_DOFS * SHELL_DOFS, 0.0);
+        for (int i = 0; i < SHELL_DOFS; ++i)
+            for (int j = 0; j < SHELL_DOFS; ++j)
+            {
+                // tmp = T local: row i of T has R(i % 3, .) on the triple of i
+                double sum = 0.0;
+                const int base = i / 3 * 3;
+                for (int q = 0; q < 3; ++q)
+                    sum += r[(i % 3) * 3 + q] * local[(base + q) * SHELL_DOFS + j];
+                tmp[i * SHELL_DOFS + j] = sum;
+            }
+        for (int i = 0; i < SHELL_DOFS; ++i)
+            for (int j = 0; j < SHELL_DOFS; ++j)
+            {
+                double sum = 0.0;
+                const int base = j / 3 * 3;
+                for (int q = 0; q < 3; ++q)
+                    sum += tmp[i * SHELL_DOFS + base + q] * r[(j % 3) * 3 + q];
+                global[i * SHELL_DOFS + j] = sum;
+            }
+        matrices.push_back(std::move(global));
+    }
+    model.m_lumpedMass.assign(static_cast<std::size_t>(model.m_nodeCount) * 6, 0.0);
+    for (std::size_t e = 0; e < elements.size(); ++e)
+    {
+        const Group& g = groups[static_cast<std::size_t>(groupOf[e])];
+        model.addElement(elements[e], matrices[static_cast<std::size_t>(groupOf[e])].data());
+        const double area = g.a * g.b;
+        const double translation = density * g.thickness * area / 4.0;
+        const double rotary = density * g.thickness * g.thickness * g.thickness * area / 48.0;
+        for (const std::int32_t node : elements[e])
+            if (node >= 0)
+                for (int c = 0; c < 6; ++c)
+                    model.m_lumpedMass[static_cast<std::size_t>(node) * 6 + c] += c < 3 ? translation : rotary;
+    }
+    model.m_pressureLoad.assign(static_cast<std::size_t>(model.m_nodeCount) * 6, 0.0);
+    return model;
+}
+
 Model Model::hexBlock(std::int32_t n, double edge, double young, double poisson, double density)
 {
     if (n < 1 || !(edge > 0) || !(young > 0) || !(poisson > -1.0 && poisson < 0.5) || !(density > 0))

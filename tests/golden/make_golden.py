@@ -13,7 +13,7 @@ Writes, for each workload of the benchmark and the tests:
   modes/<name>.npz       the reference's lowest modes of a pencil (SparsePencil + BlockLanczos::solve, block 8): the
                          eigenvalues, the shifts with their Sturm counts, the factorisations.
 
-    python tests/golden/make_golden.py [--modes-only] [--with-large-modes]
+    python tests/golden/make_golden.py [--modes-only] [--with-large-modes] [--only=name,name,...]
 """
 
 from __future__ import annotations
@@ -40,6 +40,10 @@ ORDERINGS = {
     "hex14": ("hex", 14),
     "hex30": ("hex", 30),
     "hex60": ("hex", 60),
+    # the batched stiffened panels: one skin topology per mesh size (the blades add no adjacency)
+    **{f"panel{m}": ("panel", m) for m in (18, 22, 26, 30, 34, 38, 42, 46, 50, 55, 60, 65, 70, 75, 78, 81)},
+    # the wing box of the learned start (one topology; the design variables change values only)
+    "wingbox": ("wingbox", 0),
 }
 SOLUTIONS = ["plate6", "plate20", "hex4", "hex8"]
 # name: (modes, block size); the large ones (minutes on a few cores) only with --with-large-modes.
@@ -85,7 +89,13 @@ def make_modes(names, threads):
 def model_of(kind, size):
     from o_o_solver_b200 import workloads
 
-    return workloads.Model(workloads.PlateSpec(size, size) if kind == "plate" else workloads.HexSpec(size))
+    if kind == "plate":
+        return workloads.Model(workloads.PlateSpec(size, size))
+    if kind == "panel":
+        return workloads.Model(workloads.PlateSpec(size, size, 0.5, 0.5))
+    if kind == "wingbox":
+        return workloads.Model(workloads.WingBoxSpec(thicknesses=(0.002,) * 24))
+    return workloads.Model(workloads.HexSpec(size))
 
 
 def main():
@@ -94,6 +104,8 @@ def main():
     threads = os.cpu_count() or 1
     if "--modes-only" not in sys.argv:
         make_orderings(threads)
+    if any(a.startswith("--only=") for a in sys.argv):
+        return
     make_modes(MODES, threads)
     if "--with-large-modes" in sys.argv:
         make_modes(LARGE_MODES, threads)
@@ -104,7 +116,10 @@ def make_orderings(threads):
 
     os.makedirs(os.path.join(HERE, "orderings"), exist_ok=True)
     os.makedirs(os.path.join(HERE, "solutions"), exist_ok=True)
+    only = next((a.split("=", 1)[1].split(",") for a in sys.argv if a.startswith("--only=")), None)
     for name, (kind, size) in ORDERINGS.items():
+        if only is not None and name not in only:
+            continue
         model = model_of(kind, size)
         sym = oracle.analyse(model.offsets, model.neighbours, model.weights, model.coordinates, threads=threads)
         np.savez_compressed(os.path.join(HERE, "orderings", name + ".npz"), node_order=sym.node_order,
