@@ -262,6 +262,13 @@ typedef struct oosgpu_modes oosgpu_modes;
  * counts or unbounded negative roots, OOSGPU_MEMORY_BUDGET when the basis does not fit in device memory. */
 int oosgpu_modes_solve(oosgpu_pencil* pencil, const oosgpu_eigen_request* request,
                        const oosgpu_lanczos_options* options, oosgpu_modes** out);
+/* The same with the first Lanczos run started from `start` (device memory, dimension x columns, leading dimension ld,
+ * columns = the block size) instead of a random block: a learned start block (the predicted modes of a design); the
+ * later runs, at other shifts, start from random blocks. start NULL: oosgpu_modes_solve. No counterpart in the
+ * reference (LanczosRun::startBlock, LanczosRun.cpp:217-229, draws the block). */
+int oosgpu_modes_solve_start(oosgpu_pencil* pencil, const oosgpu_eigen_request* request,
+                             const oosgpu_lanczos_options* options, const double* start, int64_t ld, int64_t columns,
+                             oosgpu_modes** out);
 /* counts: [0] eigenpairs, [1] factorisations, [2] shifts, [3] verified by the Sturm counts, [4] complete (0/1),
  * [5] Lanczos block steps; seconds: [0] wall seconds of the solve, [1] device seconds of its factorisations, then
  * wall seconds of [2] the factorisations, [3] the operator (solves and mass products), [4] the M-orthogonalisation
@@ -294,6 +301,27 @@ int oosgpu_sturm_verify(int64_t points, const double* shifts, const int64_t* cou
 int oosgpu_shift_next(double lower, double upper, int64_t mode_count, double scale, const double verification[6],
                       int64_t values, const double* sorted, int64_t ritz_count, const double* ritz,
                       int64_t shift_count, const double* lanczos_shifts, double* shift, int32_t* purpose);
+
+/* ---- the learned start block's network (no counterpart in the reference) -----------------------------------------
+ * A multilayer perceptron inputs -> hidden -> hidden -> outputs, ReLU after each hidden layer, FP32 on the GPU: He
+ * initialised from `seed`, trained by full-batch Adam on the mean squared error, every step by this library's kernels.
+ * Parameters (flat, oosgpu_mlp_parameter_count floats): W1 (inputs x hidden, row-major), b1, W2 (hidden x hidden), b2,
+ * W3 (hidden x outputs), b3. Samples are rows (batch x inputs, batch x outputs, row-major, host). */
+typedef struct oosgpu_mlp oosgpu_mlp;
+int oosgpu_mlp_create(int32_t inputs, int32_t hidden, int32_t outputs, uint64_t seed, int device, oosgpu_mlp** out);
+void oosgpu_mlp_destroy(oosgpu_mlp* mlp);
+int64_t oosgpu_mlp_parameter_count(const oosgpu_mlp* mlp);
+int oosgpu_mlp_get_parameters(oosgpu_mlp* mlp, float* parameters);
+int oosgpu_mlp_set_parameters(oosgpu_mlp* mlp, const float* parameters);
+int oosgpu_mlp_predict(oosgpu_mlp* mlp, const float* inputs, int32_t batch, float* outputs);
+/* The gradients of the mean squared error (mean over the batch and the outputs) at the current parameters, and the
+ * loss; either output may be NULL. */
+int oosgpu_mlp_gradients(oosgpu_mlp* mlp, const float* inputs, const float* targets, int32_t batch, float* gradients,
+                         float* loss);
+/* `epochs` full-batch Adam steps (beta 0.9 / 0.999, epsilon 1e-8) at `rate`; losses (epochs values, or NULL): the loss
+ * before each step. */
+int oosgpu_mlp_train(oosgpu_mlp* mlp, const float* inputs, const float* targets, int32_t batch, int32_t epochs,
+                     float rate, float* losses);
 
 /* ---- model-side helpers (no counterpart in the reference's linalg: they stand in for its assembly and DOF
  *      selection, src/assembly and SymmetricCsc::fromBlocks, src/linalg/sparse/SymmetricCsc.cpp:41) ---------------- */

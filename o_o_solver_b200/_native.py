@@ -100,6 +100,8 @@ SIGNATURES = [
     ("oosgpu_lanczos_defaults", None, [ctypes.POINTER(LanczosOptions)]),
     ("oosgpu_modes_solve", ctypes.c_int, [_vp, ctypes.POINTER(EigenRequest), ctypes.POINTER(LanczosOptions),
                                           ctypes.POINTER(_vp)]),
+    ("oosgpu_modes_solve_start", ctypes.c_int, [_vp, ctypes.POINTER(EigenRequest), ctypes.POINTER(LanczosOptions),
+                                                _vp, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(_vp)]),
     ("oosgpu_modes_summary", ctypes.c_int, [_vp, _i64p, _f64p]),
     ("oosgpu_modes_values", ctypes.c_int, [_vp, _f64p, _f64p]),
     ("oosgpu_modes_vectors", ctypes.c_int, [_vp, _f64p, ctypes.c_int64]),
@@ -116,6 +118,15 @@ SIGNATURES = [
                                           ctypes.POINTER(_vp)]),
     ("oosgpu_model_hex", ctypes.c_int, [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, ctypes.POINTER(_vp)]),
+    ("oosgpu_mlp_create", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, ctypes.c_int,
+                                         ctypes.POINTER(_vp)]),
+    ("oosgpu_mlp_destroy", None, [_vp]),
+    ("oosgpu_mlp_parameter_count", ctypes.c_int64, [_vp]),
+    ("oosgpu_mlp_get_parameters", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    ("oosgpu_mlp_set_parameters", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    ("oosgpu_mlp_predict", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int32, ctypes.POINTER(ctypes.c_float)]),
+    ("oosgpu_mlp_gradients", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), ctypes.c_int32, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+    ("oosgpu_mlp_train", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]),
     ("oosgpu_model_stiffened_panel", ctypes.c_int, [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                     ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_double,
                                                     ctypes.c_double, ctypes.c_double, ctypes.POINTER(_vp)]),

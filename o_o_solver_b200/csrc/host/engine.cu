@@ -2271,8 +2271,11 @@ extern "C" void oosgpu_lanczos_defaults(oosgpu_lanczos_options* options)
     options->seed = defaults.seed;
 }
 
-extern "C" int oosgpu_modes_solve(oosgpu_pencil* pencil, const oosgpu_eigen_request* request,
-                                  const oosgpu_lanczos_options* options, oosgpu_modes** out)
+namespace
+{
+
+int modesSolve(oosgpu_pencil* pencil, const oosgpu_eigen_request* request, const oosgpu_lanczos_options* options,
+               const double* start, int64_t ld, int64_t columns, oosgpu_modes** out)
 {
     return guarded(
         [&]
@@ -2304,12 +2307,39 @@ extern "C" int oosgpu_modes_solve(oosgpu_pencil* pencil, const oosgpu_eigen_requ
                 lanczos.maximumRestarts = count(options->maximum_restarts, "restart limit");
                 lanczos.seed = options->seed;
             }
+            if (start != nullptr)
+            {
+                const int64_t n = pencil->pencil->factor().plan().dimension;
+                if (columns != static_cast<int64_t>(lanczos.blockSize) || ld < n)
+                    throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT,
+                                        "learned start: expected a start block of " + std::to_string(n) + " rows (ld >= "
+                                        "rows) and the block size's " + std::to_string(lanczos.blockSize) +
+                                        " columns, found " + std::to_string(columns) + " columns, ld " +
+                                        std::to_string(ld));
+            }
             oosgpu::check(cudaSetDevice(pencil->pencil->factor().deviceOrdinal()), "cudaSetDevice");
             oosgpu::PencilOperations operations(*pencil->pencil);
             auto handle = std::make_unique<oosgpu_modes>();
-            handle->solution = oosgpu::eigen::solveModes(operations, eigenRequest, lanczos);
+            handle->solution = oosgpu::eigen::solveModes(operations, eigenRequest, lanczos, start, ld);
             *out = handle.release();
         });
+}
+
+} // namespace
+
+extern "C" int oosgpu_modes_solve(oosgpu_pencil* pencil, const oosgpu_eigen_request* request,
+                                  const oosgpu_lanczos_options* options, oosgpu_modes** out)
+{
+    return modesSolve(pencil, request, options, nullptr, 0, 0, out);
+}
+
+extern "C" int oosgpu_modes_solve_start(oosgpu_pencil* pencil, const oosgpu_eigen_request* request,
+                                        const oosgpu_lanczos_options* options, const double* start, int64_t ld,
+                                        int64_t columns, oosgpu_modes** out)
+{
+    if (start == nullptr)
+        return modesSolve(pencil, request, options, nullptr, 0, 0, out);
+    return modesSolve(pencil, request, options, start, ld, columns, out);
 }
 
 extern "C" int oosgpu_modes_summary(const oosgpu_modes* modes, int64_t counts[6], double seconds[6])

@@ -351,6 +351,9 @@ struct RunSettings
     double convergenceTolerance = 1.0e-10;
     std::size_t maximumRestarts = 1;
     std::uint64_t seed = 0;
+    // A start block given by the caller (device, n x blockSize, leading dimension startLd), in place of the random one.
+    const double* startBlock = nullptr;
+    std::int64_t startLd = 0;
 };
 
 struct RunResult
@@ -606,7 +609,10 @@ private:
         timed(m_phases.operatorSeconds, stream,
               [&]
               {
-                  m_ops.random(next, n, b, m_randomState);
+                  if (m_settings.startBlock != nullptr)
+                      m_ops.copy(next, n, m_settings.startBlock, m_settings.startLd, b);
+                  else
+                      m_ops.random(next, n, b, m_randomState);
                   applyOperator(next, b);
               });
         m_referenceNorms.assign(b, 0.0);
@@ -1298,7 +1304,8 @@ BasisShape shapeFor(const LanczosOptions& options, std::size_t dimension, const 
     return shape;
 }
 
-EigenSolution solveModes(ShiftedPencil& pencil, const EigenRequest& request, const LanczosOptions& options)
+EigenSolution solveModes(ShiftedPencil& pencil, const EigenRequest& request, const LanczosOptions& options,
+                         const double* startBlock, std::int64_t startLd)
 {
     validate(options);
     const auto started = std::chrono::steady_clock::now();
@@ -1394,6 +1401,11 @@ EigenSolution solveModes(ShiftedPencil& pencil, const EigenRequest& request, con
         settings.convergenceTolerance = options.convergenceTolerance;
         settings.maximumRestarts = options.maximumRestarts;
         settings.seed = options.seed + SEED_STEP * (runIndex + 1);
+        if (runIndex == 0)
+        {
+            settings.startBlock = startBlock;
+            settings.startLd = startLd;
+        }
         Run run(pencil, ops, *workspace, settings, phases);
         const RunResult result = run.run(current, store);
         solution.blockSteps += result.blockSteps;

@@ -217,6 +217,9 @@ BasisShape shapeFor(const LanczosOptions& options, std::size_t dimension, const 
 void validate(const LanczosOptions& options);
 
 // BlockLanczos::solve.
-EigenSolution solveModes(ShiftedPencil& pencil, const EigenRequest& request, const LanczosOptions& options);
+// startBlock: the first run's start block (device, dimension x blockSize, leading dimension startLd) given by the
+// caller in place of the random one (a learned start); the later runs start from random blocks.
+EigenSolution solveModes(ShiftedPencil& pencil, const EigenRequest& request, const LanczosOptions& options,
+                         const double* startBlock = nullptr, std::int64_t startLd = 0);
 
 } // namespace oosgpu::eigen

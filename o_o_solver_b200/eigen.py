@@ -94,14 +94,24 @@ class BlockLanczos:
     def __init__(self, options: LanczosOptions | None = None):
         self.options = options or LanczosOptions()
 
-    def solve(self, pencil: SparsePencil, request: EigenRequest, vectors: bool = True) -> EigenSolution:
+    def solve(self, pencil: SparsePencil, request: EigenRequest, vectors: bool = True,
+              start_block=None) -> EigenSolution:
+        """BlockLanczos::solve. start_block: a device tensor of the first run's start vectors (block size x dimension,
+        contiguous: each row a vector in the pencil's equation order) in place of the random start block."""
         lib = nat.load()
         native_request = nat.EigenRequest(float(request.lower_bound), float(request.upper_bound),
                                           int(request.mode_count))
         options = self.options.native()
         handle = nat.vp()
-        _check(lib.oosgpu_modes_solve(pencil._handle, ctypes.byref(native_request), ctypes.byref(options),
-                                      ctypes.byref(handle)))
+        if start_block is None:
+            _check(lib.oosgpu_modes_solve(pencil._handle, ctypes.byref(native_request), ctypes.byref(options),
+                                          ctypes.byref(handle)))
+        else:
+            if start_block.dim() != 2 or not start_block.is_contiguous() or start_block.shape[1] != pencil.dimension:
+                raise ValueError("BlockLanczos.solve: expected a contiguous (block size, dimension) start block")
+            _check(lib.oosgpu_modes_solve_start(pencil._handle, ctypes.byref(native_request), ctypes.byref(options),
+                                                start_block.data_ptr(), pencil.dimension, start_block.shape[0],
+                                                ctypes.byref(handle)))
         try:
             counts = np.zeros(6, dtype=np.int64)
             seconds = np.zeros(6)

@@ -44,6 +44,8 @@ ORDERINGS = {
     **{f"panel{m}": ("panel", m) for m in (18, 22, 26, 30, 34, 38, 42, 46, 50, 55, 60, 65, 70, 75, 78, 81)},
     # the wing box of the learned start (one topology; the design variables change values only)
     "wingbox": ("wingbox", 0),
+    # a small wing box for the tests of the learned start
+    "wingbox_small": ("wingbox", 1),
 }
 SOLUTIONS = ["plate6", "plate20", "hex4", "hex8"]
 # name: (modes, block size); the large ones (minutes on a few cores) only with --with-large-modes.
@@ -86,6 +88,16 @@ def make_modes(names, threads):
               f"{result['factorisations']} factorisations, lowest {result['eigenvalues'][0]:.6e}")
 
 
+def wing_box_spec(thicknesses, small=False):
+    """The wing box of the learned start (span 10 m, chord 2 m, height 0.3 m, ribs every 0.5 m, shells of 0.05 m), or
+    the small one of its tests (span 2 m, chord 0.6 m, height 0.15 m)."""
+    from o_o_solver_b200 import workloads
+
+    if small:
+        return workloads.WingBoxSpec(thicknesses=tuple(thicknesses), span=2.0, chord=0.6, height=0.15)
+    return workloads.WingBoxSpec(thicknesses=tuple(thicknesses))
+
+
 def model_of(kind, size):
     from o_o_solver_b200 import workloads
 
@@ -94,7 +106,7 @@ def model_of(kind, size):
     if kind == "panel":
         return workloads.Model(workloads.PlateSpec(size, size, 0.5, 0.5))
     if kind == "wingbox":
-        return workloads.Model(workloads.WingBoxSpec(thicknesses=(0.002,) * 24))
+        return workloads.Model(wing_box_spec((0.002,) * 24, small=size == 1))
     return workloads.Model(workloads.HexSpec(size))
 
 
