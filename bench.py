@@ -65,6 +65,10 @@ def parse():
     parser.add_argument("--batch-models", type=int, default=BATCH_MODELS)
     parser.add_argument("--batch-steps", type=int, default=3)
     parser.add_argument("--batch-reference-sample", type=int, default=16)
+    parser.add_argument("--no-learned", action="store_true", help="skip the learned start block")
+    parser.add_argument("--learned-train", type=int, default=64)
+    parser.add_argument("--learned-test", type=int, default=16)
+    parser.add_argument("--learned-epochs", type=int, default=3000)
     parser.add_argument("--factor-only", metavar="MODEL:PRECISION[:PIVOTING]", default=None,
                         help="factorise one model (plate<N> or hex<N> with an ordering under tests/golden/orderings; "
                              "precision fp64 or mixed) --steps times and print the factor's kernel statistics: the "
@@ -459,6 +463,77 @@ def batched_leg(args, dev, torch):
     return out
 
 
+LEARNED_MODES = 15
+
+
+def wing_box(design):
+    from o_o_solver_b200 import workloads
+
+    return workloads.Model(workloads.WingBoxSpec(thicknesses=tuple(design)))
+
+
+def learned_leg(args):
+    """The learned start block on the wing box (span 10 m, chord 2 m, height 0.3 m, ribs every 0.5 m, shells of
+    0.05 m: 133,800 equations), 24 zone thicknesses U[1, 4] mm: the lowest LEARNED_MODES modes of `learned_train`
+    seeded designs by the solver with random starts, a network (24 -> 256 -> 256 -> 2,080) trained on the GPU on
+    the projectors onto their modes' subspace in a 64-mode snapshot basis, then the `learned_test` unseen designs
+    solved from the random and from the learned start (the leading subspace of the predicted projector): the Lanczos
+    seconds (the solve's wall time less its factorisations'), the block steps, the whole solve, the agreement of the
+    two answers (eigenvalues, Sturm verification), and how far the predicted subspace lies from the true one (the sine
+    of the largest principal angle in the M inner product)."""
+    from o_o_solver_b200.learned import DesignSweep, LearnedStart
+
+    fixture = dict(np.load(os.path.join(GOLDEN, "wingbox.npz")))
+    sweep = DesignSweep(wing_box, fixture, modes=LEARNED_MODES, block_size=8)
+    rng = np.random.default_rng(0xB200)
+    designs = rng.uniform(0.001, 0.004, (args.learned_train + args.learned_test, 24))
+    train, test = designs[:args.learned_train], designs[args.learned_train:]
+    t0 = time.perf_counter()
+    solved = [sweep.solve(d) for d in train]
+    data_seconds = time.perf_counter() - t0
+    mass = solved[0][1]
+    t1 = time.perf_counter()
+    learned = LearnedStart.train(train, [s.eigenvectors for s, _ in solved], mass, basis_size=64, block_size=8,
+                                 hidden=256, epochs=args.learned_epochs, rate=1e-3)
+    train_seconds = time.perf_counter() - t1
+    rows = []
+    same = True
+    for d in test:
+        plain, _ = sweep.solve(d, vectors=True)
+        predicted = learned.predicted_modes(d)
+        cosines = np.linalg.svd(plain.eigenvectors.T @ (mass[:, None] * predicted), compute_uv=False)
+        angle = float(np.sqrt(max(0.0, 1.0 - cosines.min() ** 2)))
+        guided, _ = sweep.solve(d, start=learned.start_block(d), vectors=False)
+        same = same and plain.verified_count == guided.verified_count and plain.is_complete == guided.is_complete \
+            and len(plain.eigenvalues) == len(guided.eigenvalues)
+        error = float(np.max(np.abs(guided.eigenvalues - plain.eigenvalues) / np.abs(plain.eigenvalues)))
+        rows.append({"random_s": plain.seconds, "learned_s": guided.seconds,
+                     "random_lanczos_s": plain.seconds - plain.phases["factorisation"],
+                     "learned_lanczos_s": guided.seconds - guided.phases["factorisation"],
+                     "random_steps": plain.block_steps, "learned_steps": guided.block_steps,
+                     "eigenvalue_rel_difference": error, "subspace_sine": angle,
+                     "sturm": [(r.shift, r.sturm_count) for r in plain.shifts] == [(r.shift, r.sturm_count)
+                                                                               for r in guided.shifts]})
+    total = lambda key: sum(r[key] for r in rows)  # noqa: E731
+    learned.network.close()
+    return {
+        "workload": f"wing box 10 m x 2 m x 0.3 m, ribs every 0.5 m, 0.05 m shells ({mass.shape[0]} equations), "
+                    f"24 zone thicknesses U[1,4] mm, lowest {LEARNED_MODES} modes, block 8",
+        "train_designs": len(train), "test_designs": len(test), "basis": 64,
+        "network": f"24 -> 256 -> 256 -> {64 * 65 // 2} (the projector onto the modes' subspace in the basis), "
+                   f"FP32, Adam, {args.learned_epochs} epochs on the GPU",
+        "final_loss": float(learned.losses[-1]), "initial_loss": float(learned.losses[0]),
+        "data_s": data_seconds, "train_s": train_seconds,
+        "lanczos_speedup": total("random_lanczos_s") / total("learned_lanczos_s"),
+        "solve_speedup": total("random_s") / total("learned_s"),
+        "block_steps": {"random": total("random_steps"), "learned": total("learned_steps")},
+        "same_verification": bool(same), "same_sturm_points": all(r["sturm"] for r in rows),
+        "max_eigenvalue_rel_difference": max(r["eigenvalue_rel_difference"] for r in rows),
+        "median_subspace_sine": float(np.median([r["subspace_sine"] for r in rows])),
+        "per_design": rows,
+    }
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -611,6 +686,7 @@ def run_gpu(args, rank, world, local_rank):
     modes = modes_leg(args, local_rank, rank, world) if args.modes_workload != "none" else None
     mixed = None if args.no_mixed else mixed_leg(factor, d_csc, d_loads, d_x, stats, args.tolerance, dev, torch)
     batched = None if args.no_batched else batched_leg(args, dev, torch)
+    learned = None if args.no_learned else learned_leg(args)
 
     if rank == 0:
         line = {
@@ -624,7 +700,7 @@ def run_gpu(args, rank, world, local_rank):
                        "parallelism": f"replicas x{world}"},
             "residual": resid, "backward_error": backward, "refinement": refinement, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "kernels": kernel_table, "clocks": clocks.summary(), "cpu_baseline": baseline,
-            "factor_tflops": symbolic.flop_count / seconds / 1e12, "modes": modes, "forms": {"mixed": mixed, "batched": batched},
+            "factor_tflops": symbolic.flop_count / seconds / 1e12, "modes": modes, "forms": {"mixed": mixed, "batched": batched, "learned_start": learned},
         }
         print(json.dumps(line), flush=True)
     replicas.close()

@@ -614,10 +614,10 @@ public:
         check(cudaGetLastError(), "diagonal inverse launch");
     }
 
-    [[nodiscard]] Error delayedPivot(std::int32_t s, std::int32_t flags) const
+    [[nodiscard]] DelayedPivotError delayedPivot(std::int32_t s, std::int32_t flags) const
     {
         const device::FrontDesc& f = m_plan.fronts[static_cast<std::size_t>(s)];
-        return Error(STATUS_SOLVER,
+        return DelayedPivotError(
                      "indefinite factorisation: a pivot of supernode " + std::to_string(s) + " (level " +
                          std::to_string(m_plan.level[static_cast<std::size_t>(s)]) + ", " + std::to_string(f.c) +
                          " columns, " + std::to_string(f.r) + " rows below, " + std::to_string(f.childCount) +

@@ -1332,10 +1332,19 @@ EigenSolution solveModes(ShiftedPencil& pencil, const EigenRequest& request, con
         for (std::size_t attempt = 0; attempt <= MAX_SINGULAR_MOVES; ++attempt)
         {
             Inertia inertia;
-            timed(solution.factorWallSeconds, pencil.stream(), [&] { inertia = pencil.factorise(trial); });
+            bool refused = false;
+            try
+            {
+                timed(solution.factorWallSeconds, pencil.stream(), [&] { inertia = pencil.factorise(trial); });
+            }
+            catch (const DelayedPivotError&)
+            {
+                // a front of K - sigma M too near singular for a pivot within it: moved off like a singular shift
+                refused = true;
+            }
             ++solution.factorisationCount;
-            solution.factorSeconds += pencil.lastFactorSeconds();
-            if (inertia.zero == 0)
+            solution.factorSeconds += refused ? 0.0 : pencil.lastFactorSeconds();
+            if (!refused && inertia.zero == 0)
             {
                 sturm.addPoint({trial, static_cast<std::size_t>(inertia.negative)});
                 ShiftRecord record;

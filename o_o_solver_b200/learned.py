@@ -7,9 +7,11 @@ does not depend on the start (the Sturm counts decide what is found and verified
   full-batch Adam on the mean squared error; inference and training run on this library's kernels (oosgpu_mlp_*).
 - Snapshot basis: the M-orthonormal principal directions of the training designs' modes (each mode's sign fixed by a
   seeded probe vector so that a mode keeps one sign across designs), the first `basis_size` of them.
-- Targets: the coefficients of a design's wanted modes on the basis, Phi^T M psi_j (basis_size x modes).
-- Start block: Phi C W, the predicted modes mixed by a seeded Gaussian (modes x block size) matrix, so that the block
-  and one application of the operator span the predicted modes' space.
+- Targets: the projector onto a design's wanted modes in the basis's coordinates, P = C C^T with C = Phi^T M Psi
+  (basis_size x modes): the subspace of the wanted modes, indifferent to their signs and to the order of modes that
+  cross between designs (which make the coefficients of "mode j" jump); its upper triangle is the network's output.
+- Start block: Phi U W, U the leading `modes` eigenvectors of the predicted projector, mixed by a seeded Gaussian
+  (modes x block size) matrix, so that the block and one application of the operator span the predicted subspace.
 """
 
 from __future__ import annotations
@@ -138,7 +140,12 @@ class LearnedStart:
         signed = [signed_modes(m, mass, probe) for m in modes_of_designs]
         basis = SnapshotBasis.of(signed, mass, basis_size)
         modes = signed[0].shape[1]
-        targets = np.stack([basis.coefficients(m, mass).ravel() for m in signed])
+        upper = np.triu_indices(basis_size)
+        targets = []
+        for m in signed:
+            c = basis.coefficients(m, mass)
+            targets.append((c @ c.T)[upper])
+        targets = np.stack(targets)
         mean = designs.mean(axis=0)
         scale = designs.std(axis=0) + 1e-12
         network = Network(designs.shape[1], hidden, targets.shape[1], seed=seed)
@@ -150,8 +157,14 @@ class LearnedStart:
         return learned
 
     def predicted_modes(self, design: np.ndarray) -> np.ndarray:
-        c = self.network.predict(((design - self.mean) / self.scale)[None, :])[0].astype(np.float64)
-        return self.basis.phi @ c.reshape(self.basis.phi.shape[1], self.modes)
+        """An M-orthonormal basis (n x modes) of the predicted subspace of the wanted modes."""
+        size = self.basis.phi.shape[1]
+        out = self.network.predict(((design - self.mean) / self.scale)[None, :])[0].astype(np.float64)
+        projector = np.zeros((size, size))
+        projector[np.triu_indices(size)] = out
+        projector = projector + np.triu(projector, 1).T
+        values, vectors = np.linalg.eigh(projector)
+        return self.basis.phi @ vectors[:, np.argsort(values)[::-1][:self.modes]]
 
     def start_block(self, design: np.ndarray) -> np.ndarray:
         """The start block (block size x n, rows the vectors) for a design."""
