@@ -364,7 +364,7 @@ def panel_fixture(cache={}):  # noqa: B006 (a cache of the reference's orderings
     return fixture_of
 
 
-def batched_leg(args, dev, torch):
+def batched_leg(args, dev, torch, replicas=None):
     """The batched form: BATCH_MODELS seeded stiffened panels (2,052 to 39,852 equations each, 4 to 12 blades,
     skin U[1, 4] mm), each with BATCH_RHS load cases, joined into one block-diagonal system (o_o_solver_b200.batch)
     and factorised and solved together, each factorisation and solve a replayed CUDA graph of launches: in FP64
@@ -375,7 +375,11 @@ def batched_leg(args, dev, torch):
     from o_o_solver_b200 import FactorOptions, SupernodalFactor, SymmetricCsc, batch, linalg
 
     t0 = time.perf_counter()
-    cases = batch.panel_cases(args.batch_models)
+    all_cases = batch.panel_cases(args.batch_models)
+    # several GPUs: the panels dealt by their flops (longest first), each rank factorising its share
+    rank, world = (replicas.rank, replicas.world) if replicas is not None else (0, 1)
+    flops = [np.load(os.path.join(GOLDEN, f"panel{c.n}.npz"))["flops"] for c in all_cases]
+    cases = [all_cases[i] for i in batch.deal(flops, world)[rank]]
     joined, rhs, parts = batch.panel_batch(cases, panel_fixture(), columns=BATCH_RHS)
     build_seconds = time.perf_counter() - t0
     d_csc = SymmetricCsc(torch.from_numpy(joined.matrix.offsets).to(dev), torch.from_numpy(joined.matrix.rows).to(dev),
@@ -410,6 +414,9 @@ def batched_leg(args, dev, torch):
 
     fp64 = timed(FactorOptions(), 0, 10)
     mixed = timed(FactorOptions(precision="mixed"), 8, 3)
+    if replicas is not None:
+        fp64["s"] = replicas.slowest(fp64["s"])
+        mixed["s"] = replicas.slowest(mixed["s"])
     seconds = fp64["s"]
     x = d_x.t().cpu().numpy()
     # every panel's normwise backward error per column, on the host
@@ -421,16 +428,19 @@ def batched_leg(args, dev, torch):
         "workload": f"{len(cases)} seeded stiffened panels ({min(p.dof_count for p in parts)} to "
                     f"{max(p.dof_count for p in parts)} equations, 4-12 blades, skin U[1,4] mm), {BATCH_RHS} load "
                     "cases each, one block-diagonal factorisation",
-        "models": len(cases), "equations": joined.dimension, "flops": joined.symbolic.flop_count,
-        "value": seconds, "unit": "s", "models_per_s": len(cases) / seconds,
+        "models": len(all_cases), "ranks": world, "models_on_rank0": len(cases),
+        "equations_on_rank0": joined.dimension, "flops_on_rank0": joined.symbolic.flop_count,
+        "value": seconds, "unit": "s", "models_per_s": len(all_cases) / seconds,
         "form": "FP64 factorisation and solve (CUDA graphs), backward error checked at 1e-10",
         "fp64": fp64,
         "mixed": dict(mixed, form="3xTF32 update matrices (tcgen05) + FP64 GMRES-IR (8 Krylov vectors, at most 3 "
                                   "corrections) to backward error 1e-10"),
         "max_backward_error_host": worst, "host_build_s": build_seconds,
     }
-    # the reference on a sample of the panels, scaled by the flops
+    # the reference on a sample of the panels, scaled by the flops (rank 0, on its share)
     sample = list(range(0, len(cases), max(1, len(cases) // args.batch_reference_sample)))
+    if rank != 0:
+        return out
     try:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
@@ -685,7 +695,7 @@ def run_gpu(args, rank, world, local_rank):
 
     modes = modes_leg(args, local_rank, rank, world) if args.modes_workload != "none" else None
     mixed = None if args.no_mixed else mixed_leg(factor, d_csc, d_loads, d_x, stats, args.tolerance, dev, torch)
-    batched = None if args.no_batched else batched_leg(args, dev, torch)
+    batched = None if args.no_batched else batched_leg(args, dev, torch, replicas)
     learned = None if args.no_learned else learned_leg(args)
 
     if rank == 0:

@@ -152,3 +152,18 @@ def panel_batch(cases, fixture_of, columns: int = 8, seed: int = 0xB200):
         model.close()
     joined = join(parts)
     return joined, joined.stack(loads), parts
+
+
+def deal(work, ranks: int):
+    """Longest processing time first: the items (by index) dealt to `ranks` workers, each item to the worker with the
+    least work so far (ties to the lowest rank), the heaviest items first; returns each worker's item indices in
+    increasing order. The same on every rank (no exchange needed)."""
+    work = np.asarray(work, dtype=np.float64)
+    order = sorted(range(len(work)), key=lambda i: (-work[i], i))
+    loads = [0.0] * ranks
+    share = [[] for _ in range(ranks)]
+    for i in order:
+        r = min(range(ranks), key=lambda k: (loads[k], k))
+        loads[r] += work[i]
+        share[r].append(i)
+    return [sorted(s) for s in share]

@@ -61,3 +61,48 @@ def test_blades_stiffen_the_skin(lib):
     k_panel = lower(panel_csc, panel.dof_count).toarray()
     assert np.all(np.diag(k_panel) >= np.diag(k_skin) - 1e-9 * np.abs(np.diag(k_skin)))
     assert np.diag(k_panel).sum() > np.diag(k_skin).sum()
+
+
+def test_deal_covers_every_panel_once_and_balances():
+    rng = np.random.default_rng(4)
+    work = rng.uniform(1, 100, 97)
+    for ranks in (1, 2, 3, 8):
+        shares = batch.deal(work, ranks)
+        flat = sorted(i for s in shares for i in s)
+        assert flat == list(range(97))
+        loads = [work[s].sum() for s in shares]
+        assert max(loads) - min(loads) <= work.max()
+
+
+def _deal_rank(rank, world, port, out):
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    cases = batch.panel_cases(40)
+    flops = [float(np.load(os.path.join(GOLDEN, f"panel{c.n}.npz"))["flops"]) for c in cases]
+    mine = batch.deal(flops, world)[rank]
+    gathered = [None] * world
+    dist.all_gather_object(gathered, mine)
+    out.put((rank, gathered))
+    dist.destroy_process_group()
+
+
+def test_deal_agrees_across_two_gloo_ranks():
+    import multiprocessing as mp
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    procs = [ctx.Process(target=_deal_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    results = dict(out.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+    assert results[0] == results[1]
+    shares = results[0]
+    assert sorted(shares[0] + shares[1]) == list(range(40)) and not set(shares[0]) & set(shares[1])
