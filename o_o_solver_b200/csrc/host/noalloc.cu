@@ -13,8 +13,8 @@
 // call therefore does this set-up, and should come before any stream capture.
 //
 // Sharing: every call on a device uses the same array and leaves its contents behind; the solve writes every scratch
-// value before it reads it (the column tile's rows are copied in, each supernode zeroes its update rows before its
-// children add to them), so nothing carries over. Two calls whose work overlaps on the GPU (on two streams, or from two
+// value before it reads it (the column tile's rows are copied in; each supernode's update rows are written whole by
+// its own forward step before its parent gathers them), so nothing carries over. Two calls whose work overlaps on the GPU (on two streams, or from two
 // threads) race on the array: issue them one after the other.
 //
 // The limit: a factor needs (equations + update rows of its supernodes) scratch values per right-hand side; the
