@@ -352,7 +352,7 @@ def mixed_leg(factor, d_csc, d_loads, d_x, fp64_stats, tolerance, dev, torch):
 
 
 # DRAM traffic of the plate's update-matrix launches (the statics roofline's kernel), measured by ncu
-# (--metrics dram__bytes_read.sum,dram__bytes_write.sum, a single pass, -k regex:"^updateMatrix$" -c 16 over
+# (--metrics dram__bytes_read.sum,dram__bytes_write.sum only, -k regex:"^updateMatrix$" -c 16 over
 # `bench.py --factor-only plate580:fp64 --steps 1 --warmup 1`): 12.23 GB read + 6.81 GB written over 16 launches.
 UPDATE_MATRIX_TRAFFIC = (12227441920 + 6808305664) / 16
 
@@ -673,8 +673,8 @@ def run_gpu(args, rank, world, local_rank):
                     "traffic": UPDATE_MATRIX_TRAFFIC if (dominant == "update_matrix" and args.workload == "plate580")
                     else None,
                     "traffic_note": "DRAM bytes read + written per launch, averaged over the 16 update-matrix launches "
-                                    "of one plate factorisation (ncu dram__bytes_read.sum + dram__bytes_write.sum, "
-                                    "one pass); algorithmic: " + str(round(d["bytes"] / d["launches"] / 1e9, 3)) +
+                                    "of one plate factorisation (ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                    "only); algorithmic: " + str(round(d["bytes"] / d["launches"] / 1e9, 3)) +
                                     " GB per launch",
                     "kernel": dominant, "launches": d["launches"],
                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor)",

@@ -121,9 +121,11 @@ __global__ void toRows(const double* b, std::int64_t ld, int c0, int width, int 
                        const double* scale);
 __global__ void fromRows(const double* x, int c0, int width, int dimension, double* b, std::int64_t ld,
                          const double* scale);
+// Rows of one group (consecutive rows with the same columns, at most RESIDUAL_GROUP) share one warp in residualRows.
+constexpr int RESIDUAL_GROUP = 8;
 __global__ void residualRows(const std::int64_t* rowStart, const std::int32_t* columns, const std::int32_t* source,
-                             const double* values, const double* b, const double* x, double* r, int width,
-                             int dimension, double* norms);
+                             const std::int32_t* groupFirst, int groups, const double* values, const double* b,
+                             const double* x, double* r, int width, double* norms);
 __global__ void addRows(double* x, const double* r, std::int64_t count);
 
 // The GMRES refinement (gmres_kernels.cu).

@@ -292,24 +292,49 @@ __global__ void __launch_bounds__(TILE_THREADS) forwardGather(SolveArgs a, const
             }
 }
 
-// The inverse of the unit lower 64 x 64 diagonal block of step k0 of a large supernode, after each factorisation: one
-// thread per column j of L11^-1 carries it through the forward substitution of e_j in registers, reading L11 from shared
-// memory by broadcast; the strict lower part of L11^-1 is written transposed into the block's strict upper triangle
-// (unused by the factor: L11^-1(i, j) at panel position (k0 + j, k0 + i)), where the solves' diagonal steps read it.
+// The inverse of the unit lower diagonal block (kb <= 64 columns) of step k0 of a supernode, after each
+// factorisation: one thread per column j of L11^-1 carries it through the forward substitution of e_j in registers,
+// reading L11 from shared memory by broadcast; the strict lower part of L11^-1 is written transposed into the block's
+// strict upper triangle (unused by the factor: L11^-1(i, j) at panel position (k0 + j, k0 + i)), where the solves'
+// diagonal steps read it. The substitution is unrolled for the smallest of 8, 16, 32 or 64 columns that holds kb, so
+// a supernode of a few columns costs a few terms per thread.
+template <int N>
+__device__ __forceinline__ void invertUnitLower(const double* l, int ld, int j, int kb, double* block, std::int64_t n)
+{
+    double x[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        x[i] = i == j ? 1.0 : 0.0;
+#pragma unroll
+    for (int i = 1; i < N; ++i)
+    {
+        double v = x[i];
+#pragma unroll
+        for (int q = 0; q < i; ++q)
+            v -= l[q * ld + i] * x[q];
+        x[i] = v;
+    }
+#pragma unroll
+    for (int i = 1; i < N; ++i)
+        if (i > j && i < kb)
+            block[j + static_cast<std::int64_t>(i) * n] = x[i];
+}
+
 __global__ void __launch_bounds__(SOLVE_BLOCK) invertDiagonal(FactorArgs args, const TileTask* tasks)
 {
     constexpr int LD = SOLVE_BLOCK + 1;
-    __shared__ double l[SOLVE_BLOCK * LD]; // l[q * LD + i] = L(k0 + i, k0 + q), i > q
+    __shared__ double l[SOLVE_BLOCK * LD]; // l[q * LD + i] = L(k0 + i, k0 + q), i > q; zero elsewhere below kb
     const TileTask task = tasks[blockIdx.x];
     const FrontDesc f = args.fronts[task.front];
     const std::int64_t n = f.c + f.r;
     const int k0 = task.i0;
     const int kb = min(SOLVE_BLOCK, f.c - k0);
+    const int width = kb <= 8 ? 8 : kb <= 16 ? 16 : kb <= 32 ? 32 : SOLVE_BLOCK;
     double* block = args.panels + f.panel + k0 + static_cast<std::int64_t>(k0) * n;
-    for (int e = threadIdx.x; e < SOLVE_BLOCK * SOLVE_BLOCK; e += blockDim.x)
+    for (int e = threadIdx.x; e < width * width; e += blockDim.x)
     {
-        const int q = e / SOLVE_BLOCK;
-        const int i = e - q * SOLVE_BLOCK;
+        const int q = e / width;
+        const int i = e - q * width;
         const bool inside = q < kb && i < kb && i > q;
         copyAsync8(l + q * LD + i, inside ? block + i + static_cast<std::int64_t>(q) * n : block, inside);
     }
@@ -319,23 +344,14 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) invertDiagonal(FactorArgs args, c
     const int j = threadIdx.x;
     if (j >= kb)
         return;
-    double x[SOLVE_BLOCK];
-#pragma unroll
-    for (int i = 0; i < SOLVE_BLOCK; ++i)
-        x[i] = i == j ? 1.0 : 0.0;
-#pragma unroll
-    for (int i = 1; i < SOLVE_BLOCK; ++i)
-    {
-        double v = x[i];
-#pragma unroll
-        for (int q = 0; q < i; ++q)
-            v -= l[q * LD + i] * x[q];
-        x[i] = v;
-    }
-#pragma unroll
-    for (int i = 1; i < SOLVE_BLOCK; ++i)
-        if (i > j && i < kb)
-            block[j + static_cast<std::int64_t>(i) * n] = x[i];
+    if (width == 8)
+        invertUnitLower<8>(l, LD, j, kb, block, n);
+    else if (width == 16)
+        invertUnitLower<16>(l, LD, j, kb, block, n);
+    else if (width == 32)
+        invertUnitLower<32>(l, LD, j, kb, block, n);
+    else
+        invertUnitLower<SOLVE_BLOCK>(l, LD, j, kb, block, n);
 }
 
 // Stages the strict lower triangle of the inverse of the unit lower 64 x 64 diagonal block at column k0 of a large
@@ -790,7 +806,7 @@ namespace oosgpu::device
 // Iterative refinement in FP64 (the fixed-precision refinement of LAPACK xPORFS, which the reference applies to free
 // bodies, include/oos/linalg/dense/IterativeRefinement.hpp:39-64): R = B - A X on the rows of a tile, with A given by
 // the full symmetric pattern of its lower CSC (both triangles, each row's columns ascending, `source` the index of
-// each term in the CSC's values), one warp per row, each lane its columns. For the convergence test it accumulates,
+// each term in the CSC's values), one warp per group of rows with the same columns, each lane its columns. For the convergence test it accumulates,
 // per column, the squared 2-norms of R and B and the infinity norms of R, B and X, and the infinity norm of A (the
 // largest row sum of |a_ij|): the normwise backward error ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf) (Rigal and
 // Gaches) and the relative residual ||r||_2 / ||b||_2 follow. norms: [0, 64) sum r^2, [64, 128) sum b^2,
@@ -802,12 +818,17 @@ __device__ __forceinline__ void atomicMaxNonNegative(double* target, double valu
     atomicMax(reinterpret_cast<unsigned long long*>(target), static_cast<unsigned long long>(__double_as_longlong(value)));
 }
 
-// Each warp takes rows row0, row0 + (all warps), ...; each lane keeps its columns' norms (at most two columns, width
-// <= 64) in registers and adds them to the accumulators once at the end.
+// Each warp takes a group of consecutive rows with the same columns (the DOFs of one node: at most RESIDUAL_GROUP
+// rows, groupFirst[g] .. groupFirst[g + 1] - 1), groups g0, g0 + (all warps), ...; each lane holds its columns (at
+// most two, width <= 64). The group's terms are read 32 at a time, one per lane (its column and each row's value),
+// then passed round by shuffles, so every row of X is read once per group instead of once per row. Each row's sum
+// still takes its terms in increasing column order, and each row's |a_ij| sum its lane-strided partial sums, so R
+// and the norms are those of a warp per row. The norms stay in registers and reach the accumulators once at the end.
 __global__ void residualRows(const std::int64_t* rowStart, const std::int32_t* columns, const std::int32_t* source,
-                             const double* values, const double* b, const double* x, double* r, int width,
-                             int dimension, double* norms)
+                             const std::int32_t* groupFirst, int groups, const double* values, const double* b,
+                             const double* x, double* r, int width, double* norms)
 {
+    constexpr unsigned FULL = 0xffffffffu;
     const int warpsPerBlock = blockDim.x >> 5;
     const int lane = threadIdx.x & 31;
     const int totalWarps = gridDim.x * warpsPerBlock;
@@ -817,34 +838,74 @@ __global__ void residualRows(const std::int64_t* rowStart, const std::int32_t* c
     double maxB[2] = {0.0, 0.0};
     double maxX[2] = {0.0, 0.0};
     double maxRowSum = 0.0;
-    for (int row = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5); row < dimension; row += totalWarps)
+    for (int g = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5); g < groups; g += totalWarps)
     {
-        const std::int64_t begin = rowStart[row];
-        const std::int64_t end = rowStart[row + 1];
-        double rowSum = 0.0;
-        for (std::int64_t k = begin + lane; k < end; k += 32)
-            rowSum += fabs(values[source[k]]);
-        for (int offset = 16; offset > 0; offset >>= 1)
-            rowSum += __shfl_xor_sync(0xffffffffu, rowSum, offset);
-        maxRowSum = fmax(maxRowSum, rowSum);
+        const int first = groupFirst[g];
+        const int count = groupFirst[g + 1] - first;
+        const std::int64_t begin = rowStart[first];
+        const int length = static_cast<int>(rowStart[first + 1] - begin);
+        double acc[RESIDUAL_GROUP][2];
+        double rowSum[RESIDUAL_GROUP];
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
+        for (int u = 0; u < RESIDUAL_GROUP; ++u)
         {
-            const int c = lane + 32 * h;
-            if (c >= width)
-                continue;
-            double sum = 0.0;
-            for (std::int64_t k = begin; k < end; ++k)
-                sum += values[source[k]] * x[static_cast<std::int64_t>(columns[k]) * width + c];
-            const std::int64_t at = static_cast<std::int64_t>(row) * width + c;
-            const double bc = b[at];
-            const double rc = bc - sum;
-            r[at] = rc;
-            sumR[h] += rc * rc;
-            sumB[h] += bc * bc;
-            maxR[h] = fmax(maxR[h], fabs(rc));
-            maxB[h] = fmax(maxB[h], fabs(bc));
-            maxX[h] = fmax(maxX[h], fabs(x[at]));
+            acc[u][0] = 0.0;
+            acc[u][1] = 0.0;
+            rowSum[u] = 0.0;
+        }
+        for (int t0 = 0; t0 < length; t0 += 32)
+        {
+            const int t = t0 + lane;
+            const bool live = t < length;
+            const int myColumn = live ? columns[begin + t] : 0;
+            double myValue[RESIDUAL_GROUP];
+#pragma unroll
+            for (int u = 0; u < RESIDUAL_GROUP; ++u)
+            {
+                myValue[u] = u < count && live ? values[source[rowStart[first + u] + t]] : 0.0;
+                rowSum[u] += fabs(myValue[u]);
+            }
+            const int chunk = min(32, length - t0);
+            for (int q = 0; q < chunk; ++q)
+            {
+                const double* xRow = x + static_cast<std::int64_t>(__shfl_sync(FULL, myColumn, q)) * width;
+                const double x0 = lane < width ? xRow[lane] : 0.0;
+                const double x1 = lane + 32 < width ? xRow[lane + 32] : 0.0;
+#pragma unroll
+                for (int u = 0; u < RESIDUAL_GROUP; ++u)
+                    if (u < count) // the same on every lane
+                    {
+                        const double v = __shfl_sync(FULL, myValue[u], q);
+                        acc[u][0] += v * x0;
+                        acc[u][1] += v * x1;
+                    }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < RESIDUAL_GROUP; ++u)
+        {
+            if (u >= count)
+                break;
+            double sum = rowSum[u];
+            for (int offset = 16; offset > 0; offset >>= 1)
+                sum += __shfl_xor_sync(FULL, sum, offset);
+            maxRowSum = fmax(maxRowSum, sum);
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+            {
+                const int c = lane + 32 * h;
+                if (c >= width)
+                    continue;
+                const std::int64_t at = static_cast<std::int64_t>(first + u) * width + c;
+                const double bc = b[at];
+                const double rc = bc - acc[u][h];
+                r[at] = rc;
+                sumR[h] += rc * rc;
+                sumB[h] += bc * bc;
+                maxR[h] = fmax(maxR[h], fabs(rc));
+                maxB[h] = fmax(maxB[h], fabs(bc));
+                maxX[h] = fmax(maxX[h], fabs(x[at]));
+            }
         }
     }
 #pragma unroll

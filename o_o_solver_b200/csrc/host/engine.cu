@@ -867,9 +867,28 @@ public:
                 source[at] = static_cast<std::int32_t>(k);
             }
         }
+        // Groups of consecutive rows with the same columns (a node's DOFs), at most RESIDUAL_GROUP rows each.
+        std::vector<std::int32_t> groupFirst;
+        groupFirst.reserve(static_cast<std::size_t>(n) + 1);
+        for (std::int32_t i = 0; i < n;)
+        {
+            groupFirst.push_back(i);
+            const std::int64_t begin = start[static_cast<std::size_t>(i)];
+            const std::int64_t length = start[static_cast<std::size_t>(i) + 1] - begin;
+            std::int32_t next = i + 1;
+            while (next < n && next - i < device::RESIDUAL_GROUP &&
+                   start[static_cast<std::size_t>(next) + 1] - start[static_cast<std::size_t>(next)] == length &&
+                   std::equal(columns.begin() + begin, columns.begin() + begin + length,
+                              columns.begin() + start[static_cast<std::size_t>(next)]))
+                ++next;
+            i = next;
+        }
+        groupFirst.push_back(n);
+        m_residualGroups = static_cast<std::int32_t>(groupFirst.size()) - 1;
         m_fullStart.upload(start, m_stream, "refinement: pattern");
         m_fullColumns.upload(columns, m_stream, "refinement: pattern");
         m_fullSource.upload(source, m_stream, "refinement: pattern");
+        m_groupFirst.upload(groupFirst, m_stream, "refinement: pattern");
         check(cudaStreamSynchronize(m_stream), "refinement pattern");
         m_fullTerms = m_matrixTerms;
     }
@@ -1074,10 +1093,10 @@ public:
                 check(cudaMemsetAsync(m_norms.get(), 0, 384 * sizeof(double), m_stream), "memset");
                 constexpr int WARPS = 8;
                 // A grid of a few blocks per SM: each warp strides over the rows, its norms flushed once.
-                const unsigned residualBlocks = std::min<unsigned>(blocksFor(n, WARPS), 148u * 8u);
+                const unsigned residualBlocks = std::min<unsigned>(blocksFor(m_residualGroups, WARPS), 148u * 8u);
                 device::residualRows<<<residualBlocks, 32 * WARPS, 0, m_stream>>>(
-                    m_fullStart.get(), m_fullColumns.get(), m_fullSource.get(), m_matrixValues, m_bRows.get(),
-                    m_work.get(), m_rRows.get(), width, n, m_norms.get());
+                    m_fullStart.get(), m_fullColumns.get(), m_fullSource.get(), m_groupFirst.get(), m_residualGroups,
+                    m_matrixValues, m_bRows.get(), m_work.get(), m_rRows.get(), width, m_norms.get());
                 check(cudaMemcpyAsync(norms.data(), m_norms.get(), 384 * sizeof(double), cudaMemcpyDeviceToHost,
                                       m_stream),
                       "download norms");
@@ -1480,6 +1499,8 @@ private:
     DeviceArray<std::int64_t> m_fullStart;
     DeviceArray<std::int32_t> m_fullColumns;
     DeviceArray<std::int32_t> m_fullSource;
+    DeviceArray<std::int32_t> m_groupFirst;
+    std::int32_t m_residualGroups = 0;
     std::int64_t m_fullTerms = -1;
     const std::int64_t* m_matrixOffsets = nullptr;
     const std::int32_t* m_matrixRows = nullptr;

@@ -5,11 +5,14 @@ does not depend on the start (the Sturm counts decide what is found and verified
 
 - Network: a multilayer perceptron (inputs -> hidden -> hidden -> outputs, ReLU) in FP32 on the GPU, trained by
   full-batch Adam on the mean squared error; inference and training run on this library's kernels (oosgpu_mlp_*).
-- Snapshot basis: the M-orthonormal principal directions of the training designs' modes (each mode's sign fixed by a
-  seeded probe vector so that a mode keeps one sign across designs), the first `basis_size` of them.
-- Targets: the projector onto a design's wanted modes in the basis's coordinates, P = C C^T with C = Phi^T M Psi
-  (basis_size x modes): the subspace of the wanted modes, indifferent to their signs and to the order of modes that
-  cross between designs (which make the coefficients of "mode j" jump); its upper triangle is the network's output.
+- Snapshot basis: the principal directions of the training designs' modes in the inner product of their mean mass
+  (each mode's sign fixed by a seeded probe vector so that a mode keeps one sign across designs), the first
+  `basis_size` of them.
+- Targets: the orthogonal projector onto a design's wanted modes in the basis's coordinates, P = Q Q^T, Q an
+  orthonormal basis of the modes' least-squares coefficients A = (Phi^T M Phi)^-1 Phi^T M Psi in the design's own
+  mass M (the thicknesses change the mass several-fold): the subspace of the wanted modes, indifferent to their
+  signs and to the order of modes that cross between designs (which make the coefficients of "mode j" jump); its
+  upper triangle is the network's output.
 - Start block: Phi U W, U the leading `modes` eigenvectors of the predicted projector, mixed by a seeded Gaussian
   (modes x block size) matrix, so that the block and one application of the operator span the predicted subspace.
 """
@@ -100,6 +103,19 @@ def signed_modes(modes: np.ndarray, mass: np.ndarray, probe: np.ndarray) -> np.n
     return modes * signs
 
 
+def subspace_sines(modes: np.ndarray, predicted: np.ndarray, mass: np.ndarray) -> np.ndarray:
+    """The sines of the principal angles between span(modes) and span(predicted) in the M inner product, increasing:
+    the last one is how far the worst-placed direction of the modes lies from the predicted subspace."""
+
+    def orthonormal(v):
+        values, vectors = np.linalg.eigh(v.T @ (mass[:, None] * v))
+        keep = values > values.max() * 1e-12
+        return v @ (vectors[:, keep] / np.sqrt(values[keep]))
+
+    cosines = np.linalg.svd(orthonormal(modes).T @ (mass[:, None] * orthonormal(predicted)), compute_uv=False)
+    return np.sort(np.sqrt(np.clip(1.0 - cosines ** 2, 0.0, None)))
+
+
 @dataclass
 class SnapshotBasis:
     """An M-orthonormal basis (n x size) of the training designs' modes."""
@@ -119,6 +135,10 @@ class SnapshotBasis:
         """Phi^T M psi_j (size x k)."""
         return self.phi.T @ (mass[:, None] * modes)
 
+    def least_squares(self, modes: np.ndarray, mass: np.ndarray) -> np.ndarray:
+        """The coefficients A (size x k) of the M-closest combinations Phi A of the basis to the modes."""
+        return np.linalg.solve(self.phi.T @ (mass[:, None] * self.phi), self.coefficients(modes, mass))
+
 
 @dataclass
 class LearnedStart:
@@ -132,19 +152,23 @@ class LearnedStart:
     mixing: np.ndarray  # modes x block size
 
     @classmethod
-    def train(cls, designs: np.ndarray, modes_of_designs, mass: np.ndarray, basis_size: int, block_size: int,
+    def train(cls, designs: np.ndarray, modes_of_designs, masses, basis_size: int, block_size: int,
               hidden: int = 256, epochs: int = 2000, rate: float = 1.0e-3, seed: int = 0x5EED):
-        """designs: (count x variables); modes_of_designs: the solver's modes of each (n x modes, M-orthonormal)."""
+        """designs: (count x variables); modes_of_designs: the solver's modes of each (n x modes, M-orthonormal);
+        masses: each design's lumped mass diagonal (a list), or one diagonal shared by all."""
+        if isinstance(masses, np.ndarray) and masses.ndim == 1:
+            masses = [masses] * len(modes_of_designs)
         rng = np.random.default_rng(seed)
-        probe = rng.standard_normal(mass.shape[0])
-        signed = [signed_modes(m, mass, probe) for m in modes_of_designs]
-        basis = SnapshotBasis.of(signed, mass, basis_size)
+        mean_mass = np.mean(masses, axis=0)
+        probe = rng.standard_normal(mean_mass.shape[0])
+        signed = [signed_modes(m, mass, probe) for m, mass in zip(modes_of_designs, masses)]
+        basis = SnapshotBasis.of(signed, mean_mass, basis_size)
         modes = signed[0].shape[1]
         upper = np.triu_indices(basis_size)
         targets = []
-        for m in signed:
-            c = basis.coefficients(m, mass)
-            targets.append((c @ c.T)[upper])
+        for m, mass in zip(signed, masses):
+            q, _ = np.linalg.qr(basis.least_squares(m, mass))
+            targets.append((q @ q.T)[upper])
         targets = np.stack(targets)
         mean = designs.mean(axis=0)
         scale = designs.std(axis=0) + 1e-12
