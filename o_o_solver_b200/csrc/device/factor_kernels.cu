@@ -313,21 +313,24 @@ __global__ void smallFronts(FactorArgs args, const std::int32_t* list, std::int3
 //   trailing panel update and final update-matrix SYRK: tile products (tileProduct).
 // ------------------------------------------------------------------------------------------------------------------
 constexpr int BLOCK = 64;
+constexpr int INVERSE_SUB = 16; // the blocks of the diagonal block's inverse
 
 // The diagonal block's LDL^T and the inverse of its unit lower factor, in shared memory by DIAGONAL_THREADS threads
 // with loops kept rolled: a single block runs at the top of the tree, where every instruction is fetched once, so the
 // code stays small enough for the instruction cache (a fully unrolled register version stalled on instruction fetch).
 //   elimination: for k = 0, 1, ...: l_ik = a_ik / d_k, then a_ij -= l_ik (l_jk d_k) for k < j <= i, each element's
-//   terms in k order as the reference's unblocked algorithm;
-//   inverse: X = L11^-1 row by row, X(i, j) = -sum_{j <= q < i} L(i, q) X(q, j) (four interleaved partial sums), kept
-//   in the strict upper triangle (X(i, j) at (j, i)), where panelRowsInverse and the solves read it.
+//   terms in k order as the reference's unblocked algorithm, one barrier per column;
+//   inverse: X = L11^-1 by 16 x 16 blocks (the diagonal blocks by substitution, one thread per column, then the
+//   off-diagonal blocks by block diagonals: eight barrier phases in all), kept in the strict upper triangle
+//   (X(i, j) at (j, i)), where panelRowsInverse and the solves read it.
 __global__ void __launch_bounds__(DIAGONAL_THREADS) diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0)
 {
     constexpr int LD = BLOCK + 1;
     constexpr int PARTS = DIAGONAL_THREADS / BLOCK;
     __shared__ double a[BLOCK * LD];
-    __shared__ double scaled[BLOCK];         // w_j = l_jk d_k of the step
-    __shared__ double partial[PARTS * BLOCK]; // partial sums of a row of the inverse
+    __shared__ double scaled[2][BLOCK];      // w_j = l_jk d_k of step k in scaled[k & 1]
+    // products T of the inverse's off-diagonal blocks (at most three 16 x 16 blocks at a time)
+    __shared__ double products[(BLOCK / INVERSE_SUB - 1) * INVERSE_SUB * INVERSE_SUB];
     const std::int32_t s = list[blockIdx.x];
     const FrontDesc f = args.fronts[s];
     const int n = f.c + f.r;
@@ -346,49 +349,119 @@ __global__ void __launch_bounds__(DIAGONAL_THREADS) diagonalBlocks(FactorArgs ar
     __syncthreads();
     const int row = t & (BLOCK - 1);
     const int part = t / BLOCK;
+    // Column 0: l_i0 = a_i0 / d_0 and the scaled values w_i = l_i0 d_0.
+    if (t == 0 && kb > 0 && isBadPivot(a[0]))
+        atomicMin(args.zeroPivot + s, k0);
+    if (t > 0 && t < kb)
+    {
+        const double pivot = a[0];
+        const double l = a[t] / pivot;
+        a[t] = l;
+        scaled[0][t] = l * pivot;
+    }
+    __syncthreads();
+    // Step k, one barrier: the rows below k take column k's terms, a_ij -= l_ik w_j (thread (row, part): the columns
+    // j = k + 1 + part, k + 1 + part + PARTS, ... of its row), and column k + 1 is finished in the same phase: the
+    // thread holding a_{i,k+1} (part 0) forms the pivot d_{k+1} = a_{k+1,k+1} - l_{k+1,k} w_{k+1} itself (every one
+    // of them from the same values, so the same bits; the pivot's own thread leaves a_{k+1,k+1} unchanged in this
+    // step and stores d_{k+1} at the start of the next), then l_{i,k+1} = a_{i,k+1} / d_{k+1} and its scaled value.
+    double pendingPivot = 0.0;
 #pragma unroll 1
     for (int k = 0; k < kb; ++k)
     {
-        const double pivot = a[k + k * LD];
-        if (t == 0 && isBadPivot(pivot))
-            atomicMin(args.zeroPivot + s, k0 + k);
-        if (t > k && t < kb)
+        const double* w = scaled[k & 1];
+        double* wNext = scaled[(k + 1) & 1];
+        if (k > 0 && part == 0 && row == k)
         {
-            const double l = a[t + k * LD] / pivot;
-            a[t + k * LD] = l;
-            scaled[t] = l * pivot;
+            a[k + k * LD] = pendingPivot;
+            if (isBadPivot(pendingPivot))
+                atomicMin(args.zeroPivot + s, k0 + k);
         }
-        __syncthreads();
         if (row > k && row < kb)
         {
             const double l = a[row + k * LD];
 #pragma unroll 4
             for (int j = k + 1 + part; j <= row; j += PARTS)
-                a[row + j * LD] -= l * scaled[j];
+                if (j != row || j != k + 1) // the next pivot waits for its own step
+                    a[row + j * LD] -= l * w[j];
+            if (part == 0 && k + 1 < kb)
+            {
+                double pivot = a[(k + 1) + (k + 1) * LD];
+                pivot -= a[(k + 1) + k * LD] * w[k + 1];
+                if (row == k + 1)
+                {
+                    pendingPivot = pivot;
+                }
+                else
+                {
+                    const double next = a[row + (k + 1) * LD] / pivot;
+                    a[row + (k + 1) * LD] = next;
+                    wNext[row] = next * pivot;
+                }
+            }
         }
         __syncthreads();
     }
-    // the inverse, row i from rows < i (thread (part, j): the terms q = part, part + PARTS, ... of X(i, j))
-#pragma unroll 1
-    for (int i = 1; i < kb; ++i)
+    // the inverse by 16 x 16 blocks: first the four diagonal blocks by substitution (thread t < BLOCK takes column t
+    // of its block, X(i, j) = -sum_{j <= q < i} L(i, q) X(q, j) in q order), then the off-diagonal blocks by block
+    // diagonals, X_IJ = -X_II (sum_{J <= K < I} L_IK X_KJ); X(i, j) is kept at (j, i). Beyond kb the block holds the
+    // identity, so every value stays finite.
+    if (t >= kb && t < BLOCK)
+        a[t + t * LD] = 1.0;
+    __syncthreads();
+    if (t < BLOCK)
     {
-        const int j = row;
-        double sum = 0.0;
-#pragma unroll 4
-        for (int q = part; q < i; q += PARTS)
-        {
-            const double x = q > j ? a[j + q * LD] : (q == j ? 1.0 : 0.0);
-            sum += a[i + q * LD] * x;
-        }
-        partial[part * BLOCK + j] = sum;
-        __syncthreads();
-        if (t < i)
-        {
-            double total = partial[t];
+        const int j0 = t & ~(INVERSE_SUB - 1);
+        const int jj = t - j0;
+        double x[INVERSE_SUB];
 #pragma unroll
-            for (int p = 1; p < PARTS; ++p)
-                total += partial[p * BLOCK + t];
-            a[t + i * LD] = -total;
+        for (int i = 0; i < INVERSE_SUB; ++i)
+        {
+            double sum = 0.0;
+#pragma unroll
+            for (int q = 0; q < i; ++q)
+                if (q >= jj)
+                    sum += a[(j0 + i) + (j0 + q) * LD] * x[q];
+            x[i] = i == jj ? 1.0 : -sum;
+            if (i > jj)
+                a[t + (j0 + i) * LD] = x[i];
+        }
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int d = 1; d < BLOCK / INVERSE_SUB; ++d)
+    {
+        const int count = (BLOCK / INVERSE_SUB - d) * INVERSE_SUB * INVERSE_SUB;
+        for (int e = t; e < count; e += DIAGONAL_THREADS) // T_IJ = sum_{J <= K < I} L_IK X_KJ
+        {
+            const int b = e / (INVERSE_SUB * INVERSE_SUB);
+            const int p = (e / INVERSE_SUB) % INVERSE_SUB;
+            const int q = e % INVERSE_SUB;
+            const int jBase = b * INVERSE_SUB;
+            const int iRow = (b + d) * INVERSE_SUB + p;
+            double sum = a[iRow + (jBase + q) * LD]; // X_JJ(q, q) = 1
+#pragma unroll 1
+            for (int r = q + 1; r < INVERSE_SUB; ++r)
+                sum += a[iRow + (jBase + r) * LD] * a[(jBase + q) + (jBase + r) * LD];
+#pragma unroll 1
+            for (int kBase = jBase + INVERSE_SUB; kBase < (b + d) * INVERSE_SUB; kBase += INVERSE_SUB)
+#pragma unroll 4
+                for (int r = 0; r < INVERSE_SUB; ++r)
+                    sum += a[iRow + (kBase + r) * LD] * a[(jBase + q) + (kBase + r) * LD];
+            products[e] = sum;
+        }
+        __syncthreads();
+        for (int e = t; e < count; e += DIAGONAL_THREADS) // X_IJ = -X_II T_IJ
+        {
+            const int b = e / (INVERSE_SUB * INVERSE_SUB);
+            const int p = (e / INVERSE_SUB) % INVERSE_SUB;
+            const int q = e % INVERSE_SUB;
+            const int iBase = (b + d) * INVERSE_SUB;
+            double sum = products[e];
+#pragma unroll 1
+            for (int r = 0; r < p; ++r)
+                sum += a[(iBase + r) + (iBase + p) * LD] * products[b * INVERSE_SUB * INVERSE_SUB + r * INVERSE_SUB + q];
+            a[(b * INVERSE_SUB + q) + (iBase + p) * LD] = -sum;
         }
         __syncthreads();
     }
