@@ -527,23 +527,32 @@ Plan buildPlan(const Symbolic& symbolic)
         // ---- forward sweep ----
         std::vector<std::int32_t> solveSmall;
         std::vector<std::int32_t> solveLarge;
-        std::int32_t maxSmallColumns = 0;
         std::int32_t maxColumns = 0;
         for (const std::int32_t s : members)
         {
             const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
             if (f.c <= SOLVE_SMALL_COLUMNS)
-            {
                 solveSmall.push_back(s);
-                maxSmallColumns = std::max(maxSmallColumns, f.c);
-            }
             else
             {
                 solveLarge.push_back(s);
                 maxColumns = std::max(maxColumns, f.c);
             }
         }
-        addList(plan, plan.forwardLaunches, LaunchKind::ForwardSmall, solveSmall, 0, maxSmallColumns);
+        // The small supernodes by width class (at most 16, 32 or SOLVE_SMALL_COLUMNS columns): each launch's shared
+        // memory is sized for its widest supernode, so the narrow ones (most of the lowest levels) fit more blocks
+        // per SM. The supernodes of one level are independent, so the split changes no result.
+        std::vector<std::vector<std::int32_t>> smallClasses(3);
+        std::vector<std::int32_t> smallClassColumns(3, 0);
+        for (const std::int32_t s : solveSmall)
+        {
+            const std::int32_t c = plan.fronts[static_cast<std::size_t>(s)].c;
+            const std::size_t k = c <= 16 ? 0 : c <= 32 ? 1 : 2;
+            smallClasses[k].push_back(s);
+            smallClassColumns[k] = std::max(smallClassColumns[k], c);
+        }
+        for (std::size_t k = 0; k < smallClasses.size(); ++k)
+            addList(plan, plan.forwardLaunches, LaunchKind::ForwardSmall, smallClasses[k], 0, smallClassColumns[k]);
         {
             // The children's update rows of the large supernodes, by ranges of GATHER_POSITIONS front positions.
             constexpr std::int32_t GATHER_POSITIONS = 64;
@@ -584,7 +593,8 @@ Plan buildPlan(const Symbolic& symbolic)
 
         // ---- backward sweep (collected per level, emitted top level first) ----
         std::vector<Launch>& backward = backwardByLevel[static_cast<std::size_t>(level)];
-        addList(plan, backward, LaunchKind::BackwardSmall, solveSmall, 0, maxSmallColumns);
+        for (std::size_t k = 0; k < smallClasses.size(); ++k)
+            addList(plan, backward, LaunchKind::BackwardSmall, smallClasses[k], 0, smallClassColumns[k]);
         // x_F -= L21^T X[R(s)] by 64-column tiles; R(s) longer than SOLVE_ROWS_CHUNK in chunks (task j0: the chunk's
         // first row, k0: its partial's slot, -1 for an unsplit tile), then the partials summed in chunk order.
         std::vector<TileTask> rowTiles;
