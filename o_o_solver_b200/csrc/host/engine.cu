@@ -168,7 +168,16 @@ public:
     {
         check(cudaSetDevice(device), "cudaSetDevice");
         m_plan = buildPlan(symbolic);
-        check(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        // The main stream at the highest priority, the lookahead's side stream at the lowest: when an SM frees up,
+        // the chain of a front's steps (one or a few blocks a launch) is scheduled before the side's update tiles.
+        int leastPriority = 0;
+        int greatestPriority = 0;
+        check(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority), "stream priorities");
+        check(cudaStreamCreateWithPriority(&m_stream, cudaStreamNonBlocking, greatestPriority), "cudaStreamCreate");
+        check(cudaStreamCreateWithPriority(&m_side, cudaStreamNonBlocking, leastPriority), "cudaStreamCreate");
+        check(cudaEventCreateWithFlags(&m_fork, cudaEventDisableTiming), "cudaEventCreate");
+        for (cudaEvent_t& e : m_groupDone)
+            check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
         check(cudaEventCreate(&m_start), "cudaEventCreate");
         check(cudaEventCreate(&m_stop), "cudaEventCreate");
         m_fronts.upload(m_plan.fronts, m_stream, "plan: fronts");
@@ -232,6 +241,11 @@ public:
         cudaSetDevice(m_device);
         if (m_stream != nullptr)
             cudaStreamSynchronize(m_stream);
+        if (m_side != nullptr)
+            cudaStreamSynchronize(m_side);
+        cudaEventDestroy(m_fork);
+        for (cudaEvent_t e : m_groupDone)
+            cudaEventDestroy(e);
         cudaEventDestroy(m_start);
         cudaEventDestroy(m_stop);
         for (cudaEvent_t e : m_profileEvents)
@@ -240,6 +254,8 @@ public:
             cudaEventDestroy(e);
         if (m_stream != nullptr)
             cudaStreamDestroy(m_stream);
+        if (m_side != nullptr)
+            cudaStreamDestroy(m_side);
     }
 
     [[nodiscard]] cudaStream_t stream() const noexcept { return m_stream; }
@@ -1288,11 +1304,19 @@ public:
     }
 
 private:
+    // The factor launches in plan order on the main stream, except the side groups (the far part of a finished
+    // macro panel's update, Launch::sideGroup), which fork onto the side stream and are waited for where the plan
+    // says (Launch::waitGroup) and at the end. A profiled factorisation runs everything on the main stream.
     void runFactorLaunches(const device::FactorArgs& args)
     {
         std::size_t index = 0;
+        std::int32_t forkedGroup = -1;
+        std::int32_t lastGroup = -1;
         for (const Launch& launch : m_plan.factorLaunches)
         {
+            const bool lookahead = !m_profile;
+            if (lookahead && launch.waitGroup >= 0)
+                check(cudaStreamWaitEvent(m_stream, m_groupDone[launch.waitGroup & 1], 0), "wait for a side group");
             if (m_profile)
                 check(cudaEventRecord(profileEvent(2 * index), m_stream), "profile event");
             const std::int32_t mixed = m_mixed ? m_plan.mixedOfFactorLaunch[index] : -1;
@@ -1304,12 +1328,26 @@ private:
                     args, m_tiles.get() + replacement.offset, m_mixedError.get());
                 check(cudaGetLastError(), "mixed update launch");
             }
+            else if (lookahead && launch.sideGroup >= 0)
+            {
+                if (launch.sideGroup != forkedGroup)
+                {
+                    check(cudaEventRecord(m_fork, m_stream), "fork the side stream");
+                    check(cudaStreamWaitEvent(m_side, m_fork, 0), "fork the side stream");
+                    forkedGroup = launch.sideGroup;
+                }
+                launchFactor(launch, args, m_side);
+                check(cudaEventRecord(m_groupDone[launch.sideGroup & 1], m_side), "side group");
+                lastGroup = launch.sideGroup;
+            }
             else
-                launchFactor(launch, args);
+                launchFactor(launch, args, m_stream);
             if (m_profile)
                 check(cudaEventRecord(profileEvent(2 * index + 1), m_stream), "profile event");
             ++index;
         }
+        if (lastGroup >= 0)
+            check(cudaStreamWaitEvent(m_stream, m_groupDone[lastGroup & 1], 0), "join the side stream");
         check(cudaGetLastError(), "factorisation launch");
     }
 
@@ -1324,7 +1362,7 @@ private:
         return m_profileEvents[k];
     }
 
-    void launchFactor(const Launch& launch, const device::FactorArgs& args)
+    void launchFactor(const Launch& launch, const device::FactorArgs& args, cudaStream_t stream)
     {
         {
             switch (launch.kind)
@@ -1332,28 +1370,28 @@ private:
             case LaunchKind::SmallFronts:
             {
                 const std::size_t smem = device::smallFrontSmem(launch.smemOrder);
-                device::smallFronts<<<launch.count, SMALL_THREADS, smem, m_stream>>>(
+                device::smallFronts<<<launch.count, SMALL_THREADS, smem, stream>>>(
                     args, m_lists.get() + launch.offset, m_structureError.get());
                 break;
             }
             case LaunchKind::AssembleFronts:
-                device::assembleFronts<<<launch.count, 256, 0, m_stream>>>(args, m_pieces.get() + launch.offset,
+                device::assembleFronts<<<launch.count, 256, 0, stream>>>(args, m_pieces.get() + launch.offset,
                                                                            m_structureError.get());
                 break;
             case LaunchKind::DiagonalBlocks:
-                device::diagonalBlocks<<<launch.count, device::DIAGONAL_THREADS, 0, m_stream>>>(
+                device::diagonalBlocks<<<launch.count, device::DIAGONAL_THREADS, 0, stream>>>(
                     args, m_lists.get() + launch.offset, launch.k0);
                 break;
             case LaunchKind::PanelRows:
                 device::panelRowsInverse<<<launch.count, device::TILE_THREADS, device::PANEL_ROWS_INVERSE_SMEM,
-                                           m_stream>>>(args, m_tiles.get() + launch.offset, launch.k0);
+                                           stream>>>(args, m_tiles.get() + launch.offset, launch.k0);
                 break;
             case LaunchKind::PanelUpdate:
-                device::panelUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(
+                device::panelUpdate<<<launch.count, device::TILE_THREADS, 0, stream>>>(
                     args, m_tiles.get() + launch.offset, launch.k0);
                 break;
             case LaunchKind::UpdateMatrix:
-                device::updateMatrix<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(
+                device::updateMatrix<<<launch.count, device::TILE_THREADS, 0, stream>>>(
                     args, m_tiles.get() + launch.offset);
                 break;
             default:
@@ -1437,6 +1475,10 @@ private:
     int m_device = 0;
     Plan m_plan;
     cudaStream_t m_stream = nullptr;
+    // the lookahead's side stream, its fork point and the completion of its groups (alternating)
+    cudaStream_t m_side = nullptr;
+    cudaEvent_t m_fork = nullptr;
+    cudaEvent_t m_groupDone[2] = {nullptr, nullptr};
     cudaEvent_t m_start = nullptr;
     cudaEvent_t m_stop = nullptr;
     DeviceArray<device::FrontDesc> m_fronts;

@@ -384,13 +384,19 @@ Plan buildPlan(const Symbolic& symbolic)
             plan.pieces.insert(plan.pieces.end(), pieces.begin(), pieces.end());
             // Two-level blocking: the 64-column steps update the trailing columns of their PANEL_MACRO-column macro
             // panel only (K = 64); after a macro panel's last step, its columns update every later column of the panel
-            // at once (K = PANEL_MACRO), a quarter of the passes over the trailing panel.
+            // at once (K = PANEL_MACRO), a quarter of the passes over the trailing panel. Lookahead: that update is
+            // split into the next macro panel's columns (the main stream, before its steps) and the columns beyond
+            // (a side group, which runs while the next macro panel's steps run; the next split waits for it, since its
+            // near part covers columns the side group updates). The two streams touch disjoint columns, and every
+            // element still receives its macro panels' terms in order.
+            std::int32_t levelLastGroup = -1;
             for (std::int32_t k0 = 0; k0 < maxColumns; k0 += BLOCK)
             {
                 std::vector<std::int32_t> diagonal;
                 std::vector<TileTask> rowTasks;
                 std::vector<TileTask> updateTiles;
                 std::vector<TileTask> macroTiles;
+                std::vector<TileTask> farTiles;
                 const std::int32_t macroStart = k0 / device::PANEL_MACRO * device::PANEL_MACRO;
                 for (const std::int32_t s : large)
                 {
@@ -410,12 +416,25 @@ Plan buildPlan(const Symbolic& symbolic)
                     if (origin >= macroEnd)
                         for (std::int32_t j0 = macroEnd; j0 < f.c; j0 += device::TILE)
                             for (std::int32_t i0 = j0; i0 < n; i0 += device::TILE)
-                                macroTiles.push_back({s, i0, j0, macroEnd - macroStart});
+                                (j0 < macroEnd + device::PANEL_MACRO ? macroTiles : farTiles)
+                                    .push_back({s, i0, j0, macroEnd - macroStart});
                 }
                 addList(plan, plan.factorLaunches, LaunchKind::DiagonalBlocks, diagonal, k0);
                 addTiles(plan, plan.factorLaunches, LaunchKind::PanelRows, rowTasks, k0);
                 addTiles(plan, plan.factorLaunches, LaunchKind::PanelUpdate, updateTiles, k0);
-                addTiles(plan, plan.factorLaunches, LaunchKind::PanelUpdate, macroTiles, macroStart);
+                const std::int32_t previousGroup = plan.sideGroups - 1;
+                if (!farTiles.empty())
+                {
+                    addTiles(plan, plan.factorLaunches, LaunchKind::PanelUpdate, farTiles, macroStart);
+                    plan.factorLaunches.back().sideGroup = plan.sideGroups;
+                    levelLastGroup = plan.sideGroups++;
+                }
+                if (!macroTiles.empty())
+                {
+                    addTiles(plan, plan.factorLaunches, LaunchKind::PanelUpdate, macroTiles, macroStart);
+                    if (previousGroup >= 0)
+                        plan.factorLaunches.back().waitGroup = previousGroup;
+                }
             }
             std::vector<TileTask> schur;
             for (const std::int32_t s : large)
@@ -431,6 +450,8 @@ Plan buildPlan(const Symbolic& symbolic)
                                       plan.fronts[static_cast<std::size_t>(y.front)].c; });
             const std::size_t at = plan.factorLaunches.size();
             addTiles(plan, plan.factorLaunches, LaunchKind::UpdateMatrix, schur);
+            if (levelLastGroup >= 0 && plan.factorLaunches.size() > at)
+                plan.factorLaunches.back().waitGroup = levelLastGroup;
             // The same update matrices by 128 x 128 tiles, for the mixed-precision form.
             std::vector<TileTask> mixed;
             for (const std::int32_t s : large)

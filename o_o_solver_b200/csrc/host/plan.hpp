@@ -67,6 +67,11 @@ struct Launch
     // triangles a launch updates, twice) and the bytes it must move at least.
     double flops = 0.0;
     double bytes = 0.0;
+    // Lookahead (positive definite factorisation): sideGroup >= 0 runs the launch on the side stream, after all the
+    // launches before it in the list on the main stream (a group's first launch forks the side stream off there);
+    // waitGroup >= 0 makes the launch wait until side group waitGroup has finished. Groups count up from 0.
+    std::int32_t sideGroup = -1;
+    std::int32_t waitGroup = -1;
 };
 
 constexpr int LAUNCH_KIND_COUNT = 14;
@@ -109,6 +114,8 @@ struct Plan
     // Mixed precision: for each factorisation launch, the index of the launch that replaces it (-1: none).
     std::vector<Launch> mixedLaunches;
     std::vector<std::int32_t> mixedOfFactorLaunch;
+    // The side groups of the factor launches (Launch::sideGroup): 0 .. sideGroups - 1.
+    std::int32_t sideGroups = 0;
 
     // Indefinite mode: the launches (assembly shared with the positive definite sequence), the large fronts of each
     // level, and each large front's W buffer (n x min(c, PANEL_MACRO) values at wOffset: the W = L D columns of its
