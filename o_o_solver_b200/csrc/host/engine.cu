@@ -358,7 +358,7 @@ public:
         const auto launches = [&]
         {
             runFactorLaunches(args);
-            invertDiagonalBlocks(args);
+            invertDiagonalBlocks(args, false);
             device::pivotSummary<<<summaryBlocks, 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), dimension,
                                                                        referenceDiagonal, maxRatio, m_counters.get(),
                                                                        m_issues.get(), ISSUE_CAPACITY,
@@ -579,7 +579,7 @@ public:
             ++profiled;
         }
         check(cudaGetLastError(), "indefinite factorisation launch");
-        invertDiagonalBlocks(args);
+        invertDiagonalBlocks(args, true);
         device::inertiaPivoted<<<blocksFor(std::max(dimension, 1), 256), 256, 0, m_stream>>>(
             args, pivots, m_supernodeOfColumn.get(), dimension, m_counters.get());
         device::invertPermutation<<<blocksFor(std::max(dimension, 1), 256), 256, 0, m_stream>>>(
@@ -623,10 +623,15 @@ public:
     }
 
     // The inverses of the diagonal blocks the solves' 64-column steps apply (into the blocks' upper triangles).
-    void invertDiagonalBlocks(const device::FactorArgs& args)
+    // The inverses of the diagonal blocks the solves apply: the small fronts' always; the large fronts' only after
+    // an indefinite factorisation (in positive definite mode diagonalBlocks has written them already).
+    void invertDiagonalBlocks(const device::FactorArgs& args, bool largeFronts)
     {
         for (const Launch& launch : m_plan.inverseLaunches)
             device::invertDiagonal<<<launch.count, 64, 0, m_stream>>>(args, m_tiles.get() + launch.offset);
+        if (largeFronts)
+            for (const Launch& launch : m_plan.inverseLaunchesLarge)
+                device::invertDiagonal<<<launch.count, 64, 0, m_stream>>>(args, m_tiles.get() + launch.offset);
         check(cudaGetLastError(), "diagonal inverse launch");
     }
 

@@ -318,7 +318,8 @@ Plan buildPlan(const Symbolic& symbolic)
         byLevel[static_cast<std::size_t>(plan.level[static_cast<std::size_t>(s)])].push_back(s);
 
     std::vector<std::vector<Launch>> backwardByLevel(static_cast<std::size_t>(plan.levelCount));
-    std::vector<TileTask> inverseTasks;
+    std::vector<TileTask> inverseTasks;      // the blocks of the small fronts (smallFronts inverts none)
+    std::vector<TileTask> inverseTasksLarge; // those of the large fronts (diagonalBlocks inverts them itself)
     for (std::int32_t level = 0; level < plan.levelCount; ++level)
     {
         const auto& members = byLevel[static_cast<std::size_t>(level)];
@@ -588,8 +589,12 @@ Plan buildPlan(const Symbolic& symbolic)
             addTiles(plan, plan.forwardLaunches, LaunchKind::ForwardGather, ranges);
         }
         for (const std::int32_t s : members)
-            for (std::int32_t k0 = 0; k0 < plan.fronts[static_cast<std::size_t>(s)].c; k0 += BLOCK)
-                inverseTasks.push_back({s, k0, 0, 0});
+        {
+            const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+            const bool isLarge = f.c + f.r > SMALL_ORDER; // the factorisation's own split, above
+            for (std::int32_t k0 = 0; k0 < f.c; k0 += BLOCK)
+                (isLarge ? inverseTasksLarge : inverseTasks).push_back({s, k0, 0, 0});
+        }
         // Steps of SOLVE_STEP columns: the step's diagonal blocks in one launch, then its products with the rows below.
         constexpr std::int32_t STEP = device::SOLVE_STEP;
         for (std::int32_t k0 = 0; k0 < maxColumns; k0 += STEP)
@@ -669,6 +674,7 @@ Plan buildPlan(const Symbolic& symbolic)
         plan.backwardLaunches.insert(plan.backwardLaunches.end(), launches.begin(), launches.end());
     }
     addTiles(plan, plan.inverseLaunches, LaunchKind::InvertDiagonal, inverseTasks);
+    addTiles(plan, plan.inverseLaunchesLarge, LaunchKind::InvertDiagonal, inverseTasksLarge);
     plan.mixedOfFactorLaunch.resize(plan.factorLaunches.size(), -1);
     return plan;
 }

@@ -110,7 +110,10 @@ struct Plan
     std::vector<Launch> backwardLaunches;
     // The 64-column diagonal blocks (front, k0) of every supernode, inverted after each factorisation into the blocks'
     // upper triangles (the solves apply the inverses).
+    // The diagonal inverses after a factorisation: of the small fronts' blocks, and of the large fronts' blocks
+    // (which diagonalBlocks writes itself; the indefinite path recomputes them).
     std::vector<Launch> inverseLaunches;
+    std::vector<Launch> inverseLaunchesLarge;
     // Mixed precision: for each factorisation launch, the index of the launch that replaces it (-1: none).
     std::vector<Launch> mixedLaunches;
     std::vector<std::int32_t> mixedOfFactorLaunch;
