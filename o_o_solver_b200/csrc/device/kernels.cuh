@@ -111,7 +111,9 @@ constexpr std::size_t smallSolveSmem(int columns)
 }
 __global__ void forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0);
 __global__ void forwardUpdate(SolveArgs a, const TileTask* tasks, int k0);
-__global__ void diagonalSweep(SolveArgs a, const std::int32_t* supernodeOfColumn, int dimension);
+__global__ void diagonalSweep(SolveArgs a, const double* diagonal, int dimension);
+// D of a positive definite factor as one contiguous vector (diagonal[eq] = d_eq), gathered once per factorisation.
+__global__ void gatherDiagonal(FactorArgs args, const std::int32_t* supernodeOfColumn, int dimension, double* diagonal);
 __global__ void backwardSmall(SolveArgs a, const std::int32_t* list, int cmax);
 __global__ void backwardRows(SolveArgs a, const TileTask* tasks);
 __global__ void backwardRowsReduce(SolveArgs a, const TileTask* tasks);

@@ -500,17 +500,24 @@ __global__ void __launch_bounds__(TILE_THREADS) forwardUpdate(SolveArgs a, const
 }
 
 // The diagonal sweep: X[eq] /= d_eq.
-__global__ void diagonalSweep(SolveArgs a, const std::int32_t* supernodeOfColumn, int dimension)
+__global__ void diagonalSweep(SolveArgs a, const double* diagonal, int dimension)
 {
     const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int w = a.width;
     if (e >= static_cast<std::int64_t>(dimension) * w)
         return;
-    const int eq = static_cast<int>(e / w);
-    const FrontDesc f = a.fronts[supernodeOfColumn[eq]];
+    a.x[e] = a.x[e] / diagonal[e / w];
+}
+
+__global__ void gatherDiagonal(FactorArgs args, const std::int32_t* supernodeOfColumn, int dimension, double* diagonal)
+{
+    const int eq = blockIdx.x * blockDim.x + threadIdx.x;
+    if (eq >= dimension)
+        return;
+    const FrontDesc f = args.fronts[supernodeOfColumn[eq]];
     const int k = eq - f.first;
     const std::int64_t n = f.c + f.r;
-    a.x[e] = a.x[e] / a.panels[f.panel + k + k * n];
+    diagonal[eq] = args.panels[f.panel + k + k * n];
 }
 
 // Backward sweep of a small supernode (c <= 64), one block of TILE_THREADS: x_F <- L11^-T (x_F - L21^T X[R(s)]),

@@ -194,6 +194,7 @@ public:
         m_tiles.upload(m_plan.tiles, m_stream, "plan: tiles");
         m_pieces.upload(m_plan.pieces, m_stream, "plan: pieces");
         m_zeroPivot.allocate(static_cast<std::size_t>(m_plan.supernodeCount), "factor: zero pivots");
+        m_diagonal.allocate(static_cast<std::size_t>(std::max(m_plan.dimension, 1)), "factor: diagonal");
         m_counters.allocate(8, "factor: counters");
         m_issues.allocate(ISSUE_CAPACITY, "factor: issues");
         const std::size_t summaryBlocks = blocksFor(std::max(m_plan.dimension, 1), 256);
@@ -363,6 +364,8 @@ public:
                                                                        referenceDiagonal, maxRatio, m_counters.get(),
                                                                        m_issues.get(), ISSUE_CAPACITY,
                                                                        m_blockRatio.get(), m_blockEquation.get());
+            device::gatherDiagonal<<<summaryBlocks, 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), dimension,
+                                                                         m_diagonal.get());
             check(cudaGetLastError(), "pivot summary launch");
         };
         // Profiled factorisations launch one by one (events between the launches); the others replay a graph.
@@ -781,7 +784,7 @@ public:
                 device::diagonalSweepPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(
                     args, m_supernodeOfColumn.get(), m_subdiagonal.get(), n);
             else
-                device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), n);
+                device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_diagonal.get(), n);
             endSolveRecord(record);
             runSweep(args, m_plan.backwardLaunches);
         };
@@ -1300,7 +1303,8 @@ public:
     }
     [[nodiscard]] std::int64_t factorLaunchCount() const noexcept
     {
-        return static_cast<std::int64_t>(m_plan.factorLaunches.size()) + 1;
+        // the plan's launches, the diagonal inverses, the pivot summary and the gathered diagonal
+        return static_cast<std::int64_t>(m_plan.factorLaunches.size() + m_plan.inverseLaunches.size()) + 2;
     }
     [[nodiscard]] std::int64_t solveLaunchCount(std::int64_t columns) const noexcept
     {
@@ -1547,6 +1551,7 @@ private:
     DeviceArray<std::int32_t> m_fullColumns;
     DeviceArray<std::int32_t> m_fullSource;
     DeviceArray<std::int32_t> m_groupFirst;
+    DeviceArray<double> m_diagonal; // D of a positive definite factor, contiguous (gatherDiagonal)
     std::int32_t m_residualGroups = 0;
     std::int64_t m_fullTerms = -1;
     const std::int64_t* m_matrixOffsets = nullptr;
