@@ -57,6 +57,8 @@ constexpr int SOLVE_STEP = 256;
 // The columns of a macro panel of the factorisation: the 64-column steps inside it update its own later columns, and
 // once it is done it updates the rest of the front's panel in one product of K = PANEL_MACRO.
 constexpr int PANEL_MACRO = 256;
+// panelRowsInverse: the 64-row halves of one task (a task covers TILE * PANEL_ROW_HALVES rows below the block).
+constexpr int PANEL_ROW_HALVES = 1;
 // The rows of R(s) one block of the backward product x_F -= L21^T X[R(s)] takes; longer R(s) are split into chunks
 // whose partial products are summed in chunk order.
 constexpr int SOLVE_ROWS_CHUNK = 512;

@@ -476,9 +476,9 @@ __global__ void __launch_bounds__(DIAGONAL_THREADS) diagonalBlocks(FactorArgs ar
 }
 
 // The rows below step k0's diagonal block, L21 = A21 L11^-T D^-1, as products on the FP64 tensor cores: for each
-// 64-row half of a 128-row task, Y = A21 (L11^-1)^T with L11^-1 from the block's strict upper triangle (unit diagonal),
-// then l_ij = y_ij / d_j, written in place (a block stages its rows before it writes them). Dynamic shared memory:
-// PANEL_ROWS_INVERSE_SMEM bytes.
+// 64-row half of a task (64 * PANEL_ROW_HALVES rows), Y = A21 (L11^-1)^T with L11^-1 from the block's strict upper
+// triangle (unit diagonal), then l_ij = y_ij / d_j, written in place (a block stages its rows before it writes them).
+// Dynamic shared memory: PANEL_ROWS_INVERSE_SMEM bytes.
 __global__ void __launch_bounds__(TILE_THREADS) panelRowsInverse(FactorArgs args, const TileTask* tasks, int k0)
 {
     constexpr int LD = TILE + TILE_PAD;
@@ -513,7 +513,7 @@ __global__ void __launch_bounds__(TILE_THREADS) panelRowsInverse(FactorArgs args
         sd[j] = j < kb ? sB[j * LD + j] : 1.0;
         sB[j * LD + j] = j < kb ? 1.0 : 0.0;
     }
-    for (int half = 0; half < 2; ++half)
+    for (int half = 0; half < PANEL_ROW_HALVES; ++half)
     {
         const std::int64_t i0 = task.i0 + half * TILE;
         if (i0 >= n)

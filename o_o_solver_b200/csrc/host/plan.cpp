@@ -16,7 +16,8 @@ using device::FrontDesc;
 using device::TileTask;
 
 constexpr int BLOCK = 64;
-constexpr int PANEL_ROWS = 128;
+constexpr int PANEL_ROWS = 128;                                     // rows of a pivoted panel-rows task
+constexpr int PANEL_ROWS_TASK = device::TILE * device::PANEL_ROW_HALVES; // rows of a panelRowsInverse task
 
 void addList(Plan& plan, std::vector<Launch>& launches, LaunchKind kind, const std::vector<std::int32_t>& list,
              std::int32_t k0 = 0, std::int32_t smemOrder = 0)
@@ -127,7 +128,7 @@ void annotate(Plan& plan, const std::vector<std::int64_t>& cscTermsOfFront)
                 const FrontDesc& f = front(t.front);
                 const std::int64_t n = f.c + f.r;
                 const std::int64_t kb = std::min<std::int64_t>(BLOCK, f.c - launch.k0);
-                const std::int64_t rows = std::min<std::int64_t>(PANEL_ROWS, n - t.i0);
+                const std::int64_t rows = std::min<std::int64_t>(PANEL_ROWS_TASK, n - t.i0);
                 flops += static_cast<double>(rows) * static_cast<double>(kb * (kb - 1) + kb);
                 bytes += 2.0 * V * static_cast<double>(rows * kb);
                 break;
@@ -408,7 +409,7 @@ Plan buildPlan(const Symbolic& symbolic)
                     const std::int32_t kb = std::min(BLOCK, f.c - k0);
                     const std::int32_t macroEnd = std::min(macroStart + device::PANEL_MACRO, f.c);
                     diagonal.push_back(s);
-                    for (std::int32_t i0 = k0 + kb; i0 < n; i0 += PANEL_ROWS)
+                    for (std::int32_t i0 = k0 + kb; i0 < n; i0 += PANEL_ROWS_TASK)
                         rowTasks.push_back({s, i0, 0, 0});
                     const std::int32_t origin = k0 + BLOCK;
                     for (std::int32_t j0 = origin; j0 < macroEnd; j0 += device::TILE)
