@@ -77,6 +77,9 @@ def parse():
                         help="with --factor-only: also solve 64 load columns and write both launch lists (kind, "
                              "blocks, step column, device seconds) to PATH as JSON")
     parser.add_argument("--profile-rhs", type=int, default=64, help="with --launch-profile: the solve's columns")
+    parser.add_argument("--detail", metavar="PATH", default=None,
+                        help="write the whole result record (kernel tables, every leg's detail) to PATH as JSON; "
+                             "without it the record goes to stderr as one line")
     return parser.parse_args()
 
 
@@ -183,19 +186,20 @@ def accuracy(csc, x, b):
     return float(residual.max()), float(backward.max())
 
 
-def cpu_baseline(fixture, csc, loads, threads, tolerance):
-    """The reference's factorisation + solve (oracle/_ref/liboos_ref.so) of the same matrix on the host cores."""
+def cpu_baseline(fixture, csc, loads, threads, graph):
+    """The reference's factorisation + solve (oracle/_ref/liboos_ref.so) of the same matrix on the host cores. The
+    matrix and loads may come from the package's generator or from oracle/plate_model.py (the same values bit for
+    bit); the accuracy check is the oracle's own, so this leg loads nothing of the package."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    from o_o_solver_b200 import workloads
+    import plate_model
 
-    model_graph = fixture["_graph"]
-    sym = oracle.analyse(*model_graph, given_order=fixture["node_order"], threads=threads)
+    sym = oracle.analyse(*graph, given_order=fixture["node_order"], threads=threads)
     start = time.perf_counter()
     factor = oracle.factorise(sym, csc.offsets, csc.rows, csc.values, threads=threads)
     x = factor.solve(loads, threads=threads)
     seconds = time.perf_counter() - start
-    resid, backward = accuracy(csc, x, loads)
+    resid, backward = plate_model.accuracy(plate_model.Csc(csc.offsets, csc.rows, csc.values), x, loads)
     return {"seconds": seconds, "factor_seconds": factor.seconds, "residual": resid, "backward_error": backward,
             "kernel": ["reference", "avx2", "avx512"][factor.kernel] if factor.kernel < 3 else str(factor.kernel)}
 
@@ -351,10 +355,32 @@ def mixed_leg(factor, d_csc, d_loads, d_x, fp64_stats, tolerance, dev, torch):
     }
 
 
-# DRAM traffic of the plate's update-matrix launches (the statics roofline's kernel), measured by ncu
-# (--metrics dram__bytes_read.sum,dram__bytes_write.sum only, -k regex:"^updateMatrix$" -c 16 over
-# `bench.py --factor-only plate580:fp64 --steps 1 --warmup 1`): 12.23 GB read + 6.81 GB written over 16 launches.
-UPDATE_MATRIX_TRAFFIC = (12227441920 + 6808305664) / 16
+# The kernel behind each kernel kind of the factorisation's statistics.
+KERNEL_OF_KIND = {"small_fronts": "smallFronts", "assemble_fronts": "assembleFronts",
+                  "diagonal_blocks": "diagonalBlocks", "panel_rows": "panelRowsInverse",
+                  "panel_update": "panelUpdate", "update_matrix": "updateMatrix"}
+TRAFFIC_TABLE = os.path.join(ROOT, "profiles", "dram_traffic.md")
+
+
+def measured_traffic(kind, algorithmic_bytes_per_launch):
+    """DRAM bytes per launch of a kernel kind: the ratio of ncu's dram__bytes_read.sum + dram__bytes_write.sum to the
+    algorithmic bytes, measured on a capture small enough for the capture rules (profiles/dram_traffic.md, a row
+    `| kernel | workload | dram bytes | algorithmic bytes | ratio |`), applied to this run's algorithmic bytes per
+    launch. None when the kernel has no row."""
+    kernel = KERNEL_OF_KIND.get(kind, kind)
+    if not os.path.exists(TRAFFIC_TABLE):
+        return None, None
+    with open(TRAFFIC_TABLE) as table:
+        for row in table:
+            cells = [c.strip().strip("`") for c in row.strip().strip("|").split("|")]
+            if len(cells) >= 5 and cells[0] == kernel:
+                try:
+                    ratio = float(cells[4])
+                except ValueError:
+                    continue
+                return ratio * algorithmic_bytes_per_launch, f"{cells[1]}: {ratio:.3f} x the algorithmic bytes"
+    return None, None
+
 
 BATCH_MODELS = 512
 BATCH_RHS = 8
@@ -572,22 +598,29 @@ def learned_leg(args):
 
 
 def run_reference(args, rank, world):
+    """The reference's own CPU path on the workload: its factorisation and solve (oracle/_ref, built from the
+    reference's sources) on all host cores. The plate, its node graph and its loads come from oracle/plate_model.py,
+    so this process never loads the package's CUDA library. Under torchrun rank 0 alone runs; the others exit."""
     if rank != 0:
         return
-    model, fixture, csc, loads = load_workload(args.workload)
-    fixture = dict(fixture)
-    fixture["_graph"] = (model.offsets, model.neighbours, model.weights)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import plate_model
+
+    size, columns = WORKLOADS[args.workload]
+    fixture = dict(np.load(os.path.join(GOLDEN, f"plate{size}.npz")))
+    plate = plate_model.Plate(size, size)
+    csc = plate.csc(fixture["node_order"])
+    loads = plate.loads(fixture["node_order"], columns)
     threads = os.cpu_count() or 1
     times = []
     result = None
     for step in range(args.warmup + args.steps):
-        result = cpu_baseline(fixture, csc, loads, threads, args.tolerance)
+        result = cpu_baseline(fixture, csc, loads, threads, (plate.offsets, plate.neighbours, plate.weights))
         if step >= args.warmup:
             times.append(result["seconds"])
     value = statistics.median(times)
     line = {
-        "metric": "plate statics factor+solve time (2M-dof, 64 RHS)" if args.workload == "plate580" else
-        f"{args.workload} statics factor+solve time",
+        "metric": metric_name(args.workload),
         "value": value, "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded loads on a generated shell plate)",
@@ -595,10 +628,17 @@ def run_reference(args, rank, world):
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "reference",
                          "sample": f"full {args.workload} factor + {loads.shape[1]}-column solve, kernel family "
-                                   f"{result['kernel']}, residual {result['residual']:.2e}, backward error {result['backward_error']:.1e}"},
+                                   f"{result['kernel']}, residual {result['residual']:.2e}, backward error "
+                                   f"{result['backward_error']:.1e}"},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def metric_name(workload):
+    if workload == "plate580":
+        return "plate statics factor+solve time (2M-dof, 64 RHS)"
+    return f"{workload} statics factor+solve time"
 
 
 def run_gpu(args, rank, world, local_rank):
@@ -691,20 +731,19 @@ def run_gpu(args, rank, world, local_rank):
     if compute_bound:
         fp64 = fp64_gemm_peak(torch, dev)
         achieved = d["flops"] / d["seconds"] / 1e12
+        traffic, traffic_source = measured_traffic(dominant, d["bytes"] / d["launches"])
         roofline = {"bound": "tensor", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64,
-                    "traffic": UPDATE_MATRIX_TRAFFIC if (dominant == "update_matrix" and args.workload == "plate580")
-                    else None,
-                    "traffic_note": "DRAM bytes read + written per launch, averaged over the 16 update-matrix launches "
-                                    "of one plate factorisation (ncu dram__bytes_read.sum + dram__bytes_write.sum "
-                                    "only); algorithmic: " + str(round(d["bytes"] / d["launches"] / 1e9, 3)) +
-                                    " GB per launch",
+                    "traffic": traffic, "traffic_source": traffic_source,
+                    "algorithmic_bytes_per_launch": d["bytes"] / d["launches"],
                     "kernel": dominant, "launches": d["launches"],
                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor)",
                     "share": d["seconds"] / sum(v["seconds"] for v in stats.values())}
     else:
         achieved = d["bytes"] / d["seconds"] / 1e9
+        traffic, traffic_source = measured_traffic(dominant, d["bytes"] / d["launches"])
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                    "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": dominant,
+                    "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "traffic_source": traffic_source,
+                    "kernel": dominant,
                     "launches": d["launches"], "peak_source": f"hbm_gbs ({peak_source})",
                     "share": d["seconds"] / sum(v["seconds"] for v in stats.values())}
     kernel_table = {k: {"ms": round(v["seconds"] * 1e3, 3), "launches": v["launches"],
@@ -715,10 +754,8 @@ def run_gpu(args, rank, world, local_rank):
     baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            fixture = dict(fixture)
-            fixture["_graph"] = (model.offsets, model.neighbours, model.weights)
             threads = os.cpu_count() or 1
-            cb = cpu_baseline(fixture, csc, loads, threads, args.tolerance)
+            cb = cpu_baseline(fixture, csc, loads, threads, (model.offsets, model.neighbours, model.weights))
             baseline = {"value": cb["seconds"], "unit": "s", "cores": threads, "kind": "reference",
                         "sample": f"one full {args.workload} factor + {columns}-column solve "
                                   f"({cb['kernel']} kernels, factor {cb['factor_seconds']:.3f} s, "
@@ -733,20 +770,84 @@ def run_gpu(args, rank, world, local_rank):
 
     if rank == 0:
         line = {
-            "metric": "plate statics factor+solve time (2M-dof, 64 RHS)" if args.workload == "plate580" else
-            f"{args.workload} statics factor+solve time",
-            "value": seconds / world, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "metric": metric_name(args.workload),
+            "value": seconds, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": seconds * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded loads on a generated shell plate)",
             "config": {"workload": args.workload, "equations": n, "rhs": columns, "form": "plain FP64",
                        "flops_per_factor": symbolic.flop_count, "l2": "inputs larger than L2 (panels 6 GB)",
-                       "parallelism": f"replicas x{world}"},
-            "residual": resid, "backward_error": backward, "refinement": refinement, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
-            "kernels": kernel_table, "clocks": clocks.summary(), "cpu_baseline": baseline,
-            "factor_tflops": symbolic.flop_count / seconds / 1e12, "modes": modes, "forms": {"mixed": mixed, "batched": batched, "learned_start": learned},
+                       "parallelism": f"replicas x{world}" if world > 1 else "one GPU"},
+            "residual": resid, "backward_error": backward, "refinement": refinement, "e2e": e2e,
+            "gpu_launches": launches, "roofline": roofline, "kernels": kernel_table, "clocks": clocks.summary(),
+            "cpu_baseline": baseline, "factor_tflops": symbolic.flop_count / refinement["factor_seconds"] / 1e12,
+            "modes": modes, "forms": {"mixed": mixed, "batched": batched, "learned_start": learned},
         }
-        print(json.dumps(line), flush=True)
+        emit(line, args.detail)
     replicas.close()
+
+
+def _round(value, digits=4):
+    if isinstance(value, float):
+        return float(f"{value:.{digits}g}")
+    if isinstance(value, dict):
+        return {k: _round(v, digits) for k, v in value.items()}
+    if isinstance(value, list):
+        return [_round(v, digits) for v in value]
+    return value
+
+
+def _pick(source, *keys):
+    if not source:
+        return None
+    return {k: source[k] for k in keys if k in source}
+
+
+def compact_line(full):
+    """The final stdout line: the fields a reader of the result needs, a few numbers per leg, well under 4 KB.
+    Everything else (kernel tables, per-design rows, phases) goes to the detail record."""
+    line = {k: full[k] for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+                                 "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config")}
+    line.update({k: full.get(k) for k in ("residual", "backward_error", "e2e", "gpu_launches", "clocks",
+                                          "cpu_baseline", "factor_tflops")})
+    line["refinement"] = _pick(full.get("refinement"), "steps", "factor_seconds", "solve_seconds")
+    line["roofline"] = _pick(full.get("roofline"), "bound", "achieved", "peak", "unit", "frac", "traffic", "kernel",
+                             "launches", "share", "peak_source")
+    modes = full.get("modes")
+    if modes:
+        line["modes"] = _pick(modes, "value", "unit", "factorisations", "block_steps", "verified",
+                              "eigenvalue_max_rel_error_vs_reference", "operator_gbs")
+        if modes.get("e2e"):
+            line["modes"]["e2e"] = modes["e2e"]["value"]
+        if modes.get("cpu_baseline"):
+            line["modes"]["cpu_baseline"] = _pick(modes["cpu_baseline"], "value", "cores", "kind", "sample")
+    forms = full.get("forms") or {}
+    compact_forms = {}
+    if forms.get("mixed"):
+        m = forms["mixed"]
+        compact_forms["mixed"] = {"step_s": m.get("step_s"), "factor_device_s": m.get("factor_device_s"),
+                                  **_pick(m.get("gmres_ir"), "backward_error", "reaches_tolerance", "corrections",
+                                          "max_rel_difference_vs_fp64_solution")}
+    if forms.get("batched"):
+        b = forms["batched"]
+        compact_forms["batched"] = {**_pick(b, "value", "models_per_s", "models", "max_backward_error_host"),
+                                    "mixed_s": (b.get("mixed") or {}).get("s"),
+                                    "cpu_baseline": (b.get("cpu_baseline") or {}).get("value")}
+    if forms.get("learned_start"):
+        compact_forms["learned_start"] = _pick(forms["learned_start"], "lanczos_speedup", "median_lanczos_speedup",
+                                               "ceiling_lanczos_speedup", "same_verification", "same_sturm_points",
+                                               "max_eigenvalue_rel_difference")
+    line["forms"] = compact_forms
+    return _round(line)
+
+
+def emit(full, detail_path):
+    """Write the whole record (to `detail_path`, else as one line on stderr) and print the compact line last."""
+    if detail_path:
+        with open(detail_path, "w") as out:
+            json.dump(full, out, indent=1)
+    else:
+        print(json.dumps(full), file=sys.stderr, flush=True)
+    print(json.dumps(compact_line(full)), flush=True)
 
 
 def factor_only(args):

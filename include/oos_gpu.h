@@ -149,8 +149,11 @@ double oosgpu_last_solve_seconds(oosgpu_factor* factor);
  * callers that cannot call cudaMalloc once running (a fixed device-memory budget handed over at set-up, allocations
  * forbidden afterwards). Its scratch is a fixed 16 MiB device array in the library (2^21 doubles, held on every GPU
  * that loads the library until exit); a factor needing more than that for one right-hand side (equations plus update
- * rows) is refused with OOSGPU_INVALID_ARGUMENT. The first call on a device looks the array's address up (make it
- * before any stream capture). All calls share the array: calls that overlap on the GPU race. */
+ * rows) is refused with OOSGPU_INVALID_ARGUMENT. The first call on a device looks the array's address up; under
+ * CUDA's lazy module loading that first call is also when the array and the solve's kernels are loaded onto the
+ * device, which takes device memory. So make the first call during set-up, before any stream capture: a call with
+ * columns = 0 is enough. Later calls take no device memory. All calls share the array: calls that overlap on the GPU
+ * race. The looked-up address, like every handle of this library, does not survive a cudaDeviceReset. */
 int oosgpu_solve_device_noalloc(oosgpu_factor* factor, double* b, int64_t ld, int64_t columns);
 
 /* FP64 iterative refinement around the solve (the fixed-precision refinement of LAPACK xPORFS that the reference

@@ -10,7 +10,11 @@
 // library holds that array until the process exits. In host code `g_noallocScratch` is only a host-side stand-in for
 // the array, not a device address: it is never passed to a kernel. Its device address is taken once per device with
 // cudaGetSymbolAddress, with that device current, on the first call of the entry point on that device; that first
-// call therefore does this set-up, and should come before any stream capture.
+// call therefore does this set-up, and should come before any stream capture. Under CUDA's lazy module loading (the
+// default), that lookup is also when this file's module, and with it the array, is loaded onto the device, and the
+// first solve loads the solve kernels: the first call takes device memory, later calls take none. A call with zero
+// columns does the set-up alone. The cached address belongs to the device's primary context: like every factor
+// handle, it does not survive a cudaDeviceReset.
 //
 // Sharing: every call on a device uses the same array and leaves its contents behind; the solve writes every scratch
 // value before it reads it (the column tile's rows are copied in; each supernode's update rows are written whole by

@@ -47,3 +47,13 @@ def relative_columns(a, b):
         a = a[:, None]
         b = b[:, None]
     return np.linalg.norm(a - b, axis=0) / np.maximum(np.linalg.norm(b, axis=0), 1e-300)
+
+
+def solution_bound(spread):
+    """The bound on the relative difference between a GPU solution and the reference's: where the reference's own
+    two kernel families agree to 1e-11 or better (well-conditioned matrices), the smaller of 1e-9 (the displacement
+    tolerance of the path) and 100 x that spread + 1e-12; on the thin plates, whose conditioning makes two correct FP64
+    solves differ by 1e-8 or more, 100 x the spread."""
+    if spread <= 1e-11:
+        return min(1e-9, 100.0 * spread + 1e-12)
+    return 100.0 * spread

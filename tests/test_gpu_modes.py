@@ -178,7 +178,7 @@ def test_refusals(lib, oracle_mod, gpu):
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
-@pytest.mark.parametrize("name", ["hex8", "hex14", "plate20", "hex30"])
+@pytest.mark.parametrize("name", ["hex8", "hex14", "plate20", "hex30", "hex60"])
 def test_modes_match_golden(name, lib, gpu):
     """Against the reference's own solve recorded in tests/golden/modes (no reference library needed): the symbolic
     structure from the reference's ordering, the eigenvalues within 1e-9, the same Sturm count at every shift the
