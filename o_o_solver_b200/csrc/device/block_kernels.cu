@@ -231,6 +231,37 @@ __global__ void combineRows(const double* a, std::int64_t lda, int m, const doub
     }
 }
 
+// Column c of a block after its Gram-Schmidt passes, decided on the device: its M-norm sqrt(max(0, *dot)) against the
+// dependence threshold factor * reference, where reference is the M-norm the block's column c had before its
+// projections (perColumn: sqrt(max(0, gram(c, c)))) or the largest such norm of the block and floorNorm (otherwise;
+// gram width x width, leading dimension width). Above it, x and its M-image mx are scaled to unit M-norm and the norm
+// is written to *diagonal; at or below it (or not a number), the column is left as it is, *diagonal is 0 and
+// *accepted 0: the host redoes that block along the path with random replacements. Every thread forms the same
+// scalars from the same values, so the whole grid agrees.
+__global__ void acceptColumn(double* x, double* mx, int rows, const double* dot, const double* gram, int width, int c,
+                             int perColumn, double floorNorm, double factor, double* diagonal, double* accepted)
+{
+    double reference = floorNorm;
+    if (perColumn != 0)
+        reference = sqrt(fmax(0.0, gram[c + c * width]));
+    else
+        for (int j = 0; j < width; ++j)
+            reference = fmax(reference, sqrt(fmax(0.0, gram[j + j * width])));
+    const double norm = sqrt(fmax(0.0, *dot));
+    const bool keep = norm > factor * reference;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0)
+    {
+        *diagonal = keep ? norm : 0.0;
+        *accepted = keep ? 1.0 : 0.0;
+    }
+    if (!keep || i >= rows)
+        return;
+    const double inverse = 1.0 / norm;
+    x[i] *= inverse;
+    mx[i] *= inverse;
+}
+
 // x <- s x, and y <- s y when y is given (one column).
 __global__ void scaleColumn(double* x, double* y, double s, int rows)
 {

@@ -70,6 +70,7 @@ constexpr std::size_t smallFrontSmem(int order)
 }
 constexpr int DIAGONAL_THREADS = 256;
 __global__ void diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0);
+__global__ void diagonalBlocksByColumn(FactorArgs args, const std::int32_t* list, int k0);
 __global__ void panelRowsInverse(FactorArgs args, const TileTask* tasks, int k0);
 constexpr std::size_t PANEL_ROWS_INVERSE_SMEM = (2 * 64 * (TILE + TILE_PAD) + 64) * sizeof(double);
 __global__ void panelUpdate(FactorArgs args, const TileTask* tasks, int k0);
@@ -182,6 +183,8 @@ __global__ void combineRows(const double* a, std::int64_t lda, int m, const doub
                             double* out, std::int64_t ldo, int rows, const double* next, std::int64_t ldn, int b,
                             const double* correction);
 __global__ void scaleColumn(double* x, double* y, double s, int rows);
+__global__ void acceptColumn(double* x, double* mx, int rows, const double* dot, const double* gram, int width, int c,
+                             int perColumn, double floorNorm, double factor, double* diagonal, double* accepted);
 __global__ void scaleColumns(double* x, std::int64_t ldx, double* y, std::int64_t ldy, const double* s, int rows,
                              int columns);
 

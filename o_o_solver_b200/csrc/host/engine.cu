@@ -8,7 +8,7 @@
 #include "../device/kernels.cuh"
 #include "factor_internal.hpp"
 #include "host_api.hpp"
-#include "lanczos.hpp"
+#include "spectrum.hpp"
 #include "plan.hpp"
 
 #include "oos_gpu.h"
@@ -1753,8 +1753,8 @@ private:
     DeviceArray<double> m_shifted;
 };
 
-// The GPU pencil behind the Lanczos driver's ShiftedPencil interface.
-class PencilOperations final : public eigen::ShiftedPencil
+// The GPU pencil behind the eigen solver's PencilPort interface.
+class PencilOperations final : public eigen::PencilPort
 {
 public:
     explicit PencilOperations(GpuPencil& pencil) : m_pencil(pencil) {}
@@ -1789,7 +1789,7 @@ struct oosgpu_pencil
 
 struct oosgpu_modes
 {
-    oosgpu::eigen::EigenSolution solution;
+    oosgpu::eigen::ModeResult solution;
 };
 
 struct oosgpu_model
@@ -2335,12 +2335,12 @@ extern "C" void oosgpu_lanczos_defaults(oosgpu_lanczos_options* options)
 {
     if (options == nullptr)
         return;
-    const oosgpu::eigen::LanczosOptions defaults;
-    options->block_size = static_cast<int64_t>(defaults.blockSize);
+    const oosgpu::eigen::KrylovSettings defaults;
+    options->block_size = static_cast<int64_t>(defaults.block);
     options->modes_per_shift = static_cast<int64_t>(defaults.modesPerShift);
-    options->convergence_tolerance = defaults.convergenceTolerance;
-    options->maximum_shifts = static_cast<int64_t>(defaults.maximumShifts);
-    options->maximum_restarts = static_cast<int64_t>(defaults.maximumRestarts);
+    options->convergence_tolerance = defaults.tolerance;
+    options->maximum_shifts = static_cast<int64_t>(defaults.shiftLimit);
+    options->maximum_restarts = static_cast<int64_t>(defaults.restartLimit);
     options->seed = defaults.seed;
 }
 
@@ -2359,11 +2359,11 @@ int modesSolve(oosgpu_pencil* pencil, const oosgpu_eigen_request* request, const
             *out = nullptr;
             if (request->mode_count < 0)
                 throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT, "eigenvalue request: a negative mode count");
-            oosgpu::eigen::EigenRequest eigenRequest;
-            eigenRequest.lowerBound = request->lower_bound;
-            eigenRequest.upperBound = request->upper_bound;
-            eigenRequest.modeCount = static_cast<std::size_t>(request->mode_count);
-            oosgpu::eigen::LanczosOptions lanczos;
+            oosgpu::eigen::ModeRequest eigenRequest;
+            eigenRequest.low = request->lower_bound;
+            eigenRequest.high = request->upper_bound;
+            eigenRequest.count = static_cast<std::size_t>(request->mode_count);
+            oosgpu::eigen::KrylovSettings lanczos;
             if (options != nullptr)
             {
                 const auto count = [](int64_t value, const char* what)
@@ -2373,20 +2373,20 @@ int modesSolve(oosgpu_pencil* pencil, const oosgpu_eigen_request* request, const
                                             std::string("BlockLanczos: a negative ") + what);
                     return static_cast<std::size_t>(value);
                 };
-                lanczos.blockSize = count(options->block_size, "block size");
+                lanczos.block = count(options->block_size, "block size");
                 lanczos.modesPerShift = count(options->modes_per_shift, "count of modes per shift");
-                lanczos.convergenceTolerance = options->convergence_tolerance;
-                lanczos.maximumShifts = count(options->maximum_shifts, "shift limit");
-                lanczos.maximumRestarts = count(options->maximum_restarts, "restart limit");
+                lanczos.tolerance = options->convergence_tolerance;
+                lanczos.shiftLimit = count(options->maximum_shifts, "shift limit");
+                lanczos.restartLimit = count(options->maximum_restarts, "restart limit");
                 lanczos.seed = options->seed;
             }
             if (start != nullptr)
             {
                 const int64_t n = pencil->pencil->factor().plan().dimension;
-                if (columns != static_cast<int64_t>(lanczos.blockSize) || ld < n)
+                if (columns != static_cast<int64_t>(lanczos.block) || ld < n)
                     throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT,
                                         "learned start: expected a start block of " + std::to_string(n) + " rows (ld >= "
-                                        "rows) and the block size's " + std::to_string(lanczos.blockSize) +
+                                        "rows) and the block size's " + std::to_string(lanczos.block) +
                                         " columns, found " + std::to_string(columns) + " columns, ld " +
                                         std::to_string(ld));
             }
@@ -2424,11 +2424,11 @@ extern "C" int oosgpu_modes_summary(const oosgpu_modes* modes, int64_t counts[6]
             const auto& s = modes->solution;
             if (counts != nullptr)
             {
-                counts[0] = static_cast<int64_t>(s.eigenvalues.size());
-                counts[1] = static_cast<int64_t>(s.factorisationCount);
+                counts[0] = static_cast<int64_t>(s.values.size());
+                counts[1] = static_cast<int64_t>(s.factorisations);
                 counts[2] = static_cast<int64_t>(s.shifts.size());
-                counts[3] = static_cast<int64_t>(s.verifiedCount);
-                counts[4] = s.isComplete ? 1 : 0;
+                counts[3] = static_cast<int64_t>(s.confirmed);
+                counts[4] = s.complete ? 1 : 0;
                 counts[5] = static_cast<int64_t>(s.blockSteps);
             }
             if (seconds != nullptr)
@@ -2451,7 +2451,7 @@ extern "C" int oosgpu_modes_values(const oosgpu_modes* modes, double* eigenvalue
             requirePointer(modes, "modes");
             const auto& s = modes->solution;
             if (eigenvalues != nullptr)
-                std::copy(s.eigenvalues.begin(), s.eigenvalues.end(), eigenvalues);
+                std::copy(s.values.begin(), s.values.end(), eigenvalues);
             if (residual_bounds != nullptr)
                 std::copy(s.residualBounds.begin(), s.residualBounds.end(), residual_bounds);
         });
@@ -2467,11 +2467,11 @@ extern "C" int oosgpu_modes_vectors(const oosgpu_modes* modes, double* vectors, 
             const auto& s = modes->solution;
             if (ld < s.dimension)
                 throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT, "modes: the leading dimension is below the rows");
-            if (s.eigenvalues.empty() || s.dimension == 0)
+            if (s.values.empty() || s.dimension == 0)
                 return;
-            oosgpu::check(cudaMemcpy2D(vectors, static_cast<std::size_t>(ld) * sizeof(double), s.eigenvectors.get(),
+            oosgpu::check(cudaMemcpy2D(vectors, static_cast<std::size_t>(ld) * sizeof(double), s.vectors.get(),
                                        static_cast<std::size_t>(s.dimension) * sizeof(double),
-                                       static_cast<std::size_t>(s.dimension) * sizeof(double), s.eigenvalues.size(),
+                                       static_cast<std::size_t>(s.dimension) * sizeof(double), s.values.size(),
                                        cudaMemcpyDeviceToHost),
                           "download eigenvectors");
         });
@@ -2479,7 +2479,7 @@ extern "C" int oosgpu_modes_vectors(const oosgpu_modes* modes, double* vectors, 
 
 extern "C" const double* oosgpu_modes_vectors_device(const oosgpu_modes* modes)
 {
-    return modes == nullptr ? nullptr : modes->solution.eigenvectors.get();
+    return modes == nullptr ? nullptr : modes->solution.vectors.get();
 }
 
 extern "C" int oosgpu_modes_shifts(const oosgpu_modes* modes, double* records)
@@ -2494,12 +2494,12 @@ extern "C" int oosgpu_modes_shifts(const oosgpu_modes* modes, double* records)
             {
                 double* out = records + 7 * k++;
                 out[0] = record.shift;
-                out[1] = static_cast<double>(static_cast<int>(record.purpose));
-                out[2] = static_cast<double>(record.sturmCount);
-                out[3] = record.hasLanczosRun ? 1.0 : 0.0;
+                out[1] = static_cast<double>(static_cast<int>(record.role));
+                out[2] = static_cast<double>(record.countBelow);
+                out[3] = record.ran ? 1.0 : 0.0;
                 out[4] = static_cast<double>(record.blockSteps);
                 out[5] = static_cast<double>(record.restarts);
-                out[6] = static_cast<double>(record.convergedCount);
+                out[6] = static_cast<double>(record.converged);
             }
         });
 }
@@ -2512,15 +2512,15 @@ extern "C" void oosgpu_modes_destroy(oosgpu_modes* modes)
 namespace
 {
 
-oosgpu::eigen::SturmVerification verificationFrom(const double v[6])
+oosgpu::eigen::Confirmation confirmationFrom(const double v[6])
 {
-    oosgpu::eigen::SturmVerification verification;
-    verification.verifiedUpTo = v[0];
-    verification.verifiedCount = static_cast<std::size_t>(v[1]);
-    verification.hasMismatch = v[2] != 0.0;
-    verification.mismatch.lower = v[3];
-    verification.mismatch.upper = v[4];
-    return verification;
+    oosgpu::eigen::Confirmation confirmation;
+    confirmation.reach = v[0];
+    confirmation.confirmed = static_cast<std::size_t>(v[1]);
+    confirmation.hasGap = v[2] != 0.0;
+    confirmation.gapLow = v[3];
+    confirmation.gapHigh = v[4];
+    return confirmation;
 }
 
 std::span<const double> valuesOf(const double* values, int64_t count, const char* name)
@@ -2567,21 +2567,20 @@ extern "C" int oosgpu_sturm_verify(int64_t points, const double* shifts, const i
             const std::span<const double> shiftSpan = valuesOf(shifts, points, "shifts");
             if (points > 0)
                 requirePointer(counts, "counts");
-            oosgpu::eigen::SturmCheck sturm;
+            oosgpu::eigen::CountLedger ledger;
             for (std::size_t k = 0; k < shiftSpan.size(); ++k)
             {
                 if (counts[k] < 0)
                     throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT, "Sturm point: a negative count");
-                sturm.addPoint({shiftSpan[k], static_cast<std::size_t>(counts[k])});
+                ledger.record(shiftSpan[k], static_cast<std::size_t>(counts[k]));
             }
-            const oosgpu::eigen::SturmVerification v = sturm.verify(valuesOf(sorted, values, "sorted"));
-            result[0] = v.verifiedUpTo;
-            result[1] = static_cast<double>(v.verifiedCount);
-            result[2] = v.hasMismatch ? 1.0 : 0.0;
-            result[3] = v.mismatch.lower;
-            result[4] = v.mismatch.upper;
-            result[5] = static_cast<double>(v.mismatch.expectedCount) * 1e6 +
-                        static_cast<double>(v.mismatch.foundCount);
+            const oosgpu::eigen::Confirmation c = ledger.confirm(valuesOf(sorted, values, "sorted"));
+            result[0] = c.reach;
+            result[1] = static_cast<double>(c.confirmed);
+            result[2] = c.hasGap ? 1.0 : 0.0;
+            result[3] = c.gapLow;
+            result[4] = c.gapHigh;
+            result[5] = static_cast<double>(c.proven) * 1e6 + static_cast<double>(c.found);
         });
 }
 
@@ -2598,15 +2597,15 @@ extern "C" int oosgpu_shift_next(double lower, double upper, int64_t mode_count,
             requirePointer(purpose, "purpose");
             if (mode_count < 0)
                 throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT, "eigenvalue request: a negative mode count");
-            oosgpu::eigen::EigenRequest request;
-            request.lowerBound = lower;
-            request.upperBound = upper;
-            request.modeCount = static_cast<std::size_t>(mode_count);
-            const oosgpu::eigen::ShiftStrategy strategy(request, scale);
-            const oosgpu::eigen::ShiftChoice choice = strategy.nextShift(
-                verificationFrom(verification), valuesOf(sorted, values, "sorted"), valuesOf(ritz, ritz_count, "ritz"),
+            oosgpu::eigen::ModeRequest request;
+            request.low = lower;
+            request.high = upper;
+            request.count = static_cast<std::size_t>(mode_count);
+            const oosgpu::eigen::ShiftPlanner planner(request, scale);
+            const oosgpu::eigen::ShiftPick pick = planner.next(
+                confirmationFrom(verification), valuesOf(sorted, values, "sorted"), valuesOf(ritz, ritz_count, "ritz"),
                 valuesOf(lanczos_shifts, shift_count, "lanczos shifts"));
-            *shift = choice.shift;
-            *purpose = static_cast<int32_t>(choice.purpose);
+            *shift = pick.shift;
+            *purpose = static_cast<int32_t>(pick.role);
         });
 }

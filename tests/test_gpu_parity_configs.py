@@ -6,9 +6,10 @@
   factorisation and solve.
 
 Tolerances, stated per check:
-- inertia, pivot diagnostics: exact;
-- panels: within 1e-10 of the reference panel's largest magnitude (the top fronts of the plate, every supernode of the
-  panels);
+- inertia, the count of ratio-test issues and the equation of the largest ratio: exact;
+- panels: within 1e-10 of the reference panel's largest magnitude (every supernode of the panels); on the 2 M plate,
+  whose top pivots are small against their diagonals (largest ratio about 3e5), within 100 x the distance between the
+  reference's own two kernel families (scalar and SIMD) where that is larger, and so for the largest ratio (1e-8);
 - backward error ||b - Ax||_inf / (||A||_inf ||x||_inf + ||b||_inf) of the GPU solution: at most 1e-15;
 - solutions: relative 2-norm difference per column at most min(1e-9, 100 x spread) where the reference's own two
   kernel families agree to 1e-11 or better (spread = their difference). On the thin plates they do not: the 2 mm
@@ -63,42 +64,52 @@ def test_plate580_statics_matches_reference(lib, oracle_mod, gpu):
     symbolic = SymbolicFactor.from_arrays(sym.dof_count, sym.first_column, sym.parent, sym.row_start, sym.rows)
     assert symbolic.flop_count == pytest.approx(sym.flops, rel=1e-12)
 
-    ref = oracle_mod.factorise(sym, csc.offsets, csc.rows, csc.values, threads=THREADS)
-    x_ref = ref.solve(b, threads=THREADS)
-    # the largest fronts: the top of the tree, where the factorisation's long chains run
+    # the reference twice: its automatic (SIMD) kernel family, the comparison, and its scalar family, whose
+    # distance from the first measures what two correct FP64 factorisations of this matrix can differ by
     sizes = np.diff(sym.first_column) * (np.diff(sym.first_column) + np.diff(sym.row_start))
-    top = np.argsort(sizes)[-16:]
-    ref_panels = {int(s): ref.panel(int(s)) for s in top}
-    ref_inertia = (ref.positive, ref.negative, ref.zero)
-    ref_diagnostics = (ref.issue_count, ref.equation_of_largest, ref.largest_ratio)
-    ref.close()
+    top = [int(s) for s in np.argsort(sizes)[-16:]]  # the largest fronts: the top of the tree
+    runs = []
+    for family in (-1, 0):
+        ref = oracle_mod.factorise(sym, csc.offsets, csc.rows, csc.values, family=family, threads=THREADS)
+        runs.append({"x": ref.solve(b, threads=THREADS), "panels": {s: ref.panel(s) for s in top},
+                     "inertia": (ref.positive, ref.negative, ref.zero),
+                     "diagnostics": (ref.issue_count, ref.equation_of_largest, ref.largest_ratio)})
+        ref.close()
+    ref, scalar = runs
+    assert ref["inertia"] == scalar["inertia"]
+
+    def panel_distance(panels):
+        worst = 0.0
+        for s, (theirs, ref_rows, _) in ref["panels"].items():
+            mine, rows, _ = panels(s)
+            assert np.array_equal(rows, ref_rows)
+            worst = max(worst, np.abs(mine - theirs).max() / max(np.abs(theirs).max(), 1e-300))
+        return worst
+
+    panel_spread = panel_distance(lambda s: scalar["panels"][s])
+    ratio_spread = abs(scalar["diagnostics"][2] - ref["diagnostics"][2]) / ref["diagnostics"][2]
+    solution_spread = relative_columns(scalar["x"], ref["x"]).max()
 
     d_csc = SymmetricCsc(torch.from_numpy(csc.offsets).cuda(), torch.from_numpy(csc.rows).cuda(),
                          torch.from_numpy(csc.values).cuda())
     factor = SupernodalFactor.factorise(symbolic, d_csc)
-    assert (factor.inertia.positive, factor.inertia.negative, factor.inertia.zero) == ref_inertia
-    assert factor.pivot_diagnostics.issue_count == ref_diagnostics[0]
-    assert factor.pivot_diagnostics.equation_of_largest_ratio == ref_diagnostics[1]
-    assert factor.pivot_diagnostics.largest_ratio == pytest.approx(ref_diagnostics[2], rel=1e-8)
-    worst_panel = 0.0
-    for s, (theirs, ref_rows, _) in ref_panels.items():
-        mine, rows, _ = factor.panel(s)
-        assert np.array_equal(rows, ref_rows)
-        worst_panel = max(worst_panel, np.abs(mine - theirs).max() / max(np.abs(theirs).max(), 1e-300))
-    assert worst_panel <= 1e-10, worst_panel
-
+    assert (factor.inertia.positive, factor.inertia.negative, factor.inertia.zero) == ref["inertia"]
+    assert factor.pivot_diagnostics.issue_count == ref["diagnostics"][0]
+    assert factor.pivot_diagnostics.equation_of_largest_ratio == ref["diagnostics"][1]
+    ratio = abs(factor.pivot_diagnostics.largest_ratio - ref["diagnostics"][2]) / ref["diagnostics"][2]
+    worst_panel = panel_distance(lambda s: factor.panel(s))
     x = np.asfortranarray(b.copy())
     FactorSolve(factor).solve(x)
     factor.close()
     eta = backward_error(csc, x, b).max()
-    difference = relative_columns(x, x_ref).max()
-    # the reference's own spread on this matrix: its scalar kernel family against its automatic (SIMD) one
-    scalar = oracle_mod.factorise(sym, csc.offsets, csc.rows, csc.values, family=0, threads=THREADS)
-    spread = relative_columns(scalar.solve(b, threads=THREADS), x_ref).max()
-    print(f"plate580: panels {worst_panel:.2e}, backward error {eta:.2e}, solution difference {difference:.2e} "
-          f"(reference families differ by {spread:.2e})")
+    difference = relative_columns(x, ref["x"]).max()
+    print(f"plate580 against the reference (its own two kernel families in brackets): top panels {worst_panel:.2e} "
+          f"({panel_spread:.2e}), largest pivot ratio {ratio:.2e} ({ratio_spread:.2e}), solutions {difference:.2e} "
+          f"({solution_spread:.2e}), GPU backward error {eta:.2e}")
+    assert worst_panel <= max(1e-10, 100.0 * panel_spread), (worst_panel, panel_spread)
+    assert ratio <= max(1e-8, 100.0 * ratio_spread), (ratio, ratio_spread)
     assert eta <= 1e-15, eta
-    assert difference <= solution_bound(spread), (difference, spread)
+    assert difference <= solution_bound(solution_spread), (difference, solution_spread)
 
 
 PANEL_COUNT = 12
