@@ -77,6 +77,8 @@ def parse():
                         help="with --factor-only: also solve 64 load columns and write both launch lists (kind, "
                              "blocks, step column, device seconds) to PATH as JSON")
     parser.add_argument("--profile-rhs", type=int, default=64, help="with --launch-profile: the solve's columns")
+    parser.add_argument("--kernels", choices=["tune", "default", "alternative"], default="tune",
+                        help="with --factor-only: the kernel choice of the launch kinds with two kernels")
     parser.add_argument("--detail", metavar="PATH", default=None,
                         help="write the whole result record (kernel tables, every leg's detail) to PATH as JSON; "
                              "without it the record goes to stderr as one line")
@@ -420,8 +422,10 @@ def batched_leg(args, dev, torch, replicas=None):
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
 
-    def timed(options, krylov, max_steps):
-        factor = SupernodalFactor.factorise(joined.symbolic, d_csc, options)
+    def timed(options, krylov, max_steps, kernels="tune"):
+        factor = SupernodalFactor(joined.symbolic, device=dev.index or 0)
+        factor.set_tuning(kernels)
+        factor.refactorise(d_csc, options)
         info = None
         for _ in range(max(args.warmup, 1)):  # the first runs also capture the graphs
             factor.refactorise(d_csc, options)
@@ -439,10 +443,11 @@ def batched_leg(args, dev, torch, replicas=None):
             times.append(start.elapsed_time(stop) / 1e3)
         result = {"s": statistics.median(times), "factor_device_s": factor.device_seconds,
                   "refinement_steps": info.steps, "backward_error": info.backward_error,
-                  "inertia_negative": factor.inertia.negative}
+                  "inertia_negative": factor.inertia.negative, "kernels": kernels, "tuning": factor.tuning()}
         factor.close()
         return result
 
+    fixed = timed(FactorOptions(), 0, 10, kernels="default")
     fp64 = timed(FactorOptions(), 0, 10)
     mixed = timed(FactorOptions(precision="mixed"), 8, 3)
     if replicas is not None:
@@ -464,6 +469,7 @@ def batched_leg(args, dev, torch, replicas=None):
         "value": seconds, "unit": "s", "models_per_s": len(all_cases) / seconds,
         "form": "FP64 factorisation and solve (CUDA graphs), backward error checked at 1e-10",
         "fp64": fp64,
+        "fp64_fixed_kernels": fixed,
         "mixed": dict(mixed, form="3xTF32 update matrices (tcgen05) + FP64 GMRES-IR (8 Krylov vectors, at most 3 "
                                   "corrections) to backward error 1e-10"),
         "max_backward_error_host": worst, "host_build_s": build_seconds,
@@ -678,8 +684,9 @@ def run_gpu(args, rank, world, local_rank):
         refinement["factor_seconds"] = factor.device_seconds
 
     for _ in range(args.warmup):
-        step()
+        step()  # the first also runs the autotuner's timing factorisations
     torch.cuda.synchronize()
+    tuning = factor.tuning()
     replicas.barrier()
     torch.cuda.synchronize()
     start = torch.cuda.Event(enable_timing=True)
@@ -780,6 +787,7 @@ def run_gpu(args, rank, world, local_rank):
             "residual": resid, "backward_error": backward, "refinement": refinement, "e2e": e2e,
             "gpu_launches": launches, "roofline": roofline, "kernels": kernel_table, "clocks": clocks.summary(),
             "cpu_baseline": baseline, "factor_tflops": symbolic.flop_count / refinement["factor_seconds"] / 1e12,
+            "tuning": tuning,
             "modes": modes, "forms": {"mixed": mixed, "batched": batched, "learned_start": learned},
         }
         emit(line, args.detail)
@@ -830,6 +838,7 @@ def compact_line(full):
     if forms.get("batched"):
         b = forms["batched"]
         compact_forms["batched"] = {**_pick(b, "value", "models_per_s", "models", "max_backward_error_host"),
+                                    "fixed_kernels_s": (b.get("fp64_fixed_kernels") or {}).get("s"),
                                     "mixed_s": (b.get("mixed") or {}).get("s"),
                                     "cpu_baseline": (b.get("cpu_baseline") or {}).get("value")}
     if forms.get("learned_start"):
@@ -868,7 +877,9 @@ def factor_only(args):
     options = FactorOptions(precision=precision or "fp64", pivoting=pivoting or "positive_definite")
     stiffness = model.csc(order, 0)
     torch.cuda.init()
-    factor = SupernodalFactor.factorise(symbolic, stiffness, options)
+    factor = SupernodalFactor(symbolic)
+    factor.set_tuning(args.kernels)
+    factor.refactorise(stiffness, options)
     for _ in range(max(args.warmup - 1, 0)):
         factor.refactorise(stiffness, options)
     factor.profile(True)
@@ -886,7 +897,8 @@ def factor_only(args):
         with open(args.launch_profile, "w") as out:
             json.dump({"factor": factor.launch_profile("factor"), "solve": factor.launch_profile("solve")}, out)
     print(json.dumps({"factor_only": name, "precision": options.precision, "equations": int(symbolic.dof_count),
-                      "wall_seconds_per_factor": seconds, "kernels": factor.kernel_stats()}), flush=True)
+                      "kernel_choice": args.kernels, "wall_seconds_per_factor": seconds,
+                      "kernels": factor.kernel_stats(), "tuning": factor.tuning()}), flush=True)
     factor.close()
 
 

@@ -207,6 +207,22 @@ int oosgpu_factor_kernel_stats(oosgpu_factor* factor, int32_t kinds, double* sec
  * launches. */
 int oosgpu_factor_launch_counts(oosgpu_factor* factor, int64_t columns, int64_t counts[2]);
 
+/* ---- kernel choice (no counterpart in the reference: its kernel family is chosen per process, by the CPU's
+ *      instruction set, include/oos/linalg/dense/KernelSelection.hpp) ------------------------------------------- */
+/* The kernel choice of the launch kinds that have two kernels (the diagonal blocks by 16-column sub-panels or column
+ * by column; the extend-add element-wise or staged in shared memory; the update matrix by 64 x 64 tiles or by
+ * TMA-fed 128 x 128 tiles). mode 1 (the default): the autotuner, which on the next positive definite FP64
+ * factorisation of the handle runs the factorisation twice with each kernel, every launch timed (its shorter time
+ * kept), and lets each size
+ * class of launch (1, <= 8, <= 148, <= 592, more blocks) keep the faster one. mode 0: the first kernel of each pair;
+ * mode 2: the second everywhere. Any call forgets an earlier choice. */
+int oosgpu_factor_set_tuning(oosgpu_factor* factor, int32_t mode);
+/* The autotuner's choices: per (launch kind, size class), the launches, the seconds of kernel 0 and kernel 1 in the
+ * timing factorisations, and the kernel chosen. At most `capacity` records; *total is how many there are (0 before the
+ * tuning factorisation). */
+int oosgpu_factor_tuning_report(oosgpu_factor* factor, int64_t capacity, int32_t* kinds, int32_t* size_classes,
+                                int32_t* launches, double* seconds0, double* seconds1, int32_t* chosen, int64_t* total);
+
 /* ---- shifted pencil: the ShiftedPencil plug-in (include/oos/linalg/eigen/ShiftedPencil.hpp:55-88) as SparsePencil
  *      implements it (include/oos/linalg/eigen/SparsePencil.hpp:29-85) -------------------------------------------- */
 typedef struct oosgpu_pencil oosgpu_pencil;
@@ -355,6 +371,14 @@ int oosgpu_model_csc_terms(const oosgpu_model* model, const int32_t* node_at_pos
 /* which: 0 stiffness, 1 lumped mass on the stiffness pattern. */
 int oosgpu_model_csc(const oosgpu_model* model, const int32_t* node_at_position, int32_t which, int64_t* col_offsets,
                      int32_t* rows, double* values);
+/* The same columns written by the GPU `device` into device arrays (col_offsets: dimension + 1, rows and values:
+ * oosgpu_model_csc_terms), from the model's element list: the element matrices, the node blocks and the columns are
+ * formed on the device, with the host's arithmetic in the host's order (the same values bit for bit). The role of the
+ * reference's StiffnessAssembler and SymmetricCsc::fromBlocks (include/oos/assembly/assemble/StiffnessAssembler.hpp:
+ * 21-33, src/linalg/sparse/SymmetricCsc.cpp:41) for this project's workload models. which 1 (lumped mass) copies the
+ * host's mass. */
+int oosgpu_model_csc_device(const oosgpu_model* model, const int32_t* node_at_position, int32_t which, int32_t device,
+                            int64_t* col_offsets, int32_t* rows, double* values);
 /* Column 0 the pressure load; columns j >= 1: `points` seeded nodes (splitmix64, seed_base + j) with N(0, sigma)
  * forces on their out-of-plane translation. rhs column-major, leading dimension ld. */
 int oosgpu_model_loads(const oosgpu_model* model, const int32_t* node_at_position, int64_t columns,

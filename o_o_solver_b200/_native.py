@@ -87,6 +87,9 @@ SIGNATURES = [
     ("oosgpu_factor_launch_profile", ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _i32p,
                                                     _f64p, _i64p]),
     ("oosgpu_factor_kernel_stats", ctypes.c_int, [_vp, ctypes.c_int32, _f64p, _i64p, _f64p, _f64p]),
+    ("oosgpu_factor_set_tuning", ctypes.c_int, [_vp, ctypes.c_int32]),
+    ("oosgpu_factor_tuning_report", ctypes.c_int, [_vp, ctypes.c_int64, _i32p, _i32p, _i32p, _f64p, _f64p, _i32p,
+                                                    ctypes.POINTER(ctypes.c_int64)]),
     ("oosgpu_factor_launch_counts", ctypes.c_int, [_vp, ctypes.c_int64, _i64p]),
     ("oosgpu_pencil_create", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int32, _i64p, _i32p, _f64p, _f64p,
                                             ctypes.POINTER(_vp)]),
@@ -138,6 +141,7 @@ SIGNATURES = [
     ("oosgpu_model_graph", ctypes.c_int, [_vp, _i64p, _i32p, _f64p]),
     ("oosgpu_model_csc_terms", ctypes.c_int, [_vp, _i32p, _i64p]),
     ("oosgpu_model_csc", ctypes.c_int, [_vp, _i32p, ctypes.c_int32, _i64p, _i32p, _f64p]),
+    ("oosgpu_model_csc_device", ctypes.c_int, [_vp, _i32p, ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp]),
     ("oosgpu_model_loads", ctypes.c_int, [_vp, _i32p, ctypes.c_int64, ctypes.c_uint64, ctypes.c_int32,
                                           ctypes.c_double, _f64p, ctypes.c_int64]),
 ]

@@ -2,6 +2,7 @@
 // tile product (mma.sync m8n8k4 .f64, the FP64 MMA path of sm_100a) and small helpers.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -57,6 +58,20 @@ constexpr int SOLVE_STEP = 256;
 // The columns of a macro panel of the factorisation: the 64-column steps inside it update its own later columns, and
 // once it is done it updates the rest of the front's panel in one product of K = PANEL_MACRO.
 constexpr int PANEL_MACRO = 256;
+// The staged extend-add (assembleStaged): a piece of a front is STAGE_COLUMNS columns by up to STAGE_ROWS front
+// positions, built in STAGE_SMEM bytes of shared memory (two blocks per SM).
+constexpr int STAGE_COLUMNS = 32;
+constexpr int STAGE_ROWS = 384;
+constexpr int STAGE_THREADS = 256;
+constexpr std::size_t STAGE_SMEM = static_cast<std::size_t>(STAGE_COLUMNS) * STAGE_ROWS * sizeof(double);
+// The TMA-fed update-matrix kernel (updateMatrixTma): 128 x 128 tiles, 16 warps, UPDATE_STAGES stages of UPDATE_SLICE
+// columns of K (A and B: 32 KB a stage), plus 1 KB to align the stages to the 128-byte swizzle's 1024-byte atoms.
+constexpr int UPDATE_TILE = 128;
+constexpr int UPDATE_THREADS = 512;
+constexpr int UPDATE_STAGES = 4;
+constexpr int UPDATE_SLICE = 16;
+constexpr std::size_t UPDATE_TMA_SMEM = static_cast<std::size_t>(UPDATE_STAGES) * 2 * UPDATE_TILE * UPDATE_SLICE *
+                                            sizeof(double) + 1024;
 // panelRowsInverse: the 64-row halves of one task (a task covers TILE * PANEL_ROW_HALVES rows below the block).
 constexpr int PANEL_ROW_HALVES = 1;
 // The rows of R(s) one block of the backward product x_F -= L21^T X[R(s)] takes; longer R(s) are split into chunks

@@ -323,7 +323,8 @@ constexpr int INVERSE_SUB = 16; // the blocks of the diagonal block's inverse
 //   inverse: X = L11^-1 by 16 x 16 blocks (the diagonal blocks by substitution, one thread per column, then the
 //   off-diagonal blocks by block diagonals: eight barrier phases in all), kept in the strict upper triangle
 //   (X(i, j) at (j, i)), where panelRowsInverse and the solves read it.
-__global__ void __launch_bounds__(DIAGONAL_THREADS) diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0)
+__global__ void __launch_bounds__(DIAGONAL_THREADS) diagonalBlocksByColumn(FactorArgs args, const std::int32_t* list,
+                                                                          int k0)
 {
     constexpr int LD = BLOCK + 1;
     constexpr int PARTS = DIAGONAL_THREADS / BLOCK;
@@ -466,6 +467,213 @@ __global__ void __launch_bounds__(DIAGONAL_THREADS) diagonalBlocks(FactorArgs ar
         __syncthreads();
     }
     // L and D (lower triangle) and L11^-1 (strict upper triangle) back into the panel
+    for (int e = t; e < BLOCK * BLOCK; e += DIAGONAL_THREADS)
+    {
+        const int j = e / BLOCK;
+        const int i = e - j * BLOCK;
+        if (i < kb && j < kb)
+            panel[i + static_cast<std::int64_t>(j) * n] = a[i + j * LD];
+    }
+}
+
+// The diagonal block's LDL^T by 16-column sub-panels, and the inverse of its unit lower factor (the same results as
+// diagonalBlocksByColumn, to rounding: the rows below each 16 x 16 block take their L as products with its inverse).
+// For each sub-panel J (columns j0 = 16 J ...):
+//   1. one warp eliminates the 16 x 16 diagonal block in registers (lane i holds row j0 + i): per column k the pivot
+//      d_k is shuffled from lane k, l_ik = a_ik / d_k, w_ik = l_ik d_k, and a_ij -= l_ik w_jk for k < j <= i, w_jk
+//      shuffled from lane j; then the same lanes invert the unit lower block, X_JJ = L_JJ^-1 (lane j: column j,
+//      X(i, j) = -sum_{j <= q < i} L(i, q) X(q, j)), into the block's strict upper triangle (X(i, j) at (j, i));
+//   2. the rows below the sub-panel: l_iq = (sum_{p <= q} a_ip X(q, p)) / d_q, and w_iq = l_iq d_q, each element alone;
+//   3. the trailing lower triangle: a_ij -= sum_q l_iq w_jq, q in increasing order (the reference's term order).
+// The 64 x 64 inverse then needs only its off-diagonal 16 x 16 blocks, by block diagonals as in diagonalBlocksByColumn.
+// Barriers: four per sub-panel and two per block diagonal, against one per column before; the chain of dependent
+// steps runs in one warp's registers.
+__global__ void __launch_bounds__(DIAGONAL_THREADS, 3) diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0)
+{
+    constexpr int LD = BLOCK + 1;
+    constexpr int SUB = INVERSE_SUB; // 16
+    __shared__ double a[BLOCK * LD];
+    __shared__ double wRows[BLOCK * SUB]; // w(i, q) = l_iq d_q of the current sub-panel, at wRows[i * SUB + q]
+    __shared__ double products[(BLOCK / SUB - 1) * SUB * SUB];
+    const std::int32_t s = list[blockIdx.x];
+    const FrontDesc f = args.fronts[s];
+    const int n = f.c + f.r;
+    const int kb = min(BLOCK, f.c - k0);
+    double* panel = args.panels + f.panel + static_cast<std::int64_t>(k0) * n + k0;
+    const int t = threadIdx.x;
+    const int lane = t & 31;
+    for (int e = t; e < BLOCK * BLOCK; e += DIAGONAL_THREADS)
+    {
+        const int j = e / BLOCK;
+        const int i = e - j * BLOCK;
+        const bool inside = i < kb && j < kb;
+        copyAsync8(a + i + j * LD, inside ? panel + i + static_cast<std::int64_t>(j) * n : panel, inside);
+    }
+    commitAsyncCopies();
+    waitAsyncCopies<0>();
+    __syncthreads();
+    // Beyond kb the block is the identity (its L rows are zero from the load), so the inverse stays finite.
+    if (t >= kb && t < BLOCK)
+        a[t + t * LD] = 1.0;
+    __syncthreads();
+
+#pragma unroll 1
+    for (int j0 = 0; j0 < kb; j0 += SUB)
+    {
+        const int width = min(SUB, kb - j0); // columns of this sub-panel
+        // 1. the 16 x 16 diagonal block and its inverse, warp 0
+        if (t < 32)
+        {
+            const int i = lane; // row j0 + i; lanes 16..31 take part in the shuffles only
+            const bool row = i < width;
+            double x[SUB];
+#pragma unroll
+            for (int q = 0; q < SUB; ++q)
+                x[q] = row && q <= i ? a[(j0 + i) + (j0 + q) * LD] : 0.0;
+#pragma unroll
+            for (int k = 0; k < SUB; ++k)
+            {
+                if (k < width)
+                {
+                    const double d = __shfl_sync(0xffffffffu, x[k], k);
+                    double l = 0.0;
+                    if (i == k && isBadPivot(d))
+                        atomicMin(args.zeroPivot + s, k0 + j0 + k);
+                    if (row && i > k)
+                    {
+                        l = x[k] / d;
+                        x[k] = l;
+                    }
+                    const double w = l * d; // w_ik, for the lanes below the pivot
+#pragma unroll
+                    for (int j = k + 1; j < SUB; ++j)
+                    {
+                        const double wj = __shfl_sync(0xffffffffu, w, j);
+                        if (row && j <= i)
+                            x[j] = fma(-l, wj, x[j]);
+                    }
+                }
+            }
+            if (row)
+            {
+#pragma unroll
+                for (int q = 0; q < SUB; ++q)
+                    if (q <= i)
+                        a[(j0 + i) + (j0 + q) * LD] = x[q];
+            }
+            __syncwarp();
+            // X = L_JJ^-1, lane j: column j (unit diagonal; rows and columns beyond width give the identity)
+            if (i < SUB)
+            {
+                double column[SUB];
+#pragma unroll
+                for (int r = 0; r < SUB; ++r)
+                {
+                    double sum = 0.0;
+#pragma unroll
+                    for (int q = 0; q < r; ++q)
+                        if (q >= i)
+                            sum += a[(j0 + r) + (j0 + q) * LD] * column[q];
+                    column[r] = r == i ? 1.0 : (r > i ? -sum : 0.0);
+                    if (r > i)
+                        a[(j0 + i) + (j0 + r) * LD] = column[r]; // X(r, i) at (i, r)
+                }
+            }
+        }
+        __syncthreads();
+        // 2. the rows below the sub-panel inside the block: l_iq and w_iq (results held until every thread has read)
+        const int below = kb - (j0 + SUB);
+        constexpr int PER_THREAD = (BLOCK - SUB) * SUB / DIAGONAL_THREADS; // 3
+        double lValue[PER_THREAD];
+#pragma unroll
+        for (int u = 0; u < PER_THREAD; ++u)
+        {
+            const int e = t + u * DIAGONAL_THREADS;
+            const int i = j0 + SUB + e / SUB;
+            const int q = e % SUB;
+            lValue[u] = 0.0;
+            if (below > 0 && e < below * SUB && q < width)
+            {
+                double sum = a[i + (j0 + q) * LD]; // X(q, q) = 1
+#pragma unroll 4
+                for (int p = 0; p < q; ++p)
+                    sum = fma(a[i + (j0 + p) * LD], a[(j0 + p) + (j0 + q) * LD], sum);
+                lValue[u] = sum / a[(j0 + q) + (j0 + q) * LD];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < PER_THREAD; ++u)
+        {
+            const int e = t + u * DIAGONAL_THREADS;
+            const int i = j0 + SUB + e / SUB;
+            const int q = e % SUB;
+            if (below > 0 && e < below * SUB && q < width)
+            {
+                a[i + (j0 + q) * LD] = lValue[u];
+                wRows[i * SUB + q] = lValue[u] * a[(j0 + q) + (j0 + q) * LD];
+            }
+        }
+        __syncthreads();
+        // 3. the trailing lower triangle of the block: a_ij -= sum_q l_iq w_jq
+        if (below > 0)
+        {
+            for (int e = t; e < below * below; e += DIAGONAL_THREADS)
+            {
+                const int jj = e / below;
+                const int ii = e - jj * below;
+                if (ii < jj)
+                    continue;
+                const int i = j0 + SUB + ii;
+                const int j = j0 + SUB + jj;
+                double value = a[i + j * LD];
+#pragma unroll
+                for (int q = 0; q < SUB; ++q)
+                    if (q < width)
+                        value = fma(-a[i + (j0 + q) * LD], wRows[j * SUB + q], value);
+                a[i + j * LD] = value;
+            }
+        }
+        __syncthreads();
+    }
+    // the inverse's off-diagonal 16 x 16 blocks by block diagonals, X_IJ = -X_II (sum_{J <= K < I} L_IK X_KJ)
+#pragma unroll 1
+    for (int d = 1; d < BLOCK / SUB; ++d)
+    {
+        const int count = (BLOCK / SUB - d) * SUB * SUB;
+        for (int e = t; e < count; e += DIAGONAL_THREADS) // T_IJ = sum_{J <= K < I} L_IK X_KJ
+        {
+            const int b = e / (SUB * SUB);
+            const int p = (e / SUB) % SUB;
+            const int q = e % SUB;
+            const int jBase = b * SUB;
+            const int iRow = (b + d) * SUB + p;
+            double sum = a[iRow + (jBase + q) * LD]; // X_JJ(q, q) = 1
+#pragma unroll 1
+            for (int r = q + 1; r < SUB; ++r)
+                sum += a[iRow + (jBase + r) * LD] * a[(jBase + q) + (jBase + r) * LD];
+#pragma unroll 1
+            for (int kBase = jBase + SUB; kBase < (b + d) * SUB; kBase += SUB)
+#pragma unroll 4
+                for (int r = 0; r < SUB; ++r)
+                    sum += a[iRow + (kBase + r) * LD] * a[(jBase + q) + (kBase + r) * LD];
+            products[e] = sum;
+        }
+        __syncthreads();
+        for (int e = t; e < count; e += DIAGONAL_THREADS) // X_IJ = -X_II T_IJ
+        {
+            const int b = e / (SUB * SUB);
+            const int p = (e / SUB) % SUB;
+            const int q = e % SUB;
+            const int iBase = (b + d) * SUB;
+            double sum = products[e];
+#pragma unroll 1
+            for (int r = 0; r < p; ++r)
+                sum += a[(iBase + r) + (iBase + p) * LD] * products[b * SUB * SUB + r * SUB + q];
+            a[(b * SUB + q) + (iBase + p) * LD] = -sum;
+        }
+        __syncthreads();
+    }
     for (int e = t; e < BLOCK * BLOCK; e += DIAGONAL_THREADS)
     {
         const int j = e / BLOCK;

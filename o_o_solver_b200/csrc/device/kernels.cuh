@@ -69,6 +69,53 @@ constexpr std::size_t smallFrontSmem(int order)
            static_cast<std::size_t>(order) * sizeof(std::int32_t);
 }
 constexpr int DIAGONAL_THREADS = 256;
+// ---- the workload models' stiffness on the GPU (model_kernels.cu) ----
+// One kind of element matrix (family 0 flat shell of a x b, thickness, young, poisson, turned by orientation 0..2;
+// 1 hexahedron of edge a; 2 given at `given` + givenOffset, row-major); dofs x dofs, at most 24.
+struct ElementKindDesc
+{
+    int family;
+    int orientation;
+    int dofs;
+    int givenOffset;
+    double a;
+    double b;
+    double thickness;
+    double young;
+    double poisson;
+};
+// A model's graph (CSR, sorted neighbours), its elements (nodes at elementStart, -1 for a clamped node; kind per
+// element), the elements of each node in increasing order (CSR), and the element matrices (576 values per kind).
+struct ModelArgs
+{
+    int nodes;
+    int nodeDofs;
+    std::int64_t slots;
+    const std::int64_t* graphOffsets;
+    const std::int32_t* neighbours;
+    const std::int64_t* elementStart;
+    const std::int32_t* elementNodes;
+    const std::int32_t* elementKind;
+    const std::int64_t* elementsOfNodeStart;
+    const std::int32_t* elementsOfNode;
+    const double* matrices;
+};
+__global__ void elementMatrices(const ElementKindDesc* kinds, const double* given, double* out);
+__global__ void nodeBlocks(ModelArgs m, double* diagonalBlocks, double* offBlocks);
+__global__ void cscCounts(ModelArgs m, const std::int32_t* nodeAtPosition, const std::int32_t* positionOf,
+                          std::int64_t* terms);
+__global__ void cscFill(ModelArgs m, const std::int32_t* nodeAtPosition, const std::int32_t* positionOf,
+                        const std::int64_t* termStart, const double* diagonalBlocks, const double* offBlocks,
+                        const double* lumpedMass, int which, std::int64_t* offsets, std::int32_t* rows, double* values);
+__global__ void scatterPositions(const std::int32_t* nodeAtPosition, std::int32_t* positionOf, int nodes);
+
+// The extend-add of the large fronts by pieces staged in shared memory (assembly_kernels.cu); AssemblyTask.pad holds
+// the piece's first front position. Dynamic shared memory: STAGE_SMEM bytes.
+__global__ void assembleStaged(FactorArgs args, const AssemblyTask* pieces, std::int32_t* structureError);
+// The update matrices' Schur products fed by TMA (update_tma_kernels.cu): 128 x 128 lower tiles {front, i0, j0,
+// tensor map index}; maps: the fronts' tensor maps (128 bytes each); error set to 1 when a bounded wait ran out.
+// Dynamic shared memory: UPDATE_TMA_SMEM bytes.
+__global__ void updateMatrixTma(FactorArgs args, const TileTask* tasks, const void* maps, int* error);
 __global__ void diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0);
 __global__ void diagonalBlocksByColumn(FactorArgs args, const std::int32_t* list, int k0);
 __global__ void panelRowsInverse(FactorArgs args, const TileTask* tasks, int k0);

@@ -13,12 +13,15 @@
 
 #include "oos_gpu.h"
 
+#include <cuda.h> // CUtensorMap and the types of cuTensorMapEncodeTiled
+
 #include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <functional>
+#include <limits>
 #include <memory>
 #include <string>
 #include <vector>
@@ -83,6 +86,27 @@ private:
     T* m_data = nullptr;
     std::size_t m_count = 0;
 };
+
+// cuTensorMapEncodeTiled, reached through the runtime's driver entry point (no link against the driver library).
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled tensorMapEncoder()
+{
+    static EncodeTiled encoder = nullptr;
+    if (encoder == nullptr)
+    {
+        void* function = nullptr;
+        cudaDriverEntryPointQueryResult found = cudaDriverEntryPointSymbolNotFound;
+        check(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &function, cudaEnableDefault, &found),
+              "cuTensorMapEncodeTiled entry point");
+        if (function == nullptr || found != cudaDriverEntryPointSuccess)
+            throw Error(STATUS_CUDA, "the driver offers no cuTensorMapEncodeTiled");
+        encoder = reinterpret_cast<EncodeTiled>(function);
+    }
+    return encoder;
+}
 
 unsigned blocksFor(std::int64_t items, int threads)
 {
@@ -193,6 +217,7 @@ public:
         m_lists.upload(m_plan.lists, m_stream, "plan: lists");
         m_tiles.upload(m_plan.tiles, m_stream, "plan: tiles");
         m_pieces.upload(m_plan.pieces, m_stream, "plan: pieces");
+        m_stagedPieces.upload(m_plan.stagedPieces, m_stream, "plan: staged pieces");
         m_zeroPivot.allocate(static_cast<std::size_t>(m_plan.supernodeCount), "factor: zero pivots");
         m_diagonal.allocate(static_cast<std::size_t>(std::max(m_plan.dimension, 1)), "factor: diagonal");
         m_counters.allocate(8, "factor: counters");
@@ -214,6 +239,12 @@ public:
         check(cudaFuncSetAttribute(device::smallFrontsPivoted, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    smallLimit),
               "smallFrontsPivoted shared memory");
+        check(cudaFuncSetAttribute(device::updateMatrixTma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(device::UPDATE_TMA_SMEM)),
+              "TMA update shared memory");
+        check(cudaFuncSetAttribute(device::assembleStaged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(device::STAGE_SMEM)),
+              "staged assembly shared memory");
         check(cudaFuncSetAttribute(device::updateMatrixMixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(device::MIXED_UPDATE_SMEM)),
               "mixed update shared memory");
@@ -275,6 +306,7 @@ public:
         const int bailout = options != nullptr ? options->bailout : 0;
         m_panels.allocate(static_cast<std::size_t>(m_plan.panelValues), "factor: panels");
         m_updates.allocate(static_cast<std::size_t>(m_plan.updateValues), "factor: update matrices");
+        buildTensorMaps();
         const std::int64_t* dOffsets = offsets;
         const std::int32_t* dRows = rows;
         const double* dValues = values;
@@ -353,11 +385,13 @@ public:
         if (options != nullptr && options->precision != 0 && options->precision != 1)
             throw Error(STATUS_INVALID_ARGUMENT, "FactorOptions: precision must be 0 (FP64) or 1 (mixed), found " +
                                                      std::to_string(options->precision));
-        if (m_mixed)
-            check(cudaMemsetAsync(m_mixedError.get(), 0, sizeof(int), m_stream), "memset");
+        check(cudaMemsetAsync(m_mixedError.get(), 0, sizeof(int), m_stream), "memset"); // tcgen05 and TMA waits
         const unsigned summaryBlocks = blocksFor(std::max(dimension, 1), 256);
         const auto launches = [&]
         {
+            // the pivot summary's counters from zero in every run of the sequence (the autotuner's timing runs, the
+            // graph's replays)
+            check(cudaMemsetAsync(m_counters.get(), 0, 8 * sizeof(unsigned long long), m_stream), "memset");
             runFactorLaunches(args);
             invertDiagonalBlocks(args, false);
             device::pivotSummary<<<summaryBlocks, 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), dimension,
@@ -368,6 +402,8 @@ public:
                                                                          m_diagonal.get());
             check(cudaGetLastError(), "pivot summary launch");
         };
+        if (m_tuning && !m_tuned && !m_mixed)
+            tune(launches);
         // Profiled factorisations launch one by one (events between the launches); the others replay a graph.
         if (m_profile)
             launches();
@@ -405,16 +441,15 @@ public:
                               m_stream),
               "download structure check");
         int mixedError = 0;
-        if (m_mixed)
-            check(cudaMemcpyAsync(&mixedError, m_mixedError.get(), sizeof(int), cudaMemcpyDeviceToHost, m_stream),
-                  "download tensor-core status");
+        check(cudaMemcpyAsync(&mixedError, m_mixedError.get(), sizeof(int), cudaMemcpyDeviceToHost, m_stream),
+              "download tensor-core status");
         check(cudaStreamSynchronize(m_stream), "factorisation");
         m_profileValid = m_profile;
         m_profiledPivoted = false;
         if (mixedError != 0)
         {
             m_factorised = false;
-            throw Error(STATUS_INTERNAL, "mixed-precision factorisation: a bounded wait on the tensor cores ran out "
+            throw Error(STATUS_INTERNAL, "factorisation: a bounded wait on the tensor cores or on a TMA load ran out "
                                          "(the update matrices are incomplete)");
         }
         float milliseconds = 0.0f;
@@ -1207,6 +1242,42 @@ public:
     // algorithmic flops and bytes of each launch kind of it.
     void setProfile(bool enable) { m_profile = enable; }
 
+    // The autotuner. Some launch kinds have more than one kernel (Launch::variant): the diagonal blocks by 16-column
+    // sub-panels or column by column, the extend-add element-wise or staged in shared memory, the update matrix by
+    // 64 x 64 tiles or by TMA-fed 128 x 128 tiles. Which is faster depends
+    // on the launch: how many fronts share it, how large they are. On the first positive definite factorisation of
+    // this factor (tuning on, FP64), the whole factorisation runs twice per variant, every launch timed by events on
+    // the stream; for each launch kind and size class (blocks in the launch: 1, up to 8, up to 148, up to 592, more)
+    // the variant with the smaller total time wins, and every launch of that class takes it from then on. Each of
+    // those factorisations is a complete, correct one (the variants compute the same factor to rounding); the
+    // factorisation that follows, with the chosen variants, is the one the caller gets. Graphs are recorded after
+    // the choice.
+    // mode 0: the plan's defaults; 1: tune on the next positive definite FP64 factorisation; 2: the alternative
+    // kernel of every tunable launch (the staged extend-add, the column-by-column diagonal blocks, the TMA-fed
+    // update tiles).
+    void setTuning(int mode)
+    {
+        if (mode < 0 || mode > 2)
+            throw Error(STATUS_INVALID_ARGUMENT, "kernel choice: mode must be 0 (defaults), 1 (autotune) or 2 "
+                                                 "(alternatives), found " + std::to_string(mode));
+        resetVariants();
+        m_tuning = mode == 1;
+        if (mode == 2)
+            for (Launch& launch : m_plan.factorLaunches)
+                if (tunable(launch))
+                    launch.variant = 1 - defaultVariant(launch);
+    }
+
+    struct TuneRecord
+    {
+        std::int32_t kind = 0;
+        std::int32_t sizeClass = 0;
+        std::int32_t launches = 0;
+        double seconds[2] = {0.0, 0.0};
+        std::int32_t chosen = 0;
+    };
+    [[nodiscard]] const std::vector<TuneRecord>& tuneReport() const noexcept { return m_tuneReport; }
+
     // The scale every solve applies to its right-hand sides and its solutions (a pencil's S: X <- S A^-1 S B); null
     // for none. Device memory, dimension values, owned by the caller.
     void setSolveScale(const double* scale) { m_solveScale = scale; }
@@ -1284,7 +1355,7 @@ public:
             {
                 const Launch& launch = profiledLaunches[index];
                 kinds[index] = static_cast<std::int32_t>(launch.kind);
-                counts[index] = launch.count;
+                counts[index] = blocksLaunched(launch);
                 k0[index] = launch.k0;
                 check(cudaEventElapsedTime(&ms, m_profileEvents[2 * index], m_profileEvents[2 * index + 1]),
                       "profile time");
@@ -1313,6 +1384,141 @@ public:
     }
 
 private:
+    // The tensor maps of the TMA-fed update-matrix kernel, one per front of Plan::tmaFronts: the front's panel as rows
+    // (contiguous, n of them) by its c columns, 16 x 16 boxes, the 128-byte swizzle, zeros outside. Built once per
+    // panel arena.
+    void buildTensorMaps()
+    {
+        if (m_plan.tmaFronts.empty() || m_mapsOf == m_panels.get())
+            return;
+        std::vector<CUtensorMap> maps(m_plan.tmaFronts.size());
+        const EncodeTiled encode = tensorMapEncoder();
+        for (std::size_t k = 0; k < maps.size(); ++k)
+        {
+            const device::FrontDesc& f = m_plan.fronts[static_cast<std::size_t>(m_plan.tmaFronts[k])];
+            const std::uint64_t n = static_cast<std::uint64_t>(f.c) + static_cast<std::uint64_t>(f.r);
+            const cuuint64_t dims[2] = {n, static_cast<cuuint64_t>(f.c)};
+            const cuuint64_t strides[1] = {n * sizeof(double)};
+            const cuuint32_t box[2] = {16, 16};
+            const cuuint32_t elementStrides[2] = {1, 1};
+            const CUresult result =
+                encode(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, m_panels.get() + f.panel, dims, strides, box,
+                       elementStrides, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (result != CUDA_SUCCESS)
+                throw Error(STATUS_CUDA, "tensor map of front " + std::to_string(m_plan.tmaFronts[k]) + ": error " +
+                                             std::to_string(static_cast<int>(result)));
+        }
+        m_tensorMaps.upload(maps, m_stream, "factor: tensor maps");
+        check(cudaStreamSynchronize(m_stream), "tensor maps");
+        m_mapsOf = m_panels.get();
+    }
+
+    static bool tunable(const Launch& launch)
+    {
+        return launch.kind == LaunchKind::DiagonalBlocks ||
+               ((launch.kind == LaunchKind::AssembleFronts || launch.kind == LaunchKind::UpdateMatrix) &&
+                launch.altCount > 0);
+    }
+
+    // The kernel a launch runs untuned: the element-wise extend-add (on the 2 M plate 10.5 ms against the staged
+    // one's 23.6), the diagonal blocks by sub-panels, the 64 x 64 update tiles (27.1 ms against the TMA-fed 128 x 128
+    // tiles' 38.1).
+    static std::int32_t defaultVariant(const Launch&) { return 0; }
+
+    // The blocks a launch runs with its current kernel (some variants run their alternative task range).
+    static std::int32_t blocksLaunched(const Launch& launch)
+    {
+        return launch.variant == 1 && launch.altCount > 0 ? launch.altCount : launch.count;
+    }
+
+    static std::int32_t sizeClass(std::int32_t blocks)
+    {
+        return blocks <= 1 ? 0 : blocks <= 8 ? 1 : blocks <= 148 ? 2 : blocks <= 592 ? 3 : 4;
+    }
+
+    // The untuned choices (every tunable launch on variant 0).
+    void resetVariants()
+    {
+        for (Launch& launch : m_plan.factorLaunches)
+            if (tunable(launch))
+                launch.variant = defaultVariant(launch);
+        m_factorGraph.reset();
+        m_tuned = false;
+        m_tuneReport.clear();
+    }
+
+    template <typename Launches> void tune(const Launches& launches)
+    {
+        constexpr int VARIANTS = 2;
+        const std::size_t count = m_plan.factorLaunches.size();
+        m_tuneReport.clear();
+        if (std::none_of(m_plan.factorLaunches.begin(), m_plan.factorLaunches.end(), tunable))
+        {
+            m_tuned = true; // nothing to choose
+            return;
+        }
+        std::vector<double> seconds(count * VARIANTS, 0.0);
+        // the timing runs launch one by one with events around each launch; the caller's profiling setting comes back
+        // whatever happens
+        struct Restore
+        {
+            bool& flag;
+            bool value;
+            ~Restore() { flag = value; }
+        } restore{m_profile, m_profile};
+        m_profile = true;
+        // Two timed factorisations per variant, each launch keeping its shorter time: the first launch of a kernel in
+        // a process also loads its module, which must not count against it.
+        constexpr int RUNS = 2;
+        std::fill(seconds.begin(), seconds.end(), std::numeric_limits<double>::infinity());
+        for (int v = 0; v < VARIANTS; ++v)
+        {
+            for (Launch& launch : m_plan.factorLaunches)
+                if (tunable(launch))
+                    launch.variant = v;
+            for (int run = 0; run < RUNS; ++run)
+            {
+                launches();
+                check(cudaStreamSynchronize(m_stream), "tuning factorisation");
+                for (std::size_t i = 0; i < count; ++i)
+                {
+                    float ms = 0.0f;
+                    check(cudaEventElapsedTime(&ms, profileEvent(2 * i), profileEvent(2 * i + 1)), "tuning time");
+                    double& kept = seconds[i * VARIANTS + static_cast<std::size_t>(v)];
+                    kept = std::min(kept, ms / 1000.0);
+                }
+            }
+        }
+        const auto recordOf = [&](const Launch& launch) -> TuneRecord&
+        {
+            const std::int32_t kind = static_cast<std::int32_t>(launch.kind);
+            const std::int32_t size = sizeClass(launch.count);
+            for (TuneRecord& r : m_tuneReport)
+                if (r.kind == kind && r.sizeClass == size)
+                    return r;
+            m_tuneReport.push_back({kind, size, 0, {0.0, 0.0}, 0});
+            return m_tuneReport.back();
+        };
+        for (std::size_t i = 0; i < count; ++i)
+        {
+            const Launch& launch = m_plan.factorLaunches[i];
+            if (!tunable(launch))
+                continue;
+            TuneRecord& r = recordOf(launch);
+            ++r.launches;
+            for (int v = 0; v < VARIANTS; ++v)
+                r.seconds[v] += seconds[i * VARIANTS + static_cast<std::size_t>(v)];
+        }
+        for (TuneRecord& r : m_tuneReport)
+            r.chosen = r.seconds[1] < r.seconds[0] ? 1 : 0;
+        for (Launch& launch : m_plan.factorLaunches)
+            if (tunable(launch))
+                launch.variant = recordOf(launch).chosen;
+        m_factorGraph.reset();
+        m_tuned = true;
+    }
+
     // The factor launches in plan order on the main stream, except the side groups (the far part of a finished
     // macro panel's update, Launch::sideGroup), which fork onto the side stream and are waited for where the plan
     // says (Launch::waitGroup) and at the end. A profiled factorisation runs everything on the main stream.
@@ -1384,12 +1590,20 @@ private:
                 break;
             }
             case LaunchKind::AssembleFronts:
-                device::assembleFronts<<<launch.count, 256, 0, stream>>>(args, m_pieces.get() + launch.offset,
-                                                                           m_structureError.get());
+                if (launch.variant == 1)
+                    device::assembleStaged<<<launch.altCount, device::STAGE_THREADS, device::STAGE_SMEM, stream>>>(
+                        args, m_stagedPieces.get() + launch.altOffset, m_structureError.get());
+                else
+                    device::assembleFronts<<<launch.count, 256, 0, stream>>>(args, m_pieces.get() + launch.offset,
+                                                                               m_structureError.get());
                 break;
             case LaunchKind::DiagonalBlocks:
-                device::diagonalBlocks<<<launch.count, device::DIAGONAL_THREADS, 0, stream>>>(
-                    args, m_lists.get() + launch.offset, launch.k0);
+                if (launch.variant == 1)
+                    device::diagonalBlocksByColumn<<<launch.count, device::DIAGONAL_THREADS, 0, stream>>>(
+                        args, m_lists.get() + launch.offset, launch.k0);
+                else
+                    device::diagonalBlocks<<<launch.count, device::DIAGONAL_THREADS, 0, stream>>>(
+                        args, m_lists.get() + launch.offset, launch.k0);
                 break;
             case LaunchKind::PanelRows:
                 device::panelRowsInverse<<<launch.count, device::TILE_THREADS, device::PANEL_ROWS_INVERSE_SMEM,
@@ -1400,8 +1614,13 @@ private:
                     args, m_tiles.get() + launch.offset, launch.k0);
                 break;
             case LaunchKind::UpdateMatrix:
-                device::updateMatrix<<<launch.count, device::TILE_THREADS, 0, stream>>>(
-                    args, m_tiles.get() + launch.offset);
+                if (launch.variant == 1)
+                    device::updateMatrixTma<<<launch.altCount, device::UPDATE_THREADS, device::UPDATE_TMA_SMEM,
+                                              stream>>>(args, m_tiles.get() + launch.altOffset, m_tensorMaps.get(),
+                                                        m_mixedError.get());
+                else
+                    device::updateMatrix<<<launch.count, device::TILE_THREADS, 0, stream>>>(
+                        args, m_tiles.get() + launch.offset);
                 break;
             default:
                 throw Error(STATUS_INTERNAL, "factorisation plan: a solve launch in the factor sequence");
@@ -1503,6 +1722,9 @@ private:
     DeviceArray<std::int32_t> m_lists;
     DeviceArray<device::TileTask> m_tiles;
     DeviceArray<device::AssemblyTask> m_pieces;
+    DeviceArray<device::AssemblyTask> m_stagedPieces;
+    DeviceArray<CUtensorMap> m_tensorMaps;
+    const double* m_mapsOf = nullptr; // the panel arena the tensor maps describe
     DeviceArray<std::int32_t> m_zeroPivot;
     DeviceArray<unsigned long long> m_counters;
     DeviceArray<std::int32_t> m_issues;
@@ -1561,6 +1783,9 @@ private:
     std::size_t m_smallSmem = 0;
     bool m_factorised = false;
     bool m_profile = false;
+    bool m_tuning = true;
+    bool m_tuned = false;
+    std::vector<TuneRecord> m_tuneReport;
     bool m_profileValid = false;
     bool m_solveProfileValid = false;
     bool m_profiledPivoted = false; // the last profiled factorisation ran the indefinite launches
@@ -2157,6 +2382,20 @@ extern "C" int oosgpu_model_csc(const oosgpu_model* model, const int32_t* node_a
         });
 }
 
+extern "C" int oosgpu_model_csc_device(const oosgpu_model* model, const int32_t* node_at_position, int32_t which,
+                                       int32_t device, int64_t* col_offsets, int32_t* rows, double* values)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(model, "model");
+            requirePointer(node_at_position, "node_at_position");
+            requirePointer(col_offsets, "col_offsets");
+            oosgpu::check(cudaSetDevice(device), "cudaSetDevice");
+            model->model.toCscOnDevice(node_at_position, which, col_offsets, rows, values);
+        });
+}
+
 extern "C" int oosgpu_model_loads(const oosgpu_model* model, const int32_t* node_at_position, int64_t columns,
                                   uint64_t seed_base, int32_t points, double sigma, double* rhs, int64_t ld)
 {
@@ -2176,6 +2415,45 @@ extern "C" int oosgpu_factor_profile(oosgpu_factor* factor, int32_t enable)
         {
             requirePointer(factor, "factor");
             factor->factor->setProfile(enable != 0);
+        });
+}
+
+extern "C" int oosgpu_factor_set_tuning(oosgpu_factor* factor, int32_t enable)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            factor->factor->setTuning(enable);
+        });
+}
+
+extern "C" int oosgpu_factor_tuning_report(oosgpu_factor* factor, int64_t capacity, int32_t* kinds,
+                                           int32_t* size_classes, int32_t* launches, double* seconds0,
+                                           double* seconds1, int32_t* chosen, int64_t* total)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            requirePointer(total, "total");
+            const auto& report = factor->factor->tuneReport();
+            *total = static_cast<int64_t>(report.size());
+            for (std::size_t k = 0; k < report.size() && static_cast<int64_t>(k) < capacity; ++k)
+            {
+                if (kinds != nullptr)
+                    kinds[k] = report[k].kind;
+                if (size_classes != nullptr)
+                    size_classes[k] = report[k].sizeClass;
+                if (launches != nullptr)
+                    launches[k] = report[k].launches;
+                if (seconds0 != nullptr)
+                    seconds0[k] = report[k].seconds[0];
+                if (seconds1 != nullptr)
+                    seconds1[k] = report[k].seconds[1];
+                if (chosen != nullptr)
+                    chosen[k] = report[k].chosen;
+            }
         });
 }
 

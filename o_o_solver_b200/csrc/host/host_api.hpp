@@ -82,8 +82,33 @@ public:
                double* values) const;
     void loads(const std::int32_t* nodeAtPosition, std::int64_t columns, std::uint64_t seedBase,
                std::int32_t pointsPerPattern, double sigma, double* rhs, std::int64_t ld) const;
+    // toCsc on the GPU (model_kernels.cu): the element matrices computed there, the node blocks assembled there in
+    // the host's order (so the same values), the columns written there. offsets (dimension + 1), rows and values
+    // (cscTermCount) are device arrays; the call returns when they are written.
+    void toCscOnDevice(const std::int32_t* nodeAtPosition, int which, std::int64_t* offsets, std::int32_t* rows,
+                       double* values) const;
+
+    // One kind of element matrix: a flat shell (a x b, thickness, E, nu, turned into the global axes by one of three
+    // orientations), a trilinear hexahedron (edge, E, nu), or a matrix given by the host (row-major, dofs x dofs).
+    struct ElementKind
+    {
+        int family = 0; // 0 shell, 1 hexahedron, 2 given
+        double a = 0.0, b = 0.0, thickness = 0.0, young = 0.0, poisson = 0.0;
+        int orientation = 0;
+        int dofs = 24;
+        std::vector<double> given;
+    };
 
 private:
+    // The element list the device assembly works from: nodes of element e at m_elementStart[e] (-1 for a clamped
+    // node), its kind m_elementKind[e]; kinds in m_kinds.
+    int addKind(const ElementKind& kind);
+    void recordElement(const std::vector<std::int32_t>& nodes, int kind);
+    std::vector<std::int64_t> m_elementStart{0};
+    std::vector<std::int32_t> m_elementNodes;
+    std::vector<std::int32_t> m_elementKind;
+    std::vector<ElementKind> m_kinds;
+
     void buildGraph(const std::vector<std::vector<std::int32_t>>& elements);
     // Adds an element matrix (nodes.size() x nodeDofs square, row-major) into the node blocks (after clearBlocks).
     void clearBlocks();

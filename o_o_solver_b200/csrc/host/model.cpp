@@ -214,6 +214,19 @@ double uniform01(std::uint64_t& state)
 
 Model::Model() = default;
 
+int Model::addKind(const ElementKind& kind)
+{
+    m_kinds.push_back(kind);
+    return static_cast<int>(m_kinds.size()) - 1;
+}
+
+void Model::recordElement(const std::vector<std::int32_t>& nodes, int kind)
+{
+    m_elementNodes.insert(m_elementNodes.end(), nodes.begin(), nodes.end());
+    m_elementStart.push_back(static_cast<std::int64_t>(m_elementNodes.size()));
+    m_elementKind.push_back(kind);
+}
+
 std::int64_t Model::slot(std::int32_t node, std::int32_t neighbour) const
 {
     const auto begin = m_offsets.begin() + m_offsets[static_cast<std::size_t>(node)];
@@ -335,6 +348,15 @@ Model Model::plate(std::int32_t nx, std::int32_t ny, double lx, double ly, doubl
     std::vector<double> ke(SHELL_DOFS * SHELL_DOFS);
     shellStiffness(a, b, thickness, young, poisson, ke.data());
     model.assemble(elements, ke.data(), 6);
+    ElementKind shell;
+    shell.a = a;
+    shell.b = b;
+    shell.thickness = thickness;
+    shell.young = young;
+    shell.poisson = poisson;
+    const int kind = model.addKind(shell);
+    for (const auto& nodes : elements)
+        model.recordElement(nodes, kind);
     // The consistent load of a uniform pressure on the bilinear deflection: p*a*b/4 on w at each node.
     model.m_pressureLoad.assign(static_cast<std::size_t>(model.m_nodeCount) * 6, 0.0);
     for (const auto& nodes : elements)
@@ -414,6 +436,11 @@ Model Model::stiffenedPanel(std::int32_t n, double lx, double ly, double thickne
     };
     bend(1, 5, young * inPlane, 1.0);
     bend(2, 4, young * outOfPlane, -1.0);
+    ElementKind frame;
+    frame.family = 2;
+    frame.dofs = 12;
+    frame.given.assign(ke, ke + 12 * 12);
+    const int frameKind = model.addKind(frame);
     for (std::int32_t k = 0; k < stringers; ++k)
     {
         const auto iy = static_cast<std::int32_t>(std::lround(static_cast<double>(k + 1) * n / (stringers + 1)));
@@ -422,6 +449,7 @@ Model Model::stiffenedPanel(std::int32_t n, double lx, double ly, double thickne
             const std::int32_t first = ix == 0 ? -1 : iy * n + ix - 1;
             const std::int32_t second = iy * n + ix;
             model.addElement({first, second}, ke);
+            model.recordElement({first, second}, frameKind);
         }
     }
     return model;
@@ -515,8 +543,17 @@ Model Model::wingBox(double span, double chord, double height, double ribPitch, 
                                    {0, 0, 1, 1, 0, 0, 0, 1, 0},   // yz: local x = y, local y = z, n = x
                                    {1, 0, 0, 0, 0, -1, 0, 1, 0}}; // xz: local x = x, local y = z, n = -y
     std::vector<std::vector<double>> matrices;
+    std::vector<int> kindOfGroup;
     for (const Group& g : groups)
     {
+        ElementKind shell;
+        shell.a = g.a;
+        shell.b = g.b;
+        shell.thickness = g.thickness;
+        shell.young = young;
+        shell.poisson = poisson;
+        shell.orientation = g.orientation;
+        kindOfGroup.push_back(model.addKind(shell));
         std::vector<double> local(SHELL_DOFS * SHELL_DOFS);
         shellStiffness(g.a, g.b, g.thickness, young, poisson, local.data());
         // global = T local T^T with T = blockdiag(R) over the 8 triples of DOFs (R(i, j) = rotation[i * 3 + j])
@@ -549,6 +586,7 @@ Model Model::wingBox(double span, double chord, double height, double ribPitch, 
     {
         const Group& g = groups[static_cast<std::size_t>(groupOf[e])];
         model.addElement(elements[e], matrices[static_cast<std::size_t>(groupOf[e])].data());
+        model.recordElement(elements[e], kindOfGroup[static_cast<std::size_t>(groupOf[e])]);
         const double area = g.a * g.b;
         const double translation = density * g.thickness * area / 4.0;
         const double rotary = density * g.thickness * g.thickness * g.thickness * area / 48.0;
@@ -597,6 +635,14 @@ Model Model::hexBlock(std::int32_t n, double edge, double young, double poisson,
     std::vector<double> ke(HEX_DOFS * HEX_DOFS);
     hexStiffness(h, young, poisson, ke.data());
     model.assemble(elements, ke.data(), 3);
+    ElementKind solid;
+    solid.family = 1;
+    solid.a = h;
+    solid.young = young;
+    solid.poisson = poisson;
+    const int kind = model.addKind(solid);
+    for (const auto& nodes : elements)
+        model.recordElement(nodes, kind);
     // Lumped mass: an eighth of each element's mass at each of its nodes, in every direction.
     model.m_lumpedMass.assign(static_cast<std::size_t>(model.m_nodeCount) * 3, 0.0);
     for (const auto& nodes : elements)

@@ -105,6 +105,8 @@ void annotate(Plan& plan, const std::vector<std::int64_t>& cscTermsOfFront)
             }
             case LaunchKind::AssembleFronts:
             {
+                // The launch's own range is the element-wise pieces; the accounting follows that range whichever
+                // kernel runs it (the staged pieces of the alternative cover the same elements).
                 const AssemblyTask& piece = plan.pieces[at];
                 const FrontDesc& f = front(piece.front);
                 const std::int64_t n = f.c + f.r;
@@ -359,6 +361,7 @@ Plan buildPlan(const Symbolic& symbolic)
         addList(plan, plan.factorLaunches, LaunchKind::SmallFronts, small64, 0, order64);
         addList(plan, plan.factorLaunches, LaunchKind::SmallFronts, small96, 0, order96);
         addList(plan, plan.factorLaunches, LaunchKind::SmallFronts, small128, 0, order128);
+        Launch elementwiseAssembly{LaunchKind::AssembleFronts, 0, 0, 0, 0};
         if (!large.empty())
         {
             std::vector<AssemblyTask> pieces;
@@ -381,9 +384,31 @@ Plan buildPlan(const Symbolic& symbolic)
                     }
                 }
             }
-            plan.factorLaunches.push_back({LaunchKind::AssembleFronts, static_cast<std::int64_t>(plan.pieces.size()),
-                                           static_cast<std::int32_t>(pieces.size()), 0, 0});
+            // The indefinite sequence assembles element-wise (its launch is kept for it below); the positive definite
+            // one by pieces staged in shared memory: bands of STAGE_COLUMNS columns that stop at the panel's edge, each
+            // cut into STAGE_ROWS positions (a panel band from row 0, its zeros above the diagonal included; an update
+            // band from its diagonal).
+            elementwiseAssembly = Launch{LaunchKind::AssembleFronts, static_cast<std::int64_t>(plan.pieces.size()),
+                                         static_cast<std::int32_t>(pieces.size()), 0, 0};
             plan.pieces.insert(plan.pieces.end(), pieces.begin(), pieces.end());
+            std::vector<AssemblyTask> staged;
+            for (const std::int32_t s : large)
+            {
+                const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+                const std::int32_t n = f.c + f.r;
+                for (std::int32_t j0 = 0; j0 < n;)
+                {
+                    const std::int32_t j1 = std::min(j0 + device::STAGE_COLUMNS, j0 < f.c ? f.c : n);
+                    for (std::int32_t i0 = j0 < f.c ? 0 : j0; i0 < n; i0 += device::STAGE_ROWS)
+                        staged.push_back({s, j0, j1, i0});
+                    j0 = j1;
+                }
+            }
+            Launch assembly = elementwiseAssembly; // variant 1: the staged pieces (altOffset, altCount)
+            assembly.altOffset = static_cast<std::int64_t>(plan.stagedPieces.size());
+            assembly.altCount = static_cast<std::int32_t>(staged.size());
+            plan.factorLaunches.push_back(assembly);
+            plan.stagedPieces.insert(plan.stagedPieces.end(), staged.begin(), staged.end());
             // Two-level blocking: the 64-column steps update the trailing columns of their PANEL_MACRO-column macro
             // panel only (K = 64); after a macro panel's last step, its columns update every later column of the panel
             // at once (K = PANEL_MACRO), a quarter of the passes over the trailing panel. Lookahead: that update is
@@ -454,6 +479,40 @@ Plan buildPlan(const Symbolic& symbolic)
             addTiles(plan, plan.factorLaunches, LaunchKind::UpdateMatrix, schur);
             if (levelLastGroup >= 0 && plan.factorLaunches.size() > at)
                 plan.factorLaunches.back().waitGroup = levelLastGroup;
+            // The TMA-fed kernel's 128 x 128 tiles (variant 1, the launch's alternative range), when every front of
+            // the launch can be read by a tensor map: a panel that starts on a 16-byte boundary, an even order (its
+            // stride a multiple of 16 bytes) and an even c, so that every box's first row, c + i0 + 16 b, is even (a
+            // TMA copy's contiguous coordinate times 8 bytes must be a multiple of 16). Each tile carries its front's
+            // tensor map index in k0.
+            bool tmaFed = !schur.empty();
+            for (const std::int32_t s : large)
+            {
+                const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+                if (f.r > 0 && (f.c % 2 != 0 || f.r % 2 != 0 || f.panel % 2 != 0))
+                    tmaFed = false;
+            }
+            if (tmaFed && plan.factorLaunches.size() > at)
+            {
+                std::vector<TileTask> wide;
+                for (const std::int32_t s : large)
+                {
+                    const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+                    if (f.r == 0)
+                        continue;
+                    const auto map = static_cast<std::int32_t>(plan.tmaFronts.size());
+                    plan.tmaFronts.push_back(s);
+                    for (std::int32_t j0 = 0; j0 < f.r; j0 += device::UPDATE_TILE)
+                        for (std::int32_t i0 = j0; i0 < f.r; i0 += device::UPDATE_TILE)
+                            wide.push_back({s, i0, j0, map});
+                }
+                std::stable_sort(wide.begin(), wide.end(), [&](const TileTask& x, const TileTask& y)
+                                 { return plan.fronts[static_cast<std::size_t>(x.front)].c >
+                                          plan.fronts[static_cast<std::size_t>(y.front)].c; });
+                Launch& update = plan.factorLaunches.back();
+                update.altOffset = static_cast<std::int64_t>(plan.tiles.size());
+                update.altCount = static_cast<std::int32_t>(wide.size());
+                plan.tiles.insert(plan.tiles.end(), wide.begin(), wide.end());
+            }
             // The same update matrices by 128 x 128 tiles, for the mixed-precision form.
             std::vector<TileTask> mixed;
             for (const std::int32_t s : large)
@@ -482,12 +541,7 @@ Plan buildPlan(const Symbolic& symbolic)
         addList(plan, plan.pivotedLaunches, LaunchKind::SmallFrontsPivoted, small128, 0, order128);
         if (!large.empty())
         {
-            for (auto it = plan.factorLaunches.rbegin(); it != plan.factorLaunches.rend(); ++it)
-                if (it->kind == LaunchKind::AssembleFronts)
-                {
-                    plan.pivotedLaunches.push_back(*it);
-                    break;
-                }
+            plan.pivotedLaunches.push_back(elementwiseAssembly);
             std::int64_t w = 0;
             std::int32_t maxColumns = 0;
             for (const std::int32_t s : large)

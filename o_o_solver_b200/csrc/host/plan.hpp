@@ -72,6 +72,15 @@ struct Launch
     // waitGroup >= 0 makes the launch wait until side group waitGroup has finished. Groups count up from 0.
     std::int32_t sideGroup = -1;
     std::int32_t waitGroup = -1;
+    // Which kernel runs a launch of this kind, where there are several (AssembleFronts: 0 element-wise on
+    // Plan::pieces, 1 staged in shared memory on Plan::stagedPieces; DiagonalBlocks: 0 by 16-column sub-panels,
+    // 1 column by column; UpdateMatrix: 0 64 x 64 tiles by cp.async, 1 128 x 128 tiles by TMA).
+    std::int32_t variant = 0;
+    // The task range of variant 1 where it reads another task array than variant 0 (AssembleFronts: the staged
+    // pieces in Plan::stagedPieces; UpdateMatrix: the 128 x 128 tiles of the TMA-fed kernel in Plan::tiles); the
+    // launch's own range (offset, count) is variant 0's.
+    std::int64_t altOffset = 0;
+    std::int32_t altCount = 0;
 };
 
 constexpr int LAUNCH_KIND_COUNT = 14;
@@ -105,6 +114,10 @@ struct Plan
     std::vector<std::int32_t> lists;
     std::vector<device::TileTask> tiles;
     std::vector<device::AssemblyTask> pieces;
+    // The fronts whose update matrices the TMA-fed kernel can take, in the order of their tensor maps.
+    std::vector<std::int32_t> tmaFronts;
+    // The staged extend-add's pieces (AssemblyTask.pad: the piece's first front position).
+    std::vector<device::AssemblyTask> stagedPieces;
     std::vector<Launch> factorLaunches;
     std::vector<Launch> forwardLaunches;
     std::vector<Launch> backwardLaunches;

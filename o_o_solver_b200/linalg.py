@@ -277,6 +277,32 @@ class SupernodalFactor:
         return {name: {"seconds": float(seconds[k]), "launches": int(launches[k]), "flops": float(flops[k]),
                        "bytes": float(bytes_[k])} for k, name in enumerate(self.KERNEL_KINDS)}
 
+    SIZE_CLASSES = ["1 block", "up to 8", "up to 148", "up to 592", "more"]
+
+    def set_tuning(self, mode="tune"):
+        """The kernel choice of the launch kinds with two kernels: "tune" (the default: on the next positive definite
+        FP64 factorisation each is timed and each size class of launch keeps the faster), "default" (the plan's own
+        kernels) or "alternative" (the other kernel everywhere)."""
+        code = {"default": 0, "tune": 1, "alternative": 2}[mode]
+        _check(nat.load().oosgpu_factor_set_tuning(self._handle, code))
+
+    def tuning(self) -> list:
+        """The autotuner's choices: per (launch kind, size class) the launches, the seconds of each kernel in the timing
+        factorisations and the kernel chosen (0 or 1); empty before the tuning factorisation."""
+        lib = nat.load()
+        total = ctypes.c_int64()
+        _check(lib.oosgpu_factor_tuning_report(self._handle, 0, None, None, None, None, None, None, ctypes.byref(total)))
+        count = int(total.value)
+        kinds, classes, launches, chosen = (np.zeros(max(count, 1), dtype=np.int32) for _ in range(4))
+        seconds0, seconds1 = np.zeros(max(count, 1)), np.zeros(max(count, 1))
+        _check(lib.oosgpu_factor_tuning_report(self._handle, count, nat.ptr(kinds, nat.i32p), nat.ptr(classes, nat.i32p),
+                                               nat.ptr(launches, nat.i32p), nat.ptr(seconds0, nat.f64p),
+                                               nat.ptr(seconds1, nat.f64p), nat.ptr(chosen, nat.i32p),
+                                               ctypes.byref(total)))
+        return [{"kind": self.LAUNCH_KINDS[kinds[k]], "size_class": self.SIZE_CLASSES[classes[k]],
+                 "launches": int(launches[k]), "seconds": [float(seconds0[k]), float(seconds1[k])],
+                 "chosen": int(chosen[k])} for k in range(count)]
+
     LAUNCH_KINDS = ["small_fronts", "assemble_fronts", "diagonal_blocks", "panel_rows", "panel_update",
                     "update_matrix", "forward_small", "forward_gather", "forward_diagonal", "forward_update",
                     "backward_small", "backward_rows", "backward_diagonal", "backward_update",

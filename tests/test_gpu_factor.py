@@ -281,3 +281,36 @@ def test_refinement_on_device_arrays(lib, oracle_mod, gpu):
     torch.cuda.synchronize()
     assert backward_error(csc, d_x.cpu().numpy().T, b).max() <= 1.0e-15, info
     assert np.array_equal(d_b.cpu().numpy().T, b)  # B untouched
+
+
+@pytest.mark.parametrize("name", ["hex14", "plate100"])
+@pytest.mark.parametrize("mode", ["default", "alternative", "tune"])
+def test_kernel_choices_match_reference(name, mode, lib, oracle_mod, gpu):
+    """Both kernels of the launch kinds that have two (the diagonal blocks by sub-panels or by columns, the extend-add
+    staged or element-wise), and the autotuner's mix of them, give the reference's factor: exact inertia, panels within
+    1e-10; the autotuner reports a timed choice for each size class of those launches."""
+    from o_o_solver_b200 import SupernodalFactor
+
+    model, sym, csc = build_case(name, oracle_mod)
+    ref = oracle_mod.factorise(sym, csc.offsets, csc.rows, csc.values, family=0)
+    factor = SupernodalFactor(gpu_symbolic(sym))
+    factor.set_tuning(mode)
+    factor.refactorise(csc)
+    factor.refactorise(csc)  # a replay of the recorded launches, with the choice made
+    assert (factor.inertia.positive, factor.inertia.negative, factor.inertia.zero) == (ref.positive, ref.negative,
+                                                                                       ref.zero)
+    worst = 0.0
+    for s in range(sym.supernode_count):
+        mine, _, _ = factor.panel(s)
+        theirs, _, _ = ref.panel(s)
+        worst = max(worst, np.abs(mine - theirs).max() / max(np.abs(theirs).max(), 1e-300))
+    assert worst <= 1e-10, worst
+    report = factor.tuning()
+    if mode == "tune":
+        assert report and {r["kind"] for r in report} <= {"assemble_fronts", "diagonal_blocks", "update_matrix"}
+        for r in report:
+            assert r["launches"] > 0 and min(r["seconds"]) > 0.0 and r["chosen"] in (0, 1)
+            assert r["seconds"][r["chosen"]] == min(r["seconds"])
+    else:
+        assert report == []
+    factor.close()
