@@ -88,9 +88,9 @@ typedef struct
     int32_t bailout;                 /* PivotPolicy::bailout (SingularityBailOut): < 0 continues past flagged pivots */
     const double* reference_diagonal; /* FactorOptions::referenceDiagonal (host, dimension values) or NULL */
     /* FactorOptions::pivoting: 0 PivotingMode::PositiveDefinite, 1 PivotingMode::Indefinite (Bunch-Kaufman 1x1/2x2
-     * pivots within each front; zero pivots counted in the inertia, not refused; the ratio test is not applied; a
-     * pivot the reference would delay to a parent front is taken in place when its diagonal is at least 1e-3 of its
-     * column maximum (info->forced), refused with OOSGPU_SOLVER below that) */
+     * pivots among each front's candidates, a candidate that cannot be pivoted delayed to the parent front, which
+     * grows by it (info->delayed counts them); zero pivots counted in the inertia, not refused; the ratio test is not
+     * applied) */
     int32_t pivoting;
     /* FP64 (0), or mixed (1, positive definite mode only): the update matrices of the large fronts by 3xTF32 products
      * on the tcgen05 tensor cores with FP32 accumulation (about FP32 accuracy; refine the solves in FP64). No
@@ -104,7 +104,7 @@ typedef struct
     int64_t positive;
     int64_t negative;
     int64_t zero;
-    int64_t delayed;
+    int64_t delayed;                /* SupernodalFactor::delayedPivotCount: candidates delayed to a parent front */
     int64_t two_by_two;
     int64_t issue_count;            /* pivots flagged by the ratio test */
     int32_t equation_of_largest;    /* PivotDiagnostics::equationOfLargestRatio */
@@ -113,8 +113,6 @@ typedef struct
     int32_t issues[16];             /* the first flagged equations, increasing */
     int32_t zero_pivots[16];        /* the first zero-pivot equations, increasing */
     double device_seconds;          /* the factorisation's device time (CUDA events) */
-    int64_t forced;                 /* indefinite mode: pivots the reference would delay to a parent front, taken in
-                                       place (|d| >= 1e-3 of the column maximum; no counterpart in the reference) */
 } oosgpu_factor_info;
 
 /* A factor of `symbolic` on CUDA device `device` (the symbolic structure is copied: it may be destroyed after). */
@@ -132,6 +130,28 @@ int oosgpu_factorise(oosgpu_factor* factor, int32_t dimension, const int64_t* co
 int oosgpu_factorise_device(oosgpu_factor* factor, int32_t dimension, int64_t terms, const int64_t* col_offsets,
                             const int32_t* rows, const double* values, const oosgpu_factor_options* options,
                             oosgpu_factor_info* info);
+
+/* ---- partial factorisation: PartialFactor (include/oos/linalg/supernodal/PartialFactor.hpp:48-112) ------------ */
+/* PartialFactor::factorise: the symbolic factor's last supernode is the trailing set (the unit's boundary: the last
+ * `trailing` equations, a root with no rows below, alone in its level; the reference's SymbolicFactor with a trailing
+ * node count). Every other supernode is factorised in positive definite FP64 mode (options->pivoting 0, precision 0,
+ * the ratio test as oosgpu_factorise); the trailing front, assembled from the matrix's boundary entries and its
+ * children's update matrices, is K* = K_bb - K_bi K_ii^-1 K_ib, written to schur_complement (host, trailing x
+ * trailing, column-major, both triangles). info covers the interior pivots. A partial factor refuses
+ * oosgpu_solve (FactorSolve::solve refuses a partial factor too). */
+int oosgpu_factorise_partial(oosgpu_factor* factor, int32_t dimension, const int64_t* col_offsets, const int32_t* rows,
+                             const double* values, int32_t trailing, const oosgpu_factor_options* options,
+                             double* schur_complement, oosgpu_factor_info* info);
+/* PartialFactor::condenseLoads: f* = f_b - K_bi K_ii^-1 f_i of the loads (host, dimension x columns, leading
+ * dimension ld) into condensed (host, trailing x columns, leading dimension ld_condensed): the forward sweep over the
+ * interior, the trailing rows gathered from the children of the trailing supernode. */
+int oosgpu_partial_condense(oosgpu_factor* factor, const double* loads, int64_t ld, int64_t columns, double* condensed,
+                            int64_t ld_condensed);
+/* PartialFactor::recover: the loads (host, dimension x columns, leading dimension ld) replaced by the solution with
+ * the trailing rows given (trailing_values, trailing x columns): u_i = K_ii^-1 (f_i - K_ib u_b), the trailing rows
+ * u_b. */
+int oosgpu_partial_recover(oosgpu_factor* factor, double* loads_to_solution, int64_t ld, int64_t columns,
+                           const double* trailing_values, int64_t ld_trailing);
 
 /* The panel of supernode s (host copies): eliminated columns, rows; values (rows x eliminated, column-major),
  * row equations and the 2x2 subdiagonal (zeros in positive definite mode) when the pointers are not NULL. */

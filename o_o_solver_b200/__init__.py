@@ -7,6 +7,7 @@ from .linalg import (  # noqa: F401
     FactorSolve,
     Inertia,
     MemoryBudgetError,
+    PartialFactor,
     PivotPolicy,
     ShiftFactorisation,
     SingularityError,

@@ -33,7 +33,6 @@ class FactorInfo(ctypes.Structure):
         ("issues", ctypes.c_int32 * 16),
         ("zero_pivots", ctypes.c_int32 * 16),
         ("device_seconds", ctypes.c_double),
-        ("forced", ctypes.c_int64),
     ]
 
 
@@ -70,6 +69,10 @@ SIGNATURES = [
     ("oosgpu_factor_create", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),
     ("oosgpu_factor_destroy", None, [_vp]),
     ("oosgpu_factor_stream", _vp, [_vp]),
+    ("oosgpu_factorise_partial", ctypes.c_int, [_vp, ctypes.c_int32, _i64p, _i32p, _f64p, ctypes.c_int32,
+                                                 ctypes.POINTER(FactorOptions), _f64p, ctypes.POINTER(FactorInfo)]),
+    ("oosgpu_partial_condense", ctypes.c_int, [_vp, _f64p, ctypes.c_int64, ctypes.c_int64, _f64p, ctypes.c_int64]),
+    ("oosgpu_partial_recover", ctypes.c_int, [_vp, _f64p, ctypes.c_int64, ctypes.c_int64, _f64p, ctypes.c_int64]),
     ("oosgpu_factorise", ctypes.c_int, [_vp, ctypes.c_int32, _i64p, _i32p, _f64p, ctypes.POINTER(FactorOptions),
                                         ctypes.POINTER(FactorInfo)]),
     ("oosgpu_factorise_device", ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int64, _vp, _vp, _vp,

@@ -483,18 +483,22 @@ __global__ void __launch_bounds__(DIAGONAL_THREADS) diagonalBlocksByColumn(Facto
 //      d_k is shuffled from lane k, l_ik = a_ik / d_k, w_ik = l_ik d_k, and a_ij -= l_ik w_jk for k < j <= i, w_jk
 //      shuffled from lane j; then the same lanes invert the unit lower block, X_JJ = L_JJ^-1 (lane j: column j,
 //      X(i, j) = -sum_{j <= q < i} L(i, q) X(q, j)), into the block's strict upper triangle (X(i, j) at (j, i));
-//   2. the rows below the sub-panel: l_iq = (sum_{p <= q} a_ip X(q, p)) / d_q, and w_iq = l_iq d_q, each element alone;
-//   3. the trailing lower triangle: a_ij -= sum_q l_iq w_jq, q in increasing order (the reference's term order).
-// The 64 x 64 inverse then needs only its off-diagonal 16 x 16 blocks, by block diagonals as in diagonalBlocksByColumn.
-// Barriers: four per sub-panel and two per block diagonal, against one per column before; the chain of dependent
-// steps runs in one warp's registers.
-__global__ void __launch_bounds__(DIAGONAL_THREADS, 3) diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0)
+//   2. the rows below the sub-panel: Y = A X_JJ^T on the FP64 tensor cores, then l_iq = y_iq / d_q and w_iq = y_iq;
+//   3. the trailing lower triangle: A -= L W^T on the tensor cores, lower 8 x 8 tiles.
+// The 64 x 64 inverse then needs only its off-diagonal 16 x 16 blocks, by block diagonals on the tensor cores:
+// T_IJ = sum_{J <= K < I} L_IK X_KJ, X_IJ = -X_II T_IJ. Products of 8 x 8 tiles (DMMA m8n8k4: lane g = lane / 4
+// holds row g of A and column g of B at k = lane mod 4, and results (g, 2 (lane mod 4)) and the next column), spread
+// over the block's warps; beyond kb the block is the identity, so the tiles run over all 64 rows.
+__global__ void __launch_bounds__(DIAGONAL_THREADS, 2) diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0)
 {
     constexpr int LD = BLOCK + 1;
     constexpr int SUB = INVERSE_SUB; // 16
+    constexpr int W_LD = SUB + 1;    // rows of W apart by 17 doubles: a tile's 8 rows on distinct banks
+    constexpr int P_LD = SUB + 1;
+    constexpr int P_BLOCK = SUB * P_LD;
     __shared__ double a[BLOCK * LD];
-    __shared__ double wRows[BLOCK * SUB]; // w(i, q) = l_iq d_q of the current sub-panel, at wRows[i * SUB + q]
-    __shared__ double products[(BLOCK / SUB - 1) * SUB * SUB];
+    __shared__ double wRows[BLOCK * W_LD]; // w(i, q) = y_iq of the current sub-panel, at wRows[i * W_LD + q]
+    __shared__ double products[(BLOCK / SUB - 1) * P_BLOCK];
     const std::int32_t s = list[blockIdx.x];
     const FrontDesc f = args.fronts[s];
     const int n = f.c + f.r;
@@ -530,20 +534,18 @@ __global__ void __launch_bounds__(DIAGONAL_THREADS, 3) diagonalBlocks(FactorArgs
 #pragma unroll
             for (int q = 0; q < SUB; ++q)
                 x[q] = row && q <= i ? a[(j0 + i) + (j0 + q) * LD] : 0.0;
+            // The reciprocal of each pivot by every lane, outside any branch (a division under a branch keeps the
+            // row in local memory), l_ik = a_ik (1 / d_k); the pivots checked once the block is eliminated.
 #pragma unroll
             for (int k = 0; k < SUB; ++k)
             {
                 if (k < width)
                 {
                     const double d = __shfl_sync(0xffffffffu, x[k], k);
-                    double l = 0.0;
-                    if (i == k && isBadPivot(d))
-                        atomicMin(args.zeroPivot + s, k0 + j0 + k);
+                    const double reciprocal = 1.0 / d;
+                    const double l = row && i > k ? x[k] * reciprocal : 0.0;
                     if (row && i > k)
-                    {
-                        l = x[k] / d;
                         x[k] = l;
-                    }
                     const double w = l * d; // w_ik, for the lanes below the pivot
 #pragma unroll
                     for (int j = k + 1; j < SUB; ++j)
@@ -560,6 +562,8 @@ __global__ void __launch_bounds__(DIAGONAL_THREADS, 3) diagonalBlocks(FactorArgs
                 for (int q = 0; q < SUB; ++q)
                     if (q <= i)
                         a[(j0 + i) + (j0 + q) * LD] = x[q];
+                if (isBadPivot(a[(j0 + i) + (j0 + i) * LD]))
+                    atomicMin(args.zeroPivot + s, k0 + j0 + i);
             }
             __syncwarp();
             // X = L_JJ^-1, lane j: column j (unit diagonal; rows and columns beyond width give the identity)
@@ -581,96 +585,126 @@ __global__ void __launch_bounds__(DIAGONAL_THREADS, 3) diagonalBlocks(FactorArgs
             }
         }
         __syncthreads();
-        // 2. the rows below the sub-panel inside the block: l_iq and w_iq (results held until every thread has read)
-        const int below = kb - (j0 + SUB);
-        constexpr int PER_THREAD = (BLOCK - SUB) * SUB / DIAGONAL_THREADS; // 3
-        double lValue[PER_THREAD];
-#pragma unroll
-        for (int u = 0; u < PER_THREAD; ++u)
+        // 2. the rows below the sub-panel: Y = A X_JJ^T (8-row tiles x 2 column halves), then L = Y / d and W = Y
+        const int below = BLOCK - (j0 + SUB);
+        const int g = lane >> 2;
+        const int tq = lane & 3;
+        const int warp = t >> 5;
+        constexpr int WARPS = DIAGONAL_THREADS / 32;
+        double y[2][2];
+        const int rowTasks = below / 8 * 2;
+        for (int u = 0; u < 2; ++u)
         {
-            const int e = t + u * DIAGONAL_THREADS;
-            const int i = j0 + SUB + e / SUB;
-            const int q = e % SUB;
-            lValue[u] = 0.0;
-            if (below > 0 && e < below * SUB && q < width)
+            const int task = warp + u * WARPS;
+            y[u][0] = 0.0;
+            y[u][1] = 0.0;
+            if (task >= rowTasks)
+                continue;
+            const int i0 = j0 + SUB + (task >> 1) * 8;
+            const int nn = (task & 1) * 8 + g;
+#pragma unroll
+            for (int ks = 0; ks < SUB; ks += 4)
             {
-                double sum = a[i + (j0 + q) * LD]; // X(q, q) = 1
-#pragma unroll 4
-                for (int p = 0; p < q; ++p)
-                    sum = fma(a[i + (j0 + p) * LD], a[(j0 + p) + (j0 + q) * LD], sum);
-                lValue[u] = sum / a[(j0 + q) + (j0 + q) * LD];
+                const int k = ks + tq;
+                const double fa = a[(i0 + g) + (j0 + k) * LD];
+                const double fb = nn > k ? a[(j0 + k) + (j0 + nn) * LD] : (nn == k ? 1.0 : 0.0);
+                dmma8x8x4(y[u], fa, fb);
             }
         }
         __syncthreads();
-#pragma unroll
-        for (int u = 0; u < PER_THREAD; ++u)
+        for (int u = 0; u < 2; ++u)
         {
-            const int e = t + u * DIAGONAL_THREADS;
-            const int i = j0 + SUB + e / SUB;
-            const int q = e % SUB;
-            if (below > 0 && e < below * SUB && q < width)
+            const int task = warp + u * WARPS;
+            if (task >= rowTasks)
+                continue;
+            const int i = j0 + SUB + (task >> 1) * 8 + g;
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
             {
-                a[i + (j0 + q) * LD] = lValue[u];
-                wRows[i * SUB + q] = lValue[u] * a[(j0 + q) + (j0 + q) * LD];
+                const int q = (task & 1) * 8 + 2 * tq + h;
+                a[i + (j0 + q) * LD] = y[u][h] / a[(j0 + q) + (j0 + q) * LD];
+                wRows[i * W_LD + q] = y[u][h];
             }
         }
         __syncthreads();
-        // 3. the trailing lower triangle of the block: a_ij -= sum_q l_iq w_jq
-        if (below > 0)
+        // 3. the trailing lower triangle, A -= L W^T by lower 8 x 8 tiles (each tile's terms in q order on its lanes)
+        const int tilesAcross = below / 8;
+        for (int task = warp; task < tilesAcross * (tilesAcross + 1) / 2; task += WARPS)
         {
-            for (int e = t; e < below * below; e += DIAGONAL_THREADS)
-            {
-                const int jj = e / below;
-                const int ii = e - jj * below;
-                if (ii < jj)
-                    continue;
-                const int i = j0 + SUB + ii;
-                const int j = j0 + SUB + jj;
-                double value = a[i + j * LD];
+            int ti = 0;
+            while ((ti + 1) * (ti + 2) / 2 <= task)
+                ++ti;
+            const int tj = task - ti * (ti + 1) / 2;
+            const int i0 = j0 + SUB + ti * 8;
+            const int c0 = j0 + SUB + tj * 8;
+            double acc[2] = {a[(i0 + g) + (c0 + 2 * tq) * LD], a[(i0 + g) + (c0 + 2 * tq + 1) * LD]};
 #pragma unroll
-                for (int q = 0; q < SUB; ++q)
-                    if (q < width)
-                        value = fma(-a[i + (j0 + q) * LD], wRows[j * SUB + q], value);
-                a[i + j * LD] = value;
+            for (int ks = 0; ks < SUB; ks += 4)
+            {
+                const int k = ks + tq;
+                dmma8x8x4(acc, -a[(i0 + g) + (j0 + k) * LD], wRows[(c0 + g) * W_LD + k]);
             }
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                if (i0 + g >= c0 + 2 * tq + h)
+                    a[(i0 + g) + (c0 + 2 * tq + h) * LD] = acc[h];
         }
         __syncthreads();
     }
-    // the inverse's off-diagonal 16 x 16 blocks by block diagonals, X_IJ = -X_II (sum_{J <= K < I} L_IK X_KJ)
+    // the inverse's off-diagonal 16 x 16 blocks by block diagonals: T_IJ = sum_{J <= K < I} L_IK X_KJ, then
+    // X_IJ = -X_II T_IJ (X stored transposed: X(i, j) at (j, i)); a task is one 8 x 8 quarter of a block
+    const int warp = t >> 5;
+    const int g = lane >> 2;
+    const int tq = lane & 3;
+    constexpr int WARPS = DIAGONAL_THREADS / 32;
 #pragma unroll 1
     for (int d = 1; d < BLOCK / SUB; ++d)
     {
-        const int count = (BLOCK / SUB - d) * SUB * SUB;
-        for (int e = t; e < count; e += DIAGONAL_THREADS) // T_IJ = sum_{J <= K < I} L_IK X_KJ
+        const int tasks = (BLOCK / SUB - d) * 4;
+        for (int task = warp; task < tasks; task += WARPS)
         {
-            const int b = e / (SUB * SUB);
-            const int p = (e / SUB) % SUB;
-            const int q = e % SUB;
-            const int jBase = b * SUB;
-            const int iRow = (b + d) * SUB + p;
-            double sum = a[iRow + (jBase + q) * LD]; // X_JJ(q, q) = 1
-#pragma unroll 1
-            for (int r = q + 1; r < SUB; ++r)
-                sum += a[iRow + (jBase + r) * LD] * a[(jBase + q) + (jBase + r) * LD];
-#pragma unroll 1
-            for (int kBase = jBase + SUB; kBase < (b + d) * SUB; kBase += SUB)
-#pragma unroll 4
-                for (int r = 0; r < SUB; ++r)
-                    sum += a[iRow + (kBase + r) * LD] * a[(jBase + q) + (kBase + r) * LD];
-            products[e] = sum;
+            const int b = task >> 2;
+            const int m0 = ((task >> 1) & 1) * 8;
+            const int nn = (task & 1) * 8 + g;
+            const int bj = b * SUB;
+            const int bi = (b + d) * SUB;
+            double acc[2] = {0.0, 0.0};
+            for (int bk = bj; bk < bi; bk += SUB)
+            {
+#pragma unroll
+                for (int ks = 0; ks < SUB; ks += 4)
+                {
+                    const int k = ks + tq;
+                    const double fa = a[(bi + m0 + g) + (bk + k) * LD];
+                    const double fb = bk > bj ? a[(bj + nn) + (bk + k) * LD]
+                                              : (k > nn ? a[(bj + nn) + (bj + k) * LD] : (k == nn ? 1.0 : 0.0));
+                    dmma8x8x4(acc, fa, fb);
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                products[b * P_BLOCK + (m0 + g) * P_LD + (task & 1) * 8 + 2 * tq + h] = acc[h];
         }
         __syncthreads();
-        for (int e = t; e < count; e += DIAGONAL_THREADS) // X_IJ = -X_II T_IJ
+        for (int task = warp; task < tasks; task += WARPS)
         {
-            const int b = e / (SUB * SUB);
-            const int p = (e / SUB) % SUB;
-            const int q = e % SUB;
-            const int iBase = (b + d) * SUB;
-            double sum = products[e];
-#pragma unroll 1
-            for (int r = 0; r < p; ++r)
-                sum += a[(iBase + r) + (iBase + p) * LD] * products[b * SUB * SUB + r * SUB + q];
-            a[(b * SUB + q) + (iBase + p) * LD] = -sum;
+            const int b = task >> 2;
+            const int m0 = ((task >> 1) & 1) * 8;
+            const int n0 = (task & 1) * 8;
+            const int bj = b * SUB;
+            const int bi = (b + d) * SUB;
+            const int m = m0 + g;
+            double acc[2] = {0.0, 0.0};
+#pragma unroll
+            for (int ks = 0; ks < SUB; ks += 4)
+            {
+                const int k = ks + tq;
+                const double fa = m > k ? a[(bi + k) + (bi + m) * LD] : (m == k ? 1.0 : 0.0);
+                dmma8x8x4(acc, fa, products[b * P_BLOCK + k * P_LD + n0 + g]);
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                a[(bj + n0 + 2 * tq + h) + (bi + m) * LD] = -acc[h];
         }
         __syncthreads();
     }
@@ -685,7 +719,8 @@ __global__ void __launch_bounds__(DIAGONAL_THREADS, 3) diagonalBlocks(FactorArgs
 
 // The rows below step k0's diagonal block, L21 = A21 L11^-T D^-1, as products on the FP64 tensor cores: for each
 // 64-row half of a task (64 * PANEL_ROW_HALVES rows), Y = A21 (L11^-1)^T with L11^-1 from the block's strict upper
-// triangle (unit diagonal), then l_ij = y_ij / d_j, written in place (a block stages its rows before it writes them).
+// triangle (unit diagonal), then l_ij = y_ij (1 / d_j), written in place (a block stages its rows before it writes
+// them). The inverse and the first rows arrive in one group of asynchronous copies.
 // Dynamic shared memory: PANEL_ROWS_INVERSE_SMEM bytes.
 __global__ void __launch_bounds__(TILE_THREADS) panelRowsInverse(FactorArgs args, const TileTask* tasks, int k0)
 {
@@ -713,12 +748,28 @@ __global__ void __launch_bounds__(TILE_THREADS) panelRowsInverse(FactorArgs args
         const bool inside = p <= jj && jj < kb;
         copyAsync8(sB + p * LD + jj, inside ? block + p + static_cast<std::int64_t>(jj) * n : block, inside);
     }
+    // The rows of a half into sA, as asynchronous copies (the first half's in flight with the inverse's).
+    const auto loadRows = [&](std::int64_t i0)
+    {
+        const int m = static_cast<int>(n - i0 < TILE ? n - i0 : TILE);
+        const double* rows = args.panels + f.panel + i0 + static_cast<std::int64_t>(k0) * n;
+        for (int e = tid; e < BLOCK * TILE; e += blockDim.x)
+        {
+            const int p = e / TILE;
+            const int ii = e - p * TILE;
+            const bool inside = p < kb && ii < m;
+            copyAsync8(sA + p * LD + ii, inside ? rows + ii + static_cast<std::int64_t>(p) * n : rows, inside);
+        }
+    };
+    if (task.i0 < n)
+        loadRows(task.i0);
     commitAsyncCopies();
     waitAsyncCopies<0>();
     __syncthreads();
+    // sd: 1 / d_j, applied as a product in the write-out
     for (int j = tid; j < BLOCK; j += blockDim.x)
     {
-        sd[j] = j < kb ? sB[j * LD + j] : 1.0;
+        sd[j] = j < kb ? 1.0 / sB[j * LD + j] : 1.0;
         sB[j * LD + j] = j < kb ? 1.0 : 0.0;
     }
     for (int half = 0; half < PANEL_ROW_HALVES; ++half)
@@ -728,15 +779,12 @@ __global__ void __launch_bounds__(TILE_THREADS) panelRowsInverse(FactorArgs args
             break;
         const int m = static_cast<int>(n - i0 < TILE ? n - i0 : TILE);
         double* rows = args.panels + f.panel + i0 + static_cast<std::int64_t>(k0) * n;
-        for (int e = tid; e < BLOCK * TILE; e += blockDim.x)
+        if (half > 0)
         {
-            const int p = e / TILE;
-            const int ii = e - p * TILE;
-            const bool inside = p < kb && ii < m;
-            copyAsync8(sA + p * LD + ii, inside ? rows + ii + static_cast<std::int64_t>(p) * n : rows, inside);
+            loadRows(i0);
+            commitAsyncCopies();
+            waitAsyncCopies<0>();
         }
-        commitAsyncCopies();
-        waitAsyncCopies<0>();
         __syncthreads();
         double acc[4][4][2];
 #pragma unroll
@@ -775,7 +823,7 @@ __global__ void __launch_bounds__(TILE_THREADS) panelRowsInverse(FactorArgs args
                     const int ii = wm + mi * 8 + (lane >> 2);
                     const int jj = wn + ni * 8 + (lane & 3) * 2 + h;
                     if (ii < m && jj < kb)
-                        rows[ii + static_cast<std::int64_t>(jj) * n] = acc[mi][ni][h] / sd[jj];
+                        rows[ii + static_cast<std::int64_t>(jj) * n] = acc[mi][ni][h] * sd[jj];
                 }
         __syncthreads();
     }

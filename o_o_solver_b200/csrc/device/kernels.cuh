@@ -34,8 +34,29 @@ struct PivotArgs
     std::int32_t* stepSwapped; // per supernode: the current step's diagonal block interchanged columns
     double* w;                 // W = L D of the current step's rows, n x 64 per large front at wOffset
     const std::int64_t* wOffset;
-    std::int32_t* frontPerm;   // scratch of the exact path (one front at a time)
-    double* frontSub;
+};
+
+// A source of an exact front's assembly: a child's update matrix (order x order, lower triangle, column-major) and
+// the front position of each of its rows.
+struct FrontSource
+{
+    const double* values;
+    const std::int32_t* positions;
+    std::int32_t order;
+    std::int32_t unused;
+};
+
+// One front of the exact path: its order (candidates, then its rows R(s)), its candidates (its c columns, then the
+// columns its children delayed), its sources (children in increasing order) and where its panel goes (order x
+// candidates, leading dimension order).
+struct ExactFront
+{
+    std::int32_t supernode;
+    std::int32_t order;
+    std::int32_t candidates;
+    std::int32_t sourceCount;
+    const FrontSource* sources;
+    double* panel;
 };
 
 struct SolveArgs
@@ -130,6 +151,7 @@ __global__ void pivotSummary(FactorArgs args, const std::int32_t* supernodeOfCol
                              const double* referenceDiagonal, double maxRatio, unsigned long long* counters,
                              std::int32_t* issues, int issueCapacity, double* blockRatio, std::int32_t* blockEquation);
 __global__ void forwardSmall(SolveArgs a, const std::int32_t* list, int cmax);
+__global__ void gatherColumns(SolveArgs a, std::int32_t s);
 __global__ void forwardGather(SolveArgs a, const TileTask* tasks);
 __global__ void invertDiagonal(FactorArgs args, const TileTask* tasks);
 // Dynamic shared memory of forwardDiagonal / backwardDiagonal: the tile pipeline, one block's inverse and a 64-row block
@@ -194,12 +216,13 @@ __global__ void smallFrontsPivoted(FactorArgs args, PivotArgs pivots, const std:
                                    std::int32_t* structureError);
 __global__ void pivotedDiagonal(FactorArgs args, PivotArgs pivots, const std::int32_t* list, int k0);
 __global__ void permuteEarlierRows(FactorArgs args, PivotArgs pivots, const TileTask* tasks, int k0);
-__global__ void panelRowsPivoted(FactorArgs args, PivotArgs pivots, const TileTask* tasks, int k0);
 __global__ void panelRowsPivotedInverse(FactorArgs args, PivotArgs pivots, const TileTask* tasks, int k0);
 constexpr std::size_t PANEL_ROWS_PIVOTED_SMEM = PANEL_ROWS_INVERSE_SMEM + 64 * (sizeof(double) + sizeof(int));
 __global__ void updatePivoted(FactorArgs args, PivotArgs pivots, const TileTask* tasks, int k0);
-__global__ void pivotedFront(FactorArgs args, PivotArgs pivots, std::int32_t s, double* work,
-                             std::int32_t* structureError);
+__global__ void exactFront(FactorArgs args, ExactFront x, double* work, std::int32_t* perm, double* sub,
+                           std::int32_t* eliminated, std::int32_t* structureError);
+__global__ void copyTrailing(const double* work, std::int64_t ld, int from, int count, double* update);
+__global__ void trailingFront(FactorArgs args, ExactFront x, double* schur, std::int32_t* structureError);
 __global__ void inertiaPivoted(FactorArgs args, PivotArgs pivots, const std::int32_t* supernodeOfColumn, int dimension,
                                unsigned long long* counters);
 __global__ void identityPermutation(std::int32_t* perm, int dimension);

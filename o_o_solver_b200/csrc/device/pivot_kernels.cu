@@ -6,20 +6,22 @@
 //   alpha = (1 + sqrt 17) / 8, a candidate whose column maximum lies outside the candidates taken as a 1x1 pivot when
 //   |a_kk| >= 0.01 colmax and delayed otherwise, ties of the maxima to the first index. It runs on a whole small front
 //   in shared memory (smallFrontsPivoted), on a large front's diagonal block (pivotedDiagonal), and on a whole front
-//   in global memory (pivotedFront, the exact path of a front the block path refuses).
-//   Where the reference would delay a candidate to the parent front (its passes make no progress), the GPU path takes
-//   it in place as a 1x1 pivot when |a_kk| >= 1e-3 colmax (a "forced" pivot: the growth of its column of L at most
-//   1e3, ten times the reference's bound, so the factor stays backward stable and its inertia, by Sylvester's law, is
-//   the reference's); below that the factorisation is refused. The fronts keep their symbolic sizes.
+//   in global memory (exactFront, the exact path of a front the block path refuses, or that delays, or grows).
+//   The candidates its passes cannot pivot are delayed to the parent front, as the reference delays them
+//   (MultifrontalDriver.cpp:346-436): a front that delays is refactorised by the exact path (exactFront), which
+//   leaves the delayed candidates in its update matrix; its parent is assembled with them as extra candidate columns
+//   (a grown front) by the exact path too.
 // - large fronts, per 64-column block: Bunch-Kaufman inside the diagonal block (its columns are all candidates and its
 //   rows the only ones searched), then the rows below solved against it (L = A L11^-T D^-1, 2x2 blocks by the dsytf2
 //   formula) with an a-posteriori threshold test |l_ij| <= 1/u, u = 0.01 (the reference's delay threshold), and the
 //   trailing front updated by tile products C -= L W^T with W = L D. A front whose test fails is refactorised by the
 //   exact path. The pivots may differ from the reference's, the inertia may not (Sylvester's law): every Sturm count
 //   is the reference's.
-// - the pivot order: every supernode permutes only its own columns (no delayed pivot crosses a front), so the factor
-//   is P A P^T = L D L^T with P a permutation within each supernode's columns; the solves run in pivot order on the
-//   same kernels, with the maps of rows remapped (remapPivotOrder) and 2x2 blocks in the diagonal sweep.
+// - the pivot order: without delays every supernode permutes only its own columns, so the factor is P A P^T = L D L^T
+//   with P a permutation within each supernode's columns; the solves run in pivot order on the same kernels, with the
+//   maps of rows remapped (remapPivotOrder) and 2x2 blocks in the diagonal sweep. With delays the host restates the
+//   structure in the order the equations were eliminated (each supernode's eliminated columns, its delayed candidates
+//   among its rows) and the same solve kernels run on that.
 
 #include "assembly.cuh"
 #include "kernels.cuh"
@@ -34,7 +36,6 @@ namespace
 
 constexpr double BK_ALPHA = 0.6403882032022076;  // (1 + sqrt(17)) / 8
 constexpr double DELAY_THRESHOLD = 0.01;          // the reference's DELAYED_PIVOT_THRESHOLD
-constexpr double FORCED_THRESHOLD = 1.0e-3;       // a candidate the reference would delay, taken in place
 constexpr double GROWTH_LIMIT = 1.0 / DELAY_THRESHOLD;
 
 // The column maximum |a(i, k)| over i in (k, n) and its first row, on the whole block (ties to the first index).
@@ -154,18 +155,18 @@ __device__ __forceinline__ TwoByTwoInverse invertTwoByTwo(double a, double b, do
 {
     const double d11 = c / b;
     const double d22 = a / b;
-    const double t = 1.0 / (d11 * d22 - 1.0);
+    const double t = 1.0 / __dsub_rn(__dmul_rn(d11, d22), 1.0);
     return {d11, d22, t / b};
 }
 
 // Bunch-Kaufman on the block `at` (n x n lower, the first `candidates` columns the candidates) by the whole thread
 // block. perm: the block positions' origins (permuted with the interchanges); subdiagonal: e_k of each 2x2 pivot at its
-// first column, 0 elsewhere. With allowForced, the candidates left when a pass makes no progress get one more pass at
-// the forced threshold; `forced` (when given) receives the pivots taken below the delay threshold. Returns the columns
-// eliminated (< candidates when some were delayed).
+// first column, 0 elsewhere. A candidate whose column maximum lies outside the untried candidates and whose diagonal is
+// below DELAY_THRESHOLD of it is moved behind them and retried in the next pass, as long as a pass eliminates
+// something. Returns the columns eliminated; positions [eliminated, candidates) then hold the delayed candidates.
 template <typename At>
 __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* subdiagonal, double* scratchValue,
-                            int* scratchIndex, bool allowForced, int* forced)
+                            int* scratchIndex)
 {
     for (int i = threadIdx.x; i < candidates; i += blockDim.x)
     {
@@ -176,8 +177,6 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
     int k = 0;
     int end = candidates;
     int passStart = 0;
-    double threshold = DELAY_THRESHOLD;
-    int forcedCount = 0;
     while (true)
     {
         while (k < end)
@@ -195,7 +194,7 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
             int swapWith = k;
             if (absakk < BK_ALPHA * colmax && imax >= end)
             {
-                if (absakk < threshold * colmax)
+                if (absakk < DELAY_THRESHOLD * colmax)
                 {
                     --end;
                     if (k != end)
@@ -211,8 +210,6 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
                     }
                     continue;
                 }
-                if (absakk < DELAY_THRESHOLD * colmax)
-                    ++forcedCount;
             }
             else if (absakk < BK_ALPHA * colmax)
             {
@@ -239,6 +236,8 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
                 }
                 __syncthreads();
             }
+            // Every product and difference rounded on its own (no fused multiply-adds), in the reference family's
+            // order: the same bits as its unblocked kernel on the same front.
             if (blockSize == 1)
             {
                 const double pivot = at(k, k);
@@ -250,9 +249,9 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
                 const int lane = threadIdx.x & 31;
                 for (int j = k + 1 + warp; j < n; j += warps)
                 {
-                    const double w = at(j, k) * pivot;
+                    const double w = __dmul_rn(at(j, k), pivot);
                     for (int i = j + lane; i < n; i += 32)
-                        at(i, j) -= at(i, k) * w;
+                        at(i, j) = __dsub_rn(at(i, j), __dmul_rn(at(i, k), w));
                 }
                 __syncthreads();
             }
@@ -267,8 +266,8 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
                 {
                     const double r0 = at(i, k);
                     const double r1 = at(i, k + 1);
-                    at(i, k) = inverse.s * (inverse.d11 * r0 - r1);
-                    at(i, k + 1) = inverse.s * (inverse.d22 * r1 - r0);
+                    at(i, k) = __dmul_rn(inverse.s, __dsub_rn(__dmul_rn(inverse.d11, r0), r1));
+                    at(i, k + 1) = __dmul_rn(inverse.s, __dsub_rn(__dmul_rn(inverse.d22, r1), r0));
                 }
                 if (threadIdx.x == 0)
                 {
@@ -281,13 +280,13 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
                 const int lane = threadIdx.x & 31;
                 for (int j = k + 2 + warp; j < n; j += warps)
                 {
-                    const double w0 = at(j, k) * d0 + at(j, k + 1) * e;
-                    const double w1 = at(j, k) * e + at(j, k + 1) * d1;
+                    const double w0 = __dadd_rn(__dmul_rn(at(j, k), d0), __dmul_rn(at(j, k + 1), e));
+                    const double w1 = __dadd_rn(__dmul_rn(at(j, k), e), __dmul_rn(at(j, k + 1), d1));
                     for (int i = j + lane; i < n; i += 32)
                     {
                         double v = at(i, j);
-                        v -= at(i, k) * w0;
-                        v -= at(i, k + 1) * w1;
+                        v = __dsub_rn(v, __dmul_rn(at(i, k), w0));
+                        v = __dsub_rn(v, __dmul_rn(at(i, k + 1), w1));
                         at(i, j) = v;
                     }
                 }
@@ -295,19 +294,12 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
             }
             k += blockSize;
         }
-        if (end == candidates)
+        // the delayed candidates get another pass after this one's pivots, as long as a pass eliminates something
+        if (end == candidates || k == passStart)
             break;
-        if (k == passStart)
-        {
-            if (!allowForced || threshold == FORCED_THRESHOLD)
-                break;
-            threshold = FORCED_THRESHOLD;
-        }
         passStart = k;
         end = candidates;
     }
-    if (forced != nullptr && threadIdx.x == 0)
-        *forced = forcedCount;
     return k;
 }
 
@@ -356,7 +348,8 @@ struct GlobalAt
 // ------------------------------------------------------------------------------------------------------------------
 // Small fronts, indefinite: assembled in shared memory as smallFronts does, then Bunch-Kaufman on the c candidates;
 // the panel (pivot order), the 2x2 subdiagonals, the permutation of the supernode's columns and the update matrix
-// written out. A front that delays a pivot is flagged (status bit 2).
+// written out. A front that delays a pivot is flagged (status bit 2, the columns it eliminated from bit 8) and
+// refactorised by the exact path, which keeps the delayed candidates.
 // ------------------------------------------------------------------------------------------------------------------
 __global__ void smallFrontsPivoted(FactorArgs args, PivotArgs pivots, const std::int32_t* list,
                                    std::int32_t* structureError)
@@ -372,15 +365,9 @@ __global__ void smallFrontsPivoted(FactorArgs args, PivotArgs pivots, const std:
     const int ld = n + 1;
     assembleFrontBy(
         args, f, [&](int i, int j) -> double& { return front[i + j * ld]; }, structureError);
-    __shared__ int forced;
-    const int eliminated = bunchKaufman(SharedAt{front, ld}, n, f.c, perm, sub, scratchValue, scratchIndex, true, &forced);
-    if (threadIdx.x == 0)
-    {
-        if (eliminated < f.c)
-            atomicOr(pivots.status + s, 2 | (min(eliminated, 0xfffff) << 8));
-        else if (forced > 0)
-            atomicOr(pivots.status + s, 4 | (min(forced, 0xfffff) << 8));
-    }
+    const int eliminated = bunchKaufman(SharedAt{front, ld}, n, f.c, perm, sub, scratchValue, scratchIndex);
+    if (threadIdx.x == 0 && eliminated < f.c)
+        atomicOr(pivots.status + s, 2 | (min(eliminated, 0xfffff) << 8));
     double* panel = args.panels + f.panel;
     for (int e = threadIdx.x; e < n * f.c; e += blockDim.x)
     {
@@ -409,7 +396,7 @@ __global__ void smallFrontsPivoted(FactorArgs args, PivotArgs pivots, const std:
 // ------------------------------------------------------------------------------------------------------------------
 // Large fronts, indefinite, step k0: Bunch-Kaufman inside the kb x kb diagonal block. The block's interchanges are
 // carried to the supernode's permutation and to the rows of L already computed (columns before k0); the rows below
-// the block take them when panelRowsPivoted reads them (pivots.stepPerm).
+// the block take them when panelRowsPivotedInverse reads them (pivots.stepPerm).
 // ------------------------------------------------------------------------------------------------------------------
 __global__ void pivotedDiagonal(FactorArgs args, PivotArgs pivots, const std::int32_t* list, int k0)
 {
@@ -436,7 +423,7 @@ __global__ void pivotedDiagonal(FactorArgs args, PivotArgs pivots, const std::in
     waitAsyncCopies<0>();
     __syncthreads();
     // A candidate the block cannot pivot sends the front to the exact path (status bit 1), as a failed growth test.
-    const int eliminated = bunchKaufman(SharedAt{a, LD}, kb, kb, perm, sub, scratchValue, scratchIndex, false, nullptr);
+    const int eliminated = bunchKaufman(SharedAt{a, LD}, kb, kb, perm, sub, scratchValue, scratchIndex);
     if (eliminated < kb && threadIdx.x == 0)
         atomicOr(pivots.status + s, 1);
     for (int e = threadIdx.x; e < kb * kb; e += blockDim.x)
@@ -656,86 +643,6 @@ __global__ void identityPermutation(std::int32_t* perm, int dimension)
         perm[j] = j;
 }
 
-// The rows below the diagonal block of step k0, one thread each: the row's entries in the block's columns read in
-// pivot order, Y = A L11^-T (the unit lower block from pivotedDiagonal), L = Y D^-1 (2x2 blocks by the dsytf2 formula),
-// L written to the panel and W = L D = Y to the front's W buffer; a coefficient above 1/u (or not finite) flags the
-// front (status bit 1).
-__global__ void __launch_bounds__(128) panelRowsPivoted(FactorArgs args, PivotArgs pivots, const TileTask* tasks,
-                                                        int k0)
-{
-    constexpr int B = 64;
-    __shared__ double l11[B * B]; // l11[j * B + q] = L(k0 + j, k0 + q), q < j
-    __shared__ double d[B];
-    __shared__ double e[B];
-    __shared__ int perm[B];
-    const TileTask task = tasks[blockIdx.x];
-    const std::int32_t s = task.front;
-    const FrontDesc f = args.fronts[s];
-    const std::int64_t n = f.c + f.r;
-    const int kb = min(B, f.c - k0);
-    const double* block = args.panels + f.panel + k0 + k0 * n;
-    for (int x = threadIdx.x; x < B * B; x += blockDim.x)
-    {
-        const int j = x / B;
-        const int q = x - j * B;
-        l11[x] = j < kb && q < j ? block[j + static_cast<std::int64_t>(q) * n] : 0.0;
-    }
-    for (int j = threadIdx.x; j < B; j += blockDim.x)
-    {
-        d[j] = j < kb ? block[j + static_cast<std::int64_t>(j) * n] : 1.0;
-        e[j] = j < kb ? pivots.subdiagonal[f.first + k0 + j] : 0.0;
-        perm[j] = j < kb ? pivots.stepPerm[static_cast<std::int64_t>(s) * B + j] : j;
-    }
-    __syncthreads();
-    const std::int64_t row = task.i0 + threadIdx.x;
-    if (row >= n)
-        return;
-    double* base = args.panels + f.panel + k0 * n + row;
-    double y[B];
-#pragma unroll
-    for (int j = 0; j < B; ++j)
-        y[j] = j < kb ? base[static_cast<std::int64_t>(perm[j]) * n] : 0.0;
-#pragma unroll
-    for (int j = 1; j < B; ++j)
-    {
-        double v = y[j];
-#pragma unroll
-        for (int q = 0; q < j; ++q)
-            v -= y[q] * l11[j * B + q];
-        y[j] = v;
-    }
-    double* w = pivots.w + pivots.wOffset[s] + row + static_cast<std::int64_t>(k0 % PANEL_MACRO) * n;
-    bool bad = false;
-    int j = 0;
-    while (j < kb)
-    {
-        if (j + 1 < kb && e[j] != 0.0)
-        {
-            const TwoByTwoInverse inverse = invertTwoByTwo(d[j], e[j], d[j + 1]);
-            const double r0 = y[j];
-            const double r1 = y[j + 1];
-            const double l0 = inverse.s * (inverse.d11 * r0 - r1);
-            const double l1 = inverse.s * (inverse.d22 * r1 - r0);
-            base[static_cast<std::int64_t>(j) * n] = l0;
-            base[static_cast<std::int64_t>(j + 1) * n] = l1;
-            w[static_cast<std::int64_t>(j) * n] = r0;
-            w[static_cast<std::int64_t>(j + 1) * n] = r1;
-            bad = bad || !(fabs(l0) <= GROWTH_LIMIT) || !(fabs(l1) <= GROWTH_LIMIT);
-            j += 2;
-        }
-        else
-        {
-            const double l = y[j] / d[j];
-            base[static_cast<std::int64_t>(j) * n] = l;
-            w[static_cast<std::int64_t>(j) * n] = y[j];
-            bad = bad || !(fabs(l) <= GROWTH_LIMIT);
-            j += 1;
-        }
-    }
-    if (bad)
-        atomicOr(pivots.status + s, 1);
-}
-
 // A tile of the trailing front minus L W^T over the K = task.k0 columns from k0 (a step's columns within its macro
 // panel, or a finished macro panel's): task (front, i0, j0) a 64 x 64 tile of the front, j0 < c in the panel, j0 >= c
 // in the update matrix (tiles never straddle c); W's columns for k0 at slice k0 % PANEL_MACRO of the front's buffer.
@@ -778,51 +685,141 @@ __global__ void __launch_bounds__(TILE_THREADS) updatePivoted(FactorArgs args, P
 }
 
 // ------------------------------------------------------------------------------------------------------------------
-// The exact path of one front (a front the block path refused): assembled whole in `work` (n x n, global memory),
-// Bunch-Kaufman on its candidates by one block, then the panel, the permutation, the subdiagonals and the update
-// matrix written out as smallFrontsPivoted writes them.
+// The exact path of one front (the reference's eliminatePivoted, MultifrontalDriver.cpp:346-436): a front the block
+// path refused, a small front that delays pivots, or a front grown by its children's delayed columns. Assembled whole
+// in `work` (order x order, global memory; FrontAssembly.cpp:166-300 with delays): its c columns, then the candidate
+// columns its children delayed, then its rows R(s); the matrix's entries of its c columns, then each child's update
+// matrix in increasing child order at the front positions the host mapped (a delayed child's rows start with its
+// delayed columns, whose positions may lie above another row's: such a term lands in the lower triangle, transposed).
+// Then Bunch-Kaufman on the candidates by one block; the panel (order x candidates, pivot order) written to x.panel,
+// the permutation of the candidates (front positions), their subdiagonals and the count eliminated to the scratch;
+// the update matrix stays in `work`, at [eliminated, order), for copyTrailing.
 // ------------------------------------------------------------------------------------------------------------------
-__global__ void pivotedFront(FactorArgs args, PivotArgs pivots, std::int32_t s, double* work,
-                             std::int32_t* structureError)
+// The whole front of x assembled by one block into at(i, j) (i >= j, order x order): cleared, the matrix's entries of
+// its c columns (rows in the columns, or in R(s) after the candidates), then each source's update matrix at its rows'
+// front positions in increasing source order (a term whose positions are out of order lands transposed).
+template <typename At>
+__device__ void assembleWholeFront(const FactorArgs& args, const ExactFront& x, At at, std::int32_t* structureError)
+{
+    const FrontDesc f = args.fronts[x.supernode];
+    const int order = x.order;
+    const int candidates = x.candidates;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int warps = blockDim.x >> 5;
+    for (std::int64_t e = tid; e < static_cast<std::int64_t>(order) * order; e += blockDim.x)
+    {
+        const int j = static_cast<int>(e / order);
+        const int i = static_cast<int>(e - static_cast<std::int64_t>(j) * order);
+        if (i >= j)
+            at(i, j) = 0.0;
+    }
+    __syncthreads();
+    const std::int32_t* rowsOfFront = args.rows + f.rowStart;
+    for (int j = warp; j < f.c; j += warps)
+    {
+        const std::int32_t column = f.first + j;
+        for (std::int64_t k = args.colOffsets[column] + lane; k < args.colOffsets[column + 1]; k += 32)
+        {
+            const std::int32_t row = args.colRows[k];
+            int position = -1;
+            if (row >= column && row < f.first + f.c)
+                position = row - f.first;
+            else if (row >= f.first + f.c)
+            {
+                int lo = 0;
+                int hi = f.r;
+                while (lo < hi)
+                {
+                    const int mid = (lo + hi) >> 1;
+                    if (rowsOfFront[mid] < row)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                if (lo < f.r && rowsOfFront[lo] == row)
+                    position = candidates + lo;
+            }
+            if (position < 0)
+            {
+                atomicMin(structureError, column);
+                continue;
+            }
+            at(position, j) += args.colValues[k];
+        }
+    }
+    __syncthreads();
+    for (int q = 0; q < x.sourceCount; ++q)
+    {
+        const FrontSource source = x.sources[q];
+        for (int jc = warp; jc < source.order; jc += warps)
+        {
+            const int pj = source.positions[jc];
+            const double* column = source.values + static_cast<std::int64_t>(jc) * source.order;
+            for (int ic = jc + lane; ic < source.order; ic += 32)
+            {
+                const int pi = source.positions[ic];
+                if (pi >= pj)
+                    at(pi, pj) += column[ic];
+                else
+                    at(pj, pi) += column[ic];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void exactFront(FactorArgs args, ExactFront x, double* work, std::int32_t* perm, double* sub,
+                           std::int32_t* eliminated, std::int32_t* structureError)
 {
     __shared__ double scratchValue[32];
     __shared__ int scratchIndex[32];
-    const FrontDesc f = args.fronts[s];
-    const int n = f.c + f.r;
-    const std::int64_t ld = n;
-    assembleFrontBy(
-        args, f, [&](int i, int j) -> double& { return work[i + static_cast<std::int64_t>(j) * ld]; },
-        structureError);
-    int* perm = pivots.frontPerm;
-    double* sub = pivots.frontSub;
-    __shared__ int forced;
-    const int eliminated = bunchKaufman(GlobalAt{work, ld}, n, f.c, perm, sub, scratchValue, scratchIndex, true, &forced);
-    if (threadIdx.x == 0)
-        pivots.status[s] = eliminated < f.c ? 2 | (min(eliminated, 0xfffff) << 8)
-                                            : (forced > 0 ? 4 | (min(forced, 0xfffff) << 8) : 0);
-    double* panel = args.panels + f.panel;
-    for (std::int64_t x = threadIdx.x; x < static_cast<std::int64_t>(n) * f.c; x += blockDim.x)
+    const int order = x.order;
+    const int candidates = x.candidates;
+    const std::int64_t ld = order;
+    const int tid = threadIdx.x;
+    const auto at = [&](int i, int j) -> double& { return work[i + static_cast<std::int64_t>(j) * ld]; };
+    assembleWholeFront(args, x, at, structureError);
+    const int done = bunchKaufman(GlobalAt{work, ld}, order, candidates, perm, sub, scratchValue, scratchIndex);
+    if (tid == 0)
+        *eliminated = done;
+    for (std::int64_t e = tid; e < static_cast<std::int64_t>(order) * candidates; e += blockDim.x)
     {
-        const std::int64_t j = x / n;
-        const std::int64_t i = x - j * n;
-        panel[x] = i >= j ? work[i + j * ld] : 0.0;
+        const std::int64_t j = e / order;
+        const std::int64_t i = e - j * order;
+        x.panel[e] = i >= j ? at(static_cast<int>(i), static_cast<int>(j)) : 0.0;
     }
-    for (int j = threadIdx.x; j < f.c; j += blockDim.x)
+}
+
+// The trailing front of a partial factorisation (the reference's PartialFactor: the front of the trailing supernode,
+// assembled from the matrix's boundary entries and its children's update matrices, is K* itself): assembled whole
+// by one block into `schur` (order x order, column-major), then its upper triangle mirrored from the lower.
+__global__ void trailingFront(FactorArgs args, ExactFront x, double* schur, std::int32_t* structureError)
+{
+    const std::int64_t ld = x.order;
+    const auto at = [&](int i, int j) -> double& { return schur[i + static_cast<std::int64_t>(j) * ld]; };
+    assembleWholeFront(args, x, at, structureError);
+    for (std::int64_t e = threadIdx.x; e < ld * ld; e += blockDim.x)
     {
-        pivots.perm[f.first + j] = f.first + perm[j];
-        pivots.subdiagonal[f.first + j] = sub[j];
+        const std::int64_t j = e / ld;
+        const std::int64_t i = e - j * ld;
+        if (i < j)
+            schur[e] = schur[j + i * ld];
     }
-    if (f.r > 0)
-    {
-        double* update = args.updates + f.update;
-        for (std::int64_t x = threadIdx.x; x < static_cast<std::int64_t>(f.r) * f.r; x += blockDim.x)
-        {
-            const std::int64_t j = x / f.r;
-            const std::int64_t i = x - j * f.r;
-            if (i >= j)
-                update[x] = work[(f.c + i) + (f.c + j) * ld];
-        }
-    }
+}
+
+// The update matrix an exact front leaves to its parent: the lower triangle of work's trailing block from position
+// `from` (count x count, column-major) into `update`.
+__global__ void copyTrailing(const double* work, std::int64_t ld, int from, int count, double* update)
+{
+    const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= static_cast<std::int64_t>(count) * count)
+        return;
+    const std::int64_t j = e / count;
+    const std::int64_t i = e - j * count;
+    if (i >= j)
+        update[e] = work[(from + i) + (from + j) * ld];
 }
 
 // ------------------------------------------------------------------------------------------------------------------
@@ -953,8 +950,8 @@ __global__ void diagonalSweepPivoted(SolveArgs a, const std::int32_t* supernodeO
             invertTwoByTwo(panel[k + k * n], subdiagonal[j], panel[(k + 1) + (k + 1) * n]);
         const double r0 = x[0];
         const double r1 = x[w];
-        x[0] = inverse.s * (inverse.d11 * r0 - r1);
-        x[w] = inverse.s * (inverse.d22 * r1 - r0);
+        x[0] = __dmul_rn(inverse.s, __dsub_rn(__dmul_rn(inverse.d11, r0), r1));
+        x[w] = __dmul_rn(inverse.s, __dsub_rn(__dmul_rn(inverse.d22, r1), r0));
         return;
     }
     x[0] = x[0] / panel[k + k * n];

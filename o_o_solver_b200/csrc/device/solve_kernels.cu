@@ -243,6 +243,26 @@ __global__ void __launch_bounds__(TILE_THREADS) forwardSmall(SolveArgs a, const 
     }
 }
 
+// The children's update rows gathered into the columns of supernode s, one thread per value, the children in
+// increasing order (forwardGather's sums): the forward sweep's first step of a supernode whose elimination is left
+// out (the trailing supernode of a partial factorisation, whose columns then hold f* = f_b - K_bi K_ii^-1 f_i).
+__global__ void gatherColumns(SolveArgs a, std::int32_t s)
+{
+    const FrontDesc f = a.fronts[s];
+    const int w = a.width;
+    const std::int64_t e = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= static_cast<std::int64_t>(f.c) * w)
+        return;
+    const int p = static_cast<int>(e / w);
+    const int col = static_cast<int>(e - static_cast<std::int64_t>(p) * w);
+    const std::int64_t slot = columnSlot(a, f, p);
+    double* x = a.x + static_cast<std::int64_t>(f.first + p) * w + col;
+    double value = *x;
+    for (std::int64_t q = a.gatherStart[slot]; q < a.gatherStart[slot + 1]; ++q)
+        value += a.updates[static_cast<std::int64_t>(a.gatherRows[q]) * w + col];
+    *x = value;
+}
+
 // The children's update rows of a large supernode, for the front positions [i0, j0) of a task (at most 64): added into
 // X's rows of its columns (in place) and into its own update rows (which they set), by the gather lists (gatherTile):
 // every value one thread, the children in increasing order, so every sum is the same whatever the split. One block

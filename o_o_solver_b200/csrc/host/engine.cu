@@ -6,6 +6,7 @@
 // launch of a factorisation or a solve on its own stream; a factorisation reads back only its pivot summary.
 
 #include "../device/kernels.cuh"
+#include "delayed.hpp"
 #include "factor_internal.hpp"
 #include "host_api.hpp"
 #include "spectrum.hpp"
@@ -293,10 +294,19 @@ public:
     [[nodiscard]] cudaStream_t stream() const noexcept { return m_stream; }
     [[nodiscard]] const Plan& plan() const noexcept { return m_plan; }
 
+    // trailing > 0: the partial factorisation (PartialFactor::factorise): every supernode below the trailing one
+    // (the last supernode: the trailing set's equations, a root alone in its level, no rows below) factorised in
+    // positive definite mode; its front, assembled from the matrix's boundary entries and its children's update
+    // matrices, is K* = K_bb - K_bi K_ii^-1 K_ib, written to `schur` (host, trailing x trailing, both triangles).
     void factorise(std::int32_t dimension, std::int64_t terms, const std::int64_t* offsets, const std::int32_t* rows,
-                   const double* values, bool onDevice, const oosgpu_factor_options* options, oosgpu_factor_info* info)
+                   const double* values, bool onDevice, const oosgpu_factor_options* options, oosgpu_factor_info* info,
+                   std::int32_t trailing = 0, double* schur = nullptr)
     {
         check(cudaSetDevice(m_device), "cudaSetDevice");
+        m_partialLevel = -1;
+        m_isPartial = false;
+        if (trailing != 0)
+            preparePartial(dimension, trailing, options);
         if (dimension != m_plan.dimension)
             throw Error(STATUS_INVALID_ARGUMENT,
                         "supernodal factorisation: the matrix has " + std::to_string(dimension) +
@@ -386,7 +396,9 @@ public:
             throw Error(STATUS_INVALID_ARGUMENT, "FactorOptions: precision must be 0 (FP64) or 1 (mixed), found " +
                                                      std::to_string(options->precision));
         check(cudaMemsetAsync(m_mixedError.get(), 0, sizeof(int), m_stream), "memset"); // tcgen05 and TMA waits
-        const unsigned summaryBlocks = blocksFor(std::max(dimension, 1), 256);
+        // the equations the pivot summary covers: all of them, or the interior of a partial factorisation
+        const std::int32_t summarised = m_partialLevel >= 0 ? dimension - m_trailing : dimension;
+        const unsigned summaryBlocks = blocksFor(std::max(summarised, 1), 256);
         const auto launches = [&]
         {
             // the pivot summary's counters from zero in every run of the sequence (the autotuner's timing runs, the
@@ -394,11 +406,11 @@ public:
             check(cudaMemsetAsync(m_counters.get(), 0, 8 * sizeof(unsigned long long), m_stream), "memset");
             runFactorLaunches(args);
             invertDiagonalBlocks(args, false);
-            device::pivotSummary<<<summaryBlocks, 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), dimension,
+            device::pivotSummary<<<summaryBlocks, 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), summarised,
                                                                        referenceDiagonal, maxRatio, m_counters.get(),
                                                                        m_issues.get(), ISSUE_CAPACITY,
                                                                        m_blockRatio.get(), m_blockEquation.get());
-            device::gatherDiagonal<<<summaryBlocks, 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), dimension,
+            device::gatherDiagonal<<<summaryBlocks, 256, 0, m_stream>>>(args, m_supernodeOfColumn.get(), summarised,
                                                                          m_diagonal.get());
             check(cudaGetLastError(), "pivot summary launch");
         };
@@ -414,7 +426,7 @@ public:
             m_factorGraph.run(m_stream,
                               {keyOf(dOffsets), keyOf(dRows), keyOf(dValues), keyOf(referenceDiagonal),
                                static_cast<std::uintptr_t>(ratioBits), static_cast<std::uintptr_t>(m_mixed),
-                               static_cast<std::uintptr_t>(dimension)},
+                               static_cast<std::uintptr_t>(dimension), static_cast<std::uintptr_t>(m_partialLevel + 1)},
                               launches);
         }
         check(cudaEventRecord(m_stop, m_stream), "event");
@@ -519,13 +531,151 @@ public:
             throw Error(STATUS_SINGULAR, "the ratio test flagged " + std::to_string(result.issue_count) +
                                              " pivots (MaxDiagonalRatio " + std::to_string(maxRatio) +
                                              "; the first at equation " + std::to_string(result.issues[0]) + ")");
+        if (m_partialLevel >= 0)
+            trailingComplement(args, schur);
         m_factorised = true;
     }
 
+    // The checks of a partial factorisation and its launch filter: the last supernode holds the trailing equations
+    // (the last `trailing` ones), has no rows below and no other supernode shares its level.
+    void preparePartial(std::int32_t dimension, std::int32_t trailing, const oosgpu_factor_options* options)
+    {
+        const std::int32_t last = m_plan.supernodeCount - 1;
+        if (last < 0 || trailing < 0)
+            throw Error(STATUS_INVALID_ARGUMENT, "PartialFactor: expected a trailing count in [1, dimension]");
+        const device::FrontDesc& f = m_plan.fronts[static_cast<std::size_t>(last)];
+        if (f.parent >= 0 || f.r != 0 || f.c != trailing || f.first + f.c != dimension)
+            throw Error(STATUS_INVALID_ARGUMENT,
+                        "PartialFactor: the symbolic factor's last supernode must be the trailing set (" +
+                            std::to_string(trailing) + " equations, ordered last, a root); it has " +
+                            std::to_string(f.c) + " columns from equation " + std::to_string(f.first) +
+                            "; analyse with the unit's boundary as the trailing nodes");
+        const std::int32_t level = m_plan.level[static_cast<std::size_t>(last)];
+        if (m_plan.frontsOfLevel[static_cast<std::size_t>(level)].size() != 1)
+            throw Error(STATUS_INVALID_ARGUMENT, "PartialFactor: the interior has a part that reaches no boundary "
+                                                 "equation (another root beside the trailing supernode)");
+        if (options != nullptr && (options->pivoting != 0 || options->precision != 0))
+            throw Error(STATUS_INVALID_ARGUMENT,
+                        "PartialFactor: the interior of a unit is factorised in positive definite mode, FP64 (a "
+                        "delayed pivot would move an interior equation into the boundary); pass pivoting 0");
+        m_partialLevel = level;
+        m_trailing = trailing;
+        m_partialForward.clear();
+        m_partialBackward.clear();
+        for (const Launch& launch : m_plan.forwardLaunches)
+            if (launch.level < level)
+                m_partialForward.push_back(launch);
+        for (const Launch& launch : m_plan.backwardLaunches)
+            if (launch.level < level)
+                m_partialBackward.push_back(launch);
+    }
+
+    // K* of a partial factorisation: the trailing front assembled from its children's update matrices (at their
+    // positions in it, the plan's maps) and the matrix's boundary entries, into `schur` (host).
+    void trailingComplement(const device::FactorArgs& args, double* schur)
+    {
+        const std::int32_t last = m_plan.supernodeCount - 1;
+        const device::FrontDesc& f = m_plan.fronts[static_cast<std::size_t>(last)];
+        std::vector<device::FrontSource> sources;
+        for (std::int32_t q = 0; q < f.childCount; ++q)
+        {
+            const device::FrontDesc& child =
+                m_plan.fronts[static_cast<std::size_t>(m_plan.children[static_cast<std::size_t>(f.childStart + q)])];
+            if (child.r > 0)
+                sources.push_back({m_updates.get() + child.update, m_relpos.get() + child.rowStart, child.r, 0});
+        }
+        m_exactSources.upload(sources, m_stream, "partial factor: sources");
+        const auto t = static_cast<std::size_t>(m_trailing);
+        m_schur.allocate(t * t, "partial factor: K*");
+        const device::ExactFront front{last, m_trailing, m_trailing, static_cast<std::int32_t>(sources.size()),
+                                       m_exactSources.get(), nullptr};
+        device::trailingFront<<<1, 1024, 0, m_stream>>>(args, front, m_schur.get(), m_structureError.get());
+        check(cudaGetLastError(), "trailing front launch");
+        std::int32_t structureError = 0;
+        check(cudaMemcpyAsync(&structureError, m_structureError.get(), sizeof(std::int32_t), cudaMemcpyDeviceToHost,
+                              m_stream),
+              "download structure check");
+        if (schur != nullptr)
+            check(cudaMemcpyAsync(schur, m_schur.get(), t * t * sizeof(double), cudaMemcpyDeviceToHost, m_stream),
+                  "download K*");
+        check(cudaStreamSynchronize(m_stream), "partial factorisation");
+        if (structureError != NO_PIVOT)
+            throw Error(STATUS_INVALID_ARGUMENT,
+                        "supernodal factorisation: column " + std::to_string(structureError) +
+                            " of the matrix has an entry outside the structure of the symbolic factor");
+        m_isPartial = true;
+    }
+
+    // PartialFactor::condenseLoads (condense) and PartialFactor::recover (recover) on host arrays: loads n x columns
+    // (ld); condense writes f* = f_b - K_bi K_ii^-1 f_i (trailing x columns, ld ldOut) to `out`; recover replaces the
+    // loads by u (its interior u_i = K_ii^-1 (f_i - K_ib u_b), its trailing rows the given u_b, `trailingValues`).
+    void partialSolve(double* loads, std::int64_t ld, std::int64_t columns, double* out, std::int64_t ldOut,
+                      const double* trailingValues, bool recover)
+    {
+        check(cudaSetDevice(m_device), "cudaSetDevice");
+        if (!m_factorised || !m_isPartial)
+            throw Error(STATUS_NOT_FACTORISED, "PartialFactor: no partial factorisation (call factorise_partial)");
+        const std::int32_t n = m_plan.dimension;
+        const std::int32_t t = m_trailing;
+        if (ld < n || columns < 0 || ldOut < t)
+            throw Error(STATUS_INVALID_ARGUMENT, "PartialFactor: expected " + std::to_string(n) + " load rows and " +
+                                                     std::to_string(t) + " trailing rows (leading dimensions)");
+        if (columns == 0)
+            return;
+        const auto rowsOf = [](std::int64_t k) { return static_cast<std::size_t>(k) * sizeof(double); };
+        m_work.allocate(static_cast<std::size_t>(n) * SOLVE_WIDTH, "solve: rows");
+        m_updateRows.allocate(updateRowsPerColumn() * SOLVE_WIDTH, "solve: update rows");
+        m_hostB.allocate(static_cast<std::size_t>(n) * static_cast<std::size_t>(columns), "partial factor: loads");
+        double* b = m_hostB.get();
+        check(cudaMemcpy2DAsync(b, rowsOf(n), loads, rowsOf(ld), rowsOf(n), static_cast<std::size_t>(columns),
+                                cudaMemcpyHostToDevice, m_stream),
+              "upload loads");
+        if (recover)
+            check(cudaMemcpy2DAsync(b + (n - t), rowsOf(n), trailingValues, rowsOf(ldOut), rowsOf(t),
+                                    static_cast<std::size_t>(columns), cudaMemcpyHostToDevice, m_stream),
+                  "upload trailing values");
+        const std::int32_t last = m_plan.supernodeCount - 1;
+        for (std::int64_t c0 = 0; c0 < columns; c0 += SOLVE_WIDTH)
+        {
+            const int width = static_cast<int>(std::min<std::int64_t>(SOLVE_WIDTH, columns - c0));
+            double* x = m_work.get();
+            rowsIn(b, n, static_cast<int>(c0), width, x);
+            const SolveView view = solveView();
+            const device::SolveArgs args{view.fronts,       m_children.get(), view.rows,       view.relpos,
+                                         m_panels.get(),    x,                m_updateRows.get(), width,
+                                         view.gatherStart,  view.gatherRows,  nullptr,          n,
+                                         m_rowPartials.get()};
+            runSweep(args, view, m_partialForward);
+            if (recover)
+            {
+                const std::int64_t items = static_cast<std::int64_t>(n - t) * width;
+                device::diagonalSweep<<<blocksFor(std::max<std::int64_t>(items, 1), 256), 256, 0, m_stream>>>(
+                    args, m_diagonal.get(), n - t);
+                runSweep(args, view, m_partialBackward);
+            }
+            else
+                device::gatherColumns<<<blocksFor(static_cast<std::int64_t>(t) * width, 256), 256, 0, m_stream>>>(
+                    args, last);
+            check(cudaGetLastError(), "partial solve launch");
+            rowsOut(x, static_cast<int>(c0), width, b, n);
+        }
+        if (recover)
+            check(cudaMemcpy2DAsync(loads, rowsOf(ld), b, rowsOf(n), rowsOf(n), static_cast<std::size_t>(columns),
+                                    cudaMemcpyDeviceToHost, m_stream),
+                  "download solutions");
+        else
+            check(cudaMemcpy2DAsync(out, rowsOf(ldOut), b + (n - t), rowsOf(n), rowsOf(t),
+                                    static_cast<std::size_t>(columns), cudaMemcpyDeviceToHost, m_stream),
+                  "download condensed loads");
+        check(cudaStreamSynchronize(m_stream), "partial solve");
+    }
+
     // The indefinite factorisation (the reference's PivotingMode::Indefinite), after the common set-up of factorise():
-    // the pivoted launches level by level; at the end of each level the host reads the fronts' status, refactorises by
-    // the exact path every large front whose threshold test failed, and refuses a pivot delayed to a parent (the GPU
-    // path keeps each front's pivots inside it). Then the inertia with 2x2 blocks and the maps of the pivot order.
+    // the pivoted launches level by level; at the end of each level the host reads the fronts' status and refactorises
+    // by the exact path every front whose block path failed its threshold test, every front that delays pivots to its
+    // parent, and every front whose children delayed pivots into it (grown by their columns). Then, without delays,
+    // the inertia with 2x2 blocks and the maps of the pivot order; with delays, the same on the structure restated in
+    // the order the equations were eliminated.
     void factoriseIndefinite(const device::FactorArgs& args, std::int32_t dimension, oosgpu_factor_info* info)
     {
         const auto count = static_cast<std::size_t>(m_plan.supernodeCount);
@@ -542,20 +692,22 @@ public:
         m_w.allocate(static_cast<std::size_t>(std::max<std::int64_t>(m_plan.wValues, 1)), "indefinite: W");
         if (m_wOffset.get() == nullptr)
             m_wOffset.upload(m_plan.wOffset, m_stream, "indefinite: W offsets");
-        m_frontPerm.allocate(static_cast<std::size_t>(std::max(m_plan.largestColumns, 1)), "indefinite: front scratch");
-        m_frontSub.allocate(static_cast<std::size_t>(std::max(m_plan.largestColumns, 1)), "indefinite: front scratch");
         m_rowsPivot.allocate(static_cast<std::size_t>(std::max<std::int64_t>(m_plan.rowEntries, 1)), "indefinite: rows");
         m_relposPivot.allocate(static_cast<std::size_t>(std::max<std::int64_t>(m_plan.rowEntries, 1)),
                                "indefinite: positions");
-        device::PivotArgs pivots{m_perm.get(),  m_subdiagonal.get(), m_status.get(),    m_stepPerm.get(),
-                                 m_stepSwapped.get(), m_w.get(),    m_wOffset.get(),   m_frontPerm.get(),
-                                 m_frontSub.get()};
+        device::PivotArgs pivots{m_perm.get(),        m_subdiagonal.get(), m_status.get(), m_stepPerm.get(),
+                                 m_stepSwapped.get(), m_w.get(),           m_wOffset.get()};
+        m_exact.clear();
+        m_exact.resize(count);
+        m_grown.clear();
+        m_delayedPivots = 0;
+        m_isRestated = false;
+        ++m_structureGeneration;
         device::identityPermutation<<<blocksFor(dimension, 256), 256, 0, m_stream>>>(m_perm.get(), dimension);
         check(cudaMemsetAsync(m_subdiagonal.get(), 0, n * sizeof(double), m_stream), "memset");
         check(cudaMemsetAsync(m_status.get(), 0, count * sizeof(std::int32_t), m_stream), "memset");
         check(cudaMemsetAsync(m_stepSwapped.get(), 0, count * sizeof(std::int32_t), m_stream), "memset");
         std::vector<std::int32_t> status(count);
-        m_forcedPivots = 0;
         std::size_t profiled = 0;
         for (const Launch& launch : m_plan.pivotedLaunches)
         {
@@ -598,15 +750,8 @@ public:
                       "download status");
                 check(cudaStreamSynchronize(m_stream), "indefinite factorisation level");
                 for (const std::int32_t s : m_plan.frontsOfLevel[static_cast<std::size_t>(launch.k0)])
-                {
-                    const std::int32_t flags = status[static_cast<std::size_t>(s)];
-                    if ((flags & 2) != 0)
-                        throw delayedPivot(s, flags);
-                    if ((flags & 1) != 0)
-                        exactFront(args, pivots, s);
-                    else if ((flags & 4) != 0)
-                        m_forcedPivots += flags >> 8;
-                }
+                    if ((status[static_cast<std::size_t>(s)] & 3) != 0 || receivesDelayed(s))
+                        exactFront(args, s);
                 break;
             }
             default:
@@ -617,14 +762,19 @@ public:
             ++profiled;
         }
         check(cudaGetLastError(), "indefinite factorisation launch");
-        invertDiagonalBlocks(args, true);
-        device::inertiaPivoted<<<blocksFor(std::max(dimension, 1), 256), 256, 0, m_stream>>>(
-            args, pivots, m_supernodeOfColumn.get(), dimension, m_counters.get());
-        device::invertPermutation<<<blocksFor(std::max(dimension, 1), 256), 256, 0, m_stream>>>(
-            m_perm.get(), m_inversePerm.get(), dimension);
-        device::remapPivotOrder<<<std::max(m_plan.supernodeCount, 1), 128, 0, m_stream>>>(
-            m_fronts.get(), m_rows.get(), m_relpos.get(), m_inversePerm.get(), m_rowsPivot.get(), m_relposPivot.get(),
-            m_plan.supernodeCount);
+        if (m_delayedPivots == 0)
+        {
+            invertDiagonalBlocks(args, true);
+            device::inertiaPivoted<<<blocksFor(std::max(dimension, 1), 256), 256, 0, m_stream>>>(
+                args, pivots, m_supernodeOfColumn.get(), dimension, m_counters.get());
+            device::invertPermutation<<<blocksFor(std::max(dimension, 1), 256), 256, 0, m_stream>>>(
+                m_perm.get(), m_inversePerm.get(), dimension);
+            device::remapPivotOrder<<<std::max(m_plan.supernodeCount, 1), 128, 0, m_stream>>>(
+                m_fronts.get(), m_rows.get(), m_relpos.get(), m_inversePerm.get(), m_rowsPivot.get(),
+                m_relposPivot.get(), m_plan.supernodeCount);
+        }
+        else
+            restate(args, pivots);
         check(cudaGetLastError(), "indefinite summary launch");
         check(cudaEventRecord(m_stop, m_stream), "event");
         std::vector<unsigned long long> counters(8);
@@ -650,7 +800,7 @@ public:
         result.negative = static_cast<std::int64_t>(counters[1]);
         result.zero = static_cast<std::int64_t>(counters[2]);
         result.two_by_two = static_cast<std::int64_t>(counters[3]);
-        result.forced = m_forcedPivots;
+        result.delayed = m_delayedPivots;
         result.equation_of_largest = -1;
         result.device_seconds = milliseconds / 1000.0;
         if (info != nullptr)
@@ -673,39 +823,209 @@ public:
         check(cudaGetLastError(), "diagonal inverse launch");
     }
 
-    [[nodiscard]] DelayedPivotError delayedPivot(std::int32_t s, std::int32_t flags) const
+    // Front s received delayed columns from a child.
+    [[nodiscard]] bool receivesDelayed(std::int32_t s) const
     {
         const device::FrontDesc& f = m_plan.fronts[static_cast<std::size_t>(s)];
-        return DelayedPivotError(
-                     "indefinite factorisation: a pivot of supernode " + std::to_string(s) + " (level " +
-                         std::to_string(m_plan.level[static_cast<std::size_t>(s)]) + ", " + std::to_string(f.c) +
-                         " columns, " + std::to_string(f.r) + " rows below, " + std::to_string(f.childCount) +
-                         " children) would be delayed to its parent front after " + std::to_string(flags >> 8) +
-                         " pivots (its column maximum lies outside its candidates and its diagonal is below 0.01 of "
-                         "it); the GPU path keeps every pivot in its own front");
+        for (std::int32_t q = 0; q < f.childCount; ++q)
+        {
+            const ExactOutcome* x = m_exact[static_cast<std::size_t>(m_plan.children[static_cast<std::size_t>(f.childStart + q)])].get();
+            if (x != nullptr && x->delayed() > 0)
+                return true;
+        }
+        return false;
     }
 
-    // The exact path of front s: assembled whole, Bunch-Kaufman on its candidates by one block.
-    void exactFront(const device::FactorArgs& args, const device::PivotArgs& pivots, std::int32_t s)
+    // A grown panel or update matrix of this factorisation (device memory of its own, freed at the next one).
+    double* grownBuffer(std::size_t values, const char* what)
+    {
+        m_grown.push_back(std::make_unique<DeviceArray<double>>());
+        m_grown.back()->allocate(values, what);
+        return m_grown.back()->get();
+    }
+
+    // The exact path of front s (the reference's eliminatePivoted): its candidates are its c columns and the columns
+    // its children delayed (children in increasing order); its sources are its children's update matrices, each row
+    // at the front position positionsInFront gives it. Bunch-Kaufman by one block leaves `eliminated` pivots; the
+    // candidates left are delayed to the parent (a root front cannot delay: an internal error, as in the reference).
+    // A front of its symbolic shape (nothing delayed in or out) keeps its panel, update matrix and pivot order where
+    // the batched kernels keep them; a grown front's panel goes to a grown buffer; an update matrix with delayed rows
+    // goes to a grown buffer, one without to the front's own place (its order is then r).
+    void exactFront(const device::FactorArgs& args, std::int32_t s)
     {
         const device::FrontDesc& f = m_plan.fronts[static_cast<std::size_t>(s)];
-        const std::size_t order = static_cast<std::size_t>(f.c) + static_cast<std::size_t>(f.r);
-        m_frontWork.allocate(order * order, "indefinite: exact front");
-        device::pivotedFront<<<1, 1024, 0, m_stream>>>(args, pivots, s, m_frontWork.get(), m_structureError.get());
+        std::vector<std::int32_t> delayedIn;
+        for (std::int32_t q = 0; q < f.childCount; ++q)
+        {
+            const ExactOutcome* x = m_exact[static_cast<std::size_t>(m_plan.children[static_cast<std::size_t>(f.childStart + q)])].get();
+            if (x != nullptr && x->delayed() > 0)
+                delayedIn.insert(delayedIn.end(), x->equations.begin() + x->eliminated,
+                                 x->equations.begin() + x->candidates);
+        }
+        const auto candidates = static_cast<std::int32_t>(f.c + static_cast<std::int64_t>(delayedIn.size()));
+        const std::int32_t order = candidates + f.r;
+        const bool symbolicShape = delayedIn.empty();
+        // the sources: each child's update matrix and the front positions of its rows
+        std::vector<device::FrontSource> sources;
+        std::vector<std::int32_t> positions;
+        std::vector<std::size_t> positionStart;
+        std::int32_t delayedStart = f.c;
+        for (std::int32_t q = 0; q < f.childCount; ++q)
+        {
+            const std::int32_t ch = m_plan.children[static_cast<std::size_t>(f.childStart + q)];
+            const device::FrontDesc& cf = m_plan.fronts[static_cast<std::size_t>(ch)];
+            const ExactOutcome* x = m_exact[static_cast<std::size_t>(ch)].get();
+            const std::int32_t* childRows = x != nullptr ? x->equations.data() + x->eliminated
+                                                         : m_plan.rows.data() + cf.rowStart;
+            const std::int32_t childOrder = x != nullptr ? x->order - x->eliminated : cf.r;
+            const std::int32_t childDelayed = x != nullptr ? x->delayed() : 0;
+            if (childOrder == 0)
+                continue;
+            const std::vector<std::int32_t> p =
+                positionsInFront(m_plan, s, candidates, childRows, childOrder, childDelayed, delayedStart);
+            delayedStart += childDelayed;
+            positionStart.push_back(positions.size());
+            positions.insert(positions.end(), p.begin(), p.end());
+            sources.push_back({x != nullptr ? x->update : m_updates.get() + cf.update, nullptr, childOrder, 0});
+        }
+        m_exactPositions.upload(positions, m_stream, "exact front: positions");
+        for (std::size_t k = 0; k < sources.size(); ++k)
+            sources[k].positions = m_exactPositions.get() + positionStart[k];
+        m_exactSources.upload(sources, m_stream, "exact front: sources");
+        const std::size_t orderSize = static_cast<std::size_t>(order);
+        double* panel = symbolicShape ? m_panels.get() + f.panel
+                                      : grownBuffer(orderSize * static_cast<std::size_t>(candidates),
+                                                    "indefinite: grown panel");
+        m_frontWork.allocate(orderSize * orderSize, "indefinite: exact front");
+        m_exactPerm.allocate(static_cast<std::size_t>(std::max(candidates, 1)), "exact front: permutation");
+        m_exactSub.allocate(static_cast<std::size_t>(std::max(candidates, 1)), "exact front: subdiagonal");
+        m_exactCount.allocate(1, "exact front: eliminated");
+        const device::ExactFront front{s, order, candidates, static_cast<std::int32_t>(sources.size()),
+                                       m_exactSources.get(), panel};
+        device::exactFront<<<1, 1024, 0, m_stream>>>(args, front, m_frontWork.get(), m_exactPerm.get(), m_exactSub.get(),
+                                                     m_exactCount.get(), m_structureError.get());
         check(cudaGetLastError(), "exact front launch");
-        std::int32_t flags = 0;
-        check(cudaMemcpyAsync(&flags, m_status.get() + s, sizeof(std::int32_t), cudaMemcpyDeviceToHost, m_stream),
-              "download status");
+        std::vector<std::int32_t> perm(static_cast<std::size_t>(candidates));
+        std::vector<double> sub(static_cast<std::size_t>(candidates));
+        std::int32_t eliminated = 0;
+        if (candidates > 0)
+        {
+            check(cudaMemcpyAsync(perm.data(), m_exactPerm.get(), perm.size() * sizeof(std::int32_t),
+                                  cudaMemcpyDeviceToHost, m_stream),
+                  "download exact front");
+            check(cudaMemcpyAsync(sub.data(), m_exactSub.get(), sub.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                  m_stream),
+                  "download exact front");
+        }
+        check(cudaMemcpyAsync(&eliminated, m_exactCount.get(), sizeof(std::int32_t), cudaMemcpyDeviceToHost, m_stream),
+              "download exact front");
         check(cudaStreamSynchronize(m_stream), "exact front");
         ++m_exactFronts;
-        if ((flags & 2) != 0)
-            throw delayedPivot(s, flags);
-        if ((flags & 4) != 0)
-            m_forcedPivots += flags >> 8;
+        auto out = std::make_unique<ExactOutcome>();
+        out->order = order;
+        out->candidates = candidates;
+        out->eliminated = eliminated;
+        // the equation at each front position: the candidates permuted, then R(s)
+        std::vector<std::int32_t> origin(orderSize);
+        for (std::int32_t j = 0; j < f.c; ++j)
+            origin[static_cast<std::size_t>(j)] = f.first + j;
+        std::copy(delayedIn.begin(), delayedIn.end(), origin.begin() + f.c);
+        std::copy_n(m_plan.rows.data() + f.rowStart, f.r, origin.begin() + candidates);
+        out->equations.resize(orderSize);
+        for (std::int32_t k = 0; k < order; ++k)
+            out->equations[static_cast<std::size_t>(k)] =
+                origin[static_cast<std::size_t>(k < candidates ? perm[static_cast<std::size_t>(k)] : k)];
+        out->subdiagonal.assign(sub.begin(), sub.begin() + eliminated);
+        // the panel's place from the arena's base, in values (a grown panel lies in an allocation of its own, before
+        // or after the arena: the kernels reach it as args.panels + offset)
+        out->panel = static_cast<std::int64_t>(reinterpret_cast<std::intptr_t>(panel) -
+                                               reinterpret_cast<std::intptr_t>(m_panels.get())) /
+                     static_cast<std::int64_t>(sizeof(double));
+        if (out->delayed() > 0 && f.parent < 0)
+            throw Error(STATUS_INTERNAL, "supernodal factorisation: the root front " + std::to_string(s) + " delayed " +
+                                             std::to_string(out->delayed()) + " pivots, which a root front cannot do");
+        const std::int32_t updateOrder = order - eliminated;
+        const bool keepsShape = symbolicShape && out->delayed() == 0;
+        if (updateOrder > 0)
+        {
+            // Without delays out the update matrix has its symbolic order r (a grown front eliminated its delayed
+            // columns too): it goes where the parent's batched assembly reads it.
+            double* update = out->delayed() == 0 ? m_updates.get() + f.update
+                                                 : grownBuffer(static_cast<std::size_t>(updateOrder) * updateOrder,
+                                                               "indefinite: grown update matrix");
+            const std::int64_t items = static_cast<std::int64_t>(updateOrder) * updateOrder;
+            device::copyTrailing<<<blocksFor(items, 256), 256, 0, m_stream>>>(m_frontWork.get(), order, eliminated,
+                                                                            updateOrder, update);
+            check(cudaGetLastError(), "exact front update launch");
+            out->update = update;
+        }
+        if (keepsShape && f.c > 0)
+        {
+            // the front's pivot order where the batched kernels keep it
+            std::vector<std::int32_t> pivotOrder(static_cast<std::size_t>(f.c));
+            for (std::int32_t j = 0; j < f.c; ++j)
+                pivotOrder[static_cast<std::size_t>(j)] = f.first + perm[static_cast<std::size_t>(j)];
+            check(cudaMemcpyAsync(m_perm.get() + f.first, pivotOrder.data(), pivotOrder.size() * sizeof(std::int32_t),
+                                  cudaMemcpyHostToDevice, m_stream),
+                  "upload exact front");
+            check(cudaMemcpyAsync(m_subdiagonal.get() + f.first, sub.data(), static_cast<std::size_t>(f.c) * sizeof(double),
+                                  cudaMemcpyHostToDevice, m_stream),
+                  "upload exact front");
+        }
+        check(cudaStreamSynchronize(m_stream), "exact front");
+        m_delayedPivots += out->delayed();
+        m_exact[static_cast<std::size_t>(s)] = std::move(out);
+    }
+
+    // After a factorisation that delayed pivots: the structure restated in elimination order (restateDelayed), its
+    // solve plan and maps on the device, the diagonal inverses of its panels and the inertia counted on it.
+    void restate(const device::FactorArgs& args, const device::PivotArgs& pivots)
+    {
+        const auto n = static_cast<std::size_t>(m_plan.dimension);
+        std::vector<std::int32_t> perm(n);
+        std::vector<double> sub(n);
+        check(cudaMemcpyAsync(perm.data(), m_perm.get(), n * sizeof(std::int32_t), cudaMemcpyDeviceToHost, m_stream),
+              "download pivot order");
+        check(cudaMemcpyAsync(sub.data(), m_subdiagonal.get(), n * sizeof(double), cudaMemcpyDeviceToHost, m_stream),
+              "download subdiagonals");
+        check(cudaStreamSynchronize(m_stream), "download pivot order");
+        DelayedStructure d = restateDelayed(m_plan, perm, sub, m_exact);
+        Restated& r = m_restated;
+        r.plan = std::move(d.plan);
+        r.perm = std::move(d.perm);
+        r.subdiagonal = std::move(d.subdiagonal);
+        r.fronts.upload(r.plan.fronts, m_stream, "restated: fronts");
+        r.rows.upload(r.plan.rows, m_stream, "restated: rows");
+        r.relpos.upload(r.plan.relpos, m_stream, "restated: positions");
+        r.gatherStart.upload(r.plan.gatherStart, m_stream, "restated: gather lists");
+        r.gatherRows.upload(r.plan.gatherRows, m_stream, "restated: gather lists");
+        r.supernodeOfColumn.upload(r.plan.supernodeOfColumn, m_stream, "restated: columns");
+        r.lists.upload(r.plan.lists, m_stream, "restated: lists");
+        r.tiles.upload(r.plan.tiles, m_stream, "restated: tiles");
+        r.devicePerm.upload(r.perm, m_stream, "restated: pivot order");
+        r.deviceSubdiagonal.upload(r.subdiagonal, m_stream, "restated: subdiagonals");
+        if (r.plan.rowPartialSlots > m_plan.rowPartialSlots)
+            m_rowPartials.allocate(static_cast<std::size_t>(r.plan.rowPartialSlots) * device::TILE * device::TILE,
+                                   "solve: split products");
+        device::FactorArgs restatedArgs = args;
+        restatedArgs.fronts = r.fronts.get();
+        for (const std::vector<Launch>* launches : {&r.plan.inverseLaunches, &r.plan.inverseLaunchesLarge})
+            for (const Launch& launch : *launches)
+                device::invertDiagonal<<<launch.count, 64, 0, m_stream>>>(restatedArgs, r.tiles.get() + launch.offset);
+        device::PivotArgs restatedPivots = pivots;
+        restatedPivots.subdiagonal = r.deviceSubdiagonal.get();
+        restatedPivots.perm = r.devicePerm.get();
+        device::inertiaPivoted<<<blocksFor(std::max(m_plan.dimension, 1), 256), 256, 0, m_stream>>>(
+            restatedArgs, restatedPivots, r.supernodeOfColumn.get(), m_plan.dimension, m_counters.get());
+        check(cudaGetLastError(), "restated structure launch");
+        m_isRestated = true;
     }
 
     void requireSolvable() const
     {
+        if (m_isPartial)
+            throw Error(STATUS_INVALID_ARGUMENT, "FactorSolve::solve: a partial factor (its trailing supernode is not "
+                                                 "eliminated); use condense and recover");
         if (!m_factorised)
             throw Error(STATUS_NOT_FACTORISED, "FactorSolve: no factor (factorise first, or the last one failed)");
         if (m_singular)
@@ -725,7 +1045,7 @@ public:
         if (columns == 0 || n == 0)
             return;
         m_work.allocate(static_cast<std::size_t>(n) * SOLVE_WIDTH, "solve: rows");
-        m_updateRows.allocate(static_cast<std::size_t>(std::max<std::int64_t>(m_plan.rowEntries, 1)) * SOLVE_WIDTH,
+        m_updateRows.allocate(updateRowsPerColumn() * SOLVE_WIDTH,
                               "solve: update rows");
         double* deviceB = b;
         if (!onDevice)
@@ -763,13 +1083,56 @@ public:
 
     // A column tile of B (columns [c0, c0 + width), leading dimension ld) into rows of x, in pivot order after an
     // indefinite factorisation, scaled by the solve's scale when one is set (a pencil's S).
+    // The structure the solves run on: the plan's, in pivot order after an indefinite factorisation, or the
+    // restated one after a factorisation that delayed pivots.
+    struct SolveView
+    {
+        const Plan* plan;
+        const device::FrontDesc* fronts;
+        const std::int32_t* rows;
+        const std::int32_t* relpos;
+        const std::int64_t* gatherStart;
+        const std::int32_t* gatherRows;
+        const std::int32_t* supernodeOfColumn;
+        const std::int32_t* lists;
+        const device::TileTask* tiles;
+        const std::int32_t* perm;
+        const double* subdiagonal;
+    };
+    [[nodiscard]] SolveView solveView() const
+    {
+        if (m_pivoted && m_isRestated)
+        {
+            const Restated& r = m_restated;
+            return {&r.plan,           r.fronts.get(),     r.rows.get(),  r.relpos.get(),      r.gatherStart.get(),
+                    r.gatherRows.get(), r.supernodeOfColumn.get(), r.lists.get(), r.tiles.get(), r.devicePerm.get(),
+                    r.deviceSubdiagonal.get()};
+        }
+        return {&m_plan,
+                m_fronts.get(),
+                m_pivoted ? m_rowsPivot.get() : m_rows.get(),
+                m_pivoted ? m_relposPivot.get() : m_relpos.get(),
+                m_gatherStart.get(),
+                m_gatherRows.get(),
+                m_supernodeOfColumn.get(),
+                m_lists.get(),
+                m_tiles.get(),
+                m_perm.get(),
+                m_subdiagonal.get()};
+    }
+    // The update rows of the forward sweep, per right-hand side.
+    [[nodiscard]] std::size_t updateRowsPerColumn() const
+    {
+        return static_cast<std::size_t>(std::max<std::int64_t>(solveView().plan->rowEntries, 1));
+    }
+
     void rowsIn(const double* b, std::int64_t ld, int c0, int width, double* x)
     {
         const std::int32_t n = m_plan.dimension;
         const std::int64_t items = static_cast<std::int64_t>(n) * width;
         if (m_pivoted)
-            device::toRowsPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(b, ld, c0, width, n, x, m_perm.get(),
-                                                                               m_solveScale);
+            device::toRowsPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(b, ld, c0, width, n, x,
+                                                                               solveView().perm, m_solveScale);
         else
             device::toRows<<<dim3(blocksFor(n, 32), blocksFor(width, 32)), dim3(32, 8), 0, m_stream>>>(
                 b, ld, c0, width, n, x, m_solveScale);
@@ -781,8 +1144,8 @@ public:
         const std::int32_t n = m_plan.dimension;
         const std::int64_t items = static_cast<std::int64_t>(n) * width;
         if (m_pivoted)
-            device::fromRowsPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(x, c0, width, n, b, ld, m_perm.get(),
-                                                                                 m_solveScale);
+            device::fromRowsPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(x, c0, width, n, b, ld,
+                                                                                 solveView().perm, m_solveScale);
         else
             device::fromRows<<<dim3(blocksFor(n, 32), blocksFor(width, 32)), dim3(32, 8), 0, m_stream>>>(
                 x, c0, width, n, b, ld, m_solveScale);
@@ -797,31 +1160,33 @@ public:
     {
         const std::int32_t n = m_plan.dimension;
         const std::int64_t items = static_cast<std::int64_t>(n) * width;
-        device::SolveArgs args{m_fronts.get(),
+        const SolveView view = solveView();
+        device::SolveArgs args{view.fronts,
                                m_children.get(),
-                               m_pivoted ? m_rowsPivot.get() : m_rows.get(),
-                               m_pivoted ? m_relposPivot.get() : m_relpos.get(),
+                               view.rows,
+                               view.relpos,
                                m_panels.get(),
                                x,
                                updateRows != nullptr ? updateRows : m_updateRows.get(),
                                width,
-                               m_gatherStart.get(),
-                               m_gatherRows.get(),
-                               m_pivoted ? m_perm.get() : nullptr,
+                               view.gatherStart,
+                               view.gatherRows,
+                               // the plan's gather slots are equations, the restated structure's are positions
+                               m_pivoted && !m_isRestated ? view.perm : nullptr,
                                n,
                                m_rowPartials.get()};
         const auto launches = [&]
         {
-            runSweep(args, m_plan.forwardLaunches);
+            runSweep(args, view, view.plan->forwardLaunches);
             const std::size_t record =
                 beginSolveRecord(DIAGONAL_SWEEP_KIND, static_cast<std::int32_t>(blocksFor(items, 256)), 0);
             if (m_pivoted)
                 device::diagonalSweepPivoted<<<blocksFor(items, 256), 256, 0, m_stream>>>(
-                    args, m_supernodeOfColumn.get(), m_subdiagonal.get(), n);
+                    args, view.supernodeOfColumn, view.subdiagonal, n);
             else
                 device::diagonalSweep<<<blocksFor(items, 256), 256, 0, m_stream>>>(args, m_diagonal.get(), n);
             endSolveRecord(record);
-            runSweep(args, m_plan.backwardLaunches);
+            runSweep(args, view, view.plan->backwardLaunches);
         };
         m_solveRecords.clear();
         if (m_profile || !replay)
@@ -829,7 +1194,8 @@ public:
         else
             m_sweepGraph.run(m_stream,
                              {keyOf(x), keyOf(args.updates), static_cast<std::uintptr_t>(width),
-                              static_cast<std::uintptr_t>(m_pivoted)},
+                              static_cast<std::uintptr_t>(m_pivoted),
+                              m_pivoted && m_isRestated ? m_structureGeneration : 0},
                              launches);
         m_solveProfileValid = m_profile;
     }
@@ -844,7 +1210,7 @@ public:
     {
         check(cudaSetDevice(m_device), "cudaSetDevice");
         const std::int32_t n = m_plan.dimension;
-        const std::size_t perColumn = static_cast<std::size_t>(n) + static_cast<std::size_t>(std::max<std::int64_t>(m_plan.rowEntries, 1));
+        const std::size_t perColumn = static_cast<std::size_t>(n) + updateRowsPerColumn();
         if (perColumn > capacity)
             throw Error(STATUS_INVALID_ARGUMENT,
                         "solve without allocation: this factor needs " + std::to_string(perColumn) +
@@ -1117,7 +1483,7 @@ public:
         m_bRows.allocate(tile, "refinement: right-hand side rows");
         m_rRows.allocate(tile, "refinement: residual rows");
         m_norms.allocate(384, "refinement: norms");
-        m_updateRows.allocate(static_cast<std::size_t>(std::max<std::int64_t>(m_plan.rowEntries, 1)) * SOLVE_WIDTH,
+        m_updateRows.allocate(updateRowsPerColumn() * SOLVE_WIDTH,
                               "solve: update rows");
         const double* deviceB = b;
         double* deviceX = x;
@@ -1213,7 +1579,10 @@ public:
             throw Error(STATUS_INVALID_ARGUMENT, "panel: supernode out of range");
         if (!m_factorised)
             throw Error(STATUS_NOT_FACTORISED, "panel: no factor");
-        const device::FrontDesc& f = m_plan.fronts[static_cast<std::size_t>(s)];
+        // After a factorisation that delayed pivots, the panel of the restated structure: its eliminated columns over
+        // its front's rows (eliminated and delayed candidates, then R(s)), as the reference's grown panels.
+        const bool restated = m_pivoted && m_isRestated;
+        const device::FrontDesc& f = (restated ? m_restated.plan.fronts : m_plan.fronts)[static_cast<std::size_t>(s)];
         const std::int64_t n = f.c + f.r;
         *eliminated = f.c;
         *rowCount = n;
@@ -1226,14 +1595,40 @@ public:
             for (std::int64_t j = 0; j < f.c; ++j)
                 std::fill_n(values + j * n, j, 0.0);
         }
-        if (rows != nullptr)
+        // The row equations in pivot order and the 2x2 subdiagonals (positive definite: the natural order, zeros).
+        std::vector<std::int32_t> pivotOrder(static_cast<std::size_t>(f.c));
+        std::vector<double> sub(static_cast<std::size_t>(f.c), 0.0);
+        if (restated)
         {
             for (std::int32_t k = 0; k < f.c; ++k)
-                rows[k] = f.first + k;
-            std::copy_n(m_plan.rows.data() + f.rowStart, f.r, rows + f.c);
+            {
+                pivotOrder[static_cast<std::size_t>(k)] = m_restated.perm[static_cast<std::size_t>(f.first + k)];
+                sub[static_cast<std::size_t>(k)] = m_restated.subdiagonal[static_cast<std::size_t>(f.first + k)];
+            }
+        }
+        else if (m_pivoted && f.c > 0)
+        {
+            check(cudaMemcpy(pivotOrder.data(), m_perm.get() + f.first, pivotOrder.size() * sizeof(std::int32_t),
+                             cudaMemcpyDeviceToHost),
+                  "download pivot order");
+            check(cudaMemcpy(sub.data(), m_subdiagonal.get() + f.first, sub.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost),
+                  "download subdiagonals");
+        }
+        else
+            for (std::int32_t k = 0; k < f.c; ++k)
+                pivotOrder[static_cast<std::size_t>(k)] = f.first + k;
+        if (rows != nullptr)
+        {
+            std::copy(pivotOrder.begin(), pivotOrder.end(), rows);
+            for (std::int32_t k = 0; k < f.r; ++k)
+            {
+                const std::int32_t row = (restated ? m_restated.plan.rows : m_plan.rows)[static_cast<std::size_t>(f.rowStart + k)];
+                rows[f.c + k] = restated ? m_restated.perm[static_cast<std::size_t>(row)] : row;
+            }
         }
         if (subdiagonal != nullptr)
-            std::fill_n(subdiagonal, f.c, 0.0);
+            std::copy(sub.begin(), sub.end(), subdiagonal);
     }
 
     [[nodiscard]] double lastSolveSeconds() const noexcept { return m_lastSolveSeconds; }
@@ -1380,7 +1775,8 @@ public:
     [[nodiscard]] std::int64_t solveLaunchCount(std::int64_t columns) const noexcept
     {
         const std::int64_t tiles = (columns + SOLVE_WIDTH - 1) / SOLVE_WIDTH;
-        return tiles * (static_cast<std::int64_t>(m_plan.forwardLaunches.size() + m_plan.backwardLaunches.size()) + 3);
+        const Plan& plan = *solveView().plan;
+        return tiles * (static_cast<std::int64_t>(plan.forwardLaunches.size() + plan.backwardLaunches.size()) + 3);
     }
 
 private:
@@ -1529,6 +1925,17 @@ private:
         std::int32_t lastGroup = -1;
         for (const Launch& launch : m_plan.factorLaunches)
         {
+            if (m_partialLevel >= 0 && launch.level >= m_partialLevel)
+            {
+                // a partial factorisation leaves the trailing supernode's level out (its front becomes K*)
+                if (m_profile)
+                {
+                    check(cudaEventRecord(profileEvent(2 * index), m_stream), "profile event");
+                    check(cudaEventRecord(profileEvent(2 * index + 1), m_stream), "profile event");
+                }
+                ++index;
+                continue;
+            }
             const bool lookahead = !m_profile;
             if (lookahead && launch.waitGroup >= 0)
                 check(cudaStreamWaitEvent(m_stream, m_groupDone[launch.waitGroup & 1], 0), "wait for a side group");
@@ -1628,12 +2035,12 @@ private:
         }
     }
 
-    void runSweep(const device::SolveArgs& args, const std::vector<Launch>& launches)
+    void runSweep(const device::SolveArgs& args, const SolveView& view, const std::vector<Launch>& launches)
     {
         for (const Launch& launch : launches)
         {
-            const std::int32_t* list = m_lists.get() + launch.offset;
-            const device::TileTask* tiles = m_tiles.get() + launch.offset;
+            const std::int32_t* list = view.lists + launch.offset;
+            const device::TileTask* tiles = view.tiles + launch.offset;
             const std::size_t smallSmem = device::smallSolveSmem(std::max(launch.smemOrder, 1));
             const std::size_t record = beginSolveRecord(static_cast<std::int32_t>(launch.kind), launch.count, launch.k0);
             switch (launch.kind)
@@ -1751,14 +2158,49 @@ private:
     DeviceArray<std::int32_t> m_inversePerm;
     DeviceArray<double> m_subdiagonal;
     DeviceArray<std::int32_t> m_status;
-    std::int64_t m_forcedPivots = 0;
     DeviceArray<std::int32_t> m_stepPerm;
     DeviceArray<std::int32_t> m_stepSwapped;
     DeviceArray<double> m_w;
     DeviceArray<std::int64_t> m_wOffset;
-    DeviceArray<std::int32_t> m_frontPerm;
-    DeviceArray<double> m_frontSub;
     DeviceArray<double> m_frontWork;
+    // Delayed pivots: the exact path's outcome of each front it factorised (null elsewhere), the grown panels and
+    // update matrices of this factorisation, the exact path's scratch, and the restated structure the solves use when
+    // some front delayed.
+    std::vector<std::unique_ptr<ExactOutcome>> m_exact;
+    std::vector<std::unique_ptr<DeviceArray<double>>> m_grown;
+    DeviceArray<device::FrontSource> m_exactSources;
+    DeviceArray<std::int32_t> m_exactPositions;
+    DeviceArray<std::int32_t> m_exactPerm;
+    DeviceArray<double> m_exactSub;
+    DeviceArray<std::int32_t> m_exactCount;
+    std::int64_t m_delayedPivots = 0;
+    struct Restated
+    {
+        Plan plan;
+        std::vector<std::int32_t> perm; // position -> equation (host copy)
+        std::vector<double> subdiagonal;
+        DeviceArray<device::FrontDesc> fronts;
+        DeviceArray<std::int32_t> rows;
+        DeviceArray<std::int32_t> relpos;
+        DeviceArray<std::int64_t> gatherStart;
+        DeviceArray<std::int32_t> gatherRows;
+        DeviceArray<std::int32_t> supernodeOfColumn;
+        DeviceArray<std::int32_t> lists;
+        DeviceArray<device::TileTask> tiles;
+        DeviceArray<std::int32_t> devicePerm;
+        DeviceArray<double> deviceSubdiagonal;
+    };
+    Restated m_restated;
+    bool m_isRestated = false;
+    // Partial factorisation: the trailing supernode's level (-1: a full factorisation), its equations, K* on the
+    // device, and the solve launches below that level.
+    std::int32_t m_partialLevel = -1;
+    std::int32_t m_trailing = 0;
+    bool m_isPartial = false;
+    DeviceArray<double> m_schur;
+    std::vector<Launch> m_partialForward;
+    std::vector<Launch> m_partialBackward;
+    std::uintptr_t m_structureGeneration = 0;
     DeviceArray<std::int32_t> m_rowsPivot;
     DeviceArray<std::int32_t> m_relposPivot;
     bool m_pivoted = false;
@@ -2203,6 +2645,51 @@ extern "C" void oosgpu_factor_destroy(oosgpu_factor* factor)
 extern "C" void* oosgpu_factor_stream(oosgpu_factor* factor)
 {
     return factor == nullptr ? nullptr : static_cast<void*>(factor->factor->stream());
+}
+
+extern "C" int oosgpu_factorise_partial(oosgpu_factor* factor, int32_t dimension, const int64_t* col_offsets,
+                                        const int32_t* rows, const double* values, int32_t trailing,
+                                        const oosgpu_factor_options* options, double* schur_complement,
+                                        oosgpu_factor_info* info)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            requirePointer(col_offsets, "col_offsets");
+            requirePointer(schur_complement, "schur_complement");
+            if (trailing <= 0)
+                throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT, "PartialFactor: expected a trailing count in [1, dimension]");
+            factor->factor->factorise(dimension, -1, col_offsets, rows, values, false, options, info, trailing,
+                                      schur_complement);
+        });
+}
+
+extern "C" int oosgpu_partial_condense(oosgpu_factor* factor, const double* loads, int64_t ld, int64_t columns,
+                                       double* condensed, int64_t ld_condensed)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            requirePointer(loads, "loads");
+            requirePointer(condensed, "condensed");
+            factor->factor->partialSolve(const_cast<double*>(loads), ld, columns, condensed, ld_condensed, nullptr,
+                                         false);
+        });
+}
+
+extern "C" int oosgpu_partial_recover(oosgpu_factor* factor, double* loads_to_solution, int64_t ld, int64_t columns,
+                                      const double* trailing_values, int64_t ld_trailing)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            requirePointer(loads_to_solution, "loads_to_solution");
+            requirePointer(trailing_values, "trailing_values");
+            factor->factor->partialSolve(loads_to_solution, ld, columns, nullptr, ld_trailing, trailing_values, true);
+        });
 }
 
 extern "C" int oosgpu_factorise(oosgpu_factor* factor, int32_t dimension, const int64_t* col_offsets,

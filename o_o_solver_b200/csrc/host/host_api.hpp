@@ -35,15 +35,6 @@ private:
     Status m_status;
 };
 
-// An indefinite factorisation refused because a pivot would have to be delayed to a parent front (the GPU path keeps
-// every pivot in its own front): a SolverError for the caller; the eigenvalue driver moves the shift off it, as off a
-// singular shift.
-class DelayedPivotError : public Error
-{
-public:
-    explicit DelayedPivotError(const std::string& message) : Error(STATUS_SOLVER, message) {}
-};
-
 // A structured finite-element model: free nodes, their graph, node-block stiffness, lumped mass and loads.
 class Model
 {

@@ -66,6 +66,184 @@ double columnFlops(std::int64_t n, std::int64_t k0, std::int64_t k1)
     return flops;
 }
 
+// The forward solve's gather lists of plan.relpos (its transpose, children in increasing order within each slot).
+void buildGatherLists(Plan& plan)
+{
+    const std::int32_t count = plan.supernodeCount;
+    if (static_cast<std::int64_t>(plan.rows.size()) > INT32_MAX)
+        throw Error(STATUS_INVALID_ARGUMENT, "plan: more than 2^31 row entries");
+    const std::size_t slots = static_cast<std::size_t>(plan.dimension) + plan.rows.size();
+    plan.gatherStart.assign(slots + 1, 0);
+    const auto slotOf = [&](const FrontDesc& p, std::int32_t position)
+    {
+        return position < p.c ? static_cast<std::size_t>(p.first + position)
+                              : static_cast<std::size_t>(plan.dimension) + static_cast<std::size_t>(p.rowStart) +
+                                    static_cast<std::size_t>(position - p.c);
+    };
+    for (std::int32_t s = 0; s < count; ++s)
+    {
+        const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+        if (f.parent < 0)
+            continue;
+        const FrontDesc& p = plan.fronts[static_cast<std::size_t>(f.parent)];
+        for (std::int64_t k = f.rowStart; k < f.rowStart + f.r; ++k)
+            ++plan.gatherStart[slotOf(p, plan.relpos[static_cast<std::size_t>(k)]) + 1];
+    }
+    for (std::size_t slot = 0; slot < slots; ++slot)
+        plan.gatherStart[slot + 1] += plan.gatherStart[slot];
+    plan.gatherRows.assign(static_cast<std::size_t>(plan.gatherStart[slots]), 0);
+    std::vector<std::int64_t> next(plan.gatherStart.begin(), plan.gatherStart.end() - 1);
+    // children of each parent in increasing order: the parent's child list is in that order
+    for (std::int32_t s = 0; s < count; ++s)
+    {
+        const FrontDesc& p = plan.fronts[static_cast<std::size_t>(s)];
+        for (std::int32_t q = 0; q < p.childCount; ++q)
+        {
+            const FrontDesc& ch =
+                plan.fronts[static_cast<std::size_t>(plan.children[static_cast<std::size_t>(p.childStart + q)])];
+            for (std::int64_t k = ch.rowStart; k < ch.rowStart + ch.r; ++k)
+            {
+                const std::size_t slot = slotOf(p, plan.relpos[static_cast<std::size_t>(k)]);
+                plan.gatherRows[static_cast<std::size_t>(next[slot]++)] = static_cast<std::int32_t>(k);
+            }
+        }
+    }
+}
+
+// The solve launches of one level's supernodes (the forward sweep's into plan.forwardLaunches, the backward sweep's
+// into `backward`, emitted later top level first) and the 64-column diagonal blocks whose inverses the solves apply.
+void addSolveLevel(Plan& plan, const std::vector<std::int32_t>& members, std::int32_t level,
+                   std::vector<Launch>& backward, std::vector<TileTask>& inverseTasks,
+                   std::vector<TileTask>& inverseTasksLarge)
+{
+    const std::size_t forwardBefore = plan.forwardLaunches.size();
+    const std::size_t backwardBefore = backward.size();
+    // ---- forward sweep ----
+    std::vector<std::int32_t> solveSmall;
+    std::vector<std::int32_t> solveLarge;
+    std::int32_t maxColumns = 0;
+    for (const std::int32_t s : members)
+    {
+        const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+        if (f.c <= SOLVE_SMALL_COLUMNS)
+            solveSmall.push_back(s);
+        else
+        {
+            solveLarge.push_back(s);
+            maxColumns = std::max(maxColumns, f.c);
+        }
+    }
+    // The small supernodes by width class (at most 16, 32 or SOLVE_SMALL_COLUMNS columns): each launch's shared
+    // memory is sized for its widest supernode, so the narrow ones (most of the lowest levels) fit more blocks
+    // per SM. The supernodes of one level are independent, so the split changes no result.
+    std::vector<std::vector<std::int32_t>> smallClasses(3);
+    std::vector<std::int32_t> smallClassColumns(3, 0);
+    for (const std::int32_t s : solveSmall)
+    {
+        const std::int32_t c = plan.fronts[static_cast<std::size_t>(s)].c;
+        const std::size_t k = c <= 16 ? 0 : c <= 32 ? 1 : 2;
+        smallClasses[k].push_back(s);
+        smallClassColumns[k] = std::max(smallClassColumns[k], c);
+    }
+    for (std::size_t k = 0; k < smallClasses.size(); ++k)
+        addList(plan, plan.forwardLaunches, LaunchKind::ForwardSmall, smallClasses[k], 0, smallClassColumns[k]);
+    {
+        // The children's update rows of the large supernodes, by ranges of GATHER_POSITIONS front positions.
+        constexpr std::int32_t GATHER_POSITIONS = 64;
+        std::vector<TileTask> ranges;
+        for (const std::int32_t s : solveLarge)
+        {
+            const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+            const std::int32_t n = f.c + f.r;
+            for (std::int32_t p0 = 0; p0 < n; p0 += GATHER_POSITIONS)
+                ranges.push_back({s, p0, std::min(n, p0 + GATHER_POSITIONS), 0});
+        }
+        addTiles(plan, plan.forwardLaunches, LaunchKind::ForwardGather, ranges);
+    }
+    for (const std::int32_t s : members)
+    {
+        const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+        const bool isLarge = f.c + f.r > SMALL_ORDER; // the factorisation's own split, above
+        for (std::int32_t k0 = 0; k0 < f.c; k0 += BLOCK)
+            (isLarge ? inverseTasksLarge : inverseTasks).push_back({s, k0, 0, 0});
+    }
+    // Steps of SOLVE_STEP columns: the step's diagonal blocks in one launch, then its products with the rows below.
+    constexpr std::int32_t STEP = device::SOLVE_STEP;
+    for (std::int32_t k0 = 0; k0 < maxColumns; k0 += STEP)
+    {
+        std::vector<std::int32_t> diagonal;
+        std::vector<TileTask> below;
+        for (const std::int32_t s : solveLarge)
+        {
+            const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+            if (f.c <= k0)
+                continue;
+            diagonal.push_back(s);
+            const std::int32_t kb = std::min(STEP, f.c - k0);
+            for (std::int32_t i0 = k0 + kb; i0 < f.c; i0 += device::TILE)
+                below.push_back({s, i0, 0, 0});
+            for (std::int32_t i0 = f.c; i0 < f.c + f.r; i0 += device::TILE)
+                below.push_back({s, i0, 0, 1});
+        }
+        addList(plan, plan.forwardLaunches, LaunchKind::ForwardDiagonal, diagonal, k0);
+        addTiles(plan, plan.forwardLaunches, LaunchKind::ForwardUpdate, below, k0);
+    }
+
+    // ---- backward sweep (collected per level, emitted top level first) ----
+    for (std::size_t k = 0; k < smallClasses.size(); ++k)
+        addList(plan, backward, LaunchKind::BackwardSmall, smallClasses[k], 0, smallClassColumns[k]);
+    // x_F -= L21^T X[R(s)] by 64-column tiles; R(s) longer than SOLVE_ROWS_CHUNK in chunks (task j0: the chunk's
+    // first row, k0: its partial's slot, -1 for an unsplit tile), then the partials summed in chunk order.
+    std::vector<TileTask> rowTiles;
+    std::vector<TileTask> rowSums;
+    std::int64_t slots = 0;
+    for (const std::int32_t s : solveLarge)
+    {
+        const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+        if (f.r == 0)
+            continue;
+        const std::int32_t chunks = (f.r + device::SOLVE_ROWS_CHUNK - 1) / device::SOLVE_ROWS_CHUNK;
+        for (std::int32_t i0 = 0; i0 < f.c; i0 += device::TILE)
+        {
+            if (chunks == 1)
+            {
+                rowTiles.push_back({s, i0, 0, -1});
+                continue;
+            }
+            rowSums.push_back({s, i0, static_cast<std::int32_t>(slots), chunks});
+            for (std::int32_t q = 0; q < chunks; ++q)
+                rowTiles.push_back({s, i0, q * device::SOLVE_ROWS_CHUNK, static_cast<std::int32_t>(slots++)});
+        }
+    }
+    if (slots > INT32_MAX)
+        throw Error(STATUS_INVALID_ARGUMENT, "plan: too many split backward products in one level");
+    plan.rowPartialSlots = std::max(plan.rowPartialSlots, slots);
+    addTiles(plan, backward, LaunchKind::BackwardRows, rowTiles);
+    addTiles(plan, backward, LaunchKind::BackwardRowsReduce, rowSums);
+    const std::int32_t steps = (maxColumns + STEP - 1) / STEP;
+    for (std::int32_t t = steps - 1; t >= 0; --t)
+    {
+        const std::int32_t k0 = t * STEP;
+        std::vector<std::int32_t> diagonal;
+        std::vector<TileTask> above;
+        for (const std::int32_t s : solveLarge)
+        {
+            const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+            if (f.c <= k0)
+                continue;
+            diagonal.push_back(s);
+            for (std::int32_t i0 = 0; i0 < k0; i0 += device::TILE)
+                above.push_back({s, i0, 0, 0});
+        }
+        addList(plan, backward, LaunchKind::BackwardDiagonal, diagonal, k0);
+        addTiles(plan, backward, LaunchKind::BackwardUpdate, above, k0);
+    }
+    for (std::size_t k = forwardBefore; k < plan.forwardLaunches.size(); ++k)
+        plan.forwardLaunches[k].level = level;
+    for (std::size_t k = backwardBefore; k < backward.size(); ++k)
+        backward[k].level = level;
+}
+
 } // namespace
 
 // The algorithmic flops and bytes of every launch of the factorisation (Launch::flops, Launch::bytes).
@@ -251,46 +429,7 @@ Plan buildPlan(const Symbolic& symbolic)
         }
     }
 
-    // Gather lists (the transpose of relpos, children in increasing order within each slot).
-    if (static_cast<std::int64_t>(symbolic.rows.size()) > INT32_MAX)
-        throw Error(STATUS_INVALID_ARGUMENT, "plan: more than 2^31 row entries");
-    const std::size_t slots = static_cast<std::size_t>(plan.dimension) + symbolic.rows.size();
-    plan.gatherStart.assign(slots + 1, 0);
-    const auto slotOf = [&](const FrontDesc& p, std::int32_t position)
-    {
-        return position < p.c ? static_cast<std::size_t>(p.first + position)
-                              : static_cast<std::size_t>(plan.dimension) + static_cast<std::size_t>(p.rowStart) +
-                                    static_cast<std::size_t>(position - p.c);
-    };
-    for (std::int32_t s = 0; s < count; ++s)
-    {
-        const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
-        if (f.parent < 0)
-            continue;
-        const FrontDesc& p = plan.fronts[static_cast<std::size_t>(f.parent)];
-        for (std::int64_t k = f.rowStart; k < f.rowStart + f.r; ++k)
-            ++plan.gatherStart[slotOf(p, plan.relpos[static_cast<std::size_t>(k)]) + 1];
-    }
-    for (std::size_t slot = 0; slot < slots; ++slot)
-        plan.gatherStart[slot + 1] += plan.gatherStart[slot];
-    plan.gatherRows.assign(static_cast<std::size_t>(plan.gatherStart[slots]), 0);
-    {
-        std::vector<std::int64_t> next(plan.gatherStart.begin(), plan.gatherStart.end() - 1);
-        // children of each parent in increasing order: the parent's child list is in that order
-        for (std::int32_t s = 0; s < count; ++s)
-        {
-            const FrontDesc& p = plan.fronts[static_cast<std::size_t>(s)];
-            for (std::int32_t q = 0; q < p.childCount; ++q)
-            {
-                const FrontDesc& ch = plan.fronts[static_cast<std::size_t>(plan.children[static_cast<std::size_t>(p.childStart + q)])];
-                for (std::int64_t k = ch.rowStart; k < ch.rowStart + ch.r; ++k)
-                {
-                    const std::size_t slot = slotOf(p, plan.relpos[static_cast<std::size_t>(k)]);
-                    plan.gatherRows[static_cast<std::size_t>(next[slot]++)] = static_cast<std::int32_t>(k);
-                }
-            }
-        }
-    }
+    buildGatherLists(plan);
 
     plan.wOffset.assign(total, 0);
     for (const FrontDesc& f : plan.fronts)
@@ -326,6 +465,7 @@ Plan buildPlan(const Symbolic& symbolic)
     for (std::int32_t level = 0; level < plan.levelCount; ++level)
     {
         const auto& members = byLevel[static_cast<std::size_t>(level)];
+        const std::size_t factorBefore = plan.factorLaunches.size();
         // ---- factorisation ----
         // Small fronts in three classes of order (shared memory per block follows the class's largest front).
         std::vector<std::int32_t> small64;
@@ -601,127 +741,10 @@ Plan buildPlan(const Symbolic& symbolic)
         }
         plan.pivotedLaunches.push_back({LaunchKind::LevelEnd, 0, 0, level, 0});
 
-        // ---- forward sweep ----
-        std::vector<std::int32_t> solveSmall;
-        std::vector<std::int32_t> solveLarge;
-        std::int32_t maxColumns = 0;
-        for (const std::int32_t s : members)
-        {
-            const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
-            if (f.c <= SOLVE_SMALL_COLUMNS)
-                solveSmall.push_back(s);
-            else
-            {
-                solveLarge.push_back(s);
-                maxColumns = std::max(maxColumns, f.c);
-            }
-        }
-        // The small supernodes by width class (at most 16, 32 or SOLVE_SMALL_COLUMNS columns): each launch's shared
-        // memory is sized for its widest supernode, so the narrow ones (most of the lowest levels) fit more blocks
-        // per SM. The supernodes of one level are independent, so the split changes no result.
-        std::vector<std::vector<std::int32_t>> smallClasses(3);
-        std::vector<std::int32_t> smallClassColumns(3, 0);
-        for (const std::int32_t s : solveSmall)
-        {
-            const std::int32_t c = plan.fronts[static_cast<std::size_t>(s)].c;
-            const std::size_t k = c <= 16 ? 0 : c <= 32 ? 1 : 2;
-            smallClasses[k].push_back(s);
-            smallClassColumns[k] = std::max(smallClassColumns[k], c);
-        }
-        for (std::size_t k = 0; k < smallClasses.size(); ++k)
-            addList(plan, plan.forwardLaunches, LaunchKind::ForwardSmall, smallClasses[k], 0, smallClassColumns[k]);
-        {
-            // The children's update rows of the large supernodes, by ranges of GATHER_POSITIONS front positions.
-            constexpr std::int32_t GATHER_POSITIONS = 64;
-            std::vector<TileTask> ranges;
-            for (const std::int32_t s : solveLarge)
-            {
-                const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
-                const std::int32_t n = f.c + f.r;
-                for (std::int32_t p0 = 0; p0 < n; p0 += GATHER_POSITIONS)
-                    ranges.push_back({s, p0, std::min(n, p0 + GATHER_POSITIONS), 0});
-            }
-            addTiles(plan, plan.forwardLaunches, LaunchKind::ForwardGather, ranges);
-        }
-        for (const std::int32_t s : members)
-        {
-            const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
-            const bool isLarge = f.c + f.r > SMALL_ORDER; // the factorisation's own split, above
-            for (std::int32_t k0 = 0; k0 < f.c; k0 += BLOCK)
-                (isLarge ? inverseTasksLarge : inverseTasks).push_back({s, k0, 0, 0});
-        }
-        // Steps of SOLVE_STEP columns: the step's diagonal blocks in one launch, then its products with the rows below.
-        constexpr std::int32_t STEP = device::SOLVE_STEP;
-        for (std::int32_t k0 = 0; k0 < maxColumns; k0 += STEP)
-        {
-            std::vector<std::int32_t> diagonal;
-            std::vector<TileTask> below;
-            for (const std::int32_t s : solveLarge)
-            {
-                const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
-                if (f.c <= k0)
-                    continue;
-                diagonal.push_back(s);
-                const std::int32_t kb = std::min(STEP, f.c - k0);
-                for (std::int32_t i0 = k0 + kb; i0 < f.c; i0 += device::TILE)
-                    below.push_back({s, i0, 0, 0});
-                for (std::int32_t i0 = f.c; i0 < f.c + f.r; i0 += device::TILE)
-                    below.push_back({s, i0, 0, 1});
-            }
-            addList(plan, plan.forwardLaunches, LaunchKind::ForwardDiagonal, diagonal, k0);
-            addTiles(plan, plan.forwardLaunches, LaunchKind::ForwardUpdate, below, k0);
-        }
-
-        // ---- backward sweep (collected per level, emitted top level first) ----
-        std::vector<Launch>& backward = backwardByLevel[static_cast<std::size_t>(level)];
-        for (std::size_t k = 0; k < smallClasses.size(); ++k)
-            addList(plan, backward, LaunchKind::BackwardSmall, smallClasses[k], 0, smallClassColumns[k]);
-        // x_F -= L21^T X[R(s)] by 64-column tiles; R(s) longer than SOLVE_ROWS_CHUNK in chunks (task j0: the chunk's
-        // first row, k0: its partial's slot, -1 for an unsplit tile), then the partials summed in chunk order.
-        std::vector<TileTask> rowTiles;
-        std::vector<TileTask> rowSums;
-        std::int64_t slots = 0;
-        for (const std::int32_t s : solveLarge)
-        {
-            const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
-            if (f.r == 0)
-                continue;
-            const std::int32_t chunks = (f.r + device::SOLVE_ROWS_CHUNK - 1) / device::SOLVE_ROWS_CHUNK;
-            for (std::int32_t i0 = 0; i0 < f.c; i0 += device::TILE)
-            {
-                if (chunks == 1)
-                {
-                    rowTiles.push_back({s, i0, 0, -1});
-                    continue;
-                }
-                rowSums.push_back({s, i0, static_cast<std::int32_t>(slots), chunks});
-                for (std::int32_t q = 0; q < chunks; ++q)
-                    rowTiles.push_back({s, i0, q * device::SOLVE_ROWS_CHUNK, static_cast<std::int32_t>(slots++)});
-            }
-        }
-        if (slots > INT32_MAX)
-            throw Error(STATUS_INVALID_ARGUMENT, "plan: too many split backward products in one level");
-        plan.rowPartialSlots = std::max(plan.rowPartialSlots, slots);
-        addTiles(plan, backward, LaunchKind::BackwardRows, rowTiles);
-        addTiles(plan, backward, LaunchKind::BackwardRowsReduce, rowSums);
-        const std::int32_t steps = (maxColumns + STEP - 1) / STEP;
-        for (std::int32_t t = steps - 1; t >= 0; --t)
-        {
-            const std::int32_t k0 = t * STEP;
-            std::vector<std::int32_t> diagonal;
-            std::vector<TileTask> above;
-            for (const std::int32_t s : solveLarge)
-            {
-                const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
-                if (f.c <= k0)
-                    continue;
-                diagonal.push_back(s);
-                for (std::int32_t i0 = 0; i0 < k0; i0 += device::TILE)
-                    above.push_back({s, i0, 0, 0});
-            }
-            addList(plan, backward, LaunchKind::BackwardDiagonal, diagonal, k0);
-            addTiles(plan, backward, LaunchKind::BackwardUpdate, above, k0);
-        }
+        for (std::size_t k = factorBefore; k < plan.factorLaunches.size(); ++k)
+            plan.factorLaunches[k].level = level;
+        addSolveLevel(plan, members, level, backwardByLevel[static_cast<std::size_t>(level)], inverseTasks,
+                      inverseTasksLarge);
     }
     for (std::int32_t level = plan.levelCount; level-- > 0;)
     {
@@ -731,6 +754,52 @@ Plan buildPlan(const Symbolic& symbolic)
     addTiles(plan, plan.inverseLaunches, LaunchKind::InvertDiagonal, inverseTasks);
     addTiles(plan, plan.inverseLaunchesLarge, LaunchKind::InvertDiagonal, inverseTasksLarge);
     plan.mixedOfFactorLaunch.resize(plan.factorLaunches.size(), -1);
+    return plan;
+}
+
+Plan buildSolvePlan(std::int32_t dimension, std::vector<FrontDesc> fronts, std::vector<std::int32_t> children,
+                    std::vector<std::int32_t> rows, std::vector<std::int32_t> relpos, const std::vector<std::int32_t>& level)
+{
+    Plan plan;
+    plan.dimension = dimension;
+    plan.supernodeCount = static_cast<std::int32_t>(fronts.size());
+    plan.fronts = std::move(fronts);
+    plan.children = std::move(children);
+    plan.rows = std::move(rows);
+    plan.relpos = std::move(relpos);
+    plan.rowEntries = static_cast<std::int64_t>(plan.rows.size());
+    plan.level = level;
+    buildGatherLists(plan);
+    plan.supernodeOfColumn.assign(static_cast<std::size_t>(dimension), 0);
+    std::int32_t maxLevel = -1;
+    for (std::int32_t s = 0; s < plan.supernodeCount; ++s)
+    {
+        const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
+        if (f.first < 0 || f.c < 0 || f.first + f.c > dimension)
+            throw Error(STATUS_INTERNAL, "solve plan: supernode " + std::to_string(s) + " outside the equations");
+        for (std::int32_t j = f.first; j < f.first + f.c; ++j)
+            plan.supernodeOfColumn[static_cast<std::size_t>(j)] = s;
+        plan.largestFrontOrder = std::max(plan.largestFrontOrder, f.c + f.r);
+        plan.largestColumns = std::max(plan.largestColumns, f.c);
+        maxLevel = std::max(maxLevel, level[static_cast<std::size_t>(s)]);
+    }
+    plan.levelCount = maxLevel + 1;
+    std::vector<std::vector<std::int32_t>> byLevel(static_cast<std::size_t>(plan.levelCount));
+    for (std::int32_t s = 0; s < plan.supernodeCount; ++s)
+        byLevel[static_cast<std::size_t>(level[static_cast<std::size_t>(s)])].push_back(s);
+    std::vector<std::vector<Launch>> backwardByLevel(static_cast<std::size_t>(plan.levelCount));
+    std::vector<TileTask> inverseTasks;
+    std::vector<TileTask> inverseTasksLarge;
+    for (std::int32_t lv = 0; lv < plan.levelCount; ++lv)
+        addSolveLevel(plan, byLevel[static_cast<std::size_t>(lv)], lv, backwardByLevel[static_cast<std::size_t>(lv)],
+                      inverseTasks, inverseTasksLarge);
+    for (std::int32_t lv = plan.levelCount; lv-- > 0;)
+    {
+        const auto& launches = backwardByLevel[static_cast<std::size_t>(lv)];
+        plan.backwardLaunches.insert(plan.backwardLaunches.end(), launches.begin(), launches.end());
+    }
+    addTiles(plan, plan.inverseLaunches, LaunchKind::InvertDiagonal, inverseTasks);
+    addTiles(plan, plan.inverseLaunchesLarge, LaunchKind::InvertDiagonal, inverseTasksLarge);
     return plan;
 }
 

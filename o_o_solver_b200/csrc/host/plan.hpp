@@ -81,6 +81,9 @@ struct Launch
     // launch's own range (offset, count) is variant 0's.
     std::int64_t altOffset = 0;
     std::int32_t altCount = 0;
+    // The level of the supernodes the launch works on (factorisation and solve launches): a partial factorisation
+    // runs the levels below its trailing supernode's.
+    std::int32_t level = -1;
 };
 
 constexpr int LAUNCH_KIND_COUNT = 14;
@@ -147,6 +150,14 @@ struct Plan
 
 // Builds the plan of a validated symbolic structure.
 Plan buildPlan(const Symbolic& symbolic);
+
+// The solve part of a plan (the gather lists, the columns' supernodes, the forward and backward sweeps' launches and
+// the diagonal blocks to invert) over a structure given directly: supernode s owns the equations [first, first + c)
+// of the solve's order, its panel (c + r rows, ld c + r) at fronts[s].panel, its r rows below at rows[rowStart ..]
+// (equations of the solve's order) and their positions in the parent's front at relpos[rowStart ..] (< c of the
+// parent: its column; else c + its row). `level`: each supernode's level (a parent above its children).
+Plan buildSolvePlan(std::int32_t dimension, std::vector<device::FrontDesc> fronts, std::vector<std::int32_t> children,
+                    std::vector<std::int32_t> rows, std::vector<std::int32_t> relpos, const std::vector<std::int32_t>& level);
 
 // Sets the algorithmic flops and bytes of every factorisation launch; cscTermsOfFront: the matrix terms in each
 // supernode's columns.

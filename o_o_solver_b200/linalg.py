@@ -248,7 +248,6 @@ class SupernodalFactor:
         self.zero_pivots = list(info.zero_pivots[: min(16, int(info.zero_pivot_count))])
         self.delayed_pivot_count = int(info.delayed)
         self.two_by_two_pivot_count = int(info.two_by_two)
-        self.forced_pivot_count = int(info.forced)
         self.is_singular = self.inertia.zero > 0
         self.device_seconds = float(info.device_seconds)
 
@@ -358,6 +357,65 @@ class SupernodalFactor:
             pass
 
 
+class PartialFactor:
+    """PartialFactor (include/oos/linalg/supernodal/PartialFactor.hpp:48-112): the interior of a unit factorised on
+    the GPU, its boundary (the symbolic factor's trailing set, ordered last: its last supernode) left as the Schur
+    complement K* = K_bb - K_bi K_ii^-1 K_ib; condensed loads f* = f_b - K_bi K_ii^-1 f_i and the recovery of the
+    interior u_i = K_ii^-1 (f_i - K_ib u_b) from boundary values. Positive definite FP64 only, as the reference."""
+
+    def __init__(self, symbolic: SymbolicFactor, trailing: int, device: int = 0):
+        self._factor = SupernodalFactor(symbolic, device)
+        self.dimension = symbolic.dof_count
+        self.trailing = int(trailing)
+        self.schur_complement = None
+
+    @classmethod
+    def factorise(cls, symbolic: SymbolicFactor, matrix: SymmetricCsc, trailing: int,
+                  options: FactorOptions | None = None, device: int = 0) -> "PartialFactor":
+        partial = cls(symbolic, trailing, device)
+        partial.refactorise(matrix, options)
+        return partial
+
+    def refactorise(self, matrix: SymmetricCsc, options: FactorOptions | None = None):
+        native = self._factor._options(options)
+        info = nat.FactorInfo()
+        offsets = np.ascontiguousarray(matrix.offsets, dtype=np.int64)
+        rows = np.ascontiguousarray(matrix.rows, dtype=np.int32)
+        values = np.ascontiguousarray(matrix.values, dtype=np.float64)
+        schur = np.zeros((self.trailing, self.trailing), order="F")
+        status = nat.load().oosgpu_factorise_partial(
+            self._factor._handle, len(offsets) - 1, nat.ptr(offsets, nat.i64p), nat.ptr(rows, nat.i32p),
+            nat.ptr(values, nat.f64p), self.trailing, ctypes.byref(native), nat.ptr(schur, nat.f64p),
+            ctypes.byref(info))
+        self._factor._record(info)
+        _check(status)
+        self.schur_complement = schur
+        return self
+
+    @property
+    def inertia(self) -> Inertia:
+        return self._factor.inertia
+
+    def condense_loads(self, loads) -> np.ndarray:
+        """f* = f_b - K_bi K_ii^-1 f_i (trailing x columns) of loads (dimension x columns)."""
+        x = np.asfortranarray(np.asarray(loads, dtype=np.float64).reshape(self.dimension, -1))
+        out = np.zeros((self.trailing, x.shape[1]), order="F")
+        _check(nat.load().oosgpu_partial_condense(self._factor._handle, nat.ptr(x, nat.f64p), self.dimension,
+                                                   x.shape[1], nat.ptr(out, nat.f64p), self.trailing))
+        return out
+
+    def recover(self, loads, trailing_values) -> np.ndarray:
+        """The solution of the unit (dimension x columns) from its loads and its boundary values u_b."""
+        x = np.array(np.asarray(loads, dtype=np.float64).reshape(self.dimension, -1), order="F", copy=True)
+        t = np.asfortranarray(np.asarray(trailing_values, dtype=np.float64).reshape(self.trailing, -1))
+        _check(nat.load().oosgpu_partial_recover(self._factor._handle, nat.ptr(x, nat.f64p), self.dimension,
+                                                  x.shape[1], nat.ptr(t, nat.f64p), self.trailing))
+        return x
+
+    def close(self):
+        self._factor.close()
+
+
 class FactorSolve:
     """Solves with a supernodal factor (FactorSolve.hpp:59-100): B <- A^-1 B for many right-hand sides."""
 
@@ -453,7 +511,7 @@ class ShiftFactorisation:
     shift: float
     inertia: Inertia
     two_by_two: int = 0
-    forced: int = 0
+    delayed: int = 0
 
     @property
     def sturm_count(self) -> int:
@@ -517,7 +575,7 @@ class SparsePencil:
         info = nat.FactorInfo()
         _check(nat.load().oosgpu_pencil_factorise(self._handle, float(shift), ctypes.byref(info)))
         return ShiftFactorisation(float(shift), Inertia(int(info.positive), int(info.negative), int(info.zero)),
-                                  int(info.two_by_two), int(info.forced))
+                                  int(info.two_by_two), int(info.delayed))
 
     def _device_call(self, fn, *blocks):
         """Runs fn on device blocks; host blocks are copied to the device and the last one back."""

@@ -49,6 +49,14 @@ def ref_lib():
     lib.ref_analyse.restype = _vp
     lib.ref_analyse.argtypes = [ctypes.c_int32, _i64p, _i32p, _i32p, _f64p, ctypes.c_int, _i32p, ctypes.c_int,
                                 ctypes.c_int]
+    lib.ref_analyse_trailing.restype = _vp
+    lib.ref_analyse_trailing.argtypes = [ctypes.c_int32, _i64p, _i32p, _i32p, _f64p, ctypes.c_int, _i32p, ctypes.c_int,
+                                         ctypes.c_int, _i32p, ctypes.c_int32]
+    lib.ref_partial_factorise.restype = _vp
+    lib.ref_partial_factorise.argtypes = [_vp, ctypes.c_int32, _i64p, _i32p, _f64p, ctypes.c_int, _f64p]
+    lib.ref_partial_free.argtypes = [_vp]
+    lib.ref_partial_condense.argtypes = [_vp, _f64p, ctypes.c_int64, _f64p]
+    lib.ref_partial_recover.argtypes = [_vp, _f64p, ctypes.c_int64, _f64p]
     lib.ref_symbolic_free.argtypes = [_vp]
     lib.ref_sym_sizes.argtypes = [_vp, _i64p]
     lib.ref_sym_flops.restype = ctypes.c_double
@@ -102,6 +110,7 @@ class RefSymbolic:
     factor_entries: int
     ordering_seconds: float
     analyse_seconds: float
+    trailing_dofs: int = 0
 
     @property
     def first_column(self) -> np.ndarray:
@@ -119,19 +128,23 @@ class RefSymbolic:
             pass
 
 
-def analyse(offsets, neighbours, weights, coords=None, method=0, given_order=None, amalgamate=True, threads=1):
+def analyse(offsets, neighbours, weights, coords=None, method=0, given_order=None, amalgamate=True, threads=1,
+            trailing_nodes=None):
     """ConstrainedOrdering + SymbolicFactor::analyse of the reference on a node graph (method 0 automatic, 1 AMD,
-    2 nested dissection, 3 natural, 4 given order)."""
+    2 nested dissection, 3 natural, 4 given order); trailing_nodes: a trailing set, ordered last (the boundary of a
+    unit: the last supernode)."""
     lib = ref_lib()
+    trailing = None if trailing_nodes is None else np.ascontiguousarray(trailing_nodes, dtype=np.int32)
     offsets = np.ascontiguousarray(offsets, dtype=np.int64)
     neighbours = np.ascontiguousarray(neighbours, dtype=np.int32)
     weights = np.ascontiguousarray(weights, dtype=np.int32)
     n = len(weights)
     coords = None if coords is None else np.ascontiguousarray(coords, dtype=np.float64)
     order = None if given_order is None else np.ascontiguousarray(given_order, dtype=np.int32)
-    handle = lib.ref_analyse(n, _ptr(offsets, _i64p), _ptr(neighbours, _i32p), _ptr(weights, _i32p),
-                             _ptr(coords, _f64p), method if order is None else 4, _ptr(order, _i32p),
-                             1 if amalgamate else 0, threads)
+    handle = lib.ref_analyse_trailing(n, _ptr(offsets, _i64p), _ptr(neighbours, _i32p), _ptr(weights, _i32p),
+                                      _ptr(coords, _f64p), method if order is None else 4, _ptr(order, _i32p),
+                                      1 if amalgamate else 0, threads, _ptr(trailing, _i32p),
+                                      0 if trailing is None else len(trailing))
     if not handle:
         raise RuntimeError("reference analyse: " + lib.ref_last_error().decode())
     sizes = np.zeros(10, dtype=np.int64)
@@ -151,7 +164,7 @@ def analyse(offsets, neighbours, weights, coords=None, method=0, given_order=Non
     lib.ref_sym_times(handle, _ptr(times, _f64p))
     return RefSymbolic(handle, nodes, dofs, count, node_order, fcp, first_position, parent, row_start,
                        rows[:row_entries], float(lib.ref_sym_flops(handle)), int(sizes[4]), int(sizes[5]),
-                       float(times[0]), float(times[1]))
+                       float(times[0]), float(times[1]), int(sizes[8]))
 
 
 @dataclass
@@ -219,6 +232,47 @@ def factorise(symbolic: RefSymbolic, offsets, rows, values, indefinite=False, fa
     ratio = ctypes.c_double()
     lib.ref_factor_info(handle, _ptr(info, _i64p), ctypes.byref(ratio))
     return RefFactor(handle, *(int(v) for v in info[:7]), float(ratio.value), int(info[7]), float(seconds[0]))
+
+
+class RefPartial:
+    """PartialFactor of the reference (src/linalg/supernodal/PartialFactor.cpp): the interior factorised, K* kept."""
+
+    def __init__(self, symbolic, offsets, rows, values, family=-1):
+        lib = ref_lib()
+        self.dimension = symbolic.dof_count
+        self.trailing = symbolic.trailing_dofs
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+        values = np.ascontiguousarray(values, dtype=np.float64)
+        schur = np.zeros((self.trailing, self.trailing), order="F")
+        self.handle = lib.ref_partial_factorise(symbolic.handle, self.dimension, _ptr(offsets, _i64p),
+                                                _ptr(rows, _i32p), _ptr(values, _f64p), family, _ptr(schur, _f64p))
+        if not self.handle:
+            raise RuntimeError("reference partial factorise: " + lib.ref_last_error().decode())
+        self.schur_complement = schur
+
+    def condense(self, loads):
+        x = np.asfortranarray(np.asarray(loads, dtype=np.float64).reshape(self.dimension, -1))
+        out = np.zeros((self.trailing, x.shape[1]), order="F")
+        _check(ref_lib().ref_partial_condense(self.handle, _ptr(x, _f64p), x.shape[1], _ptr(out, _f64p)))
+        return out
+
+    def recover(self, loads, trailing_values):
+        x = np.array(np.asarray(loads, dtype=np.float64).reshape(self.dimension, -1), order="F", copy=True)
+        t = np.asfortranarray(np.asarray(trailing_values, dtype=np.float64).reshape(self.trailing, -1))
+        _check(ref_lib().ref_partial_recover(self.handle, _ptr(x, _f64p), x.shape[1], _ptr(t, _f64p)))
+        return x
+
+    def close(self):
+        if self.handle:
+            ref_lib().ref_partial_free(self.handle)
+            self.handle = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def modes(symbolic: RefSymbolic, offsets, rows, stiffness, mass, mode_count, block_size=8, family=-1, threads=1,

@@ -21,6 +21,7 @@
 #include "oos/linalg/ordering/NodePermutation.hpp"
 #include "oos/linalg/sparse/SymmetricCsc.hpp"
 #include "oos/linalg/supernodal/FactorSolve.hpp"
+#include "oos/linalg/supernodal/PartialFactor.hpp"
 #include "oos/linalg/supernodal/SupernodalFactor.hpp"
 #include "oos/linalg/symbolic/SymbolicFactor.hpp"
 
@@ -105,9 +106,25 @@ extern "C" const char* ref_last_error(void)
     return g_error.c_str();
 }
 
+extern "C" ref_symbolic* ref_analyse_trailing(int32_t node_count, const int64_t* offsets, const int32_t* neighbours,
+                                              const int32_t* weights, const double* coords, int method,
+                                              const int32_t* given_order, int amalgamate, int threads,
+                                              const int32_t* trailing_nodes, int32_t trailing_count);
+
 extern "C" ref_symbolic* ref_analyse(int32_t node_count, const int64_t* offsets, const int32_t* neighbours,
                                      const int32_t* weights, const double* coords, int method,
                                      const int32_t* given_order, int amalgamate, int threads)
+{
+    return ref_analyse_trailing(node_count, offsets, neighbours, weights, coords, method, given_order, amalgamate,
+                                threads, nullptr, 0);
+}
+
+// The same with a trailing set (the boundary of a unit, ordered last: ConstrainedOrdering's trailing nodes, the last
+// supernode of SymbolicFactor::analyse).
+extern "C" ref_symbolic* ref_analyse_trailing(int32_t node_count, const int64_t* offsets, const int32_t* neighbours,
+                                              const int32_t* weights, const double* coords, int method,
+                                              const int32_t* given_order, int amalgamate, int threads,
+                                              const int32_t* trailing_nodes, int32_t trailing_count)
 {
     auto result = std::make_unique<ref_symbolic>();
     const int status = guarded(
@@ -136,15 +153,17 @@ extern "C" ref_symbolic* ref_analyse(int32_t node_count, const int64_t* offsets,
                                               : method == 2 ? OrderingMethod::NestedDissection
                                               : method == 3 ? OrderingMethod::Natural
                                                             : OrderingMethod::Automatic;
-                order = ConstrainedOrdering().order(result->graph, result->weights, positions, {}, chosen,
+                const std::span<const std::int32_t> trailing(trailing_nodes,
+                                                             static_cast<std::size_t>(trailing_count));
+                order = ConstrainedOrdering().order(result->graph, result->weights, positions, trailing, chosen,
                                                     result->budget, pool.get());
             }
             result->orderingSeconds = secondsSince(start);
             const auto analyseStart = std::chrono::steady_clock::now();
             const AmalgamationThresholds thresholds =
                 amalgamate != 0 ? AmalgamationThresholds{} : AmalgamationThresholds::none();
-            result->symbolic =
-                SymbolicFactor::analyse(result->graph, result->weights, order, 0, thresholds, result->budget);
+            result->symbolic = SymbolicFactor::analyse(result->graph, result->weights, order, trailing_count,
+                                                       thresholds, result->budget);
             result->analyseSeconds = secondsSince(analyseStart);
         });
     return status == 0 ? result.release() : nullptr;
@@ -303,6 +322,73 @@ extern "C" int ref_solve(const ref_factor* f, double* b, int64_t ld, int64_t col
             FactorSolve(f->factor, *f->kernels).solve(view);
             if (seconds != nullptr)
                 seconds[0] = secondsSince(start);
+        });
+}
+
+// PartialFactor (src/linalg/supernodal/PartialFactor.cpp): K*, condensed loads and recovery.
+struct ref_partial
+{
+    base::MemoryBudget budget{UNBOUNDED};
+    std::unique_ptr<DenseKernels> kernels;
+    SymmetricCsc matrix;
+    PartialFactor factor;
+};
+
+extern "C" ref_partial* ref_partial_factorise(const ref_symbolic* s, int32_t dimension, const int64_t* col_offsets,
+                                              const int32_t* rows, const double* values, int family,
+                                              double* schur_complement)
+{
+    auto result = std::make_unique<ref_partial>();
+    const int status = guarded(
+        [&]
+        {
+            const auto terms = static_cast<std::size_t>(col_offsets[dimension]);
+            result->matrix = SymmetricCsc::fromCompressedColumns(
+                dimension, std::span<const std::int64_t>(col_offsets, static_cast<std::size_t>(dimension) + 1),
+                std::span<const std::int32_t>(rows, terms), std::span<const double>(values, terms), result->budget);
+            result->kernels = std::make_unique<DenseKernels>(kindOf(family), DenseKernelOptions{});
+            result->factor = PartialFactor::factorise(s->symbolic, result->matrix, *result->kernels, FactorOptions{},
+                                                      result->budget);
+            const DenseMatrix& k = result->factor.schurComplement();
+            for (std::size_t j = 0; j < k.columns(); ++j)
+                for (std::size_t i = 0; i < k.rows(); ++i)
+                    schur_complement[i + j * k.rows()] = k(i, j);
+        });
+    return status == 0 ? result.release() : nullptr;
+}
+
+extern "C" void ref_partial_free(ref_partial* p)
+{
+    delete p;
+}
+
+// f* (trailing x columns, column-major) of loads (dimension x columns, column-major).
+extern "C" int ref_partial_condense(const ref_partial* p, const double* loads, int64_t columns, double* condensed)
+{
+    return guarded(
+        [&]
+        {
+            const auto n = static_cast<std::size_t>(p->factor.dimension());
+            const ConstDenseMatrixView view{loads, n, static_cast<std::size_t>(columns), n};
+            base::MemoryBudget budget{UNBOUNDED};
+            const DenseMatrix f = p->factor.condenseLoads(view, *p->kernels, budget);
+            for (std::size_t j = 0; j < f.columns(); ++j)
+                for (std::size_t i = 0; i < f.rows(); ++i)
+                    condensed[i + j * f.rows()] = f(i, j);
+        });
+}
+
+// loads (dimension x columns) -> the solution with the trailing rows given (trailing x columns).
+extern "C" int ref_partial_recover(const ref_partial* p, double* loads, int64_t columns, const double* trailing)
+{
+    return guarded(
+        [&]
+        {
+            const auto n = static_cast<std::size_t>(p->factor.dimension());
+            const auto t = static_cast<std::size_t>(p->factor.trailingDofCount());
+            const DenseMatrixView x{loads, n, static_cast<std::size_t>(columns), n};
+            const ConstDenseMatrixView b{trailing, t, static_cast<std::size_t>(columns), t};
+            p->factor.recover(x, b, *p->kernels);
         });
 }
 

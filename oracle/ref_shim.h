@@ -28,6 +28,12 @@ const char* ref_last_error(void);
 ref_symbolic* ref_analyse(int32_t node_count, const int64_t* offsets, const int32_t* neighbours,
                           const int32_t* weights, const double* coords, int method, const int32_t* given_order,
                           int amalgamate, int threads);
+/* The same with a trailing set of nodes (the boundary of a unit, ordered last in their given order and forming the
+ * last supernode: ConstrainedOrdering's trailing nodes, SymbolicFactor::analyse's trailingNodeCount). */
+ref_symbolic* ref_analyse_trailing(int32_t node_count, const int64_t* offsets, const int32_t* neighbours,
+                                   const int32_t* weights, const double* coords, int method,
+                                   const int32_t* given_order, int amalgamate, int threads,
+                                   const int32_t* trailing_nodes, int32_t trailing_count);
 void ref_symbolic_free(ref_symbolic* s);
 
 /* sizes[0..9]: nodes, dofs, supernodes, row entries, panel values, factor entries, largest front values,
@@ -89,6 +95,17 @@ int ref_symmetric_eigen(const double* a, int64_t p, int64_t ld, double* eigenval
 /* pencilScaleOf (src/linalg/eigen/PencilScaling.cpp:64-80): the power-of-two scales of a stiffness CSC. */
 int ref_pencil_scale(int32_t dimension, const int64_t* col_offsets, const int32_t* rows, const double* values,
                      double* scale);
+
+/* PartialFactor (src/linalg/supernodal/PartialFactor.cpp:65): the interior of a unit factorised, K* = K_bb -
+ * K_bi K_ii^-1 K_ib written to schur_complement (trailing x trailing, column-major, both triangles). NULL on error. */
+typedef struct ref_partial ref_partial;
+ref_partial* ref_partial_factorise(const ref_symbolic* s, int32_t dimension, const int64_t* col_offsets,
+                                   const int32_t* rows, const double* values, int family, double* schur_complement);
+void ref_partial_free(ref_partial* p);
+/* PartialFactor::condenseLoads: f* = f_b - K_bi K_ii^-1 f_i (trailing x columns) of loads (dimension x columns). */
+int ref_partial_condense(const ref_partial* p, const double* loads, int64_t columns, double* condensed);
+/* PartialFactor::recover: loads (dimension x columns, in place) -> the solution with the trailing rows given. */
+int ref_partial_recover(const ref_partial* p, double* loads, int64_t columns, const double* trailing);
 
 #ifdef __cplusplus
 }

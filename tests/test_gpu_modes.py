@@ -14,6 +14,9 @@ from conftest import has_gpu
 pytestmark = pytest.mark.gpu
 
 EIGENVALUE_TOLERANCE = 1e-9
+# The 20 x 20 plate's lowest root differs by 1.21e-9 between the reference's scalar and AVX2 families (measured with
+# the oracle: modes of this pencil, 12 modes, block 7, family 0 against family 1): three times that.
+GOLDEN_TOLERANCE = {"plate20": 3.6e-9}
 
 
 @pytest.fixture(scope="module")
@@ -85,7 +88,13 @@ def test_lowest_modes_match_reference(kind, size, modes, block, lib, oracle_mod,
     assert len(solution.eigenvalues) == modes
     assert np.all(np.diff(solution.eigenvalues) >= 0)
     relative = np.abs(solution.eigenvalues - ref["eigenvalues"]) / np.abs(ref["eigenvalues"])
-    assert relative.max() <= EIGENVALUE_TOLERANCE, relative
+    # The reference's own kernel families differ on a thin plate's lowest roots by up to a few 1e-9 (the pencil's
+    # conditioning): the bound is 1e-9 or three times that spread, whichever is larger.
+    families = [oracle_mod.modes(sym, k.offsets, k.rows, k.values, m.values, modes, block_size=block, family=f,
+                                 vectors=False)["eigenvalues"] for f in (0, 1)]
+    spread = (np.abs(families[0] - families[1]) / np.abs(families[1])).max()
+    print(f"{kind}{size}: largest relative difference {relative.max():.2e} (reference families {spread:.2e})")
+    assert relative.max() <= max(EIGENVALUE_TOLERANCE, 3.0 * spread), relative
     assert np.all(solution.residual_bounds <= 1e-10)
     check_pairs(k, m, solution.eigenvalues, solution.eigenvectors, (ref["eigenvalues"], ref["eigenvectors"]))
     # Every Sturm point of the GPU's walk is the reference's inertia at that shift.
@@ -207,7 +216,7 @@ def test_modes_match_golden(name, lib, gpu):
         pencil, EigenRequest(mode_count=len(expected)))
     assert solution.is_complete and solution.verified_count == len(expected)
     relative = np.abs(solution.eigenvalues - expected) / np.abs(expected)
-    assert relative.max() <= EIGENVALUE_TOLERANCE, relative
+    assert relative.max() <= GOLDEN_TOLERANCE.get(name, EIGENVALUE_TOLERANCE), relative
     reference_counts = {float(row[0]): int(row[2]) for row in golden["shifts"]}
     for record in solution.shifts:
         if record.shift in reference_counts:
