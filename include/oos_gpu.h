@@ -158,6 +158,13 @@ int oosgpu_partial_recover(oosgpu_factor* factor, double* loads_to_solution, int
 int oosgpu_factor_panel(oosgpu_factor* factor, int32_t s, int64_t* eliminated, int64_t* row_count, double* values,
                         int32_t* rows, double* subdiagonal);
 
+/* No counterpart in the reference: host right-hand sides (dimension x columns, leading dimension ld) copied to the
+ * device ahead of their solve, on a copy stream of the handle's own, so that the copy overlaps what the handle does
+ * meanwhile. deferred 0: the copy starts now; deferred 1: it starts when the next oosgpu_factorise has queued the
+ * upload of its matrix (the two copies share the host link: the matrix first, then the loads while the matrix is
+ * factorised). The next oosgpu_solve or oosgpu_solve_refined on host arrays with the same b, ld and columns uses the
+ * copy; any other solve drops it. b must stay unchanged (and allocated) until that solve. */
+int oosgpu_solve_prefetch(oosgpu_factor* factor, const double* b, int64_t ld, int64_t columns, int32_t deferred);
 /* B <- A^-1 B, B column-major dimension x columns (leading dimension ld), host memory. */
 int oosgpu_solve(oosgpu_factor* factor, double* b, int64_t ld, int64_t columns);
 /* The same on device memory (stream-ordered on the handle's stream). */

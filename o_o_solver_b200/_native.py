@@ -69,6 +69,7 @@ SIGNATURES = [
     ("oosgpu_factor_create", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),
     ("oosgpu_factor_destroy", None, [_vp]),
     ("oosgpu_factor_stream", _vp, [_vp]),
+    ("oosgpu_solve_prefetch", ctypes.c_int, [_vp, _f64p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32]),
     ("oosgpu_factorise_partial", ctypes.c_int, [_vp, ctypes.c_int32, _i64p, _i32p, _f64p, ctypes.c_int32,
                                                  ctypes.POINTER(FactorOptions), _f64p, ctypes.POINTER(FactorInfo)]),
     ("oosgpu_partial_condense", ctypes.c_int, [_vp, _f64p, ctypes.c_int64, ctypes.c_int64, _f64p, ctypes.c_int64]),

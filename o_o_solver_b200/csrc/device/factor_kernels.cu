@@ -489,33 +489,24 @@ __global__ void __launch_bounds__(DIAGONAL_THREADS) diagonalBlocksByColumn(Facto
 // T_IJ = sum_{J <= K < I} L_IK X_KJ, X_IJ = -X_II T_IJ. Products of 8 x 8 tiles (DMMA m8n8k4: lane g = lane / 4
 // holds row g of A and column g of B at k = lane mod 4, and results (g, 2 (lane mod 4)) and the next column), spread
 // over the block's warps; beyond kb the block is the identity, so the tiles run over all 64 rows.
-__global__ void __launch_bounds__(DIAGONAL_THREADS, 2) diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0)
+constexpr int DIAGONAL_LD = BLOCK + 1;                        // the block in shared memory, by columns
+constexpr int DIAGONAL_W_LD = INVERSE_SUB + 1;                // rows of W apart by 17 doubles (distinct banks)
+constexpr int DIAGONAL_P_BLOCK = INVERSE_SUB * (INVERSE_SUB + 1);
+
+// The elimination of a 64 x 64 diagonal block held in shared memory (a: column-major, leading dimension 65, loaded,
+// zero outside its kb x kb corner) by the DIAGONAL_THREADS threads of a block, as diagonalBlocks describes; wRows
+// (64 x 17) and products (3 x 16 x 17) are its scratch. Leaves L below the diagonal, D on it and L^-1 transposed in the
+// strict upper triangle; a zero or non-finite pivot recorded for supernode s.
+__device__ void eliminateDiagonalBlock(const FactorArgs& args, std::int32_t s, int k0, int kb, double* a,
+                                       double* wRows, double* products)
 {
-    constexpr int LD = BLOCK + 1;
+    constexpr int LD = DIAGONAL_LD;
     constexpr int SUB = INVERSE_SUB; // 16
-    constexpr int W_LD = SUB + 1;    // rows of W apart by 17 doubles: a tile's 8 rows on distinct banks
+    constexpr int W_LD = DIAGONAL_W_LD;
     constexpr int P_LD = SUB + 1;
-    constexpr int P_BLOCK = SUB * P_LD;
-    __shared__ double a[BLOCK * LD];
-    __shared__ double wRows[BLOCK * W_LD]; // w(i, q) = y_iq of the current sub-panel, at wRows[i * W_LD + q]
-    __shared__ double products[(BLOCK / SUB - 1) * P_BLOCK];
-    const std::int32_t s = list[blockIdx.x];
-    const FrontDesc f = args.fronts[s];
-    const int n = f.c + f.r;
-    const int kb = min(BLOCK, f.c - k0);
-    double* panel = args.panels + f.panel + static_cast<std::int64_t>(k0) * n + k0;
+    constexpr int P_BLOCK = DIAGONAL_P_BLOCK;
     const int t = threadIdx.x;
     const int lane = t & 31;
-    for (int e = t; e < BLOCK * BLOCK; e += DIAGONAL_THREADS)
-    {
-        const int j = e / BLOCK;
-        const int i = e - j * BLOCK;
-        const bool inside = i < kb && j < kb;
-        copyAsync8(a + i + j * LD, inside ? panel + i + static_cast<std::int64_t>(j) * n : panel, inside);
-    }
-    commitAsyncCopies();
-    waitAsyncCopies<0>();
-    __syncthreads();
     // Beyond kb the block is the identity (its L rows are zero from the load), so the inverse stays finite.
     if (t >= kb && t < BLOCK)
         a[t + t * LD] = 1.0;
@@ -708,12 +699,168 @@ __global__ void __launch_bounds__(DIAGONAL_THREADS, 2) diagonalBlocks(FactorArgs
         }
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(DIAGONAL_THREADS, 2) diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0)
+{
+    constexpr int LD = DIAGONAL_LD;
+    __shared__ double a[BLOCK * LD];
+    __shared__ double wRows[BLOCK * DIAGONAL_W_LD]; // w(i, q) = y_iq of the current sub-panel
+    __shared__ double products[(BLOCK / INVERSE_SUB - 1) * DIAGONAL_P_BLOCK];
+    const std::int32_t s = list[blockIdx.x];
+    const FrontDesc f = args.fronts[s];
+    const int n = f.c + f.r;
+    const int kb = min(BLOCK, f.c - k0);
+    double* panel = args.panels + f.panel + static_cast<std::int64_t>(k0) * n + k0;
+    const int t = threadIdx.x;
+    for (int e = t; e < BLOCK * BLOCK; e += DIAGONAL_THREADS)
+    {
+        const int j = e / BLOCK;
+        const int i = e - j * BLOCK;
+        const bool inside = i < kb && j < kb;
+        copyAsync8(a + i + j * LD, inside ? panel + i + static_cast<std::int64_t>(j) * n : panel, inside);
+    }
+    commitAsyncCopies();
+    waitAsyncCopies<0>();
+    __syncthreads();
+    eliminateDiagonalBlock(args, s, k0, kb, a, wRows, products);
     for (int e = t; e < BLOCK * BLOCK; e += DIAGONAL_THREADS)
     {
         const int j = e / BLOCK;
         const int i = e - j * BLOCK;
         if (i < kb && j < kb)
             panel[i + static_cast<std::int64_t>(j) * n] = a[i + j * LD];
+    }
+}
+
+// A step of the fronts at the top of the tree (a launch with few fronts), the diagonal block and the rows below it
+// in one launch: every task (front, i0, owner j0, slot k0) loads the step's 64 x 64 diagonal block and its own 64 rows
+// below it (one group of asynchronous copies), eliminates the block in shared memory exactly as diagonalBlocks does (so
+// every task of a front holds the same bits), then forms its rows as panelRowsInverse does, L = A21 L11^-T (1 / d), on
+// the FP64 tensor cores. The task with owner = 1 writes the eliminated block (L, D and L^-1) to its front's slot of
+// `blocks` (64 x 64 each), not to the panel, where another task of the front may still be reading the block;
+// copyDiagonalBlocks puts it in place after the launch. Against diagonalBlocks then panelRowsInverse, one memory
+// latency fewer a step and the block's elimination overlapped with the rows' loads, at the price of the elimination
+// repeated by each task of the front. Dynamic shared memory: DIAGONAL_ROWS_SMEM bytes.
+__global__ void __launch_bounds__(DIAGONAL_THREADS, 1) diagonalRows(FactorArgs args, const TileTask* tasks, int k0,
+                                                                   double* blocks)
+{
+    constexpr int LD = DIAGONAL_LD;
+    constexpr int ROWS_LD = TILE + TILE_PAD;
+    extern __shared__ double dynamic[];
+    double* a = dynamic;                                   // 64 x 65
+    double* wRows = a + BLOCK * LD;                        // 64 x 17
+    double* products = wRows + BLOCK * DIAGONAL_W_LD;      // 3 x 16 x 17
+    double* sA = products + (BLOCK / INVERSE_SUB - 1) * DIAGONAL_P_BLOCK; // sA[p * ROWS_LD + ii] = A21(ii, p)
+    double* reciprocal = sA + BLOCK * ROWS_LD;             // 1 / d_j
+    const TileTask task = tasks[blockIdx.x];
+    const FrontDesc f = args.fronts[task.front];
+    const std::int64_t n = f.c + f.r;
+    const int kb = min(BLOCK, f.c - k0);
+    double* block = args.panels + f.panel + static_cast<std::int64_t>(k0) * n + k0;
+    const int t = threadIdx.x;
+    const std::int64_t i0 = task.i0;
+    const int m = i0 < n ? static_cast<int>(n - i0 < TILE ? n - i0 : TILE) : 0;
+    double* rows = args.panels + f.panel + i0 + static_cast<std::int64_t>(k0) * n;
+    for (int e = t; e < BLOCK * BLOCK; e += DIAGONAL_THREADS)
+    {
+        const int j = e / BLOCK;
+        const int i = e - j * BLOCK;
+        const bool inside = i < kb && j < kb;
+        copyAsync8(a + i + j * LD, inside ? block + i + static_cast<std::int64_t>(j) * n : block, inside);
+    }
+    for (int e = t; e < BLOCK * TILE; e += DIAGONAL_THREADS)
+    {
+        const int p = e / TILE;
+        const int ii = e - p * TILE;
+        const bool inside = p < kb && ii < m;
+        copyAsync8(sA + p * ROWS_LD + ii, inside ? rows + ii + static_cast<std::int64_t>(p) * n : block, inside);
+    }
+    commitAsyncCopies();
+    waitAsyncCopies<0>();
+    __syncthreads();
+    eliminateDiagonalBlock(args, task.front, k0, kb, a, wRows, products);
+    if (task.j0 != 0)
+    {
+        double* slot = blocks + static_cast<std::int64_t>(task.k0) * BLOCK * BLOCK;
+        for (int e = t; e < BLOCK * BLOCK; e += DIAGONAL_THREADS)
+        {
+            const int j = e / BLOCK;
+            const int i = e - j * BLOCK;
+            slot[e] = a[i + j * LD];
+        }
+    }
+    if (m == 0)
+        return;
+    for (int j = t; j < BLOCK; j += DIAGONAL_THREADS)
+        reciprocal[j] = j < kb ? 1.0 / a[j + j * LD] : 1.0;
+    __syncthreads();
+    // Y = A21 (L11^-1)^T: 8 warps, each a 32 x 16 part of the 64 x 64 tile; B(p, jj) = L11^-1(jj, p), read from the
+    // block's upper triangle (X(jj, p) at (p, jj)), the unit diagonal, zero above and beyond kb
+    const int lane = t & 31;
+    const int warp = t >> 5;
+    const int wm = (warp >> 2) * 32;
+    const int wn = (warp & 3) * 16;
+    const int g = lane >> 2;
+    const int tq = lane & 3;
+    double acc[4][2][2];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni)
+        {
+            acc[mi][ni][0] = 0.0;
+            acc[mi][ni][1] = 0.0;
+        }
+#pragma unroll 4
+    for (int kk = 0; kk < BLOCK; kk += 4)
+    {
+        const int p = kk + tq;
+        double fa[4];
+        double fb[2];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+            fa[mi] = sA[p * ROWS_LD + wm + mi * 8 + g];
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni)
+        {
+            const int jj = wn + ni * 8 + g;
+            fb[ni] = jj >= kb ? 0.0 : (p < jj ? a[p + jj * LD] : (p == jj ? 1.0 : 0.0));
+        }
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni)
+                dmma8x8x4(acc[mi][ni], fa[mi], fb[ni]);
+    }
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+            {
+                const int ii = wm + mi * 8 + g;
+                const int jj = wn + ni * 8 + 2 * tq + h;
+                if (ii < m && jj < kb)
+                    rows[ii + static_cast<std::int64_t>(jj) * n] = acc[mi][ni][h] * reciprocal[jj];
+            }
+}
+
+// The diagonal blocks diagonalRows eliminated, from their slots (the launch's list order) into the panels.
+__global__ void copyDiagonalBlocks(FactorArgs args, const std::int32_t* list, int k0, const double* blocks)
+{
+    const FrontDesc f = args.fronts[list[blockIdx.x]];
+    const std::int64_t n = f.c + f.r;
+    const int kb = min(BLOCK, f.c - k0);
+    double* block = args.panels + f.panel + static_cast<std::int64_t>(k0) * n + k0;
+    const double* slot = blocks + static_cast<std::int64_t>(blockIdx.x) * BLOCK * BLOCK;
+    for (int e = threadIdx.x; e < BLOCK * BLOCK; e += blockDim.x)
+    {
+        const int j = e / BLOCK;
+        const int i = e - j * BLOCK;
+        if (i < kb && j < kb)
+            block[i + static_cast<std::int64_t>(j) * n] = slot[e];
     }
 }
 

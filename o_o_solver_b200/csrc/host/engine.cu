@@ -200,6 +200,9 @@ public:
         check(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority), "stream priorities");
         check(cudaStreamCreateWithPriority(&m_stream, cudaStreamNonBlocking, greatestPriority), "cudaStreamCreate");
         check(cudaStreamCreateWithPriority(&m_side, cudaStreamNonBlocking, leastPriority), "cudaStreamCreate");
+        check(cudaStreamCreateWithFlags(&m_copyStream, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaEventCreateWithFlags(&m_prefetchDone, cudaEventDisableTiming), "cudaEventCreate");
+        check(cudaEventCreateWithFlags(&m_prefetchStart, cudaEventDisableTiming), "cudaEventCreate");
         check(cudaEventCreateWithFlags(&m_fork, cudaEventDisableTiming), "cudaEventCreate");
         for (cudaEvent_t& e : m_groupDone)
             check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
@@ -227,6 +230,8 @@ public:
         m_blockRatio.allocate(summaryBlocks, "factor: ratios");
         m_blockEquation.allocate(summaryBlocks, "factor: ratio equations");
         m_structureError.allocate(1, "factor: structure check");
+        // the slots of the diagonal blocks a fused step eliminates (at most FUSED_STEP_FRONTS fronts a step)
+        m_diagonalSlots.allocate(8 * 64 * 64, "factor: fused diagonal blocks");
         m_mixedError.allocate(1, "factor: tensor-core status");
         // Shared memory of the small-front kernel: the largest small front, square.
         const int order = m_plan.largestSmallOrder;
@@ -252,6 +257,9 @@ public:
         check(cudaFuncSetAttribute(device::panelRowsInverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(device::PANEL_ROWS_INVERSE_SMEM)),
               "panel rows shared memory");
+        check(cudaFuncSetAttribute(device::diagonalRows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(device::DIAGONAL_ROWS_SMEM)),
+              "fused diagonal shared memory");
         check(cudaFuncSetAttribute(device::panelRowsPivotedInverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(device::PANEL_ROWS_PIVOTED_SMEM)),
               "pivoted panel rows shared memory");
@@ -276,6 +284,10 @@ public:
             cudaStreamSynchronize(m_stream);
         if (m_side != nullptr)
             cudaStreamSynchronize(m_side);
+        if (m_copyStream != nullptr)
+            cudaStreamSynchronize(m_copyStream);
+        cudaEventDestroy(m_prefetchDone);
+        cudaEventDestroy(m_prefetchStart);
         cudaEventDestroy(m_fork);
         for (cudaEvent_t e : m_groupDone)
             cudaEventDestroy(e);
@@ -289,9 +301,70 @@ public:
             cudaStreamDestroy(m_stream);
         if (m_side != nullptr)
             cudaStreamDestroy(m_side);
+        if (m_copyStream != nullptr)
+            cudaStreamDestroy(m_copyStream);
     }
 
     [[nodiscard]] cudaStream_t stream() const noexcept { return m_stream; }
+
+    // Right-hand sides copied ahead of a solve (oosgpu_solve_prefetch): host B (n x columns, ld) into the device
+    // buffer the next host-array solve of the same B uses, on a copy stream of its own, so that the copy overlaps
+    // whatever the factor does meanwhile. The copy starts at once, or, when a factorisation follows, once that
+    // factorisation's matrix is on the device (the two copies would otherwise share the host link and delay the
+    // factorisation's start). B must stay unchanged until the solve.
+    void prefetch(const double* b, std::int64_t ld, std::int64_t columns, bool deferred)
+    {
+        check(cudaSetDevice(m_device), "cudaSetDevice");
+        const std::int32_t n = m_plan.dimension;
+        if (b == nullptr || ld < n || columns < 0)
+            throw Error(STATUS_INVALID_ARGUMENT, "solve prefetch: expected " + std::to_string(n) +
+                                                     " rows (leading dimension >= rows) and columns >= 0");
+        check(cudaStreamSynchronize(m_copyStream), "an earlier prefetch");
+        m_prefetch = {b, ld, columns, false};
+        m_hostB.allocate(static_cast<std::size_t>(n) * static_cast<std::size_t>(columns), "solve: right-hand sides");
+        if (!deferred)
+            issuePrefetch();
+    }
+
+    // The copy of a prefetch not yet issued, on the copy stream after the work the main stream has queued so far.
+    void issuePrefetch()
+    {
+        if (m_prefetch.host == nullptr || m_prefetch.issued)
+            return;
+        const std::int32_t n = m_plan.dimension;
+        check(cudaEventRecord(m_prefetchStart, m_stream), "prefetch event");
+        check(cudaStreamWaitEvent(m_copyStream, m_prefetchStart, 0), "prefetch after the matrix");
+        if (m_prefetch.columns > 0 && n > 0)
+            check(cudaMemcpy2DAsync(m_hostB.get(), static_cast<std::size_t>(n) * sizeof(double), m_prefetch.host,
+                                    static_cast<std::size_t>(m_prefetch.ld) * sizeof(double),
+                                    static_cast<std::size_t>(n) * sizeof(double),
+                                    static_cast<std::size_t>(m_prefetch.columns), cudaMemcpyHostToDevice,
+                                    m_copyStream),
+                  "prefetch right-hand sides");
+        check(cudaEventRecord(m_prefetchDone, m_copyStream), "prefetch event");
+        m_prefetch.issued = true;
+    }
+
+    // The device copy (n x columns, leading dimension n) of host right-hand sides for a solve on the main stream: the
+    // prefetched one when it is this B, else uploaded now.
+    double* rightHandSides(const double* b, std::int64_t ld, std::int64_t columns, const char* what)
+    {
+        const std::int32_t n = m_plan.dimension;
+        const Prefetch ahead = m_prefetch;
+        m_prefetch = {};
+        if (ahead.host == b && ahead.ld == ld && ahead.columns == columns && b != nullptr && ahead.issued)
+        {
+            check(cudaStreamWaitEvent(m_stream, m_prefetchDone, 0), "wait for the prefetched right-hand sides");
+            return m_hostB.get();
+        }
+        check(cudaStreamSynchronize(m_copyStream), "an unused prefetch");
+        m_hostB.allocate(static_cast<std::size_t>(n) * static_cast<std::size_t>(columns), what);
+        check(cudaMemcpy2DAsync(m_hostB.get(), static_cast<std::size_t>(n) * sizeof(double), b,
+                                static_cast<std::size_t>(ld) * sizeof(double), static_cast<std::size_t>(n) * sizeof(double),
+                                static_cast<std::size_t>(columns), cudaMemcpyHostToDevice, m_stream),
+              "upload right-hand sides");
+        return m_hostB.get();
+    }
     [[nodiscard]] const Plan& plan() const noexcept { return m_plan; }
 
     // trailing > 0: the partial factorisation (PartialFactor::factorise): every supernode below the trailing one
@@ -341,6 +414,7 @@ public:
             dRows = m_cscRows.get();
             dValues = m_cscValues.get();
         }
+        issuePrefetch(); // loads prefetched for the solve travel once the matrix has
         if (!m_annotated)
         {
             // The matrix terms of each supernode's columns, for the launches' algorithmic bytes.
@@ -625,6 +699,8 @@ public:
         const auto rowsOf = [](std::int64_t k) { return static_cast<std::size_t>(k) * sizeof(double); };
         m_work.allocate(static_cast<std::size_t>(n) * SOLVE_WIDTH, "solve: rows");
         m_updateRows.allocate(updateRowsPerColumn() * SOLVE_WIDTH, "solve: update rows");
+        check(cudaStreamSynchronize(m_copyStream), "an unused prefetch");
+        m_prefetch = {};
         m_hostB.allocate(static_cast<std::size_t>(n) * static_cast<std::size_t>(columns), "partial factor: loads");
         double* b = m_hostB.get();
         check(cudaMemcpy2DAsync(b, rowsOf(n), loads, rowsOf(ld), rowsOf(n), static_cast<std::size_t>(columns),
@@ -1049,14 +1125,9 @@ public:
                               "solve: update rows");
         double* deviceB = b;
         if (!onDevice)
-        {
-            m_hostB.allocate(static_cast<std::size_t>(n) * static_cast<std::size_t>(columns), "solve: right-hand sides");
-            deviceB = m_hostB.get();
-            check(cudaMemcpy2DAsync(deviceB, static_cast<std::size_t>(n) * sizeof(double), b,
-                                    static_cast<std::size_t>(ld) * sizeof(double), static_cast<std::size_t>(n) * sizeof(double),
-                                    static_cast<std::size_t>(columns), cudaMemcpyHostToDevice, m_stream),
-                  "upload right-hand sides");
-        }
+            deviceB = rightHandSides(b, ld, columns, "solve: right-hand sides");
+        else
+            m_prefetch = {}; // a prefetched host B is dropped by any other solve
         const std::int64_t deviceLd = onDevice ? ld : n;
         check(cudaEventRecord(m_start, m_stream), "event");
         for (std::int64_t c0 = 0; c0 < columns; c0 += SOLVE_WIDTH)
@@ -1491,17 +1562,14 @@ public:
         std::int64_t dLdx = ldx;
         if (!onDevice)
         {
-            m_hostB.allocate(static_cast<std::size_t>(n) * static_cast<std::size_t>(columns), "refinement: B");
             m_hostX.allocate(static_cast<std::size_t>(n) * static_cast<std::size_t>(columns), "refinement: X");
-            check(cudaMemcpy2DAsync(m_hostB.get(), static_cast<std::size_t>(n) * sizeof(double), b,
-                                    static_cast<std::size_t>(ldb) * sizeof(double), static_cast<std::size_t>(n) * sizeof(double),
-                                    static_cast<std::size_t>(columns), cudaMemcpyHostToDevice, m_stream),
-                  "upload right-hand sides");
-            deviceB = m_hostB.get();
+            deviceB = rightHandSides(b, ldb, columns, "refinement: B");
             deviceX = m_hostX.get();
             dLdb = n;
             dLdx = n;
         }
+        else
+            m_prefetch = {}; // a prefetched host B is dropped by any other solve
         check(cudaEventRecord(m_start, m_stream), "event");
         std::vector<double> norms(384);
         for (std::int64_t c0 = 0; c0 < columns; c0 += SOLVE_WIDTH)
@@ -2013,8 +2081,19 @@ private:
                         args, m_lists.get() + launch.offset, launch.k0);
                 break;
             case LaunchKind::PanelRows:
+                if (launch.variant == 1)
+                {
+                    device::diagonalRows<<<launch.count, device::DIAGONAL_THREADS, device::DIAGONAL_ROWS_SMEM,
+                                           stream>>>(args, m_tiles.get() + launch.offset, launch.k0,
+                                                     m_diagonalSlots.get());
+                    break;
+                }
                 device::panelRowsInverse<<<launch.count, device::TILE_THREADS, device::PANEL_ROWS_INVERSE_SMEM,
                                            stream>>>(args, m_tiles.get() + launch.offset, launch.k0);
+                break;
+            case LaunchKind::DiagonalCopy:
+                device::copyDiagonalBlocks<<<launch.count, 256, 0, stream>>>(args, m_lists.get() + launch.offset,
+                                                                             launch.k0, m_diagonalSlots.get());
                 break;
             case LaunchKind::PanelUpdate:
                 device::panelUpdate<<<launch.count, device::TILE_THREADS, 0, stream>>>(
@@ -2112,6 +2191,17 @@ private:
     cudaStream_t m_stream = nullptr;
     // the lookahead's side stream, its fork point and the completion of its groups (alternating)
     cudaStream_t m_side = nullptr;
+    cudaStream_t m_copyStream = nullptr; // prefetched right-hand sides
+    cudaEvent_t m_prefetchDone = nullptr;
+    cudaEvent_t m_prefetchStart = nullptr;
+    struct Prefetch
+    {
+        const double* host = nullptr;
+        std::int64_t ld = 0;
+        std::int64_t columns = 0;
+        bool issued = false;
+    };
+    Prefetch m_prefetch;
     cudaEvent_t m_fork = nullptr;
     cudaEvent_t m_groupDone[2] = {nullptr, nullptr};
     cudaEvent_t m_start = nullptr;
@@ -2163,6 +2253,7 @@ private:
     DeviceArray<double> m_w;
     DeviceArray<std::int64_t> m_wOffset;
     DeviceArray<double> m_frontWork;
+    DeviceArray<double> m_diagonalSlots;
     // Delayed pivots: the exact path's outcome of each front it factorised (null elsewhere), the grown panels and
     // update matrices of this factorisation, the exact path's scratch, and the restated structure the solves use when
     // some front delayed.
@@ -2238,7 +2329,7 @@ private:
         std::int32_t k0;
     };
     // The kind code of the diagonal sweep in a solve's launch profile (after the plan's launch kinds).
-    static constexpr std::int32_t DIAGONAL_SWEEP_KIND = 23;
+    static constexpr std::int32_t DIAGONAL_SWEEP_KIND = 24;
     std::vector<SolveRecord> m_solveRecords;
     std::vector<cudaEvent_t> m_solveEvents;
     bool m_annotated = false;
@@ -2645,6 +2736,17 @@ extern "C" void oosgpu_factor_destroy(oosgpu_factor* factor)
 extern "C" void* oosgpu_factor_stream(oosgpu_factor* factor)
 {
     return factor == nullptr ? nullptr : static_cast<void*>(factor->factor->stream());
+}
+
+extern "C" int oosgpu_solve_prefetch(oosgpu_factor* factor, const double* b, int64_t ld, int64_t columns,
+                                     int32_t deferred)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(factor, "factor");
+            factor->factor->prefetch(b, ld, columns, deferred != 0);
+        });
 }
 
 extern "C" int oosgpu_factorise_partial(oosgpu_factor* factor, int32_t dimension, const int64_t* col_offsets,

@@ -307,7 +307,7 @@ class SupernodalFactor:
                     "backward_small", "backward_rows", "backward_diagonal", "backward_update",
                     "small_fronts_pivoted", "pivoted_diagonal", "permute_earlier_rows", "panel_rows_pivoted",
                     "update_pivoted", "level_end", "invert_diagonal", "update_matrix_mixed", "backward_rows_reduce",
-                    "diagonal_sweep"]
+                    "diagonal_copy", "diagonal_sweep"]
 
     def launch_profile(self, which: str = "factor"):
         """The launches of the last profiled factorisation ("factor") or solve ("solve"), in order: a list of
@@ -331,6 +331,16 @@ class SupernodalFactor:
         counts = np.zeros(2, dtype=np.int64)
         _check(nat.load().oosgpu_factor_launch_counts(self._handle, columns, nat.ptr(counts, nat.i64p)))
         return int(counts[0]), int(counts[1])
+
+    def prefetch(self, b: np.ndarray, deferred: bool = True):
+        """Copies host right-hand sides (n x k, column-major) to the device ahead of their solve, overlapping what the
+        factor does meanwhile: with `deferred`, from the moment the next refactorisation has queued its matrix's
+        upload (the matrix first on the host link, then the loads while it is factorised). The next host-array solve
+        of the same array uses the copy; the array must stay unchanged until then."""
+        if b.ndim != 2 or not b.flags.f_contiguous or b.dtype != np.float64:
+            raise ValueError("prefetch: expected a column-major float64 matrix")
+        _check(nat.load().oosgpu_solve_prefetch(self._handle, nat.ptr(b, nat.f64p), b.shape[0], b.shape[1],
+                                                1 if deferred else 0))
 
     def panel(self, s: int):
         """(values rows x eliminated, row equations, subdiagonal) of supernode s (SupernodalFactor::panel)."""

@@ -314,3 +314,31 @@ def test_kernel_choices_match_reference(name, mode, lib, oracle_mod, gpu):
     else:
         assert report == []
     factor.close()
+
+
+def test_prefetched_right_hand_sides(lib, oracle_mod, gpu):
+    """Loads prefetched before a refactorisation give the same solutions as loads uploaded by the solve; a prefetch of
+    another array, or of the same array with other columns, is not used."""
+    from o_o_solver_b200 import FactorSolve, SupernodalFactor
+
+    model, sym, csc = build_case("plate20", oracle_mod)
+    factor = SupernodalFactor(gpu_symbolic(sym))
+    factor.refactorise(csc)
+    b = np.asfortranarray(model.loads(sym.node_order, 5))
+    plain = b.copy(order="F")
+    FactorSolve(factor).solve(plain)
+    ahead = b.copy(order="F")
+    factor.prefetch(ahead)
+    factor.refactorise(csc)
+    FactorSolve(factor).solve(ahead)
+    assert np.array_equal(ahead, plain)
+    other = b.copy(order="F")
+    factor.prefetch(np.asfortranarray(np.zeros_like(b)))
+    FactorSolve(factor).solve(other)
+    assert np.array_equal(other, plain)
+    narrow = b[:, :3].copy(order="F")
+    factor.prefetch(narrow)
+    x = b[:, :3].copy(order="F")
+    FactorSolve(factor).solve(x)
+    assert np.array_equal(x, plain[:, :3])
+    factor.close()
