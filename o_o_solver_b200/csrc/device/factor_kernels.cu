@@ -733,137 +733,6 @@ __global__ void __launch_bounds__(DIAGONAL_THREADS, 2) diagonalBlocks(FactorArgs
     }
 }
 
-// A step of the fronts at the top of the tree (a launch with few fronts), the diagonal block and the rows below it
-// in one launch: every task (front, i0, owner j0, slot k0) loads the step's 64 x 64 diagonal block and its own 64 rows
-// below it (one group of asynchronous copies), eliminates the block in shared memory exactly as diagonalBlocks does (so
-// every task of a front holds the same bits), then forms its rows as panelRowsInverse does, L = A21 L11^-T (1 / d), on
-// the FP64 tensor cores. The task with owner = 1 writes the eliminated block (L, D and L^-1) to its front's slot of
-// `blocks` (64 x 64 each), not to the panel, where another task of the front may still be reading the block;
-// copyDiagonalBlocks puts it in place after the launch. Against diagonalBlocks then panelRowsInverse, one memory
-// latency fewer a step and the block's elimination overlapped with the rows' loads, at the price of the elimination
-// repeated by each task of the front. Dynamic shared memory: DIAGONAL_ROWS_SMEM bytes.
-__global__ void __launch_bounds__(DIAGONAL_THREADS, 1) diagonalRows(FactorArgs args, const TileTask* tasks, int k0,
-                                                                   double* blocks)
-{
-    constexpr int LD = DIAGONAL_LD;
-    constexpr int ROWS_LD = TILE + TILE_PAD;
-    extern __shared__ double dynamic[];
-    double* a = dynamic;                                   // 64 x 65
-    double* wRows = a + BLOCK * LD;                        // 64 x 17
-    double* products = wRows + BLOCK * DIAGONAL_W_LD;      // 3 x 16 x 17
-    double* sA = products + (BLOCK / INVERSE_SUB - 1) * DIAGONAL_P_BLOCK; // sA[p * ROWS_LD + ii] = A21(ii, p)
-    double* reciprocal = sA + BLOCK * ROWS_LD;             // 1 / d_j
-    const TileTask task = tasks[blockIdx.x];
-    const FrontDesc f = args.fronts[task.front];
-    const std::int64_t n = f.c + f.r;
-    const int kb = min(BLOCK, f.c - k0);
-    double* block = args.panels + f.panel + static_cast<std::int64_t>(k0) * n + k0;
-    const int t = threadIdx.x;
-    const std::int64_t i0 = task.i0;
-    const int m = i0 < n ? static_cast<int>(n - i0 < TILE ? n - i0 : TILE) : 0;
-    double* rows = args.panels + f.panel + i0 + static_cast<std::int64_t>(k0) * n;
-    for (int e = t; e < BLOCK * BLOCK; e += DIAGONAL_THREADS)
-    {
-        const int j = e / BLOCK;
-        const int i = e - j * BLOCK;
-        const bool inside = i < kb && j < kb;
-        copyAsync8(a + i + j * LD, inside ? block + i + static_cast<std::int64_t>(j) * n : block, inside);
-    }
-    for (int e = t; e < BLOCK * TILE; e += DIAGONAL_THREADS)
-    {
-        const int p = e / TILE;
-        const int ii = e - p * TILE;
-        const bool inside = p < kb && ii < m;
-        copyAsync8(sA + p * ROWS_LD + ii, inside ? rows + ii + static_cast<std::int64_t>(p) * n : block, inside);
-    }
-    commitAsyncCopies();
-    waitAsyncCopies<0>();
-    __syncthreads();
-    eliminateDiagonalBlock(args, task.front, k0, kb, a, wRows, products);
-    if (task.j0 != 0)
-    {
-        double* slot = blocks + static_cast<std::int64_t>(task.k0) * BLOCK * BLOCK;
-        for (int e = t; e < BLOCK * BLOCK; e += DIAGONAL_THREADS)
-        {
-            const int j = e / BLOCK;
-            const int i = e - j * BLOCK;
-            slot[e] = a[i + j * LD];
-        }
-    }
-    if (m == 0)
-        return;
-    for (int j = t; j < BLOCK; j += DIAGONAL_THREADS)
-        reciprocal[j] = j < kb ? 1.0 / a[j + j * LD] : 1.0;
-    __syncthreads();
-    // Y = A21 (L11^-1)^T: 8 warps, each a 32 x 16 part of the 64 x 64 tile; B(p, jj) = L11^-1(jj, p), read from the
-    // block's upper triangle (X(jj, p) at (p, jj)), the unit diagonal, zero above and beyond kb
-    const int lane = t & 31;
-    const int warp = t >> 5;
-    const int wm = (warp >> 2) * 32;
-    const int wn = (warp & 3) * 16;
-    const int g = lane >> 2;
-    const int tq = lane & 3;
-    double acc[4][2][2];
-#pragma unroll
-    for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 2; ++ni)
-        {
-            acc[mi][ni][0] = 0.0;
-            acc[mi][ni][1] = 0.0;
-        }
-#pragma unroll 4
-    for (int kk = 0; kk < BLOCK; kk += 4)
-    {
-        const int p = kk + tq;
-        double fa[4];
-        double fb[2];
-#pragma unroll
-        for (int mi = 0; mi < 4; ++mi)
-            fa[mi] = sA[p * ROWS_LD + wm + mi * 8 + g];
-#pragma unroll
-        for (int ni = 0; ni < 2; ++ni)
-        {
-            const int jj = wn + ni * 8 + g;
-            fb[ni] = jj >= kb ? 0.0 : (p < jj ? a[p + jj * LD] : (p == jj ? 1.0 : 0.0));
-        }
-#pragma unroll
-        for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-            for (int ni = 0; ni < 2; ++ni)
-                dmma8x8x4(acc[mi][ni], fa[mi], fb[ni]);
-    }
-#pragma unroll
-    for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-            {
-                const int ii = wm + mi * 8 + g;
-                const int jj = wn + ni * 8 + 2 * tq + h;
-                if (ii < m && jj < kb)
-                    rows[ii + static_cast<std::int64_t>(jj) * n] = acc[mi][ni][h] * reciprocal[jj];
-            }
-}
-
-// The diagonal blocks diagonalRows eliminated, from their slots (the launch's list order) into the panels.
-__global__ void copyDiagonalBlocks(FactorArgs args, const std::int32_t* list, int k0, const double* blocks)
-{
-    const FrontDesc f = args.fronts[list[blockIdx.x]];
-    const std::int64_t n = f.c + f.r;
-    const int kb = min(BLOCK, f.c - k0);
-    double* block = args.panels + f.panel + static_cast<std::int64_t>(k0) * n + k0;
-    const double* slot = blocks + static_cast<std::int64_t>(blockIdx.x) * BLOCK * BLOCK;
-    for (int e = threadIdx.x; e < BLOCK * BLOCK; e += blockDim.x)
-    {
-        const int j = e / BLOCK;
-        const int i = e - j * BLOCK;
-        if (i < kb && j < kb)
-            block[i + static_cast<std::int64_t>(j) * n] = slot[e];
-    }
-}
-
 // The rows below step k0's diagonal block, L21 = A21 L11^-T D^-1, as products on the FP64 tensor cores: for each
 // 64-row half of a task (64 * PANEL_ROW_HALVES rows), Y = A21 (L11^-1)^T with L11^-1 from the block's strict upper
 // triangle (unit diagonal), then l_ij = y_ij (1 / d_j), written in place (a block stages its rows before it writes

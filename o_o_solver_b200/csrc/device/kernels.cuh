@@ -138,11 +138,6 @@ __global__ void assembleStaged(FactorArgs args, const AssemblyTask* pieces, std:
 // Dynamic shared memory: UPDATE_TMA_SMEM bytes.
 __global__ void updateMatrixTma(FactorArgs args, const TileTask* tasks, const void* maps, int* error);
 __global__ void diagonalBlocks(FactorArgs args, const std::int32_t* list, int k0);
-__global__ void diagonalRows(FactorArgs args, const TileTask* tasks, int k0, double* blocks);
-__global__ void copyDiagonalBlocks(FactorArgs args, const std::int32_t* list, int k0, const double* blocks);
-// diagonalRows' shared memory: the block (64 x 65), W (64 x 17), the inverse's products (3 x 16 x 17), the task's rows
-// (64 x 68) and the reciprocal pivots (64), doubles.
-constexpr std::size_t DIAGONAL_ROWS_SMEM = (64 * 65 + 64 * 17 + 3 * 16 * 17 + 64 * 68 + 64) * sizeof(double);
 __global__ void diagonalBlocksByColumn(FactorArgs args, const std::int32_t* list, int k0);
 __global__ void panelRowsInverse(FactorArgs args, const TileTask* tasks, int k0);
 constexpr std::size_t PANEL_ROWS_INVERSE_SMEM = (2 * 64 * (TILE + TILE_PAD) + 64) * sizeof(double);

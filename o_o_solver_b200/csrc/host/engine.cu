@@ -230,8 +230,6 @@ public:
         m_blockRatio.allocate(summaryBlocks, "factor: ratios");
         m_blockEquation.allocate(summaryBlocks, "factor: ratio equations");
         m_structureError.allocate(1, "factor: structure check");
-        // the slots of the diagonal blocks a fused step eliminates (at most FUSED_STEP_FRONTS fronts a step)
-        m_diagonalSlots.allocate(8 * 64 * 64, "factor: fused diagonal blocks");
         m_mixedError.allocate(1, "factor: tensor-core status");
         // Shared memory of the small-front kernel: the largest small front, square.
         const int order = m_plan.largestSmallOrder;
@@ -257,9 +255,6 @@ public:
         check(cudaFuncSetAttribute(device::panelRowsInverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(device::PANEL_ROWS_INVERSE_SMEM)),
               "panel rows shared memory");
-        check(cudaFuncSetAttribute(device::diagonalRows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(device::DIAGONAL_ROWS_SMEM)),
-              "fused diagonal shared memory");
         check(cudaFuncSetAttribute(device::panelRowsPivotedInverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(device::PANEL_ROWS_PIVOTED_SMEM)),
               "pivoted panel rows shared memory");
@@ -2081,19 +2076,8 @@ private:
                         args, m_lists.get() + launch.offset, launch.k0);
                 break;
             case LaunchKind::PanelRows:
-                if (launch.variant == 1)
-                {
-                    device::diagonalRows<<<launch.count, device::DIAGONAL_THREADS, device::DIAGONAL_ROWS_SMEM,
-                                           stream>>>(args, m_tiles.get() + launch.offset, launch.k0,
-                                                     m_diagonalSlots.get());
-                    break;
-                }
                 device::panelRowsInverse<<<launch.count, device::TILE_THREADS, device::PANEL_ROWS_INVERSE_SMEM,
                                            stream>>>(args, m_tiles.get() + launch.offset, launch.k0);
-                break;
-            case LaunchKind::DiagonalCopy:
-                device::copyDiagonalBlocks<<<launch.count, 256, 0, stream>>>(args, m_lists.get() + launch.offset,
-                                                                             launch.k0, m_diagonalSlots.get());
                 break;
             case LaunchKind::PanelUpdate:
                 device::panelUpdate<<<launch.count, device::TILE_THREADS, 0, stream>>>(
@@ -2253,7 +2237,6 @@ private:
     DeviceArray<double> m_w;
     DeviceArray<std::int64_t> m_wOffset;
     DeviceArray<double> m_frontWork;
-    DeviceArray<double> m_diagonalSlots;
     // Delayed pivots: the exact path's outcome of each front it factorised (null elsewhere), the grown panels and
     // update matrices of this factorisation, the exact path's scratch, and the restated structure the solves use when
     // some front delayed.
@@ -2329,7 +2312,7 @@ private:
         std::int32_t k0;
     };
     // The kind code of the diagonal sweep in a solve's launch profile (after the plan's launch kinds).
-    static constexpr std::int32_t DIAGONAL_SWEEP_KIND = 24;
+    static constexpr std::int32_t DIAGONAL_SWEEP_KIND = 23;
     std::vector<SolveRecord> m_solveRecords;
     std::vector<cudaEvent_t> m_solveEvents;
     bool m_annotated = false;

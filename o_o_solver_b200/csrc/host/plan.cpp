@@ -18,8 +18,6 @@ using device::TileTask;
 constexpr int BLOCK = 64;
 constexpr int PANEL_ROWS = 128;                                     // rows of a pivoted panel-rows task
 constexpr int PANEL_ROWS_TASK = device::TILE * device::PANEL_ROW_HALVES; // rows of a panelRowsInverse task
-// Steps of at most this many fronts run their diagonal blocks and rows below in one launch (diagonalRows).
-constexpr int FUSED_STEP_FRONTS = 8; // the engine keeps 8 slots of 64 x 64 for their blocks
 
 void addList(Plan& plan, std::vector<Launch>& launches, LaunchKind kind, const std::vector<std::int32_t>& list,
              std::int32_t k0 = 0, std::int32_t smemOrder = 0)
@@ -310,21 +308,9 @@ void annotate(Plan& plan, const std::vector<std::int64_t>& cscTermsOfFront)
                 const FrontDesc& f = front(t.front);
                 const std::int64_t n = f.c + f.r;
                 const std::int64_t kb = std::min<std::int64_t>(BLOCK, f.c - launch.k0);
-                const std::int64_t rows = std::max<std::int64_t>(std::min<std::int64_t>(PANEL_ROWS_TASK, n - t.i0), 0);
+                const std::int64_t rows = std::min<std::int64_t>(PANEL_ROWS_TASK, n - t.i0);
                 flops += static_cast<double>(rows) * static_cast<double>(kb * (kb - 1) + kb);
                 bytes += 2.0 * V * static_cast<double>(rows * kb);
-                if (launch.variant == 1 && t.j0 != 0) // the fused form's diagonal block, once per front
-                {
-                    flops += columnFlops(kb, 0, kb);
-                    bytes += 2.0 * V * static_cast<double>(kb * (kb + 1) / 2);
-                }
-                break;
-            }
-            case LaunchKind::DiagonalCopy:
-            {
-                const FrontDesc& f = front(plan.lists[at]);
-                const std::int64_t kb = std::min<std::int64_t>(BLOCK, f.c - launch.k0);
-                bytes += 2.0 * V * static_cast<double>(kb * kb);
                 break;
             }
             case LaunchKind::PanelUpdate:
@@ -575,7 +561,6 @@ Plan buildPlan(const Symbolic& symbolic)
             {
                 std::vector<std::int32_t> diagonal;
                 std::vector<TileTask> rowTasks;
-                std::vector<TileTask> fusedTasks;
                 std::vector<TileTask> updateTiles;
                 std::vector<TileTask> macroTiles;
                 std::vector<TileTask> farTiles;
@@ -591,11 +576,6 @@ Plan buildPlan(const Symbolic& symbolic)
                     diagonal.push_back(s);
                     for (std::int32_t i0 = k0 + kb; i0 < n; i0 += PANEL_ROWS_TASK)
                         rowTasks.push_back({s, i0, 0, 0});
-                    // the fused form: the first task of a front writes its diagonal block (a front without rows
-                    // below has that task alone, i0 = n)
-                    fusedTasks.push_back({s, k0 + kb < n ? k0 + kb : n, 1, static_cast<std::int32_t>(diagonal.size() - 1)});
-                    for (std::int32_t i0 = k0 + kb + PANEL_ROWS_TASK; i0 < n; i0 += PANEL_ROWS_TASK)
-                        fusedTasks.push_back({s, i0, 0, 0});
                     const std::int32_t origin = k0 + BLOCK;
                     for (std::int32_t j0 = origin; j0 < macroEnd; j0 += device::TILE)
                         for (std::int32_t i0 = j0; i0 < n; i0 += device::TILE)
@@ -606,20 +586,8 @@ Plan buildPlan(const Symbolic& symbolic)
                                 (j0 < macroEnd + device::PANEL_MACRO ? macroTiles : farTiles)
                                     .push_back({s, i0, j0, macroEnd - macroStart});
                 }
-                // A step of a few fronts (the top of the tree, where one launch holds a front or a handful): its
-                // diagonal blocks and rows in one launch (PanelRows, variant 1: diagonalRows), every task repeating
-                // its front's block elimination; otherwise the block elimination once per front, then the rows.
-                if (diagonal.size() <= static_cast<std::size_t>(FUSED_STEP_FRONTS))
-                {
-                    addTiles(plan, plan.factorLaunches, LaunchKind::PanelRows, fusedTasks, k0);
-                    plan.factorLaunches.back().variant = 1;
-                    addList(plan, plan.factorLaunches, LaunchKind::DiagonalCopy, diagonal, k0);
-                }
-                else
-                {
-                    addList(plan, plan.factorLaunches, LaunchKind::DiagonalBlocks, diagonal, k0);
-                    addTiles(plan, plan.factorLaunches, LaunchKind::PanelRows, rowTasks, k0);
-                }
+                addList(plan, plan.factorLaunches, LaunchKind::DiagonalBlocks, diagonal, k0);
+                addTiles(plan, plan.factorLaunches, LaunchKind::PanelRows, rowTasks, k0);
                 addTiles(plan, plan.factorLaunches, LaunchKind::PanelUpdate, updateTiles, k0);
                 const std::int32_t previousGroup = plan.sideGroups - 1;
                 if (!farTiles.empty())

@@ -51,9 +51,7 @@ enum class LaunchKind : int
     // mixed precision: the update matrices by 128 x 128 tiles on tcgen05 (3xTF32), in place of UpdateMatrix
     UpdateMatrixMixed,
     // the sums of the split products of BackwardRows (supernodes with more than SOLVE_ROWS_CHUNK rows)
-    BackwardRowsReduce,
-    // after a fused step (PanelRows, variant 1): the eliminated diagonal blocks from their slots into the panels
-    DiagonalCopy
+    BackwardRowsReduce
 };
 
 // One batched launch: `count` items from `offset` in the array of its kind (front lists: int32; tiles: TileTask;

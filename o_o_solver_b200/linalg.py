@@ -307,7 +307,7 @@ class SupernodalFactor:
                     "backward_small", "backward_rows", "backward_diagonal", "backward_update",
                     "small_fronts_pivoted", "pivoted_diagonal", "permute_earlier_rows", "panel_rows_pivoted",
                     "update_pivoted", "level_end", "invert_diagonal", "update_matrix_mixed", "backward_rows_reduce",
-                    "diagonal_copy", "diagonal_sweep"]
+                    "diagonal_sweep"]
 
     def launch_profile(self, which: str = "factor"):
         """The launches of the last profiled factorisation ("factor") or solve ("solve"), in order: a list of
