@@ -122,6 +122,7 @@ struct TileOperands
 // (TILE_SLICE rows of TILE + TILE_PAD doubles) and the slice's d values.
 constexpr int TILE_SLICE = 8;
 constexpr int TILE_STAGES = 4;
+constexpr int NARROW_COLUMNS = 16; // a product with at most this many columns of C runs narrow (tileAccumulate)
 constexpr int TILE_STAGE_DOUBLES = 2 * TILE_SLICE * (TILE + TILE_PAD) + TILE_SLICE;
 constexpr int TILE_SMEM_DOUBLES = TILE_STAGES * TILE_STAGE_DOUBLES; // 37,120 bytes
 
@@ -174,8 +175,14 @@ __device__ __forceinline__ void tileAccumulate(const TileOperands& op, double* s
     const int wm = (warp >> 1) * 32;
     const int wn = (warp & 1) * 32;
     const bool scaled = op.d != nullptr;
+    // A narrow product (n <= 16 columns: the solves' 8-column blocks, the edges of a panel) has only the two column
+    // tiles of the even warps to fill: the odd warps take every other slice of K for the same tiles instead (the
+    // slices' parities split between the pair), and hand their sums to their even partner at the end (in slice
+    // order per parity, so the sums do not depend on timing).
+    const bool narrow = op.n <= NARROW_COLUMNS;
+    const bool helper = narrow && (warp & 1) != 0;
 
-    if (!ACCUMULATE)
+    if (!ACCUMULATE || helper)
     {
 #pragma unroll
         for (int mi = 0; mi < 4; ++mi)
@@ -214,7 +221,8 @@ __device__ __forceinline__ void tileAccumulate(const TileOperands& op, double* s
                 const std::int64_t row = op.bIndex != nullptr ? op.bIndex[kpb] : kpb;
                 srcB = op.b + jj * op.bRowStride + row * op.bColStride;
             }
-            copyAsync8(sB + pb * LD + jj, srcB, okB);
+            if (!narrow || jj < NARROW_COLUMNS) // a narrow product reads no column of B beyond the first 16
+                copyAsync8(sB + pb * LD + jj, srcB, okB);
         }
         if (tid < TILE_SLICE)
         {
@@ -243,6 +251,31 @@ __device__ __forceinline__ void tileAccumulate(const TileOperands& op, double* s
         const double* sA = smem + (t % TILE_STAGES) * TILE_STAGE_DOUBLES;
         const double* sB = sA + TILE_SLICE * LD;
         const double* sD = sB + TILE_SLICE * LD;
+        if (narrow)
+        {
+            if ((warp & 1) != (t & 1))
+                continue; // the partner's slice
+#pragma unroll
+            for (int kk = 0; kk < TILE_SLICE; kk += 4)
+            {
+                const int pr = kk + (lane & 3);
+                const double dp = scaled ? sD[pr] : 1.0;
+                double fa[4];
+                double fb[2];
+#pragma unroll
+                for (int mi = 0; mi < 4; ++mi)
+                    fa[mi] = sA[pr * LD + wm + mi * 8 + (lane >> 2)];
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni)
+                    fb[ni] = scaled ? sB[pr * LD + ni * 8 + (lane >> 2)] * dp : sB[pr * LD + ni * 8 + (lane >> 2)];
+#pragma unroll
+                for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 2; ++ni)
+                        dmma8x8x4(acc[mi][ni], fa[mi], fb[ni]);
+            }
+            continue;
+        }
 #pragma unroll
         for (int kk = 0; kk < TILE_SLICE; kk += 4)
         {
@@ -264,6 +297,35 @@ __device__ __forceinline__ void tileAccumulate(const TileOperands& op, double* s
         }
     }
     waitAsyncCopies<0>();
+    if (narrow)
+    {
+        // the odd warps' sums into their even partners' tiles (the pipeline's shared memory, every stage read)
+        __syncthreads();
+        double* hand = smem + (warp >> 1) * (32 * 16) + lane * 16;
+        if (helper)
+        {
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni)
+                {
+                    hand[(mi * 2 + ni) * 2] = acc[mi][ni][0];
+                    hand[(mi * 2 + ni) * 2 + 1] = acc[mi][ni][1];
+                }
+        }
+        __syncthreads();
+        if (!helper)
+        {
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni)
+                {
+                    acc[mi][ni][0] += hand[(mi * 2 + ni) * 2];
+                    acc[mi][ni][1] += hand[(mi * 2 + ni) * 2 + 1];
+                }
+        }
+    }
 }
 
 // acc += A B on one 64 x 64 tile with both operands in shared memory (TILE_THREADS threads, the fragments of
