@@ -286,7 +286,7 @@ def modes_leg(args, device, rank, world):
            "value": run["seconds"], "unit": "s", "factorisations": solution.factorisation_count,
            "block_steps": solution.block_steps, "complete": solution.is_complete,
            "verified": solution.verified_count, "phases_s": {k: round(v, 4) for k, v in solution.phases.items()},
-           "factor_device_s": round(solution.factor_seconds, 4)}
+           "slow_paths": solution.slow_paths, "factor_device_s": round(solution.factor_seconds, 4)}
     golden = os.path.join(ROOT, "tests", "golden", "modes", f"{name}.npz")
     if os.path.exists(golden):
         expected = np.load(golden)["eigenvalues"]

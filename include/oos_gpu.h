@@ -75,6 +75,10 @@ int oosgpu_symbolic_from_partition(int32_t node_count, const int64_t* offsets, c
 /* sizes[0..7]: dofs, supernodes, row entries, panel values, factor entries, levels, update values, 0;
  * flops: SymbolicFactor::flopCount. */
 int oosgpu_symbolic_sizes(const oosgpu_symbolic* symbolic, int64_t sizes[8], double* flops);
+/* The solves' chain launches of the symbolic structure's plan, built on the host (no device needed): [0] launches,
+ * [1] tasks, [2] ready flags, [3] tasks of the largest launch. Building the plan checks that every chain task is listed
+ * after the blocks it waits on (an internal error otherwise). No counterpart in the reference's API. */
+int oosgpu_symbolic_solve_chains(const oosgpu_symbolic* symbolic, int64_t counts[4]);
 int oosgpu_symbolic_rows(const oosgpu_symbolic* symbolic, int64_t* row_start, int32_t* rows);
 void oosgpu_symbolic_destroy(oosgpu_symbolic* symbolic);
 
@@ -320,6 +324,11 @@ int oosgpu_modes_solve_start(oosgpu_pencil* pencil, const oosgpu_eigen_request* 
  * wall seconds of [2] the factorisations, [3] the operator (solves and mass products), [4] the M-orthogonalisation
  * and the basis products, [5] the projected problem. */
 int oosgpu_modes_summary(const oosgpu_modes* modes, int64_t counts[6], double seconds[6]);
+/* Where a solve's orthogonalisation went. counts: [0] blocks that met a dependent column and were orthonormalised
+ * column by column (the reference's MassOrthogonalizer fallback), [1] one-column operator applications that replaced
+ * dependent columns; seconds (wall, parts of seconds[4] of the summary): [0] start blocks, [1] block steps, [2] thick
+ * restarts, [3] harvests of converged pairs. Either may be null. No counterpart in the reference's API. */
+int oosgpu_modes_work(const oosgpu_modes* modes, int64_t counts[2], double seconds[4]);
 /* The eigenvalues (increasing) and their residual bounds ||Op y - theta y||_M / |theta|. */
 int oosgpu_modes_values(const oosgpu_modes* modes, double* eigenvalues, double* residual_bounds);
 /* The M-orthonormal eigenvectors, dimension x count, into host memory of leading dimension ld. */

@@ -64,6 +64,7 @@ SIGNATURES = [
     ("oosgpu_symbolic_from_partition", ctypes.c_int, [ctypes.c_int32, _i64p, _i32p, _i32p, _i32p, ctypes.c_int32,
                                                       _i32p, _i32p, ctypes.POINTER(_vp)]),
     ("oosgpu_symbolic_sizes", ctypes.c_int, [_vp, _i64p, _f64p]),
+    ("oosgpu_symbolic_solve_chains", ctypes.c_int, [_vp, _i64p]),
     ("oosgpu_symbolic_rows", ctypes.c_int, [_vp, _i64p, _i32p]),
     ("oosgpu_symbolic_destroy", None, [_vp]),
     ("oosgpu_factor_create", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),
@@ -110,6 +111,7 @@ SIGNATURES = [
     ("oosgpu_modes_solve_start", ctypes.c_int, [_vp, ctypes.POINTER(EigenRequest), ctypes.POINTER(LanczosOptions),
                                                 _vp, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(_vp)]),
     ("oosgpu_modes_summary", ctypes.c_int, [_vp, _i64p, _f64p]),
+    ("oosgpu_modes_work", ctypes.c_int, [_vp, _i64p, _f64p]),
     ("oosgpu_modes_values", ctypes.c_int, [_vp, _f64p, _f64p]),
     ("oosgpu_modes_vectors", ctypes.c_int, [_vp, _f64p, ctypes.c_int64]),
     ("oosgpu_modes_vectors_device", _vp, [_vp]),

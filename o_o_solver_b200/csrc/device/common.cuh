@@ -52,9 +52,6 @@ constexpr int TILE_PAD = 4;
 // The row stride of a staged 64 x 64 inverse block read as an m8n8k4 operand (either orientation): conflict-free too.
 constexpr int INVERSE_LD = TILE + TILE_PAD;
 constexpr int TILE_THREADS = 128;
-// The columns of a large supernode one diagonal step of the solves covers (four 64 x 64 diagonal blocks; the products
-// with the rows below or above then run with K = SOLVE_STEP).
-constexpr int SOLVE_STEP = 256;
 // The columns of a macro panel of the factorisation: the 64-column steps inside it update its own later columns, and
 // once it is done it updates the rest of the front's panel in one product of K = PANEL_MACRO.
 constexpr int PANEL_MACRO = 256;
@@ -131,6 +128,15 @@ __device__ __forceinline__ void copyAsync8(double* sharedDst, const double* glob
 {
     const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(sharedDst));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(globalSrc), "r"(valid ? 8 : 0)
+                 : "memory");
+}
+
+// A 16-byte asynchronous copy global -> shared through L2 only (both addresses 16-byte aligned); zero-filled when
+// `valid` is false.
+__device__ __forceinline__ void copyAsync16(double* sharedDst, const double* globalSrc, bool valid)
+{
+    const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(sharedDst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(globalSrc), "r"(valid ? 16 : 0)
                  : "memory");
 }
 

@@ -78,6 +78,12 @@ struct SolveArgs
     int dimension;
     // The partial products of split backward row tiles: slot q at rowPartials + q * TILE * TILE (64 x 64 by rows).
     double* rowPartials;
+    // The chain launches' ticket counters and ready flags (zero before each sweep), the word that makes every chain
+    // task stop waiting once one wait has run out, and the host-visible record of that (mapped host memory).
+    int* chainTickets;
+    int* chainFlags;
+    int* chainStop;
+    int* chainFailed;
 };
 
 __global__ void assembleFronts(FactorArgs args, const AssemblyTask* tasks, std::int32_t* structureError);
@@ -154,10 +160,6 @@ __global__ void forwardSmall(SolveArgs a, const std::int32_t* list, int cmax);
 __global__ void gatherColumns(SolveArgs a, std::int32_t s);
 __global__ void forwardGather(SolveArgs a, const TileTask* tasks);
 __global__ void invertDiagonal(FactorArgs args, const TileTask* tasks);
-// Dynamic shared memory of forwardDiagonal / backwardDiagonal: the tile pipeline, one block's inverse and a 64-row block
-// of TILE + TILE_PAD (laid out for the widest tile of right-hand sides).
-constexpr std::size_t STEP_SOLVE_SMEM = static_cast<std::size_t>(TILE_SMEM_DOUBLES + 64 * INVERSE_LD + 64 * (TILE + TILE_PAD)) *
-                                        sizeof(double);
 // The row stride of a small supernode's staged inverse for c4 (its columns rounded up to 4): at least c4 and 4 more than
 // a multiple of 16 (conflict-free fragment reads).
 __host__ __device__ constexpr int smallInverseLd(int c4)
@@ -179,16 +181,25 @@ constexpr std::size_t smallSolveSmem(int columns)
                                     ((columns + 3) & ~3) * (TILE + TILE_PAD)) *
            sizeof(double);
 }
-__global__ void forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0);
-__global__ void forwardUpdate(SolveArgs a, const TileTask* tasks, int k0);
+// The chains of the large supernodes (solve_kernels.cu). A task's shared memory: a region for its product's pipeline
+// (CHAIN_STAGES slices of CHAIN_SLICE columns of A and of x; or, with an odd number of right-hand sides, the A slices
+// and then CHAIN_B_DOUBLES for a chunk of solved blocks of x), reused at the end for the 64-row block b, and the
+// inverse of its diagonal block.
+constexpr int CHAIN_SLICE = 16;
+constexpr int CHAIN_STAGES = 4;
+constexpr int CHAIN_LD = TILE + TILE_PAD;
+constexpr int CHAIN_B_DOUBLES = TILE * CHAIN_LD;
+constexpr int CHAIN_REGION_DOUBLES = CHAIN_STAGES * 2 * CHAIN_SLICE * CHAIN_LD;
+static_assert(CHAIN_REGION_DOUBLES >= CHAIN_STAGES * CHAIN_SLICE * CHAIN_LD + CHAIN_B_DOUBLES, "chain region");
+constexpr std::size_t CHAIN_SMEM = static_cast<std::size_t>(CHAIN_REGION_DOUBLES + 64 * INVERSE_LD) * sizeof(double);
+__global__ void forwardChain(SolveArgs a, const TileTask* tasks, int slot);
+__global__ void backwardChain(SolveArgs a, const TileTask* tasks, int slot);
 __global__ void diagonalSweep(SolveArgs a, const double* diagonal, int dimension);
 // D of a positive definite factor as one contiguous vector (diagonal[eq] = d_eq), gathered once per factorisation.
 __global__ void gatherDiagonal(FactorArgs args, const std::int32_t* supernodeOfColumn, int dimension, double* diagonal);
 __global__ void backwardSmall(SolveArgs a, const std::int32_t* list, int cmax);
 __global__ void backwardRows(SolveArgs a, const TileTask* tasks);
 __global__ void backwardRowsReduce(SolveArgs a, const TileTask* tasks);
-__global__ void backwardDiagonal(SolveArgs a, const std::int32_t* list, int k0);
-__global__ void backwardUpdate(SolveArgs a, const TileTask* tasks, int k0);
 __global__ void toRows(const double* b, std::int64_t ld, int c0, int width, int dimension, double* x,
                        const double* scale);
 __global__ void fromRows(const double* x, int c0, int width, int dimension, double* b, std::int64_t ld,

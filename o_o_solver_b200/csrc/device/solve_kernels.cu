@@ -7,8 +7,8 @@
 // rows and leaves the update rows of R(s) for its parent, so no two supernodes write one value and the sums do not
 // depend on the scheduling. The backward sweep gathers the solved rows R(s) and substitutes back.
 //
-// Small supernodes (c <= 64) run one block each; larger ones run as 64-column steps of a diagonal block solve and tile
-// products on the FP64 tensor cores (tileProduct).
+// Small supernodes (c <= 64) run one block each; the larger ones of a level run as one launch of dataflow tasks, one
+// per 64-row block (the chains, below), their products on the FP64 tensor cores.
 
 #include "kernels.cuh"
 
@@ -421,104 +421,6 @@ __device__ __forceinline__ void stepTriangle(const double* inv, const double* b,
             }
 }
 
-// The rows [k0, k0 + kb) of x_F of a large supernode, kb <= SOLVE_STEP, by 64-row blocks j: b_j = x_j - L(j, <j) x_<j
-// (the earlier blocks of the step, one tile product on the FP64 tensor cores), then x_j = L_jj^-1 b_j as the product
-// with the stored inverse (every value independent). One block of TILE_THREADS per supernode; dynamic shared memory
-// STEP_SOLVE_SMEM.
-__global__ void __launch_bounds__(TILE_THREADS) forwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
-{
-    constexpr int LD = INVERSE_LD;
-    extern __shared__ double stage[];
-    double* pipe = stage;
-    double* inv = stage + TILE_SMEM_DOUBLES;  // 64 x INVERSE_LD
-    double* b = inv + SOLVE_BLOCK * LD;       // 64 x XF_LD
-    const FrontDesc f = a.fronts[list[blockIdx.x]];
-    const int w = a.width;
-    const std::int64_t n = f.c + f.r;
-    const int kb = min(SOLVE_STEP, f.c - k0);
-    double* xStep = a.x + static_cast<std::int64_t>(f.first + k0) * w;
-    for (int j0 = 0; j0 < kb; j0 += SOLVE_BLOCK)
-    {
-        const int jb = min(SOLVE_BLOCK, kb - j0);
-        stageBlockInverse(a, f, k0 + j0, jb, inv);
-        commitAsyncCopies();
-        TileOperands op;
-        op.a = a.panels + f.panel + (k0 + j0) + static_cast<std::int64_t>(k0) * n; // A(ii, p) = L(k0 + j0 + ii, k0 + p)
-        op.aRowStride = 1;
-        op.aColStride = n;
-        op.b = xStep;
-        op.bRowStride = 1;
-        op.bColStride = w;
-        op.bIndex = nullptr;
-        op.d = nullptr;
-        op.dStride = 0;
-        op.c = nullptr;
-        op.cRowStride = 0;
-        op.cColStride = 0;
-        op.m = jb;
-        op.n = w;
-        op.k = j0;
-        op.lower = false;
-        op.lowerOffset = 0;
-        TileAccumulators acc;
-        tileAccumulate(op, pipe, acc);
-        double* xBlock = xStep + static_cast<std::int64_t>(j0) * w;
-#pragma unroll
-        for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-                for (int h = 0; h < 2; ++h)
-                {
-                    const int ii = tileRow(mi);
-                    const int jj = tileColumn(ni, h);
-                    b[ii * XF_LD + jj] = ii < jb && jj < w ? xBlock[ii * w + jj] - acc[mi][ni][h] : 0.0;
-                }
-        __syncthreads();
-        stepTriangle<false>(inv, b, jb, w, xBlock, acc);
-        __syncthreads();
-    }
-}
-
-// Step t's block applied to the rows below it: a tile of 64 rows either in x_F (i0 < c, task.k0 = 0) or in the update
-// rows (i0 >= c, task.k0 = 1); C -= L(i, k0:k0+kb) x_block.
-__global__ void __launch_bounds__(TILE_THREADS) forwardUpdate(SolveArgs a, const TileTask* tasks, int k0)
-{
-    __shared__ double smem[TILE_SMEM_DOUBLES];
-    const TileTask task = tasks[blockIdx.x];
-    const FrontDesc f = a.fronts[task.front];
-    const std::int64_t n = f.c + f.r;
-    const int w = a.width;
-    const double* panel = a.panels + f.panel;
-    TileOperands op;
-    op.a = panel + task.i0 + static_cast<std::int64_t>(k0) * n;
-    op.aRowStride = 1;
-    op.aColStride = n;
-    op.b = a.x + static_cast<std::int64_t>(f.first + k0) * w;
-    op.bRowStride = 1;
-    op.bColStride = w;
-    op.bIndex = nullptr;
-    op.d = nullptr;
-    op.dStride = 0;
-    if (task.i0 < f.c)
-    {
-        op.c = a.x + static_cast<std::int64_t>(f.first + task.i0) * w;
-        op.m = min(TILE, f.c - task.i0);
-    }
-    else
-    {
-        op.c = a.updates + (f.rowStart + (task.i0 - f.c)) * w;
-        op.m = static_cast<int>(n - task.i0 < TILE ? n - task.i0 : TILE);
-    }
-    op.cRowStride = w;
-    op.cColStride = 1;
-    op.n = w;
-    op.k = min(SOLVE_STEP, f.c - k0);
-    op.lower = false;
-    op.lowerOffset = 0;
-    tileProduct(op, smem);
-}
-
 // The diagonal sweep: X[eq] /= d_eq.
 __global__ void diagonalSweep(SolveArgs a, const double* diagonal, int dimension)
 {
@@ -682,95 +584,562 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardRowsReduce(SolveArgs a, 
     }
 }
 
-// The rows [k0, k0 + kb) of x_F of a large supernode in the backward sweep, by 64-row blocks j from the last:
-// b_j = x_j - L(>j, j)^T x_>j (the later blocks of the step, one tile product), then x_j = L_jj^-T b_j as the product
-// with the transposed inverse. One block of TILE_THREADS per supernode; dynamic shared memory STEP_SOLVE_SMEM.
-__global__ void __launch_bounds__(TILE_THREADS) backwardDiagonal(SolveArgs a, const std::int32_t* list, int k0)
+// ------------------------------------------------------------------------------------------------------------------
+// The chains of the large supernodes. The triangular solves with a large supernode's L11 are chains of 64-row blocks:
+// forward, block i needs the blocks before it (x_i = L_ii^-1 (x_i - sum_{q<i} L_iq x_q)), backward the blocks after it.
+// One launch per level runs every large supernode's chain as dataflow tasks, one 64-row block each: a task streams
+// its row of L through a cp.async pipeline from the start (L is constant), takes the solved blocks x_q as their ready
+// flags are set, a chunk of ready blocks at a time, then applies the stored inverse of its diagonal block, stores its
+// rows and sets its own flag. The forward launch also carries the update rows' blocks (u_i -= sum_q L_iq x_q), which
+// wait on every block of x_F.
+//
+// Progress: a task takes a ticket (atomicAdd on the launch's counter) as it starts and runs the task at that place
+// of the launch's list, which puts every block a task waits on earlier in the list (blocks by block index, forward;
+// by distance from the last, backward; update rows last). So every task waited on has started before: it runs or has
+// finished, and waits only on earlier ones itself. Every wait is bounded as well (CHAIN_WAIT_NS, CHAIN_WAIT_POLLS); a
+// wait that runs out sets chainStop, which ends every other wait of the sweep at once, and chainFailed, which the host
+// reads after the solve (the sweep's results are then void).
+//
+// The solved rows of x are written by other blocks of the launch while it runs, so they are read through L2 only
+// (ld.global.cg), after the acquire of their flag; a block publishes its rows with a fence and a release store.
+// Each sum runs in a fixed order (the chain's block order, each block's products in column order, the narrow
+// products' two slice parities added at the end), so the result does not depend on the timing.
+// ------------------------------------------------------------------------------------------------------------------
+
+constexpr unsigned long long CHAIN_WAIT_NS = 2000000000ull; // a wait gives up after 2 s of global time
+constexpr unsigned CHAIN_WAIT_POLLS = 1u << 26;              // or after this many polls
+
+__device__ __forceinline__ int loadAcquire(const int* p)
 {
-    constexpr int LD = INVERSE_LD;
-    extern __shared__ double stage[];
-    double* pipe = stage;
-    double* inv = stage + TILE_SMEM_DOUBLES;  // 64 x INVERSE_LD
-    double* b = inv + SOLVE_BLOCK * LD;       // 64 x XF_LD
-    const FrontDesc f = a.fronts[list[blockIdx.x]];
-    const int w = a.width;
-    const std::int64_t n = f.c + f.r;
-    const int kb = min(SOLVE_STEP, f.c - k0);
-    double* xStep = a.x + static_cast<std::int64_t>(f.first + k0) * w;
-    for (int j0 = ((kb - 1) / SOLVE_BLOCK) * SOLVE_BLOCK; j0 >= 0; j0 -= SOLVE_BLOCK)
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void storeRelease(int* p, int v)
+{
+    asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long globalNanoseconds()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+
+// One task's product: acc += sum over the chain's blocks in its order o = 0 .. count - 1 (block q = first + step * o)
+// of A_q x_q, with A_q(ii, p) = a[ii * aRowStride + (64 q + p) * aColStride] for ii < m and p < kb(q) =
+// min(64, c - 64 q), and x_q the rows 64 q + p of x (w values each, by rows).
+struct ChainProduct
+{
+    const double* a;
+    std::int64_t aRowStride;
+    std::int64_t aColStride;
+    const double* x;
+    const int* flags;
+    int first;
+    int step;
+    int count;
+    int c;
+    int m;
+    int w;
+};
+
+// Warp 0 (all its lanes): waits (lane 0, bounded) until block o of the chain is solved, then counts the solved blocks
+// after it, up to `limit`, 32 flags at a time; returns one past the last. After a wait that ran out (here or in another
+// task) it returns `limit` without waiting further.
+__device__ int waitReady(const ChainProduct& op, const SolveArgs& a, int o, int limit)
+{
+    const int lane = threadIdx.x & 31;
+    int stopped = 0;
+    if (lane == 0)
     {
-        const int jb = min(SOLVE_BLOCK, kb - j0);
-        stageBlockInverse(a, f, k0 + j0, jb, inv);
-        commitAsyncCopies();
-        const int later = j0 + jb;
-        TileOperands op;
-        // A(ii, p) = L(k0 + later + p, k0 + j0 + ii)
-        op.a = a.panels + f.panel + (k0 + later) + static_cast<std::int64_t>(k0 + j0) * n;
-        op.aRowStride = n;
-        op.aColStride = 1;
-        op.b = xStep + static_cast<std::int64_t>(later) * w;
-        op.bRowStride = 1;
-        op.bColStride = w;
-        op.bIndex = nullptr;
-        op.d = nullptr;
-        op.dStride = 0;
-        op.c = nullptr;
-        op.cRowStride = 0;
-        op.cColStride = 0;
-        op.m = jb;
-        op.n = w;
-        op.k = kb - later;
-        op.lower = false;
-        op.lowerOffset = 0;
-        TileAccumulators acc;
-        tileAccumulate<true>(op, pipe, acc);
-        double* xBlock = xStep + static_cast<std::int64_t>(j0) * w;
+        const int* flag = op.flags + op.first + op.step * o;
+        if (loadAcquire(flag) == 0)
+        {
+            const unsigned long long start = globalNanoseconds();
+            for (unsigned polls = 0;; ++polls)
+            {
+                __nanosleep(32);
+                if (loadAcquire(flag) != 0)
+                    break;
+                if (*reinterpret_cast<volatile int*>(a.chainStop) != 0)
+                {
+                    stopped = 1;
+                    break;
+                }
+                if (polls >= CHAIN_WAIT_POLLS || globalNanoseconds() - start > CHAIN_WAIT_NS)
+                {
+                    atomicExch(a.chainStop, 1);
+                    *reinterpret_cast<volatile int*>(a.chainFailed) = 1;
+                    stopped = 1;
+                    break;
+                }
+            }
+        }
+    }
+    if (__shfl_sync(0xffffffffu, stopped, 0) != 0)
+        return limit;
+    int end = o + 1;
+    while (end < limit)
+    {
+        const int k = end + lane;
+        const bool set = k < limit && loadAcquire(op.flags + op.first + op.step * k) != 0;
+        const unsigned solved = __ballot_sync(0xffffffffu, set);
+        if (solved != 0xffffffffu)
+            return end + __ffs(~solved) - 1;
+        end += 32;
+    }
+    return limit;
+}
+
+// Does this thread hold element (tileRow(mi), tileColumn(ni, h)) of a chain task's result? A narrow product (at most
+// NARROW_COLUMNS right-hand sides) keeps it in the even warps' first two column fragments.
+__device__ __forceinline__ bool chainOwner(bool narrow, int ni)
+{
+    return narrow ? ((threadIdx.x >> 5) & 1) == 0 && ni < 2 : true;
+}
+
+// acc = -(the task's own rows): the sums then end at -(rows - products).
+__device__ __forceinline__ void chainStart(const double* rows, int m, int w, TileAccumulators& acc)
+{
+    const bool narrow = w <= NARROW_COLUMNS;
 #pragma unroll
-        for (int mi = 0; mi < 4; ++mi)
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+            {
+                const int ii = tileRow(mi);
+                const int jj = tileColumn(ni, h);
+                acc[mi][ni][h] = chainOwner(narrow, ni) && ii < m && jj < w ? -__ldcg(rows + ii * w + jj) : 0.0;
+            }
+}
+
+// The product of a task (ChainProduct), A_BY_ROWS: A's rows run along p (aColStride 1), in the CHAIN_REGION_DOUBLES
+// of shared memory at `region`; readyShared: a shared int. With an even number of right-hand sides, the slices of x
+// come through the same cp.async pipeline as those of A (16-byte copies, through L2 only), issued once their block is
+// known solved; with an odd number (no 16-byte alignment), the solved blocks are read a chunk at a time into a buffer
+// of their own. Every asynchronous copy of the block has completed on return, and the threads are synchronised.
+template <bool A_BY_ROWS>
+__device__ void chainAccumulate(const ChainProduct& op, const SolveArgs& args, double* region, int* readyShared,
+                                TileAccumulators& acc)
+{
+    constexpr int LD = CHAIN_LD;
+    constexpr int SLICES_PER_BLOCK = SOLVE_BLOCK / CHAIN_SLICE;
+    constexpr int A_DOUBLES = CHAIN_SLICE * LD;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int wm = (warp >> 1) * 32;
+    const int wn = (warp & 1) * 32;
+    const bool narrow = op.w <= NARROW_COLUMNS;
+    const bool helper = narrow && (warp & 1) != 0;
+    const bool pipelined = (op.w & 1) == 0 && (reinterpret_cast<std::uintptr_t>(op.x) & 15) == 0;
+    const int columns = narrow ? NARROW_COLUMNS : TILE; // the columns of x the products read
+    const int ldb = narrow ? NARROW_COLUMNS + TILE_PAD : LD;
+    const int stageDoubles = pipelined ? A_DOUBLES + CHAIN_SLICE * ldb : A_DOUBLES;
+    double* ready = region + CHAIN_STAGES * A_DOUBLES; // the unpipelined path's solved blocks
+    const int chunkBlocks = CHAIN_B_DOUBLES / (SOLVE_BLOCK * ldb);
+    const int slices = op.count * SLICES_PER_BLOCK;
+    int readyEnd = 0; // the blocks [0, readyEnd) of the order are known solved
+
+    // (pipelined) the columns [w, columns) of every stage's x slice stay zero: the copies write columns < w only
+    if (pipelined)
+        for (int e = tid; e < CHAIN_STAGES * CHAIN_SLICE * columns; e += TILE_THREADS)
+        {
+            const int row = e / columns;
+            const int jj = e - row * columns;
+            if (jj >= op.w)
+                region[(row / CHAIN_SLICE) * stageDoubles + A_DOUBLES + (row % CHAIN_SLICE) * ldb + jj] = 0.0;
+        }
+    // block o of the order known solved (thread 0 waits; a barrier for all)
+    const auto ensureReady = [&](int o)
+    {
+        if (o < readyEnd)
+            return;
+        if (warp == 0)
+        {
+            const int solved = waitReady(op, args, o, op.count);
+            if (lane == 0)
+                *readyShared = solved;
+        }
+        __syncthreads();
+        readyEnd = *readyShared;
+        __syncthreads();
+    };
+    const auto issue = [&](int t)
+    {
+        double* sA = region + (t % CHAIN_STAGES) * stageDoubles;
+        const int o = t / SLICES_PER_BLOCK;
+        const int q = op.first + op.step * o;
+        const int kb = min(SOLVE_BLOCK, op.c - q * SOLVE_BLOCK);
+        const int p0 = (t % SLICES_PER_BLOCK) * CHAIN_SLICE;
+        const double* base = op.a + static_cast<std::int64_t>(q) * SOLVE_BLOCK * op.aColStride;
+#pragma unroll
+        for (int r = 0; r < TILE * CHAIN_SLICE / TILE_THREADS; ++r)
+        {
+            const int e = tid + r * TILE_THREADS;
+            const int ii = A_BY_ROWS ? e / CHAIN_SLICE : (e & (TILE - 1));
+            const int pp = A_BY_ROWS ? (e & (CHAIN_SLICE - 1)) : e / TILE;
+            const int p = p0 + pp;
+            const bool ok = ii < op.m && p < kb;
+            copyAsync8(sA + pp * LD + ii,
+                       ok ? base + ii * op.aRowStride + static_cast<std::int64_t>(p) * op.aColStride : op.a, ok);
+        }
+        if (pipelined)
+        {
+            // x rows 64 q + p0 + pp, w values each (pairs of 16 bytes), zero beyond the block's columns
+            double* sB = sA + A_DOUBLES;
+            const int pairs = op.w >> 1;
+            for (int e = tid; e < CHAIN_SLICE * pairs; e += TILE_THREADS)
+            {
+                const int pp = e / pairs;
+                const int jj = (e - pp * pairs) * 2;
+                const int p = p0 + pp;
+                const bool ok = p < kb;
+                copyAsync16(sB + pp * ldb + jj,
+                            ok ? op.x + static_cast<std::int64_t>(q * SOLVE_BLOCK + p) * op.w + jj : op.x, ok);
+            }
+        }
+        commitAsyncCopies();
+    };
+
+#pragma unroll
+    for (int t = 0; t < CHAIN_STAGES - 1; ++t)
+    {
+        if (t < slices)
+        {
+            if (pipelined)
+                ensureReady(t / SLICES_PER_BLOCK);
+            issue(t);
+        }
+        else
+            commitAsyncCopies();
+    }
+    int oBase = 0; // (unpipelined) the blocks [oBase, oLoaded) of the order are in `ready`
+    int oLoaded = 0;
+    for (int t = 0; t < slices; ++t)
+    {
+        waitAsyncCopies<CHAIN_STAGES - 2>();
+        __syncthreads();
+        const int next = t + CHAIN_STAGES - 1;
+        if (next < slices)
+        {
+            if (pipelined)
+                ensureReady(next / SLICES_PER_BLOCK);
+            issue(next);
+        }
+        else
+            commitAsyncCopies();
+        const int o = t / SLICES_PER_BLOCK;
+        const double* sA = region + (t % CHAIN_STAGES) * stageDoubles;
+        const double* sB;
+        if (pipelined)
+            sB = sA + A_DOUBLES;
+        else
+        {
+            if (o >= oLoaded)
+            {
+                // the next solved blocks into `ready` (every thread is done with the last ones: the barrier above)
+                if (warp == 0)
+                {
+                    const int solved = waitReady(op, args, o, min(op.count, o + chunkBlocks));
+                    if (lane == 0)
+                        *readyShared = solved;
+                }
+                __syncthreads();
+                oBase = o;
+                oLoaded = *readyShared;
+                const int rows = (oLoaded - oBase) * SOLVE_BLOCK;
+                for (int e = tid; e < rows * columns; e += TILE_THREADS)
+                {
+                    const int row = e / columns;
+                    const int jj = e - row * columns;
+                    const int q = op.first + op.step * (oBase + row / SOLVE_BLOCK);
+                    const int p = row % SOLVE_BLOCK;
+                    const bool inside = p < op.c - q * SOLVE_BLOCK && jj < op.w;
+                    ready[row * ldb + jj] =
+                        inside ? __ldcg(op.x + static_cast<std::int64_t>(q * SOLVE_BLOCK + p) * op.w + jj) : 0.0;
+                }
+                __syncthreads();
+            }
+            sB = ready + ((o - oBase) * SOLVE_BLOCK + (t % SLICES_PER_BLOCK) * CHAIN_SLICE) * ldb;
+        }
+        if (narrow)
+        {
+            if ((warp & 1) != (t & 1))
+                continue; // the partner's slice
+#pragma unroll
+            for (int kk = 0; kk < CHAIN_SLICE; kk += 4)
+            {
+                const int pr = kk + (lane & 3);
+                double fa[4];
+                double fb[2];
+#pragma unroll
+                for (int mi = 0; mi < 4; ++mi)
+                    fa[mi] = sA[pr * LD + wm + mi * 8 + (lane >> 2)];
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni)
+                    fb[ni] = sB[pr * ldb + ni * 8 + (lane >> 2)];
+#pragma unroll
+                for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 2; ++ni)
+                        dmma8x8x4(acc[mi][ni], fa[mi], fb[ni]);
+            }
+            continue;
+        }
+#pragma unroll
+        for (int kk = 0; kk < CHAIN_SLICE; kk += 4)
+        {
+            const int pr = kk + (lane & 3);
+            double fa[4];
+            double fb[4];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+                fa[mi] = sA[pr * LD + wm + mi * 8 + (lane >> 2)];
 #pragma unroll
             for (int ni = 0; ni < 4; ++ni)
+                fb[ni] = sB[pr * ldb + wn + ni * 8 + (lane >> 2)];
 #pragma unroll
-                for (int h = 0; h < 2; ++h)
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+                    dmma8x8x4(acc[mi][ni], fa[mi], fb[ni]);
+        }
+    }
+    waitAsyncCopies<0>();
+    __syncthreads();
+    if (narrow)
+    {
+        // the odd warps' sums into their even partners' (through the first stage's shared memory)
+        double* hand = region + (warp >> 1) * (32 * 16) + lane * 16;
+        if (helper)
+        {
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni)
                 {
-                    const int ii = tileRow(mi);
-                    const int jj = tileColumn(ni, h);
-                    b[ii * XF_LD + jj] = ii < jb && jj < w ? xBlock[ii * w + jj] - acc[mi][ni][h] : 0.0;
+                    hand[(mi * 2 + ni) * 2] = acc[mi][ni][0];
+                    hand[(mi * 2 + ni) * 2 + 1] = acc[mi][ni][1];
                 }
+        }
         __syncthreads();
-        stepTriangle<true>(inv, b, jb, w, xBlock, acc);
+        if (!helper)
+        {
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni)
+                {
+                    acc[mi][ni][0] += hand[(mi * 2 + ni) * 2];
+                    acc[mi][ni][1] += hand[(mi * 2 + ni) * 2 + 1];
+                }
+        }
         __syncthreads();
     }
 }
 
-// After step t's block is solved, its terms leave the rows above it: x_F[q] -= sum_{i in block} L(i, q) x_F[i] for
-// q in a tile of [0, k0).
-__global__ void __launch_bounds__(TILE_THREADS) backwardUpdate(SolveArgs a, const TileTask* tasks, int k0)
+// The end of a task of x_F: b = -acc (the task's rows less the products) in shared memory (64 x XF_LD at `b`), then
+// x = b + (strict lower of L_ii^-1) b (TRANSPOSED: of L_ii^-T) with the staged inverse, into the task's rows; then its
+// flag. A narrow product (at most NARROW_COLUMNS right-hand sides) splits the inverse's K between the warps of a pair
+// (the odd warps' half added through `scratch`, at least 1024 doubles).
+template <bool TRANSPOSED>
+__device__ __forceinline__ void chainFinish(const double* inv, double* b, double* scratch, int m, int w, double* rows,
+                                            int* flag, TileAccumulators& acc)
 {
-    __shared__ double smem[TILE_SMEM_DOUBLES];
-    const TileTask task = tasks[blockIdx.x];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const bool narrow = w <= NARROW_COLUMNS;
+    for (int e = threadIdx.x; e < SOLVE_BLOCK * XF_LD; e += blockDim.x)
+        b[e] = 0.0;
+    __syncthreads();
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+            {
+                const int ii = tileRow(mi);
+                const int jj = tileColumn(ni, h);
+                if (chainOwner(narrow, ni) && ii < m && jj < w)
+                    b[ii * XF_LD + jj] = -acc[mi][ni][h];
+            }
+    __syncthreads();
+    if (!narrow)
+        stepTriangle<TRANSPOSED>(inv, b, m, w, rows, acc);
+    else
+    {
+        const int wm = (warp >> 1) * 32;
+        const int k0 = (warp & 1) * (SOLVE_BLOCK / 2);
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni)
+            {
+                acc[mi][ni][0] = 0.0;
+                acc[mi][ni][1] = 0.0;
+            }
+#pragma unroll
+        for (int kk = 0; kk < SOLVE_BLOCK / 2; kk += 4)
+        {
+            const int pr = k0 + kk + (lane & 3);
+            double fa[4];
+            double fb[2];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+            {
+                const int ii = wm + mi * 8 + (lane >> 2);
+                fa[mi] = TRANSPOSED ? inv[pr * INVERSE_LD + ii] : inv[ii * INVERSE_LD + pr];
+            }
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni)
+                fb[ni] = b[pr * XF_LD + ni * 8 + (lane >> 2)];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni)
+                    dmma8x8x4(acc[mi][ni], fa[mi], fb[ni]);
+        }
+        double* hand = scratch + (warp >> 1) * (32 * 16) + lane * 16;
+        if (warp & 1)
+        {
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni)
+                {
+                    hand[(mi * 2 + ni) * 2] = acc[mi][ni][0];
+                    hand[(mi * 2 + ni) * 2 + 1] = acc[mi][ni][1];
+                }
+        }
+        __syncthreads();
+        if ((warp & 1) == 0)
+        {
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                    {
+                        const int ii = tileRow(mi);
+                        const int jj = tileColumn(ni, h);
+                        if (ii < m && jj < w)
+                            rows[ii * w + jj] =
+                                b[ii * XF_LD + jj] + (acc[mi][ni][h] + hand[(mi * 2 + ni) * 2 + h]);
+                    }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        __threadfence();
+        storeRelease(flag, 1);
+    }
+}
+
+// The forward chains of one level (tasks: front, first row i0, own block (-1: update rows), first flag).
+__global__ void __launch_bounds__(TILE_THREADS) forwardChain(SolveArgs a, const TileTask* tasks, int slot)
+{
+    extern __shared__ double chainShared[];
+    __shared__ int ticket[2];
+    double* region = chainShared;
+    double* inv = region + CHAIN_REGION_DOUBLES;
+    if (threadIdx.x == 0)
+        ticket[0] = atomicAdd(a.chainTickets + slot, 1);
+    __syncthreads();
+    const TileTask task = tasks[ticket[0]];
     const FrontDesc f = a.fronts[task.front];
     const std::int64_t n = f.c + f.r;
     const int w = a.width;
-    TileOperands op;
-    // A(ii, p) = L(k0 + p, i0 + ii) = panel[k0 + p + (i0 + ii) n]
-    op.a = a.panels + f.panel + k0 + static_cast<std::int64_t>(task.i0) * n;
+    const bool pivotRows = task.j0 >= 0;
+    const int m = pivotRows ? min(TILE, f.c - task.i0) : static_cast<int>(n - task.i0 < TILE ? n - task.i0 : TILE);
+    double* rows = pivotRows ? a.x + static_cast<std::int64_t>(f.first + task.i0) * w
+                             : a.updates + (f.rowStart + (task.i0 - f.c)) * w;
+    if (pivotRows)
+    {
+        stageBlockInverse(a, f, task.i0, m, inv);
+        commitAsyncCopies();
+    }
+    TileAccumulators acc;
+    chainStart(rows, m, w, acc);
+    ChainProduct op;
+    op.a = a.panels + f.panel + task.i0; // A(ii, p) = L(i0 + ii, 64 q + p)
+    op.aRowStride = 1;
+    op.aColStride = n;
+    op.x = a.x + static_cast<std::int64_t>(f.first) * w;
+    op.flags = a.chainFlags + task.k0;
+    op.first = 0;
+    op.step = 1;
+    op.count = pivotRows ? task.j0 : (f.c + SOLVE_BLOCK - 1) / SOLVE_BLOCK;
+    op.c = f.c;
+    op.m = m;
+    op.w = w;
+    chainAccumulate<false>(op, a, region, ticket + 1, acc);
+    if (pivotRows)
+    {
+        chainFinish<false>(inv, region + CHAIN_REGION_DOUBLES - SOLVE_BLOCK * XF_LD, region, m, w, rows,
+                           a.chainFlags + task.k0 + task.j0, acc);
+        return;
+    }
+    const bool narrow = w <= NARROW_COLUMNS;
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+            {
+                const int ii = tileRow(mi);
+                const int jj = tileColumn(ni, h);
+                if (chainOwner(narrow, ni) && ii < m && jj < w)
+                    rows[ii * w + jj] = -acc[mi][ni][h];
+            }
+}
+
+// The backward chains of one level (tasks: front, first row i0, own block, first flag), after the products with the
+// rows R(s) (backwardRows): x_i = L_ii^-T (x_i - sum_{q>i} L_qi^T x_q), the blocks q from the last.
+__global__ void __launch_bounds__(TILE_THREADS) backwardChain(SolveArgs a, const TileTask* tasks, int slot)
+{
+    extern __shared__ double chainShared[];
+    __shared__ int ticket[2];
+    double* region = chainShared;
+    double* inv = region + CHAIN_REGION_DOUBLES;
+    if (threadIdx.x == 0)
+        ticket[0] = atomicAdd(a.chainTickets + slot, 1);
+    __syncthreads();
+    const TileTask task = tasks[ticket[0]];
+    const FrontDesc f = a.fronts[task.front];
+    const std::int64_t n = f.c + f.r;
+    const int w = a.width;
+    const int blocks = (f.c + SOLVE_BLOCK - 1) / SOLVE_BLOCK;
+    const int m = min(TILE, f.c - task.i0);
+    double* rows = a.x + static_cast<std::int64_t>(f.first + task.i0) * w;
+    stageBlockInverse(a, f, task.i0, m, inv);
+    commitAsyncCopies();
+    TileAccumulators acc;
+    chainStart(rows, m, w, acc);
+    ChainProduct op;
+    op.a = a.panels + f.panel + static_cast<std::int64_t>(task.i0) * n; // A(ii, p) = L(64 q + p, i0 + ii)
     op.aRowStride = n;
     op.aColStride = 1;
-    op.b = a.x + static_cast<std::int64_t>(f.first + k0) * w;
-    op.bRowStride = 1;
-    op.bColStride = w;
-    op.bIndex = nullptr;
-    op.d = nullptr;
-    op.dStride = 0;
-    op.c = a.x + static_cast<std::int64_t>(f.first + task.i0) * w;
-    op.cRowStride = w;
-    op.cColStride = 1;
-    op.m = min(TILE, k0 - task.i0);
-    op.n = w;
-    op.k = min(SOLVE_STEP, f.c - k0);
-    op.lower = false;
-    op.lowerOffset = 0;
-    tileProduct<true>(op, smem);
+    op.x = a.x + static_cast<std::int64_t>(f.first) * w;
+    op.flags = a.chainFlags + task.k0;
+    op.first = blocks - 1;
+    op.step = -1;
+    op.count = blocks - 1 - task.j0;
+    op.c = f.c;
+    op.m = m;
+    op.w = w;
+    chainAccumulate<true>(op, a, region, ticket + 1, acc);
+    chainFinish<true>(inv, region + CHAIN_REGION_DOUBLES - SOLVE_BLOCK * XF_LD, region, m, w, rows,
+                      a.chainFlags + task.k0 + task.j0, acc);
 }
 
 // Column-major B (ld) <-> rows of X (width columns from column c0), by 32 x 32 tiles transposed in shared memory so

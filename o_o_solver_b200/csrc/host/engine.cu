@@ -217,6 +217,11 @@ public:
         if (m_plan.rowPartialSlots > 0)
             m_rowPartials.allocate(static_cast<std::size_t>(m_plan.rowPartialSlots) * device::TILE * device::TILE,
                                    "solve: split products");
+        allocateChains(m_plan);
+        void* failed = nullptr;
+        check(cudaHostAlloc(&failed, sizeof(int), cudaHostAllocMapped), "solve: chain status");
+        m_chainFailed = static_cast<int*>(failed);
+        *m_chainFailed = 0;
         m_supernodeOfColumn.upload(m_plan.supernodeOfColumn, m_stream, "plan: columns");
         m_lists.upload(m_plan.lists, m_stream, "plan: lists");
         m_tiles.upload(m_plan.tiles, m_stream, "plan: tiles");
@@ -258,12 +263,12 @@ public:
         check(cudaFuncSetAttribute(device::panelRowsPivotedInverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(device::PANEL_ROWS_PIVOTED_SMEM)),
               "pivoted panel rows shared memory");
-        // The diagonal steps of the solves: the tile pipeline, a block's inverse and the rows of a 64-column tile.
-        for (const void* kernel : {reinterpret_cast<const void*>(device::forwardDiagonal),
-                                   reinterpret_cast<const void*>(device::backwardDiagonal)})
+        // The chains of the solves: the A pipeline, the ready rows of x and a block's inverse.
+        for (const void* kernel : {reinterpret_cast<const void*>(device::forwardChain),
+                                   reinterpret_cast<const void*>(device::backwardChain)})
             check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(device::STEP_SOLVE_SMEM)),
-                  "diagonal solve shared memory");
+                                       static_cast<int>(device::CHAIN_SMEM)),
+                  "chain solve shared memory");
         for (const void* kernel : {reinterpret_cast<const void*>(device::forwardSmall),
                                    reinterpret_cast<const void*>(device::backwardSmall)})
             check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -298,9 +303,30 @@ public:
             cudaStreamDestroy(m_side);
         if (m_copyStream != nullptr)
             cudaStreamDestroy(m_copyStream);
+        if (m_chainFailed != nullptr)
+            cudaFreeHost(m_chainFailed);
     }
 
     [[nodiscard]] cudaStream_t stream() const noexcept { return m_stream; }
+
+    // The chain state for a plan's sweeps (ticket counters, ready flags, the stop word), grown when a plan needs more;
+    // a new array starts cleared.
+    void allocateChains(const Plan& plan)
+    {
+        const std::size_t needed = static_cast<std::size_t>(plan.chainSlots) + static_cast<std::size_t>(plan.chainFlags) + 1;
+        if (m_chainState.get() != nullptr && needed <= m_chainState.size())
+            return;
+        m_chainState.allocate(needed, "solve: chain state");
+        check(cudaMemsetAsync(m_chainState.get(), 0, m_chainState.size() * sizeof(int), m_stream), "chain state");
+    }
+
+    // A sweep whose chain wait ran out (the mapped status the kernels set) voids the factor's solves from then on.
+    void checkChains() const
+    {
+        if (m_chainFailed != nullptr && *reinterpret_cast<volatile int*>(m_chainFailed) != 0)
+            throw Error(STATUS_INTERNAL, "FactorSolve: a solve's chain step waited past its limit (the results are "
+                                         "void; the factor's solves are disabled)");
+    }
 
     // Right-hand sides copied ahead of a solve (oosgpu_solve_prefetch): host B (n x columns, ld) into the device
     // buffer the next host-array solve of the same B uses, on a copy stream of its own, so that the copy overlaps
@@ -715,7 +741,11 @@ public:
             const device::SolveArgs args{view.fronts,       m_children.get(), view.rows,       view.relpos,
                                          m_panels.get(),    x,                m_updateRows.get(), width,
                                          view.gatherStart,  view.gatherRows,  nullptr,          n,
-                                         m_rowPartials.get()};
+                                         m_rowPartials.get(),
+                                         m_chainState.get(),
+                                         m_chainState.get() + view.plan->chainSlots,
+                                         m_chainState.get() + (m_chainState.size() - 1),
+                                         m_chainFailed};
             runSweep(args, view, m_partialForward);
             if (recover)
             {
@@ -739,6 +769,7 @@ public:
                                     static_cast<std::size_t>(columns), cudaMemcpyDeviceToHost, m_stream),
                   "download condensed loads");
         check(cudaStreamSynchronize(m_stream), "partial solve");
+        checkChains();
     }
 
     // The indefinite factorisation (the reference's PivotingMode::Indefinite), after the common set-up of factorise():
@@ -1078,6 +1109,7 @@ public:
         if (r.plan.rowPartialSlots > m_plan.rowPartialSlots)
             m_rowPartials.allocate(static_cast<std::size_t>(r.plan.rowPartialSlots) * device::TILE * device::TILE,
                                    "solve: split products");
+        allocateChains(r.plan);
         device::FactorArgs restatedArgs = args;
         restatedArgs.fronts = r.fronts.get();
         for (const std::vector<Launch>* launches : {&r.plan.inverseLaunches, &r.plan.inverseLaunchesLarge})
@@ -1102,6 +1134,7 @@ public:
         if (m_singular)
             throw Error(STATUS_SINGULAR, "FactorSolve: the factor has a zero pivot (the shifted matrix is singular); "
                                          "move the shift");
+        checkChains();
     }
 
     void solve(double* b, std::int64_t ld, std::int64_t columns, bool onDevice)
@@ -1142,6 +1175,7 @@ public:
                                     static_cast<std::size_t>(columns), cudaMemcpyDeviceToHost, m_stream),
                   "download solutions");
         check(cudaStreamSynchronize(m_stream), "solve");
+        checkChains();
         float milliseconds = 0.0f;
         check(cudaEventElapsedTime(&milliseconds, m_start, m_stop), "event time");
         m_lastSolveSeconds = milliseconds / 1000.0;
@@ -1240,7 +1274,11 @@ public:
                                // the plan's gather slots are equations, the restated structure's are positions
                                m_pivoted && !m_isRestated ? view.perm : nullptr,
                                n,
-                               m_rowPartials.get()};
+                               m_rowPartials.get(),
+                               m_chainState.get(),
+                               m_chainState.get() + view.plan->chainSlots,
+                               m_chainState.get() + (m_chainState.size() - 1),
+                               m_chainFailed};
         const auto launches = [&]
         {
             runSweep(args, view, view.plan->forwardLaunches);
@@ -1305,6 +1343,7 @@ public:
         }
         check(cudaEventRecord(m_stop, m_stream), "event");
         check(cudaStreamSynchronize(m_stream), "solve");
+        checkChains();
         float milliseconds = 0.0f;
         check(cudaEventElapsedTime(&milliseconds, m_start, m_stop), "event time");
         m_lastSolveSeconds = milliseconds / 1000.0;
@@ -2100,6 +2139,14 @@ private:
 
     void runSweep(const device::SolveArgs& args, const SolveView& view, const std::vector<Launch>& launches)
     {
+        // the chain launches' tickets and flags start cleared in every sweep
+        if (std::any_of(launches.begin(), launches.end(), [](const Launch& l)
+                        { return l.kind == LaunchKind::ForwardChain || l.kind == LaunchKind::BackwardChain; }))
+            check(cudaMemsetAsync(m_chainState.get(), 0,
+                                  (static_cast<std::size_t>(view.plan->chainSlots) +
+                                   static_cast<std::size_t>(view.plan->chainFlags)) * sizeof(int),
+                                  m_stream),
+                  "chain state");
         for (const Launch& launch : launches)
         {
             const std::int32_t* list = view.lists + launch.offset;
@@ -2115,12 +2162,9 @@ private:
             case LaunchKind::ForwardGather:
                 device::forwardGather<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles);
                 break;
-            case LaunchKind::ForwardDiagonal:
-                device::forwardDiagonal<<<launch.count, device::TILE_THREADS, device::STEP_SOLVE_SMEM,
-                                           m_stream>>>(args, list, launch.k0);
-                break;
-            case LaunchKind::ForwardUpdate:
-                device::forwardUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles, launch.k0);
+            case LaunchKind::ForwardChain:
+                device::forwardChain<<<launch.count, device::TILE_THREADS, device::CHAIN_SMEM, m_stream>>>(
+                    args, tiles, launch.k0);
                 break;
             case LaunchKind::BackwardSmall:
                 device::backwardSmall<<<launch.count, device::TILE_THREADS, smallSmem, m_stream>>>(
@@ -2132,12 +2176,9 @@ private:
             case LaunchKind::BackwardRowsReduce:
                 device::backwardRowsReduce<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles);
                 break;
-            case LaunchKind::BackwardDiagonal:
-                device::backwardDiagonal<<<launch.count, device::TILE_THREADS, device::STEP_SOLVE_SMEM,
-                                            m_stream>>>(args, list, launch.k0);
-                break;
-            case LaunchKind::BackwardUpdate:
-                device::backwardUpdate<<<launch.count, device::TILE_THREADS, 0, m_stream>>>(args, tiles, launch.k0);
+            case LaunchKind::BackwardChain:
+                device::backwardChain<<<launch.count, device::TILE_THREADS, device::CHAIN_SMEM, m_stream>>>(
+                    args, tiles, launch.k0);
                 break;
             default:
                 throw Error(STATUS_INTERNAL, "solve plan: a factorisation launch in a sweep");
@@ -2199,6 +2240,10 @@ private:
     LaunchGraph m_sweepGraph;
     DeviceArray<std::int32_t> m_gatherRows;
     DeviceArray<double> m_rowPartials;
+    // The chain launches' state: ticket counters and ready flags of the plan's (or the restated plan's) sweeps, then
+    // the stop word (last); and the host-mapped word a wait that ran out sets.
+    DeviceArray<int> m_chainState;
+    int* m_chainFailed = nullptr;
     DeviceArray<std::int32_t> m_supernodeOfColumn;
     DeviceArray<std::int32_t> m_lists;
     DeviceArray<device::TileTask> m_tiles;
@@ -2312,7 +2357,7 @@ private:
         std::int32_t k0;
     };
     // The kind code of the diagonal sweep in a solve's launch profile (after the plan's launch kinds).
-    static constexpr std::int32_t DIAGONAL_SWEEP_KIND = 23;
+    static constexpr std::int32_t DIAGONAL_SWEEP_KIND = static_cast<std::int32_t>(LaunchKind::DiagonalSweep);
     std::vector<SolveRecord> m_solveRecords;
     std::vector<cudaEvent_t> m_solveEvents;
     bool m_annotated = false;
@@ -2678,6 +2723,31 @@ extern "C" int oosgpu_symbolic_sizes(const oosgpu_symbolic* symbolic, int64_t si
             sizes[7] = 0;
             if (flops != nullptr)
                 *flops = s.flopCount();
+        });
+}
+
+extern "C" int oosgpu_symbolic_solve_chains(const oosgpu_symbolic* symbolic, int64_t counts[4])
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(symbolic, "symbolic");
+            requirePointer(counts, "counts");
+            const oosgpu::Plan plan = oosgpu::buildPlan(symbolic->symbolic);
+            std::int64_t tasks = 0;
+            std::int64_t longest = 0;
+            for (const auto* launches : {&plan.forwardLaunches, &plan.backwardLaunches})
+                for (const oosgpu::Launch& launch : *launches)
+                    if (launch.kind == oosgpu::LaunchKind::ForwardChain ||
+                        launch.kind == oosgpu::LaunchKind::BackwardChain)
+                    {
+                        tasks += launch.count;
+                        longest = std::max<std::int64_t>(longest, launch.count);
+                    }
+            counts[0] = plan.chainSlots;
+            counts[1] = tasks;
+            counts[2] = plan.chainFlags;
+            counts[3] = longest;
         });
 }
 
@@ -3290,6 +3360,23 @@ extern "C" int oosgpu_modes_summary(const oosgpu_modes* modes, int64_t counts[6]
                 seconds[4] = s.orthogonalisationSeconds;
                 seconds[5] = s.projectedSeconds;
             }
+        });
+}
+
+extern "C" int oosgpu_modes_work(const oosgpu_modes* modes, int64_t counts[2], double seconds[4])
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(modes, "modes");
+            const auto& s = modes->solution;
+            if (counts != nullptr)
+            {
+                counts[0] = static_cast<int64_t>(s.hostBlocks);
+                counts[1] = static_cast<int64_t>(s.replacementSolves);
+            }
+            if (seconds != nullptr)
+                std::copy(s.orthogonalisationParts.begin(), s.orthogonalisationParts.end(), seconds);
         });
 }
 

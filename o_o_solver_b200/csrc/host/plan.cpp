@@ -110,6 +110,33 @@ void buildGatherLists(Plan& plan)
     }
 }
 
+// The chains' progress rests on the order of a chain launch's tasks: every block a task waits on is listed before it
+// (forward: a supernode's blocks in increasing order, its update rows after all of them; backward: its blocks from the
+// last). Checked on every plan.
+void checkChainOrder(const Plan& plan, const std::vector<TileTask>& chain, const std::vector<std::int32_t>& large,
+                     const std::vector<std::int32_t>& blocks, bool forward)
+{
+    std::vector<std::int32_t> listed(large.size(), 0);
+    for (const TileTask& task : chain)
+    {
+        const auto at = std::find(large.begin(), large.end(), task.front);
+        if (at == large.end())
+            throw Error(STATUS_INTERNAL, "plan: a chain task of a supernode outside its level");
+        const auto k = static_cast<std::size_t>(at - large.begin());
+        const FrontDesc& f = plan.fronts[static_cast<std::size_t>(task.front)];
+        bool inOrder;
+        if (task.j0 < 0)
+            inOrder = forward && listed[k] == blocks[k] && task.i0 >= f.c && task.i0 < f.c + f.r;
+        else
+        {
+            inOrder = task.j0 == (forward ? listed[k] : blocks[k] - 1 - listed[k]) && task.i0 == task.j0 * BLOCK;
+            ++listed[k];
+        }
+        if (!inOrder)
+            throw Error(STATUS_INTERNAL, "plan: a chain task listed before a block it waits on");
+    }
+}
+
 // The solve launches of one level's supernodes (the forward sweep's into plan.forwardLaunches, the backward sweep's
 // into `backward`, emitted later top level first) and the 64-column diagonal blocks whose inverses the solves apply.
 void addSolveLevel(Plan& plan, const std::vector<std::int32_t>& members, std::int32_t level,
@@ -121,18 +148,8 @@ void addSolveLevel(Plan& plan, const std::vector<std::int32_t>& members, std::in
     // ---- forward sweep ----
     std::vector<std::int32_t> solveSmall;
     std::vector<std::int32_t> solveLarge;
-    std::int32_t maxColumns = 0;
     for (const std::int32_t s : members)
-    {
-        const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
-        if (f.c <= SOLVE_SMALL_COLUMNS)
-            solveSmall.push_back(s);
-        else
-        {
-            solveLarge.push_back(s);
-            maxColumns = std::max(maxColumns, f.c);
-        }
-    }
+        (plan.fronts[static_cast<std::size_t>(s)].c <= SOLVE_SMALL_COLUMNS ? solveSmall : solveLarge).push_back(s);
     // The small supernodes by width class (at most 16, 32 or SOLVE_SMALL_COLUMNS columns): each launch's shared
     // memory is sized for its widest supernode, so the narrow ones (most of the lowest levels) fit more blocks
     // per SM. The supernodes of one level are independent, so the split changes no result.
@@ -167,26 +184,39 @@ void addSolveLevel(Plan& plan, const std::vector<std::int32_t>& members, std::in
         for (std::int32_t k0 = 0; k0 < f.c; k0 += BLOCK)
             (isLarge ? inverseTasksLarge : inverseTasks).push_back({s, k0, 0, 0});
     }
-    // Steps of SOLVE_STEP columns: the step's diagonal blocks in one launch, then its products with the rows below.
-    constexpr std::int32_t STEP = device::SOLVE_STEP;
-    for (std::int32_t k0 = 0; k0 < maxColumns; k0 += STEP)
+    // The large supernodes' forward chains, one launch: a task per 64-row block, the blocks of x_F in block order
+    // (across the supernodes) before the blocks of the update rows, so that a task waits only on blocks listed before
+    // it (TileTask: front, first row, own block or -1, the supernode's first flag).
+    std::vector<std::int32_t> chainBlocks(solveLarge.size());
+    std::vector<std::int64_t> forwardBase(solveLarge.size());
+    std::vector<std::int64_t> backwardBase(solveLarge.size());
+    std::int32_t maxBlocks = 0;
+    for (std::size_t k = 0; k < solveLarge.size(); ++k)
     {
-        std::vector<std::int32_t> diagonal;
-        std::vector<TileTask> below;
-        for (const std::int32_t s : solveLarge)
+        const FrontDesc& f = plan.fronts[static_cast<std::size_t>(solveLarge[k])];
+        chainBlocks[k] = (f.c + BLOCK - 1) / BLOCK;
+        maxBlocks = std::max(maxBlocks, chainBlocks[k]);
+        forwardBase[k] = plan.chainFlags;
+        backwardBase[k] = plan.chainFlags + chainBlocks[k];
+        plan.chainFlags += 2 * static_cast<std::int64_t>(chainBlocks[k]);
+    }
+    if (plan.chainFlags > INT32_MAX)
+        throw Error(STATUS_INVALID_ARGUMENT, "plan: too many 64-column blocks in the large supernodes");
+    if (!solveLarge.empty())
+    {
+        std::vector<TileTask> chain;
+        for (std::int32_t b = 0; b < maxBlocks; ++b)
+            for (std::size_t k = 0; k < solveLarge.size(); ++k)
+                if (b < chainBlocks[k])
+                    chain.push_back({solveLarge[k], b * BLOCK, b, static_cast<std::int32_t>(forwardBase[k])});
+        for (std::size_t k = 0; k < solveLarge.size(); ++k)
         {
-            const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
-            if (f.c <= k0)
-                continue;
-            diagonal.push_back(s);
-            const std::int32_t kb = std::min(STEP, f.c - k0);
-            for (std::int32_t i0 = k0 + kb; i0 < f.c; i0 += device::TILE)
-                below.push_back({s, i0, 0, 0});
+            const FrontDesc& f = plan.fronts[static_cast<std::size_t>(solveLarge[k])];
             for (std::int32_t i0 = f.c; i0 < f.c + f.r; i0 += device::TILE)
-                below.push_back({s, i0, 0, 1});
+                chain.push_back({solveLarge[k], i0, -1, static_cast<std::int32_t>(forwardBase[k])});
         }
-        addList(plan, plan.forwardLaunches, LaunchKind::ForwardDiagonal, diagonal, k0);
-        addTiles(plan, plan.forwardLaunches, LaunchKind::ForwardUpdate, below, k0);
+        checkChainOrder(plan, chain, solveLarge, chainBlocks, true);
+        addTiles(plan, plan.forwardLaunches, LaunchKind::ForwardChain, chain, plan.chainSlots++);
     }
 
     // ---- backward sweep (collected per level, emitted top level first) ----
@@ -220,23 +250,19 @@ void addSolveLevel(Plan& plan, const std::vector<std::int32_t>& members, std::in
     plan.rowPartialSlots = std::max(plan.rowPartialSlots, slots);
     addTiles(plan, backward, LaunchKind::BackwardRows, rowTiles);
     addTiles(plan, backward, LaunchKind::BackwardRowsReduce, rowSums);
-    const std::int32_t steps = (maxColumns + STEP - 1) / STEP;
-    for (std::int32_t t = steps - 1; t >= 0; --t)
+    // The backward chains, one launch: the blocks of x_F from each supernode's last, by distance from the last.
+    if (!solveLarge.empty())
     {
-        const std::int32_t k0 = t * STEP;
-        std::vector<std::int32_t> diagonal;
-        std::vector<TileTask> above;
-        for (const std::int32_t s : solveLarge)
-        {
-            const FrontDesc& f = plan.fronts[static_cast<std::size_t>(s)];
-            if (f.c <= k0)
-                continue;
-            diagonal.push_back(s);
-            for (std::int32_t i0 = 0; i0 < k0; i0 += device::TILE)
-                above.push_back({s, i0, 0, 0});
-        }
-        addList(plan, backward, LaunchKind::BackwardDiagonal, diagonal, k0);
-        addTiles(plan, backward, LaunchKind::BackwardUpdate, above, k0);
+        std::vector<TileTask> chain;
+        for (std::int32_t d = 0; d < maxBlocks; ++d)
+            for (std::size_t k = 0; k < solveLarge.size(); ++k)
+                if (d < chainBlocks[k])
+                {
+                    const std::int32_t b = chainBlocks[k] - 1 - d;
+                    chain.push_back({solveLarge[k], b * BLOCK, b, static_cast<std::int32_t>(backwardBase[k])});
+                }
+        checkChainOrder(plan, chain, solveLarge, chainBlocks, false);
+        addTiles(plan, backward, LaunchKind::BackwardChain, chain, plan.chainSlots++);
     }
     for (std::size_t k = forwardBefore; k < plan.forwardLaunches.size(); ++k)
         plan.forwardLaunches[k].level = level;

@@ -33,12 +33,12 @@ enum class LaunchKind : int
     UpdateMatrix,
     ForwardSmall,
     ForwardGather,
-    ForwardDiagonal,
-    ForwardUpdate,
+    // the large supernodes of a level in one launch of dataflow tasks, one per 64-row block (k0: the launch's ticket
+    // counter): the forward sweep's blocks of x_F and of the update rows, the backward sweep's blocks of x_F
+    ForwardChain,
     BackwardSmall,
     BackwardRows,
-    BackwardDiagonal,
-    BackwardUpdate,
+    BackwardChain,
     // indefinite mode
     SmallFrontsPivoted,
     PivotedDiagonal,
@@ -51,7 +51,9 @@ enum class LaunchKind : int
     // mixed precision: the update matrices by 128 x 128 tiles on tcgen05 (3xTF32), in place of UpdateMatrix
     UpdateMatrixMixed,
     // the sums of the split products of BackwardRows (supernodes with more than SOLVE_ROWS_CHUNK rows)
-    BackwardRowsReduce
+    BackwardRowsReduce,
+    // the diagonal sweep between the two sweeps (not a plan launch; named in the solves' launch records)
+    DiagonalSweep
 };
 
 // One batched launch: `count` items from `offset` in the array of its kind (front lists: int32; tiles: TileTask;
@@ -109,6 +111,10 @@ struct Plan
     std::int64_t rowEntries = 0;
     // Partial products of the split BackwardRows tiles one level needs at most (each 64 x 64 values).
     std::int64_t rowPartialSlots = 0;
+    // The chain launches' ticket counters (one per launch) and ready flags (one per 64-column block of a large
+    // supernode and sweep direction), reset before each sweep.
+    std::int32_t chainSlots = 0;
+    std::int64_t chainFlags = 0;
     std::int32_t largestSmallOrder = 0;
     double flops = 0.0;
     std::int64_t factorEntries = 0;

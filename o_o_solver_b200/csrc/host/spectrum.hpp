@@ -14,6 +14,7 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstddef>
 #include <cstdint>
 #include <limits>
@@ -123,6 +124,12 @@ struct ModeResult
     double orthogonalisationSeconds = 0.0;
     double projectedSeconds = 0.0;
     std::size_t blockSteps = 0;
+    // Blocks that met a dependent column and were orthonormalised column by column on the host, and the one-column
+    // operator applications that replaced dependent columns.
+    std::size_t hostBlocks = 0;
+    std::size_t replacementSolves = 0;
+    // orthogonalisationSeconds by part: start blocks, block steps, thick restarts, harvests.
+    std::array<double, 4> orthogonalisationParts{};
 };
 
 // ---- proven counts --------------------------------------------------------------------------------------------------

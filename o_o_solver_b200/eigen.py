@@ -73,7 +73,9 @@ class ShiftRecord:
 @dataclass
 class EigenSolution:
     """EigenSolution (BlockLanczos.hpp:81-100): eigenvalues increasing, M-orthonormal eigenvectors (host copy, n x k),
-    the residual bounds, the shifts, and the solve's wall seconds and its factorisations' device seconds."""
+    the residual bounds, the shifts, and the solve's wall seconds and its factorisations' device seconds; phases: wall
+    seconds by phase; slow_paths: blocks orthonormalised column by column on the host and the one-column operator
+    applications that replaced dependent columns."""
 
     eigenvalues: np.ndarray
     eigenvectors: np.ndarray | None
@@ -86,6 +88,7 @@ class EigenSolution:
     seconds: float = 0.0
     factor_seconds: float = 0.0
     phases: dict = field(default_factory=dict)
+    slow_paths: dict = field(default_factory=dict)
 
 
 class BlockLanczos:
@@ -131,8 +134,14 @@ class BlockLanczos:
                                   int(r[6])) for r in records[: int(counts[2])]]
             phases = {"factorisation": float(seconds[2]), "operator": float(seconds[3]),
                       "orthogonalisation": float(seconds[4]), "projected": float(seconds[5])}
+            work = np.zeros(2, dtype=np.int64)
+            parts = np.zeros(4)
+            _check(lib.oosgpu_modes_work(handle, nat.ptr(work, nat.i64p), nat.ptr(parts, nat.f64p)))
+            slow = {"host_blocks": int(work[0]), "replacement_solves": int(work[1])}
+            phases.update({"orthogonalisation_start": float(parts[0]), "orthogonalisation_steps": float(parts[1]),
+                           "orthogonalisation_restarts": float(parts[2]), "orthogonalisation_harvest": float(parts[3])})
             return EigenSolution(values[:k], phi, bounds[:k], shifts, int(counts[1]), int(counts[3]),
-                                 bool(counts[4]), int(counts[5]), float(seconds[0]), float(seconds[1]), phases)
+                                 bool(counts[4]), int(counts[5]), float(seconds[0]), float(seconds[1]), phases, slow)
         finally:
             lib.oosgpu_modes_destroy(handle)
 

