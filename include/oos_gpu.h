@@ -262,6 +262,15 @@ typedef struct oosgpu_pencil oosgpu_pencil;
  * dimension (OOSGPU_INVALID_ARGUMENT), a negative or infinite mass diagonal term (OOSGPU_SOLVER). */
 int oosgpu_pencil_create(const oosgpu_symbolic* symbolic, int device, int32_t dimension, const int64_t* col_offsets,
                          const int32_t* rows, const double* stiffness, const double* mass, oosgpu_pencil** out);
+/* BucklingPencil (include/oos/linalg/eigen/BucklingPencil.hpp:29-72): the pencil K phi = lambda B phi of the stiffness
+ * K and the differential stiffness K_d of a preload (B = -K_d), both lower CSC on one pattern in the symbolic factor's
+ * order. Its shifted matrices K + sigma K_d are factorised in indefinite mode with the powers-of-two scaling of K; the
+ * operator's inner product is K's. oosgpu_modes_solve on it runs BlockLanczos::solveBuckling (BlockLanczos.cpp:90-91):
+ * the load factors nearest 0 of either sign in [lower_bound, upper_bound), by increasing magnitude (the positive first
+ * on a tie); K must be positive definite (OOSGPU_SOLVER otherwise). */
+int oosgpu_pencil_create_buckling(const oosgpu_symbolic* symbolic, int device, int32_t dimension,
+                                  const int64_t* col_offsets, const int32_t* rows, const double* stiffness,
+                                  const double* differential, oosgpu_pencil** out);
 void oosgpu_pencil_destroy(oosgpu_pencil* pencil);
 void* oosgpu_pencil_stream(oosgpu_pencil* pencil);
 /* ShiftedPencil::factorise: S (K - shift M) S factorised in indefinite mode; info->negative is the Sturm count of the

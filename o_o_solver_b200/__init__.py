@@ -1,8 +1,10 @@
 """B200 implementation of O_o_Solver's numeric hot path: the supernodal multifrontal LDL^T factorisation and its
 solves on the GPU, behind the reference's factorisation interface (SymbolicFactor, SupernodalFactor.factorise,
-FactorSolve.solve), the shifted pencil of its eigenvalue analysis (SparsePencil) and a C ABI (include/oos_gpu.h)."""
+FactorSolve.solve), the shifted pencils of its eigenvalue analyses (SparsePencil, BucklingPencil) and a C ABI
+(include/oos_gpu.h)."""
 
 from .linalg import (  # noqa: F401
+    BucklingPencil,
     FactorOptions,
     FactorSolve,
     Inertia,

@@ -98,6 +98,8 @@ SIGNATURES = [
     ("oosgpu_factor_launch_counts", ctypes.c_int, [_vp, ctypes.c_int64, _i64p]),
     ("oosgpu_pencil_create", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int32, _i64p, _i32p, _f64p, _f64p,
                                             ctypes.POINTER(_vp)]),
+    ("oosgpu_pencil_create_buckling", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int32, _i64p, _i32p, _f64p, _f64p,
+                                                     ctypes.POINTER(_vp)]),
     ("oosgpu_pencil_destroy", None, [_vp]),
     ("oosgpu_pencil_stream", _vp, [_vp]),
     ("oosgpu_pencil_factorise", ctypes.c_int, [_vp, ctypes.c_double, ctypes.POINTER(FactorInfo)]),

@@ -2419,12 +2419,17 @@ namespace oosgpu
 class GpuPencil
 {
 public:
+    // The vibration pencil (K, M) (SparsePencil), or with `buckling` the buckling pencil K phi = lambda B phi of the
+    // stiffness and the differential stiffness K_d given as `mass` (BucklingPencil: B = -K_d, held negated, so that
+    // the shifted matrix K - sigma B = K + sigma K_d rounds as the reference's combine(1, K, sigma, K_d); the inner
+    // product is K's).
     GpuPencil(const Symbolic& symbolic, int device, std::int32_t dimension, const std::int64_t* offsets,
-              const std::int32_t* rows, const double* stiffness, const double* mass)
-        : m_factor(symbolic, device), m_device(device), m_dimension(dimension)
+              const std::int32_t* rows, const double* stiffness, const double* mass, bool buckling = false)
+        : m_factor(symbolic, device), m_device(device), m_dimension(dimension), m_buckling(buckling)
     {
+        const char* name = buckling ? "BucklingPencil" : "SparsePencil";
         if (dimension != symbolic.dofCount)
-            throw Error(STATUS_INVALID_ARGUMENT, "SparsePencil: the matrices have " + std::to_string(dimension) +
+            throw Error(STATUS_INVALID_ARGUMENT, std::string(name) + ": the matrices have " + std::to_string(dimension) +
                                                      " equations, the symbolic factor " +
                                                      std::to_string(symbolic.dofCount) +
                                                      "; analyse the pattern the matrices were converted on");
@@ -2432,6 +2437,14 @@ public:
         m_terms = offsets[dimension];
         std::vector<double> scale(n, 1.0);
         std::vector<double> massDiagonal(n, 0.0);
+        std::vector<double> right;
+        if (buckling)
+        {
+            right.resize(static_cast<std::size_t>(m_terms));
+            for (std::size_t t = 0; t < right.size(); ++t)
+                right[t] = -mass[t];
+            mass = right.data();
+        }
         m_rayleighBound = INFINITY;
         m_lumped = true;
         for (std::size_t j = 0; j < n; ++j)
@@ -2440,12 +2453,21 @@ public:
             const bool hasDiagonal = first < offsets[j + 1] && static_cast<std::size_t>(rows[first]) == j;
             const double k = hasDiagonal ? stiffness[first] : 0.0;
             const double m = hasDiagonal ? mass[first] : 0.0;
-            if (!std::isfinite(m) || m < 0.0)
-                throw Error(STATUS_SOLVER, "eigenvalue analysis: the mass matrix has the diagonal term " +
-                                               std::to_string(m) + " at equation " + std::to_string(j) +
-                                               "; the Lanczos method needs a positive semi-definite mass matrix");
-            if (m > 0.0 && k > 0.0)
-                m_rayleighBound = std::min(m_rayleighBound, k / m);
+            if (buckling)
+            {
+                // min K_ii / |K_d,ii| over K_d,ii != 0 (finite) and K_ii > 0 (BucklingPencil.cpp:31-44)
+                if (m != 0.0 && std::isfinite(m) && k > 0.0)
+                    m_rayleighBound = std::min(m_rayleighBound, k / std::abs(m));
+            }
+            else
+            {
+                if (!std::isfinite(m) || m < 0.0)
+                    throw Error(STATUS_SOLVER, "eigenvalue analysis: the mass matrix has the diagonal term " +
+                                                   std::to_string(m) + " at equation " + std::to_string(j) +
+                                                   "; the Lanczos method needs a positive semi-definite mass matrix");
+                if (m > 0.0 && k > 0.0)
+                    m_rayleighBound = std::min(m_rayleighBound, k / m);
+            }
             massDiagonal[j] = m;
             // pencilScaleOf: K_ii = f 2^e with f in [0.5, 1): the scale 2^(-(e/2)) leaves a scaled diagonal in [1/4, 2).
             if (k > 0.0 && std::isfinite(k))
@@ -2513,6 +2535,23 @@ public:
                                        static_cast<int>(std::min<std::int64_t>(32, columns - c0)));
     }
 
+    // Y <- G X, G the matrix of the inner product: M, or K for a buckling pencil (BucklingPencil::multiplyInnerProduct).
+    void multiplyInnerProduct(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, std::int64_t columns)
+    {
+        if (!m_buckling)
+        {
+            multiplyMass(x, ldx, y, ldy, columns);
+            return;
+        }
+        check(cudaSetDevice(m_device), "cudaSetDevice");
+        if (ldx < m_dimension || ldy < m_dimension || columns < 0)
+            throw Error(STATUS_INVALID_ARGUMENT, "BucklingPencil::multiplyInnerProduct: leading dimensions below the rows");
+        for (std::int64_t c0 = 0; c0 < columns; c0 += 32)
+            m_factor.multiplySymmetric(m_stiffness.get(), x + c0 * ldx, ldx, y + c0 * ldy, ldy,
+                                       static_cast<int>(std::min<std::int64_t>(32, columns - c0)));
+    }
+
+    [[nodiscard]] bool buckling() const noexcept { return m_buckling; }
     [[nodiscard]] cudaStream_t stream() const noexcept { return m_factor.stream(); }
     [[nodiscard]] double rayleighBound() const noexcept { return m_rayleighBound; }
     [[nodiscard]] bool lumped() const noexcept { return m_lumped; }
@@ -2525,6 +2564,7 @@ private:
     GpuFactor m_factor;
     int m_device = 0;
     std::int32_t m_dimension = 0;
+    bool m_buckling = false;
     std::int64_t m_terms = 0;
     double m_rayleighBound = 0.0;
     bool m_lumped = true;
@@ -2556,6 +2596,11 @@ public:
     void multiplyMass(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, std::int64_t columns) override
     {
         m_pencil.multiplyMass(x, ldx, y, ldy, columns);
+    }
+    void multiplyInnerProduct(const double* x, std::int64_t ldx, double* y, std::int64_t ldy,
+                              std::int64_t columns) override
+    {
+        m_pencil.multiplyInnerProduct(x, ldx, y, ldy, columns);
     }
     [[nodiscard]] double diagonalRayleighBound() const override { return m_pencil.rayleighBound(); }
     [[nodiscard]] cudaStream_t stream() const override { return m_pencil.stream(); }
@@ -3191,6 +3236,26 @@ extern "C" int oosgpu_pencil_create(const oosgpu_symbolic* symbolic, int device,
         });
 }
 
+extern "C" int oosgpu_pencil_create_buckling(const oosgpu_symbolic* symbolic, int device, int32_t dimension,
+                                             const int64_t* col_offsets, const int32_t* rows, const double* stiffness,
+                                             const double* differential, oosgpu_pencil** out)
+{
+    return guarded(
+        [&]
+        {
+            requirePointer(symbolic, "symbolic");
+            requirePointer(col_offsets, "col_offsets");
+            requirePointer(rows, "rows");
+            requirePointer(stiffness, "stiffness");
+            requirePointer(differential, "differential");
+            requirePointer(out, "out");
+            auto handle = std::make_unique<oosgpu_pencil>();
+            handle->pencil = std::make_unique<oosgpu::GpuPencil>(symbolic->symbolic, device, dimension, col_offsets,
+                                                                 rows, stiffness, differential, true);
+            *out = handle.release();
+        });
+}
+
 extern "C" void oosgpu_pencil_destroy(oosgpu_pencil* pencil)
 {
     delete pencil;
@@ -3313,7 +3378,15 @@ int modesSolve(oosgpu_pencil* pencil, const oosgpu_eigen_request* request, const
             oosgpu::check(cudaSetDevice(pencil->pencil->factor().deviceOrdinal()), "cudaSetDevice");
             oosgpu::PencilOperations operations(*pencil->pencil);
             auto handle = std::make_unique<oosgpu_modes>();
-            handle->solution = oosgpu::eigen::solveModes(operations, eigenRequest, lanczos, start, ld);
+            if (pencil->pencil->buckling())
+            {
+                if (start != nullptr)
+                    throw oosgpu::Error(oosgpu::STATUS_INVALID_ARGUMENT,
+                                        "learned start: a buckling pencil takes no start block");
+                handle->solution = oosgpu::eigen::solveBuckling(operations, eigenRequest, lanczos);
+            }
+            else
+                handle->solution = oosgpu::eigen::solveModes(operations, eigenRequest, lanczos, start, ld);
             *out = handle.release();
         });
 }

@@ -45,8 +45,12 @@ public:
     virtual Inertia factorise(double shift) = 0;
     // X <- (K - shift M)^-1 X with the last factorisation.
     virtual void solve(double* x, std::int64_t ld, std::int64_t columns) = 0;
-    // Y <- M X (Y distinct from X).
+    // Y <- M X (Y distinct from X): the right-hand matrix of the pencil (the mass of a vibration problem, B = -K_d of
+    // a buckling problem).
     virtual void multiplyMass(const double* x, std::int64_t ldx, double* y, std::int64_t ldy, std::int64_t columns) = 0;
+    // Y <- G X, G the matrix of the inner product the operator is self-adjoint in (M for vibration, K for buckling).
+    virtual void multiplyInnerProduct(const double* x, std::int64_t ldx, double* y, std::int64_t ldy,
+                                      std::int64_t columns) = 0;
     // An estimate of the pencil's scale (max K_ii / M_ii over the DOFs with mass), the unit of the shift rules.
     [[nodiscard]] virtual double diagonalRayleighBound() const = 0;
     [[nodiscard]] virtual cudaStream_t stream() const = 0;
@@ -258,5 +262,10 @@ void validate(const KrylovSettings& settings);
 // random start block (a learned start); later runs start from random blocks.
 ModeResult solveModes(PencilPort& pencil, const ModeRequest& request, const KrylovSettings& settings,
                       const double* start = nullptr, std::int64_t startLd = 0);
+// The load factors of a buckling pencil (K phi = lambda B phi, B = -K_d; PencilPort: multiplyMass gives B X,
+// multiplyInnerProduct K X) nearest 0 of either sign in the request's range [low, high), at most `count` of them
+// (the reference's BlockLanczos::solveBuckling, src/linalg/eigen/BlockLanczosBuckling.cpp): values by increasing
+// magnitude, the positive first on a tie.
+ModeResult solveBuckling(PencilPort& pencil, const ModeRequest& request, const KrylovSettings& settings);
 
 } // namespace oosgpu::eigen

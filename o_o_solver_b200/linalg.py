@@ -545,19 +545,22 @@ class SparsePencil:
     PencilScaling); solve() applies (K - shift M)^-1 and multiply_mass() M to device blocks with contiguous columns
     (torch tensors) or to column-major host arrays (copied through the device)."""
 
+    _CREATE = "oosgpu_pencil_create"
+    _NAME = "SparsePencil"
+
     def __init__(self, symbolic: SymbolicFactor, stiffness: SymmetricCsc, mass: SymmetricCsc, device: int = 0):
         offsets = np.ascontiguousarray(stiffness.offsets, dtype=np.int64)
         rows = np.ascontiguousarray(stiffness.rows, dtype=np.int32)
         if not (np.array_equal(offsets, np.asarray(mass.offsets)) and np.array_equal(rows, np.asarray(mass.rows))):
-            raise ValueError("SparsePencil: the stiffness and the mass differ in structure")
+            raise ValueError(f"{self._NAME}: the two matrices differ in structure")
         k = np.ascontiguousarray(stiffness.values, dtype=np.float64)
         m = np.ascontiguousarray(mass.values, dtype=np.float64)
         self.symbolic = symbolic
         self.device = device
         self._handle = nat.vp()
-        _check(nat.load().oosgpu_pencil_create(symbolic._handle, device, len(offsets) - 1, nat.ptr(offsets, nat.i64p),
-                                               nat.ptr(rows, nat.i32p), nat.ptr(k, nat.f64p), nat.ptr(m, nat.f64p),
-                                               ctypes.byref(self._handle)))
+        _check(getattr(nat.load(), self._CREATE)(symbolic._handle, device, len(offsets) - 1, nat.ptr(offsets, nat.i64p),
+                                                 nat.ptr(rows, nat.i32p), nat.ptr(k, nat.f64p), nat.ptr(m, nat.f64p),
+                                                 ctypes.byref(self._handle)))
         self._dimension = len(offsets) - 1
 
     @property
@@ -638,3 +641,17 @@ class SparsePencil:
             self.close()
         except Exception:
             pass
+
+
+class BucklingPencil(SparsePencil):
+    """BucklingPencil (include/oos/linalg/eigen/BucklingPencil.hpp:29-72) on the GPU: K phi = lambda B phi with B = -K_d,
+    K the stiffness and K_d the differential stiffness of a preload, two lower CSC matrices of one structure.
+    factorise(shift) factorises S (K + shift K_d) S in indefinite mode (S the powers of two of K's diagonal);
+    multiply_mass() applies B = -K_d. BlockLanczos.solve on it finds the load factors nearest 0 of either sign
+    (BlockLanczos::solveBuckling)."""
+
+    _CREATE = "oosgpu_pencil_create_buckling"
+    _NAME = "BucklingPencil"
+
+    def __init__(self, symbolic: SymbolicFactor, stiffness: SymmetricCsc, differential: SymmetricCsc, device: int = 0):
+        super().__init__(symbolic, stiffness, differential, device)

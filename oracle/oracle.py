@@ -76,6 +76,7 @@ def ref_lib():
     lib.ref_modes.argtypes = [_vp, ctypes.c_int32, _i64p, _i32p, _f64p, _f64p, ctypes.c_double, ctypes.c_double,
                               ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int, _f64p,
                               ctypes.c_int64, _f64p, _f64p, ctypes.c_int64, _i64p, _f64p]
+    lib.ref_buckling.argtypes = lib.ref_modes.argtypes
     lib.ref_pencil_scale.argtypes = [ctypes.c_int32, _i64p, _i32p, _f64p, _f64p]
     lib.ref_symmetric_eigen.argtypes = [_f64p, ctypes.c_int64, ctypes.c_int64, _f64p, _f64p]
     lib.ref_sturm_verify.argtypes = [ctypes.c_int64, _f64p, _i64p, ctypes.c_int64, _f64p, _f64p]
@@ -276,10 +277,13 @@ class RefPartial:
 
 
 def modes(symbolic: RefSymbolic, offsets, rows, stiffness, mass, mode_count, block_size=8, family=-1, threads=1,
-          vectors=True, lower=-np.inf, upper=np.inf, modes_per_shift=0, capacity=None):
+          vectors=True, lower=-np.inf, upper=np.inf, modes_per_shift=0, capacity=None, buckling=False):
     """SparsePencil + BlockLanczos::solve of the request (lower, upper, mode_count). shifts: one row per shift of
-    (shift, purpose, sturm count, has run, block steps, restarts, converged)."""
+    (shift, purpose, sturm count, has run, block steps, restarts, converged). buckling: BucklingPencil instead, `mass`
+    then being the differential stiffness K_d (BlockLanczos::solveBuckling, the load factors of K x = -lambda K_d x
+    nearest 0)."""
     lib = ref_lib()
+    solve = lib.ref_buckling if buckling else lib.ref_modes
     n = symbolic.dof_count
     offsets = np.ascontiguousarray(offsets, dtype=np.int64)
     rows = np.ascontiguousarray(rows, dtype=np.int32)
@@ -291,10 +295,10 @@ def modes(symbolic: RefSymbolic, offsets, rows, stiffness, mass, mode_count, blo
     shifts = np.zeros((64, 7))
     counts = np.zeros(5, dtype=np.int64)
     seconds = np.zeros(1)
-    _check(lib.ref_modes(symbolic.handle, n, _ptr(offsets, _i64p), _ptr(rows, _i32p), _ptr(stiffness, _f64p),
-                         _ptr(mass, _f64p), lower, upper, mode_count, block_size, modes_per_shift, family, threads,
-                         _ptr(values, _f64p), capacity, _ptr(vecs, _f64p), _ptr(shifts, _f64p), 64,
-                         _ptr(counts, _i64p), _ptr(seconds, _f64p)))
+    _check(solve(symbolic.handle, n, _ptr(offsets, _i64p), _ptr(rows, _i32p), _ptr(stiffness, _f64p),
+                 _ptr(mass, _f64p), lower, upper, mode_count, block_size, modes_per_shift, family, threads,
+                 _ptr(values, _f64p), capacity, _ptr(vecs, _f64p), _ptr(shifts, _f64p), 64,
+                 _ptr(counts, _i64p), _ptr(seconds, _f64p)))
     found = int(counts[0])
     return {
         "eigenvalues": values[:found],

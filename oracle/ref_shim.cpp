@@ -12,6 +12,7 @@
 #include "oos/linalg/dense/KernelSelection.hpp"
 #include "oos/linalg/dense/SmallEigenSolver.hpp"
 #include "oos/linalg/eigen/BlockLanczos.hpp"
+#include "oos/linalg/eigen/BucklingPencil.hpp"
 #include "oos/linalg/eigen/PencilScaling.hpp"
 #include "oos/linalg/eigen/ShiftStrategy.hpp"
 #include "oos/linalg/eigen/SparsePencil.hpp"
@@ -392,7 +393,11 @@ extern "C" int ref_partial_recover(const ref_partial* p, double* loads, int64_t 
         });
 }
 
-extern "C" int ref_modes(const ref_symbolic* s, int32_t dimension, const int64_t* col_offsets, const int32_t* rows,
+namespace
+{
+
+// SparsePencil (buckling false) or BucklingPencil (the second matrix K_d) + BlockLanczos::solve of one request.
+int eigenSolve(bool buckling, const ref_symbolic* s, int32_t dimension, const int64_t* col_offsets, const int32_t* rows,
                          const double* stiffness, const double* mass, double lower, double upper, int64_t mode_count,
                          int64_t block_size, int64_t modes_per_shift, int family, int threads, double* eigenvalues,
                          int64_t capacity, double* eigenvectors, double* shifts, int64_t max_shifts,
@@ -419,7 +424,11 @@ extern "C" int ref_modes(const ref_symbolic* s, int32_t dimension, const int64_t
             const DenseKernels kernels(kindOf(family), options);
             FactorOptions factorOptions;
             const auto start = std::chrono::steady_clock::now();
-            SparsePencil pencil(s->symbolic, k, m, kernels, factorOptions, budget);
+            std::unique_ptr<ShiftedPencil> pencil;
+            if (buckling)
+                pencil = std::make_unique<BucklingPencil>(s->symbolic, k, m, kernels, factorOptions, budget);
+            else
+                pencil = std::make_unique<SparsePencil>(s->symbolic, k, m, kernels, factorOptions, budget);
             LanczosOptions lanczos;
             if (block_size > 0)
                 lanczos.blockSize = static_cast<std::size_t>(block_size);
@@ -429,7 +438,7 @@ extern "C" int ref_modes(const ref_symbolic* s, int32_t dimension, const int64_t
             request.lowerBound = lower;
             request.upperBound = upper;
             request.modeCount = static_cast<std::size_t>(mode_count);
-            const EigenSolution solution = BlockLanczos(lanczos).solve(pencil, request, kernels, budget);
+            const EigenSolution solution = BlockLanczos(lanczos).solve(*pencil, request, kernels, budget);
             if (seconds != nullptr)
                 seconds[0] = secondsSince(start);
             const std::size_t found = std::min<std::size_t>(solution.eigenvalues.size(),
@@ -461,6 +470,30 @@ extern "C" int ref_modes(const ref_symbolic* s, int32_t dimension, const int64_t
             counts[3] = static_cast<int64_t>(solution.verifiedCount);
             counts[4] = solution.isComplete ? 1 : 0;
         });
+}
+
+} // namespace
+
+extern "C" int ref_modes(const ref_symbolic* s, int32_t dimension, const int64_t* col_offsets, const int32_t* rows,
+                         const double* stiffness, const double* mass, double lower, double upper, int64_t mode_count,
+                         int64_t block_size, int64_t modes_per_shift, int family, int threads, double* eigenvalues,
+                         int64_t capacity, double* eigenvectors, double* shifts, int64_t max_shifts,
+                         int64_t counts[5], double* seconds)
+{
+    return eigenSolve(false, s, dimension, col_offsets, rows, stiffness, mass, lower, upper, mode_count, block_size,
+                      modes_per_shift, family, threads, eigenvalues, capacity, eigenvectors, shifts, max_shifts, counts,
+                      seconds);
+}
+
+extern "C" int ref_buckling(const ref_symbolic* s, int32_t dimension, const int64_t* col_offsets,
+                            const int32_t* rows, const double* stiffness, const double* differential, double lower,
+                            double upper, int64_t mode_count, int64_t block_size, int64_t modes_per_shift, int family,
+                            int threads, double* eigenvalues, int64_t capacity, double* eigenvectors, double* shifts,
+                            int64_t max_shifts, int64_t counts[5], double* seconds)
+{
+    return eigenSolve(true, s, dimension, col_offsets, rows, stiffness, differential, lower, upper, mode_count,
+                      block_size, modes_per_shift, family, threads, eigenvalues, capacity, eigenvectors, shifts,
+                      max_shifts, counts, seconds);
 }
 
 extern "C" int ref_pencil_scale(int32_t dimension, const int64_t* col_offsets, const int32_t* rows,

@@ -78,6 +78,14 @@ int ref_modes(const ref_symbolic* s, int32_t dimension, const int64_t* col_offse
               int64_t capacity, double* eigenvectors, double* shifts, int64_t max_shifts, int64_t counts[5],
               double* seconds);
 
+/* The same for the buckling pencil (BucklingPencil, BlockLanczos::solveBuckling): K x = lambda (-K_d) x, the load
+ * factors nearest 0 of either sign in [lower, upper); `differential` is K_d on the pattern of K. */
+int ref_buckling(const ref_symbolic* s, int32_t dimension, const int64_t* col_offsets, const int32_t* rows,
+                 const double* stiffness, const double* differential, double lower, double upper, int64_t mode_count,
+                 int64_t block_size, int64_t modes_per_shift, int family, int threads, double* eigenvalues,
+                 int64_t capacity, double* eigenvectors, double* shifts, int64_t max_shifts, int64_t counts[5],
+                 double* seconds);
+
 /* SturmCheck::addPoint + verify (src/linalg/eigen/SturmCheck.cpp): result = verifiedUpTo, verifiedCount,
  * hasMismatch, mismatch.lower, mismatch.upper, expected * 1e6 + found. */
 int ref_sturm_verify(int64_t points, const double* shifts, const int64_t* counts, int64_t values, const double* sorted,
