@@ -333,11 +333,12 @@ int oosgpu_modes_solve_start(oosgpu_pencil* pencil, const oosgpu_eigen_request* 
  * wall seconds of [2] the factorisations, [3] the operator (solves and mass products), [4] the M-orthogonalisation
  * and the basis products, [5] the projected problem. */
 int oosgpu_modes_summary(const oosgpu_modes* modes, int64_t counts[6], double seconds[6]);
-/* Where a solve's orthogonalisation went. counts: [0] blocks that met a dependent column and were orthonormalised
- * column by column (the reference's MassOrthogonalizer fallback), [1] one-column operator applications that replaced
- * dependent columns; seconds (wall, parts of seconds[4] of the summary): [0] start blocks, [1] block steps, [2] thick
- * restarts, [3] harvests of converged pairs. Either may be null. No counterpart in the reference's API. */
-int oosgpu_modes_work(const oosgpu_modes* modes, int64_t counts[2], double seconds[4]);
+/* Where a solve's time went. counts: [0] blocks that met a dependent column and were orthonormalised column by column
+ * (the reference's MassOrthogonalizer fallback), [1] one-column operator applications that replaced dependent columns;
+ * seconds (wall): the parts of seconds[4] of the summary, [0] start blocks, [1] block steps, [2] thick restarts,
+ * [3] harvests of converged pairs; then outside the summary's phases, [4] the workspace's set-up, [5] the answer's
+ * gathering, [6] the workspace's release. Either may be null. No counterpart in the reference's API. */
+int oosgpu_modes_work(const oosgpu_modes* modes, int64_t counts[2], double seconds[7]);
 /* The eigenvalues (increasing) and their residual bounds ||Op y - theta y||_M / |theta|. */
 int oosgpu_modes_values(const oosgpu_modes* modes, double* eigenvalues, double* residual_bounds);
 /* The M-orthonormal eigenvectors, dimension x count, into host memory of leading dimension ld. */

@@ -3436,7 +3436,7 @@ extern "C" int oosgpu_modes_summary(const oosgpu_modes* modes, int64_t counts[6]
         });
 }
 
-extern "C" int oosgpu_modes_work(const oosgpu_modes* modes, int64_t counts[2], double seconds[4])
+extern "C" int oosgpu_modes_work(const oosgpu_modes* modes, int64_t counts[2], double seconds[7])
 {
     return guarded(
         [&]
@@ -3449,7 +3449,10 @@ extern "C" int oosgpu_modes_work(const oosgpu_modes* modes, int64_t counts[2], d
                 counts[1] = static_cast<int64_t>(s.replacementSolves);
             }
             if (seconds != nullptr)
+            {
                 std::copy(s.orthogonalisationParts.begin(), s.orthogonalisationParts.end(), seconds);
+                std::copy(s.outsideParts.begin(), s.outsideParts.end(), seconds + 4);
+            }
         });
 }
 

@@ -6,6 +6,8 @@
 #include "host_api.hpp"
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <string>
 
@@ -46,10 +48,88 @@ double hypotenuse(double a, double b)
 
 } // namespace
 
+namespace
+{
+
+// Freed buffers kept for reuse, at most CACHE_LIMIT bytes in all; beyond that a buffer is freed at once.
+constexpr std::size_t CACHE_LIMIT = std::size_t{4} << 30;
+
+struct BufferCache
+{
+    std::mutex lock;
+    std::multimap<std::pair<int, std::size_t>, double*> idle;
+    std::size_t idleBytes = 0;
+};
+
+BufferCache& bufferCache()
+{
+    static BufferCache* cache = new BufferCache(); // never destroyed: the context's teardown frees the buffers
+    return *cache;
+}
+
+} // namespace
+
+double* takeDeviceBuffer(std::size_t bytes, const char* what)
+{
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess)
+        throw Error(STATUS_CUDA, std::string(what) + ": no current device");
+    BufferCache& cache = bufferCache();
+    {
+        const std::lock_guard<std::mutex> guard(cache.lock);
+        const auto found = cache.idle.find({device, bytes});
+        if (found != cache.idle.end())
+        {
+            double* p = found->second;
+            cache.idle.erase(found);
+            cache.idleBytes -= bytes;
+            return p;
+        }
+    }
+    void* p = nullptr;
+    cudaError_t status = cudaMalloc(&p, bytes);
+    if (status == cudaErrorMemoryAllocation)
+    {
+        // give this device's idle buffers back and try once more
+        (void)cudaGetLastError();
+        const std::lock_guard<std::mutex> guard(cache.lock);
+        for (auto it = cache.idle.begin(); it != cache.idle.end();)
+            if (it->first.first == device)
+            {
+                cudaFree(it->second);
+                cache.idleBytes -= it->first.second;
+                it = cache.idle.erase(it);
+            }
+            else
+                ++it;
+        status = cudaMalloc(&p, bytes);
+    }
+    if (status != cudaSuccess)
+        throw Error(status == cudaErrorMemoryAllocation ? STATUS_MEMORY_BUDGET : STATUS_CUDA,
+                    std::string(what) + ": " + cudaGetErrorString(status));
+    return static_cast<double*>(p);
+}
+
+void giveDeviceBuffer(double* p, std::size_t bytes, int device) noexcept
+{
+    if (p == nullptr)
+        return;
+    BufferCache& cache = bufferCache();
+    {
+        const std::lock_guard<std::mutex> guard(cache.lock);
+        if (cache.idleBytes + bytes <= CACHE_LIMIT)
+        {
+            cache.idle.insert({{device, bytes}, p});
+            cache.idleBytes += bytes;
+            return;
+        }
+    }
+    cudaFree(p);
+}
+
 void DeviceFree::operator()(double* p) const noexcept
 {
-    if (p != nullptr)
-        cudaFree(p);
+    giveDeviceBuffer(p, bytes, device);
 }
 
 // ---- CountLedger ----------------------------------------------------------------------------------------------------

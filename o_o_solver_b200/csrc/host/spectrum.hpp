@@ -102,8 +102,16 @@ struct ShiftLog
     std::size_t converged = 0;
 };
 
+// Device buffers of the eigen solves come from a process-wide cache of freed buffers (per device and size), so that
+// the solves after the first allocate and free nothing: cudaFree synchronises the device, and freeing a solve's
+// workspace was measured at up to 1.1 s on a B200 holding a large factor.
+double* takeDeviceBuffer(std::size_t bytes, const char* what);
+void giveDeviceBuffer(double* p, std::size_t bytes, int device) noexcept;
+
 struct DeviceFree
 {
+    std::size_t bytes = 0;
+    int device = 0;
     void operator()(double* p) const noexcept;
 };
 
@@ -134,6 +142,8 @@ struct ModeResult
     std::size_t replacementSolves = 0;
     // orthogonalisationSeconds by part: start blocks, block steps, thick restarts, harvests.
     std::array<double, 4> orthogonalisationParts{};
+    // Wall seconds outside the phases: the workspace's set-up, the answer's gathering, the workspace's release.
+    std::array<double, 3> outsideParts{};
 };
 
 // ---- proven counts --------------------------------------------------------------------------------------------------

@@ -135,11 +135,12 @@ class BlockLanczos:
             phases = {"factorisation": float(seconds[2]), "operator": float(seconds[3]),
                       "orthogonalisation": float(seconds[4]), "projected": float(seconds[5])}
             work = np.zeros(2, dtype=np.int64)
-            parts = np.zeros(4)
+            parts = np.zeros(7)
             _check(lib.oosgpu_modes_work(handle, nat.ptr(work, nat.i64p), nat.ptr(parts, nat.f64p)))
             slow = {"host_blocks": int(work[0]), "replacement_solves": int(work[1])}
             phases.update({"orthogonalisation_start": float(parts[0]), "orthogonalisation_steps": float(parts[1]),
-                           "orthogonalisation_restarts": float(parts[2]), "orthogonalisation_harvest": float(parts[3])})
+                           "orthogonalisation_restarts": float(parts[2]), "orthogonalisation_harvest": float(parts[3]),
+                           "setup": float(parts[4]), "answer": float(parts[5]), "release": float(parts[6])})
             return EigenSolution(values[:k], phi, bounds[:k], shifts, int(counts[1]), int(counts[3]),
                                  bool(counts[4]), int(counts[5]), float(seconds[0]), float(seconds[1]), phases, slow)
         finally:
