@@ -403,69 +403,11 @@ __global__ void __launch_bounds__(DIAGONAL_THREADS) diagonalBlocksByColumn(Facto
         }
         __syncthreads();
     }
-    // the inverse by 16 x 16 blocks: first the four diagonal blocks by substitution (thread t < BLOCK takes column t
-    // of its block, X(i, j) = -sum_{j <= q < i} L(i, q) X(q, j) in q order), then the off-diagonal blocks by block
-    // diagonals, X_IJ = -X_II (sum_{J <= K < I} L_IK X_KJ); X(i, j) is kept at (j, i). Beyond kb the block holds the
-    // identity, so every value stays finite.
+    // the inverse by 16 x 16 blocks, X(i, j) kept at (j, i)
     if (t >= kb && t < BLOCK)
         a[t + t * LD] = 1.0;
     __syncthreads();
-    if (t < BLOCK)
-    {
-        const int j0 = t & ~(INVERSE_SUB - 1);
-        const int jj = t - j0;
-        double x[INVERSE_SUB];
-#pragma unroll
-        for (int i = 0; i < INVERSE_SUB; ++i)
-        {
-            double sum = 0.0;
-#pragma unroll
-            for (int q = 0; q < i; ++q)
-                if (q >= jj)
-                    sum += a[(j0 + i) + (j0 + q) * LD] * x[q];
-            x[i] = i == jj ? 1.0 : -sum;
-            if (i > jj)
-                a[t + (j0 + i) * LD] = x[i];
-        }
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int d = 1; d < BLOCK / INVERSE_SUB; ++d)
-    {
-        const int count = (BLOCK / INVERSE_SUB - d) * INVERSE_SUB * INVERSE_SUB;
-        for (int e = t; e < count; e += DIAGONAL_THREADS) // T_IJ = sum_{J <= K < I} L_IK X_KJ
-        {
-            const int b = e / (INVERSE_SUB * INVERSE_SUB);
-            const int p = (e / INVERSE_SUB) % INVERSE_SUB;
-            const int q = e % INVERSE_SUB;
-            const int jBase = b * INVERSE_SUB;
-            const int iRow = (b + d) * INVERSE_SUB + p;
-            double sum = a[iRow + (jBase + q) * LD]; // X_JJ(q, q) = 1
-#pragma unroll 1
-            for (int r = q + 1; r < INVERSE_SUB; ++r)
-                sum += a[iRow + (jBase + r) * LD] * a[(jBase + q) + (jBase + r) * LD];
-#pragma unroll 1
-            for (int kBase = jBase + INVERSE_SUB; kBase < (b + d) * INVERSE_SUB; kBase += INVERSE_SUB)
-#pragma unroll 4
-                for (int r = 0; r < INVERSE_SUB; ++r)
-                    sum += a[iRow + (kBase + r) * LD] * a[(jBase + q) + (kBase + r) * LD];
-            products[e] = sum;
-        }
-        __syncthreads();
-        for (int e = t; e < count; e += DIAGONAL_THREADS) // X_IJ = -X_II T_IJ
-        {
-            const int b = e / (INVERSE_SUB * INVERSE_SUB);
-            const int p = (e / INVERSE_SUB) % INVERSE_SUB;
-            const int q = e % INVERSE_SUB;
-            const int iBase = (b + d) * INVERSE_SUB;
-            double sum = products[e];
-#pragma unroll 1
-            for (int r = 0; r < p; ++r)
-                sum += a[(iBase + r) + (iBase + p) * LD] * products[b * INVERSE_SUB * INVERSE_SUB + r * INVERSE_SUB + q];
-            a[(b * INVERSE_SUB + q) + (iBase + p) * LD] = -sum;
-        }
-        __syncthreads();
-    }
+    invertUnitLowerBlocked(a, products);
     // L and D (lower triangle) and L11^-1 (strict upper triangle) back into the panel
     for (int e = t; e < BLOCK * BLOCK; e += DIAGONAL_THREADS)
     {

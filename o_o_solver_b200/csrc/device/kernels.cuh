@@ -96,6 +96,76 @@ constexpr std::size_t smallFrontSmem(int order)
            static_cast<std::size_t>(order) * sizeof(std::int32_t);
 }
 constexpr int DIAGONAL_THREADS = 256;
+// The inverse of a 64 x 64 unit lower block by 16 x 16 blocks, in shared memory by DIAGONAL_THREADS threads: `a`
+// (leading dimension 65) holds L's strict lower triangle (the diagonal taken as 1; beyond the block's order the
+// caller puts the identity); X = L^-1 is written into the strict upper triangle, X(i, j) at (j, i). First the four
+// diagonal blocks by substitution (thread t < 64 takes column t of its block, X(i, j) = -sum_{j <= q < i} L(i, q)
+// X(q, j) in q order), then the off-diagonal blocks by block diagonals, X_IJ = -X_II (sum_{J <= K < I} L_IK X_KJ).
+// products: 3 x 16 x 16 doubles of shared memory. Synchronises before and after.
+__device__ __forceinline__ void invertUnitLowerBlocked(double* a, double* products)
+{
+    constexpr int B = 64;
+    constexpr int LD = B + 1;
+    constexpr int SUB = 16;
+    const int t = threadIdx.x;
+    __syncthreads();
+    if (t < B)
+    {
+        const int j0 = t & ~(SUB - 1);
+        const int jj = t - j0;
+        double x[SUB];
+#pragma unroll
+        for (int i = 0; i < SUB; ++i)
+        {
+            double sum = 0.0;
+#pragma unroll
+            for (int q = 0; q < i; ++q)
+                if (q >= jj)
+                    sum += a[(j0 + i) + (j0 + q) * LD] * x[q];
+            x[i] = i == jj ? 1.0 : -sum;
+            if (i > jj)
+                a[t + (j0 + i) * LD] = x[i];
+        }
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int d = 1; d < B / SUB; ++d)
+    {
+        const int count = (B / SUB - d) * SUB * SUB;
+        for (int e = t; e < count; e += DIAGONAL_THREADS) // T_IJ = sum_{J <= K < I} L_IK X_KJ
+        {
+            const int b = e / (SUB * SUB);
+            const int p = (e / SUB) % SUB;
+            const int q = e % SUB;
+            const int jBase = b * SUB;
+            const int iRow = (b + d) * SUB + p;
+            double sum = a[iRow + (jBase + q) * LD]; // X_JJ(q, q) = 1
+#pragma unroll 1
+            for (int r = q + 1; r < SUB; ++r)
+                sum += a[iRow + (jBase + r) * LD] * a[(jBase + q) + (jBase + r) * LD];
+#pragma unroll 1
+            for (int kBase = jBase + SUB; kBase < (b + d) * SUB; kBase += SUB)
+#pragma unroll 4
+                for (int r = 0; r < SUB; ++r)
+                    sum += a[iRow + (kBase + r) * LD] * a[(jBase + q) + (kBase + r) * LD];
+            products[e] = sum;
+        }
+        __syncthreads();
+        for (int e = t; e < count; e += DIAGONAL_THREADS) // X_IJ = -X_II T_IJ
+        {
+            const int b = e / (SUB * SUB);
+            const int p = (e / SUB) % SUB;
+            const int q = e % SUB;
+            const int iBase = (b + d) * SUB;
+            double sum = products[e];
+#pragma unroll 1
+            for (int r = 0; r < p; ++r)
+                sum += a[(iBase + r) + (iBase + p) * LD] * products[b * SUB * SUB + r * SUB + q];
+            a[(b * SUB + q) + (iBase + p) * LD] = -sum;
+        }
+        __syncthreads();
+    }
+}
 // ---- the workload models' stiffness on the GPU (model_kernels.cu) ----
 // One kind of element matrix (family 0 flat shell of a x b, thickness, young, poisson, turned by orientation 0..2;
 // 1 hexahedron of edge a; 2 given at `given` + givenOffset, row-major); dofs x dofs, at most 24.

@@ -303,32 +303,6 @@ __device__ int bunchKaufman(At at, int n, int candidates, int* perm, double* sub
     return k;
 }
 
-// Column j of the inverse of the unit lower 64 x 64 block `a` (column-major, leading dimension 65, zero outside its
-// kb x kb corner) by forward substitution of e_j in registers, written into block's strict upper triangle
-// (L^-1(i, j) at (j, i)). Not inlined: its registers are its own, not added to the Bunch-Kaufman kernel's.
-__device__ __noinline__ void invertColumn(const double* a, int j, int kb, double* block, std::int64_t n)
-{
-    constexpr int B = 64;
-    constexpr int LD = B + 1;
-    double x[B];
-#pragma unroll
-    for (int i = 0; i < B; ++i)
-        x[i] = i == j ? 1.0 : 0.0;
-#pragma unroll
-    for (int i = 1; i < B; ++i)
-    {
-        double v = x[i];
-#pragma unroll
-        for (int q = 0; q < i; ++q)
-            v -= a[i + q * LD] * x[q];
-        x[i] = v;
-    }
-#pragma unroll
-    for (int i = 1; i < B; ++i)
-        if (i > j && i < kb)
-            block[j + static_cast<std::int64_t>(i) * n] = x[i];
-}
-
 struct SharedAt
 {
     double* a;
@@ -408,6 +382,7 @@ __global__ void pivotedDiagonal(FactorArgs args, PivotArgs pivots, const std::in
     __shared__ int perm[B];
     __shared__ double sub[B];
     __shared__ std::int32_t oldOrigin[B];
+    __shared__ double products[3 * 16 * 16];
     const std::int32_t s = list[blockIdx.x];
     const FrontDesc f = args.fronts[s];
     const std::int64_t n = f.c + f.r;
@@ -449,18 +424,23 @@ __global__ void pivotedDiagonal(FactorArgs args, PivotArgs pivots, const std::in
             swapped |= perm[j] != j;
         pivots.stepSwapped[s] = swapped;
     }
-    // L11^-1 (unit lower, zero below each 2x2 pivot) into the block's strict upper triangle, as diagonalBlocks does:
-    // the columns of the inverse by forward substitution of e_j, a column per thread at a time.
+    // L11^-1 (unit lower, zero below each 2x2 pivot) into the block's strict upper triangle, as diagonalBlocks does,
+    // by 16 x 16 blocks (the identity beyond kb).
     for (int e = threadIdx.x; e < B * B; e += blockDim.x)
     {
         const int q = e / B;
         const int i = e - q * B;
         if (i >= kb || q >= kb)
-            a[i + q * LD] = 0.0;
+            a[i + q * LD] = i == q ? 1.0 : 0.0;
     }
-    __syncthreads();
-    for (int j = threadIdx.x; j < kb; j += blockDim.x)
-        invertColumn(a, j, kb, block, n);
+    invertUnitLowerBlocked(a, products);
+    for (int e = threadIdx.x; e < kb * kb; e += blockDim.x)
+    {
+        const int i = e / kb;
+        const int j = e - i * kb;
+        if (i < j)
+            block[i + static_cast<std::int64_t>(j) * n] = a[i + j * LD];
+    }
 }
 
 // The rows below step k0's diagonal block of an indefinite front, as products with the block's inverse: the row's

@@ -23,7 +23,10 @@
 #include <cstring>
 #include <functional>
 #include <limits>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -1946,6 +1949,21 @@ private:
         m_tuneReport.clear();
     }
 
+    // The tuner's choices for one structure on one device, kept for the process: a new factor of the same structure
+    // (a fresh pencil of the same model) takes them without timing again.
+    using TuneKey = std::tuple<int, std::int32_t, std::int32_t, std::int64_t, std::size_t>;
+    static std::map<TuneKey, std::vector<TuneRecord>>& tuneCache(std::mutex*& lock)
+    {
+        static std::mutex mutex;
+        static auto* cache = new std::map<TuneKey, std::vector<TuneRecord>>();
+        lock = &mutex;
+        return *cache;
+    }
+    [[nodiscard]] TuneKey tuneKey() const
+    {
+        return {m_device, m_plan.dimension, m_plan.supernodeCount, m_plan.panelValues, m_plan.factorLaunches.size()};
+    }
+
     template <typename Launches> void tune(const Launches& launches)
     {
         constexpr int VARIANTS = 2;
@@ -1955,6 +1973,24 @@ private:
         {
             m_tuned = true; // nothing to choose
             return;
+        }
+        {
+            std::mutex* lock = nullptr;
+            auto& cache = tuneCache(lock);
+            const std::lock_guard<std::mutex> guard(*lock);
+            const auto known = cache.find(tuneKey());
+            if (known != cache.end())
+            {
+                m_tuneReport = known->second;
+                for (Launch& launch : m_plan.factorLaunches)
+                    if (tunable(launch))
+                        for (const TuneRecord& r : m_tuneReport)
+                            if (r.kind == static_cast<std::int32_t>(launch.kind) && r.sizeClass == sizeClass(launch.count))
+                                launch.variant = r.chosen;
+                m_factorGraph.reset();
+                m_tuned = true;
+                return;
+            }
         }
         std::vector<double> seconds(count * VARIANTS, 0.0);
         // the timing runs launch one by one with events around each launch; the caller's profiling setting comes back
@@ -2015,6 +2051,10 @@ private:
                 launch.variant = recordOf(launch).chosen;
         m_factorGraph.reset();
         m_tuned = true;
+        std::mutex* lock = nullptr;
+        auto& cache = tuneCache(lock);
+        const std::lock_guard<std::mutex> guard(*lock);
+        cache[tuneKey()] = m_tuneReport;
     }
 
     // The factor launches in plan order on the main stream, except the side groups (the far part of a finished
@@ -2507,11 +2547,34 @@ public:
             m_offsets.get(), m_rows.get(), m_stiffness.get(), m_mass.get(), shift, m_scale.get(), m_shifted.get(),
             m_dimension);
         check(cudaGetLastError(), "shifted matrix launch");
-        oosgpu_factor_options options{1.0e7, -1, nullptr, 1};
         oosgpu_factor_info info{};
-        m_factor.factorise(m_dimension, m_terms, m_offsets.get(), m_rows.get(), m_shifted.get(), true, &options, &info);
         ++m_factorisations;
         m_shift = shift;
+        // Below the spectrum (a vibration pencil at a shift <= 0: K + |sigma| M; a buckling pencil at 0: K) the
+        // shifted matrix is positive definite whenever its count can be trusted at all, so it is factorised first
+        // without pivots, which a positive definite matrix does not need; a negative or zero pivot sends it to the
+        // pivoted factorisation after all. The inertia is the same either way (Sylvester's law).
+        if (m_buckling ? shift == 0.0 : shift <= 0.0)
+        {
+            oosgpu_factor_options definite{1.0e7, -1, nullptr, 0};
+            bool accepted = false;
+            try
+            {
+                m_factor.factorise(m_dimension, m_terms, m_offsets.get(), m_rows.get(), m_shifted.get(), true,
+                                   &definite, &info);
+                accepted = info.negative == 0 && info.zero == 0;
+            }
+            catch (const Error& e)
+            {
+                if (e.status() != STATUS_SINGULAR)
+                    throw;
+            }
+            if (accepted)
+                return info;
+            info = oosgpu_factor_info{};
+        }
+        oosgpu_factor_options options{1.0e7, -1, nullptr, 1};
+        m_factor.factorise(m_dimension, m_terms, m_offsets.get(), m_rows.get(), m_shifted.get(), true, &options, &info);
         return info;
     }
 
