@@ -79,7 +79,9 @@ def parse():
                              "blocks, step column, device seconds) to PATH as JSON")
     parser.add_argument("--profile-rhs", type=int, default=64, help="with --launch-profile: the solve's columns")
     parser.add_argument("--kernels", choices=["tune", "default", "alternative"], default="tune",
-                        help="with --factor-only: the kernel choice of the launch kinds with two kernels")
+                        help="the kernel choice of the launch kinds with two kernels (statics and --factor-only): the "
+                             "autotuner's, or fixed; fixed for launch lists taken under ncu, whose serialised launches "
+                             "would mislead the tuner's timing")
     parser.add_argument("--detail", metavar="PATH", default=None,
                         help="write the whole result record (kernel tables, every leg's detail) to PATH as JSON; "
                              "without it the record goes to stderr as one line")
@@ -664,6 +666,7 @@ def run_gpu(args, rank, world, local_rank):
     symbolic = SymbolicFactor.from_partition(model.offsets, model.neighbours, model.weights, fixture["node_order"],
                                              fixture["first_position"], fixture["parent"])
     factor = SupernodalFactor(symbolic, device=local_rank)
+    factor.set_tuning(args.kernels)
     stream = torch.cuda.ExternalStream(factor.stream)
     dev = torch.device("cuda", local_rank)
     d_csc = SymmetricCsc(torch.from_numpy(csc.offsets).to(dev), torch.from_numpy(csc.rows).to(dev),
