@@ -102,3 +102,33 @@ def test_replayed_factorisation_is_bitwise_the_same(small_batch, gpu):
     for a, b in zip(first, again):
         assert np.array_equal(a, b)
     factor.close()
+
+
+def test_batch_solutions_match_reference(small_batch, lib, oracle_mod, gpu):
+    """Each panel's block of the joined GPU solve against the reference's own factorisation and solve of that panel
+    alone, on the reference's partition of its ordering: within the bound the reference's two kernel families set
+    (conftest.solution_bound)."""
+    from conftest import relative_columns, solution_bound
+
+    from o_o_solver_b200 import FactorSolve, SupernodalFactor, workloads
+
+    cases, joined, rhs, parts = small_batch
+    factor = SupernodalFactor.factorise(joined.symbolic, joined.matrix)
+    x = np.asfortranarray(rhs.copy())
+    FactorSolve(factor).solve(x)
+    for i, (case, part, xi, bi) in enumerate(zip(cases, parts, joined.split(x), joined.split(rhs))):
+        if i == 4:
+            break
+        model = workloads.Model(workloads.PanelSpec(n=case.n, stringers=case.stringers, thickness=case.thickness))
+        sym = oracle_mod.analyse(model.offsets, model.neighbours, model.weights,
+                                 given_order=fixture_of(case.n)["node_order"])
+        assert np.array_equal(sym.first_column, part.first_column)
+        m = part.matrix
+        solutions = [oracle_mod.factorise(sym, m.offsets, m.rows, m.values, family=f).solve(np.asfortranarray(bi))
+                     for f in (0, 1)]
+        spread = relative_columns(solutions[1], solutions[0]).max()
+        difference = relative_columns(xi, solutions[0]).max()
+        print(f"panel {i} ({part.dof_count} equations): difference {difference:.2e} (reference families {spread:.2e})")
+        assert difference <= solution_bound(spread), (i, difference, spread)
+        model.close()
+    factor.close()
