@@ -371,10 +371,26 @@ __device__ __forceinline__ void sharedTileProduct(const double* a, int lda, cons
 
 // C -= A B (D) on one 64 x 64 tile (tileAccumulate), C read, reduced and written once; op.lower keeps the elements
 // ii + lowerOffset >= jj only.
+// The lines of C's tile (column-major: op.cRowStride 1) asked into L2 ahead of the product, so that the epilogue's
+// read of C, after K columns of products, finds them there instead of in HBM.
+__device__ __forceinline__ void prefetchColumnTile(const TileOperands& op)
+{
+    // 64 columns of up to 64 rows: 512 bytes, four 128-byte lines, per column
+    const int column = threadIdx.x >> 1;
+    if (op.cRowStride != 1 || column >= op.n)
+        return;
+    const double* top = op.c + column * op.cColStride;
+    for (int line = (threadIdx.x & 1) * 2; line < (threadIdx.x & 1) * 2 + 2; ++line)
+        if (line * 16 < op.m)
+            asm volatile("prefetch.global.L2 [%0];\n" ::"l"(top + line * 16));
+}
+
 template <bool A_BY_ROWS = false>
 __device__ __forceinline__ void tileProduct(const TileOperands& op, double* smem)
 {
     TileAccumulators acc;
+    if (op.k >= 2 * TILE_SLICE * TILE_STAGES)
+        prefetchColumnTile(op);
     tileAccumulate<A_BY_ROWS>(op, smem, acc);
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
