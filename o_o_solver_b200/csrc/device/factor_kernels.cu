@@ -789,7 +789,7 @@ __global__ void __launch_bounds__(TILE_THREADS) panelRowsInverse(FactorArgs args
 
 // Trailing panel update: the tile (i0, j0) of the panel's columns minus the products with the K = task.k0 columns from
 // k0 (a 64-column step within its macro panel, or a finished macro panel of PANEL_MACRO columns).
-__global__ void __launch_bounds__(TILE_THREADS) panelUpdate(FactorArgs args, const TileTask* tasks, int k0)
+__global__ void __launch_bounds__(TILE_THREADS, 5) panelUpdate(FactorArgs args, const TileTask* tasks, int k0)
 {
     __shared__ double smem[TILE_SMEM_DOUBLES];
     const TileTask task = tasks[blockIdx.x];

@@ -523,7 +523,7 @@ __global__ void __launch_bounds__(TILE_THREADS) backwardSmall(SolveArgs a, const
 // x_F -= L21^T X[R(s)] for a large supernode, by tiles of 64 of its columns (A = L21^T read along its rows). A task
 // covers the rows [j0, j0 + SOLVE_ROWS_CHUNK) of R(s) and writes its partial product to slot k0 when R(s) is split
 // (k0 >= 0), or all of R(s) straight into x_F (k0 = -1).
-__global__ void __launch_bounds__(TILE_THREADS) backwardRows(SolveArgs a, const TileTask* tasks)
+__global__ void __launch_bounds__(TILE_THREADS, 5) backwardRows(SolveArgs a, const TileTask* tasks)
 {
     __shared__ double smem[TILE_SMEM_DOUBLES];
     const TileTask task = tasks[blockIdx.x];
