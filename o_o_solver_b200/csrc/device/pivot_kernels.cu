@@ -626,7 +626,7 @@ __global__ void identityPermutation(std::int32_t* perm, int dimension)
 // A tile of the trailing front minus L W^T over the K = task.k0 columns from k0 (a step's columns within its macro
 // panel, or a finished macro panel's): task (front, i0, j0) a 64 x 64 tile of the front, j0 < c in the panel, j0 >= c
 // in the update matrix (tiles never straddle c); W's columns for k0 at slice k0 % PANEL_MACRO of the front's buffer.
-__global__ void __launch_bounds__(TILE_THREADS) updatePivoted(FactorArgs args, PivotArgs pivots, const TileTask* tasks,
+__global__ void __launch_bounds__(TILE_THREADS, 5) updatePivoted(FactorArgs args, PivotArgs pivots, const TileTask* tasks,
                                                               int k0)
 {
     __shared__ double smem[TILE_SMEM_DOUBLES];
