@@ -56,6 +56,11 @@ enum
 const char* oosgpu_last_error(void);
 /* 1 when a CUDA device is usable, 0 otherwise (the library never falls back to the CPU). */
 int oosgpu_device_count(void);
+/* The eigenvalue solves keep the device buffers of their workspaces and eigenvectors in a process-wide cache once
+ * freed (at most 4 GiB), so that later solves allocate nothing. This frees the idle ones of `device` (-1: of every
+ * device) and returns the bytes freed: to give the memory back, and before a cudaDeviceReset, after which cached
+ * buffers would belong to a destroyed context (destroy every handle first). */
+int64_t oosgpu_release_cached_buffers(int device);
 
 /* ---- symbolic structure ---------------------------------------------------------------------------------------- */
 typedef struct oosgpu_symbolic oosgpu_symbolic;

@@ -59,6 +59,7 @@ class LanczosOptions(ctypes.Structure):
 SIGNATURES = [
     ("oosgpu_last_error", ctypes.c_char_p, []),
     ("oosgpu_device_count", ctypes.c_int, []),
+    ("oosgpu_release_cached_buffers", ctypes.c_int64, [ctypes.c_int]),
     ("oosgpu_symbolic_create", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _i32p, _i32p, _i64p, _i32p,
                                               ctypes.POINTER(_vp)]),
     ("oosgpu_symbolic_from_partition", ctypes.c_int, [ctypes.c_int32, _i64p, _i32p, _i32p, _i32p, ctypes.c_int32,

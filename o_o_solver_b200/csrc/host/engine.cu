@@ -2753,6 +2753,11 @@ extern "C" const char* oosgpu_last_error(void)
     return oosgpu::g_lastError.c_str();
 }
 
+extern "C" int64_t oosgpu_release_cached_buffers(int device)
+{
+    return static_cast<int64_t>(oosgpu::eigen::releaseDeviceBuffers(device));
+}
+
 extern "C" int oosgpu_device_count(void)
 {
     int count = 0;

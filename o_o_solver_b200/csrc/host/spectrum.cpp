@@ -127,6 +127,28 @@ void giveDeviceBuffer(double* p, std::size_t bytes, int device) noexcept
     cudaFree(p);
 }
 
+std::size_t releaseDeviceBuffers(int device) noexcept
+{
+    BufferCache& cache = bufferCache();
+    const std::lock_guard<std::mutex> guard(cache.lock);
+    std::size_t freed = 0;
+    int current = 0;
+    cudaGetDevice(&current);
+    for (auto it = cache.idle.begin(); it != cache.idle.end();)
+        if (device < 0 || it->first.first == device)
+        {
+            cudaSetDevice(it->first.first);
+            cudaFree(it->second);
+            freed += it->first.second;
+            cache.idleBytes -= it->first.second;
+            it = cache.idle.erase(it);
+        }
+        else
+            ++it;
+    cudaSetDevice(current);
+    return freed;
+}
+
 void DeviceFree::operator()(double* p) const noexcept
 {
     giveDeviceBuffer(p, bytes, device);

@@ -107,6 +107,8 @@ struct ShiftLog
 // workspace was measured at up to 1.1 s on a B200 holding a large factor.
 double* takeDeviceBuffer(std::size_t bytes, const char* what);
 void giveDeviceBuffer(double* p, std::size_t bytes, int device) noexcept;
+// Frees every idle buffer of the cache (device -1: of every device); returns the bytes freed.
+std::size_t releaseDeviceBuffers(int device) noexcept;
 
 struct DeviceFree
 {

@@ -63,6 +63,12 @@ def device_count() -> int:
     return int(nat.load().oosgpu_device_count())
 
 
+def release_cached_buffers(device: int = -1) -> int:
+    """Frees the idle device buffers the eigenvalue solves keep for reuse (of `device`, or of every device); returns
+    the bytes freed."""
+    return int(nat.load().oosgpu_release_cached_buffers(int(device)))
+
+
 # ---- symbolic structure ----------------------------------------------------------------------------------------------
 
 

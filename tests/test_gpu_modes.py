@@ -224,3 +224,20 @@ def test_modes_match_golden(name, lib, gpu):
     assert solution.factorisation_count == int(golden["factorisations"])
     residual, gram = pair_residuals(k, m, solution.eigenvalues, solution.eigenvectors)
     assert np.abs(gram - np.eye(len(expected))).max() <= 1e-10
+
+
+def test_cached_buffers_are_reused_and_released(lib, oracle_mod, gpu):
+    """The solves keep their freed device buffers for the next solve; releasing them frees memory (and nothing the
+    second time), and a solve after the release still gives the same eigenvalues."""
+    from o_o_solver_b200 import SparsePencil, linalg
+    from o_o_solver_b200.eigen import BlockLanczos, EigenRequest, LanczosOptions
+
+    sym, symbolic, k, m = problem("hex", 8, oracle_mod)
+    pencil = SparsePencil(symbolic, k, m)
+    solver = BlockLanczos(LanczosOptions(block_size=8))
+    first = solver.solve(pencil, EigenRequest(mode_count=10), vectors=False)
+    assert linalg.release_cached_buffers() > 0
+    assert linalg.release_cached_buffers() == 0
+    again = solver.solve(pencil, EigenRequest(mode_count=10), vectors=False)
+    assert np.array_equal(first.eigenvalues, again.eigenvalues)
+    pencil.close()
