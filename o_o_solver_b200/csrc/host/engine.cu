@@ -192,10 +192,13 @@ std::uintptr_t keyOf(const void* p)
 class GpuFactor
 {
 public:
-    GpuFactor(const Symbolic& symbolic, int device) : m_symbolic(symbolic), m_device(device)
+    // prebuilt: the structure's plan when the caller has it already (a copy is taken: the factor's own choices change
+    // its launches), else it is built here.
+    GpuFactor(const Symbolic& symbolic, int device, const Plan* prebuilt = nullptr)
+        : m_symbolic(symbolic), m_device(device)
     {
         check(cudaSetDevice(device), "cudaSetDevice");
-        m_plan = buildPlan(symbolic);
+        m_plan = prebuilt != nullptr ? *prebuilt : buildPlan(symbolic);
         // The main stream at the highest priority, the lookahead's side stream at the lowest: when an SM frees up,
         // the chain of a front's steps (one or a few blocks a launch) is scheduled before the side's update tiles.
         int leastPriority = 0;
@@ -2440,7 +2443,25 @@ struct oosgpu_symbolic
     oosgpu::Symbolic symbolic;
     std::int32_t levels = 0;
     std::int64_t updateValues = 0;
+    // The launch plan of the structure, built by the first factor or pencil made on it and copied by the later ones
+    // (on the 60^3 block the build takes about half a second; a fresh pencil of the same model then skips it).
+    std::mutex planLock;
+    std::shared_ptr<const oosgpu::Plan> plan;
 };
+
+namespace
+{
+
+const oosgpu::Plan* planOf(const oosgpu_symbolic* handle)
+{
+    auto* s = const_cast<oosgpu_symbolic*>(handle);
+    const std::lock_guard<std::mutex> guard(s->planLock);
+    if (!s->plan)
+        s->plan = std::make_shared<const oosgpu::Plan>(oosgpu::buildPlan(s->symbolic));
+    return s->plan.get();
+}
+
+} // namespace
 
 struct oosgpu_factor
 {
@@ -2464,8 +2485,9 @@ public:
     // the shifted matrix K - sigma B = K + sigma K_d rounds as the reference's combine(1, K, sigma, K_d); the inner
     // product is K's).
     GpuPencil(const Symbolic& symbolic, int device, std::int32_t dimension, const std::int64_t* offsets,
-              const std::int32_t* rows, const double* stiffness, const double* mass, bool buckling = false)
-        : m_factor(symbolic, device), m_device(device), m_dimension(dimension), m_buckling(buckling)
+              const std::int32_t* rows, const double* stiffness, const double* mass, bool buckling = false,
+              const Plan* prebuilt = nullptr)
+        : m_factor(symbolic, device, prebuilt), m_device(device), m_dimension(dimension), m_buckling(buckling)
     {
         const char* name = buckling ? "BucklingPencil" : "SparsePencil";
         if (dimension != symbolic.dofCount)
@@ -2889,7 +2911,7 @@ extern "C" int oosgpu_factor_create(const oosgpu_symbolic* symbolic, int device,
             requirePointer(symbolic, "symbolic");
             requirePointer(out, "out");
             auto handle = std::make_unique<oosgpu_factor>();
-            handle->factor = std::make_unique<oosgpu::GpuFactor>(symbolic->symbolic, device);
+            handle->factor = std::make_unique<oosgpu::GpuFactor>(symbolic->symbolic, device, planOf(symbolic));
             *out = handle.release();
         });
 }
@@ -3299,7 +3321,7 @@ extern "C" int oosgpu_pencil_create(const oosgpu_symbolic* symbolic, int device,
             requirePointer(out, "out");
             auto handle = std::make_unique<oosgpu_pencil>();
             handle->pencil = std::make_unique<oosgpu::GpuPencil>(symbolic->symbolic, device, dimension, col_offsets,
-                                                                 rows, stiffness, mass);
+                                                                 rows, stiffness, mass, false, planOf(symbolic));
             *out = handle.release();
         });
 }
@@ -3319,7 +3341,8 @@ extern "C" int oosgpu_pencil_create_buckling(const oosgpu_symbolic* symbolic, in
             requirePointer(out, "out");
             auto handle = std::make_unique<oosgpu_pencil>();
             handle->pencil = std::make_unique<oosgpu::GpuPencil>(symbolic->symbolic, device, dimension, col_offsets,
-                                                                 rows, stiffness, differential, true);
+                                                                 rows, stiffness, differential, true,
+                                                                 planOf(symbolic));
             *out = handle.release();
         });
 }
