@@ -178,6 +178,45 @@ def fp64_gemm_peak(torch, device):
     return best / 1e12
 
 
+def library_same_shapes(torch, device, symbolic, weights, fixture, small_order=128):
+    """The update matrices of the factorisation done by the library instead: for every front above the small-front
+    order with rows below its columns (c columns, r rows below), the product L_r L_r^T of an r x c block with itself,
+    as one batched cuBLAS DGEMM (torch.bmm float64) per distinct (r, c), full r x r results (cuBLAS has no batched
+    symmetric rank-k update). Device time of all the groups, best of 3, and its rate over the full products' 2 r^2 c
+    flops; the fronts and their shapes come from the symbolic structure."""
+    row_start, _ = symbolic.row_structure()
+    r = np.diff(row_start)
+    columns_before = np.concatenate([[0], np.cumsum(np.asarray(weights)[fixture["node_order"]])])
+    first = np.asarray(fixture["first_position"])
+    c = columns_before[first[1:]] - columns_before[first[:-1]]
+    chosen = (c + r > small_order) & (r > 0)
+    shapes = {}
+    for rr, cc in zip(r[chosen].tolist(), c[chosen].tolist()):
+        shapes[(rr, cc)] = shapes.get((rr, cc), 0) + 1
+    groups = []
+    for (rr, cc), count in shapes.items():
+        per_batch = max(1, min(count, (1 << 27) // (rr * rr + rr * cc)))  # at most 1 GiB of operands and results
+        for first_front in range(0, count, per_batch):
+            batch = min(per_batch, count - first_front)
+            groups.append(torch.randn(batch, rr, cc, dtype=torch.float64, device=device))
+    flops = sum(2.0 * g.shape[0] * g.shape[1] * g.shape[1] * g.shape[2] for g in groups)
+    best = None
+    for _ in range(4):
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record()
+        for g in groups:
+            torch.bmm(g, g.transpose(1, 2))
+        stop.record()
+        torch.cuda.synchronize()
+        seconds = start.elapsed_time(stop) / 1e3
+        best = seconds if best is None else min(best, seconds)  # the first run warms cuBLAS up
+    del groups
+    torch.cuda.empty_cache()
+    return {"fronts": int(chosen.sum()), "shapes": len(shapes), "ms": round(best * 1e3, 3),
+            "tflops": round(flops / best / 1e12, 2)}
+
+
 def accuracy(csc, x, b):
     """(largest relative residual ||b - Ax||_2/||b||_2, largest normwise backward error
     ||b - Ax||_inf / (||A||_inf ||x||_inf + ||b||_inf)) over the columns, on the host."""
@@ -754,6 +793,11 @@ def run_gpu(args, rank, world, local_rank):
                     "kernel": dominant, "launches": d["launches"],
                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor)",
                     "share": d["seconds"] / sum(v["seconds"] for v in stats.values())}
+        if dominant == "update_matrix":
+            # The same update matrices by the library, against this kernel's own event time (`ms`).
+            roofline["library_same_shapes"] = {
+                **library_same_shapes(torch, dev, symbolic, model.weights, fixture),
+                "kernel_ms": round(d["seconds"] * 1e3, 3)}
     else:
         achieved = d["bytes"] / d["seconds"] / 1e9
         traffic, traffic_source = measured_traffic(dominant, d["bytes"] / d["launches"])
@@ -828,7 +872,7 @@ def compact_line(full):
                                           "cpu_baseline", "factor_tflops")})
     line["refinement"] = _pick(full.get("refinement"), "steps", "factor_seconds", "solve_seconds")
     line["roofline"] = _pick(full.get("roofline"), "bound", "achieved", "peak", "unit", "frac", "traffic", "kernel",
-                             "launches", "share", "peak_source")
+                             "launches", "share", "peak_source", "library_same_shapes")
     modes = full.get("modes")
     if modes:
         line["modes"] = _pick(modes, "value", "unit", "factorisations", "block_steps", "verified",
