@@ -37,7 +37,9 @@ def full_record():
         "roofline": {"bound": "tensor", "achieved": 21.6, "peak": 35.5, "unit": "TFLOP/s", "frac": 0.61,
                      "traffic": 1.19e9, "traffic_source": "hex30: 1.280 x the algorithmic bytes",
                      "algorithmic_bytes_per_launch": 9.3e8, "kernel": "update_matrix", "launches": 16,
-                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor)", "share": 0.3},
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor)", "share": 0.3,
+                     "library_same_shapes": {"fronts": 17091, "shapes": 182, "ms": 39.442, "tflops": 29.63,
+                                             "kernel_ms": 25.365}},
         "kernels": kernels,
         "clocks": {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": [], "samples": 40},
         "cpu_baseline": {"value": 4.957, "unit": "s", "cores": 16, "kind": "reference",
@@ -105,3 +107,45 @@ def test_reference_arm_loads_nothing_of_the_package():
     assert result["impl"] == "reference" and result["value"] > 0 and result["config"]["equations"] == 60600
     isolation = json.loads(lines[-1])
     assert isolation == {"modules": [], "library": False}
+
+
+def test_library_same_shapes_takes_the_large_fronts_of_the_symbolic_structure():
+    """The library comparison's fronts: column counts from the node partition and rows from the symbolic structure
+    give back the structure's panel values, and the fronts taken are the large ones with rows below (r > 0)."""
+    import types
+
+    import numpy as np
+    import torch
+
+    from o_o_solver_b200 import SymbolicFactor
+
+    model, fixture, _, _ = bench.load_workload("plate100")
+    symbolic = SymbolicFactor.from_partition(model.offsets, model.neighbours, model.weights, fixture["node_order"],
+                                             fixture["first_position"], fixture["parent"])
+    row_start, _ = symbolic.row_structure()
+    r = np.diff(row_start)
+    before = np.concatenate([[0], np.cumsum(np.asarray(model.weights)[fixture["node_order"]])])
+    first = np.asarray(fixture["first_position"])
+    c = before[first[1:]] - before[first[:-1]]
+    assert int((c * (c + r)).sum()) == symbolic.panel_value_count
+
+    class Event:
+        def __init__(self, **_):
+            self.at = 0.0
+
+        def record(self):
+            import time
+            self.at = time.perf_counter()
+
+        def elapsed_time(self, other):
+            return max((other.at - self.at) * 1e3, 1e-6)
+
+    host_torch = types.SimpleNamespace(randn=torch.randn, float64=torch.float64, bmm=torch.bmm,
+                                       cuda=types.SimpleNamespace(Event=Event, synchronize=lambda: None,
+                                                                  empty_cache=lambda: None))
+    result = bench.library_same_shapes(host_torch, "cpu", symbolic, model.weights, fixture)
+    large = (c + r > 128) & (r > 0)
+    assert result["fronts"] == int(large.sum())
+    assert result["shapes"] == len(set(zip(r[large].tolist(), c[large].tolist())))
+    assert result["ms"] > 0 and result["tflops"] > 0
+    symbolic.close()
