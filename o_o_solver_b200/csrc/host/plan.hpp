@@ -18,9 +18,9 @@ namespace oosgpu
 constexpr int SMALL_ORDER_LOW = 64;
 constexpr int SMALL_ORDER_MIDDLE = 96;
 constexpr int SMALL_ORDER = 128;
-// The columns of a large front's assembly piece: about this many elements of its lower triangle. Small pieces keep a
-// piece's target lines in L2 between its clear and its children's additions (2 M plate: 2^16 10.6 ms, 2^14 9.2 ms,
-// 2^13 9.0 ms a factorisation).
+// The columns of a large front's assembly piece: about this many elements of its lower triangle. Smaller pieces
+// measured faster (2 M plate: 2^16 10.6 ms, 2^14 9.2 ms, 2^13 9.0 ms a factorisation), as expected if a piece's
+// target lines stay in L2 between its clear and its children's additions; no DRAM counters were taken for it.
 constexpr std::int64_t ASSEMBLY_PIECE_VALUES = std::int64_t{1} << 13;
 // Supernodes with at most this many columns are swept by one block.
 constexpr int SOLVE_SMALL_COLUMNS = 64;
